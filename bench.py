@@ -1,0 +1,390 @@
+#!/usr/bin/env python
+"""Benchmark of the compressible staggered FHD RK3 step (cell-updates/s).
+
+Workload (default): 'single-species' argon in the reference's parity form (two
+identical species), 256^3 cells, dx = 1e-6 cm, fully periodic, FP64, in-kernel
+Philox noise, dt from the acoustic + diffusive stability rule.  One step = one
+SSP-RK3 step of the whole box.  value = cells * steps * ranks / max-over-ranks
+device time; e2e = the same metric through the host-buffer C-ABI call
+(fhd_rk3_step_stag_host: H2D of cu/mom/prim/vel from pinned memory, step, D2H).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+                  [--n 256] [--ns 2] [--precision fp64|mixed] [--tile auto|<idx>]
+
+N > 1 runs one independent replica per GPU (weak scaling, no data-path
+collective; the runs do not exchange data).  --impl reference times the
+reference algorithm's CPU implementation (the oracle restatement, OpenMP over
+all host cores) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+try:
+    _CORES = len(os.sched_getaffinity(0))
+except AttributeError:  # pragma: no cover
+    _CORES = os.cpu_count() or 1
+os.environ.setdefault("OMP_NUM_THREADS", str(_CORES))
+
+HBM_FALLBACK_GBS = 6650.0
+METRIC = "cell-updates/s (RK3 steps x cells)"
+UNIT = "cell-updates/s"
+
+# DRAM traffic (read + write bytes) of one k_stage launch from an ncu capture,
+# scaled per cell; see profiles/k_stage_argon_ncu.md.  None until captured.
+STAGE_TRAFFIC_BYTES_PER_CELL = {}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+def make_params(args):
+    from fhdex_b200.params import argon, mixture4
+    prec = 1 if args.precision == "mixed" else 0
+    if args.ns == 2:
+        return argon(args.n, dx=args.dx, precision=prec, seed=args.seed)
+    if args.ns == 4:
+        return mixture4(args.n, dx=args.dx, precision=prec, seed=args.seed)
+    raise SystemExit("--ns must be 2 (argon parity form) or 4 (mixture)")
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_oracle_rate(p, target_s=15.0, max_n=None):
+    """Oracle (CPU restatement of the reference step, OpenMP over all host cores)
+    on a bounded sample: a smaller box of the same gas, enough steps for about
+    target_s seconds.  Returns (cell-updates/s, sample description)."""
+    from oracle import oracle as O
+    from fhdex_b200.params import stable_dt
+    from fhdex_b200.state import StagState, StepNoise
+    O.build()
+    n = min(64, p.n_cells[0]) if max_n is None else max_n
+    q = p.replace(n_cells=(n, n, n), prob_hi=tuple(p.dx[0] * n for _ in range(3)))
+    st = StagState(q)
+    O.init_state(st, q)
+    dt = stable_dt(p)
+    nz = StepNoise(q)
+    O.fill_step_noise(nz, q.seed, 0)
+    t = time.perf_counter()
+    O.rk3_step(st, nz, dt)  # calibration step (not counted)
+    one = time.perf_counter() - t
+    steps = max(1, int(target_s / max(one, 1e-3)))
+    t = time.perf_counter()
+    for s in range(steps):
+        O.fill_step_noise(nz, q.seed, s + 1)  # the reference fills its A/B noise every step
+        rc = O.rk3_step(st, nz, dt)
+        assert rc == 0
+    el = time.perf_counter() - t
+    return n ** 3 * steps / el, f"{n}^3 box of the same gas, {steps} RK3 steps incl. per-step noise fill, {el:.1f} s"
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU algorithm (oracle restatement) on the
+    host cores, rank 0 only; each step is a bounded sample of the workload."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    p = make_params(args)
+    from oracle import oracle as O
+    from fhdex_b200.params import stable_dt
+    from fhdex_b200.state import StagState, StepNoise
+    O.build()
+    # size the sample so that warmup + steps take about two minutes at most
+    n = 32
+    q = p.replace(n_cells=(n, n, n), prob_hi=tuple(p.dx[0] * n for _ in range(3)))
+    st = StagState(q)
+    O.init_state(st, q)
+    nz = StepNoise(q)
+    dt = stable_dt(p)
+    t = time.perf_counter()
+    O.fill_step_noise(nz, q.seed, 0)
+    O.rk3_step(st, nz, dt)
+    per_cell = (time.perf_counter() - t) / n ** 3
+    budget = 100.0 / max(1, args.steps + args.warmup)
+    n = int((budget / per_cell) ** (1 / 3))
+    n = max(16, min(p.n_cells[0], (n // 8) * 8))
+    q = p.replace(n_cells=(n, n, n), prob_hi=tuple(p.dx[0] * n for _ in range(3)))
+    st = StagState(q)
+    O.init_state(st, q)
+    nz = StepNoise(q)
+    for s in range(args.warmup):
+        O.fill_step_noise(nz, q.seed, s)
+        O.rk3_step(st, nz, dt)
+    t = time.perf_counter()
+    for s in range(args.steps):
+        O.fill_step_noise(nz, q.seed, args.warmup + s)
+        rc = O.rk3_step(st, nz, dt)
+        assert rc == 0
+    el = time.perf_counter() - t
+    val = n ** 3 * args.steps / el
+    sample = f"each step: one RK3 step of a {n}^3 box of the same gas (incl. A/B noise fill), CPU oracle"
+    out = {
+        "metric": METRIC, "value": val, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(args, p, dt, None),
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": _CORES, "kind": "port", "sample": sample},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def config_dict(args, p, dt, tile):
+    return {
+        "workload": (f"{'argon (2 identical species)' if p.nspecies == 2 else '4-species mixture'} "
+                     f"{p.n_cells[0]}^3, dx={p.dx[0]:g} cm, periodic, {args.precision}, in-kernel Philox noise"),
+        "n_cells": list(p.n_cells), "nspecies": p.nspecies, "precision": args.precision, "dt_s": dt,
+        "noise": "philox-4x32-10 in kernel", "tile": tile,
+        "l2": "inputs larger than L2 (state ~%.1f GB)" % (state_gb(p)),
+        "parallelism": f"replicas x{args.gpus}",
+    }
+
+
+def state_gb(p):
+    n = [c + 4 for c in p.n_cells]
+    cells = n[0] * n[1] * n[2]
+    return (p.nvars + p.nprimvars + 6) * cells * 8 / 1e9
+
+
+def autotune(ctx, st, dt, steps=2):
+    """Own tile autotuner: time each tile shape of the fused stage kernel on this
+    problem and keep the fastest."""
+    import torch
+    from fhdex_b200.context import Context
+    best = None
+    for t, name in enumerate(Context.tiles()):
+        ctx.set_tile(t)
+        ctx.rk3_step(st, dt, 0, aux=False)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for s in range(steps):
+            ctx.rk3_step(st, dt, s, aux=False)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        if best is None or ms < best[1]:
+            best = (t, ms, name)
+    ctx.set_tile(best[0])
+    return best
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from fhdex_b200.context import Context
+    from fhdex_b200.params import stable_dt
+    from fhdex_b200.state import StagState
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    p = make_params(args)
+    dt = stable_dt(p)
+    ctx = Context(p, local)
+    st = StagState(p, f"cuda:{local}", aux=False)
+    ctx.init_state(st)
+    if args.tile == "auto":
+        t, ms, tname = autotune(ctx, st, dt)
+    else:
+        ctx.set_tile(int(args.tile))
+        tname = Context.tiles()[int(args.tile)]
+    for s in range(args.warmup):
+        ctx.rk3_step(st, dt, s, aux=False)
+    torch.cuda.synchronize()
+    ctx.profile(True)
+    ctx.profile_read()
+    clocks = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for s in range(args.steps):
+        ctx.rk3_step(st, dt, args.warmup + s, aux=False)
+    e1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    ms = e0.elapsed_time(e1)
+    status = ctx.status()
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = t.item()
+    cells = p.n_cells[0] * p.n_cells[1] * p.n_cells[2]
+    value = cells * args.steps * world / (ms / 1e3)
+    launches = sum(v[1] for v in prof.values())
+
+    # roofline of the dominant kernel (k_stage): algorithmic bytes per launch from
+    # the per-stage state traffic (stage 1: 2 S, stages 2-3: 3 S doubles per cell,
+    # S = 5 + nspecies) over its CUDA-event launch duration on the launching stream
+    S = 5 + p.nspecies
+    stage_ms, stage_n = prof["stage"]
+    avg_launch_s = stage_ms / 1e3 / max(stage_n, 1)
+    alg_bytes = (2 + 3 + 3) / 3.0 * S * 8 * cells
+    peak, peak_kind = measured_peak()
+    achieved = alg_bytes / avg_launch_s / 1e9
+    key = f"{p.nspecies}:{args.precision}"
+    traffic = STAGE_TRAFFIC_BYTES_PER_CELL.get(key)
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic * cells if traffic else None, "peak_kind": peak_kind,
+            "kernel": "k_stage (fused fluxes + divergence + RK3 combination)",
+            "kernel_ms_per_launch": 1e3 * avg_launch_s,
+            "step_breakdown_ms": {k: v[0] / args.steps for k, v in prof.items()}}
+
+    # e2e through the host-buffer C-ABI call (H2D + step + D2H, pinned memory)
+    ctx.close()
+    del st
+    torch.cuda.empty_cache()
+    e2e = None
+    if not args.no_e2e:
+        ctx = Context(p, local)
+        hs = StagState(p, "cpu", aux=False, pin_memory=True)
+        tmp = StagState(p, f"cuda:{local}", aux=False)
+        ctx.init_state(tmp)
+        torch.cuda.synchronize()
+        hs.copy_from(tmp)
+        del tmp
+        torch.cuda.empty_cache()
+        ctx.rk3_step_host(hs, dt, 0)  # warm
+        ne = max(2, min(args.steps, 5))
+        if world > 1:
+            dist.barrier()
+        t = time.perf_counter()
+        for s in range(ne):
+            h2d, d2h = ctx.rk3_step_host(hs, dt, 1 + s)
+        el = time.perf_counter() - t
+        if world > 1:
+            tt = torch.tensor([el], device=f"cuda:{local}", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            el = tt.item()
+        e2e = {"value": cells * ne * world / el, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "steps": ne, "path": "fhd_rk3_step_stag_host (pinned host fabs)"}
+        ctx.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, sample = cpu_oracle_rate(p)
+        cpu = {"value": v, "unit": UNIT, "cores": _CORES, "kind": "port", "sample": sample}
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+        "data": "synthetic (uniform argon at rest + in-kernel Philox noise; no dataset)",
+        "config": config_dict(args, p, dt, tname),
+        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+        "clocks": clk, "status": status,
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--ns", type=int, default=2)
+    ap.add_argument("--dx", type=float, default=1e-6)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--tile", default="auto")
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

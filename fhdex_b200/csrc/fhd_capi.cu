@@ -1,0 +1,698 @@
+// fhd_capi.cu — the C ABI declared in include/fhd_capi.h: context, argument
+// validation, the fused RK3 step and the drop-in operators.  Host code only; the
+// kernels live in fhd_kern_ns.cu / fhd_exact.cu.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "fhd_host.h"
+
+using namespace fhd;
+
+struct fhd_ctx {
+    fhd_params prm;
+    int device = 0;
+    cudaStream_t own = nullptr;
+    cudaStream_t stream = nullptr;
+    int* d_status = nullptr;
+    // stage scratch: cup, cup2 (cells, nvars comps, 2 ghosts) and their face momenta
+    double* scratch = nullptr;
+    size_t scratch_bytes = 0;
+    fhd_fab cup{}, cup2{}, cupm[3]{}, cup2m[3]{};
+    // coefficient scratch (f64 for the exact path when the caller passes none; f32 mixed)
+    void* coef = nullptr;
+    size_t coef_bytes = 0;
+    int coef_dtype = -1;
+    fhd_fab ceta{}, czeta{}, ckappa{}, cchi{}, cD{};
+    int tile = 0;
+    // device mirrors for the host-buffer step
+    double* hbuf = nullptr;
+    size_t hbuf_bytes = 0;
+    // CUDA-event timing per kernel kind
+    bool prof = false;
+    struct Ev { cudaEvent_t a, b; int kind; };
+    std::vector<Ev> evs;
+    size_t nev = 0;
+};
+
+namespace {
+
+const int NGC = 2;
+
+int64_t fab_points(const fhd_fab& f) {
+    int64_t n = 1;
+    for (int d = 0; d < 3; ++d) n *= (int64_t)(f.hi[d] - f.lo[d] + 1);
+    return n;
+}
+
+fhd_fab make_fab(void* data, const int n[3], const int nodal[3], int ng, int nc, int dtype) {
+    fhd_fab f;
+    f.data = data;
+    for (int d = 0; d < 3; ++d) {
+        f.lo[d] = -ng;
+        f.hi[d] = n[d] - 1 + nodal[d] + ng;
+        f.nodal[d] = nodal[d];
+    }
+    f.ncomp = nc;
+    f.dtype = dtype;
+    return f;
+}
+
+const int CELLN[3] = {0, 0, 0};
+const int FACEN[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+const int EDGEN[3][3] = {{1, 1, 0}, {1, 0, 1}, {0, 1, 1}};
+const int EFLUXN[6][3] = {{1, 1, 0}, {1, 0, 1}, {1, 1, 0}, {0, 1, 1}, {1, 0, 1}, {0, 1, 1}};
+
+// A fab must be a one-box MultiFab of the context's domain with the given
+// centring, a uniform ghost width >= min_ng and >= min_nc components.
+bool fab_ok(const fhd_ctx* c, const fhd_fab& f, const int nodal[3], int min_ng, int min_nc, int dtype,
+            int exact_ng = -1) {
+    if (!f.data || f.dtype != dtype || f.ncomp < min_nc) return false;
+    const int g = -f.lo[0];
+    if (g < min_ng || (exact_ng >= 0 && g != exact_ng)) return false;
+    for (int d = 0; d < 3; ++d) {
+        if (f.lo[d] != -g || f.nodal[d] != nodal[d]) return false;
+        if (f.hi[d] != c->prm.n_cells[d] - 1 + nodal[d] + g) return false;
+    }
+    return true;
+}
+
+DevParams make_dev(const fhd_ctx* c, double dt, uint64_t step) {
+    const fhd_params& p = c->prm;
+    DevParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.ns = p.nspecies;
+    P.nvars = 5 + p.nspecies;
+    P.nprim = 6 + 2 * p.nspecies;
+    for (int d = 0; d < 3; ++d) {
+        P.n[d] = p.n_cells[d];
+        P.dx[d] = (p.prob_hi[d] - p.prob_lo[d]) / p.n_cells[d];
+        P.grav[d] = p.grav[d];
+    }
+    P.dt = dt;
+    P.volinv = 1. / (P.dx[0] * P.dx[1] * P.dx[2]);
+    P.dtinv = 1. / dt;
+    P.k_B = p.k_B;
+    P.Runiv = p.Runiv;
+    P.zeta_ratio = p.zeta_ratio;
+    P.visc_type = p.visc_type;
+    P.advection_type = p.advection_type;
+    P.stoch = p.stoch_stress_form;
+    const double AKL = 1.0, BKL = 1.0, CKL = 1.0;
+    for (int i = 0; i < MAXS; ++i) {
+        P.molmass[i] = p.molmass[i];
+        P.hcv[i] = p.hcv[i];
+        P.hcp[i] = p.hcp[i];
+        P.e0[i] = p.e0[i];
+        P.mm[i] = p.molmass[i] * (p.k_B / p.Runiv);
+        P.mmkB[i] = P.mm[i] * p.k_B;
+    }
+    for (int i = 0; i < MAXS; ++i)
+        for (int j = 0; j < MAXS; ++j) {
+            P.diam[i][j] = 0.5 * (p.diameter[i] + p.diameter[j]);
+            P.mu[i][j] = P.mm[i] * P.mm[j] / (P.mm[i] + P.mm[j]);
+            P.msum[i][j] = P.mm[i] + P.mm[j];
+            P.vfac[i][j] = 1.0 + 0.6 * P.mm[j] / P.mm[i] * AKL;
+            P.kfac[i][j] = 7.5 * P.mm[i] / P.mm[j] + 6.25 * P.mm[j] / P.mm[i] - 3.0 * P.mm[j] / P.mm[i] * BKL + 4.0 * AKL;
+        }
+    for (int i = 0; i < MAXS; ++i) P.eta1pre[i] = 5.0 / (16.0 * P.diam[i][i] * P.diam[i][i]);
+    P.koff = 55.0 / 4.0 - 3.0 * BKL - 4.0 * AKL;
+    P.voff = 0.6 * AKL - 1.0;
+    P.cfac = 6.0 * CKL - 5.0;
+    P.sqrt2 = std::sqrt(2.0);
+    P.sqrt3 = std::sqrt(3.0);
+    P.key0 = (uint32_t)p.seed;
+    P.key1 = (uint32_t)(p.seed >> 32);
+    P.step = step;
+    return P;
+}
+
+int ensure_scratch(fhd_ctx* c) {
+    const int* n = c->prm.n_cells;
+    const int nvars = 5 + c->prm.nspecies;
+    fhd_fab tmpl = make_fab(nullptr, n, CELLN, NGC, nvars, FHD_F64);
+    const int64_t cellpts = fab_points(tmpl);
+    int64_t fpts[3];
+    for (int d = 0; d < 3; ++d) fpts[d] = fab_points(make_fab(nullptr, n, FACEN[d], NGC, 1, FHD_F64));
+    const size_t need = (size_t)(2 * cellpts * nvars + 2 * (fpts[0] + fpts[1] + fpts[2])) * sizeof(double);
+    if (c->scratch && c->scratch_bytes >= need) return FHD_OK;
+    if (c->scratch) cudaFree(c->scratch);
+    c->scratch = nullptr;
+    if (cudaMalloc(&c->scratch, need) != cudaSuccess) { cudaGetLastError(); return FHD_ERR_OOM; }
+    // zero once so that components never written (1..3 of cup/cup2) are defined
+    if (cudaMemsetAsync(c->scratch, 0, need, c->stream) != cudaSuccess) return FHD_ERR_CUDA;
+    c->scratch_bytes = need;
+    double* p = c->scratch;
+    c->cup = make_fab(p, n, CELLN, NGC, nvars, FHD_F64); p += cellpts * nvars;
+    c->cup2 = make_fab(p, n, CELLN, NGC, nvars, FHD_F64); p += cellpts * nvars;
+    for (int d = 0; d < 3; ++d) { c->cupm[d] = make_fab(p, n, FACEN[d], NGC, 1, FHD_F64); p += fpts[d]; }
+    for (int d = 0; d < 3; ++d) { c->cup2m[d] = make_fab(p, n, FACEN[d], NGC, 1, FHD_F64); p += fpts[d]; }
+    return FHD_OK;
+}
+
+int ensure_coef(fhd_ctx* c, int dtype) {
+    const int* n = c->prm.n_cells;
+    const int ns = c->prm.nspecies;
+    const int ncomp = 3 + ns + ns * ns;
+    const int64_t pts = fab_points(make_fab(nullptr, n, CELLN, NGC, 1, dtype));
+    const size_t es = dtype == FHD_F64 ? 8 : 4;
+    const size_t need = (size_t)pts * ncomp * es;
+    if (c->coef && c->coef_bytes >= need && c->coef_dtype == dtype) return FHD_OK;
+    if (c->coef) cudaFree(c->coef);
+    c->coef = nullptr;
+    if (cudaMalloc(&c->coef, need) != cudaSuccess) { cudaGetLastError(); return FHD_ERR_OOM; }
+    c->coef_bytes = need;
+    c->coef_dtype = dtype;
+    char* p = static_cast<char*>(c->coef);
+    c->ceta = make_fab(p, n, CELLN, NGC, 1, dtype); p += pts * es;
+    c->czeta = make_fab(p, n, CELLN, NGC, 1, dtype); p += pts * es;
+    c->ckappa = make_fab(p, n, CELLN, NGC, 1, dtype); p += pts * es;
+    c->cchi = make_fab(p, n, CELLN, NGC, ns, dtype); p += pts * ns * es;
+    c->cD = make_fab(p, n, CELLN, NGC, ns * ns, dtype);
+    return FHD_OK;
+}
+
+// brackets one launch with events when profiling is on
+struct ProfScope {
+    fhd_ctx* c;
+    fhd_ctx::Ev* ev = nullptr;
+    ProfScope(fhd_ctx* c_, int kind) : c(c_) {
+        if (!c->prof) return;
+        if (c->nev == c->evs.size()) {
+            fhd_ctx::Ev e;
+            cudaEventCreate(&e.a);
+            cudaEventCreate(&e.b);
+            c->evs.push_back(e);
+        }
+        ev = &c->evs[c->nev++];
+        ev->kind = kind;
+        cudaEventRecord(ev->a, c->stream);
+    }
+    ~ProfScope() {
+        if (ev) cudaEventRecord(ev->b, c->stream);
+    }
+};
+
+int sync_rc(cudaError_t e) {
+    if (e == cudaSuccess) return FHD_OK;
+    cudaGetLastError();
+    return FHD_ERR_CUDA;
+}
+
+bool noise_ok(const fhd_ctx* c, const fhd_noise* nz) {
+    const int ns = c->prm.nspecies;
+    for (int s = 0; s < 2; ++s)
+        for (int d = 0; d < 3; ++d) {
+            if (!fab_ok(c, nz->face[s][d], FACEN[d], 0, ns + 1, FHD_F64)) return false;
+            if (!fab_ok(c, nz->edge[s][d], EDGEN[d], 0, 1, FHD_F64)) return false;
+            if (!fab_ok(c, nz->cen[s][d], CELLN, 1, 1, FHD_F64)) return false;
+        }
+    return true;
+}
+
+void set_noise(StageCall& sc, const fhd_noise* nz, bool W) {
+    for (int d = 0; d < 3; ++d) {
+        sc.nz.fa[d] = nz->face[0][d];
+        sc.nz.fb[d] = W ? nz->face[0][d] : nz->face[1][d];
+        sc.nz.ea[d] = nz->edge[0][d];
+        sc.nz.eb[d] = W ? nz->edge[0][d] : nz->edge[1][d];
+        sc.nz.ca[d] = nz->cen[0][d];
+        sc.nz.cb[d] = W ? nz->cen[0][d] : nz->cen[1][d];
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fhd_strerror(int code) {
+    switch (code) {
+        case FHD_OK: return "ok";
+        case FHD_ERR_BAD_ARG: return "bad argument (shape, dtype or parameter)";
+        case FHD_ERR_MASSFRAC: return "mass fraction outside (0,1) (reference: amrex::Abort in calculateTransportCoeffs)";
+        case FHD_ERR_NONFINITE: return "non-finite temperature or pressure";
+        case FHD_ERR_OOM: return "device allocation failed";
+        case FHD_ERR_TIMEOUT: return "bounded device wait timed out";
+        case FHD_ERR_CUDA: return "CUDA runtime error";
+        case FHD_ERR_UNSUPPORTED: return "option outside the implemented scope";
+        default: return "unknown error";
+    }
+}
+
+int fhd_create(fhd_ctx** out, const fhd_params* params, int device) {
+    if (!out || !params) return FHD_ERR_BAD_ARG;
+    *out = nullptr;
+    const fhd_params& p = *params;
+    if (p.nspecies < 1 || p.nspecies > 4) return FHD_ERR_UNSUPPORTED;
+    for (int d = 0; d < 3; ++d)
+        if (p.n_cells[d] < 2 || !(p.prob_hi[d] > p.prob_lo[d])) return FHD_ERR_BAD_ARG;
+    if ((int64_t)p.n_cells[0] * p.n_cells[1] * p.n_cells[2] >= ((int64_t)1 << 32)) return FHD_ERR_UNSUPPORTED;
+    if (p.algorithm_type != 2 || p.transport_type != 1) return FHD_ERR_UNSUPPORTED;
+    if (p.stoch_stress_form != 0 && p.stoch_stress_form != 1) return FHD_ERR_UNSUPPORTED;
+    if (p.advection_type < -1 || p.advection_type > 2) return FHD_ERR_UNSUPPORTED;
+    if (p.precision != FHD_PREC_FP64 && p.precision != FHD_PREC_MIXED) return FHD_ERR_BAD_ARG;
+    if ((p.visc_type == 3 || p.visc_type == -3) && p.zeta_ratio < 0) return FHD_ERR_BAD_ARG;
+    fhd_ctx* c = new (std::nothrow) fhd_ctx;
+    if (!c) return FHD_ERR_OOM;
+    c->prm = p;
+    // GetHcGas, compressible_functions.cpp:91-100
+    for (int i = 0; i < p.nspecies; ++i) {
+        if (c->prm.hcv[i] < 0.) c->prm.hcv[i] = 0.5 * p.dof[i] * p.Runiv / p.molmass[i];
+        if (c->prm.hcp[i] < 0.) c->prm.hcp[i] = 0.5 * (2. + p.dof[i]) * p.Runiv / p.molmass[i];
+    }
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) { cudaGetLastError(); delete c; return FHD_ERR_CUDA; }
+    if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) { delete c; return FHD_ERR_CUDA; }
+    c->stream = c->own;
+    if (cudaMalloc(&c->d_status, sizeof(int)) != cudaSuccess) {
+        cudaStreamDestroy(c->own);
+        delete c;
+        return FHD_ERR_OOM;
+    }
+    cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream);
+    *out = c;
+    return FHD_OK;
+}
+
+int fhd_destroy(fhd_ctx* c) {
+    if (!c) return FHD_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    if (c->scratch) cudaFree(c->scratch);
+    if (c->coef) cudaFree(c->coef);
+    if (c->hbuf) cudaFree(c->hbuf);
+    for (auto& e : c->evs) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
+    if (c->d_status) cudaFree(c->d_status);
+    if (c->own) cudaStreamDestroy(c->own);
+    delete c;
+    return FHD_OK;
+}
+
+int fhd_set_stream(fhd_ctx* c, void* stream) {
+    if (!c) return FHD_ERR_BAD_ARG;
+    c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own;
+    return FHD_OK;
+}
+
+int fhd_synchronize(fhd_ctx* c) {
+    if (!c) return FHD_ERR_BAD_ARG;
+    return sync_rc(cudaStreamSynchronize(c->stream));
+}
+
+int fhd_status(fhd_ctx* c) {
+    if (!c) return FHD_ERR_BAD_ARG;
+    int h = 0;
+    if (cudaMemcpyAsync(&h, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
+        return FHD_ERR_CUDA;
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) { cudaGetLastError(); return FHD_ERR_CUDA; }
+    cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream);
+    return h;
+}
+
+int fhd_get_params(const fhd_ctx* c, fhd_params* out) {
+    if (!c || !out) return FHD_ERR_BAD_ARG;
+    *out = c->prm;
+    return FHD_OK;
+}
+
+int fhd_set_tile(fhd_ctx* c, int tile) {
+    if (!c || tile < 0 || tile >= num_tiles()) return FHD_ERR_BAD_ARG;
+    c->tile = tile;
+    return FHD_OK;
+}
+
+int fhd_num_tiles(void) { return num_tiles(); }
+const char* fhd_tile_name(int t) { return tile_name(t); }
+
+int fhd_init_cons_var_stag(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], double rho0, double T_init,
+                           const double* rhobar) {
+    if (!c || !mom || !rhobar) return FHD_ERR_BAD_ARG;
+    const int ns = c->prm.nspecies;
+    if (!fab_ok(c, cu, CELLN, 0, 5 + ns, FHD_F64)) return FHD_ERR_BAD_ARG;
+    for (int d = 0; d < 3; ++d)
+        if (!fab_ok(c, mom[d], FACEN[d], 0, 1, FHD_F64)) return FHD_ERR_BAD_ARG;
+    // GetEnergy (compressible_functions.H:1497-1510) at T_init with massvec = rhobar
+    double cvmix = 0., e0mix = 0.;
+    for (int i = 0; i < ns; ++i) {
+        cvmix += rhobar[i] * c->prm.hcv[i];
+        e0mix += rhobar[i] * c->prm.e0[i];
+    }
+    const double intEnergy = e0mix + T_init * cvmix;
+    double rhoY[FHD_MAX_SPECIES];
+    for (int i = 0; i < ns; ++i) rhoY[i] = rho0 * rhobar[i];
+    cudaSetDevice(c->device);
+    int rc = init_uniform(cu, ns, rho0, rho0 * intEnergy, rhoY, c->stream);
+    if (rc) return rc;
+    for (int d = 0; d < 3; ++d)
+        if (cudaMemsetAsync(mom[d].data, 0, fab_points(mom[d]) * sizeof(double) * mom[d].ncomp, c->stream) !=
+            cudaSuccess)
+            return FHD_ERR_CUDA;
+    return FHD_OK;
+}
+
+int fhd_conserved_to_primitive_stag(fhd_ctx* c, fhd_fab prim, const fhd_fab vel[3], fhd_fab cu, const fhd_fab mom[3]) {
+    if (!c || !vel || !mom) return FHD_ERR_BAD_ARG;
+    const int ns = c->prm.nspecies;
+    if (!fab_ok(c, cu, CELLN, 1, 5 + ns, FHD_F64) || !fab_ok(c, prim, CELLN, 0, 6 + 2 * ns, FHD_F64))
+        return FHD_ERR_BAD_ARG;
+    for (int d = 0; d < 3; ++d)
+        if (!fab_ok(c, vel[d], FACEN[d], 0, 1, FHD_F64) || !fab_ok(c, mom[d], FACEN[d], 0, 1, FHD_F64))
+            return FHD_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    return exact_convert(make_dev(c, 1.0, 0), prim, vel, cu, mom, c->d_status, c->stream);
+}
+
+int fhd_transport_coeffs(fhd_ctx* c, fhd_fab prim, fhd_fab eta, fhd_fab zeta, fhd_fab kappa, fhd_fab chi, fhd_fab D) {
+    if (!c) return FHD_ERR_BAD_ARG;
+    const int ns = c->prm.nspecies;
+    if (!fab_ok(c, prim, CELLN, 0, 6 + 2 * ns, FHD_F64)) return FHD_ERR_BAD_ARG;
+    const int g = -prim.lo[0];
+    if (!fab_ok(c, eta, CELLN, g, 1, FHD_F64) || !fab_ok(c, zeta, CELLN, g, 1, FHD_F64) ||
+        !fab_ok(c, kappa, CELLN, g, 1, FHD_F64) || !fab_ok(c, chi, CELLN, g, ns, FHD_F64) ||
+        !fab_ok(c, D, CELLN, g, ns * ns, FHD_F64))
+        return FHD_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    return exact_transport(make_dev(c, 1.0, 0), prim, eta, zeta, kappa, chi, D, c->d_status, c->stream);
+}
+
+int fhd_flux_stag(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim, const fhd_fab vel[3], fhd_fab eta,
+                  fhd_fab zeta, fhd_fab kappa, fhd_fab chi, fhd_fab D, const fhd_fab faceflux[3],
+                  const fhd_fab edgeflux[6], const fhd_fab cenflux[3], const fhd_fab stochface[3],
+                  const fhd_fab stochedge[3], const fhd_fab stochcen[3], double dt) {
+    if (!c || !mom || !vel || !faceflux || !edgeflux || !cenflux) return FHD_ERR_BAD_ARG;
+    const int ns = c->prm.nspecies, nvars = 5 + ns;
+    if (!fab_ok(c, cu, CELLN, 1, nvars, FHD_F64) || !fab_ok(c, prim, CELLN, 1, 6 + 2 * ns, FHD_F64))
+        return FHD_ERR_BAD_ARG;
+    if (!fab_ok(c, eta, CELLN, 1, 1, FHD_F64) || !fab_ok(c, zeta, CELLN, 1, 1, FHD_F64) ||
+        !fab_ok(c, kappa, CELLN, 1, 1, FHD_F64) || !fab_ok(c, chi, CELLN, 1, ns, FHD_F64) ||
+        !fab_ok(c, D, CELLN, 1, ns * ns, FHD_F64))
+        return FHD_ERR_BAD_ARG;
+    for (int d = 0; d < 3; ++d) {
+        if (!fab_ok(c, vel[d], FACEN[d], 1, 1, FHD_F64) || !fab_ok(c, mom[d], FACEN[d], 1, 1, FHD_F64))
+            return FHD_ERR_BAD_ARG;
+        if (!fab_ok(c, faceflux[d], FACEN[d], 0, nvars + 4, FHD_F64, 0)) return FHD_ERR_BAD_ARG;
+        if (!fab_ok(c, cenflux[d], CELLN, 1, 1, FHD_F64, 1)) return FHD_ERR_BAD_ARG;
+    }
+    for (int e = 0; e < 6; ++e)
+        if (!fab_ok(c, edgeflux[e], EFLUXN[e], 0, 1, FHD_F64, 0)) return FHD_ERR_BAD_ARG;
+    const bool stoch = c->prm.stoch_stress_form == 1;
+    if (stoch) {
+        if (!stochface || !stochedge || !stochcen) return FHD_ERR_BAD_ARG;
+        for (int d = 0; d < 3; ++d)
+            if (!fab_ok(c, stochface[d], FACEN[d], 0, ns + 1, FHD_F64) ||
+                !fab_ok(c, stochedge[d], EDGEN[d], 0, 1, FHD_F64) || !fab_ok(c, stochcen[d], CELLN, 1, 1, FHD_F64))
+                return FHD_ERR_BAD_ARG;
+    }
+    cudaSetDevice(c->device);
+    StageCall sc;
+    std::memset(&sc, 0, sizeof(sc));
+    sc.P = make_dev(c, dt, 0);
+    sc.mode = stoch ? NM_W : NM_OFF;
+    sc.w = 0.0;
+    sc.stage = 0;
+    sc.cons_s = cu;
+    for (int d = 0; d < 3; ++d) { sc.mom_s[d] = mom[d]; sc.vel[d] = vel[d]; sc.ff[d] = faceflux[d]; sc.cf[d] = cenflux[d]; }
+    for (int e = 0; e < 6; ++e) sc.ef[e] = edgeflux[e];
+    sc.pr = prim;
+    sc.pT = 4;
+    sc.eta = eta; sc.zeta = zeta; sc.kappa = kappa; sc.chi = chi; sc.D = D;
+    if (stoch) {
+        for (int d = 0; d < 3; ++d) {
+            sc.nz.fa[d] = sc.nz.fb[d] = stochface[d];
+            sc.nz.ea[d] = sc.nz.eb[d] = stochedge[d];
+            sc.nz.ca[d] = sc.nz.cb[d] = stochcen[d];
+        }
+    }
+    sc.status = c->d_status;
+    sc.stream = c->stream;
+    return exact_aux_fluxes(sc);
+}
+
+int fhd_fill_boundary(fhd_ctx* c, fhd_fab f) {
+    if (!c || !f.data || f.dtype != FHD_F64) return FHD_ERR_BAD_ARG;
+    int nodal[3] = {f.nodal[0], f.nodal[1], f.nodal[2]};
+    if (!fab_ok(c, f, nodal, 0, 1, FHD_F64)) return FHD_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    GhostReq r{f, 0, f.ncomp};
+    return fill_ghosts(&r, 1, c->prm.n_cells, c->stream);
+}
+
+int fhd_override_sync(fhd_ctx* c, fhd_fab f) {
+    if (!c || !f.data) return FHD_ERR_BAD_ARG;
+    int nodal[3] = {f.nodal[0], f.nodal[1], f.nodal[2]};
+    if (!fab_ok(c, f, nodal, 0, 1, FHD_F64)) return FHD_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    return override_sync(f, c->prm.n_cells, c->stream);
+}
+
+int fhd_fill_random_normal(fhd_ctx* c, fhd_fab mf, int scomp, int ncomp, double mean, double variance,
+                           int overridesync, int fillboundary, uint64_t stream_id) {
+    if (!c || !mf.data || scomp < 0 || ncomp < 1 || scomp + ncomp > mf.ncomp || variance < 0) return FHD_ERR_BAD_ARG;
+    int nodal[3] = {mf.nodal[0], mf.nodal[1], mf.nodal[2]};
+    if (!fab_ok(c, mf, nodal, 0, 1, FHD_F64)) return FHD_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    DevParams P = make_dev(c, 1.0, stream_id);
+    // field ids above the step-noise range keep these streams apart from the step's noise
+    int rc = noise_fill(P, mf, scomp, ncomp, mean, std::sqrt(variance), 0x1000u + (uint32_t)scomp, 0, c->stream);
+    if (rc) return rc;
+    if (overridesync) rc = override_sync(mf, c->prm.n_cells, c->stream);
+    if (rc) return rc;
+    if (fillboundary && -mf.lo[0] > 0) {
+        GhostReq r{mf, scomp, ncomp};
+        rc = fill_ghosts(&r, 1, c->prm.n_cells, c->stream);
+    }
+    return rc;
+}
+
+int fhd_fill_step_noise(fhd_ctx* c, const fhd_noise* nz, int64_t step) {
+    if (!c || !nz) return FHD_ERR_BAD_ARG;
+    if (!noise_ok(c, nz)) return FHD_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    const int ns = c->prm.nspecies;
+    DevParams P = make_dev(c, 1.0, (uint64_t)step);
+    GhostReq g[6];
+    int ng = 0;
+    for (int s = 0; s < 2; ++s)
+        for (int d = 0; d < 3; ++d) {
+            const fhd_fab& f = nz->face[s][d];
+            int rc = noise_fill(P, f, f.ncomp - (ns + 1), ns + 1, 0.0, 1.0, (uint32_t)(d * (MAXS + 1)), s, c->stream);
+            if (!rc) rc = noise_fill(P, nz->edge[s][d], 0, 1, 0.0, 1.0, (uint32_t)(3 * (MAXS + 1) + d), s, c->stream);
+            if (!rc) rc = noise_fill(P, nz->cen[s][d], 0, 1, 0.0, std::sqrt(2.0), (uint32_t)(3 * (MAXS + 1) + 3 + d), s,
+                                     c->stream);
+            if (rc) return rc;
+            g[ng++] = GhostReq{nz->cen[s][d], 0, 1};
+        }
+    return fill_ghosts(g, ng, c->prm.n_cells, c->stream);
+}
+
+int fhd_rk3_step_stag(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim, const fhd_fab vel[3], fhd_fab source,
+                      fhd_fab eta, fhd_fab zeta, fhd_fab kappa, fhd_fab chi, fhd_fab D, const fhd_fab* faceflux,
+                      const fhd_fab* edgeflux, const fhd_fab* cenflux, const fhd_noise* injected, double dt,
+                      int64_t step) {
+    if (!c || !mom || !vel || !(dt > 0)) return FHD_ERR_BAD_ARG;
+    const int ns = c->prm.nspecies, nvars = 5 + ns, nprim = 6 + 2 * ns;
+    const bool mixed = c->prm.precision == FHD_PREC_MIXED;
+    if (!fab_ok(c, cu, CELLN, NGC, nvars, FHD_F64) || !fab_ok(c, prim, CELLN, NGC, nprim, FHD_F64)) return FHD_ERR_BAD_ARG;
+    for (int d = 0; d < 3; ++d)
+        if (!fab_ok(c, mom[d], FACEN[d], NGC, 1, FHD_F64) || !fab_ok(c, vel[d], FACEN[d], NGC, 1, FHD_F64))
+            return FHD_ERR_BAD_ARG;
+    if (source.data && !fab_ok(c, source, CELLN, 0, nvars, FHD_F64)) return FHD_ERR_BAD_ARG;
+    const bool aux_coef = eta.data != nullptr;
+    if (aux_coef) {
+        if (mixed) return FHD_ERR_UNSUPPORTED;
+        if (!fab_ok(c, eta, CELLN, 1, 1, FHD_F64) || !fab_ok(c, zeta, CELLN, 1, 1, FHD_F64) ||
+            !fab_ok(c, kappa, CELLN, 1, 1, FHD_F64) || !fab_ok(c, chi, CELLN, 1, ns, FHD_F64) ||
+            !fab_ok(c, D, CELLN, 1, ns * ns, FHD_F64))
+            return FHD_ERR_BAD_ARG;
+    }
+    const bool aux_flux = faceflux && edgeflux && cenflux && faceflux[0].data;
+    if (aux_flux) {
+        if (mixed || !aux_coef) return FHD_ERR_UNSUPPORTED;
+        for (int d = 0; d < 3; ++d)
+            if (!fab_ok(c, faceflux[d], FACEN[d], 0, nvars + 4, FHD_F64, 0) || !fab_ok(c, cenflux[d], CELLN, 1, 1, FHD_F64, 1))
+                return FHD_ERR_BAD_ARG;
+        for (int e = 0; e < 6; ++e)
+            if (!fab_ok(c, edgeflux[e], EFLUXN[e], 0, 1, FHD_F64, 0)) return FHD_ERR_BAD_ARG;
+    }
+    const bool stoch = c->prm.stoch_stress_form == 1;
+    if (stoch && injected && !noise_ok(c, injected)) return FHD_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    int rc = ensure_scratch(c);
+    if (rc) return rc;
+    if (mixed || !aux_coef) {
+        rc = ensure_coef(c, mixed ? FHD_F32 : FHD_F64);
+        if (rc) return rc;
+    }
+    const double w[3] = {(2.0 * std::sqrt(2.0) + 1.0 * std::sqrt(3.0)) / 5.0,
+                         (-4.0 * std::sqrt(2.0) + 3.0 * std::sqrt(3.0)) / 5.0,
+                         (1.0 * std::sqrt(2.0) - 2.0 * std::sqrt(3.0)) / 10.0};
+    StageCall sc;
+    std::memset(&sc, 0, sizeof(sc));
+    sc.P = make_dev(c, dt, (uint64_t)step);
+    sc.mode = !stoch ? NM_OFF : (injected ? NM_AB : NM_PHILOX);
+    if (injected && stoch) set_noise(sc, injected, false);
+    sc.pr = prim;
+    sc.pT = 4;
+    for (int d = 0; d < 3; ++d) { sc.vel[d] = vel[d]; sc.mom0[d] = mom[d]; }
+    sc.cons0 = cu;
+    if (aux_coef && !mixed) { sc.eta = eta; sc.zeta = zeta; sc.kappa = kappa; sc.chi = chi; sc.D = D; }
+    else { sc.eta = c->ceta; sc.zeta = c->czeta; sc.kappa = c->ckappa; sc.chi = c->cchi; sc.D = c->cD; }
+    sc.src = source;
+    sc.status = c->d_status;
+    sc.stream = c->stream;
+    sc.tile = c->tile;
+    const fhd_fab* ins[3] = {&cu, &c->cup, &c->cup2};
+    const fhd_fab* insm[3] = {mom, c->cupm, c->cup2m};
+    const fhd_fab* outs[3] = {&c->cup, &c->cup2, &cu};
+    const fhd_fab* outsm[3] = {c->cupm, c->cup2m, mom};
+    for (int s = 0; s < 3; ++s) {
+        sc.stage = s + 1;
+        sc.w = w[s];
+        sc.cons_s = *ins[s];
+        sc.cons_o = *outs[s];
+        for (int d = 0; d < 3; ++d) { sc.mom_s[d] = insm[s][d]; sc.mom_o[d] = outsm[s][d]; }
+        {
+            ProfScope ps(c, 0);
+            rc = mixed ? mixed_cellprep(sc) : exact_cellprep(sc);
+        }
+        if (rc) return rc;
+        if (s == 2 && aux_flux) {
+            for (int d = 0; d < 3; ++d) { sc.ff[d] = faceflux[d]; sc.cf[d] = cenflux[d]; }
+            for (int e = 0; e < 6; ++e) sc.ef[e] = edgeflux[e];
+            ProfScope ps(c, 4);
+            rc = exact_aux_fluxes(sc);
+            if (rc) return rc;
+        }
+        {
+            ProfScope ps(c, 1);
+            rc = mixed ? mixed_stage(sc) : exact_stage(sc);
+        }
+        if (rc) return rc;
+        GhostReq g[5] = {{*outs[s], 0, 1}, {*outs[s], 4, 1 + ns}, {outsm[s][0], 0, 1}, {outsm[s][1], 0, 1},
+                         {outsm[s][2], 0, 1}};
+        {
+            ProfScope ps(c, 2);
+            rc = fill_ghosts(g, 5, c->prm.n_cells, c->stream);
+        }
+        if (rc) return rc;
+    }
+    // final conservedToPrimitiveStag + FillBoundary (timeStepStag.cpp:1216-1230)
+    {
+        ProfScope ps(c, 3);
+        rc = exact_convert(sc.P, prim, vel, cu, mom, c->d_status, c->stream);
+    }
+    if (rc) return rc;
+    GhostReq g[10];
+    int ng = 0;
+    g[ng++] = GhostReq{cu, 1, 3};
+    g[ng++] = GhostReq{prim, 0, nprim};
+    for (int d = 0; d < 3; ++d) g[ng++] = GhostReq{vel[d], 0, 1};
+    if (aux_coef) {
+        g[ng++] = GhostReq{eta, 0, 1};
+        g[ng++] = GhostReq{zeta, 0, 1};
+        g[ng++] = GhostReq{kappa, 0, 1};
+        g[ng++] = GhostReq{chi, 0, ns};
+        g[ng++] = GhostReq{D, 0, ns * ns};
+    }
+    ProfScope ps(c, 2);
+    return fill_ghosts(g, ng, c->prm.n_cells, c->stream);
+}
+
+int fhd_profile(fhd_ctx* c, int enable) {
+    if (!c) return FHD_ERR_BAD_ARG;
+    c->prof = enable != 0;
+    return FHD_OK;
+}
+
+int fhd_profile_read(fhd_ctx* c, double* ms, int64_t* launches) {
+    if (!c || !ms || !launches) return FHD_ERR_BAD_ARG;
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) { cudaGetLastError(); return FHD_ERR_CUDA; }
+    for (int k = 0; k < FHD_PROF_KINDS; ++k) { ms[k] = 0.0; launches[k] = 0; }
+    for (size_t q = 0; q < c->nev; ++q) {
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, c->evs[q].a, c->evs[q].b) != cudaSuccess) { cudaGetLastError(); continue; }
+        ms[c->evs[q].kind] += t;
+        launches[c->evs[q].kind] += 1;
+    }
+    c->nev = 0;
+    return FHD_OK;
+}
+
+int fhd_rk3_step_stag_host(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim, const fhd_fab vel[3],
+                           const fhd_noise* injected, double dt, int64_t step, int64_t* h2d_bytes,
+                           int64_t* d2h_bytes) {
+    if (!c || !mom || !vel) return FHD_ERR_BAD_ARG;
+    const int ns = c->prm.nspecies;
+    if (!fab_ok(c, cu, CELLN, NGC, 5 + ns, FHD_F64) || !fab_ok(c, prim, CELLN, NGC, 6 + 2 * ns, FHD_F64))
+        return FHD_ERR_BAD_ARG;
+    for (int d = 0; d < 3; ++d)
+        if (!fab_ok(c, mom[d], FACEN[d], NGC, 1, FHD_F64) || !fab_ok(c, vel[d], FACEN[d], NGC, 1, FHD_F64))
+            return FHD_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    // device mirrors with the caller's exact geometry
+    const fhd_fab* hf[8] = {&cu, &mom[0], &mom[1], &mom[2], &prim, &vel[0], &vel[1], &vel[2]};
+    size_t bytes[8], total = 0;
+    for (int q = 0; q < 8; ++q) { bytes[q] = (size_t)fab_points(*hf[q]) * hf[q]->ncomp * sizeof(double); total += bytes[q]; }
+    fhd_noise dn;
+    size_t nzb = 0;
+    const bool inj = injected && c->prm.stoch_stress_form == 1;
+    if (inj) {
+        if (!noise_ok(c, injected)) return FHD_ERR_BAD_ARG;
+        for (int s = 0; s < 2; ++s)
+            for (int d = 0; d < 3; ++d)
+                nzb += (fab_points(injected->face[s][d]) * injected->face[s][d].ncomp + fab_points(injected->edge[s][d]) +
+                        fab_points(injected->cen[s][d])) * sizeof(double);
+    }
+    if (!c->hbuf || c->hbuf_bytes < total + nzb) {
+        if (c->hbuf) cudaFree(c->hbuf);
+        c->hbuf = nullptr;
+        if (cudaMalloc(&c->hbuf, total + nzb) != cudaSuccess) { cudaGetLastError(); return FHD_ERR_OOM; }
+        c->hbuf_bytes = total + nzb;
+    }
+    fhd_fab df[8];
+    char* p = reinterpret_cast<char*>(c->hbuf);
+    int64_t h2d = 0, d2h = 0;
+    for (int q = 0; q < 8; ++q) {
+        df[q] = *hf[q];
+        df[q].data = p;
+        if (cudaMemcpyAsync(p, hf[q]->data, bytes[q], cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+            return FHD_ERR_CUDA;
+        h2d += (int64_t)bytes[q];
+        p += bytes[q];
+    }
+    if (inj) {
+        auto mirror = [&](const fhd_fab& h, fhd_fab& d) -> int {
+            const size_t b = (size_t)fab_points(h) * h.ncomp * sizeof(double);
+            d = h;
+            d.data = p;
+            if (cudaMemcpyAsync(p, h.data, b, cudaMemcpyHostToDevice, c->stream) != cudaSuccess) return FHD_ERR_CUDA;
+            h2d += (int64_t)b;
+            p += b;
+            return FHD_OK;
+        };
+        for (int s = 0; s < 2; ++s)
+            for (int d = 0; d < 3; ++d)
+                if (mirror(injected->face[s][d], dn.face[s][d]) || mirror(injected->edge[s][d], dn.edge[s][d]) ||
+                    mirror(injected->cen[s][d], dn.cen[s][d]))
+                    return FHD_ERR_CUDA;
+    }
+    fhd_fab dmom[3] = {df[1], df[2], df[3]}, dvel[3] = {df[5], df[6], df[7]};
+    fhd_fab nf;
+    std::memset(&nf, 0, sizeof(nf));
+    int rc = fhd_rk3_step_stag(c, df[0], dmom, df[4], dvel, nf, nf, nf, nf, nf, nf, nullptr, nullptr, nullptr,
+                               inj ? &dn : nullptr, dt, step);
+    if (rc) return rc;
+    for (int q = 0; q < 8; ++q) {
+        if (cudaMemcpyAsync(hf[q]->data, df[q].data, bytes[q], cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
+            return FHD_ERR_CUDA;
+        d2h += (int64_t)bytes[q];
+    }
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) { cudaGetLastError(); return FHD_ERR_CUDA; }
+    if (h2d_bytes) *h2d_bytes = h2d;
+    if (d2h_bytes) *d2h_bytes = d2h;
+    return FHD_OK;
+}
+
+}  // extern "C"

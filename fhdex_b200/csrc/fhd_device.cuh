@@ -1,0 +1,426 @@
+// fhd_device.cuh — device data views and point physics of the staggered FHD step.
+//
+// Point physics restated from FHDeX src_compressible/compressible_functions.H for
+// sm_100a: compile-time species count NS (fully unrolled, register resident), a
+// compute type R (double for the reference-order FP64 path, float for the mixed
+// path).  With R = double and -fmad=false every expression below evaluates in the
+// reference's operation order, so results are bitwise those of the CPU path.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define FHD_HD __host__ __device__ __forceinline__
+#define FHD_D __device__ __forceinline__
+
+namespace fhd {
+
+constexpr int MAXS = 8;
+
+// AMReX Array4 view: (i,j,k,n) at p[(i-lo0) + (j-lo1)*sy + (k-lo2)*sz + n*sn].
+template <class T>
+struct Arr4 {
+    T* p;
+    int lo0, lo1, lo2;
+    int64_t sy, sz, sn;
+    FHD_HD T& operator()(int i, int j, int k, int n = 0) const {
+        return p[(i - lo0) + (j - lo1) * sy + (k - lo2) * sz + n * sn];
+    }
+    FHD_HD int64_t off(int i, int j, int k) const { return (i - lo0) + (j - lo1) * sy + (k - lo2) * sz; }
+};
+
+// Parameters as the kernels see them (by value in the kernel parameter bank).
+// Cell-independent sub-expressions of the transport model are precomputed on the
+// host in the reference's own operation order (host IEEE double arithmetic gives
+// the identical values the reference computes inside its loops).
+struct DevParams {
+    int ns, nvars, nprim;
+    int n[3];
+    double dx[3];
+    double dt;
+    double volinv, dtinv;            // 1./(dx0*dx1*dx2), 1./dt   (fluxStag.cpp:97-98)
+    double k_B, Runiv;
+    double grav[3];
+    double zeta_ratio;
+    int visc_type, advection_type, stoch;
+    double molmass[MAXS], hcv[MAXS], hcp[MAXS], e0[MAXS];
+    // Giovangigli model constants (compressible_functions.H:1180-1222)
+    double mm[MAXS];                 // molmass*(k_B/Runiv)
+    double mmkB[MAXS];               // mm*k_B (first product of the eta1 sqrt argument)
+    double eta1pre[MAXS];            // 5.0/(16.0*diam(i,i)*diam(i,i))
+    double diam[MAXS][MAXS];         // 0.5*(d_i+d_j)
+    double mu[MAXS][MAXS];           // m_i*m_j/(m_i+m_j)
+    double msum[MAXS][MAXS];         // m_i+m_j
+    double vfac[MAXS][MAXS];         // 1.0+0.6*m_k/m_i*AKL
+    double kfac[MAXS][MAXS];         // 7.5 m_i/m_k + 6.25 m_k/m_i - 3.0 m_k/m_i BKL + 4.0 AKL
+    double koff;                     // 55.0/4.0-3.0*BKL-4.0*AKL
+    double voff;                     // 0.6*AKL-1.0
+    double cfac;                     // 6.0*CKL-5.0
+    double sqrt2, sqrt3;
+    // noise
+    uint32_t key0, key1;             // Philox key
+    uint64_t step;                   // Philox counter words 2-3
+};
+
+// ---- EOS helpers (compressible_functions.H:138-219, 1497-1520) ----------------------
+
+template <int NS, class R>
+FHD_D void GetMolfrac(const DevParams& P, const R (&Y)[NS], R (&X)[NS]) {
+    R molmix = R(0.);
+#pragma unroll
+    for (int n = 0; n < NS; ++n) molmix += Y[n] / R(P.molmass[n]);
+    molmix = R(1.) / molmix;
+#pragma unroll
+    for (int n = 0; n < NS; ++n) X[n] = Y[n] * molmix / R(P.molmass[n]);
+}
+
+template <int NS, class R>
+FHD_D R GetTemperature(const DevParams& P, R energy, const R (&Y)[NS]) {
+    R cvmix = R(0.), e0mix = R(0.);
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+        cvmix += Y[n] * R(P.hcv[n]);
+        e0mix += Y[n] * R(P.e0[n]);
+    }
+    return (energy - e0mix) / cvmix;
+}
+
+template <int NS, class R>
+FHD_D R GetPressureGas(const DevParams& P, const R (&Y)[NS], R density, R temp) {
+    R molmix = R(0.);
+#pragma unroll
+    for (int n = 0; n < NS; ++n) molmix += Y[n] / R(P.molmass[n]);
+    molmix = R(1.) / molmix;
+    return density * (R(P.Runiv) / molmix) * temp;
+}
+
+template <int NS, class R>
+FHD_D void GetEnthalpies(const DevParams& P, R T, R (&hk)[NS]) {
+#pragma unroll
+    for (int i = 0; i < NS; ++i) hk[i] = R(P.e0[i]) + R(P.hcp[i]) * T;
+}
+
+template <class R>
+FHD_D R clamp01(R y) { return fmax(R(0.), fmin(R(1.), y)); }
+template <>
+FHD_D float clamp01<float>(float y) { return fmaxf(0.f, fminf(1.f, y)); }
+
+template <class R> FHD_D R dsqrt(R x);
+template <> FHD_D double dsqrt<double>(double x) { return sqrt(x); }
+template <> FHD_D float dsqrt<float>(float x) { return sqrtf(x); }
+
+// CholeskyDecomp (compressible_functions.H:460-511): lower factor of a symmetric
+// NS x NS matrix with the reference's "sum <= 0 -> zero pivot, zero column" guard.
+// Only the lower triangle reaches the result.
+template <int NS, class R>
+FHD_D void CholeskyDecomp(R (&a)[NS * NS], R (&sqda)[NS * NS]) {
+    R p[NS];
+#pragma unroll
+    for (int i = 0; i < NS; ++i) {
+        int ising = 0;
+#pragma unroll
+        for (int j = i; j < NS; ++j) {
+            R sum1 = a[i * NS + j];
+#pragma unroll
+            for (int k = i - 1; k >= 0; --k) sum1 = sum1 - a[i * NS + k] * a[j * NS + k];
+            if (i == j) {
+                if (sum1 <= R(0.)) { p[i] = R(0.); ising = 1; }
+                else p[i] = dsqrt(sum1);
+            }
+            if (ising == 0) a[j * NS + i] = sum1 / p[i];
+            else a[j * NS + i] = R(0.);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < NS; ++i)
+#pragma unroll
+        for (int j = 0; j < NS; ++j) sqda[i * NS + j] = (j < i) ? a[i * NS + j] : (j == i ? p[i] : R(0.));
+}
+
+// D_GIO1 (compressible_functions.H:647-778).  Dout[j*NS+i] = Diff_ij(i,j)*Ykp[i].
+template <int NS, class R>
+FHD_D void D_GIO1(const R (&Dbin)[NS][NS], const R (&Ykp)[NS], const R (&Xkp)[NS], R (&Dout)[NS * NS]) {
+    R Diff[NS * NS], PJ[NS * NS], M2[NS * NS], Pmat[NS * NS], Jmat[NS * NS];
+    R Di[NS], Minv[NS], Mmat[NS];
+#pragma unroll
+    for (int i = 0; i < NS; ++i) {
+        R term2 = R(0.);
+#pragma unroll
+        for (int j = 0; j < NS; ++j)
+            if (j != i) term2 = term2 + Xkp[j] / Dbin[i][j];
+        Di[i] = (R(1.) - Ykp[i]) / term2;
+    }
+#pragma unroll
+    for (int i = 0; i < NS; ++i) {
+        Mmat[i] = Xkp[i] / Di[i];
+        Minv[i] = Di[i] / Xkp[i];
+    }
+#pragma unroll
+    for (int i = 0; i < NS; ++i)
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+            R v = -Ykp[j];
+            if (i == j) v = v + R(1.);
+            Pmat[i * NS + j] = v;
+        }
+    // Zmat = -Deltamat (+ Mmat on the diagonal); Jmat = Minv*Zmat
+#pragma unroll
+    for (int i = 0; i < NS; ++i)
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+            R Deltamat;
+            if (i == j) {
+                R term1 = R(0.);
+#pragma unroll
+                for (int k = 0; k < NS; ++k)
+                    if (k != i) term1 = term1 + Xkp[i] * Xkp[k] / Dbin[i][k];
+                Deltamat = term1;
+            } else {
+                Deltamat = -Xkp[i] * Xkp[j] / Dbin[i][j];
+            }
+            R z = -Deltamat;
+            if (i == j) z = z + Mmat[i];
+            Jmat[i * NS + j] = Minv[i] * z;
+        }
+#pragma unroll
+    for (int i = 0; i < NS; ++i)
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+            R s = R(0.);
+#pragma unroll
+            for (int k = 0; k < NS; ++k) s = s + Pmat[i * NS + k] * Jmat[k * NS + j];
+            PJ[i * NS + j] = s;
+        }
+#pragma unroll
+    for (int i = 0; i < NS; ++i)
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+            R scr = R(0.);
+#pragma unroll
+            for (int k = 0; k < NS; ++k) scr = scr + Pmat[i * NS + k] * Minv[k] * Pmat[j * NS + k];
+            M2[i * NS + j] = scr;
+            Diff[i * NS + j] = scr;
+        }
+#pragma unroll
+    for (int ll = 0; ll < 3; ++ll) {
+        R M1[NS * NS];
+#pragma unroll
+        for (int i = 0; i < NS; ++i)
+#pragma unroll
+            for (int j = 0; j < NS; ++j) {
+                R scr = R(0.);
+#pragma unroll
+                for (int k = 0; k < NS; ++k) scr = scr + PJ[i * NS + k] * Diff[k * NS + j];
+                M1[i * NS + j] = scr + M2[i * NS + j];
+            }
+#pragma unroll
+        for (int q = 0; q < NS * NS; ++q) Diff[q] = M1[q];
+    }
+#pragma unroll
+    for (int i = 0; i < NS; ++i)
+#pragma unroll
+        for (int j = 0; j < NS; ++j) Dout[j * NS + i] = Diff[i * NS + j] * Ykp[i];
+}
+
+// Per-cell transport coefficients: calculateTransportCoeffs body (transCoeffs.cpp:37-89)
+// with IdealMixtureTransportGIO (compressible_functions.H:1153-1352).
+// Yraw: prim(6+n) (unclamped).  Returns false when a mass fraction is outside (0,1)
+// (the reference aborts there).
+template <int NS, class R>
+struct Coeffs {
+    R eta, kappa, zeta;
+    R chi[NS];
+    R D[NS * NS];
+};
+
+template <int NS, class R>
+FHD_D bool transport_gio(const DevParams& P, R rho, R temperature, R pressure, const R (&Yraw)[NS],
+                         Coeffs<NS, R>& c) {
+    bool ok = true;
+    R Yk[NS];
+    R sumYk = R(0.);
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+        if (Yraw[n] <= R(0.) || Yraw[n] >= R(1.)) ok = false;
+        Yk[n] = clamp01(Yraw[n]);
+        sumYk += Yk[n];
+    }
+#pragma unroll
+    for (int n = 0; n < NS; ++n) Yk[n] /= sumYk;
+
+    const R pi = R(3.1415926535897932);
+    R mbar = R(0.0);
+#pragma unroll
+    for (int n = 0; n < NS; ++n) mbar += Yk[n] / R(P.mm[n]);
+    mbar = R(1.0) / mbar;
+    R Xk[NS], Xkp[NS], Ykp[NS];
+    R Xksum = R(0.0);
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+        Xk[n] = Yk[n] * mbar / R(P.mm[n]);
+        Xksum += Xk[n];
+    }
+#pragma unroll
+    for (int n = 0; n < NS; ++n) Xkp[n] = Xk[n] + R(1.0e-16) * (Xksum / R(double(NS)) - Xk[n]);
+#pragma unroll
+    for (int n = 0; n < NS; ++n) Ykp[n] = Xkp[n] * R(P.mm[n]) / mbar;
+
+    const R kT = R(P.k_B) * temperature;
+    R Dbin[NS][NS];
+#pragma unroll
+    for (int i = 0; i < NS; ++i)
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+            if (j < i) { Dbin[i][j] = Dbin[j][i]; continue; }  // symmetric: bitwise equal
+            const R dij = R(P.diam[i][j]);
+            Dbin[i][j] = (R(3.0) / R(16.0)) * dsqrt(R(2.0) * pi * kT * kT * kT / R(P.mu[i][j])) /
+                         (pressure * pi * dij * dij);
+        }
+    // viscosity
+    R amat[NS][NS], Bi[NS], rhs[NS];
+#pragma unroll
+    for (int i = 0; i < NS; ++i) {
+        const R eta1 = R(P.eta1pre[i]) * dsqrt(R(P.mmkB[i]) * temperature / pi);
+        rhs[i] = Xkp[i];
+        Bi[i] = rhs[i];
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+            if (i == j) {
+                R a = Xkp[i] * Xkp[i] / eta1;
+#pragma unroll
+                for (int k = 0; k < NS; ++k)
+                    if (k != i)
+                        a += R(2.0) * kT * Xkp[i] * Xkp[k] / (pressure * Dbin[i][k] * R(P.msum[i][k])) *
+                             R(P.vfac[i][k]);
+                amat[i][i] = a;
+            } else {
+                amat[i][j] = R(2.0) * kT * Xkp[i] * Xkp[j] / (pressure * Dbin[i][j] * R(P.msum[i][j])) *
+                             R(P.voff);
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < NS - 1; ++j)
+#pragma unroll
+        for (int i = j + 1; i < NS; ++i) {
+            const R fact1 = amat[i][j] / amat[j][j];
+#pragma unroll
+            for (int k = 0; k < NS; ++k) amat[i][k] -= fact1 * amat[j][k];
+            Bi[i] -= fact1 * Bi[j];
+        }
+    Bi[NS - 1] /= amat[NS - 1][NS - 1];
+#pragma unroll
+    for (int i = NS - 2; i > -1; --i) {
+        R sum1 = R(0.0);
+#pragma unroll
+        for (int j = NS - 1; j > i; --j) sum1 += amat[i][j] * Bi[j];
+        Bi[i] = (Bi[i] - sum1) / amat[i][i];
+    }
+    R eta = R(0.0);
+#pragma unroll
+    for (int i = 0; i < NS; ++i) eta += Xkp[i] * Bi[i];
+    c.eta = eta;
+    c.zeta = R(0.);
+    // thermal conductivity
+#pragma unroll
+    for (int i = 0; i < NS; ++i) {
+        rhs[i] = R(2.5) * Xkp[i];
+        Bi[i] = rhs[i];
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+            if (i == j) {
+                R a = Xkp[i] * Xkp[i] / Dbin[i][j] * R(2.0) * R(1.0);
+#pragma unroll
+                for (int k = 0; k < NS; ++k)
+                    if (k != i)
+                        a += Xkp[i] * Xkp[k] / Dbin[i][k] * R(P.mu[i][k]) / R(P.msum[i][k]) * R(P.kfac[i][k]);
+                amat[i][i] = a;
+            } else {
+                amat[i][j] = R(-1.0) * Xkp[i] * Xkp[j] / Dbin[i][j] * R(P.mu[i][j]) / R(P.msum[i][j]) * R(P.koff);
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < NS - 1; ++j)
+#pragma unroll
+        for (int i = j + 1; i < NS; ++i) {
+            const R fact1 = amat[i][j] / amat[j][j];
+#pragma unroll
+            for (int k = 0; k < NS; ++k) amat[i][k] -= fact1 * amat[j][k];
+            Bi[i] -= fact1 * Bi[j];
+        }
+    Bi[NS - 1] /= amat[NS - 1][NS - 1];
+#pragma unroll
+    for (int i = NS - 2; i > -1; --i) {
+        R sum1 = R(0.0);
+#pragma unroll
+        for (int j = NS - 1; j > i; --j) sum1 += amat[i][j] * Bi[j];
+        Bi[i] = (Bi[i] - sum1) / amat[i][i];
+    }
+    R kappa = R(0.0);
+#pragma unroll
+    for (int i = 0; i < NS; ++i) kappa += rhs[i] * Bi[i];
+    kappa *= pressure / temperature;
+    c.kappa = kappa;
+    // thermal diffusion ratios
+#pragma unroll
+    for (int i = 0; i < NS; ++i) {
+        R ch = R(0.0);
+        R row[NS];
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+            if (i == j) {
+                R a = R(0.0);
+#pragma unroll
+                for (int k = 0; k < NS; ++k)
+                    if (k != i) a -= R(0.5) * Xkp[k] / Dbin[i][k] * R(P.mm[k]) / R(P.msum[i][k]) * R(P.cfac);
+                row[j] = a;
+            } else {
+                row[j] = R(0.5) * Xkp[j] / Dbin[i][j] * R(P.mm[i]) / R(P.msum[i][j]) * R(P.cfac);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < NS; ++j) ch += row[j] * Bi[j];
+        c.chi[i] = ch;
+    }
+    R Dl[NS * NS];
+    D_GIO1<NS, R>(Dbin, Ykp, Xkp, Dl);
+#pragma unroll
+    for (int q = 0; q < NS * NS; ++q) c.D[q] = Dl[q] * rho;
+    if (P.visc_type == 3 || P.visc_type == -3) c.zeta = R(P.zeta_ratio) * c.eta;
+    return ok;
+}
+
+// conservedToPrimitiveStag cell body (conservedPrimitiveConversionsStag.cpp:97-140):
+// from rho, rhoE, rhoY and the six face momenta around the cell.
+template <int NS>
+struct Prim {
+    double T, p;
+    double Y[NS], X[NS];
+};
+
+template <int NS>
+FHD_D bool cons_to_prim(const DevParams& P, double rho, double rhoE, const double (&rhoY)[NS], double mxl,
+                        double mxh, double myl, double myh, double mzl, double mzh, Prim<NS>& q) {
+    double kin = 0.;
+    kin += (mxh + mxl) * (mxh + mxl);
+    kin += (myh + myl) * (myh + myl);
+    kin += (mzh + mzl) * (mzh + mzl);
+    kin *= (0.125 / rho);
+    const double intenergy = (rhoE - kin) / rho;
+    double Yf[NS];
+    double sumYk = 0.;
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+        q.Y[n] = rhoY[n] / rho;
+        Yf[n] = clamp01(q.Y[n]);
+        sumYk += Yf[n];
+    }
+#pragma unroll
+    for (int n = 0; n < NS; ++n) Yf[n] /= sumYk;
+    q.T = GetTemperature<NS, double>(P, intenergy, Yf);
+    GetMolfrac<NS, double>(P, q.Y, q.X);
+    q.p = GetPressureGas<NS, double>(P, q.Y, rho, q.T);
+    return isfinite(q.T) && isfinite(q.p);
+}
+
+}  // namespace fhd

@@ -1,0 +1,164 @@
+// fhd_exact.cu — dispatch over the species count to the per-NS translation units
+// (fhd_kern_ns.cu) and the precision-independent utilities: periodic ghost fill,
+// OverrideSync, Philox noise fill, uniform initial state.  Built with -fmad=false.
+#include "fhd_launch.cuh"
+
+namespace fhd {
+
+int exact_cellprep_ns1(const StageCall&);
+int exact_stage_ns1(const StageCall&);
+int exact_aux_ns1(const StageCall&);
+int mixed_cellprep_ns1(const StageCall&);
+int mixed_stage_ns1(const StageCall&);
+int exact_transport_ns1(const DevParams&, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, int*, cudaStream_t);
+int exact_convert_ns1(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const fhd_fab*, int*, cudaStream_t);
+int exact_cellprep_ns2(const StageCall&);
+int exact_stage_ns2(const StageCall&);
+int exact_aux_ns2(const StageCall&);
+int mixed_cellprep_ns2(const StageCall&);
+int mixed_stage_ns2(const StageCall&);
+int exact_transport_ns2(const DevParams&, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, int*, cudaStream_t);
+int exact_convert_ns2(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const fhd_fab*, int*, cudaStream_t);
+int exact_cellprep_ns3(const StageCall&);
+int exact_stage_ns3(const StageCall&);
+int exact_aux_ns3(const StageCall&);
+int mixed_cellprep_ns3(const StageCall&);
+int mixed_stage_ns3(const StageCall&);
+int exact_transport_ns3(const DevParams&, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, int*, cudaStream_t);
+int exact_convert_ns3(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const fhd_fab*, int*, cudaStream_t);
+int exact_cellprep_ns4(const StageCall&);
+int exact_stage_ns4(const StageCall&);
+int exact_aux_ns4(const StageCall&);
+int mixed_cellprep_ns4(const StageCall&);
+int mixed_stage_ns4(const StageCall&);
+int exact_transport_ns4(const DevParams&, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, int*, cudaStream_t);
+int exact_convert_ns4(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const fhd_fab*, int*, cudaStream_t);
+
+#define FHD_DISPATCH(ns, fn, ...)            \
+    switch (ns) {                             \
+        case 1: return fn##1(__VA_ARGS__);    \
+        case 2: return fn##2(__VA_ARGS__);    \
+        case 3: return fn##3(__VA_ARGS__);    \
+        case 4: return fn##4(__VA_ARGS__);    \
+        default: return FHD_ERR_UNSUPPORTED;  \
+    }
+
+int exact_cellprep(const StageCall& c) { FHD_DISPATCH(c.P.ns, exact_cellprep_ns, c) }
+int exact_stage(const StageCall& c) { FHD_DISPATCH(c.P.ns, exact_stage_ns, c) }
+int exact_aux_fluxes(const StageCall& c) { FHD_DISPATCH(c.P.ns, exact_aux_ns, c) }
+int mixed_cellprep(const StageCall& c) { FHD_DISPATCH(c.P.ns, mixed_cellprep_ns, c) }
+int mixed_stage(const StageCall& c) { FHD_DISPATCH(c.P.ns, mixed_stage_ns, c) }
+int exact_transport(const DevParams& P, fhd_fab prim, fhd_fab eta, fhd_fab zeta, fhd_fab kappa, fhd_fab chi,
+                    fhd_fab D, int* status, cudaStream_t s) {
+    FHD_DISPATCH(P.ns, exact_transport_ns, P, prim, eta, zeta, kappa, chi, D, status, s)
+}
+int exact_convert(const DevParams& P, fhd_fab prim, const fhd_fab vel[3], fhd_fab cons, const fhd_fab mom[3],
+                  int* status, cudaStream_t s) {
+    FHD_DISPATCH(P.ns, exact_convert_ns, P, prim, vel, cons, mom, status, s)
+}
+
+int fill_ghosts(const GhostReq* reqs, int n, const int ncell[3], cudaStream_t s) {
+    for (int base = 0; base < n; base += 16) {
+        GhostArgs a;
+        a.nf = 0;
+        int64_t maxpts = 0;
+        for (int q = base; q < n && q < base + 16; ++q) {
+            const fhd_fab& f = reqs[q].f;
+            GhostFab& g = a.f[a.nf++];
+            g.p = static_cast<double*>(f.data);
+            g.lo = f.lo[0];
+            const int gw = -f.lo[0];
+            int64_t ext[3];
+            for (int d = 0; d < 3; ++d) {
+                g.vhi[d] = ncell[d] - 1 + f.nodal[d];
+                ext[d] = f.hi[d] - f.lo[d] + 1;
+            }
+            g.sy = ext[0];
+            g.sz = ext[0] * ext[1];
+            g.sn = ext[0] * ext[1] * ext[2];
+            g.c0 = reqs[q].c0;
+            g.nc = reqs[q].nc;
+            const int64_t VX = g.vhi[0] + 1, VY = g.vhi[1] + 1, VZ = g.vhi[2] + 1;
+            g.npts = 2 * gw * ext[0] * ext[1] + 2 * gw * ext[0] * VZ + 2 * gw * VY * VZ;
+            (void)VX;
+            if (gw == 0) g.npts = 0;
+            if (g.npts * g.nc > maxpts) maxpts = g.npts * g.nc;
+        }
+        for (int d = 0; d < 3; ++d) a.n[d] = ncell[d];
+        if (maxpts == 0) continue;
+        dim3 grid(grid_for(maxpts, 256, 148 * 8), a.nf);
+        k_ghosts<<<grid, 256, 0, s>>>(a);
+        if (cudaGetLastError() != cudaSuccess) return FHD_ERR_CUDA;
+    }
+    return FHD_OK;
+}
+
+int override_sync(const fhd_fab& f, const int ncell[3], cudaStream_t s) {
+    SyncArgs a;
+    a.p = static_cast<double*>(f.data);
+    a.lo = f.lo[0];
+    int64_t ext[3];
+    for (int d = 0; d < 3; ++d) {
+        a.nodal[d] = f.nodal[d];
+        a.n[d] = ncell[d];
+        ext[d] = f.hi[d] - f.lo[d] + 1;
+    }
+    a.sy = ext[0];
+    a.sz = ext[0] * ext[1];
+    a.sn = ext[0] * ext[1] * ext[2];
+    a.nc = f.ncomp;
+    const int64_t tot = (int64_t)(ncell[0] + f.nodal[0]) * (ncell[1] + f.nodal[1]) * (ncell[2] + f.nodal[2]) * f.ncomp;
+    k_override_sync<<<grid_for(tot, 256), 256, 0, s>>>(a);
+    return cuda_rc(cudaGetLastError());
+}
+
+int noise_fill(const DevParams& P, const fhd_fab& f, int c0, int nc, double mean, double sd, uint32_t fid0, int use_b,
+               cudaStream_t s) {
+    NoiseFillArgs a;
+    a.P = P;
+    a.f = view<double>(f);
+    a.vx = P.n[0] + f.nodal[0];
+    a.vy = P.n[1] + f.nodal[1];
+    a.vz = P.n[2] + f.nodal[2];
+    a.c0 = c0;
+    a.nc = nc;
+    a.mean = mean;
+    a.sd = sd;
+    a.fid0 = fid0;
+    a.use_b = use_b;
+    const int64_t tot = (int64_t)a.vx * a.vy * a.vz * nc;
+    k_noise_fill<<<grid_for(tot, 256), 256, 0, s>>>(a);
+    return cuda_rc(cudaGetLastError());
+}
+
+int init_uniform(const fhd_fab& cu, int ns, double rho0, double rhoE, const double* rhoY, cudaStream_t s) {
+    InitArgs a;
+    a.cu = view<double>(cu);
+    a.npts = a.cu.sn;
+    a.nvars = cu.ncomp;
+    a.ns = ns;
+    a.rho0 = rho0;
+    a.rhoE = rhoE;
+    for (int i = 0; i < MAXS; ++i) a.rhoY[i] = i < ns ? rhoY[i] : 0.0;
+    k_init_uniform<<<grid_for(a.npts, 256), 256, 0, s>>>(a);
+    return cuda_rc(cudaGetLastError());
+}
+
+int num_tiles() {
+    int t = 0;
+#define FHD_CNT(a, b, d) ++t;
+    FHD_TILES(FHD_CNT)
+#undef FHD_CNT
+    return t;
+}
+
+const char* tile_name(int t) {
+    static const char* names[] = {
+#define FHD_NM(a, b, d) #a "x" #b "x" #d,
+        FHD_TILES(FHD_NM)
+#undef FHD_NM
+    };
+    return (t >= 0 && t < num_tiles()) ? names[t] : "?";
+}
+
+}  // namespace fhd

@@ -1,0 +1,424 @@
+// fhd_flux.cuh — point flux functions of calculateFluxStag (fluxStag.cpp:5-1868)
+// for a fully periodic box, shared by the fused stage kernel and the drop-in
+// operator kernels.
+//
+// Accumulation order per flux component is the reference's: stochastic part
+// assigned (fluxStag.cpp:298-803), diffusive part added (:872-1448), hyperbolic
+// part added (:1508-1866), and the energy flux finally gets heat + viscous
+// heating + Dufour (:1592).  R is the compute type of the stochastic/diffusive
+// terms (double: reference order; float: mixed precision); hyperbolic terms and
+// all state sums stay in double.
+#pragma once
+#include "fhd_device.cuh"
+#include "philox.cuh"
+
+namespace fhd {
+
+// ---- field accessors ------------------------------------------------------------
+template <int NS, class R>
+struct Fields {
+    Arr4<const double> cons;     // comp 0 rho, 4 rhoE, 5.. rhoY
+    Arr4<const double> mom[3];   // face momenta
+    Arr4<const double> vel[3];   // face velocities
+    Arr4<const double> pr;       // T at comp pT, p pT+1, Y pT+2.., X pT+2+NS..
+    int pT;
+    Arr4<const R> eta, zeta, kappa, chi, D;
+
+    FHD_D double T(int i, int j, int k) const { return pr(i, j, k, pT); }
+    FHD_D double p(int i, int j, int k) const { return pr(i, j, k, pT + 1); }
+    FHD_D double Y(int i, int j, int k, int n) const { return pr(i, j, k, pT + 2 + n); }
+    FHD_D double X(int i, int j, int k, int n) const { return pr(i, j, k, pT + 2 + NS + n); }
+};
+
+// ---- noise sources --------------------------------------------------------------
+enum { NZ_OFF = 0, NZ_W = 1, NZ_AB = 2, NZ_PHILOX = 3 };
+
+struct NoiseArrays {
+    Arr4<const double> fa[3], fb[3];   // face noise (W or A, B); energy at comp foff
+    int foa[3], fob[3];
+    Arr4<const double> ea[3], eb[3];   // xy, xz, yz
+    Arr4<const double> ca[3], cb[3];   // centres (1 ghost)
+};
+
+// W = 1.0*A + w*B (MultiFab::LinComb, timeStepStag.cpp:258-326)
+template <int MODE>
+struct Noise {
+    NoiseArrays a;
+    double w;
+
+    FHD_D double gauss(const DevParams& P, uint32_t fid, int i, int j, int k, double sd) const {
+        float za, zb;
+        normal_pair(P.key0, P.key1, canon(P, i, j, k), fid, P.step, za, zb);
+        const double A = 0.0 + sd * (double)za;
+        const double B = 0.0 + sd * (double)zb;
+        return 1.0 * A + w * B;
+    }
+    FHD_D double face(const DevParams& P, int d, int c, int i, int j, int k) const {
+        if (MODE == NZ_W) return a.fa[d](i, j, k, a.foa[d] + c);
+        if (MODE == NZ_AB) return 1.0 * a.fa[d](i, j, k, a.foa[d] + c) + w * a.fb[d](i, j, k, a.fob[d] + c);
+        if (MODE == NZ_PHILOX) return gauss(P, fid_face(d, c), i, j, k, 1.0);
+        return 0.0;
+    }
+    FHD_D double edge(const DevParams& P, int e, int i, int j, int k) const {
+        if (MODE == NZ_W) return a.ea[e](i, j, k);
+        if (MODE == NZ_AB) return 1.0 * a.ea[e](i, j, k) + w * a.eb[e](i, j, k);
+        if (MODE == NZ_PHILOX) return gauss(P, fid_edge(e), i, j, k, 1.0);
+        return 0.0;
+    }
+    FHD_D double cen(const DevParams& P, int d, int i, int j, int k) const {
+        if (MODE == NZ_W) return a.ca[d](i, j, k);
+        if (MODE == NZ_AB) return 1.0 * a.ca[d](i, j, k) + w * a.cb[d](i, j, k);
+        if (MODE == NZ_PHILOX) return gauss(P, fid_cen(d), i, j, k, P.sqrt2);
+        return 0.0;
+    }
+};
+
+// ---- stresses --------------------------------------------------------------------
+template <class R>
+struct Taus {  // stochastic (s) and deterministic (d) parts
+    R s, d;
+};
+
+template <class R>
+struct CellTaus {
+    R s[3], d[3];
+};
+
+// diagonal stresses at a cell: stochastic fluxStag.cpp:163-206, deterministic :872-924
+template <int NS, class R, int NZ>
+FHD_D CellTaus<R> cell_taus(const DevParams& P, const Fields<NS, R>& F, const Noise<NZ>& nz, int i, int j, int k) {
+    CellTaus<R> t;
+    const R eta = F.eta(i, j, k);
+    const bool visc3 = (P.visc_type == 3 || P.visc_type == -3);
+    if (NZ != NZ_OFF) {
+        const R Tc = R(F.T(i, j, k));
+        const R etaT = eta * Tc;
+        const R zetaT = F.zeta(i, j, k) * Tc;
+        const R fac1 = dsqrt(R(2.0) * R(P.k_B) * etaT * R(P.volinv) * R(P.dtinv));
+        R fac2 = R(-1.0 / 3.0) * dsqrt(R(2.0) * R(P.k_B) * etaT * R(P.volinv) * R(P.dtinv));
+        if (visc3)
+            fac2 = dsqrt(R(P.k_B) * zetaT * R(P.volinv) * R(P.dtinv) / R(3.0)) -
+                   dsqrt(R(2.0) * R(P.k_B) * etaT * R(P.volinv) * R(P.dtinv)) / R(3.0);
+        const R w0 = R(nz.cen(P, 0, i, j, k)), w1 = R(nz.cen(P, 1, i, j, k)), w2 = R(nz.cen(P, 2, i, j, k));
+        const R traceZ = w0 + w1 + w2;
+        t.s[0] = (fac1 * w0) + (fac2 * traceZ);
+        t.s[1] = (fac1 * w1) + (fac2 * traceZ);
+        t.s[2] = (fac1 * w2) + (fac2 * traceZ);
+    } else {
+        t.s[0] = t.s[1] = t.s[2] = R(0.);
+    }
+    const R u_x = (R(F.vel[0](i + 1, j, k)) - R(F.vel[0](i, j, k))) / R(P.dx[0]);
+    const R v_y = (R(F.vel[1](i, j + 1, k)) - R(F.vel[1](i, j, k))) / R(P.dx[1]);
+    const R w_z = (R(F.vel[2](i, j, k + 1)) - R(F.vel[2](i, j, k))) / R(P.dx[2]);
+    const R div = u_x + v_y + w_z;
+    const R zc = visc3 ? R(F.zeta(i, j, k)) : R(0.0);
+    t.d[0] = R(2) * eta * u_x + (zc - R(2) * eta / R(3.)) * div;
+    t.d[1] = R(2) * eta * v_y + (zc - R(2) * eta / R(3.)) * div;
+    t.d[2] = R(2) * eta * w_z + (zc - R(2) * eta / R(3.)) * div;
+    return t;
+}
+
+// off-diagonal stress at an edge E (0 xy, 1 xz, 2 yz): stochastic fluxStag.cpp:209-295,
+// deterministic :927-1023.  The four cells around the edge are c00, c01, c10, c11
+// in the reference's summation order.
+template <int NS, class R, int NZ, int E>
+FHD_D Taus<R> edge_taus(const DevParams& P, const Fields<NS, R>& F, const Noise<NZ>& nz, int i, int j, int k) {
+    // cells: (a) low-low, (b) low-high, (c) high-low, (d) high-high in the edge's two directions
+    int ai, aj, ak, bi, bj, bk, ci, cj, ck;
+    if (E == 0) { ai = i - 1; aj = j - 1; ak = k; bi = i - 1; bj = j; bk = k; ci = i; cj = j - 1; ck = k; }
+    else if (E == 1) { ai = i - 1; aj = j; ak = k - 1; bi = i - 1; bj = j; bk = k; ci = i; cj = j; ck = k - 1; }
+    else { ai = i; aj = j - 1; ak = k - 1; bi = i; bj = j - 1; bk = k; ci = i; cj = j; ck = k - 1; }
+    Taus<R> t;
+    if (NZ != NZ_OFF) {
+        const R etaT = R(0.25) * (F.eta(ai, aj, ak) * R(F.T(ai, aj, ak)) + F.eta(bi, bj, bk) * R(F.T(bi, bj, bk)) +
+                                  F.eta(ci, cj, ck) * R(F.T(ci, cj, ck)) + F.eta(i, j, k) * R(F.T(i, j, k)));
+        const R fac = dsqrt(R(2.0) * R(P.k_B) * etaT * R(P.volinv) * R(P.dtinv));
+        t.s = fac * R(nz.edge(P, E, i, j, k));
+    } else {
+        t.s = R(0.);
+    }
+    R g1, g2;
+    if (E == 0) {
+        g1 = (R(F.vel[0](i, j, k)) - R(F.vel[0](i, j - 1, k))) / R(P.dx[1]);  // u_y
+        g2 = (R(F.vel[1](i, j, k)) - R(F.vel[1](i - 1, j, k))) / R(P.dx[0]);  // v_x
+    } else if (E == 1) {
+        g1 = (R(F.vel[0](i, j, k)) - R(F.vel[0](i, j, k - 1))) / R(P.dx[2]);  // u_z
+        g2 = (R(F.vel[2](i, j, k)) - R(F.vel[2](i - 1, j, k))) / R(P.dx[0]);  // w_x
+    } else {
+        g1 = (R(F.vel[1](i, j, k)) - R(F.vel[1](i, j, k - 1))) / R(P.dx[2]);  // v_z
+        g2 = (R(F.vel[2](i, j, k)) - R(F.vel[2](i, j - 1, k))) / R(P.dx[1]);  // w_y
+    }
+    const R ei = R(0.25) * (F.eta(ai, aj, ak) + F.eta(bi, bj, bk) + F.eta(ci, cj, ck) + F.eta(i, j, k));
+    t.d = ei * (g1 + g2);
+    return t;
+}
+
+// ---- face fluxes ---------------------------------------------------------------------
+template <int NS>
+struct FaceFlux {
+    double cons[2 + NS];  // comps 0 (rho), 4 (rhoE), 5.. (rhoY)
+    double aux[4];        // comps nvars .. nvars+3 (heat, visc. heating diag/shear, Dufour)
+};
+
+// TauGet: .cell(i,j,k) -> CellTaus, .edge<E>(i,j,k) -> Taus
+template <int NS, class R, int NZ, int D, class TauGet>
+FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const Noise<NZ>& nz, const TauGet& tg,
+                             int i, int j, int k) {
+    constexpr int e0 = D == 0, e1 = D == 1, e2 = D == 2;
+    const int im = i - e0, jm = j - e1, km = k - e2;
+    const Arr4<const double>& velx = F.vel[0];
+    const Arr4<const double>& vely = F.vel[1];
+    const Arr4<const double>& velz = F.vel[2];
+    // flux components in the reference's accumulation order
+    R heat = R(0.0), vdiag = R(0.0), vshear = R(0.0), duf = R(0.0);
+    R spec[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) spec[s] = R(0.0);
+
+    const CellTaus<R> tl = tg.cell(im, jm, km);
+    const CellTaus<R> th = tg.cell(i, j, k);
+    // the two transverse edge families touching this face and their (lo, hi) positions
+    Taus<R> ea0, ea1, eb0, eb1;  // ea: first transverse dir, eb: second
+    R va0l, va0h, va1l, va1h, vb0l, vb0h, vb1l, vb1h;  // transverse velocities (lo/hi sides of the face)
+    if (D == 0) {
+        ea0 = tg.template edge<0>(i, j, k);  ea1 = tg.template edge<0>(i, j + 1, k);
+        eb0 = tg.template edge<1>(i, j, k);  eb1 = tg.template edge<1>(i, j, k + 1);
+        va1h = R(vely(i, j + 1, k)); va1l = R(vely(i - 1, j + 1, k));
+        va0h = R(vely(i, j, k));     va0l = R(vely(i - 1, j, k));
+        vb1h = R(velz(i, j, k + 1)); vb1l = R(velz(i - 1, j, k + 1));
+        vb0h = R(velz(i, j, k));     vb0l = R(velz(i - 1, j, k));
+    } else if (D == 1) {
+        ea0 = tg.template edge<0>(i, j, k);  ea1 = tg.template edge<0>(i + 1, j, k);
+        eb0 = tg.template edge<2>(i, j, k);  eb1 = tg.template edge<2>(i, j, k + 1);
+        va1h = R(velx(i + 1, j, k)); va1l = R(velx(i + 1, j - 1, k));
+        va0h = R(velx(i, j, k));     va0l = R(velx(i, j - 1, k));
+        vb1h = R(velz(i, j, k + 1)); vb1l = R(velz(i, j - 1, k + 1));
+        vb0h = R(velz(i, j, k));     vb0l = R(velz(i, j - 1, k));
+    } else {
+        ea0 = tg.template edge<1>(i, j, k);  ea1 = tg.template edge<1>(i + 1, j, k);
+        eb0 = tg.template edge<2>(i, j, k);  eb1 = tg.template edge<2>(i, j + 1, k);
+        va1h = R(velx(i + 1, j, k)); va1l = R(velx(i + 1, j, k - 1));
+        va0h = R(velx(i, j, k));     va0l = R(velx(i, j, k - 1));
+        vb1h = R(vely(i, j + 1, k)); vb1l = R(vely(i, j + 1, k - 1));
+        vb0h = R(vely(i, j, k));     vb0l = R(vely(i, j, k - 1));
+    }
+    const R un = R(F.vel[D](i, j, k));
+
+    // ---- stochastic part (fluxStag.cpp:298-781) ----
+    if (NZ != NZ_OFF) {
+        const R Th = R(F.T(i, j, k)), Tl = R(F.T(im, jm, km));
+        const R kp = (F.kappa(i, j, k) * Th * Th + F.kappa(im, jm, km) * Tl * Tl);
+        const R meanT = R(0.5) * (Th + Tl);
+        const R fw0 = dsqrt(R(P.k_B) * kp * R(P.volinv) * R(P.dtinv));
+        heat = fw0 * R(nz.face(P, D, 0, i, j, k));
+        vdiag = R(0.5) * un * (tl.s[D] + th.s[D]);
+        R vsh = R(0.0);
+        vsh += R(0.25) * ((va1h + va1l) * ea1.s + (va0h + va0l) * ea0.s);
+        vsh += R(0.25) * ((vb1h + vb1l) * eb1.s + (vb0h + vb0l) * eb0.s);
+        vshear = vsh;
+        R yy[NS], yyp[NS], DY[NS * NS], sqD[NS * NS], hk[NS], wien[NS];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            wien[s] = R(0.);
+            yy[s] = clamp01(R(F.Y(im, jm, km, s)));
+            yyp[s] = clamp01(R(F.Y(i, j, k, s)));
+        }
+        R sumy = R(0.), sumyp = R(0.);
+#pragma unroll
+        for (int n = 0; n < NS; ++n) { sumy += yy[n]; sumyp += yyp[n]; }
+#pragma unroll
+        for (int n = 0; n < NS; ++n) { yy[n] /= sumy; yyp[n] /= sumyp; }
+        R MWmix = R(0.);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            MWmix = MWmix + R(0.5) * (yy[s] + yyp[s]) / R(P.molmass[s]);
+#pragma unroll
+            for (int ll = 0; ll < NS; ++ll)
+                DY[s * NS + ll] = R(0.5) * (F.D(im, jm, km, ll * NS + s) * yy[ll] + F.D(i, j, k, ll * NS + s) * yyp[ll] +
+                                            (F.D(im, jm, km, s * NS + ll) * yy[s] + F.D(i, j, k, s * NS + ll) * yyp[s]));
+        }
+#pragma unroll
+        for (int s = 0; s < NS; ++s)
+            if (fabs(yy[s]) + fabs(yyp[s]) <= R(1.e-12)) {
+#pragma unroll
+                for (int n = 0; n < NS; ++n) { DY[s * NS + n] = R(0.); DY[n * NS + s] = R(0.); }
+            }
+        MWmix = R(1.) / MWmix;
+        CholeskyDecomp<NS, R>(DY, sqD);
+        const R fwc = dsqrt(R(P.k_B) * MWmix * R(P.volinv) / (R(P.Runiv) * R(P.dt)));
+        R zs[NS];
+#pragma unroll
+        for (int ll = 0; ll < NS; ++ll) zs[ll] = R(nz.face(P, D, 1 + ll, i, j, k));
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+#pragma unroll
+            for (int ll = 0; ll <= s; ++ll) wien[s] = wien[s] + fwc * sqD[s * NS + ll] * zs[ll];
+            spec[s] = wien[s];
+        }
+        GetEnthalpies<NS, R>(P, meanT, hk);
+        R soret = R(0.);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const R soret_s = (hk[s] + R(P.Runiv) * meanT / R(P.molmass[s]) * R(0.5) *
+                                           (F.chi(im, jm, km, s) + F.chi(i, j, k, s))) * wien[s];
+            soret += soret_s;
+        }
+        duf = soret;
+    }
+
+    // ---- diffusive part (fluxStag.cpp:1026-1426) ----
+    {
+        const R h = R(P.dx[D]);
+        vdiag -= R(0.5) * un * (tl.d[D] + th.d[D]);
+        R vsh = R(0.0);
+        vsh -= R(0.25) * ((va1h + va1l) * ea1.d + (va0h + va0l) * ea0.d);
+        vsh -= R(0.25) * ((vb1h + vb1l) * eb1.d + (vb0h + vb0l) * eb0.d);
+        vshear += vsh;
+        const R Tl = R(F.T(im, jm, km)), Th = R(F.T(i, j, k));
+        const R pl = R(F.p(im, jm, km)), ph = R(F.p(i, j, k));
+        const R kp = R(0.5) * (F.kappa(im, jm, km) + F.kappa(i, j, k));
+        const R meanT = R(0.5) * (Tl + Th);
+        const R meanP = R(0.5) * (pl + ph);
+        heat -= kp * (Th - Tl) / h;
+        R dk[NS], sor[NS], Fk[NS], hk[NS];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const R Xl = R(F.X(im, jm, km, s)), Xh = R(F.X(i, j, k, s));
+            const R term1 = (Xh - Xl) / h;
+            const R mX = R(0.5) * (Xl + Xh);
+            const R mY = R(0.5) * (R(F.Y(im, jm, km, s)) + R(F.Y(i, j, k, s)));
+            const R term2 = (mX - mY) * (ph - pl) / h / meanP;
+            dk[s] = term1 + term2;
+            const R ChiX = R(0.5) * (F.chi(im, jm, km, s) * Xl + F.chi(i, j, k, s) * Xh);
+            sor[s] = ChiX * (Th - Tl) / h / meanT;
+        }
+#pragma unroll
+        for (int kk = 0; kk < NS; ++kk) {
+            R f = R(0.);
+#pragma unroll
+            for (int ll = 0; ll < NS; ++ll) {
+                const R Fks = R(0.5) * (F.D(im, jm, km, ll * NS + kk) + F.D(i, j, k, ll * NS + kk)) * (dk[ll] + sor[ll]);
+                f -= Fks;
+            }
+            Fk[kk] = f;
+        }
+        GetEnthalpies<NS, R>(P, meanT, hk);
+        R Q5 = R(0.);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            // z faces use chi(i,j,k)+chi(i,j,k), fluxStag.cpp:1407 (kept from the reference)
+            const R chs = (D == 2) ? (F.chi(i, j, k, s) + F.chi(i, j, k, s)) : (F.chi(im, jm, km, s) + F.chi(i, j, k, s));
+            Q5 += (hk[s] + R(0.5) * R(P.Runiv) * meanT * chs / R(P.molmass[s])) * Fk[s];
+        }
+        duf += Q5;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) spec[s] += Fk[s];
+    }
+
+    // ---- hyperbolic part (fluxStag.cpp:1508-1764), in double ----
+    FaceFlux<NS> out;
+    double f0 = 0.0, f4 = 0.0;
+    double fs[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) fs[s] = (double)spec[s];
+    const int adv = P.advection_type;
+    if (adv >= 0) {
+        const double m = F.mom[D](i, j, k);
+        const double u = F.vel[D](i, j, k);
+        f0 += m;
+        const double pl = F.p(im, jm, km), ph = F.p(i, j, k);
+        if (adv == 2) {
+            f4 += 0.5 * (F.cons(im, jm, km, 4) + F.cons(i, j, k, 4)) * u + 0.5 * (pl + ph) * u;
+#pragma unroll
+            for (int s = 0; s < NS; ++s) fs[s] += 0.5 * (F.cons(im, jm, km, 5 + s) + F.cons(i, j, k, 5 + s)) * u;
+        } else {
+            const double meanT = 0.5 * (F.T(im, jm, km) + F.T(i, j, k));
+            const double meanRho = 0.5 * (F.cons(im, jm, km, 0) + F.cons(i, j, k, 0));
+            double hk[NS];
+            GetEnthalpies<NS, double>(P, meanT, hk);
+            if (adv == 1) {
+                const double meanE = 0.5 * (F.cons(im, jm, km, 4) + F.cons(i, j, k, 4)) / meanRho;
+                const double meanP = 0.5 * (pl + ph);
+                f4 += m * (meanE + (meanP / meanRho));
+            }
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                const double Yk = 0.5 * (F.Y(im, jm, km, s) + F.Y(i, j, k, s));
+                fs[s] += Yk * m;
+                if (adv == 0) f4 += m * Yk * hk[s];
+            }
+            if (adv == 0) {
+                const Arr4<const double>& mx = F.mom[0];
+                const Arr4<const double>& my = F.mom[1];
+                const Arr4<const double>& mz = F.mom[2];
+                double keP = 0., keM = 0.;
+                keP += (mx(i + 1, j, k) + mx(i, j, k)) * (mx(i + 1, j, k) + mx(i, j, k));
+                keP += (my(i, j + 1, k) + my(i, j, k)) * (my(i, j + 1, k) + my(i, j, k));
+                keP += (mz(i, j, k + 1) + mz(i, j, k)) * (mz(i, j, k + 1) + mz(i, j, k));
+                keP *= (0.125 / F.cons(i, j, k, 0) / F.cons(i, j, k, 0));
+                keM += (mx(im + 1, jm, km) + mx(im, jm, km)) * (mx(im + 1, jm, km) + mx(im, jm, km));
+                keM += (my(im, jm + 1, km) + my(im, jm, km)) * (my(im, jm + 1, km) + my(im, jm, km));
+                keM += (mz(im, jm, km + 1) + mz(im, jm, km)) * (mz(im, jm, km + 1) + mz(im, jm, km));
+                // z faces divide by cons(i,j-1,k,0), fluxStag.cpp:1755 (kept from the reference)
+                const double rm = (D == 2) ? F.cons(i, j - 1, k, 0) : F.cons(im, jm, km, 0);
+                keM *= (0.125 / rm / rm);
+                f4 += m * 0.5 * (keP + keM);
+            }
+        }
+    }
+    out.aux[0] = (double)heat;
+    out.aux[1] = (double)vdiag;
+    out.aux[2] = (double)vshear;
+    out.aux[3] = (double)duf;
+    f4 += out.aux[0] + out.aux[1] + out.aux[2] + out.aux[3];
+    out.cons[0] = f0;
+    out.cons[1] = f4;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) out.cons[2 + s] = fs[s];
+    return out;
+}
+
+// ---- momentum fluxes --------------------------------------------------------------
+// advective edge terms (fluxStag.cpp:1767-1845): returns the two fluxes of edge E:
+// E=0 xy: (edgey_u, edgex_v); E=1 xz: (edgez_u, edgex_w); E=2 yz: (edgez_v, edgey_w)
+template <int NS, class R, int E>
+FHD_D void edge_adv(const DevParams& P, const Fields<NS, R>& F, int i, int j, int k, double& a, double& b) {
+    const Arr4<const double>&mx = F.mom[0], &my = F.mom[1], &mz = F.mom[2];
+    const Arr4<const double>&vx = F.vel[0], &vy = F.vel[1], &vz = F.vel[2];
+    if (P.advection_type < 0) { a = b = 0.0; return; }
+    if (E == 0) {
+        a = 0.25 * (mx(i, j - 1, k) + mx(i, j, k)) * (vy(i - 1, j, k) + vy(i, j, k));
+        b = 0.25 * (my(i - 1, j, k) + my(i, j, k)) * (vx(i, j - 1, k) + vx(i, j, k));
+    } else if (E == 1) {
+        a = 0.25 * (mx(i, j, k - 1) + mx(i, j, k)) * (vz(i - 1, j, k) + vz(i, j, k));
+        b = 0.25 * (mz(i - 1, j, k) + mz(i, j, k)) * (vx(i, j, k - 1) + vx(i, j, k));
+    } else {
+        a = 0.25 * (my(i, j, k - 1) + my(i, j, k)) * (vz(i, j - 1, k) + vz(i, j, k));
+        b = 0.25 * (mz(i, j - 1, k) + mz(i, j, k)) * (vy(i, j, k - 1) + vy(i, j, k));
+    }
+}
+
+// edge momentum flux = tau_s - tau_d + advective (fluxStag.cpp:784-796, 1429-1441, 1767-1845)
+template <class R>
+FHD_D double edge_total(const Taus<R>& t, double adv, int has_adv) {
+    double v = (double)t.s;
+    v -= (double)t.d;
+    if (has_adv) v += adv;
+    return v;
+}
+
+// centre momentum flux in direction d at a cell (fluxStag.cpp:799-803, 1444-1448, 1848-1866)
+template <int NS, class R>
+FHD_D double cen_total(const DevParams& P, const Fields<NS, R>& F, const CellTaus<R>& t, int d, int i, int j, int k) {
+    double v = (double)t.s[d];
+    v -= (double)t.d[d];
+    if (P.advection_type >= 0) {
+        const Arr4<const double>& m = F.mom[d];
+        const Arr4<const double>& u = F.vel[d];
+        const int e0 = d == 0, e1 = d == 1, e2 = d == 2;
+        v += 0.25 * (m(i, j, k) + m(i + e0, j + e1, k + e2)) * (u(i, j, k) + u(i + e0, j + e1, k + e2)) + F.p(i, j, k);
+    }
+    return v;
+}
+
+}  // namespace fhd

@@ -1,0 +1,66 @@
+// fhd_host.h — host-side launch descriptors shared by the C ABI and the kernel
+// translation units (fhd_exact.cu: FP64 in the reference's operation order,
+// built with -fmad=false; fhd_mixed.cu: FP32 fluxes/coefficients).
+#pragma once
+#include <cuda_runtime.h>
+#include "../../include/fhd_capi.h"
+#include "fhd_device.cuh"
+
+namespace fhd {
+
+enum NoiseMode { NM_OFF = 0, NM_W = 1, NM_AB = 2, NM_PHILOX = 3 };
+
+struct NoiseFabs {
+    fhd_fab fa[3], fb[3];   // faces (W or A/B)
+    fhd_fab ea[3], eb[3];   // xy, xz, yz edges
+    fhd_fab ca[3], cb[3];   // centres
+};
+
+// Everything one stage (or one flux-operator call) reads and writes.
+struct StageCall {
+    DevParams P;
+    int mode;               // NoiseMode
+    double w;               // stage weight of B
+    int stage;              // 1..3 (0: flux operator only)
+    fhd_fab cons_s, mom_s[3];   // stage input U^s
+    fhd_fab cons0, mom0[3];     // U^0
+    fhd_fab cons_o, mom_o[3];   // U^{s+1}
+    fhd_fab pr;             // T at comp pT, p, Y, X follow
+    int pT;
+    fhd_fab vel[3];
+    fhd_fab eta, zeta, kappa, chi, D;   // coefficient fabs (f64, or f32 when mixed)
+    fhd_fab src;            // data == NULL: no source
+    NoiseFabs nz;
+    fhd_fab ff[3], ef[6], cf[3];        // flux outputs of the operator path
+    int* status;
+    cudaStream_t stream;
+    int tile;               // tile-shape index of k_stage (autotuned)
+};
+
+// exact (FP64) translation unit
+int exact_cellprep(const StageCall& c);
+int exact_stage(const StageCall& c);
+int exact_aux_fluxes(const StageCall& c);
+int exact_transport(const DevParams& P, fhd_fab prim, fhd_fab eta, fhd_fab zeta, fhd_fab kappa, fhd_fab chi,
+                    fhd_fab D, int* status, cudaStream_t s);
+int exact_convert(const DevParams& P, fhd_fab prim, const fhd_fab vel[3], fhd_fab cons, const fhd_fab mom[3],
+                  int* status, cudaStream_t s);
+// mixed translation unit (coefficient fabs are f32)
+int mixed_cellprep(const StageCall& c);
+int mixed_stage(const StageCall& c);
+
+// utilities (exact TU)
+struct GhostReq {
+    fhd_fab f;
+    int c0, nc;
+};
+int fill_ghosts(const GhostReq* reqs, int n, const int ncell[3], cudaStream_t s);
+int override_sync(const fhd_fab& f, const int ncell[3], cudaStream_t s);
+int noise_fill(const DevParams& P, const fhd_fab& f, int c0, int nc, double mean, double sd, uint32_t fid0, int use_b,
+               cudaStream_t s);
+int init_uniform(const fhd_fab& cu, int ns, double rho0, double rhoE, const double* rhoY, cudaStream_t s);
+
+int num_tiles();
+const char* tile_name(int t);
+
+}  // namespace fhd

@@ -1,0 +1,88 @@
+// fhd_kern_ns.cu — kernel instantiations for one species count, compiled once per
+// (FHD_NS, precision) pair so the build runs in parallel:
+//   -DFHD_NS=<n>                 exact FP64 (built with -fmad=false)
+//   -DFHD_NS=<n> -DFHD_MIXED=1   mixed precision (FP32 compute)
+#include "fhd_launch.cuh"
+
+#ifndef FHD_NS
+#error "FHD_NS must be defined"
+#endif
+
+#define FHD_CAT2(a, b) a##b
+#define FHD_CAT(a, b) FHD_CAT2(a, b)
+
+namespace fhd {
+
+#if defined(FHD_MIXED) && FHD_MIXED
+int FHD_CAT(mixed_cellprep_ns, FHD_NS)(const StageCall& c) { return launch_cellprep<FHD_NS, float>(c); }
+int FHD_CAT(mixed_stage_ns, FHD_NS)(const StageCall& c) { return launch_stage<FHD_NS, float>(c); }
+#else
+int FHD_CAT(exact_cellprep_ns, FHD_NS)(const StageCall& c) { return launch_cellprep<FHD_NS, double>(c); }
+int FHD_CAT(exact_stage_ns, FHD_NS)(const StageCall& c) { return launch_stage<FHD_NS, double>(c); }
+
+template <int NS, int NZ>
+int launch_aux_t(const StageCall& c) {
+    AuxArgs<NS, double, NZ> a;
+    a.P = c.P;
+    a.F = make_fields<NS, double>(c);
+    a.noise = make_noise<NZ>(c);
+    for (int d = 0; d < 3; ++d) {
+        a.ff[d] = view<double>(c.ff[d]);
+        a.cf[d] = view<double>(c.cf[d]);
+    }
+    for (int e = 0; e < 6; ++e) a.ef[e] = view<double>(c.ef[e]);
+    const int* N = c.P.n;
+    const int64_t nf = (int64_t)(N[0] + 1) * N[1] * N[2] + (int64_t)N[0] * (N[1] + 1) * N[2] +
+                       (int64_t)N[0] * N[1] * (N[2] + 1);
+    const int64_t ne = (int64_t)(N[0] + 1) * (N[1] + 1) * N[2] + (int64_t)(N[0] + 1) * N[1] * (N[2] + 1) +
+                       (int64_t)N[0] * (N[1] + 1) * (N[2] + 1) + (int64_t)(N[0] + 2) * (N[1] + 2) * (N[2] + 2);
+    if (c.ff[0].data) k_aux_faces<NS, double, NZ><<<grid_for(nf, 128), 128, 0, c.stream>>>(a);
+    if (c.ef[0].data) k_aux_edges_cen<NS, double, NZ><<<grid_for(ne, 128), 128, 0, c.stream>>>(a);
+    return cuda_rc(cudaGetLastError());
+}
+
+int FHD_CAT(exact_aux_ns, FHD_NS)(const StageCall& c) {
+    switch (c.mode) {
+        case NM_OFF: return launch_aux_t<FHD_NS, NZ_OFF>(c);
+        case NM_W: return launch_aux_t<FHD_NS, NZ_W>(c);
+        case NM_AB: return launch_aux_t<FHD_NS, NZ_AB>(c);
+        case NM_PHILOX: return launch_aux_t<FHD_NS, NZ_PHILOX>(c);
+        default: return FHD_ERR_BAD_ARG;
+    }
+}
+
+int FHD_CAT(exact_transport_ns, FHD_NS)(const DevParams& P, fhd_fab prim, fhd_fab eta, fhd_fab zeta, fhd_fab kappa,
+                                        fhd_fab chi, fhd_fab D, int* status, cudaStream_t s) {
+    TransArgs<FHD_NS> a;
+    a.P = P;
+    a.prim = view<const double>(prim);
+    a.eta = view<double>(eta);
+    a.zeta = view<double>(zeta);
+    a.kappa = view<double>(kappa);
+    a.chi = view<double>(chi);
+    a.D = view<double>(D);
+    a.ng = -prim.lo[0];
+    a.status = status;
+    const int64_t tot = (int64_t)(P.n[0] + 2 * a.ng) * (P.n[1] + 2 * a.ng) * (P.n[2] + 2 * a.ng);
+    k_transport<FHD_NS><<<grid_for(tot, 128), 128, 0, s>>>(a);
+    return cuda_rc(cudaGetLastError());
+}
+
+int FHD_CAT(exact_convert_ns, FHD_NS)(const DevParams& P, fhd_fab prim, const fhd_fab vel[3], fhd_fab cons,
+                                      const fhd_fab mom[3], int* status, cudaStream_t s) {
+    ConvArgs<FHD_NS> a;
+    a.P = P;
+    a.prim = view<double>(prim);
+    a.cons = view<double>(cons);
+    for (int d = 0; d < 3; ++d) {
+        a.vel[d] = view<double>(vel[d]);
+        a.mom[d] = view<const double>(mom[d]);
+    }
+    a.status = status;
+    const int64_t tot = (int64_t)P.n[0] * P.n[1] * P.n[2];
+    k_convert<FHD_NS><<<grid_for(tot, 128), 128, 0, s>>>(a);
+    return cuda_rc(cudaGetLastError());
+}
+#endif
+
+}  // namespace fhd

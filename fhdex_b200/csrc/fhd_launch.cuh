@@ -1,0 +1,148 @@
+// fhd_launch.cuh — templated launchers included by each kernel translation unit.
+#pragma once
+#include "fhd_host.h"
+#include "fhd_kernels.cuh"
+
+namespace fhd {
+
+template <class T>
+inline Arr4<T> view(const fhd_fab& f, int comp0 = 0) {
+    Arr4<T> a;
+    const int64_t nx = f.hi[0] - f.lo[0] + 1, ny = f.hi[1] - f.lo[1] + 1, nz = f.hi[2] - f.lo[2] + 1;
+    a.lo0 = f.lo[0];
+    a.lo1 = f.lo[1];
+    a.lo2 = f.lo[2];
+    a.sy = nx;
+    a.sz = nx * ny;
+    a.sn = nx * ny * nz;
+    a.p = f.data ? static_cast<T*>(f.data) + comp0 * a.sn : nullptr;
+    return a;
+}
+
+inline int grid_for(int64_t items, int block, int cap = 148 * 32) {
+    int64_t g = (items + block - 1) / block;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+inline int cuda_rc(cudaError_t e) { return e == cudaSuccess ? FHD_OK : FHD_ERR_CUDA; }
+
+template <int NS, class R>
+Fields<NS, R> make_fields(const StageCall& c) {
+    Fields<NS, R> F;
+    F.cons = view<const double>(c.cons_s);
+    for (int d = 0; d < 3; ++d) {
+        F.mom[d] = view<const double>(c.mom_s[d]);
+        F.vel[d] = view<const double>(c.vel[d]);
+    }
+    F.pr = view<const double>(c.pr);
+    F.pT = c.pT;
+    F.eta = view<const R>(c.eta);
+    F.zeta = view<const R>(c.zeta);
+    F.kappa = view<const R>(c.kappa);
+    F.chi = view<const R>(c.chi);
+    F.D = view<const R>(c.D);
+    return F;
+}
+
+template <int MODE>
+Noise<MODE> make_noise(const StageCall& c) {
+    Noise<MODE> n;
+    n.w = c.w;
+    for (int d = 0; d < 3; ++d) {
+        n.a.fa[d] = view<const double>(c.nz.fa[d]);
+        n.a.fb[d] = view<const double>(c.nz.fb[d]);
+        n.a.foa[d] = c.nz.fa[d].ncomp - (c.P.ns + 1);
+        n.a.fob[d] = c.nz.fb[d].ncomp - (c.P.ns + 1);
+        n.a.ea[d] = view<const double>(c.nz.ea[d]);
+        n.a.eb[d] = view<const double>(c.nz.eb[d]);
+        n.a.ca[d] = view<const double>(c.nz.ca[d]);
+        n.a.cb[d] = view<const double>(c.nz.cb[d]);
+    }
+    return n;
+}
+
+template <int NS, class R>
+int launch_cellprep(const StageCall& c) {
+    PrepArgs<NS, R> a;
+    a.P = c.P;
+    a.cons = view<const double>(c.cons_s);
+    for (int d = 0; d < 3; ++d) {
+        a.mom[d] = view<const double>(c.mom_s[d]);
+        a.vel[d] = view<double>(c.vel[d]);
+    }
+    a.pr = view<double>(c.pr, c.pT);
+    a.eta = view<R>(c.eta);
+    a.zeta = view<R>(c.zeta);
+    a.kappa = view<R>(c.kappa);
+    a.chi = view<R>(c.chi);
+    a.D = view<R>(c.D);
+    a.status = c.status;
+    const int64_t tot = (int64_t)(c.P.n[0] + 3) * (c.P.n[1] + 3) * (c.P.n[2] + 3);
+    k_cellprep<NS, R><<<grid_for(tot, 128), 128, 0, c.stream>>>(a);
+    return cuda_rc(cudaGetLastError());
+}
+
+template <int NS, class R, int NZ, int TX, int TY, int TZ>
+int launch_stage_t(const StageCall& c) {
+    StageArgs<NS, R, NZ> a;
+    a.P = c.P;
+    a.F = make_fields<NS, R>(c);
+    a.noise = make_noise<NZ>(c);
+    a.cons0 = view<const double>(c.cons0);
+    a.cons_o = view<double>(c.cons_o);
+    for (int d = 0; d < 3; ++d) {
+        a.mom0[d] = view<const double>(c.mom0[d]);
+        a.mom_o[d] = view<double>(c.mom_o[d]);
+    }
+    a.src = view<const double>(c.src);
+    a.stage = c.stage;
+    using SM = StageSmem<NS, R, TX, TY, TZ>;
+    const size_t smem = sizeof(SM);
+    auto kern = k_stage<NS, R, NZ, TX, TY, TZ>;
+    static bool attr_set = false;  // per instantiation
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return FHD_ERR_CUDA;
+        attr_set = true;
+    }
+    const int ntiles = ((c.P.n[0] + TX - 1) / TX) * ((c.P.n[1] + TY - 1) / TY) * ((c.P.n[2] + TZ - 1) / TZ);
+    kern<<<ntiles, TX * TY * TZ, smem, c.stream>>>(a);
+    return cuda_rc(cudaGetLastError());
+}
+
+// tile shapes available to the autotuner
+#define FHD_TILES(X) X(8, 8, 4) X(16, 4, 4) X(8, 4, 4) X(16, 8, 2)
+
+template <int NS, class R, int NZ>
+int launch_stage_tiles(const StageCall& c) {
+    int t = 0;
+#define FHD_TRY(a, b, d)                                                      \
+    if (c.tile == t) return launch_stage_t<NS, R, NZ, a, b, d>(c);          \
+    ++t;
+    FHD_TILES(FHD_TRY)
+#undef FHD_TRY
+    return launch_stage_t<NS, R, NZ, 8, 8, 4>(c);
+}
+
+template <int NS, class R>
+int launch_stage(const StageCall& c) {
+    switch (c.mode) {
+        case NM_OFF: return launch_stage_tiles<NS, R, NZ_OFF>(c);
+        case NM_AB: return launch_stage_tiles<NS, R, NZ_AB>(c);
+        case NM_PHILOX: return launch_stage_tiles<NS, R, NZ_PHILOX>(c);
+        default: return FHD_ERR_BAD_ARG;
+    }
+}
+
+#define FHD_NS_SWITCH(ns, CALL) \
+    switch (ns) {                \
+        case 1: return CALL(1);  \
+        case 2: return CALL(2);  \
+        case 3: return CALL(3);  \
+        case 4: return CALL(4);  \
+        default: return FHD_ERR_UNSUPPORTED; \
+    }
+
+}  // namespace fhd

@@ -1,0 +1,205 @@
+"""Physics/grid parameters with the reference's defaults and inputs-deck keys.
+
+Defaults follow ``InitializeCommonNamespace`` (common_functions.cpp:332-550) and
+``InitializeCompressibleNamespace`` (compressible_functions.cpp:15-88): k_B,
+Runiv, e0 = 0, visc_type 1, advection_type 0, stoch_stress_form 1,
+transport_type 1.  ``parse_inputs`` reads an FHDeX inputs deck (``key = values``
+with ``#`` comments) using the same key names.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from dataclasses import dataclass, field
+
+from .capi import MAX_SPECIES, FhdParams
+
+K_B = 1.38064852e-16
+RUNIV = 8.314462175e7
+
+
+@dataclass
+class Params:
+    nspecies: int = 2
+    n_cells: tuple = (32, 32, 32)
+    prob_lo: tuple = (0.0, 0.0, 0.0)
+    prob_hi: tuple = (3.2e-5, 3.2e-5, 3.2e-5)
+    molmass: tuple = (39.95, 39.95)
+    diameter: tuple = (3.66e-8, 3.66e-8)
+    dof: tuple = (3.0, 3.0)
+    e0: tuple = (0.0, 0.0)
+    hcv: tuple = (-1.0, -1.0)
+    hcp: tuple = (-1.0, -1.0)
+    k_B: float = K_B
+    Runiv: float = RUNIV
+    grav: tuple = (0.0, 0.0, 0.0)
+    zeta_ratio: float = -1.0
+    algorithm_type: int = 2
+    visc_type: int = 2
+    advection_type: int = 2
+    transport_type: int = 1
+    stoch_stress_form: int = 1
+    precision: int = 0
+    seed: int = 1
+    # initial state (prob_type 1): not part of fhd_params
+    rho0: float = 1.78e-3
+    T_init: float = 273.0
+    rhobar: tuple = (0.5, 0.5)
+    ngc: int = 2
+
+    @property
+    def nvars(self):
+        return 5 + self.nspecies
+
+    @property
+    def nprimvars(self):
+        return 6 + 2 * self.nspecies
+
+    @property
+    def dx(self):
+        return tuple((self.prob_hi[d] - self.prob_lo[d]) / self.n_cells[d] for d in range(3))
+
+    def replace(self, **kw):
+        return dataclasses.replace(self, **kw)
+
+    def hc(self):
+        """(hcv, hcp) as GetHcGas derives them (compressible_functions.cpp:91-100)."""
+        hcv, hcp = [], []
+        for i in range(self.nspecies):
+            v = self.hcv[i] if self.hcv[i] >= 0 else 0.5 * self.dof[i] * self.Runiv / self.molmass[i]
+            p = self.hcp[i] if self.hcp[i] >= 0 else 0.5 * (2.0 + self.dof[i]) * self.Runiv / self.molmass[i]
+            hcv.append(v)
+            hcp.append(p)
+        return hcv, hcp
+
+    def to_c(self) -> FhdParams:
+        p = FhdParams()
+        p.nspecies = self.nspecies
+        for d in range(3):
+            p.n_cells[d] = self.n_cells[d]
+            p.prob_lo[d] = self.prob_lo[d]
+            p.prob_hi[d] = self.prob_hi[d]
+            p.grav[d] = self.grav[d]
+        for name in ("molmass", "diameter", "dof", "e0", "hcv", "hcp"):
+            src = getattr(self, name)
+            dst = getattr(p, name)
+            for i in range(MAX_SPECIES):
+                dst[i] = src[i] if i < len(src) else (0.0 if name in ("e0",) else (-1.0 if name in ("hcv", "hcp") else 1.0))
+        p.k_B = self.k_B
+        p.Runiv = self.Runiv
+        p.zeta_ratio = self.zeta_ratio
+        p.algorithm_type = self.algorithm_type
+        p.visc_type = self.visc_type
+        p.advection_type = self.advection_type
+        p.transport_type = self.transport_type
+        p.stoch_stress_form = self.stoch_stress_form
+        p.precision = self.precision
+        p.seed = self.seed & 0xFFFFFFFFFFFFFFFF
+        return p
+
+    # -- thermodynamics on the host (for dt and theory) -------------------------------
+    def sound_speed(self, T=None, Y=None):
+        """GetSoundSpeed, compressible_functions.H:201-219."""
+        T = self.T_init if T is None else T
+        Y = self.rhobar if Y is None else Y
+        hcv, hcp = self.hc()
+        molmix = sum(Y[n] / self.molmass[n] for n in range(self.nspecies))
+        molmix = 1.0 / molmix
+        cv = sum(Y[n] * hcv[n] for n in range(self.nspecies))
+        cp = sum(Y[n] * hcp[n] for n in range(self.nspecies))
+        return math.sqrt(cp / cv * (self.Runiv / molmix) * T)
+
+
+def argon(n=32, dx=1e-6, **kw) -> Params:
+    """'Single-species' argon in the reference's parity form: two identical species
+    (molmass 39.95, d = 3.66e-8 cm), rho0 = 1.78e-3 g/cm^3, T0 = 273 K."""
+    n3 = (n, n, n) if isinstance(n, int) else tuple(n)
+    base = Params(nspecies=2, n_cells=n3, prob_hi=tuple(dx * n3[d] for d in range(3)),
+                  molmass=(39.95, 39.95), diameter=(3.66e-8, 3.66e-8), dof=(3.0, 3.0),
+                  e0=(0.0, 0.0), hcv=(-1.0, -1.0), hcp=(-1.0, -1.0), rhobar=(0.5, 0.5))
+    return base.replace(**kw)
+
+
+def mixture4(n=32, dx=1e-6, **kw) -> Params:
+    """4-species ideal-gas mixture (Ar/Ne/Kr/He), equal mass fractions."""
+    n3 = (n, n, n) if isinstance(n, int) else tuple(n)
+    base = Params(nspecies=4, n_cells=n3, prob_hi=tuple(dx * n3[d] for d in range(3)),
+                  molmass=(39.95, 20.18, 83.80, 4.00),
+                  diameter=(3.66e-8, 2.58e-8, 4.16e-8, 2.18e-8), dof=(3.0,) * 4,
+                  e0=(0.0,) * 4, hcv=(-1.0,) * 4, hcp=(-1.0,) * 4, rhobar=(0.25,) * 4)
+    return base.replace(**kw)
+
+
+def hard_sphere_single_gas(p: Params, T=None):
+    """Closed-form first Chapman-Enskog hard-sphere viscosity and conductivity of a
+    pure gas: eta = 5/(16 d^2) sqrt(m k T / pi), kappa = (75/64)(k/d^2) sqrt(kT/(pi m)).
+    These are what the Giovangigli formulas (compressible_functions.H:1218-1326)
+    reduce to for identical species."""
+    T = p.T_init if T is None else T
+    m = p.molmass[0] * p.k_B / p.Runiv
+    d = p.diameter[0]
+    eta = 5.0 / (16.0 * d * d) * math.sqrt(m * p.k_B * T / math.pi)
+    kappa = 75.0 / 64.0 * p.k_B / (d * d) * math.sqrt(p.k_B * T / (math.pi * m))
+    return eta, kappa
+
+
+def stable_dt(p: Params, cfl=0.2, diff=0.1):
+    """dt = min(cfl*dx/(c+|u|), diff*dx^2/max(nu, chi)) at the initial state (|u| = 0).
+    The configured acoustic CFL 0.2 alone violates the explicit diffusive limit at
+    dx = 1e-6 cm, so the diffusive bound is applied too."""
+    dx = min(p.dx)
+    c = p.sound_speed()
+    hcv, _ = p.hc()
+    cv = sum(p.rhobar[n] * hcv[n] for n in range(p.nspecies))
+    # bound the mixture's diffusivities by each species' pure-gas hard-sphere value
+    # at the mixture's density and heat capacity (conservative for mixtures)
+    dmax = 0.0
+    for s in range(p.nspecies):
+        q = p.replace(molmass=(p.molmass[s],), diameter=(p.diameter[s],))
+        eta, kappa = hard_sphere_single_gas(q)
+        dmax = max(dmax, eta / p.rho0, kappa / (p.rho0 * cv))
+    return min(cfl * dx / c, diff * dx * dx / dmax)
+
+
+_LIST_KEYS = ("n_cells", "prob_lo", "prob_hi", "molmass", "diameter", "dof", "e0", "hcv",
+              "hcp", "rhobar", "grav", "T_init")
+
+
+def parse_inputs(text: str, base: Params | None = None) -> Params:
+    """Parse an FHDeX inputs deck (reference key names) into Params.  Keys outside
+    this path (plot_int, struct_fact_int, bc_*, ...) are ignored; only fully
+    periodic decks are accepted."""
+    kv = {}
+    for line in text.splitlines():
+        line = line.split("#", 1)[0].strip()
+        if "=" not in line:
+            continue
+        k, v = line.split("=", 1)
+        kv[k.strip()] = v.split()
+    p = base or Params()
+    upd = {}
+    ns = int(kv["nspecies"][0]) if "nspecies" in kv else p.nspecies
+    upd["nspecies"] = ns
+    for key in _LIST_KEYS:
+        if key in kv:
+            vals = [float(x) for x in kv[key]]
+            if key == "n_cells":
+                vals = [int(x) for x in vals]
+            if key == "T_init":
+                upd["T_init"] = vals[0]
+                continue
+            upd[key] = tuple(vals)
+    for key in ("rho0", "k_B", "Runiv", "zeta_ratio"):
+        if key in kv:
+            upd[key] = float(kv[key][0])
+    for key in ("algorithm_type", "visc_type", "advection_type", "transport_type",
+                "stoch_stress_form", "seed"):
+        if key in kv:
+            upd[key] = int(kv[key][0])
+    for key in ("bc_vel_lo", "bc_vel_hi", "bc_mass_lo", "bc_mass_hi", "bc_therm_lo", "bc_therm_hi"):
+        if key in kv and any(int(x) != -1 for x in kv[key]):
+            raise ValueError(f"{key}: only fully periodic boundaries are implemented")
+    if "dof" in upd and "hcv" not in upd:
+        upd["hcv"] = (-1.0,) * ns
+        upd["hcp"] = (-1.0,) * ns
+    return p.replace(**upd)

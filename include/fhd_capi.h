@@ -1,0 +1,227 @@
+/*
+ * fhd_capi.h — C ABI of the B200-native compressible staggered-grid FHD step.
+ *
+ * Drop-in boundary for FHDeX's explicit compressible staggered-grid step.  Every
+ * entry point below replaces one C++ free function of the reference; the
+ * reference function it stands for is cited beside it (paths are relative to the
+ * FHDeX source tree).  The reference passes AMReX MultiFabs and reads physics
+ * parameters from global namespaces (common::, compressible::); here a MultiFab
+ * of one box is an `fhd_fab` (plain pointer + AMReX Array4 geometry) and the
+ * parameters live in an `fhd_params` given once to `fhd_create`.
+ *
+ * Data layout (identical to AMReX Array4): element (i,j,k,n) of a fab is at
+ *   data[(i-lo0) + (j-lo1)*nx + (k-lo2)*nx*ny + n*nx*ny*nz],  nx = hi0-lo0+1, ...
+ * i.e. Fortran order with the component slowest.  lo/hi are ghost-inclusive and
+ * inclusive.  A fab that is nodal in direction d has valid indices 0..n_cells[d]
+ * in d; a cell-centred one 0..n_cells[d]-1.  Ghost width = -lo[d].
+ *
+ * Memory: fabs handed to the compute entry points are DEVICE pointers on the
+ * context's device unless the entry point says otherwise (the *_host variants
+ * take host pointers and copy).  All work is ordered on the context's stream;
+ * calls return after enqueueing unless stated.  No entry point aborts the
+ * process: failures are returned as FHD_ERR_* codes; physics faults detected on
+ * the device (non-positive/over-unity mass fraction, non-finite temperature) are
+ * latched in a device status word and returned by fhd_status().
+ *
+ * Threading: one host thread at a time per context.
+ */
+#ifndef FHD_CAPI_H
+#define FHD_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FHD_MAX_SPECIES 8
+
+/* return / status codes */
+enum {
+    FHD_OK = 0,
+    FHD_ERR_BAD_ARG = 1,     /* shape, dtype or parameter rejected on the host   */
+    FHD_ERR_MASSFRAC = 2,    /* Y <= 0 or Y >= 1 seen (transCoeffs.cpp:45-46)     */
+    FHD_ERR_NONFINITE = 3,   /* non-finite temperature/pressure produced          */
+    FHD_ERR_OOM = 4,         /* device allocation failed                          */
+    FHD_ERR_TIMEOUT = 5,     /* a bounded device wait gave up                     */
+    FHD_ERR_CUDA = 6,        /* a CUDA runtime call failed                        */
+    FHD_ERR_UNSUPPORTED = 7  /* option outside the implemented scope              */
+};
+
+/* fab element types */
+enum { FHD_F64 = 0, FHD_F32 = 1 };
+
+/* precision modes of the step */
+enum {
+    FHD_PREC_FP64 = 0,   /* every operation in FP64, reference operation order     */
+    FHD_PREC_MIXED = 1   /* FP32 fluxes/coefficients, FP64 state and RK sums       */
+};
+
+/* One box of an AMReX MultiFab (Array4 view).  `nodal[d]` = 1 for a
+ * face/edge-centred direction (AMReX IndexType). */
+typedef struct {
+    void* data;
+    int lo[3];
+    int hi[3];
+    int ncomp;
+    int nodal[3];
+    int dtype;
+} fhd_fab;
+
+/* Physics and grid parameters.  Field names follow the reference's inputs-deck
+ * keys (common_functions.cpp:293-1010, compressible_functions.cpp:15-88).
+ * hcv/hcp < 0 are derived from dof as GetHcGas does
+ * (compressible_functions.cpp:91-100). */
+typedef struct {
+    int nspecies;
+    int n_cells[3];
+    double prob_lo[3];
+    double prob_hi[3];
+    double molmass[FHD_MAX_SPECIES];
+    double diameter[FHD_MAX_SPECIES];
+    double dof[FHD_MAX_SPECIES];
+    double e0[FHD_MAX_SPECIES];
+    double hcv[FHD_MAX_SPECIES];
+    double hcp[FHD_MAX_SPECIES];
+    double k_B;
+    double Runiv;
+    double grav[3];
+    double zeta_ratio;
+    int algorithm_type;     /* only 2 (multispecies) is accepted, as in every stag deck */
+    int visc_type;          /* 1, 2 or 3 (|visc_type| == 3 adds bulk viscosity)         */
+    int advection_type;     /* 0, 1 or 2                                               */
+    int transport_type;     /* only 1 (Giovangigli) is accepted                         */
+    int stoch_stress_form;  /* 0 (no noise) or 1                                       */
+    int precision;          /* FHD_PREC_*                                               */
+    uint64_t seed;          /* key of the in-kernel Philox noise                        */
+} fhd_params;
+
+/* Injected Gaussian noise for one RK3 step: the "A" and "B" white-noise fields
+ * that RK3stepStag fills once per step (timeStepStag.cpp:99-223) and combines as
+ * W = A + w_s B per stage (timeStepStag.cpp:237/568/901).  Index [0] = A,
+ * [1] = B.  face[.][d]: nodal in d, 0 ghosts; the energy noise is component
+ * ncomp-(nspecies+1) and the species noises follow it (with ncomp = nvars this
+ * is the reference's component 4..nvars-1).  edge[.][e]: e = 0 xy, 1 xz, 2 yz
+ * edges, 0 ghosts (the reference's stochedge_x[0], stochedge_x[1],
+ * stochedge_y[1]; the other three edge fields it fills are never read,
+ * fluxStag.cpp:130-132).  cen[.][d]: cell-centred with 1 ghost, variance 2 in
+ * 3D.  Values must already be OverrideSync'ed/FillBoundary'ed, as
+ * MultiFabFillRandomNormal leaves them. */
+typedef struct {
+    fhd_fab face[2][3];
+    fhd_fab edge[2][3];
+    fhd_fab cen[2][3];
+} fhd_noise;
+
+typedef struct fhd_ctx fhd_ctx;
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Validates params, derives hcv/hcp, binds `device`, creates a stream. */
+int fhd_create(fhd_ctx** ctx, const fhd_params* params, int device);
+int fhd_destroy(fhd_ctx* ctx);
+const char* fhd_strerror(int code);
+/* Use an external CUDA stream (cudaStream_t as void*); NULL = the context's own. */
+int fhd_set_stream(fhd_ctx* ctx, void* stream);
+int fhd_synchronize(fhd_ctx* ctx);
+/* Reads and clears the device status word (blocks on the stream). */
+int fhd_status(fhd_ctx* ctx);
+/* Effective parameters (after GetHcGas). */
+int fhd_get_params(const fhd_ctx* ctx, fhd_params* out);
+/* Tile shape of the fused stage kernel (index into fhd_tile_name's list); the
+ * autotuner in the Python host layer times them and sets the fastest.  No
+ * reference counterpart (AMReX picks its own launch shapes). */
+int fhd_set_tile(fhd_ctx* ctx, int tile);
+int fhd_num_tiles(void);
+const char* fhd_tile_name(int tile);
+
+/* ---- reference operators -------------------------------------------------- */
+
+/* InitConsVarStag, prob_type 1 (uniform state at rest):
+ * compressible_functions_stag.cpp:36-56.  Fills every point incl. ghosts. */
+int fhd_init_cons_var_stag(fhd_ctx* ctx, fhd_fab cu, const fhd_fab mom[3],
+                           double rho0, double T_init, const double* rhobar);
+
+/* conservedToPrimitiveStag: conservedPrimitiveConversionsStag.cpp:5-144
+ * (declared compressible_functions_stag.H:69-70).  Writes vel on valid faces,
+ * prim and cu components 1..3 on valid cells; ghosts are left to
+ * fhd_fill_boundary, as in the reference. */
+int fhd_conserved_to_primitive_stag(fhd_ctx* ctx, fhd_fab prim, const fhd_fab vel[3],
+                                    fhd_fab cu, const fhd_fab mom[3]);
+
+/* calculateTransportCoeffs (Giovangigli model): transCoeffs.cpp:7-90
+ * (declared compressible_functions.H:37-39).  Fills eta, zeta, kappa, chi, D on
+ * the cell box grown by the ghost width of prim. */
+int fhd_transport_coeffs(fhd_ctx* ctx, fhd_fab prim, fhd_fab eta, fhd_fab zeta,
+                         fhd_fab kappa, fhd_fab chi, fhd_fab D);
+
+/* calculateFluxStag: fluxStag.cpp:5-1868 (declared
+ * compressible_functions_stag.H:127-143).  edgeflux[6] = {edgeflux_x[0..1],
+ * edgeflux_y[0..1], edgeflux_z[0..1]}; stochedge[3] = {xy, xz, yz} combined
+ * noise; stochface[3]/stochcen[3] combined noise W (already weighted). */
+int fhd_flux_stag(fhd_ctx* ctx, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim,
+                  const fhd_fab vel[3], fhd_fab eta, fhd_fab zeta, fhd_fab kappa,
+                  fhd_fab chi, fhd_fab D, const fhd_fab faceflux[3],
+                  const fhd_fab edgeflux[6], const fhd_fab cenflux[3],
+                  const fhd_fab stochface[3], const fhd_fab stochedge[3],
+                  const fhd_fab stochcen[3], double dt);
+
+/* MultiFab::FillBoundary(periodicity) for a fully periodic single box:
+ * ghosts <- periodic images of valid points; valid points untouched. */
+int fhd_fill_boundary(fhd_ctx* ctx, fhd_fab f);
+/* MultiFab::OverrideSync(periodicity): periodic duplicates of nodal points take
+ * the value of the low-side owner (point n_cells[d] <- point 0). */
+int fhd_override_sync(fhd_ctx* ctx, fhd_fab f);
+
+/* MultiFabFillRandomNormal: MultiFabFillRandom.cpp:34-50 (declared
+ * rng_functions.H:13-22).  Philox-4x32-10 normals; `stream_id` selects an
+ * independent stream under the context's seed. */
+int fhd_fill_random_normal(fhd_ctx* ctx, fhd_fab mf, int scomp, int ncomp, double mean,
+                           double variance, int overridesync, int fillboundary,
+                           uint64_t stream_id);
+
+/* Fills `noise` with exactly the A/B fields the fused step generates
+ * in-kernel for (seed, step): lets a caller replay an in-kernel-noise step
+ * through the injected-noise path. */
+int fhd_fill_step_noise(fhd_ctx* ctx, const fhd_noise* noise, int64_t step);
+
+/* RK3stepStag: timeStepStag.cpp:13-1245 (declared
+ * compressible_functions_stag.H:113-125).  Advances cu/mom/prim/vel by one
+ * SSP-RK3 step in place (ghosts refreshed, as after the reference's final
+ * FillBoundary).  source: nprimvars-component cell fab (the reference's
+ * `source`, all zeros unless chemistry is on) or data == NULL for zero.
+ * eta..D receive the stage-3 transport coefficients and faceflux/edgeflux/
+ * cenflux the stage-3 fluxes when their data pointers are non-NULL (pass NULL
+ * arrays to skip them; the fused path then never materialises them).
+ * injected == NULL -> Philox noise generated in-kernel from (seed, step). */
+int fhd_rk3_step_stag(fhd_ctx* ctx, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim,
+                      const fhd_fab vel[3], fhd_fab source, fhd_fab eta, fhd_fab zeta,
+                      fhd_fab kappa, fhd_fab chi, fhd_fab D, const fhd_fab* faceflux,
+                      const fhd_fab* edgeflux, const fhd_fab* cenflux,
+                      const fhd_noise* injected, double dt, int64_t step);
+
+/* RK3stepStag on HOST fabs (same layouts as above, host pointers; pinned memory
+ * gives full copy bandwidth): copies cu/mom/prim/vel to device buffers owned by
+ * the context, advances one step in place there (in-kernel noise, or injected
+ * noise given as host fabs), copies the four fields back and waits for the
+ * stream.  For callers whose MultiFabs live in host memory (a CPU AMReX build);
+ * no reference counterpart beyond RK3stepStag itself. */
+int fhd_rk3_step_stag_host(fhd_ctx* ctx, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim,
+                           const fhd_fab vel[3], const fhd_noise* injected, double dt,
+                           int64_t step, int64_t* h2d_bytes, int64_t* d2h_bytes);
+
+/* Per-kernel timing of the step with CUDA events on the launching stream
+ * (tracing aid in place of the reference's TinyProfiler regions).  Kinds:
+ * 0 cellprep, 1 stage (fused flux/update), 2 ghost fill, 3 conversion,
+ * 4 by-product fluxes.  fhd_profile_read synchronizes, sums the elapsed times
+ * (ms) and launch counts per kind since the last reset, and resets. */
+#define FHD_PROF_KINDS 5
+int fhd_profile(fhd_ctx* ctx, int enable);
+int fhd_profile_read(fhd_ctx* ctx, double* ms, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FHD_CAPI_H */

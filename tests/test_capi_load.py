@@ -1,0 +1,49 @@
+"""CPU checks of the drop-in boundary: the sm_100a library loads, exports every
+entry point include/fhd_capi.h declares, and its structs match the ctypes mirror.
+No compute calls (no GPU here)."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+from fhdex_b200 import capi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "fhd_capi.h")
+
+
+def declared_symbols():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(fhd_\w+)\s*\(", txt, flags=re.M)))
+
+
+def test_library_exists_and_loads():
+    assert os.path.exists(capi.LIB_PATH), "build the library first (python -m fhdex_b200.build)"
+    capi.load()
+
+
+def test_every_declared_entry_point_is_exported():
+    syms = declared_symbols()
+    assert len(syms) >= 15
+    lib = C.CDLL(capi.LIB_PATH)
+    missing = [s for s in syms if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_struct_layouts_match_header(tmp_path):
+    src = tmp_path / "sz.c"
+    src.write_text(f'#include "{HEADER}"\n#include <stdio.h>\n#include <stddef.h>\n'
+                   'int main(){printf("%zu %zu %zu %zu\\n", sizeof(fhd_fab), sizeof(fhd_params), '
+                   'sizeof(fhd_noise), offsetof(fhd_params, seed));return 0;}\n')
+    exe = tmp_path / "sz"
+    subprocess.check_call(["gcc", str(src), "-o", str(exe)])
+    vals = [int(x) for x in subprocess.check_output([str(exe)]).split()]
+    assert vals == [C.sizeof(capi.FhdFab), C.sizeof(capi.FhdParams), C.sizeof(capi.FhdNoise),
+                    capi.FhdParams.seed.offset]
+
+
+def test_strerror_is_callable_without_gpu():
+    lib = capi.load()
+    assert lib.fhd_strerror(capi.FHD_ERR_MASSFRAC).startswith(b"mass fraction")

@@ -1,0 +1,204 @@
+"""GPU parity: the sm_100a kernels through the C ABI against the CPU oracle.
+
+FP64 path: bit-for-bit (tolerance 0) — the kernels keep the reference's
+operation order and are built without FMA contraction; FP64 division and sqrt
+are correctly rounded on both sides.  Mixed path: norm-relative error per field
+against the FP64 oracle, bound stated in the test.
+"""
+import pytest
+import torch
+
+from fhdex_b200.context import Context
+from fhdex_b200.params import argon, mixture4, stable_dt
+from fhdex_b200.state import StagState, StepNoise
+from tests.helpers import compare_named, max_rel, perturbed_state, seeded_noise
+
+pytestmark = pytest.mark.gpu
+
+CASES = [("argon12", lambda **k: argon(12, dx=8e-6, **k)),
+         ("mix4_10x12x8", lambda **k: mixture4((10, 12, 8), dx=8e-6, **k))]
+
+
+def gpu_copy(st):
+    return st.clone(device="cuda")
+
+
+@pytest.mark.parametrize("name,make", CASES)
+def test_conversion_and_transport_bitwise(oracle, name, make):
+    p = make()
+    st = perturbed_state(oracle, p, seed=1)
+    d = gpu_copy(st)
+    ctx = Context(p)
+    ctx.conserved_to_primitive(d)
+    assert oracle.conserved_to_primitive(st) == 0
+    ctx.transport_coeffs(d)
+    assert oracle.transport_coeffs(st) == 0
+    torch.cuda.synchronize()
+    assert ctx.status() == 0
+    names = ["cu", "prim", "vel0", "vel1", "vel2", "eta", "zeta", "kappa", "chi", "D"]
+    bad, _ = compare_named(d.named(aux=True), {n: st.named(aux=True)[n] for n in names})
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("name,make", CASES)
+def test_flux_operator_bitwise(oracle, name, make):
+    p = make()
+    st = perturbed_state(oracle, p, seed=2)
+    assert oracle.transport_coeffs(st) == 0
+    nz = seeded_noise(oracle, p, 3, 0)
+    d = gpu_copy(st)
+    ndev = nz.to("cuda")
+    dt = stable_dt(p)
+    assert oracle.flux_stag(st, nz.face[0], nz.edge[0], nz.cen[0], dt) == 0
+    ctx = Context(p)
+    ctx.flux_stag(d, ndev.face[0], ndev.edge[0], ndev.cen[0], dt)
+    torch.cuda.synchronize()
+    ref = st.named(aux=True)
+    names = [f"faceflux{q}" for q in range(3)] + [f"edgeflux{e}" for e in range(6)] + [f"cenflux{q}" for q in range(3)]
+    bad, _ = compare_named(d.named(aux=True), {n: ref[n] for n in names})
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("name,make,nsteps", [(CASES[0][0], CASES[0][1], 10), (CASES[1][0], CASES[1][1], 3)])
+def test_rk3_step_injected_noise_bitwise(oracle, name, make, nsteps):
+    """RK3stepStag with identical injected A/B noise: state, transport
+    coefficients and stage-3 fluxes equal the oracle bit for bit after every step."""
+    p = make()
+    st = perturbed_state(oracle, p, seed=4)
+    d = gpu_copy(st)
+    ctx = Context(p)
+    dt = stable_dt(p)
+    for s in range(nsteps):
+        nz = seeded_noise(oracle, p, 9, s)
+        assert oracle.rk3_step(st, nz, dt) == 0
+        ctx.rk3_step(d, dt, s, noise=nz.to("cuda"), aux=True)
+        torch.cuda.synchronize()
+        bad, _ = compare_named(d.named(aux=(s == nsteps - 1)), st.named(aux=(s == nsteps - 1)))
+        assert not bad, (s, bad[:8])
+    assert ctx.status() == 0
+
+
+@pytest.mark.parametrize("opt", [dict(advection_type=0), dict(advection_type=1),
+                                 dict(visc_type=3, zeta_ratio=0.7), dict(stoch_stress_form=0),
+                                 dict(grav=(0.0, 0.0, -981.0))])
+def test_rk3_step_options_bitwise(oracle, opt):
+    p = argon(8, dx=8e-6, **opt)
+    st = perturbed_state(oracle, p, seed=5)
+    d = gpu_copy(st)
+    ctx = Context(p)
+    dt = stable_dt(p)
+    for s in range(2):
+        nz = seeded_noise(oracle, p, 13, s)
+        assert oracle.rk3_step(st, nz, dt) == 0
+        ctx.rk3_step(d, dt, s, noise=nz.to("cuda"), aux=True)
+    torch.cuda.synchronize()
+    bad, _ = compare_named(d.named(aux=True), st.named(aux=True))
+    assert not bad, bad[:8]
+
+
+def test_in_kernel_philox_equals_injected_replay(oracle):
+    """The fused step's in-kernel Philox noise is exactly what fhd_fill_step_noise
+    materialises: replaying those arrays through the injected path (GPU) and through
+    the oracle gives the same trajectory bit for bit."""
+    p = argon(12, dx=8e-6, seed=2024)
+    st = perturbed_state(oracle, p, seed=6)
+    a = gpu_copy(st)
+    b = gpu_copy(st)
+    ctx = Context(p)
+    dt = stable_dt(p)
+    nz = StepNoise(p, "cuda")
+    for s in range(3):
+        ctx.rk3_step(a, dt, s, noise=None, aux=False)
+        ctx.fill_step_noise(nz, s)
+        ctx.rk3_step(b, dt, s, noise=nz, aux=False)
+        torch.cuda.synchronize()
+        assert oracle.rk3_step(st, nz.to("cpu"), dt) == 0
+        bad, _ = compare_named(a.named(), b.named())
+        assert not bad, (s, bad[:4])
+        bad, _ = compare_named(a.named(), st.named())
+        assert not bad, (s, bad[:4])
+
+
+def test_all_tile_shapes_identical(oracle):
+    p = argon((12, 10, 9), dx=8e-6)
+    st = perturbed_state(oracle, p, seed=7)
+    dt = stable_dt(p)
+    outs = []
+    for t, name in enumerate(Context.tiles()):
+        d = gpu_copy(st)
+        ctx = Context(p)
+        ctx.set_tile(t)
+        for s in range(2):
+            ctx.rk3_step(d, dt, s, aux=False)
+        torch.cuda.synchronize()
+        outs.append((name, d))
+    for name, d in outs[1:]:
+        bad, _ = compare_named(d.named(), outs[0][1].named())
+        assert not bad, (name, bad[:4])
+
+
+@pytest.mark.parametrize("make", [lambda **k: argon(16, dx=8e-6, **k), lambda **k: mixture4(12, dx=8e-6, **k)])
+def test_mixed_precision_against_fp64_oracle(oracle, make):
+    """Mixed path (FP32 coefficients/stresses/dissipative fluxes, FP64 state and
+    hyperbolic terms) vs the FP64 oracle with identical noise: per-field
+    norm-relative error after 5 steps below 1e-4 (conserved state) / 1e-3
+    (face velocities, which are O(noise))."""
+    p = make(precision=1)
+    st = perturbed_state(oracle, p.replace(precision=0), seed=8)
+    st.p = p.replace(precision=0)
+    d = gpu_copy(st)
+    d.p = p
+    ctx = Context(p)
+    dt = stable_dt(p)
+    for s in range(5):
+        nz = seeded_noise(oracle, p, 17, s)
+        assert oracle.rk3_step(st, nz, dt) == 0
+        ctx.rk3_step(d, dt, s, noise=nz.to("cuda"), aux=False)
+    torch.cuda.synchronize()
+    errs = {}
+    for n, m in st.named().items():
+        g = d.named()[n]
+        for c in range(m.ncomp):
+            errs[f"{n}[{c}]"] = max_rel(g.valid(c), m.valid(c))
+    print({k: f"{v:.2e}" for k, v in errs.items()})
+    for k, v in errs.items():
+        lim = 1e-3 if (k.startswith("vel") or k.startswith("cumom") or k[:6] in ("prim[1", "prim[2", "prim[3", "cu[1]", "cu[2]", "cu[3]")) else 1e-4
+        assert v < lim, (k, v)
+
+
+def test_conservation_philox_64(oracle):
+    p = argon(64, dx=8e-6)
+    st = StagState(p, "cuda")
+    ctx = Context(p)
+    ctx.init_state(st)
+    dt = stable_dt(p)
+    N = 64
+
+    def totals():
+        t = [st.cu.valid(n).sum().item() for n in (0, 4, 5, 6)]
+        t += [m.arr[0, 2:2 + N, 2:2 + N, 2:2 + N].sum().item() for m in st.cumom]
+        return t
+
+    t0 = totals()
+    for s in range(20):
+        ctx.rk3_step(st, dt, s, aux=False)
+    torch.cuda.synchronize()
+    t1 = totals()
+    assert ctx.status() == 0
+    scale = [abs(x) for x in t0[:4]] + [p.rho0 * p.sound_speed() * N ** 3] * 3
+    for a, b, sc in zip(t0, t1, scale):
+        assert abs(a - b) <= 1e-12 * sc
+
+
+def test_massfrac_status_is_reported_not_fatal(oracle):
+    p = argon(8, dx=8e-6)
+    st = perturbed_state(oracle, p, seed=9)
+    d = gpu_copy(st)
+    d.cu[2, 3, 4, 5] = 0.0          # rho*Y_0 = 0 -> Y_0 = 0 at one cell
+    d.cu[2, 3, 4, 6] = d.cu[2, 3, 4, 0]
+    ctx = Context(p)
+    ctx.rk3_step(d, stable_dt(p), 0, aux=False)
+    assert ctx.status() == 2        # FHD_ERR_MASSFRAC
+    # the context stays usable
+    ctx.rk3_step(gpu_copy(st), stable_dt(p), 0, aux=False)
+    assert ctx.status() == 0
