@@ -2,8 +2,10 @@
 """Benchmark of the compressible staggered FHD RK3 step (cell-updates/s).
 
 Workload (default): 'single-species' argon in the reference's parity form (two
-identical species), 256^3 cells, dx = 1e-6 cm, fully periodic, FP64, in-kernel
-Philox noise, dt from the acoustic + diffusive stability rule.  One step = one
+identical species), 256^3 cells, dx = 8e-6 cm (the reference decks' spacing; at
+dx = 1e-6 cm a cell holds ~27 molecules and the reference's own mass-fraction
+guard trips after the first step), fully periodic, FP64, in-kernel Philox
+noise, dt from the acoustic + diffusive stability rule.  One step = one
 SSP-RK3 step of the whole box.  value = cells * steps * ranks / max-over-ranks
 device time; e2e = the same metric through the host-buffer C-ABI call
 (fhd_rk3_step_stag_host: H2D of cu/mom/prim/vel from pinned memory, step, D2H).
@@ -41,8 +43,9 @@ HBM_FALLBACK_GBS = 6650.0
 METRIC = "cell-updates/s (RK3 steps x cells)"
 UNIT = "cell-updates/s"
 
-# DRAM traffic (read + write bytes) of one k_stage launch from an ncu capture,
-# scaled per cell; see profiles/k_stage_argon_ncu.md.  None until captured.
+# DRAM traffic (read + write bytes) of one RK stage (k_taus + 3 x k_faces +
+# k_update) per cell, from the ncu capture summarised in profiles/ (None until
+# captured for that configuration).
 STAGE_TRAFFIC_BYTES_PER_CELL = {}
 
 
@@ -292,23 +295,28 @@ def run_ours(args):
         ms = t.item()
     cells = p.n_cells[0] * p.n_cells[1] * p.n_cells[2]
     value = cells * args.steps * world / (ms / 1e3)
-    launches = sum(v[1] for v in prof.values())
+    # every bracketed profile scope is one launch, except the face-flux scope (3 launches)
+    launches = sum(v[1] for v in prof.values()) + 2 * prof["faces"][1]
 
-    # roofline of the dominant kernel (k_stage): algorithmic bytes per launch from
-    # the per-stage state traffic (stage 1: 2 S, stages 2-3: 3 S doubles per cell,
-    # S = 5 + nspecies) over its CUDA-event launch duration on the launching stream
+    # roofline of the dominant kernel group: one RK stage = k_taus + 3 x k_faces +
+    # k_update (the work of the reference's calculateFluxStag + stage update).
+    # Algorithmic bytes per stage: the conserved state S = 5 + nspecies doubles per
+    # cell read once (stage 1) or twice (U^s and U^0, stages 2-3) and written once;
+    # averaged over the three stages: (2 + 3 + 3)/3 * S * 8 bytes per cell.
     S = 5 + p.nspecies
-    stage_ms, stage_n = prof["stage"]
-    avg_launch_s = stage_ms / 1e3 / max(stage_n, 1)
+    stage_ms = prof["taus"][0] + prof["faces"][0] + prof["update"][0]
+    nstages = max(prof["taus"][1], 1)
+    avg_stage_s = stage_ms / 1e3 / nstages
     alg_bytes = (2 + 3 + 3) / 3.0 * S * 8 * cells
     peak, peak_kind = measured_peak()
-    achieved = alg_bytes / avg_launch_s / 1e9
+    achieved = alg_bytes / avg_stage_s / 1e9
     key = f"{p.nspecies}:{args.precision}"
     traffic = STAGE_TRAFFIC_BYTES_PER_CELL.get(key)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic * cells if traffic else None, "peak_kind": peak_kind,
-            "kernel": "k_stage (fused fluxes + divergence + RK3 combination)",
-            "kernel_ms_per_launch": 1e3 * avg_launch_s,
+            "kernel": "RK stage (k_taus + 3x k_faces + k_update), per stage",
+            "kernel_ms_per_launch": 1e3 * avg_stage_s,
+            "algorithmic_bytes_per_launch": alg_bytes,
             "step_breakdown_ms": {k: v[0] / args.steps for k, v in prof.items()}}
 
     # e2e through the host-buffer C-ABI call (H2D + step + D2H, pinned memory)
@@ -371,7 +379,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--ns", type=int, default=2)
-    ap.add_argument("--dx", type=float, default=1e-6)
+    ap.add_argument("--dx", type=float, default=8e-6)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--tile", default="auto")
     ap.add_argument("--seed", type=int, default=1)

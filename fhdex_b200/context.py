@@ -69,8 +69,8 @@ class Context:
 
     def profile_read(self):
         """{kind: (ms, launches)} since the last read (CUDA events, launching stream)."""
-        ms = (C.c_double * 5)()
-        n = (C.c_int64 * 5)()
+        ms = (C.c_double * len(capi.PROF_KINDS))()
+        n = (C.c_int64 * len(capi.PROF_KINDS))()
         check(self.lib.fhd_profile_read(self._h, ms, n), "fhd_profile_read")
         return {k: (ms[q], n[q]) for q, k in enumerate(capi.PROF_KINDS)}
 

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "fhd_host.h"
+#include "philox.cuh"
 
 using namespace fhd;
 
@@ -26,6 +27,8 @@ struct fhd_ctx {
     size_t coef_bytes = 0;
     int coef_dtype = -1;
     fhd_fab ceta{}, czeta{}, ckappa{}, cchi{}, cD{};
+    fhd_fab ct{}, et{};          // stage stresses (coefficient precision)
+    fhd_fab sff[3]{};            // stage conservative face fluxes (f64)
     int tile = 0;
     // device mirrors for the host-buffer step
     double* hbuf = nullptr;
@@ -70,6 +73,7 @@ const int EFLUXN[6][3] = {{1, 1, 0}, {1, 0, 1}, {1, 1, 0}, {0, 1, 1}, {1, 0, 1},
 bool fab_ok(const fhd_ctx* c, const fhd_fab& f, const int nodal[3], int min_ng, int min_nc, int dtype,
             int exact_ng = -1) {
     if (!f.data || f.dtype != dtype || f.ncomp < min_nc) return false;
+    if (fab_points(f) * f.ncomp >= ((int64_t)1 << 31)) return false;  // kernels index with 32 bits
     const int g = -f.lo[0];
     if (g < min_ng || (exact_ng >= 0 && g != exact_ng)) return false;
     for (int d = 0; d < 3; ++d) {
@@ -136,7 +140,11 @@ int ensure_scratch(fhd_ctx* c) {
     const int64_t cellpts = fab_points(tmpl);
     int64_t fpts[3];
     for (int d = 0; d < 3; ++d) fpts[d] = fab_points(make_fab(nullptr, n, FACEN[d], NGC, 1, FHD_F64));
-    const size_t need = (size_t)(2 * cellpts * nvars + 2 * (fpts[0] + fpts[1] + fpts[2])) * sizeof(double);
+    const int ns = c->prm.nspecies;
+    const int allnod[3] = {1, 1, 1};
+    const int64_t npts = fab_points(make_fab(nullptr, n, allnod, 0, 1, FHD_F64));  // [0, n]^3
+    const size_t need = (size_t)(2 * cellpts * nvars + 2 * (fpts[0] + fpts[1] + fpts[2]) + 3 * npts * (2 + ns)) *
+                        sizeof(double);
     if (c->scratch && c->scratch_bytes >= need) return FHD_OK;
     if (c->scratch) cudaFree(c->scratch);
     c->scratch = nullptr;
@@ -149,6 +157,11 @@ int ensure_scratch(fhd_ctx* c) {
     c->cup2 = make_fab(p, n, CELLN, NGC, nvars, FHD_F64); p += cellpts * nvars;
     for (int d = 0; d < 3; ++d) { c->cupm[d] = make_fab(p, n, FACEN[d], NGC, 1, FHD_F64); p += fpts[d]; }
     for (int d = 0; d < 3; ++d) { c->cup2m[d] = make_fab(p, n, FACEN[d], NGC, 1, FHD_F64); p += fpts[d]; }
+    // face fluxes on [0, n]^3 (lo = 0, hi = n: every face box fits)
+    for (int d = 0; d < 3; ++d) {
+        c->sff[d] = make_fab(p, n, allnod, 0, 2 + ns, FHD_F64);
+        p += npts * (2 + ns);
+    }
     return FHD_OK;
 }
 
@@ -157,8 +170,11 @@ int ensure_coef(fhd_ctx* c, int dtype) {
     const int ns = c->prm.nspecies;
     const int ncomp = 3 + ns + ns * ns;
     const int64_t pts = fab_points(make_fab(nullptr, n, CELLN, NGC, 1, dtype));
+    const int allnod[3] = {1, 1, 1};
+    const int64_t ctpts = fab_points(make_fab(nullptr, n, CELLN, 1, 1, dtype));
+    const int64_t etpts = fab_points(make_fab(nullptr, n, allnod, 0, 1, dtype));
     const size_t es = dtype == FHD_F64 ? 8 : 4;
-    const size_t need = (size_t)pts * ncomp * es;
+    const size_t need = ((size_t)pts * ncomp + 6 * (size_t)(ctpts + etpts)) * es;
     if (c->coef && c->coef_bytes >= need && c->coef_dtype == dtype) return FHD_OK;
     if (c->coef) cudaFree(c->coef);
     c->coef = nullptr;
@@ -170,7 +186,9 @@ int ensure_coef(fhd_ctx* c, int dtype) {
     c->czeta = make_fab(p, n, CELLN, NGC, 1, dtype); p += pts * es;
     c->ckappa = make_fab(p, n, CELLN, NGC, 1, dtype); p += pts * es;
     c->cchi = make_fab(p, n, CELLN, NGC, ns, dtype); p += pts * ns * es;
-    c->cD = make_fab(p, n, CELLN, NGC, ns * ns, dtype);
+    c->cD = make_fab(p, n, CELLN, NGC, ns * ns, dtype); p += pts * ns * ns * es;
+    c->ct = make_fab(p, n, CELLN, 1, 6, dtype); p += ctpts * 6 * es;
+    c->et = make_fab(p, n, allnod, 0, 6, dtype);
     return FHD_OK;
 }
 
@@ -292,7 +310,8 @@ int fhd_destroy(fhd_ctx* c) {
 
 int fhd_set_stream(fhd_ctx* c, void* stream) {
     if (!c) return FHD_ERR_BAD_ARG;
-    c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own;
+    // NULL selects the legacy default stream (cudaStream_t 0), as in the CUDA API
+    c->stream = static_cast<cudaStream_t>(stream);
     return FHD_OK;
 }
 
@@ -477,10 +496,9 @@ int fhd_fill_step_noise(fhd_ctx* c, const fhd_noise* nz, int64_t step) {
     for (int s = 0; s < 2; ++s)
         for (int d = 0; d < 3; ++d) {
             const fhd_fab& f = nz->face[s][d];
-            int rc = noise_fill(P, f, f.ncomp - (ns + 1), ns + 1, 0.0, 1.0, (uint32_t)(d * (MAXS + 1)), s, c->stream);
-            if (!rc) rc = noise_fill(P, nz->edge[s][d], 0, 1, 0.0, 1.0, (uint32_t)(3 * (MAXS + 1) + d), s, c->stream);
-            if (!rc) rc = noise_fill(P, nz->cen[s][d], 0, 1, 0.0, std::sqrt(2.0), (uint32_t)(3 * (MAXS + 1) + 3 + d), s,
-                                     c->stream);
+            int rc = noise_fill(P, f, f.ncomp - (ns + 1), ns + 1, 0.0, 1.0, fid_face(d, 0), s, c->stream);
+            if (!rc) rc = noise_fill(P, nz->edge[s][d], 0, 1, 0.0, 1.0, fid_edge(d), s, c->stream);
+            if (!rc) rc = noise_fill(P, nz->cen[s][d], 0, 1, 0.0, std::sqrt(2.0), fid_cen(d), s, c->stream);
             if (rc) return rc;
             g[ng++] = GhostReq{nz->cen[s][d], 0, 1};
         }
@@ -521,10 +539,8 @@ int fhd_rk3_step_stag(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim
     cudaSetDevice(c->device);
     int rc = ensure_scratch(c);
     if (rc) return rc;
-    if (mixed || !aux_coef) {
-        rc = ensure_coef(c, mixed ? FHD_F32 : FHD_F64);
-        if (rc) return rc;
-    }
+    rc = ensure_coef(c, mixed ? FHD_F32 : FHD_F64);
+    if (rc) return rc;
     const double w[3] = {(2.0 * std::sqrt(2.0) + 1.0 * std::sqrt(3.0)) / 5.0,
                          (-4.0 * std::sqrt(2.0) + 3.0 * std::sqrt(3.0)) / 5.0,
                          (1.0 * std::sqrt(2.0) - 2.0 * std::sqrt(3.0)) / 10.0};
@@ -543,6 +559,9 @@ int fhd_rk3_step_stag(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim
     sc.status = c->d_status;
     sc.stream = c->stream;
     sc.tile = c->tile;
+    sc.ct = c->ct;
+    sc.et = c->et;
+    for (int d = 0; d < 3; ++d) sc.sff[d] = c->sff[d];
     const fhd_fab* ins[3] = {&cu, &c->cup, &c->cup2};
     const fhd_fab* insm[3] = {mom, c->cupm, c->cup2m};
     const fhd_fab* outs[3] = {&c->cup, &c->cup2, &cu};
@@ -561,26 +580,26 @@ int fhd_rk3_step_stag(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim
         if (s == 2 && aux_flux) {
             for (int d = 0; d < 3; ++d) { sc.ff[d] = faceflux[d]; sc.cf[d] = cenflux[d]; }
             for (int e = 0; e < 6; ++e) sc.ef[e] = edgeflux[e];
-            ProfScope ps(c, 4);
+            ProfScope ps(c, 6);
             rc = exact_aux_fluxes(sc);
             if (rc) return rc;
         }
-        {
-            ProfScope ps(c, 1);
-            rc = mixed ? mixed_stage(sc) : exact_stage(sc);
+        for (int part = 0; part < 3 && !rc; ++part) {
+            ProfScope ps(c, 1 + part);
+            rc = mixed ? mixed_stage_part(sc, part) : exact_stage_part(sc, part);
         }
         if (rc) return rc;
         GhostReq g[5] = {{*outs[s], 0, 1}, {*outs[s], 4, 1 + ns}, {outsm[s][0], 0, 1}, {outsm[s][1], 0, 1},
                          {outsm[s][2], 0, 1}};
         {
-            ProfScope ps(c, 2);
+            ProfScope ps(c, 4);
             rc = fill_ghosts(g, 5, c->prm.n_cells, c->stream);
         }
         if (rc) return rc;
     }
     // final conservedToPrimitiveStag + FillBoundary (timeStepStag.cpp:1216-1230)
     {
-        ProfScope ps(c, 3);
+        ProfScope ps(c, 5);
         rc = exact_convert(sc.P, prim, vel, cu, mom, c->d_status, c->stream);
     }
     if (rc) return rc;
@@ -596,7 +615,7 @@ int fhd_rk3_step_stag(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim
         g[ng++] = GhostReq{chi, 0, ns};
         g[ng++] = GhostReq{D, 0, ns * ns};
     }
-    ProfScope ps(c, 2);
+    ProfScope ps(c, 4);
     return fill_ghosts(g, ng, c->prm.n_cells, c->stream);
 }
 

@@ -17,15 +17,15 @@ namespace fhd {
 constexpr int MAXS = 8;
 
 // AMReX Array4 view: (i,j,k,n) at p[(i-lo0) + (j-lo1)*sy + (k-lo2)*sz + n*sn].
+// 32-bit offsets: the host rejects fabs with 2^31 or more elements.
 template <class T>
 struct Arr4 {
     T* p;
     int lo0, lo1, lo2;
-    int64_t sy, sz, sn;
+    int sy, sz, sn;
     FHD_HD T& operator()(int i, int j, int k, int n = 0) const {
         return p[(i - lo0) + (j - lo1) * sy + (k - lo2) * sz + n * sn];
     }
-    FHD_HD int64_t off(int i, int j, int k) const { return (i - lo0) + (j - lo1) * sy + (k - lo2) * sz; }
 };
 
 // Parameters as the kernels see them (by value in the kernel parameter bank).

@@ -6,31 +6,31 @@
 namespace fhd {
 
 int exact_cellprep_ns1(const StageCall&);
-int exact_stage_ns1(const StageCall&);
+int exact_stage_ns1(const StageCall&, int);
 int exact_aux_ns1(const StageCall&);
 int mixed_cellprep_ns1(const StageCall&);
-int mixed_stage_ns1(const StageCall&);
+int mixed_stage_ns1(const StageCall&, int);
 int exact_transport_ns1(const DevParams&, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, int*, cudaStream_t);
 int exact_convert_ns1(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const fhd_fab*, int*, cudaStream_t);
 int exact_cellprep_ns2(const StageCall&);
-int exact_stage_ns2(const StageCall&);
+int exact_stage_ns2(const StageCall&, int);
 int exact_aux_ns2(const StageCall&);
 int mixed_cellprep_ns2(const StageCall&);
-int mixed_stage_ns2(const StageCall&);
+int mixed_stage_ns2(const StageCall&, int);
 int exact_transport_ns2(const DevParams&, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, int*, cudaStream_t);
 int exact_convert_ns2(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const fhd_fab*, int*, cudaStream_t);
 int exact_cellprep_ns3(const StageCall&);
-int exact_stage_ns3(const StageCall&);
+int exact_stage_ns3(const StageCall&, int);
 int exact_aux_ns3(const StageCall&);
 int mixed_cellprep_ns3(const StageCall&);
-int mixed_stage_ns3(const StageCall&);
+int mixed_stage_ns3(const StageCall&, int);
 int exact_transport_ns3(const DevParams&, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, int*, cudaStream_t);
 int exact_convert_ns3(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const fhd_fab*, int*, cudaStream_t);
 int exact_cellprep_ns4(const StageCall&);
-int exact_stage_ns4(const StageCall&);
+int exact_stage_ns4(const StageCall&, int);
 int exact_aux_ns4(const StageCall&);
 int mixed_cellprep_ns4(const StageCall&);
-int mixed_stage_ns4(const StageCall&);
+int mixed_stage_ns4(const StageCall&, int);
 int exact_transport_ns4(const DevParams&, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, int*, cudaStream_t);
 int exact_convert_ns4(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const fhd_fab*, int*, cudaStream_t);
 
@@ -44,10 +44,10 @@ int exact_convert_ns4(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const 
     }
 
 int exact_cellprep(const StageCall& c) { FHD_DISPATCH(c.P.ns, exact_cellprep_ns, c) }
-int exact_stage(const StageCall& c) { FHD_DISPATCH(c.P.ns, exact_stage_ns, c) }
+int exact_stage_part(const StageCall& c, int part) { FHD_DISPATCH(c.P.ns, exact_stage_ns, c, part) }
 int exact_aux_fluxes(const StageCall& c) { FHD_DISPATCH(c.P.ns, exact_aux_ns, c) }
 int mixed_cellprep(const StageCall& c) { FHD_DISPATCH(c.P.ns, mixed_cellprep_ns, c) }
-int mixed_stage(const StageCall& c) { FHD_DISPATCH(c.P.ns, mixed_stage_ns, c) }
+int mixed_stage_part(const StageCall& c, int part) { FHD_DISPATCH(c.P.ns, mixed_stage_ns, c, part) }
 int exact_transport(const DevParams& P, fhd_fab prim, fhd_fab eta, fhd_fab zeta, fhd_fab kappa, fhd_fab chi,
                     fhd_fab D, int* status, cudaStream_t s) {
     FHD_DISPATCH(P.ns, exact_transport_ns, P, prim, eta, zeta, kappa, chi, D, status, s)
@@ -144,20 +144,10 @@ int init_uniform(const fhd_fab& cu, int ns, double rho0, double rhoE, const doub
     return cuda_rc(cudaGetLastError());
 }
 
-int num_tiles() {
-    int t = 0;
-#define FHD_CNT(a, b, d) ++t;
-    FHD_TILES(FHD_CNT)
-#undef FHD_CNT
-    return t;
-}
+int num_tiles() { return kNumStageBlocks; }
 
 const char* tile_name(int t) {
-    static const char* names[] = {
-#define FHD_NM(a, b, d) #a "x" #b "x" #d,
-        FHD_TILES(FHD_NM)
-#undef FHD_NM
-    };
+    static const char* names[] = {"block128", "block256", "block64"};
     return (t >= 0 && t < num_tiles()) ? names[t] : "?";
 }
 

@@ -40,35 +40,75 @@ struct NoiseArrays {
     Arr4<const double> ca[3], cb[3];   // centres (1 ghost)
 };
 
-// W = 1.0*A + w*B (MultiFab::LinComb, timeStepStag.cpp:258-326)
+// W = 1.0*A + w*B (MultiFab::LinComb, timeStepStag.cpp:258-326).  The *_all
+// accessors fetch every noise field needed at one point at once, so that the
+// in-kernel generator runs one Philox call per pair of fields.
 template <int MODE>
 struct Noise {
     NoiseArrays a;
     double w;
 
-    FHD_D double gauss(const DevParams& P, uint32_t fid, int i, int j, int k, double sd) const {
+    FHD_D double comb(double A, double B) const { return 1.0 * A + w * B; }
+    // fields fid0 and fid0+1 (fid0 even) at one point, each W = A + w B
+    FHD_D void gauss2(const DevParams& P, uint32_t fid0, int i, int j, int k, double sd, double& w0,
+                      double& w1) const {
+        float z[4];
+        normal_quad(P.key0, P.key1, canon(P, i, j, k), fid0 >> 1, P.step, z);
+        w0 = comb(0.0 + sd * (double)z[0], 0.0 + sd * (double)z[1]);
+        w1 = comb(0.0 + sd * (double)z[2], 0.0 + sd * (double)z[3]);
+    }
+    FHD_D double gauss1(const DevParams& P, uint32_t fid, int i, int j, int k, double sd) const {
         float za, zb;
         normal_pair(P.key0, P.key1, canon(P, i, j, k), fid, P.step, za, zb);
-        const double A = 0.0 + sd * (double)za;
-        const double B = 0.0 + sd * (double)zb;
-        return 1.0 * A + w * B;
+        return comb(0.0 + sd * (double)za, 0.0 + sd * (double)zb);
+    }
+    template <int NC>
+    FHD_D void face_all(const DevParams& P, int d, int i, int j, int k, double (&out)[NC]) const {
+        if (MODE == NZ_PHILOX) {
+#pragma unroll
+            for (int c = 0; c < NC; c += 2) {
+                if (c + 1 < NC) gauss2(P, fid_face(d, c), i, j, k, 1.0, out[c], out[c + 1]);
+                else out[c] = gauss1(P, fid_face(d, c), i, j, k, 1.0);
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) out[c] = face(P, d, c, i, j, k);
+        }
+    }
+    FHD_D void cen_all(const DevParams& P, int i, int j, int k, double (&out)[3]) const {
+        if (MODE == NZ_PHILOX) {
+            gauss2(P, fid_cen(0), i, j, k, P.sqrt2, out[0], out[1]);
+            out[2] = gauss1(P, fid_cen(2), i, j, k, P.sqrt2);
+        } else {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) out[d] = cen(P, d, i, j, k);
+        }
+    }
+    FHD_D void edge_all(const DevParams& P, int i, int j, int k, double (&out)[3]) const {
+        if (MODE == NZ_PHILOX) {
+            gauss2(P, fid_edge(0), i, j, k, 1.0, out[0], out[1]);
+            out[2] = gauss1(P, fid_edge(2), i, j, k, 1.0);
+        } else {
+#pragma unroll
+            for (int e = 0; e < 3; ++e) out[e] = edge(P, e, i, j, k);
+        }
     }
     FHD_D double face(const DevParams& P, int d, int c, int i, int j, int k) const {
         if (MODE == NZ_W) return a.fa[d](i, j, k, a.foa[d] + c);
-        if (MODE == NZ_AB) return 1.0 * a.fa[d](i, j, k, a.foa[d] + c) + w * a.fb[d](i, j, k, a.fob[d] + c);
-        if (MODE == NZ_PHILOX) return gauss(P, fid_face(d, c), i, j, k, 1.0);
+        if (MODE == NZ_AB) return comb(a.fa[d](i, j, k, a.foa[d] + c), a.fb[d](i, j, k, a.fob[d] + c));
+        if (MODE == NZ_PHILOX) return gauss1(P, fid_face(d, c), i, j, k, 1.0);
         return 0.0;
     }
     FHD_D double edge(const DevParams& P, int e, int i, int j, int k) const {
         if (MODE == NZ_W) return a.ea[e](i, j, k);
-        if (MODE == NZ_AB) return 1.0 * a.ea[e](i, j, k) + w * a.eb[e](i, j, k);
-        if (MODE == NZ_PHILOX) return gauss(P, fid_edge(e), i, j, k, 1.0);
+        if (MODE == NZ_AB) return comb(a.ea[e](i, j, k), a.eb[e](i, j, k));
+        if (MODE == NZ_PHILOX) return gauss1(P, fid_edge(e), i, j, k, 1.0);
         return 0.0;
     }
     FHD_D double cen(const DevParams& P, int d, int i, int j, int k) const {
         if (MODE == NZ_W) return a.ca[d](i, j, k);
-        if (MODE == NZ_AB) return 1.0 * a.ca[d](i, j, k) + w * a.cb[d](i, j, k);
-        if (MODE == NZ_PHILOX) return gauss(P, fid_cen(d), i, j, k, P.sqrt2);
+        if (MODE == NZ_AB) return comb(a.ca[d](i, j, k), a.cb[d](i, j, k));
+        if (MODE == NZ_PHILOX) return gauss1(P, fid_cen(d), i, j, k, P.sqrt2);
         return 0.0;
     }
 };
@@ -99,7 +139,9 @@ FHD_D CellTaus<R> cell_taus(const DevParams& P, const Fields<NS, R>& F, const No
         if (visc3)
             fac2 = dsqrt(R(P.k_B) * zetaT * R(P.volinv) * R(P.dtinv) / R(3.0)) -
                    dsqrt(R(2.0) * R(P.k_B) * etaT * R(P.volinv) * R(P.dtinv)) / R(3.0);
-        const R w0 = R(nz.cen(P, 0, i, j, k)), w1 = R(nz.cen(P, 1, i, j, k)), w2 = R(nz.cen(P, 2, i, j, k));
+        double wc[3];
+        nz.cen_all(P, i, j, k, wc);
+        const R w0 = R(wc[0]), w1 = R(wc[1]), w2 = R(wc[2]);
         const R traceZ = w0 + w1 + w2;
         t.s[0] = (fac1 * w0) + (fac2 * traceZ);
         t.s[1] = (fac1 * w1) + (fac2 * traceZ);
@@ -122,7 +164,7 @@ FHD_D CellTaus<R> cell_taus(const DevParams& P, const Fields<NS, R>& F, const No
 // deterministic :927-1023.  The four cells around the edge are c00, c01, c10, c11
 // in the reference's summation order.
 template <int NS, class R, int NZ, int E>
-FHD_D Taus<R> edge_taus(const DevParams& P, const Fields<NS, R>& F, const Noise<NZ>& nz, int i, int j, int k) {
+FHD_D Taus<R> edge_taus_w(const DevParams& P, const Fields<NS, R>& F, double wnoise, int i, int j, int k) {
     // cells: (a) low-low, (b) low-high, (c) high-low, (d) high-high in the edge's two directions
     int ai, aj, ak, bi, bj, bk, ci, cj, ck;
     if (E == 0) { ai = i - 1; aj = j - 1; ak = k; bi = i - 1; bj = j; bk = k; ci = i; cj = j - 1; ck = k; }
@@ -133,7 +175,7 @@ FHD_D Taus<R> edge_taus(const DevParams& P, const Fields<NS, R>& F, const Noise<
         const R etaT = R(0.25) * (F.eta(ai, aj, ak) * R(F.T(ai, aj, ak)) + F.eta(bi, bj, bk) * R(F.T(bi, bj, bk)) +
                                   F.eta(ci, cj, ck) * R(F.T(ci, cj, ck)) + F.eta(i, j, k) * R(F.T(i, j, k)));
         const R fac = dsqrt(R(2.0) * R(P.k_B) * etaT * R(P.volinv) * R(P.dtinv));
-        t.s = fac * R(nz.edge(P, E, i, j, k));
+        t.s = fac * R(wnoise);
     } else {
         t.s = R(0.);
     }
@@ -151,6 +193,11 @@ FHD_D Taus<R> edge_taus(const DevParams& P, const Fields<NS, R>& F, const Noise<
     const R ei = R(0.25) * (F.eta(ai, aj, ak) + F.eta(bi, bj, bk) + F.eta(ci, cj, ck) + F.eta(i, j, k));
     t.d = ei * (g1 + g2);
     return t;
+}
+
+template <int NS, class R, int NZ, int E>
+FHD_D Taus<R> edge_taus(const DevParams& P, const Fields<NS, R>& F, const Noise<NZ>& nz, int i, int j, int k) {
+    return edge_taus_w<NS, R, NZ, E>(P, F, NZ != NZ_OFF ? nz.edge(P, E, i, j, k) : 0.0, i, j, k);
 }
 
 // ---- face fluxes ---------------------------------------------------------------------
@@ -209,8 +256,10 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
         const R Th = R(F.T(i, j, k)), Tl = R(F.T(im, jm, km));
         const R kp = (F.kappa(i, j, k) * Th * Th + F.kappa(im, jm, km) * Tl * Tl);
         const R meanT = R(0.5) * (Th + Tl);
+        double wf[NS + 1];
+        nz.template face_all<NS + 1>(P, D, i, j, k, wf);
         const R fw0 = dsqrt(R(P.k_B) * kp * R(P.volinv) * R(P.dtinv));
-        heat = fw0 * R(nz.face(P, D, 0, i, j, k));
+        heat = fw0 * R(wf[0]);
         vdiag = R(0.5) * un * (tl.s[D] + th.s[D]);
         R vsh = R(0.0);
         vsh += R(0.25) * ((va1h + va1l) * ea1.s + (va0h + va0l) * ea0.s);
@@ -248,7 +297,7 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
         const R fwc = dsqrt(R(P.k_B) * MWmix * R(P.volinv) / (R(P.Runiv) * R(P.dt)));
         R zs[NS];
 #pragma unroll
-        for (int ll = 0; ll < NS; ++ll) zs[ll] = R(nz.face(P, D, 1 + ll, i, j, k));
+        for (int ll = 0; ll < NS; ++ll) zs[ll] = R(wf[1 + ll]);
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
 #pragma unroll

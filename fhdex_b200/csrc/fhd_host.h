@@ -32,6 +32,7 @@ struct StageCall {
     fhd_fab src;            // data == NULL: no source
     NoiseFabs nz;
     fhd_fab ff[3], ef[6], cf[3];        // flux outputs of the operator path
+    fhd_fab ct, et, sff[3];             // stage scratch: cell/edge stresses, face fluxes
     int* status;
     cudaStream_t stream;
     int tile;               // tile-shape index of k_stage (autotuned)
@@ -39,7 +40,7 @@ struct StageCall {
 
 // exact (FP64) translation unit
 int exact_cellprep(const StageCall& c);
-int exact_stage(const StageCall& c);
+int exact_stage_part(const StageCall& c, int part);  // 0 stresses, 1 face fluxes, 2 update
 int exact_aux_fluxes(const StageCall& c);
 int exact_transport(const DevParams& P, fhd_fab prim, fhd_fab eta, fhd_fab zeta, fhd_fab kappa, fhd_fab chi,
                     fhd_fab D, int* status, cudaStream_t s);
@@ -47,7 +48,7 @@ int exact_convert(const DevParams& P, fhd_fab prim, const fhd_fab vel[3], fhd_fa
                   int* status, cudaStream_t s);
 // mixed translation unit (coefficient fabs are f32)
 int mixed_cellprep(const StageCall& c);
-int mixed_stage(const StageCall& c);
+int mixed_stage_part(const StageCall& c, int part);
 
 // utilities (exact TU)
 struct GhostReq {

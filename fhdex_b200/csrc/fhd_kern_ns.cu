@@ -15,10 +15,10 @@ namespace fhd {
 
 #if defined(FHD_MIXED) && FHD_MIXED
 int FHD_CAT(mixed_cellprep_ns, FHD_NS)(const StageCall& c) { return launch_cellprep<FHD_NS, float>(c); }
-int FHD_CAT(mixed_stage_ns, FHD_NS)(const StageCall& c) { return launch_stage<FHD_NS, float>(c); }
+int FHD_CAT(mixed_stage_ns, FHD_NS)(const StageCall& c, int part) { return launch_stage_part<FHD_NS, float>(c, part); }
 #else
 int FHD_CAT(exact_cellprep_ns, FHD_NS)(const StageCall& c) { return launch_cellprep<FHD_NS, double>(c); }
-int FHD_CAT(exact_stage_ns, FHD_NS)(const StageCall& c) { return launch_stage<FHD_NS, double>(c); }
+int FHD_CAT(exact_stage_ns, FHD_NS)(const StageCall& c, int part) { return launch_stage_part<FHD_NS, double>(c, part); }
 
 template <int NS, int NZ>
 int launch_aux_t(const StageCall& c) {

@@ -2,9 +2,11 @@
 //
 //   k_cellprep  per stage: conservedToPrimitiveStag + calculateTransportCoeffs for
 //               every cell once (cells grown by 1, face velocities grown by 1)
-//   k_stage     per stage: stochastic + diffusive + hyperbolic fluxes, their
-//               divergence and the SSP-RK3 combination, one 3D tile per CTA with
-//               the stresses and conservative face fluxes exchanged in shared memory
+//   k_taus      per stage: stochastic + deterministic stresses on cells and edges
+//   k_faces<D>  per stage and direction: stochastic + diffusive + hyperbolic
+//               conservative face fluxes (one small kernel per direction)
+//   k_update    per stage: flux divergence, momentum update and the SSP-RK3
+//               combination
 //   k_convert   end of step / drop-in conversion (prim, vel, cons 1..3)
 //   k_ghosts    periodic FillBoundary of several fabs in one launch
 //   k_transport, k_aux_*  drop-in operators (transport coefficients, flux MultiFabs)
@@ -38,11 +40,11 @@ template <int NS, class R>
 __global__ void __launch_bounds__(128) k_cellprep(PrepArgs<NS, R> a) {
     const DevParams& P = a.P;
     const int nx = P.n[0] + 3, ny = P.n[1] + 3, nz = P.n[2] + 3;
-    const int64_t tot = (int64_t)nx * ny * nz;
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < tot; q += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(q % nx) - 1;
-        const int j = (int)((q / nx) % ny) - 1;
-        const int k = (int)(q / ((int64_t)nx * ny)) - 1;
+    const int tot = nx * ny * nz;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) {
+        const int i = q % nx - 1;
+        const int j = (q / nx) % ny - 1;
+        const int k = q / (nx * ny) - 1;
         const double rho = a.cons(i, j, k, 0);
         // low face velocities (conservedPrimitiveConversionsStag.cpp:61-67)
         a.vel[0](i, j, k) = 2 * a.mom[0](i, j, k) / (rho + a.cons(i - 1, j, k, 0));
@@ -80,13 +82,20 @@ __global__ void __launch_bounds__(128) k_cellprep(PrepArgs<NS, R> a) {
 }
 
 // ===================================================================================
-// fused stage kernel
+// stage pipeline: k_taus -> k_faces<D> (x3) -> k_update
 // ===================================================================================
+// Scratch of one stage (owned by the context):
+//   ct: cell stresses on the cells grown by 1, comps 0-2 stochastic xx,yy,zz,
+//       3-5 deterministic xx,yy,zz
+//   et: edge stresses on the points [0, n]^3, comps (s,d) of xy, xz, yz at 0-1, 2-3, 4-5
+//   ff[d]: conservative face fluxes (rho, rhoE, rhoY) of direction d on [0, n]^3
 template <int NS, class R, int NZ>
 struct StageArgs {
     DevParams P;
     Fields<NS, R> F;             // stage-input state U^s + derived fields
     Noise<NZ> noise;
+    Arr4<R> ct, et;
+    Arr4<double> ff[3];
     Arr4<const double> cons0;    // U^0 (for the RK combination)
     Arr4<const double> mom0[3];
     Arr4<double> cons_o;         // U^{s+1}
@@ -95,145 +104,100 @@ struct StageArgs {
     int stage;                   // 1, 2, 3
 };
 
-template <int TX, int TY, int TZ>
-struct TileGeom {
-    static constexpr int NT = TX * TY * TZ;
-    static constexpr int CX = TX + 2, CY = TY + 2, CZ = TZ + 2, NC = CX * CY * CZ;
-    static constexpr int NEXY = (TX + 1) * (TY + 1) * TZ;
-    static constexpr int NEXZ = (TX + 1) * TY * (TZ + 1);
-    static constexpr int NEYZ = TX * (TY + 1) * (TZ + 1);
-    static constexpr int NFX = (TX + 1) * TY * TZ;
-    static constexpr int NFY = TX * (TY + 1) * TZ;
-    static constexpr int NFZ = TX * TY * (TZ + 1);
-    FHD_D static int cpos(int ci, int cj, int ck) { return (ci + 1) + CX * ((cj + 1) + CY * (ck + 1)); }
-    FHD_D static int exy(int i, int j, int k) { return i + (TX + 1) * (j + (TY + 1) * k); }
-    FHD_D static int exz(int i, int j, int k) { return i + (TX + 1) * (j + TY * k); }
-    FHD_D static int eyz(int i, int j, int k) { return i + TX * (j + (TY + 1) * k); }
-    FHD_D static int fx(int i, int j, int k) { return i + (TX + 1) * (j + TY * k); }
-    FHD_D static int fy(int i, int j, int k) { return i + TX * (j + (TY + 1) * k); }
-    FHD_D static int fz(int i, int j, int k) { return i + TX * (j + TY * k); }
-};
+// stresses on cells (grown by 1) and edges; one thread per point of [-1, n]^3
+template <int NS, class R, int NZ>
+__global__ void __launch_bounds__(256) k_taus(StageArgs<NS, R, NZ> a) {
+    const DevParams& P = a.P;
+    const int nx = P.n[0] + 2, ny = P.n[1] + 2, nz = P.n[2] + 2;
+    const int tot = nx * ny * nz;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) {
+        const int i = q % nx - 1, j = (q / nx) % ny - 1, k = q / (nx * ny) - 1;
+        const CellTaus<R> t = cell_taus<NS, R, NZ>(P, a.F, a.noise, i, j, k);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            a.ct(i, j, k, d) = t.s[d];
+            a.ct(i, j, k, 3 + d) = t.d[d];
+        }
+        if (i < 0 || j < 0 || k < 0) continue;
+        double we[3] = {0.0, 0.0, 0.0};
+        if (NZ != NZ_OFF) a.noise.edge_all(P, i, j, k, we);
+        if (k < P.n[2]) {
+            const Taus<R> e = edge_taus_w<NS, R, NZ, 0>(P, a.F, we[0], i, j, k);
+            a.et(i, j, k, 0) = e.s;
+            a.et(i, j, k, 1) = e.d;
+        }
+        if (j < P.n[1]) {
+            const Taus<R> e = edge_taus_w<NS, R, NZ, 1>(P, a.F, we[1], i, j, k);
+            a.et(i, j, k, 2) = e.s;
+            a.et(i, j, k, 3) = e.d;
+        }
+        if (i < P.n[0]) {
+            const Taus<R> e = edge_taus_w<NS, R, NZ, 2>(P, a.F, we[2], i, j, k);
+            a.et(i, j, k, 4) = e.s;
+            a.et(i, j, k, 5) = e.d;
+        }
+    }
+}
 
-template <int NS, class R, int TX, int TY, int TZ>
-struct StageSmem {
-    using G = TileGeom<TX, TY, TZ>;
-    R ct[6][G::NC];              // cell diag stresses: s xx,yy,zz, d xx,yy,zz
-    R exy[2][G::NEXY];           // edge stresses (s, d)
-    R exz[2][G::NEXZ];
-    R eyz[2][G::NEYZ];
-    double fx[2 + NS][G::NFX];   // conservative face fluxes (rho, rhoE, rhoY)
-    double fy[2 + NS][G::NFY];
-    double fz[2 + NS][G::NFZ];
-};
-
-// reads the tile's stresses from shared memory (global indices in, tile-relative inside)
-template <int NS, class R, int TX, int TY, int TZ>
-struct SmemTaus {
-    using G = TileGeom<TX, TY, TZ>;
-    const StageSmem<NS, R, TX, TY, TZ>* s;
-    int x0, y0, z0;
+template <class R>
+struct GlobalTaus {
+    Arr4<R> ct, et;
     FHD_D CellTaus<R> cell(int i, int j, int k) const {
-        const int p = G::cpos(i - x0, j - y0, k - z0);
         CellTaus<R> t;
 #pragma unroll
-        for (int d = 0; d < 3; ++d) { t.s[d] = s->ct[d][p]; t.d[d] = s->ct[3 + d][p]; }
+        for (int d = 0; d < 3; ++d) {
+            t.s[d] = ct(i, j, k, d);
+            t.d[d] = ct(i, j, k, 3 + d);
+        }
         return t;
     }
     template <int E>
     FHD_D Taus<R> edge(int i, int j, int k) const {
         Taus<R> t;
-        if (E == 0) { const int p = G::exy(i - x0, j - y0, k - z0); t.s = s->exy[0][p]; t.d = s->exy[1][p]; }
-        if (E == 1) { const int p = G::exz(i - x0, j - y0, k - z0); t.s = s->exz[0][p]; t.d = s->exz[1][p]; }
-        if (E == 2) { const int p = G::eyz(i - x0, j - y0, k - z0); t.s = s->eyz[0][p]; t.d = s->eyz[1][p]; }
+        t.s = et(i, j, k, 2 * E);
+        t.d = et(i, j, k, 2 * E + 1);
         return t;
     }
 };
 
-template <int NS, class R, int NZ, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(TX * TY * TZ) k_stage(StageArgs<NS, R, NZ> a) {
-    using G = TileGeom<TX, TY, TZ>;
-    using SM = StageSmem<NS, R, TX, TY, TZ>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    SM& S = *reinterpret_cast<SM*>(smem_raw);
+// conservative fluxes of the faces of direction D; one thread per valid face
+template <int NS, class R, int NZ, int D>
+__global__ void __launch_bounds__(256) k_faces(StageArgs<NS, R, NZ> a) {
+    const DevParams& P = a.P;
+    const int nx = P.n[0] + (D == 0), ny = P.n[1] + (D == 1), nz = P.n[2] + (D == 2);
+    const int tot = nx * ny * nz;
+    const GlobalTaus<R> tg{a.ct, a.et};
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) {
+        const int i = q % nx, j = (q / nx) % ny, k = q / (nx * ny);
+        const FaceFlux<NS> f = face_flux<NS, R, NZ, D>(P, a.F, a.noise, tg, i, j, k);
+#pragma unroll
+        for (int c = 0; c < 2 + NS; ++c) a.ff[D](i, j, k, c) = f.cons[c];
+    }
+}
+
+// RK3 stage combination (timeStepStag.cpp:439-528, 771-861, 1106-1202): one thread
+// per point of [0, n]^3 updates the cell there (if valid) and the faces there
+template <int NS, class R, int NZ>
+__global__ void __launch_bounds__(256) k_update(StageArgs<NS, R, NZ> a) {
     const DevParams& P = a.P;
     const Fields<NS, R>& F = a.F;
-    const int tid = threadIdx.x;
-    const int ntx = (P.n[0] + TX - 1) / TX, nty = (P.n[1] + TY - 1) / TY;
-    const int bt = blockIdx.x;
-    const int x0 = (bt % ntx) * TX, y0 = ((bt / ntx) % nty) * TY, z0 = (bt / (ntx * nty)) * TZ;
-    const int nx = min(TX, P.n[0] - x0), ny = min(TY, P.n[1] - y0), nz = min(TZ, P.n[2] - z0);
-
-    // ---- phase 1: diagonal stresses on the tile and its cross-shaped halo ----
-    for (int q = tid; q < G::NC; q += G::NT) {
-        const int ci = q % G::CX - 1, cj = (q / G::CX) % G::CY - 1, ck = q / (G::CX * G::CY) - 1;
-        const int out = (ci < 0 || ci >= nx) + (cj < 0 || cj >= ny) + (ck < 0 || ck >= nz);
-        if (ci > nx || cj > ny || ck > nz || out > 1) continue;
-        const CellTaus<R> t = cell_taus<NS, R, NZ>(P, F, a.noise, x0 + ci, y0 + cj, z0 + ck);
-#pragma unroll
-        for (int d = 0; d < 3; ++d) { S.ct[d][q] = t.s[d]; S.ct[3 + d][q] = t.d[d]; }
-    }
-    // ---- phase 2: edge stresses ----
-    for (int q = tid; q < G::NEXY + G::NEXZ + G::NEYZ; q += G::NT) {
-        if (q < G::NEXY) {
-            const int ei = q % (TX + 1), ej = (q / (TX + 1)) % (TY + 1), ek = q / ((TX + 1) * (TY + 1));
-            if (ei > nx || ej > ny || ek >= nz) continue;
-            const Taus<R> t = edge_taus<NS, R, NZ, 0>(P, F, a.noise, x0 + ei, y0 + ej, z0 + ek);
-            S.exy[0][q] = t.s; S.exy[1][q] = t.d;
-        } else if (q < G::NEXY + G::NEXZ) {
-            const int r = q - G::NEXY;
-            const int ei = r % (TX + 1), ej = (r / (TX + 1)) % TY, ek = r / ((TX + 1) * TY);
-            if (ei > nx || ej >= ny || ek > nz) continue;
-            const Taus<R> t = edge_taus<NS, R, NZ, 1>(P, F, a.noise, x0 + ei, y0 + ej, z0 + ek);
-            S.exz[0][r] = t.s; S.exz[1][r] = t.d;
-        } else {
-            const int r = q - G::NEXY - G::NEXZ;
-            const int ei = r % TX, ej = (r / TX) % (TY + 1), ek = r / (TX * (TY + 1));
-            if (ei >= nx || ej > ny || ek > nz) continue;
-            const Taus<R> t = edge_taus<NS, R, NZ, 2>(P, F, a.noise, x0 + ei, y0 + ej, z0 + ek);
-            S.eyz[0][r] = t.s; S.eyz[1][r] = t.d;
-        }
-    }
-    __syncthreads();
-    // ---- phase 3: conservative face fluxes ----
-    const SmemTaus<NS, R, TX, TY, TZ> tg{&S, x0, y0, z0};
-    for (int q = tid; q < G::NFX + G::NFY + G::NFZ; q += G::NT) {
-        if (q < G::NFX) {
-            const int fi = q % (TX + 1), fj = (q / (TX + 1)) % TY, fk = q / ((TX + 1) * TY);
-            if (fi > nx || fj >= ny || fk >= nz) continue;
-            const FaceFlux<NS> f = face_flux<NS, R, NZ, 0>(P, F, a.noise, tg, x0 + fi, y0 + fj, z0 + fk);
-#pragma unroll
-            for (int c = 0; c < 2 + NS; ++c) S.fx[c][q] = f.cons[c];
-        } else if (q < G::NFX + G::NFY) {
-            const int r = q - G::NFX;
-            const int fi = r % TX, fj = (r / TX) % (TY + 1), fk = r / (TX * (TY + 1));
-            if (fi >= nx || fj > ny || fk >= nz) continue;
-            const FaceFlux<NS> f = face_flux<NS, R, NZ, 1>(P, F, a.noise, tg, x0 + fi, y0 + fj, z0 + fk);
-#pragma unroll
-            for (int c = 0; c < 2 + NS; ++c) S.fy[c][r] = f.cons[c];
-        } else {
-            const int r = q - G::NFX - G::NFY;
-            const int fi = r % TX, fj = (r / TX) % TY, fk = r / (TX * TY);
-            if (fi >= nx || fj >= ny || fk > nz) continue;
-            const FaceFlux<NS> f = face_flux<NS, R, NZ, 2>(P, F, a.noise, tg, x0 + fi, y0 + fj, z0 + fk);
-#pragma unroll
-            for (int c = 0; c < 2 + NS; ++c) S.fz[c][r] = f.cons[c];
-        }
-    }
-    __syncthreads();
-    // ---- phase 4: RK3 stage combination (timeStepStag.cpp:439-528, 771-861, 1106-1202) ----
+    const int nx = P.n[0] + 1, ny = P.n[1] + 1, nz = P.n[2] + 1;
+    const int tot = nx * ny * nz;
+    const GlobalTaus<R> tg{a.ct, a.et};
     const double dt = P.dt;
     const int st = a.stage;
-    {
-        const int ci = tid % TX, cj = (tid / TX) % TY, ck = tid / (TX * TY);
-        if (ci < nx && cj < ny && ck < nz) {
-            const int i = x0 + ci, j = y0 + cj, k = z0 + ck;
+    const int hadv = P.advection_type >= 0;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) {
+        const int i = q % nx, j = (q / nx) % ny, k = q / (nx * ny);
+        const bool cell = i < P.n[0] && j < P.n[1] && k < P.n[2];
+        if (cell) {
             double on[2 + NS];
 #pragma unroll
             for (int c = 0; c < 2 + NS; ++c) {
                 const int n = (c == 0) ? 0 : 3 + c;  // conserved component index
-                const double div = (S.fx[c][G::fx(ci + 1, cj, ck)] - S.fx[c][G::fx(ci, cj, ck)]) / P.dx[0] +
-                                   (S.fy[c][G::fy(ci, cj + 1, ck)] - S.fy[c][G::fy(ci, cj, ck)]) / P.dx[1] +
-                                   (S.fz[c][G::fz(ci, cj, ck + 1)] - S.fz[c][G::fz(ci, cj, ck)]) / P.dx[2];
+                const double div = (a.ff[0](i + 1, j, k, c) - a.ff[0](i, j, k, c)) / P.dx[0] +
+                                   (a.ff[1](i, j + 1, k, c) - a.ff[1](i, j, k, c)) / P.dx[1] +
+                                   (a.ff[2](i, j, k + 1, c) - a.ff[2](i, j, k, c)) / P.dx[2];
                 const double src = a.src.p ? a.src(i, j, k, n) : 0.0;
                 const double u0 = a.cons0(i, j, k, n);
                 double v;
@@ -250,72 +214,66 @@ __global__ void __launch_bounds__(TX * TY * TZ) k_stage(StageArgs<NS, R, NZ> a) 
 #pragma unroll
             for (int c = 0; c < 2 + NS; ++c) a.cons_o(i, j, k, (c == 0) ? 0 : 3 + c) = on[c];
         }
-    }
-    // face momenta: faces owned by the tile (low faces of its cells, plus the domain's
-    // high face n_cells for the last tile in that direction)
-    const int fxn = nx + ((x0 + nx) == P.n[0]), fyn = ny + ((y0 + ny) == P.n[1]), fzn = nz + ((z0 + nz) == P.n[2]);
-    const int hadv = P.advection_type >= 0;
-    for (int q = tid; q < G::NFX + G::NFY + G::NFZ; q += G::NT) {
-        int d, fi, fj, fk;
-        if (q < G::NFX) { d = 0; fi = q % (TX + 1); fj = (q / (TX + 1)) % TY; fk = q / ((TX + 1) * TY);
-            if (fi >= fxn || fj >= ny || fk >= nz) continue; }
-        else if (q < G::NFX + G::NFY) { const int r = q - G::NFX; d = 1; fi = r % TX; fj = (r / TX) % (TY + 1); fk = r / (TX * (TY + 1));
-            if (fi >= nx || fj >= fyn || fk >= nz) continue; }
-        else { const int r = q - G::NFX - G::NFY; d = 2; fi = r % TX; fj = (r / TX) % TY; fk = r / (TX * TY);
-            if (fi >= nx || fj >= ny || fk >= fzn) continue; }
-        const int i = x0 + fi, j = y0 + fj, k = z0 + fk;
-        double t1, t2, t3, ea, eb;
-        if (d == 0) {
-            t1 = cen_total<NS, R>(P, F, tg.cell(i, j, k), 0, i, j, k) - cen_total<NS, R>(P, F, tg.cell(i - 1, j, k), 0, i - 1, j, k);
-            edge_adv<NS, R, 0>(P, F, i, j + 1, k, ea, eb);
-            const double ehi = edge_total<R>(tg.template edge<0>(i, j + 1, k), ea, hadv);
-            edge_adv<NS, R, 0>(P, F, i, j, k, ea, eb);
-            const double elo = edge_total<R>(tg.template edge<0>(i, j, k), ea, hadv);
-            t2 = ehi - elo;
-            edge_adv<NS, R, 1>(P, F, i, j, k + 1, ea, eb);
-            const double zhi = edge_total<R>(tg.template edge<1>(i, j, k + 1), ea, hadv);
-            edge_adv<NS, R, 1>(P, F, i, j, k, ea, eb);
-            const double zlo = edge_total<R>(tg.template edge<1>(i, j, k), ea, hadv);
-            t3 = zhi - zlo;
-        } else if (d == 1) {
-            edge_adv<NS, R, 0>(P, F, i + 1, j, k, ea, eb);
-            const double xhi = edge_total<R>(tg.template edge<0>(i + 1, j, k), eb, hadv);
-            edge_adv<NS, R, 0>(P, F, i, j, k, ea, eb);
-            const double xlo = edge_total<R>(tg.template edge<0>(i, j, k), eb, hadv);
-            t1 = xhi - xlo;
-            t2 = cen_total<NS, R>(P, F, tg.cell(i, j, k), 1, i, j, k) - cen_total<NS, R>(P, F, tg.cell(i, j - 1, k), 1, i, j - 1, k);
-            edge_adv<NS, R, 2>(P, F, i, j, k + 1, ea, eb);
-            const double zhi = edge_total<R>(tg.template edge<2>(i, j, k + 1), ea, hadv);
-            edge_adv<NS, R, 2>(P, F, i, j, k, ea, eb);
-            const double zlo = edge_total<R>(tg.template edge<2>(i, j, k), ea, hadv);
-            t3 = zhi - zlo;
-        } else {
-            edge_adv<NS, R, 1>(P, F, i + 1, j, k, ea, eb);
-            const double xhi = edge_total<R>(tg.template edge<1>(i + 1, j, k), eb, hadv);
-            edge_adv<NS, R, 1>(P, F, i, j, k, ea, eb);
-            const double xlo = edge_total<R>(tg.template edge<1>(i, j, k), eb, hadv);
-            t1 = xhi - xlo;
-            edge_adv<NS, R, 2>(P, F, i, j + 1, k, ea, eb);
-            const double yhi = edge_total<R>(tg.template edge<2>(i, j + 1, k), eb, hadv);
-            edge_adv<NS, R, 2>(P, F, i, j, k, ea, eb);
-            const double ylo = edge_total<R>(tg.template edge<2>(i, j, k), eb, hadv);
-            t2 = yhi - ylo;
-            t3 = cen_total<NS, R>(P, F, tg.cell(i, j, k), 2, i, j, k) - cen_total<NS, R>(P, F, tg.cell(i, j, k - 1), 2, i, j, k - 1);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const int e0 = d == 0, e1 = d == 1, e2 = d == 2;
+            if (i >= P.n[0] + e0 || j >= P.n[1] + e1 || k >= P.n[2] + e2) continue;
+            double t1, t2, t3, ea, eb;
+            if (d == 0) {
+                t1 = cen_total<NS, R>(P, F, tg.cell(i, j, k), 0, i, j, k) -
+                     cen_total<NS, R>(P, F, tg.cell(i - 1, j, k), 0, i - 1, j, k);
+                edge_adv<NS, R, 0>(P, F, i, j + 1, k, ea, eb);
+                const double ehi = edge_total<R>(tg.template edge<0>(i, j + 1, k), ea, hadv);
+                edge_adv<NS, R, 0>(P, F, i, j, k, ea, eb);
+                const double elo = edge_total<R>(tg.template edge<0>(i, j, k), ea, hadv);
+                t2 = ehi - elo;
+                edge_adv<NS, R, 1>(P, F, i, j, k + 1, ea, eb);
+                const double zhi = edge_total<R>(tg.template edge<1>(i, j, k + 1), ea, hadv);
+                edge_adv<NS, R, 1>(P, F, i, j, k, ea, eb);
+                const double zlo = edge_total<R>(tg.template edge<1>(i, j, k), ea, hadv);
+                t3 = zhi - zlo;
+            } else if (d == 1) {
+                edge_adv<NS, R, 0>(P, F, i + 1, j, k, ea, eb);
+                const double xhi = edge_total<R>(tg.template edge<0>(i + 1, j, k), eb, hadv);
+                edge_adv<NS, R, 0>(P, F, i, j, k, ea, eb);
+                const double xlo = edge_total<R>(tg.template edge<0>(i, j, k), eb, hadv);
+                t1 = xhi - xlo;
+                t2 = cen_total<NS, R>(P, F, tg.cell(i, j, k), 1, i, j, k) -
+                     cen_total<NS, R>(P, F, tg.cell(i, j - 1, k), 1, i, j - 1, k);
+                edge_adv<NS, R, 2>(P, F, i, j, k + 1, ea, eb);
+                const double zhi = edge_total<R>(tg.template edge<2>(i, j, k + 1), ea, hadv);
+                edge_adv<NS, R, 2>(P, F, i, j, k, ea, eb);
+                const double zlo = edge_total<R>(tg.template edge<2>(i, j, k), ea, hadv);
+                t3 = zhi - zlo;
+            } else {
+                edge_adv<NS, R, 1>(P, F, i + 1, j, k, ea, eb);
+                const double xhi = edge_total<R>(tg.template edge<1>(i + 1, j, k), eb, hadv);
+                edge_adv<NS, R, 1>(P, F, i, j, k, ea, eb);
+                const double xlo = edge_total<R>(tg.template edge<1>(i, j, k), eb, hadv);
+                t1 = xhi - xlo;
+                edge_adv<NS, R, 2>(P, F, i, j + 1, k, ea, eb);
+                const double yhi = edge_total<R>(tg.template edge<2>(i, j + 1, k), eb, hadv);
+                edge_adv<NS, R, 2>(P, F, i, j, k, ea, eb);
+                const double ylo = edge_total<R>(tg.template edge<2>(i, j, k), eb, hadv);
+                t2 = yhi - ylo;
+                t3 = cen_total<NS, R>(P, F, tg.cell(i, j, k), 2, i, j, k) -
+                     cen_total<NS, R>(P, F, tg.cell(i, j, k - 1), 2, i, j, k - 1);
+            }
+            const double rsum = F.cons(i - e0, j - e1, k - e2, 0) + F.cons(i, j, k, 0);
+            const double m0 = a.mom0[d](i, j, k);
+            double v;
+            if (st == 1) {
+                v = m0 - dt * t1 / P.dx[0] - dt * t2 / P.dx[1] - dt * t3 / P.dx[2] + 0.5 * dt * P.grav[d] * rsum;
+            } else if (st == 2) {
+                v = 0.25 * 3.0 * m0 + 0.25 * F.mom[d](i, j, k) - 0.25 * dt * t1 / P.dx[0] - 0.25 * dt * t2 / P.dx[1] -
+                    0.25 * dt * t3 / P.dx[2] + 0.5 * 0.25 * dt * P.grav[d] * rsum;
+            } else {
+                v = (2. / 3.) * (0.5 * m0 + F.mom[d](i, j, k)) - (2. / 3.) * dt * t1 / P.dx[0] -
+                    (2. / 3.) * dt * t2 / P.dx[1] - (2. / 3.) * dt * t3 / P.dx[2] +
+                    0.5 * (2. / 3.) * dt * P.grav[d] * rsum;
+            }
+            a.mom_o[d](i, j, k) = v;
         }
-        const int e0 = d == 0, e1 = d == 1, e2 = d == 2;
-        const double rsum = F.cons(i - e0, j - e1, k - e2, 0) + F.cons(i, j, k, 0);
-        const double m0 = a.mom0[d](i, j, k);
-        double v;
-        if (st == 1) {
-            v = m0 - dt * t1 / P.dx[0] - dt * t2 / P.dx[1] - dt * t3 / P.dx[2] + 0.5 * dt * P.grav[d] * rsum;
-        } else if (st == 2) {
-            v = 0.25 * 3.0 * m0 + 0.25 * F.mom[d](i, j, k) - 0.25 * dt * t1 / P.dx[0] - 0.25 * dt * t2 / P.dx[1] -
-                0.25 * dt * t3 / P.dx[2] + 0.5 * 0.25 * dt * P.grav[d] * rsum;
-        } else {
-            v = (2. / 3.) * (0.5 * m0 + F.mom[d](i, j, k)) - (2. / 3.) * dt * t1 / P.dx[0] -
-                (2. / 3.) * dt * t2 / P.dx[1] - (2. / 3.) * dt * t3 / P.dx[2] + 0.5 * (2. / 3.) * dt * P.grav[d] * rsum;
-        }
-        a.mom_o[d](i, j, k) = v;
     }
 }
 
@@ -335,11 +293,11 @@ struct ConvArgs {
 template <int NS>
 __global__ void __launch_bounds__(128) k_convert(ConvArgs<NS> a) {
     const DevParams& P = a.P;
-    const int64_t tot = (int64_t)P.n[0] * P.n[1] * P.n[2];
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < tot; q += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(q % P.n[0]);
-        const int j = (int)((q / P.n[0]) % P.n[1]);
-        const int k = (int)(q / ((int64_t)P.n[0] * P.n[1]));
+    const int tot = P.n[0] * P.n[1] * P.n[2];
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) {
+        const int i = q % P.n[0];
+        const int j = (q / P.n[0]) % P.n[1];
+        const int k = q / (P.n[0] * P.n[1]);
         const Arr4<double>& cons = a.cons;
         const double rho = cons(i, j, k, 0);
         const Arr4<const double>&mx = a.mom[0], &my = a.mom[1], &mz = a.mom[2];

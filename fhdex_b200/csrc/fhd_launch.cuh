@@ -84,54 +84,58 @@ int launch_cellprep(const StageCall& c) {
     return cuda_rc(cudaGetLastError());
 }
 
-template <int NS, class R, int NZ, int TX, int TY, int TZ>
-int launch_stage_t(const StageCall& c) {
+// block sizes of the stage kernels available to the autotuner
+constexpr int kStageBlocks[] = {128, 256, 64};
+constexpr int kNumStageBlocks = 3;
+
+template <int NS, class R, int NZ>
+StageArgs<NS, R, NZ> make_stage_args(const StageCall& c) {
     StageArgs<NS, R, NZ> a;
     a.P = c.P;
     a.F = make_fields<NS, R>(c);
     a.noise = make_noise<NZ>(c);
-    a.cons0 = view<const double>(c.cons0);
-    a.cons_o = view<double>(c.cons_o);
+    a.ct = view<R>(c.ct);
+    a.et = view<R>(c.et);
     for (int d = 0; d < 3; ++d) {
+        a.ff[d] = view<double>(c.sff[d]);
         a.mom0[d] = view<const double>(c.mom0[d]);
         a.mom_o[d] = view<double>(c.mom_o[d]);
     }
+    a.cons0 = view<const double>(c.cons0);
+    a.cons_o = view<double>(c.cons_o);
     a.src = view<const double>(c.src);
     a.stage = c.stage;
-    using SM = StageSmem<NS, R, TX, TY, TZ>;
-    const size_t smem = sizeof(SM);
-    auto kern = k_stage<NS, R, NZ, TX, TY, TZ>;
-    static bool attr_set = false;  // per instantiation
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return FHD_ERR_CUDA;
-        attr_set = true;
+    return a;
+}
+
+inline int stage_block(const StageCall& c) {
+    return (c.tile >= 0 && c.tile < kNumStageBlocks) ? kStageBlocks[c.tile] : 128;
+}
+
+// part: 0 stresses, 1 face fluxes (all three directions), 2 update
+template <int NS, class R, int NZ>
+int launch_stage_part_t(const StageCall& c, int part) {
+    const StageArgs<NS, R, NZ> a = make_stage_args<NS, R, NZ>(c);
+    const int* N = c.P.n;
+    const int b = stage_block(c);
+    if (part == 0) {
+        k_taus<NS, R, NZ><<<grid_for((int64_t)(N[0] + 2) * (N[1] + 2) * (N[2] + 2), b), b, 0, c.stream>>>(a);
+    } else if (part == 1) {
+        k_faces<NS, R, NZ, 0><<<grid_for((int64_t)(N[0] + 1) * N[1] * N[2], b), b, 0, c.stream>>>(a);
+        k_faces<NS, R, NZ, 1><<<grid_for((int64_t)N[0] * (N[1] + 1) * N[2], b), b, 0, c.stream>>>(a);
+        k_faces<NS, R, NZ, 2><<<grid_for((int64_t)N[0] * N[1] * (N[2] + 1), b), b, 0, c.stream>>>(a);
+    } else {
+        k_update<NS, R, NZ><<<grid_for((int64_t)(N[0] + 1) * (N[1] + 1) * (N[2] + 1), b), b, 0, c.stream>>>(a);
     }
-    const int ntiles = ((c.P.n[0] + TX - 1) / TX) * ((c.P.n[1] + TY - 1) / TY) * ((c.P.n[2] + TZ - 1) / TZ);
-    kern<<<ntiles, TX * TY * TZ, smem, c.stream>>>(a);
     return cuda_rc(cudaGetLastError());
 }
 
-// tile shapes available to the autotuner
-#define FHD_TILES(X) X(8, 8, 4) X(16, 4, 4) X(8, 4, 4) X(16, 8, 2)
-
-template <int NS, class R, int NZ>
-int launch_stage_tiles(const StageCall& c) {
-    int t = 0;
-#define FHD_TRY(a, b, d)                                                      \
-    if (c.tile == t) return launch_stage_t<NS, R, NZ, a, b, d>(c);          \
-    ++t;
-    FHD_TILES(FHD_TRY)
-#undef FHD_TRY
-    return launch_stage_t<NS, R, NZ, 8, 8, 4>(c);
-}
-
 template <int NS, class R>
-int launch_stage(const StageCall& c) {
+int launch_stage_part(const StageCall& c, int part) {
     switch (c.mode) {
-        case NM_OFF: return launch_stage_tiles<NS, R, NZ_OFF>(c);
-        case NM_AB: return launch_stage_tiles<NS, R, NZ_AB>(c);
-        case NM_PHILOX: return launch_stage_tiles<NS, R, NZ_PHILOX>(c);
+        case NM_OFF: return launch_stage_part_t<NS, R, NZ_OFF>(c, part);
+        case NM_AB: return launch_stage_part_t<NS, R, NZ_AB>(c, part);
+        case NM_PHILOX: return launch_stage_part_t<NS, R, NZ_PHILOX>(c, part);
         default: return FHD_ERR_BAD_ARG;
     }
 }

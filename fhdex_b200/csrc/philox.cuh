@@ -3,12 +3,13 @@
 // Philox-4x32-10 as published by Salmon, Moraes, Dror, Shaw, "Parallel random
 // numbers: as easy as 1, 2, 3" (SC'11): 10 rounds of two 32x32->64 multiplies
 // with the Weyl key schedule.  One call per (periodic point, noise field) gives
-// the pair (z_A, z_B) of standard normals through a Box-Muller transform in FP32
-// (CUDA's logf / sincospif), so the A and B white-noise fields of one step are
-// regenerated identically in each RK stage and never stored.
+// the pairs (z_A, z_B) of standard normals of two noise fields through
+// Box-Muller transforms in FP32 (CUDA's logf / __sincosf), so the A and B
+// white-noise fields of one step are regenerated identically in each RK stage and
+// never stored.
 //
 // Counter layout: c0 = canonical periodic point index (i mod Nx) + Nx*((j mod Ny)
-// + Ny*(k mod Nz)), c1 = noise field id, c2/c3 = step (low/high).  Using the
+// + Ny*(k mod Nz)), c1 = noise field id / 2, c2/c3 = step (low/high).  Using the
 // canonical index reproduces OverrideSync/FillBoundary: periodic duplicates of a
 // nodal point and the periodic ghost images of a cell see the same numbers.
 #pragma once
@@ -40,35 +41,48 @@ FHD_HD void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
     }
 }
 
-// (z_A, z_B) for one (canonical point, field): Box-Muller on two 24-bit uniforms
-// in (0,1).
-FHD_D void normal_pair(uint32_t key0, uint32_t key1, uint32_t pidx, uint32_t fid, uint64_t step, float& za,
-                       float& zb) {
-    uint32_t c[4] = {pidx, fid, (uint32_t)step, (uint32_t)(step >> 32)};
-    philox4x32_10(c, key0, key1);
-    const float u1 = ((float)(c[0] >> 8) + 0.5f) * 5.9604644775390625e-8f;  // 2^-24
-    const float u2 = ((float)(c[1] >> 8) + 0.5f) * 5.9604644775390625e-8f;
-    const float r = sqrtf(-2.0f * logf(u1));
+// Box-Muller pair from two 32-bit words: 24-bit uniforms in (0,1), angle in
+// (-pi, pi) (the accuracy range of __sincosf).
+FHD_D void box_muller(uint32_t w0, uint32_t w1, float& za, float& zb) {
+    const float u1 = ((float)(w0 >> 8) + 0.5f) * 5.9604644775390625e-8f;  // 2^-24
+    const float u2 = ((float)(w1 >> 8) + 0.5f) * 5.9604644775390625e-8f;
+    const float r = sqrtf(fmaxf(-2.0f * logf(u1), 0.0f));
     float s, co;
-    sincospif(2.0f * u2, &s, &co);
+    __sincosf(6.28318530717958648f * (u2 - 0.5f), &s, &co);
     za = r * co;
     zb = r * s;
 }
 
-FHD_HD int wrapn(int i, int n) {
-    int r = i % n;
-    return r < 0 ? r + n : r;
+// One Philox call serves the two noise fields 2q and 2q+1 at a point:
+// words (0,1) -> field 2q, words (2,3) -> field 2q+1; each field gets (z_A, z_B).
+FHD_D void normal_quad(uint32_t key0, uint32_t key1, uint32_t pidx, uint32_t fpair, uint64_t step, float (&z)[4]) {
+    uint32_t c[4] = {pidx, fpair, (uint32_t)step, (uint32_t)(step >> 32)};
+    philox4x32_10(c, key0, key1);
+    box_muller(c[0], c[1], z[0], z[1]);
+    box_muller(c[2], c[3], z[2], z[3]);
 }
+
+// (z_A, z_B) of one field
+FHD_D void normal_pair(uint32_t key0, uint32_t key1, uint32_t pidx, uint32_t fid, uint64_t step, float& za,
+                       float& zb) {
+    float z[4];
+    normal_quad(key0, key1, pidx, fid >> 1, step, z);
+    za = (fid & 1) ? z[2] : z[0];
+    zb = (fid & 1) ? z[3] : z[1];
+}
+
+// canonical periodic index of a point within one period of the box
+FHD_HD int wrap1(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
 FHD_HD uint32_t canon(const DevParams& P, int i, int j, int k) {
-    return (uint32_t)wrapn(i, P.n[0]) +
-           (uint32_t)P.n[0] * ((uint32_t)wrapn(j, P.n[1]) + (uint32_t)P.n[1] * (uint32_t)wrapn(k, P.n[2]));
+    return (uint32_t)wrap1(i, P.n[0]) +
+           (uint32_t)P.n[0] * ((uint32_t)wrap1(j, P.n[1]) + (uint32_t)P.n[1] * (uint32_t)wrap1(k, P.n[2]));
 }
 
-// Field ids: face d comp c (c = 0 energy, 1.. species) -> d*(MAXS+1)+c;
-// edges xy,xz,yz -> 3*(MAXS+1)+e; centres -> 3*(MAXS+1)+3+d.
-FHD_HD uint32_t fid_face(int d, int c) { return (uint32_t)(d * (MAXS + 1) + c); }
-FHD_HD uint32_t fid_edge(int e) { return (uint32_t)(3 * (MAXS + 1) + e); }
-FHD_HD uint32_t fid_cen(int d) { return (uint32_t)(3 * (MAXS + 1) + 3 + d); }
+// Field ids: face d comp c (0 energy, 1.. species) -> 16 d + c; edges xy, xz, yz ->
+// 48 + e; centres -> 52 + d.  Fields 2q, 2q+1 share one Philox call.
+FHD_HD uint32_t fid_face(int d, int c) { return (uint32_t)(16 * d + c); }
+FHD_HD uint32_t fid_edge(int e) { return (uint32_t)(48 + e); }
+FHD_HD uint32_t fid_cen(int d) { return (uint32_t)(52 + d); }
 
 }  // namespace fhd

@@ -122,16 +122,17 @@ typedef struct fhd_ctx fhd_ctx;
 int fhd_create(fhd_ctx** ctx, const fhd_params* params, int device);
 int fhd_destroy(fhd_ctx* ctx);
 const char* fhd_strerror(int code);
-/* Use an external CUDA stream (cudaStream_t as void*); NULL = the context's own. */
+/* Enqueue on an external CUDA stream (cudaStream_t as void*; NULL = the legacy
+ * default stream).  Until called, the context uses a stream of its own. */
 int fhd_set_stream(fhd_ctx* ctx, void* stream);
 int fhd_synchronize(fhd_ctx* ctx);
 /* Reads and clears the device status word (blocks on the stream). */
 int fhd_status(fhd_ctx* ctx);
 /* Effective parameters (after GetHcGas). */
 int fhd_get_params(const fhd_ctx* ctx, fhd_params* out);
-/* Tile shape of the fused stage kernel (index into fhd_tile_name's list); the
- * autotuner in the Python host layer times them and sets the fastest.  No
- * reference counterpart (AMReX picks its own launch shapes). */
+/* Launch shape of the stage kernels (index into fhd_tile_name's list); the
+ * autotuner in the host layer times them and sets the fastest.  No reference
+ * counterpart (AMReX picks its own launch shapes). */
 int fhd_set_tile(fhd_ctx* ctx, int tile);
 int fhd_num_tiles(void);
 const char* fhd_tile_name(int tile);
@@ -213,10 +214,12 @@ int fhd_rk3_step_stag_host(fhd_ctx* ctx, fhd_fab cu, const fhd_fab mom[3], fhd_f
 
 /* Per-kernel timing of the step with CUDA events on the launching stream
  * (tracing aid in place of the reference's TinyProfiler regions).  Kinds:
- * 0 cellprep, 1 stage (fused flux/update), 2 ghost fill, 3 conversion,
- * 4 by-product fluxes.  fhd_profile_read synchronizes, sums the elapsed times
- * (ms) and launch counts per kind since the last reset, and resets. */
-#define FHD_PROF_KINDS 5
+ * 0 cellprep (conversion + transport), 1 stresses, 2 face fluxes (the three
+ * per-direction launches together), 3 divergence/RK update, 4 ghost fill,
+ * 5 final conversion, 6 by-product fluxes.  fhd_profile_read synchronizes, sums
+ * the elapsed times (ms) and bracketed launches per kind since the last read,
+ * and resets. */
+#define FHD_PROF_KINDS 7
 int fhd_profile(fhd_ctx* ctx, int enable);
 int fhd_profile_read(fhd_ctx* ctx, double* ms, int64_t* launches);
 
