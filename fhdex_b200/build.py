@@ -33,6 +33,7 @@ def _units():
         u.append((f"kern_mixed_ns{ns}", "fhd_kern_ns.cu", [f"-DFHD_NS={ns}", "-DFHD_MIXED=1", "-fmad=true"]))
     u.append(("exact_util", "fhd_exact.cu", ["-fmad=false"]))
     u.append(("capi", "fhd_capi.cu", ["-fmad=false"]))
+    u.append(("noalloc", "fhd_noalloc.cu", ["-fmad=false"]))
     return u
 
 

@@ -18,6 +18,7 @@ FHD_ERR_OOM = 4
 FHD_ERR_TIMEOUT = 5
 FHD_ERR_CUDA = 6
 FHD_ERR_UNSUPPORTED = 7
+FHD_ERR_TOO_LARGE = 8
 
 FHD_F64 = 0
 FHD_F32 = 1
@@ -118,6 +119,7 @@ def _declare(lib):
         "fhd_tile_name": (C.c_char_p, [i]),
         "fhd_profile": (i, [vp, i]),
         "fhd_profile_read": (i, [vp, P(d), P(C.c_int64)]),
+        "fhd_rk3_step_stag_noalloc": (i, [P(FhdParams), fab, pfab, fab, pfab, d, C.c_int64, vp, P(i)]),
     }
     for name, (res, args) in sigs.items():
         if hasattr(lib, name):

@@ -255,6 +255,7 @@ const char* fhd_strerror(int code) {
         case FHD_ERR_TIMEOUT: return "bounded device wait timed out";
         case FHD_ERR_CUDA: return "CUDA runtime error";
         case FHD_ERR_UNSUPPORTED: return "option outside the implemented scope";
+        case FHD_ERR_TOO_LARGE: return "box too large for the 16 MiB static scratch of fhd_rk3_step_stag_noalloc";
         default: return "unknown error";
     }
 }

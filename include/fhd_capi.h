@@ -46,7 +46,8 @@ enum {
     FHD_ERR_OOM = 4,         /* device allocation failed                          */
     FHD_ERR_TIMEOUT = 5,     /* a bounded device wait gave up                     */
     FHD_ERR_CUDA = 6,        /* a CUDA runtime call failed                        */
-    FHD_ERR_UNSUPPORTED = 7  /* option outside the implemented scope              */
+    FHD_ERR_UNSUPPORTED = 7, /* option outside the implemented scope              */
+    FHD_ERR_TOO_LARGE = 8    /* box does not fit fhd_rk3_step_stag_noalloc's scratch */
 };
 
 /* fab element types */
@@ -222,6 +223,30 @@ int fhd_rk3_step_stag_host(fhd_ctx* ctx, fhd_fab cu, const fhd_fab mom[3], fhd_f
 #define FHD_PROF_KINDS 7
 int fhd_profile(fhd_ctx* ctx, int enable);
 int fhd_profile_read(fhd_ctx* ctx, double* ms, int64_t* launches);
+
+/* RK3stepStag without any device allocation, for callers that cannot allocate:
+ * code whose device memory is owned by an arena that a stray cudaMalloc would
+ * fail or fragment, framework callbacks that forbid allocation on their hot
+ * path, and latency-critical loops that cannot pay the device-wide
+ * synchronisation of cudaMalloc/cudaFree.  No reference counterpart (the
+ * reference allocates its stage temporaries inside RK3stepStag,
+ * timeStepStag.cpp:30-153); this entry point has no context either.
+ *
+ * Same step as fhd_rk3_step_stag with FP64 precision, in-kernel Philox noise
+ * (or none when stoch_stress_form == 0) and no by-product outputs, on the
+ * caller's stream (NULL = legacy default stream).  Its stage scratch is a
+ * file-scope 16 MiB device array held by every GPU that loads the library until
+ * the process exits; boxes whose scratch does not fit (about 28^3 cells with 2
+ * species, 24^3 with 4) return FHD_ERR_TOO_LARGE before any GPU work.  The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress,
+ * that device current): make it before any stream capture.  Calls share the
+ * array and it keeps the last call's contents, so calls whose GPU work overlaps
+ * race; serialise them.  status (optional): when non-NULL the call waits for
+ * the stream and stores the device status word (0 or FHD_ERR_MASSFRAC /
+ * FHD_ERR_NONFINITE). */
+int fhd_rk3_step_stag_noalloc(const fhd_params* params, fhd_fab cu, const fhd_fab mom[3],
+                              fhd_fab prim, const fhd_fab vel[3], double dt, int64_t step,
+                              void* stream, int* status);
 
 #ifdef __cplusplus
 }
