@@ -225,6 +225,7 @@ def autotune(ctx, st, dt, steps=2):
     import torch
     from fhdex_b200.context import Context
     best = None
+    table = {}
     for t, name in enumerate(Context.tiles()):
         ctx.set_tile(t)
         ctx.rk3_step(st, dt, 0, aux=False)
@@ -235,10 +236,11 @@ def autotune(ctx, st, dt, steps=2):
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / steps
+        table[name] = round(ms, 3)
         if best is None or ms < best[1]:
             best = (t, ms, name)
     ctx.set_tile(best[0])
-    return best
+    return best[0], best[1], best[2], table
 
 
 def run_ours(args):
@@ -260,8 +262,9 @@ def run_ours(args):
     ctx = Context(p, local)
     st = StagState(p, f"cuda:{local}", aux=False)
     ctx.init_state(st)
+    tune = None
     if args.tile == "auto":
-        t, ms, tname = autotune(ctx, st, dt)
+        t, ms, tname, tune = autotune(ctx, st, dt)
     else:
         ctx.set_tile(int(args.tile))
         tname = Context.tiles()[int(args.tile)]
@@ -364,7 +367,7 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
         "data": "synthetic (uniform argon at rest + in-kernel Philox noise; no dataset)",
-        "config": config_dict(args, p, dt, tname),
+        "config": dict(config_dict(args, p, dt, tname), autotune_ms_per_step=tune),
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
         "clocks": clk, "status": status,
     }

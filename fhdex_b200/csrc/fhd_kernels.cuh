@@ -160,9 +160,10 @@ struct GlobalTaus {
     }
 };
 
-// conservative fluxes of the faces of direction D; one thread per valid face
-template <int NS, class R, int NZ, int D>
-__global__ void __launch_bounds__(256) k_faces(StageArgs<NS, R, NZ> a) {
+// conservative fluxes of the faces of direction D; one thread per valid face.
+// MINB = minimum resident blocks requested from the register allocator (1: no cap).
+template <int NS, class R, int NZ, int D, int BS, int MINB>
+__global__ void __launch_bounds__(BS, MINB) k_faces(StageArgs<NS, R, NZ> a) {
     const DevParams& P = a.P;
     const int nx = P.n[0] + (D == 0), ny = P.n[1] + (D == 1), nz = P.n[2] + (D == 2);
     const int tot = nx * ny * nz;

@@ -84,9 +84,11 @@ int launch_cellprep(const StageCall& c) {
     return cuda_rc(cudaGetLastError());
 }
 
-// block sizes of the stage kernels available to the autotuner
-constexpr int kStageBlocks[] = {128, 256, 64};
-constexpr int kNumStageBlocks = 3;
+// launch shapes available to the autotuner: block size of the stage kernels and
+// the register cap of the face-flux kernel (minimum resident blocks per SM)
+constexpr int kStageBlocks[] = {128, 256, 128, 128, 128};
+constexpr int kFaceMinBlocks[] = {4, 2, 6, 2, 8};
+constexpr int kNumStageBlocks = 5;
 
 template <int NS, class R, int NZ>
 StageArgs<NS, R, NZ> make_stage_args(const StageCall& c) {
@@ -121,9 +123,19 @@ int launch_stage_part_t(const StageCall& c, int part) {
     if (part == 0) {
         k_taus<NS, R, NZ><<<grid_for((int64_t)(N[0] + 2) * (N[1] + 2) * (N[2] + 2), b), b, 0, c.stream>>>(a);
     } else if (part == 1) {
-        k_faces<NS, R, NZ, 0><<<grid_for((int64_t)(N[0] + 1) * N[1] * N[2], b), b, 0, c.stream>>>(a);
-        k_faces<NS, R, NZ, 1><<<grid_for((int64_t)N[0] * (N[1] + 1) * N[2], b), b, 0, c.stream>>>(a);
-        k_faces<NS, R, NZ, 2><<<grid_for((int64_t)N[0] * N[1] * (N[2] + 1), b), b, 0, c.stream>>>(a);
+        const int t = (c.tile >= 0 && c.tile < kNumStageBlocks) ? c.tile : 0;
+#define FHD_FACES(BS, MINB)                                                                                      \
+        k_faces<NS, R, NZ, 0, BS, MINB><<<grid_for((int64_t)(N[0] + 1) * N[1] * N[2], BS), BS, 0, c.stream>>>(a); \
+        k_faces<NS, R, NZ, 1, BS, MINB><<<grid_for((int64_t)N[0] * (N[1] + 1) * N[2], BS), BS, 0, c.stream>>>(a); \
+        k_faces<NS, R, NZ, 2, BS, MINB><<<grid_for((int64_t)N[0] * N[1] * (N[2] + 1), BS), BS, 0, c.stream>>>(a);
+        switch (t) {
+            case 0: FHD_FACES(128, 4) break;
+            case 1: FHD_FACES(256, 2) break;
+            case 2: FHD_FACES(128, 6) break;
+            case 3: FHD_FACES(128, 2) break;
+            default: FHD_FACES(128, 8) break;
+        }
+#undef FHD_FACES
     } else {
         k_update<NS, R, NZ><<<grid_for((int64_t)(N[0] + 1) * (N[1] + 1) * (N[2] + 1), b), b, 0, c.stream>>>(a);
     }
