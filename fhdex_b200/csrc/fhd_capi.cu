@@ -29,6 +29,7 @@ struct fhd_ctx {
     fhd_fab ceta{}, czeta{}, ckappa{}, cchi{}, cD{};
     fhd_fab ct{}, et{};          // stage stresses (coefficient precision)
     fhd_fab sff[3]{};            // stage conservative face fluxes (f64)
+    fhd_fab smc{}, sme{};        // stage total centre / edge momentum fluxes (f64)
     int tile = 0;
     // device mirrors for the host-buffer step
     double* hbuf = nullptr;
@@ -143,8 +144,9 @@ int ensure_scratch(fhd_ctx* c) {
     const int ns = c->prm.nspecies;
     const int allnod[3] = {1, 1, 1};
     const int64_t npts = fab_points(make_fab(nullptr, n, allnod, 0, 1, FHD_F64));  // [0, n]^3
-    const size_t need = (size_t)(2 * cellpts * nvars + 2 * (fpts[0] + fpts[1] + fpts[2]) + 3 * npts * (2 + ns)) *
-                        sizeof(double);
+    const int64_t c1pts = fab_points(make_fab(nullptr, n, CELLN, 1, 1, FHD_F64));  // cells grown by 1
+    const size_t need = (size_t)(2 * cellpts * nvars + 2 * (fpts[0] + fpts[1] + fpts[2]) + 3 * npts * (2 + ns) +
+                                 3 * c1pts + 6 * npts) * sizeof(double);
     if (c->scratch && c->scratch_bytes >= need) return FHD_OK;
     if (c->scratch) cudaFree(c->scratch);
     c->scratch = nullptr;
@@ -162,6 +164,8 @@ int ensure_scratch(fhd_ctx* c) {
         c->sff[d] = make_fab(p, n, allnod, 0, 2 + ns, FHD_F64);
         p += npts * (2 + ns);
     }
+    c->smc = make_fab(p, n, CELLN, 1, 3, FHD_F64); p += c1pts * 3;
+    c->sme = make_fab(p, n, allnod, 0, 6, FHD_F64);
     return FHD_OK;
 }
 
@@ -562,6 +566,8 @@ int fhd_rk3_step_stag(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim
     sc.tile = c->tile;
     sc.ct = c->ct;
     sc.et = c->et;
+    sc.smc = c->smc;
+    sc.sme = c->sme;
     for (int d = 0; d < 3; ++d) sc.sff[d] = c->sff[d];
     const fhd_fab* ins[3] = {&cu, &c->cup, &c->cup2};
     const fhd_fab* insm[3] = {mom, c->cupm, c->cup2m};

@@ -33,6 +33,7 @@ struct StageCall {
     NoiseFabs nz;
     fhd_fab ff[3], ef[6], cf[3];        // flux outputs of the operator path
     fhd_fab ct, et, sff[3];             // stage scratch: cell/edge stresses, face fluxes
+    fhd_fab smc, sme;                   // stage scratch: total centre / edge momentum fluxes
     int* status;
     cudaStream_t stream;
     int tile;               // tile-shape index of k_stage (autotuned)

@@ -89,6 +89,9 @@ __global__ void __launch_bounds__(128) k_cellprep(PrepArgs<NS, R> a) {
 //       3-5 deterministic xx,yy,zz
 //   et: edge stresses on the points [0, n]^3, comps (s,d) of xy, xz, yz at 0-1, 2-3, 4-5
 //   ff[d]: conservative face fluxes (rho, rhoE, rhoY) of direction d on [0, n]^3
+//   mc: total centre momentum fluxes (cenflux x, y, z) on the cells grown by 1
+//   me: total edge momentum fluxes on [0, n]^3 in the reference's order
+//       edgeflux_x[0..1], edgeflux_y[0..1], edgeflux_z[0..1]
 template <int NS, class R, int NZ>
 struct StageArgs {
     DevParams P;
@@ -96,6 +99,7 @@ struct StageArgs {
     Noise<NZ> noise;
     Arr4<R> ct, et;
     Arr4<double> ff[3];
+    Arr4<double> mc, me;
     Arr4<const double> cons0;    // U^0 (for the RK combination)
     Arr4<const double> mom0[3];
     Arr4<double> cons_o;         // U^{s+1}
@@ -117,24 +121,36 @@ __global__ void __launch_bounds__(256) k_taus(StageArgs<NS, R, NZ> a) {
         for (int d = 0; d < 3; ++d) {
             a.ct(i, j, k, d) = t.s[d];
             a.ct(i, j, k, 3 + d) = t.d[d];
+            a.mc(i, j, k, d) = cen_total<NS, R>(P, a.F, t, d, i, j, k);
         }
         if (i < 0 || j < 0 || k < 0) continue;
         double we[3] = {0.0, 0.0, 0.0};
         if (NZ != NZ_OFF) a.noise.edge_all(P, i, j, k, we);
+        const int hadv = P.advection_type >= 0;
+        double ea, eb;
         if (k < P.n[2]) {
             const Taus<R> e = edge_taus_w<NS, R, NZ, 0>(P, a.F, we[0], i, j, k);
             a.et(i, j, k, 0) = e.s;
             a.et(i, j, k, 1) = e.d;
+            edge_adv<NS, R, 0>(P, a.F, i, j, k, ea, eb);
+            a.me(i, j, k, 2) = edge_total<R>(e, ea, hadv);  // edgey_u
+            a.me(i, j, k, 0) = edge_total<R>(e, eb, hadv);  // edgex_v
         }
         if (j < P.n[1]) {
             const Taus<R> e = edge_taus_w<NS, R, NZ, 1>(P, a.F, we[1], i, j, k);
             a.et(i, j, k, 2) = e.s;
             a.et(i, j, k, 3) = e.d;
+            edge_adv<NS, R, 1>(P, a.F, i, j, k, ea, eb);
+            a.me(i, j, k, 4) = edge_total<R>(e, ea, hadv);  // edgez_u
+            a.me(i, j, k, 1) = edge_total<R>(e, eb, hadv);  // edgex_w
         }
         if (i < P.n[0]) {
             const Taus<R> e = edge_taus_w<NS, R, NZ, 2>(P, a.F, we[2], i, j, k);
             a.et(i, j, k, 4) = e.s;
             a.et(i, j, k, 5) = e.d;
+            edge_adv<NS, R, 2>(P, a.F, i, j, k, ea, eb);
+            a.me(i, j, k, 5) = edge_total<R>(e, ea, hadv);  // edgez_v
+            a.me(i, j, k, 3) = edge_total<R>(e, eb, hadv);  // edgey_w
         }
     }
 }
@@ -184,10 +200,8 @@ __global__ void __launch_bounds__(256) k_update(StageArgs<NS, R, NZ> a) {
     const Fields<NS, R>& F = a.F;
     const int nx = P.n[0] + 1, ny = P.n[1] + 1, nz = P.n[2] + 1;
     const int tot = nx * ny * nz;
-    const GlobalTaus<R> tg{a.ct, a.et};
     const double dt = P.dt;
     const int st = a.stage;
-    const int hadv = P.advection_type >= 0;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) {
         const int i = q % nx, j = (q / nx) % ny, k = q / (nx * ny);
         const bool cell = i < P.n[0] && j < P.n[1] && k < P.n[2];
@@ -219,46 +233,21 @@ __global__ void __launch_bounds__(256) k_update(StageArgs<NS, R, NZ> a) {
         for (int d = 0; d < 3; ++d) {
             const int e0 = d == 0, e1 = d == 1, e2 = d == 2;
             if (i >= P.n[0] + e0 || j >= P.n[1] + e1 || k >= P.n[2] + e2) continue;
-            double t1, t2, t3, ea, eb;
+            // momentum flux differences (timeStepStag.cpp:452-482): centre and edge
+            // totals stored by k_taus
+            double t1, t2, t3;
             if (d == 0) {
-                t1 = cen_total<NS, R>(P, F, tg.cell(i, j, k), 0, i, j, k) -
-                     cen_total<NS, R>(P, F, tg.cell(i - 1, j, k), 0, i - 1, j, k);
-                edge_adv<NS, R, 0>(P, F, i, j + 1, k, ea, eb);
-                const double ehi = edge_total<R>(tg.template edge<0>(i, j + 1, k), ea, hadv);
-                edge_adv<NS, R, 0>(P, F, i, j, k, ea, eb);
-                const double elo = edge_total<R>(tg.template edge<0>(i, j, k), ea, hadv);
-                t2 = ehi - elo;
-                edge_adv<NS, R, 1>(P, F, i, j, k + 1, ea, eb);
-                const double zhi = edge_total<R>(tg.template edge<1>(i, j, k + 1), ea, hadv);
-                edge_adv<NS, R, 1>(P, F, i, j, k, ea, eb);
-                const double zlo = edge_total<R>(tg.template edge<1>(i, j, k), ea, hadv);
-                t3 = zhi - zlo;
+                t1 = a.mc(i, j, k, 0) - a.mc(i - 1, j, k, 0);
+                t2 = a.me(i, j + 1, k, 2) - a.me(i, j, k, 2);   // edgey_u
+                t3 = a.me(i, j, k + 1, 4) - a.me(i, j, k, 4);   // edgez_u
             } else if (d == 1) {
-                edge_adv<NS, R, 0>(P, F, i + 1, j, k, ea, eb);
-                const double xhi = edge_total<R>(tg.template edge<0>(i + 1, j, k), eb, hadv);
-                edge_adv<NS, R, 0>(P, F, i, j, k, ea, eb);
-                const double xlo = edge_total<R>(tg.template edge<0>(i, j, k), eb, hadv);
-                t1 = xhi - xlo;
-                t2 = cen_total<NS, R>(P, F, tg.cell(i, j, k), 1, i, j, k) -
-                     cen_total<NS, R>(P, F, tg.cell(i, j - 1, k), 1, i, j - 1, k);
-                edge_adv<NS, R, 2>(P, F, i, j, k + 1, ea, eb);
-                const double zhi = edge_total<R>(tg.template edge<2>(i, j, k + 1), ea, hadv);
-                edge_adv<NS, R, 2>(P, F, i, j, k, ea, eb);
-                const double zlo = edge_total<R>(tg.template edge<2>(i, j, k), ea, hadv);
-                t3 = zhi - zlo;
+                t1 = a.me(i + 1, j, k, 0) - a.me(i, j, k, 0);   // edgex_v
+                t2 = a.mc(i, j, k, 1) - a.mc(i, j - 1, k, 1);
+                t3 = a.me(i, j, k + 1, 5) - a.me(i, j, k, 5);   // edgez_v
             } else {
-                edge_adv<NS, R, 1>(P, F, i + 1, j, k, ea, eb);
-                const double xhi = edge_total<R>(tg.template edge<1>(i + 1, j, k), eb, hadv);
-                edge_adv<NS, R, 1>(P, F, i, j, k, ea, eb);
-                const double xlo = edge_total<R>(tg.template edge<1>(i, j, k), eb, hadv);
-                t1 = xhi - xlo;
-                edge_adv<NS, R, 2>(P, F, i, j + 1, k, ea, eb);
-                const double yhi = edge_total<R>(tg.template edge<2>(i, j + 1, k), eb, hadv);
-                edge_adv<NS, R, 2>(P, F, i, j, k, ea, eb);
-                const double ylo = edge_total<R>(tg.template edge<2>(i, j, k), eb, hadv);
-                t2 = yhi - ylo;
-                t3 = cen_total<NS, R>(P, F, tg.cell(i, j, k), 2, i, j, k) -
-                     cen_total<NS, R>(P, F, tg.cell(i, j, k - 1), 2, i, j, k - 1);
+                t1 = a.me(i + 1, j, k, 1) - a.me(i, j, k, 1);   // edgex_w
+                t2 = a.me(i, j + 1, k, 3) - a.me(i, j, k, 3);   // edgey_w
+                t3 = a.mc(i, j, k, 2) - a.mc(i, j, k - 1, 2);
             }
             const double rsum = F.cons(i - e0, j - e1, k - e2, 0) + F.cons(i, j, k, 0);
             const double m0 = a.mom0[d](i, j, k);

@@ -98,6 +98,8 @@ StageArgs<NS, R, NZ> make_stage_args(const StageCall& c) {
     a.noise = make_noise<NZ>(c);
     a.ct = view<R>(c.ct);
     a.et = view<R>(c.et);
+    a.mc = view<double>(c.smc);
+    a.me = view<double>(c.sme);
     for (int d = 0; d < 3; ++d) {
         a.ff[d] = view<double>(c.sff[d]);
         a.mom0[d] = view<const double>(c.mom0[d]);

@@ -178,8 +178,9 @@ extern "C" int fhd_rk3_step_stag_noalloc(const fhd_params* params, fhd_fab cu, c
     fhd_fab ct = box(n, cell, 1, 6, FHD_F64), et = box(n, all, 0, 6, FHD_F64);
     fhd_fab sff[3];
     for (int d = 0; d < 3; ++d) sff[d] = box(n, all, 0, 2 + ns, FHD_F64);
+    fhd_fab smc = box(n, cell, 1, 3, FHD_F64), sme = box(n, all, 0, 6, FHD_F64);
     fhd_fab* parts[] = {&st, &cup, &cup2, &cupm[0], &cupm[1], &cupm[2], &cup2m[0], &cup2m[1], &cup2m[2], &eta,
-                        &zeta, &kappa, &chi, &D, &ct, &et, &sff[0], &sff[1], &sff[2]};
+                        &zeta, &kappa, &chi, &D, &ct, &et, &sff[0], &sff[1], &sff[2], &smc, &sme};
     {
         Carver dry{nullptr};
         for (fhd_fab* f : parts)
@@ -214,6 +215,8 @@ extern "C" int fhd_rk3_step_stag_noalloc(const fhd_params* params, fhd_fab cu, c
     sc.eta = eta; sc.zeta = zeta; sc.kappa = kappa; sc.chi = chi; sc.D = D;
     sc.ct = ct;
     sc.et = et;
+    sc.smc = smc;
+    sc.sme = sme;
     sc.status = dstatus;
     sc.stream = s;
     sc.tile = 0;
