@@ -374,8 +374,68 @@ def run_ours(args):
     print(json.dumps(out), flush=True)
 
 
+def run_ensemble(args):
+    """Batched ensemble: --members realisations of argon, half 32^3 and half 64^3,
+    T0 ~ U(250,350) K, rho0 ~ U(1e-3,3e-3) g/cm^3, one graph replay per step."""
+    import torch
+    from fhdex_b200.serve import ensemble
+    torch.cuda.set_device(0)
+    prec = 1 if args.precision == "mixed" else 0
+    b, states, cells = ensemble(args.members, seed=args.seed, precision=prec)
+    s = torch.cuda.Stream()
+    b.set_stream(s)
+    b.step(args.warmup, graph=True)
+    b.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(s):
+        e0.record()
+    b.step(args.steps, graph=True)
+    with torch.cuda.stream(s):
+        e1.record()
+    b.synchronize()
+    ms = e0.elapsed_time(e1)
+    bad = sum(1 for mid in list(b.members) if b.status(mid) != 0)
+    print(json.dumps({"mode": "ensemble", "metric": METRIC, "value": cells * args.steps / (ms / 1e3), "unit": UNIT,
+                      "members": args.members, "cells_total": cells, "steps": args.steps, "ms_per_step": ms / args.steps,
+                      "precision": args.precision, "members_with_status": bad,
+                      "launch": "23 batched kernels per step, one CUDA graph replay per step"}), flush=True)
+    b.close()
+
+
+def run_serve(args):
+    """Serving: Poisson arrivals (rate --rate), box edge log-uniform 16-128,
+    nspecies in {1,2,4}, steps U{100..2000}, precision FP64/mixed; continuous
+    batching vs serving one request at a time with the plain FP64 step."""
+    import torch
+    from fhdex_b200.serve import Server, latency_stats, poisson_trace, run_alone
+    torch.cuda.set_device(0)
+    steps = (args.serve_min_steps, args.serve_max_steps)
+    trace = poisson_trace(args.requests, rate=args.rate, seed=args.seed, steps=steps)
+    srv = Server(chunk=args.chunk)
+    reqs, _, cu_b, el_b = srv.run(trace)
+    srv.close()
+    torch.cuda.empty_cache()
+    lb = latency_stats(reqs)
+    trace2 = poisson_trace(args.requests, rate=args.rate, seed=args.seed, steps=steps)
+    reqs2, cu_a, el_a = run_alone(trace2)
+    la = latency_stats(reqs2)
+    print(json.dumps({"mode": "serve", "metric": METRIC, "unit": UNIT, "requests": args.requests, "rate_per_s": args.rate,
+                      "steps_range": list(steps),
+                      "served": {"value": cu_b / el_b, "elapsed_s": el_b, **lb,
+                                 "bad_status": sum(1 for r in reqs if r.status)},
+                      "alone_fp64": {"value": cu_a / el_a, "elapsed_s": el_a, **la,
+                                     "bad_status": sum(1 for r in reqs2 if r.status)}}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--mode", default="step", choices=["step", "ensemble", "serve"])
+    ap.add_argument("--members", type=int, default=512)
+    ap.add_argument("--requests", type=int, default=48)
+    ap.add_argument("--rate", type=float, default=50.0)
+    ap.add_argument("--chunk", type=int, default=20)
+    ap.add_argument("--serve-min-steps", type=int, default=100)
+    ap.add_argument("--serve-max-steps", type=int, default=2000)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
@@ -393,6 +453,10 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.mode == "ensemble":
+        run_ensemble(args)
+    elif args.mode == "serve":
+        run_serve(args)
     else:
         run_ours(args)
 

@@ -34,6 +34,7 @@ def _units():
     u.append(("exact_util", "fhd_exact.cu", ["-fmad=false"]))
     u.append(("capi", "fhd_capi.cu", ["-fmad=false"]))
     u.append(("noalloc", "fhd_noalloc.cu", ["-fmad=false"]))
+    u.append(("batch", "fhd_batch.cu", ["-fmad=false"]))
     return u
 
 

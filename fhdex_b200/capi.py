@@ -120,6 +120,15 @@ def _declare(lib):
         "fhd_profile": (i, [vp, i]),
         "fhd_profile_read": (i, [vp, P(d), P(C.c_int64)]),
         "fhd_rk3_step_stag_noalloc": (i, [P(FhdParams), fab, pfab, fab, pfab, d, C.c_int64, vp, P(i)]),
+        "fhd_batch_create": (i, [P(vp), i, i, i]),
+        "fhd_batch_destroy": (i, [vp]),
+        "fhd_batch_set_stream": (i, [vp, vp]),
+        "fhd_batch_add": (i, [vp, P(FhdParams), fab, pfab, fab, pfab, d, C.c_int64, P(d), P(i)]),
+        "fhd_batch_remove": (i, [vp, i]),
+        "fhd_batch_step": (i, [vp, i, i]),
+        "fhd_batch_size": (i, [vp]),
+        "fhd_batch_member_status": (i, [vp, i]),
+        "fhd_batch_synchronize": (i, [vp]),
     }
     for name, (res, args) in sigs.items():
         if hasattr(lib, name):

@@ -59,7 +59,10 @@ struct DevParams {
     // noise
     uint32_t key0, key1;             // Philox key
     uint64_t step;                   // Philox counter words 2-3
+    const uint64_t* step_ptr;        // when set, the step is read here (batched graph replay)
 };
+
+FHD_D uint64_t noise_step(const DevParams& P) { return P.step_ptr ? *P.step_ptr : P.step; }
 
 // ---- EOS helpers (compressible_functions.H:138-219, 1497-1520) ----------------------
 

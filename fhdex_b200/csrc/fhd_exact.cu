@@ -34,6 +34,31 @@ int mixed_stage_ns4(const StageCall&, int);
 int exact_transport_ns4(const DevParams&, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, int*, cudaStream_t);
 int exact_convert_ns4(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const fhd_fab*, int*, cudaStream_t);
 
+size_t exact_batch_args_size_ns1(int, int);
+void exact_batch_pack_ns1(int, int, const StageCall&, void*);
+int exact_batch_launch_ns1(int, int, const void*, const int*, int, int, cudaStream_t);
+size_t mixed_batch_args_size_ns1(int, int);
+void mixed_batch_pack_ns1(int, int, const StageCall&, void*);
+int mixed_batch_launch_ns1(int, int, const void*, const int*, int, int, cudaStream_t);
+size_t exact_batch_args_size_ns2(int, int);
+void exact_batch_pack_ns2(int, int, const StageCall&, void*);
+int exact_batch_launch_ns2(int, int, const void*, const int*, int, int, cudaStream_t);
+size_t mixed_batch_args_size_ns2(int, int);
+void mixed_batch_pack_ns2(int, int, const StageCall&, void*);
+int mixed_batch_launch_ns2(int, int, const void*, const int*, int, int, cudaStream_t);
+size_t exact_batch_args_size_ns3(int, int);
+void exact_batch_pack_ns3(int, int, const StageCall&, void*);
+int exact_batch_launch_ns3(int, int, const void*, const int*, int, int, cudaStream_t);
+size_t mixed_batch_args_size_ns3(int, int);
+void mixed_batch_pack_ns3(int, int, const StageCall&, void*);
+int mixed_batch_launch_ns3(int, int, const void*, const int*, int, int, cudaStream_t);
+size_t exact_batch_args_size_ns4(int, int);
+void exact_batch_pack_ns4(int, int, const StageCall&, void*);
+int exact_batch_launch_ns4(int, int, const void*, const int*, int, int, cudaStream_t);
+size_t mixed_batch_args_size_ns4(int, int);
+void mixed_batch_pack_ns4(int, int, const StageCall&, void*);
+int mixed_batch_launch_ns4(int, int, const void*, const int*, int, int, cudaStream_t);
+
 #define FHD_DISPATCH(ns, fn, ...)            \
     switch (ns) {                             \
         case 1: return fn##1(__VA_ARGS__);    \
@@ -57,6 +82,66 @@ int exact_convert(const DevParams& P, fhd_fab prim, const fhd_fab vel[3], fhd_fa
     FHD_DISPATCH(P.ns, exact_convert_ns, P, prim, vel, cons, mom, status, s)
 }
 
+size_t batch_args_size(int ns, bool mixed, int kind, int mode) {
+    switch (ns) {
+        case 1: return mixed ? mixed_batch_args_size_ns1(kind, mode) : exact_batch_args_size_ns1(kind, mode);
+        case 2: return mixed ? mixed_batch_args_size_ns2(kind, mode) : exact_batch_args_size_ns2(kind, mode);
+        case 3: return mixed ? mixed_batch_args_size_ns3(kind, mode) : exact_batch_args_size_ns3(kind, mode);
+        case 4: return mixed ? mixed_batch_args_size_ns4(kind, mode) : exact_batch_args_size_ns4(kind, mode);
+        default: return 0;
+    }
+}
+void batch_pack(int ns, bool mixed, int kind, int mode, const StageCall& c, void* dst) {
+    switch (ns) {
+        case 1: mixed ? mixed_batch_pack_ns1(kind, mode, c, dst) : exact_batch_pack_ns1(kind, mode, c, dst); break;
+        case 2: mixed ? mixed_batch_pack_ns2(kind, mode, c, dst) : exact_batch_pack_ns2(kind, mode, c, dst); break;
+        case 3: mixed ? mixed_batch_pack_ns3(kind, mode, c, dst) : exact_batch_pack_ns3(kind, mode, c, dst); break;
+        case 4: mixed ? mixed_batch_pack_ns4(kind, mode, c, dst) : exact_batch_pack_ns4(kind, mode, c, dst); break;
+        default: break;
+    }
+}
+int batch_launch(int ns, bool mixed, int kind, int mode, const void* dargs, const int* dbpref, int nmem, int nblocks,
+                 cudaStream_t s) {
+    if (mixed) { FHD_DISPATCH(ns, mixed_batch_launch_ns, kind, mode, dargs, dbpref, nmem, nblocks, s) }
+    FHD_DISPATCH(ns, exact_batch_launch_ns, kind, mode, dargs, dbpref, nmem, nblocks, s)
+}
+
+int ghost_desc_size() { return (int)sizeof(GhostFab); }
+
+int64_t ghost_pack(const fhd_fab& f, int c0, int nc, const int ncell[3], void* dst) {
+    GhostFab g;
+    g.p = static_cast<double*>(f.data);
+    g.lo = f.lo[0];
+    const int gw = -f.lo[0];
+    int64_t ext[3];
+    for (int d = 0; d < 3; ++d) {
+        g.vhi[d] = ncell[d] - 1 + f.nodal[d];
+        ext[d] = f.hi[d] - f.lo[d] + 1;
+        g.n[d] = ncell[d];
+    }
+    g.sy = ext[0];
+    g.sz = ext[0] * ext[1];
+    g.sn = ext[0] * ext[1] * ext[2];
+    g.c0 = c0;
+    g.nc = nc;
+    const int64_t VY = g.vhi[1] + 1, VZ = g.vhi[2] + 1;
+    g.npts = gw == 0 ? 0 : 2 * gw * ext[0] * ext[1] + 2 * gw * ext[0] * VZ + 2 * gw * VY * VZ;
+    memcpy(dst, &g, sizeof(g));
+    return g.npts * g.nc;
+}
+
+int ghost_launch_b(const void* dfabs, const int* dbpref, int nfab, int nblocks, cudaStream_t s) {
+    if (nblocks <= 0 || nfab <= 0) return FHD_OK;
+    k_ghosts_b<<<nblocks, 256, 0, s>>>(static_cast<const GhostFab*>(dfabs), dbpref, nfab);
+    return cuda_rc(cudaGetLastError());
+}
+
+int steps_inc(uint64_t* steps, int n, cudaStream_t s) {
+    if (n <= 0) return FHD_OK;
+    k_steps_inc<<<(n + 255) / 256, 256, 0, s>>>(steps, n);
+    return cuda_rc(cudaGetLastError());
+}
+
 int fill_ghosts(const GhostReq* reqs, int n, const int ncell[3], cudaStream_t s) {
     for (int base = 0; base < n; base += 16) {
         GhostArgs a;
@@ -78,6 +163,7 @@ int fill_ghosts(const GhostReq* reqs, int n, const int ncell[3], cudaStream_t s)
             g.sn = ext[0] * ext[1] * ext[2];
             g.c0 = reqs[q].c0;
             g.nc = reqs[q].nc;
+            for (int d = 0; d < 3; ++d) g.n[d] = ncell[d];
             const int64_t VX = g.vhi[0] + 1, VY = g.vhi[1] + 1, VZ = g.vhi[2] + 1;
             g.npts = 2 * gw * ext[0] * ext[1] + 2 * gw * ext[0] * VZ + 2 * gw * VY * VZ;
             (void)VX;

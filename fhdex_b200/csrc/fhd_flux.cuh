@@ -53,13 +53,13 @@ struct Noise {
     FHD_D void gauss2(const DevParams& P, uint32_t fid0, int i, int j, int k, double sd, double& w0,
                       double& w1) const {
         float z[4];
-        normal_quad(P.key0, P.key1, canon(P, i, j, k), fid0 >> 1, P.step, z);
+        normal_quad(P.key0, P.key1, canon(P, i, j, k), fid0 >> 1, noise_step(P), z);
         w0 = comb(0.0 + sd * (double)z[0], 0.0 + sd * (double)z[1]);
         w1 = comb(0.0 + sd * (double)z[2], 0.0 + sd * (double)z[3]);
     }
     FHD_D double gauss1(const DevParams& P, uint32_t fid, int i, int j, int k, double sd) const {
         float za, zb;
-        normal_pair(P.key0, P.key1, canon(P, i, j, k), fid, P.step, za, zb);
+        normal_pair(P.key0, P.key1, canon(P, i, j, k), fid, noise_step(P), za, zb);
         return comb(0.0 + sd * (double)za, 0.0 + sd * (double)zb);
     }
     template <int NC>

@@ -62,6 +62,17 @@ int noise_fill(const DevParams& P, const fhd_fab& f, int c0, int nc, double mean
                cudaStream_t s);
 int init_uniform(const fhd_fab& cu, int ns, double rho0, double rhoE, const double* rhoY, cudaStream_t s);
 
+// batched launches (kinds: 0 cellprep, 1 stresses, 2-4 faces, 5 update, 6 conversion)
+size_t batch_args_size(int ns, bool mixed, int kind, int mode);
+void batch_pack(int ns, bool mixed, int kind, int mode, const StageCall& c, void* dst);
+int batch_launch(int ns, bool mixed, int kind, int mode, const void* dargs, const int* dbpref, int nmem, int nblocks,
+                 cudaStream_t s);
+struct GhostFabDesc;  // opaque to the host code
+int ghost_desc_size();
+int64_t ghost_pack(const fhd_fab& f, int c0, int nc, const int ncell[3], void* dst);  // returns work items
+int ghost_launch_b(const void* dfabs, const int* dbpref, int nfab, int nblocks, cudaStream_t s);
+int steps_inc(uint64_t* steps, int n, cudaStream_t s);
+
 int num_tiles();
 const char* tile_name(int t);
 

@@ -14,6 +14,29 @@
 namespace fhd {
 
 #if defined(FHD_MIXED) && FHD_MIXED
+#define FHD_R float
+#define FHD_PFX mixed
+#else
+#define FHD_R double
+#define FHD_PFX exact
+#endif
+
+// batched launches of this (species count, precision); mode is NM_PHILOX or NM_OFF
+size_t FHD_CAT(FHD_CAT(FHD_PFX, _batch_args_size_ns), FHD_NS)(int kind, int mode) {
+    return mode == NM_OFF ? batch_args_size_t<FHD_NS, FHD_R, NZ_OFF>(kind)
+                          : batch_args_size_t<FHD_NS, FHD_R, NZ_PHILOX>(kind);
+}
+void FHD_CAT(FHD_CAT(FHD_PFX, _batch_pack_ns), FHD_NS)(int kind, int mode, const StageCall& c, void* dst) {
+    if (mode == NM_OFF) batch_pack_t<FHD_NS, FHD_R, NZ_OFF>(kind, c, dst);
+    else batch_pack_t<FHD_NS, FHD_R, NZ_PHILOX>(kind, c, dst);
+}
+int FHD_CAT(FHD_CAT(FHD_PFX, _batch_launch_ns), FHD_NS)(int kind, int mode, const void* dargs, const int* dbpref,
+                                                       int nmem, int nblocks, cudaStream_t s) {
+    return mode == NM_OFF ? batch_launch_t<FHD_NS, FHD_R, NZ_OFF>(kind, dargs, dbpref, nmem, nblocks, s)
+                          : batch_launch_t<FHD_NS, FHD_R, NZ_PHILOX>(kind, dargs, dbpref, nmem, nblocks, s);
+}
+
+#if defined(FHD_MIXED) && FHD_MIXED
 int FHD_CAT(mixed_cellprep_ns, FHD_NS)(const StageCall& c) { return launch_cellprep<FHD_NS, float>(c); }
 int FHD_CAT(mixed_stage_ns, FHD_NS)(const StageCall& c, int part) { return launch_stage_part<FHD_NS, float>(c, part); }
 #else

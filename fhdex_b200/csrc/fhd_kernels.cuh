@@ -37,48 +37,54 @@ struct PrepArgs {
 };
 
 template <int NS, class R>
-__global__ void __launch_bounds__(128) k_cellprep(PrepArgs<NS, R> a) {
+FHD_D int cellprep_count(const PrepArgs<NS, R>& a) { return (a.P.n[0] + 3) * (a.P.n[1] + 3) * (a.P.n[2] + 3); }
+
+template <int NS, class R>
+FHD_D void cellprep_point(const PrepArgs<NS, R>& a, int q) {
     const DevParams& P = a.P;
-    const int nx = P.n[0] + 3, ny = P.n[1] + 3, nz = P.n[2] + 3;
-    const int tot = nx * ny * nz;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) {
-        const int i = q % nx - 1;
-        const int j = (q / nx) % ny - 1;
-        const int k = q / (nx * ny) - 1;
-        const double rho = a.cons(i, j, k, 0);
-        // low face velocities (conservedPrimitiveConversionsStag.cpp:61-67)
-        a.vel[0](i, j, k) = 2 * a.mom[0](i, j, k) / (rho + a.cons(i - 1, j, k, 0));
-        a.vel[1](i, j, k) = 2 * a.mom[1](i, j, k) / (rho + a.cons(i, j - 1, k, 0));
-        a.vel[2](i, j, k) = 2 * a.mom[2](i, j, k) / (rho + a.cons(i, j, k - 1, 0));
-        if (i > P.n[0] || j > P.n[1] || k > P.n[2]) continue;
-        double rY[NS];
+    const int nx = P.n[0] + 3, ny = P.n[1] + 3;
+    const int i = q % nx - 1;
+    const int j = (q / nx) % ny - 1;
+    const int k = q / (nx * ny) - 1;
+    const double rho = a.cons(i, j, k, 0);
+    // low face velocities (conservedPrimitiveConversionsStag.cpp:61-67)
+    a.vel[0](i, j, k) = 2 * a.mom[0](i, j, k) / (rho + a.cons(i - 1, j, k, 0));
+    a.vel[1](i, j, k) = 2 * a.mom[1](i, j, k) / (rho + a.cons(i, j - 1, k, 0));
+    a.vel[2](i, j, k) = 2 * a.mom[2](i, j, k) / (rho + a.cons(i, j, k - 1, 0));
+    if (i > P.n[0] || j > P.n[1] || k > P.n[2]) return;
+    double rY[NS];
 #pragma unroll
-        for (int n = 0; n < NS; ++n) rY[n] = a.cons(i, j, k, 5 + n);
-        Prim<NS> q2;
-        const bool fin = cons_to_prim<NS>(P, rho, a.cons(i, j, k, 4), rY, a.mom[0](i, j, k), a.mom[0](i + 1, j, k),
-                                          a.mom[1](i, j, k), a.mom[1](i, j + 1, k), a.mom[2](i, j, k),
-                                          a.mom[2](i, j, k + 1), q2);
-        if (!fin) flag(a.status, ST_NONFINITE);
-        a.pr(i, j, k, 0) = q2.T;
-        a.pr(i, j, k, 1) = q2.p;
+    for (int n = 0; n < NS; ++n) rY[n] = a.cons(i, j, k, 5 + n);
+    Prim<NS> q2;
+    const bool fin = cons_to_prim<NS>(P, rho, a.cons(i, j, k, 4), rY, a.mom[0](i, j, k), a.mom[0](i + 1, j, k),
+                                      a.mom[1](i, j, k), a.mom[1](i, j + 1, k), a.mom[2](i, j, k),
+                                      a.mom[2](i, j, k + 1), q2);
+    if (!fin) flag(a.status, ST_NONFINITE);
+    a.pr(i, j, k, 0) = q2.T;
+    a.pr(i, j, k, 1) = q2.p;
 #pragma unroll
-        for (int n = 0; n < NS; ++n) {
-            a.pr(i, j, k, 2 + n) = q2.Y[n];
-            a.pr(i, j, k, 2 + NS + n) = q2.X[n];
-        }
-        R Yr[NS];
-#pragma unroll
-        for (int n = 0; n < NS; ++n) Yr[n] = R(q2.Y[n]);
-        Coeffs<NS, R> c;
-        if (!transport_gio<NS, R>(P, R(rho), R(q2.T), R(q2.p), Yr, c)) flag(a.status, ST_MASSFRAC);
-        a.eta(i, j, k) = c.eta;
-        a.kappa(i, j, k) = c.kappa;
-        a.zeta(i, j, k) = c.zeta;
-#pragma unroll
-        for (int n = 0; n < NS; ++n) a.chi(i, j, k, n) = c.chi[n];
-#pragma unroll
-        for (int n = 0; n < NS * NS; ++n) a.D(i, j, k, n) = c.D[n];
+    for (int n = 0; n < NS; ++n) {
+        a.pr(i, j, k, 2 + n) = q2.Y[n];
+        a.pr(i, j, k, 2 + NS + n) = q2.X[n];
     }
+    R Yr[NS];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) Yr[n] = R(q2.Y[n]);
+    Coeffs<NS, R> c;
+    if (!transport_gio<NS, R>(P, R(rho), R(q2.T), R(q2.p), Yr, c)) flag(a.status, ST_MASSFRAC);
+    a.eta(i, j, k) = c.eta;
+    a.kappa(i, j, k) = c.kappa;
+    a.zeta(i, j, k) = c.zeta;
+#pragma unroll
+    for (int n = 0; n < NS; ++n) a.chi(i, j, k, n) = c.chi[n];
+#pragma unroll
+    for (int n = 0; n < NS * NS; ++n) a.D(i, j, k, n) = c.D[n];
+}
+
+template <int NS, class R>
+__global__ void __launch_bounds__(128) k_cellprep(PrepArgs<NS, R> a) {
+    const int tot = cellprep_count(a);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) cellprep_point(a, q);
 }
 
 // ===================================================================================
@@ -110,11 +116,13 @@ struct StageArgs {
 
 // stresses on cells (grown by 1) and edges; one thread per point of [-1, n]^3
 template <int NS, class R, int NZ>
-__global__ void __launch_bounds__(256) k_taus(StageArgs<NS, R, NZ> a) {
+FHD_D int taus_count(const StageArgs<NS, R, NZ>& a) { return (a.P.n[0] + 2) * (a.P.n[1] + 2) * (a.P.n[2] + 2); }
+
+template <int NS, class R, int NZ>
+FHD_D void taus_point(const StageArgs<NS, R, NZ>& a, int q) {
     const DevParams& P = a.P;
-    const int nx = P.n[0] + 2, ny = P.n[1] + 2, nz = P.n[2] + 2;
-    const int tot = nx * ny * nz;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) {
+    const int nx = P.n[0] + 2, ny = P.n[1] + 2;
+    {
         const int i = q % nx - 1, j = (q / nx) % ny - 1, k = q / (nx * ny) - 1;
         const CellTaus<R> t = cell_taus<NS, R, NZ>(P, a.F, a.noise, i, j, k);
 #pragma unroll
@@ -123,7 +131,7 @@ __global__ void __launch_bounds__(256) k_taus(StageArgs<NS, R, NZ> a) {
             a.ct(i, j, k, 3 + d) = t.d[d];
             a.mc(i, j, k, d) = cen_total<NS, R>(P, a.F, t, d, i, j, k);
         }
-        if (i < 0 || j < 0 || k < 0) continue;
+        if (i < 0 || j < 0 || k < 0) return;
         double we[3] = {0.0, 0.0, 0.0};
         if (NZ != NZ_OFF) a.noise.edge_all(P, i, j, k, we);
         const int hadv = P.advection_type >= 0;
@@ -155,6 +163,12 @@ __global__ void __launch_bounds__(256) k_taus(StageArgs<NS, R, NZ> a) {
     }
 }
 
+template <int NS, class R, int NZ>
+__global__ void __launch_bounds__(256) k_taus(StageArgs<NS, R, NZ> a) {
+    const int tot = taus_count(a);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) taus_point(a, q);
+}
+
 template <class R>
 struct GlobalTaus {
     Arr4<R> ct, et;
@@ -177,32 +191,43 @@ struct GlobalTaus {
 };
 
 // conservative fluxes of the faces of direction D; one thread per valid face.
-// MINB = minimum resident blocks requested from the register allocator (1: no cap).
+template <int NS, class R, int NZ, int D>
+FHD_D int faces_count(const StageArgs<NS, R, NZ>& a) {
+    return (a.P.n[0] + (D == 0)) * (a.P.n[1] + (D == 1)) * (a.P.n[2] + (D == 2));
+}
+
+template <int NS, class R, int NZ, int D>
+FHD_D void faces_point(const StageArgs<NS, R, NZ>& a, int q) {
+    const DevParams& P = a.P;
+    const int nx = P.n[0] + (D == 0), ny = P.n[1] + (D == 1);
+    const GlobalTaus<R> tg{a.ct, a.et};
+    const int i = q % nx, j = (q / nx) % ny, k = q / (nx * ny);
+    const FaceFlux<NS> f = face_flux<NS, R, NZ, D>(P, a.F, a.noise, tg, i, j, k);
+#pragma unroll
+    for (int c = 0; c < 2 + NS; ++c) a.ff[D](i, j, k, c) = f.cons[c];
+}
+
+// MINB = minimum resident blocks requested from the register allocator.
 template <int NS, class R, int NZ, int D, int BS, int MINB>
 __global__ void __launch_bounds__(BS, MINB) k_faces(StageArgs<NS, R, NZ> a) {
-    const DevParams& P = a.P;
-    const int nx = P.n[0] + (D == 0), ny = P.n[1] + (D == 1), nz = P.n[2] + (D == 2);
-    const int tot = nx * ny * nz;
-    const GlobalTaus<R> tg{a.ct, a.et};
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) {
-        const int i = q % nx, j = (q / nx) % ny, k = q / (nx * ny);
-        const FaceFlux<NS> f = face_flux<NS, R, NZ, D>(P, a.F, a.noise, tg, i, j, k);
-#pragma unroll
-        for (int c = 0; c < 2 + NS; ++c) a.ff[D](i, j, k, c) = f.cons[c];
-    }
+    const int tot = faces_count<NS, R, NZ, D>(a);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x)
+        faces_point<NS, R, NZ, D>(a, q);
 }
 
 // RK3 stage combination (timeStepStag.cpp:439-528, 771-861, 1106-1202): one thread
 // per point of [0, n]^3 updates the cell there (if valid) and the faces there
 template <int NS, class R, int NZ>
-__global__ void __launch_bounds__(256) k_update(StageArgs<NS, R, NZ> a) {
+FHD_D int update_count(const StageArgs<NS, R, NZ>& a) { return (a.P.n[0] + 1) * (a.P.n[1] + 1) * (a.P.n[2] + 1); }
+
+template <int NS, class R, int NZ>
+FHD_D void update_point(const StageArgs<NS, R, NZ>& a, int q) {
     const DevParams& P = a.P;
     const Fields<NS, R>& F = a.F;
-    const int nx = P.n[0] + 1, ny = P.n[1] + 1, nz = P.n[2] + 1;
-    const int tot = nx * ny * nz;
+    const int nx = P.n[0] + 1, ny = P.n[1] + 1;
     const double dt = P.dt;
     const int st = a.stage;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) {
+    {
         const int i = q % nx, j = (q / nx) % ny, k = q / (nx * ny);
         const bool cell = i < P.n[0] && j < P.n[1] && k < P.n[2];
         if (cell) {
@@ -267,6 +292,12 @@ __global__ void __launch_bounds__(256) k_update(StageArgs<NS, R, NZ> a) {
     }
 }
 
+template <int NS, class R, int NZ>
+__global__ void __launch_bounds__(256) k_update(StageArgs<NS, R, NZ> a) {
+    const int tot = update_count(a);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) update_point(a, q);
+}
+
 // ===================================================================================
 // conservedToPrimitiveStag on valid cells/faces (conservedPrimitiveConversionsStag.cpp)
 // ===================================================================================
@@ -281,10 +312,12 @@ struct ConvArgs {
 };
 
 template <int NS>
-__global__ void __launch_bounds__(128) k_convert(ConvArgs<NS> a) {
+FHD_D int convert_count(const ConvArgs<NS>& a) { return a.P.n[0] * a.P.n[1] * a.P.n[2]; }
+
+template <int NS>
+FHD_D void convert_point(const ConvArgs<NS>& a, int q) {
     const DevParams& P = a.P;
-    const int tot = P.n[0] * P.n[1] * P.n[2];
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) {
+    {
         const int i = q % P.n[0];
         const int j = (q / P.n[0]) % P.n[1];
         const int k = q / (P.n[0] * P.n[1]);
@@ -329,6 +362,12 @@ __global__ void __launch_bounds__(128) k_convert(ConvArgs<NS> a) {
     }
 }
 
+template <int NS>
+__global__ void __launch_bounds__(128) k_convert(ConvArgs<NS> a) {
+    const int tot = convert_count(a);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) convert_point(a, q);
+}
+
 // ===================================================================================
 // periodic FillBoundary of up to 16 fabs in one launch
 // ===================================================================================
@@ -338,6 +377,7 @@ struct GhostFab {
     int64_t sy, sz, sn;
     int c0, nc;       // component range
     int64_t npts;     // ghost points of one component
+    int n[3];         // cells of the box (period)
 };
 struct GhostArgs {
     GhostFab f[16];
@@ -345,17 +385,13 @@ struct GhostArgs {
     int n[3];
 };
 
-static __global__ void __launch_bounds__(256) k_ghosts(GhostArgs a) {
-    const int fidx = blockIdx.y;
-    if (fidx >= a.nf) return;
-    const GhostFab& f = a.f[fidx];
+FHD_D void ghost_point(const GhostFab& f, int64_t q) {
     const int g = -f.lo;
     const int NX = f.vhi[0] + 1 + 2 * g, NY = f.vhi[1] + 1 + 2 * g;
     const int VX = f.vhi[0] + 1, VY = f.vhi[1] + 1, VZ = f.vhi[2] + 1;
     const int64_t zsl = (int64_t)2 * g * NX * NY;        // two z slabs (all x, y)
     const int64_t ysl = (int64_t)2 * g * NX * VZ;        // two y slabs (valid z)
-    const int64_t tot = (f.npts) * f.nc;
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < tot; q += (int64_t)gridDim.x * blockDim.x) {
+    {
         const int c = f.c0 + (int)(q / f.npts);
         int64_t r = q % f.npts;
         int i, j, k;
@@ -378,15 +414,24 @@ static __global__ void __launch_bounds__(256) k_ghosts(GhostArgs a) {
             i = ii < g ? ii - g : VX + (ii - g);
         }
         int si = i, sj = j, sk = k;
-        while (si < 0) si += a.n[0];
-        while (si > f.vhi[0]) si -= a.n[0];
-        while (sj < 0) sj += a.n[1];
-        while (sj > f.vhi[1]) sj -= a.n[1];
-        while (sk < 0) sk += a.n[2];
-        while (sk > f.vhi[2]) sk -= a.n[2];
+        while (si < 0) si += f.n[0];
+        while (si > f.vhi[0]) si -= f.n[0];
+        while (sj < 0) sj += f.n[1];
+        while (sj > f.vhi[1]) sj -= f.n[1];
+        while (sk < 0) sk += f.n[2];
+        while (sk > f.vhi[2]) sk -= f.n[2];
         const int64_t base = (int64_t)c * f.sn;
         f.p[base + (i + g) + (j + g) * f.sy + (k + g) * f.sz] = f.p[base + (si + g) + (sj + g) * f.sy + (sk + g) * f.sz];
     }
+}
+
+static __global__ void __launch_bounds__(256) k_ghosts(GhostArgs a) {
+    const int fidx = blockIdx.y;
+    if (fidx >= a.nf) return;
+    const GhostFab& f = a.f[fidx];
+    const int64_t tot = f.npts * f.nc;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < tot; q += (int64_t)gridDim.x * blockDim.x)
+        ghost_point(f, q);
 }
 
 // OverrideSync: nodal point n_cells <- point 0 (per nodal direction)
@@ -586,6 +631,79 @@ static __global__ void k_init_uniform(InitArgs a) {
         p[4 * a.cu.sn] = a.rhoE;
         for (int s = 0; s < a.ns; ++s) p[(5 + s) * a.cu.sn] = a.rhoY[s];
     }
+}
+
+// ===================================================================================
+// batched launches: one launch covers the work items of every member of an
+// ensemble; block b belongs to the member m with bpref[m] <= b < bpref[m+1]
+// ===================================================================================
+FHD_D int member_of(const int* __restrict__ bpref, int nmem) {
+    int lo = 0, hi = nmem;
+    const int b = blockIdx.x;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (bpref[mid] <= b) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <int NS, class R>
+__global__ void __launch_bounds__(128) k_cellprep_b(const PrepArgs<NS, R>* __restrict__ args,
+                                                    const int* __restrict__ bpref, int nmem) {
+    const int m = member_of(bpref, nmem);
+    const PrepArgs<NS, R>& a = args[m];
+    const int q = (blockIdx.x - bpref[m]) * blockDim.x + threadIdx.x;
+    if (q < cellprep_count(a)) cellprep_point(a, q);
+}
+
+template <int NS, class R, int NZ>
+__global__ void __launch_bounds__(128) k_taus_b(const StageArgs<NS, R, NZ>* __restrict__ args,
+                                                const int* __restrict__ bpref, int nmem) {
+    const int m = member_of(bpref, nmem);
+    const StageArgs<NS, R, NZ>& a = args[m];
+    const int q = (blockIdx.x - bpref[m]) * blockDim.x + threadIdx.x;
+    if (q < taus_count(a)) taus_point(a, q);
+}
+
+template <int NS, class R, int NZ, int D>
+__global__ void __launch_bounds__(128, 8) k_faces_b(const StageArgs<NS, R, NZ>* __restrict__ args,
+                                                   const int* __restrict__ bpref, int nmem) {
+    const int m = member_of(bpref, nmem);
+    const StageArgs<NS, R, NZ>& a = args[m];
+    const int q = (blockIdx.x - bpref[m]) * blockDim.x + threadIdx.x;
+    if (q < faces_count<NS, R, NZ, D>(a)) faces_point<NS, R, NZ, D>(a, q);
+}
+
+template <int NS, class R, int NZ>
+__global__ void __launch_bounds__(128) k_update_b(const StageArgs<NS, R, NZ>* __restrict__ args,
+                                                  const int* __restrict__ bpref, int nmem) {
+    const int m = member_of(bpref, nmem);
+    const StageArgs<NS, R, NZ>& a = args[m];
+    const int q = (blockIdx.x - bpref[m]) * blockDim.x + threadIdx.x;
+    if (q < update_count(a)) update_point(a, q);
+}
+
+template <int NS>
+__global__ void __launch_bounds__(128) k_convert_b(const ConvArgs<NS>* __restrict__ args,
+                                                   const int* __restrict__ bpref, int nmem) {
+    const int m = member_of(bpref, nmem);
+    const ConvArgs<NS>& a = args[m];
+    const int q = (blockIdx.x - bpref[m]) * blockDim.x + threadIdx.x;
+    if (q < convert_count(a)) convert_point(a, q);
+}
+
+static __global__ void __launch_bounds__(256) k_ghosts_b(const GhostFab* __restrict__ fabs,
+                                                         const int* __restrict__ bpref, int nfab) {
+    const int m = member_of(bpref, nfab);
+    const GhostFab& f = fabs[m];
+    const int64_t q = (int64_t)(blockIdx.x - bpref[m]) * blockDim.x + threadIdx.x;
+    if (q < f.npts * f.nc) ghost_point(f, q);
+}
+
+static __global__ void k_steps_inc(uint64_t* steps, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) steps[i] += 1;
 }
 
 }  // namespace fhd

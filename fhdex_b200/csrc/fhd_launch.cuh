@@ -154,6 +154,81 @@ int launch_stage_part(const StageCall& c, int part) {
     }
 }
 
+// ---- batched launches ------------------------------------------------------------
+// kinds: 0 cellprep, 1 stresses, 2-4 face fluxes x/y/z, 5 update, 6 conversion.
+// For the conversion kind the StageCall carries prim in pr, cu in cons_o, mom in mom_o.
+template <int NS>
+ConvArgs<NS> make_conv_args(const StageCall& c) {
+    ConvArgs<NS> a;
+    a.P = c.P;
+    a.prim = view<double>(c.pr);
+    a.cons = view<double>(c.cons_o);
+    for (int d = 0; d < 3; ++d) {
+        a.vel[d] = view<double>(c.vel[d]);
+        a.mom[d] = view<const double>(c.mom_o[d]);
+    }
+    a.status = c.status;
+    return a;
+}
+
+template <int NS, class R>
+PrepArgs<NS, R> make_prep_args(const StageCall& c) {
+    PrepArgs<NS, R> a;
+    a.P = c.P;
+    a.cons = view<const double>(c.cons_s);
+    for (int d = 0; d < 3; ++d) {
+        a.mom[d] = view<const double>(c.mom_s[d]);
+        a.vel[d] = view<double>(c.vel[d]);
+    }
+    a.pr = view<double>(c.pr, c.pT);
+    a.eta = view<R>(c.eta);
+    a.zeta = view<R>(c.zeta);
+    a.kappa = view<R>(c.kappa);
+    a.chi = view<R>(c.chi);
+    a.D = view<R>(c.D);
+    a.status = c.status;
+    return a;
+}
+
+template <int NS, class R, int NZ>
+size_t batch_args_size_t(int kind) {
+    if (kind == 0) return sizeof(PrepArgs<NS, R>);
+    if (kind == 6) return sizeof(ConvArgs<NS>);
+    return sizeof(StageArgs<NS, R, NZ>);
+}
+
+template <int NS, class R, int NZ>
+void batch_pack_t(int kind, const StageCall& c, void* dst) {
+    if (kind == 0) {
+        const PrepArgs<NS, R> a = make_prep_args<NS, R>(c);
+        memcpy(dst, &a, sizeof(a));
+    } else if (kind == 6) {
+        const ConvArgs<NS> a = make_conv_args<NS>(c);
+        memcpy(dst, &a, sizeof(a));
+    } else {
+        const StageArgs<NS, R, NZ> a = make_stage_args<NS, R, NZ>(c);
+        memcpy(dst, &a, sizeof(a));
+    }
+}
+
+template <int NS, class R, int NZ>
+int batch_launch_t(int kind, const void* dargs, const int* dbpref, int nmem, int nblocks, cudaStream_t s) {
+    if (nblocks <= 0 || nmem <= 0) return FHD_OK;
+    using SA = StageArgs<NS, R, NZ>;
+    const SA* sa = static_cast<const SA*>(dargs);
+    switch (kind) {
+        case 0: k_cellprep_b<NS, R><<<nblocks, 128, 0, s>>>(static_cast<const PrepArgs<NS, R>*>(dargs), dbpref, nmem); break;
+        case 1: k_taus_b<NS, R, NZ><<<nblocks, 128, 0, s>>>(sa, dbpref, nmem); break;
+        case 2: k_faces_b<NS, R, NZ, 0><<<nblocks, 128, 0, s>>>(sa, dbpref, nmem); break;
+        case 3: k_faces_b<NS, R, NZ, 1><<<nblocks, 128, 0, s>>>(sa, dbpref, nmem); break;
+        case 4: k_faces_b<NS, R, NZ, 2><<<nblocks, 128, 0, s>>>(sa, dbpref, nmem); break;
+        case 5: k_update_b<NS, R, NZ><<<nblocks, 128, 0, s>>>(sa, dbpref, nmem); break;
+        case 6: k_convert_b<NS><<<nblocks, 128, 0, s>>>(static_cast<const ConvArgs<NS>*>(dargs), dbpref, nmem); break;
+        default: return FHD_ERR_BAD_ARG;
+    }
+    return cuda_rc(cudaGetLastError());
+}
+
 #define FHD_NS_SWITCH(ns, CALL) \
     switch (ns) {                \
         case 1: return CALL(1);  \

@@ -224,6 +224,33 @@ int fhd_rk3_step_stag_host(fhd_ctx* ctx, fhd_fab cu, const fhd_fab mom[3], fhd_f
 int fhd_profile(fhd_ctx* ctx, int enable);
 int fhd_profile_read(fhd_ctx* ctx, double* ms, int64_t* launches);
 
+/* ---- ensembles and served runs (no reference counterpart: the reference runs one
+ * simulation per process) ------------------------------------------------------
+ * A batch advances many independent runs of one species count and precision
+ * together: each kernel of the step is launched once for all members, and one
+ * step is replayed from a captured CUDA graph.  Members keep their own box size,
+ * gas state, dt, seed (Philox key) and step counter, and get exactly the result
+ * they would get alone through fhd_rk3_step_stag with in-kernel noise.  The
+ * caller owns each member's cu/mom/prim/vel device fabs; the batch owns the
+ * members' stage scratch (stream-ordered allocations). */
+typedef struct fhd_batch fhd_batch;
+int fhd_batch_create(fhd_batch** batch, int nspecies, int precision, int device);
+int fhd_batch_destroy(fhd_batch* batch);
+int fhd_batch_set_stream(fhd_batch* batch, void* stream);
+/* init == NULL: the fabs already hold a converted, ghost-filled state; else
+ * init = {rho0, T_init, rhobar[0..nspecies-1]} initialises the uniform rest state
+ * (InitConsVarStag prob_type 1 + conversion + FillBoundary). */
+int fhd_batch_add(fhd_batch* batch, const fhd_params* params, fhd_fab cu, const fhd_fab mom[3],
+                  fhd_fab prim, const fhd_fab vel[3], double dt, int64_t first_step,
+                  const double* init, int* member);
+int fhd_batch_remove(fhd_batch* batch, int member);
+/* Advances every member by nsteps RK3 steps (use_graph: replay a captured graph). */
+int fhd_batch_step(fhd_batch* batch, int nsteps, int use_graph);
+int fhd_batch_size(const fhd_batch* batch);
+/* Latched device status of one member (waits for the stream). */
+int fhd_batch_member_status(fhd_batch* batch, int member);
+int fhd_batch_synchronize(fhd_batch* batch);
+
 /* RK3stepStag without any device allocation, for callers that cannot allocate:
  * code whose device memory is owned by an arena that a stray cudaMalloc would
  * fail or fragment, framework callbacks that forbid allocation on their hot

@@ -1,0 +1,109 @@
+"""Batched ensembles / served runs: every member's result equals the same run
+alone, also when members join and leave between steps (continuous batching).
+FP64: bit for bit (the batched kernels run the same point functions in the same
+order with the member's own Philox key and step counter).  Mixed precision: the
+FP32 units are built with FMA contraction, which the compiler may apply
+differently in the batched and the single-run kernels, so members agree with the
+run alone within a norm-relative error of MIXED_TOL per field."""
+import pytest
+import torch
+
+from fhdex_b200.batch import Batch
+from fhdex_b200.context import Context
+from fhdex_b200.params import argon, mixture4, stable_dt
+from fhdex_b200.state import StagState
+
+pytestmark = pytest.mark.gpu
+
+
+def alone(p, dt, steps, first=0):
+    st = StagState(p, "cuda", aux=False)
+    ctx = Context(p)
+    ctx.init_state(st)
+    for s in range(first, first + steps):
+        ctx.rk3_step(st, dt, s, aux=False)
+    torch.cuda.synchronize()
+    ctx.close()
+    return st
+
+
+MIXED_TOL = 1e-6
+
+
+def same(a, b, tol=0.0):
+    """names of the fields of a that differ from b (tol = 0: bitwise)."""
+    from tests.helpers import max_rel
+    bad = []
+    for n, m in a.named().items():
+        r = b.named()[n]
+        if tol == 0.0:
+            if not torch.equal(m.arr, r.arr):
+                bad.append(n)
+        else:
+            for c in range(m.ncomp):
+                e = max_rel(m.valid(c), r.valid(c))
+                if not e <= tol:
+                    bad.append((n, c, e))
+    return bad
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_members_match_runs_alone(precision):
+    ps = [argon(16, dx=8e-6, T_init=260.0, rho0=1.2e-3, seed=11, precision=precision),
+          argon((20, 12, 8), dx=8e-6, T_init=330.0, rho0=2.5e-3, seed=12, precision=precision),
+          argon(12, dx=8e-6, T_init=300.0, rho0=1.78e-3, seed=13, precision=precision)]
+    dts = [stable_dt(p) for p in ps]
+    b = Batch(2, precision)
+    sts = [StagState(p, "cuda", aux=False) for p in ps]
+    ids = [b.add(p, st, dt) for p, st, dt in zip(ps, sts, dts)]
+    b.step(3, graph=True)
+    b.synchronize()
+    for p, st, dt, mid in zip(ps, sts, dts, ids):
+        assert b.status(mid) == 0
+        ref = alone(p, dt, 3)
+        tol = 0.0 if precision == 0 else MIXED_TOL
+        assert not same(st, ref, tol), (p.n_cells, same(st, ref, tol))
+    b.close()
+
+
+def test_members_join_and_leave_between_steps():
+    pa = argon(16, dx=8e-6, seed=21)
+    pb = mixture4(12, dx=8e-6, seed=22)
+    pc = argon(10, dx=8e-6, seed=23, T_init=290.0)
+    # two classes: ns=2 batch (a, c) and ns=4 batch (b)
+    b2 = Batch(2, 0)
+    b4 = Batch(4, 0)
+    sa, sb, sc = (StagState(p, "cuda", aux=False) for p in (pa, pb, pc))
+    da, db, dc = stable_dt(pa), stable_dt(pb), stable_dt(pc)
+    ia = b2.add(pa, sa, da)
+    b2.step(2)
+    ib = b4.add(pb, sb, db)
+    ic = b2.add(pc, sc, dc)          # joins while a is running
+    b2.step(2)
+    b4.step(2)
+    b2.remove(ia)                    # a leaves after 4 steps
+    b2.step(1, graph=False)
+    b2.synchronize()
+    b4.synchronize()
+    assert not same(sa, alone(pa, da, 4))
+    assert not same(sb, alone(pb, db, 2))
+    assert not same(sc, alone(pc, dc, 3))
+    b2.close()
+    b4.close()
+
+
+def test_server_results_match_runs_alone():
+    """Requests served with continuous batching (joining and leaving batches of
+    both precisions and species counts at different times) end in exactly the
+    state they reach when run alone."""
+    from fhdex_b200.serve import Server, poisson_trace, request_params
+    trace = poisson_trace(6, rate=400.0, seed=3, edge=(8, 14), steps=(3, 9))
+    srv = Server(chunk=2)
+    reqs, finals, cell_updates, elapsed = srv.run(trace, keep_states=True)
+    assert all(r.status == 0 for r in reqs)
+    for r in reqs:
+        p = request_params(r)
+        ref = alone(p, stable_dt(p), r.steps)
+        tol = 0.0 if p.precision == 0 else MIXED_TOL
+        assert not same(finals[r.rid], ref, tol), (r, same(finals[r.rid], ref, tol))
+    srv.close()
