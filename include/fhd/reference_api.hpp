@@ -1,0 +1,391 @@
+// reference_api.hpp — FHDeX's compressible staggered-grid interface with the
+// reference's own function names and argument lists, over the single-box types
+// of fhd/amrex_compat.hpp, forwarding to the C ABI of fhd_capi.h.
+//
+// A driver written against the reference (main_driver.cpp) keeps its calls:
+//
+//   RK3stepStag(cu, cumom, prim, vel, source, eta, zeta, kappa, chi, D,
+//               faceflux, edgeflux_x, edgeflux_y, edgeflux_z, cenflux,
+//               ranchem, geom, dt, step, turbforce);
+//
+// Reference declarations mirrored here (paths within the FHDeX tree):
+//   conservedToPrimitiveStag   src_compressible_stag/compressible_functions_stag.H:69-70
+//   InitConsVarStag            src_compressible_stag/compressible_functions_stag.H:72-74
+//   RK3stepStag                src_compressible_stag/compressible_functions_stag.H:113-125
+//   calculateFluxStag          src_compressible_stag/compressible_functions_stag.H:127-143
+//   calculateTransportCoeffs   src_compressible/compressible_functions.H:37-39
+//   MultiFabFillRandom,
+//   MultiFabFillRandomNormal   src_rng/rng_functions.H:13-22
+//
+// As in the reference, physics parameters are process globals in namespaces
+// `common` and `compressible` (src_common/common_namespace.H,
+// src_compressible/compressible_namespace.H) with the reference's names and
+// defaults (common_functions.cpp:332-550, compressible_functions.cpp:15-88).
+// The first call builds one fhd_ctx from them on `fhd::ref::device`; after
+// changing a global call fhd::ref::reinitialize().
+//
+// Errors: the reference calls amrex::Abort (process exit) on a bad mass
+// fraction (transCoeffs.cpp:45-46) and on bad input.  Here every failure goes
+// to fhd::ref::abort_handler, which by default prints the message and calls
+// std::abort(); a caller may install a handler that throws instead.  Device
+// physics faults are latched by the kernels; RK3stepStag and
+// calculateTransportCoeffs read the status word after their work (one stream
+// synchronisation) and report a latched fault the same way.
+//
+// MultiFabs must live in the device arena, except that RK3stepStag also accepts
+// host/pinned cu, cumom, prim and vel (a CPU build's MultiFabs): it then
+// copies them through the context's device buffers and leaves the by-product
+// MultiFabs (coefficients and fluxes) untouched.
+#ifndef FHD_REFERENCE_API_HPP
+#define FHD_REFERENCE_API_HPP
+
+#include <cstdio>
+#include <cstdlib>
+#include <string>
+
+#include "amrex_compat.hpp"
+
+#ifndef MAX_SPECIES
+#define MAX_SPECIES FHD_MAX_SPECIES
+#endif
+
+// ---- global parameters (reference names, reference defaults) -----------------
+namespace common {
+using fhd::amrex_compat::GpuArray;
+using fhd::amrex_compat::Real;
+inline GpuArray<Real, 3> prob_lo{{0.0, 0.0, 0.0}};
+inline GpuArray<Real, 3> prob_hi{{1.0, 1.0, 1.0}};
+inline GpuArray<int, 3> n_cells{{0, 0, 0}};
+inline GpuArray<Real, 3> grav{{0.0, 0.0, 0.0}};
+inline int nspecies = 2;
+inline GpuArray<Real, MAX_SPECIES> molmass{{1, 1, 1, 1, 1, 1, 1, 1}};
+inline GpuArray<Real, MAX_SPECIES> rhobar{{1, 1, 1, 1, 1, 1, 1, 1}};
+inline Real rho0 = 1.0;
+inline GpuArray<Real, MAX_SPECIES> diameter{{1, 1, 1, 1, 1, 1, 1, 1}};
+inline GpuArray<Real, MAX_SPECIES> dof{{0, 0, 0, 0, 0, 0, 0, 0}};          // no default: set it
+inline GpuArray<Real, MAX_SPECIES> e0{{0, 0, 0, 0, 0, 0, 0, 0}};
+inline GpuArray<Real, MAX_SPECIES> hcv{{-1, -1, -1, -1, -1, -1, -1, -1}};  // < 0: GetHcGas derives it
+inline GpuArray<Real, MAX_SPECIES> hcp{{-1, -1, -1, -1, -1, -1, -1, -1}};
+inline Real k_B = 1.38064852e-16;
+inline Real Runiv = 8.314462175e7;
+inline GpuArray<Real, MAX_SPECIES> T_init{{1, 1, 1, 1, 1, 1, 1, 1}};
+inline int algorithm_type = 0;  // the staggered decks set 2, the only value the step accepts
+inline int advection_type = 0;
+inline int seed = 0;
+inline int visc_type = 1;
+inline int stoch_stress_form = 1;
+}  // namespace common
+
+namespace compressible {
+using fhd::amrex_compat::Real;
+inline int transport_type = 1;
+inline Real zeta_ratio = -1.0;
+}  // namespace compressible
+
+namespace fhd {
+namespace ref {
+
+using amrex_compat::Arena;
+using amrex_compat::Geometry;
+using amrex_compat::MultiFab;
+using amrex_compat::Real;
+using amrex_compat::Vector;
+
+// Precision of the step (FHD_PREC_FP64 or FHD_PREC_MIXED); not a reference
+// parameter.
+inline int precision = FHD_PREC_FP64;
+// CUDA device of the process-wide context.
+inline int device = 0;
+// Stream the context enqueues on (cudaStream_t; nullptr = legacy default).
+inline void* stream = nullptr;
+
+[[noreturn]] inline void default_abort(const char* msg) {
+    std::fprintf(stderr, "fhd::ref abort: %s\n", msg);
+    std::fflush(stderr);
+    std::abort();
+}
+// Called on every failure; must not return normally (throw or exit).
+inline void (*abort_handler)(const char*) = default_abort;
+
+[[noreturn]] inline void fail(const std::string& where, int rc) {
+    const std::string m = where + ": " + fhd_strerror(rc);
+    abort_handler(m.c_str());
+    std::abort();  // a handler that returns still ends the call
+}
+
+inline fhd_params params_from_globals() {
+    fhd_params p;
+    std::memset(&p, 0, sizeof(p));
+    p.nspecies = common::nspecies;
+    for (int d = 0; d < 3; ++d) {
+        p.n_cells[d] = common::n_cells[d];
+        p.prob_lo[d] = common::prob_lo[d];
+        p.prob_hi[d] = common::prob_hi[d];
+        p.grav[d] = common::grav[d];
+    }
+    for (int s = 0; s < FHD_MAX_SPECIES; ++s) {
+        p.molmass[s] = common::molmass[s];
+        p.diameter[s] = common::diameter[s];
+        p.dof[s] = common::dof[s];
+        p.e0[s] = common::e0[s];
+        p.hcv[s] = common::hcv[s];
+        p.hcp[s] = common::hcp[s];
+    }
+    p.k_B = common::k_B;
+    p.Runiv = common::Runiv;
+    p.zeta_ratio = compressible::zeta_ratio;
+    p.algorithm_type = common::algorithm_type;
+    p.visc_type = common::visc_type;
+    p.advection_type = common::advection_type;
+    p.transport_type = compressible::transport_type;
+    p.stoch_stress_form = common::stoch_stress_form;
+    p.precision = precision;
+    p.seed = uint64_t(int64_t(common::seed));
+    return p;
+}
+
+struct Runtime {
+    fhd_ctx* ctx = nullptr;
+    uint64_t fill_calls = 0;  // stream ids of successive MultiFabFillRandom* calls
+    ~Runtime() {
+        if (ctx) fhd_destroy(ctx);
+    }
+};
+inline Runtime& runtime() {
+    static Runtime r;
+    return r;
+}
+
+inline void finalize() {
+    Runtime& r = runtime();
+    if (r.ctx) fhd_destroy(r.ctx);
+    r.ctx = nullptr;
+}
+
+// The process-wide context, created from the globals on first use.
+inline fhd_ctx* context() {
+    Runtime& r = runtime();
+    if (!r.ctx) {
+        const fhd_params p = params_from_globals();
+        int rc = fhd_create(&r.ctx, &p, device);
+        if (rc != FHD_OK) {
+            r.ctx = nullptr;
+            fail("fhd_create", rc);
+        }
+        rc = fhd_set_stream(r.ctx, stream);
+        if (rc != FHD_OK) fail("fhd_set_stream", rc);
+    }
+    return r.ctx;
+}
+
+inline void reinitialize() {
+    finalize();
+    context();
+}
+
+inline void check(int rc, const char* where) {
+    if (rc != FHD_OK) fail(where, rc);
+}
+
+inline void require_device(const MultiFab& mf, const char* where) {
+    if (!mf.ok() || mf.arena() != Arena::Device)
+        fail(std::string(where) + ": MultiFab must be allocated in the device arena", FHD_ERR_BAD_ARG);
+}
+
+template <size_t N>
+inline void fabs_of(const std::array<MultiFab, N>& a, fhd_fab* out) {
+    for (size_t d = 0; d < N; ++d) out[d] = a[d].fab();
+}
+
+// Whether every MultiFab of `a` was allocated (by-product arrays are optional).
+template <size_t N>
+inline bool all_ok(const std::array<MultiFab, N>& a) {
+    for (const auto& m : a)
+        if (!m.ok()) return false;
+    return true;
+}
+
+}  // namespace ref
+}  // namespace fhd
+
+// Turbulence forcing object of the reference's RK3stepStag signature; only used
+// under -DTURB there and unused here.
+struct TurbForcingComp {};
+
+inline void fhd::amrex_compat::MultiFab::FillBoundary(const Periodicity&) {
+    fhd::ref::require_device(*this, "FillBoundary");
+    fhd::ref::check(fhd_fill_boundary(fhd::ref::context(), fab()), "FillBoundary");
+}
+inline void fhd::amrex_compat::MultiFab::OverrideSync(const Periodicity&) {
+    fhd::ref::require_device(*this, "OverrideSync");
+    fhd::ref::check(fhd_override_sync(fhd::ref::context(), fab()), "OverrideSync");
+}
+
+// ---- the reference's functions --------------------------------------------------
+
+// InitConsVarStag, prob_type 1 (uniform state at rest)
+// (compressible_functions_stag.cpp:36-56): rho0, T_init[0] and rhobar from the
+// globals.
+inline void InitConsVarStag(fhd::amrex_compat::MultiFab& cons,
+                            std::array<fhd::amrex_compat::MultiFab, 3>& momStag,
+                            const fhd::amrex_compat::Geometry& /*geom*/) {
+    using namespace fhd::ref;
+    require_device(cons, "InitConsVarStag");
+    for (auto& m : momStag) require_device(m, "InitConsVarStag");
+    fhd_fab mom[3];
+    fabs_of(momStag, mom);
+    check(fhd_init_cons_var_stag(context(), cons.fab(), mom, common::rho0, common::T_init[0],
+                                 common::rhobar.data()),
+          "InitConsVarStag");
+}
+
+// conservedToPrimitiveStag (conservedPrimitiveConversionsStag.cpp:5-144).
+inline void conservedToPrimitiveStag(fhd::amrex_compat::MultiFab& prim_in,
+                                     std::array<fhd::amrex_compat::MultiFab, 3>& velStag_in,
+                                     fhd::amrex_compat::MultiFab& cons_in,
+                                     const std::array<fhd::amrex_compat::MultiFab, 3>& momStag_in) {
+    using namespace fhd::ref;
+    require_device(prim_in, "conservedToPrimitiveStag");
+    require_device(cons_in, "conservedToPrimitiveStag");
+    fhd_fab vel[3], mom[3];
+    fabs_of(velStag_in, vel);
+    fabs_of(momStag_in, mom);
+    check(fhd_conserved_to_primitive_stag(context(), prim_in.fab(), vel, cons_in.fab(), mom),
+          "conservedToPrimitiveStag");
+}
+
+// calculateTransportCoeffs (transCoeffs.cpp:7-90).  A bad mass fraction is
+// reported through abort_handler, where the reference aborts.
+inline void calculateTransportCoeffs(const fhd::amrex_compat::MultiFab& prim_in,
+                                     fhd::amrex_compat::MultiFab& eta_in,
+                                     fhd::amrex_compat::MultiFab& zeta_in,
+                                     fhd::amrex_compat::MultiFab& kappa_in,
+                                     fhd::amrex_compat::MultiFab& chi_in,
+                                     fhd::amrex_compat::MultiFab& Dij_in) {
+    using namespace fhd::ref;
+    require_device(prim_in, "calculateTransportCoeffs");
+    check(fhd_transport_coeffs(context(), prim_in.fab(), eta_in.fab(), zeta_in.fab(), kappa_in.fab(),
+                               chi_in.fab(), Dij_in.fab()),
+          "calculateTransportCoeffs");
+    check(fhd_status(context()), "calculateTransportCoeffs");
+}
+
+// calculateFluxStag (fluxStag.cpp:5-1868).  stochface/stochedge/stochcen are
+// the combined noise W = W_A + w_s W_B of the stage, as RK3stepStag passes
+// them; the reference reads only stochedge_x[0] (xy), stochedge_x[1] (xz) and
+// stochedge_y[1] (yz) (fluxStag.cpp:130-132), and so does this call.
+// stoch_weights is accepted for the signature and unused, as in the reference.
+inline void calculateFluxStag(
+    const fhd::amrex_compat::MultiFab& cons_in, const std::array<fhd::amrex_compat::MultiFab, 3>& momStag_in,
+    const fhd::amrex_compat::MultiFab& prim_in, const std::array<fhd::amrex_compat::MultiFab, 3>& velStag_in,
+    const fhd::amrex_compat::MultiFab& eta_in, const fhd::amrex_compat::MultiFab& zeta_in,
+    const fhd::amrex_compat::MultiFab& kappa_in, const fhd::amrex_compat::MultiFab& chi_in,
+    const fhd::amrex_compat::MultiFab& D_in, std::array<fhd::amrex_compat::MultiFab, 3>& faceflux_in,
+    std::array<fhd::amrex_compat::MultiFab, 2>& edgeflux_x_in, std::array<fhd::amrex_compat::MultiFab, 2>& edgeflux_y_in,
+    std::array<fhd::amrex_compat::MultiFab, 2>& edgeflux_z_in, std::array<fhd::amrex_compat::MultiFab, 3>& cenflux_in,
+    std::array<fhd::amrex_compat::MultiFab, 3>& stochface_in, std::array<fhd::amrex_compat::MultiFab, 2>& stochedge_x_in,
+    std::array<fhd::amrex_compat::MultiFab, 2>& stochedge_y_in,
+    std::array<fhd::amrex_compat::MultiFab, 2>& /*stochedge_z_in*/,
+    std::array<fhd::amrex_compat::MultiFab, 3>& stochcen_in, const fhd::amrex_compat::Geometry& /*geom*/,
+    const fhd::amrex_compat::Vector<fhd::amrex_compat::Real>& /*stoch_weights*/, const fhd::amrex_compat::Real dt) {
+    using namespace fhd::ref;
+    fhd_fab mom[3], vel[3], ff[3], ef[6], cf[3], sf[3], se[3], sc[3];
+    fabs_of(momStag_in, mom);
+    fabs_of(velStag_in, vel);
+    fabs_of(faceflux_in, ff);
+    ef[0] = edgeflux_x_in[0].fab();
+    ef[1] = edgeflux_x_in[1].fab();
+    ef[2] = edgeflux_y_in[0].fab();
+    ef[3] = edgeflux_y_in[1].fab();
+    ef[4] = edgeflux_z_in[0].fab();
+    ef[5] = edgeflux_z_in[1].fab();
+    fabs_of(cenflux_in, cf);
+    fabs_of(stochface_in, sf);
+    se[0] = stochedge_x_in[0].fab();
+    se[1] = stochedge_x_in[1].fab();
+    se[2] = stochedge_y_in[1].fab();
+    fabs_of(stochcen_in, sc);
+    check(fhd_flux_stag(context(), cons_in.fab(), mom, prim_in.fab(), vel, eta_in.fab(), zeta_in.fab(),
+                        kappa_in.fab(), chi_in.fab(), D_in.fab(), ff, ef, cf, sf, se, sc, dt),
+          "calculateFluxStag");
+}
+
+// RK3stepStag (timeStepStag.cpp:13-1245).  The white noise of step `step` is
+// Philox-4x32-10 keyed by common::seed, generated inside the step's kernels.
+// Coefficient and flux MultiFabs receive the stage-3 values when allocated;
+// leave them undefined (default-constructed) to skip them.  `source` is the
+// reference's chemistry source (zero unless chemistry is on; may be
+// undefined).  `ranchem` and `turbforce` are unused, as in the reference's
+// non-chemistry, non-TURB build.
+inline void RK3stepStag(fhd::amrex_compat::MultiFab& cu, std::array<fhd::amrex_compat::MultiFab, 3>& cumom,
+                        fhd::amrex_compat::MultiFab& prim, std::array<fhd::amrex_compat::MultiFab, 3>& facevel,
+                        fhd::amrex_compat::MultiFab& source, fhd::amrex_compat::MultiFab& eta,
+                        fhd::amrex_compat::MultiFab& zeta, fhd::amrex_compat::MultiFab& kappa,
+                        fhd::amrex_compat::MultiFab& chi, fhd::amrex_compat::MultiFab& D,
+                        std::array<fhd::amrex_compat::MultiFab, 3>& faceflux,
+                        std::array<fhd::amrex_compat::MultiFab, 2>& edgeflux_x,
+                        std::array<fhd::amrex_compat::MultiFab, 2>& edgeflux_y,
+                        std::array<fhd::amrex_compat::MultiFab, 2>& edgeflux_z,
+                        std::array<fhd::amrex_compat::MultiFab, 3>& cenflux,
+                        fhd::amrex_compat::MultiFab& /*ranchem*/, const fhd::amrex_compat::Geometry& /*geom*/,
+                        const fhd::amrex_compat::Real dt, const int step, TurbForcingComp& /*turbforce*/) {
+    using namespace fhd::ref;
+    fhd_ctx* ctx = context();
+    fhd_fab mom[3], vel[3];
+    fabs_of(cumom, mom);
+    fabs_of(facevel, vel);
+    if (cu.arena() != Arena::Device) {
+        // host MultiFabs: copies through the context's device buffers
+        int64_t h2d = 0, d2h = 0;
+        check(fhd_rk3_step_stag_host(ctx, cu.fab(), mom, prim.fab(), vel, nullptr, dt, step, &h2d, &d2h),
+              "RK3stepStag");
+    } else {
+        require_device(prim, "RK3stepStag");
+        fhd_fab ff[3], ef[6], cf[3];
+        const bool want_ff = all_ok(faceflux);
+        const bool want_ef = all_ok(edgeflux_x) && all_ok(edgeflux_y) && all_ok(edgeflux_z);
+        const bool want_cf = all_ok(cenflux);
+        if (want_ff) fabs_of(faceflux, ff);
+        if (want_ef) {
+            ef[0] = edgeflux_x[0].fab();
+            ef[1] = edgeflux_x[1].fab();
+            ef[2] = edgeflux_y[0].fab();
+            ef[3] = edgeflux_y[1].fab();
+            ef[4] = edgeflux_z[0].fab();
+            ef[5] = edgeflux_z[1].fab();
+        }
+        if (want_cf) fabs_of(cenflux, cf);
+        check(fhd_rk3_step_stag(ctx, cu.fab(), mom, prim.fab(), vel, source.fab(), eta.fab(), zeta.fab(),
+                                kappa.fab(), chi.fab(), D.fab(), want_ff ? ff : nullptr, want_ef ? ef : nullptr,
+                                want_cf ? cf : nullptr, nullptr, dt, step),
+              "RK3stepStag");
+    }
+    check(fhd_status(ctx), "RK3stepStag");
+}
+
+// MultiFabFillRandomNormal (MultiFabFillRandom.cpp:34-50): N(mean, variance) in
+// components scomp..scomp+ncomp-1 of the valid region, then OverrideSync and
+// FillBoundary when asked.  Successive calls draw independent Philox streams,
+// as successive calls on the reference's global generator draw new numbers.
+inline void MultiFabFillRandomNormal(fhd::amrex_compat::MultiFab& mf, const int& scomp, const int& ncomp,
+                                     const fhd::amrex_compat::Real& mean, const fhd::amrex_compat::Real& variance,
+                                     const fhd::amrex_compat::Geometry& /*geom*/, bool overridesync = true,
+                                     bool fillboundary = true) {
+    using namespace fhd::ref;
+    require_device(mf, "MultiFabFillRandomNormal");
+    const uint64_t id = ++runtime().fill_calls;
+    check(fhd_fill_random_normal(context(), mf.fab(), scomp, ncomp, mean, variance, overridesync ? 1 : 0,
+                                 fillboundary ? 1 : 0, id),
+          "MultiFabFillRandomNormal");
+}
+
+// MultiFabFillRandom (MultiFabFillRandom.cpp:5-31): N(0, variance) in one
+// component, then OverrideSync and FillBoundary (which leaves every ghost,
+// `ng` or not, the periodic image of a valid value on a periodic box).
+inline void MultiFabFillRandom(fhd::amrex_compat::MultiFab& mf, const int& comp,
+                               const fhd::amrex_compat::Real& variance, const fhd::amrex_compat::Geometry& geom,
+                               const int& /*ng*/ = 0) {
+    MultiFabFillRandomNormal(mf, comp, 1, 0.0, variance, geom, true, true);
+}
+
+#endif

@@ -1,0 +1,226 @@
+// Test driver for fhd/reference_api.hpp: the main_driver sequence of the
+// reference (main_driver.cpp: MultiFab set-up, InitConsVarStag,
+// conservedToPrimitiveStag, FillBoundary, calculateTransportCoeffs, then
+// RK3stepStag in the time loop) written against the reference's function
+// names, on an argon box (two identical species, the reference's parity form).
+//
+//   reference_driver shapes <n>
+//       print the Array4 bounds of every MultiFab kind (host arena, no GPU)
+//   reference_driver run <device|pinned> <n> <nsteps> <seed> <dt> <out.bin>
+//       run nsteps RK3 steps (steps 0..nsteps-1) and write cu, cumom[0..2],
+//       prim, vel[0..2] (whole buffers, ghosts included) to out.bin
+//   reference_driver massfrac <n>
+//       start from a state with a zero mass fraction: calculateTransportCoeffs
+//       must report it through the abort handler (exit code 3)
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "fhd/reference_api.hpp"
+
+using namespace fhd::amrex_compat;
+
+struct Caught : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+[[noreturn]] static void throwing_handler(const char* msg) { throw Caught(msg); }
+
+static void set_argon(int n, int seed) {
+    const double dx = 8e-6;
+    common::nspecies = 2;
+    for (int d = 0; d < 3; ++d) {
+        common::n_cells[d] = n;
+        common::prob_lo[d] = 0.0;
+        common::prob_hi[d] = n * dx;
+    }
+    for (int s = 0; s < 2; ++s) {
+        common::molmass[s] = 39.95;
+        common::diameter[s] = 3.66e-8;
+        common::dof[s] = 3.0;
+        common::rhobar[s] = 0.5;
+        common::T_init[s] = 273.0;
+    }
+    common::rho0 = 1.78e-3;
+    common::algorithm_type = 2;
+    common::visc_type = 2;
+    common::advection_type = 2;
+    common::stoch_stress_form = 1;
+    common::seed = seed;
+}
+
+struct State {
+    int ns, nvars, nprimvars, ngc = 2;
+    Geometry geom;
+    MultiFab cu, prim, source, eta, zeta, kappa, chi, D, ranchem;
+    std::array<MultiFab, 3> cumom, vel, faceflux, cenflux;
+    std::array<MultiFab, 2> edgeflux_x, edgeflux_y, edgeflux_z;
+
+    State(int n, Arena a, bool byproducts) {
+        ns = common::nspecies;
+        nvars = 5 + ns;
+        nprimvars = 6 + 2 * ns;
+        const Box dom(IntVect(0, 0, 0), IntVect(n - 1, n - 1, n - 1));
+        RealBox rb;
+        for (int d = 0; d < 3; ++d) {
+            rb.lo[d] = common::prob_lo[d];
+            rb.hi[d] = common::prob_hi[d];
+        }
+        geom = Geometry(dom, rb);
+        cu.define(dom, nvars, ngc, a);
+        prim.define(dom, nprimvars, ngc, a);
+        for (int d = 0; d < 3; ++d) {
+            cumom[d].define(convert(dom, face_nodal(d)), 1, ngc, a);
+            vel[d].define(convert(dom, face_nodal(d)), 1, ngc, a);
+        }
+        if (!byproducts) return;
+        source.define(dom, nprimvars, ngc, a);
+        eta.define(dom, 1, ngc, a);
+        zeta.define(dom, 1, ngc, a);
+        kappa.define(dom, 1, ngc, a);
+        chi.define(dom, ns, ngc, a);
+        D.define(dom, ns * ns, ngc, a);
+        for (int d = 0; d < 3; ++d) {
+            faceflux[d].define(convert(dom, face_nodal(d)), nvars + 4, 0, a);
+            cenflux[d].define(dom, 1, 1, a);
+        }
+        edgeflux_x[0].define(convert(dom, edge_nodal(0, 1)), 1, 0, a);
+        edgeflux_x[1].define(convert(dom, edge_nodal(0, 2)), 1, 0, a);
+        edgeflux_y[0].define(convert(dom, edge_nodal(0, 1)), 1, 0, a);
+        edgeflux_y[1].define(convert(dom, edge_nodal(1, 2)), 1, 0, a);
+        edgeflux_z[0].define(convert(dom, edge_nodal(0, 2)), 1, 0, a);
+        edgeflux_z[1].define(convert(dom, edge_nodal(1, 2)), 1, 0, a);
+    }
+
+    // main_driver's initialisation on device MultiFabs.
+    void init() {
+        InitConsVarStag(cu, cumom, geom);
+        conservedToPrimitiveStag(prim, vel, cu, cumom);
+        cu.FillBoundary(geom.periodicity());
+        prim.FillBoundary(geom.periodicity());
+        for (int d = 0; d < 3; ++d) {
+            cumom[d].FillBoundary(geom.periodicity());
+            vel[d].FillBoundary(geom.periodicity());
+        }
+        calculateTransportCoeffs(prim, eta, zeta, kappa, chi, D);
+    }
+};
+
+static void print_shape(const char* name, const MultiFab& m) {
+    const fhd_fab f = m.fab();
+    std::printf("%s %d %d %d %d %d %d %d %d %d %d\n", name, f.lo[0], f.lo[1], f.lo[2], f.hi[0], f.hi[1], f.hi[2],
+                f.ncomp, f.nodal[0], f.nodal[1], f.nodal[2]);
+}
+
+static int cmd_shapes(int n) {
+    set_argon(n, 1);
+    State s(n, Arena::Host, true);
+    print_shape("cu", s.cu);
+    print_shape("prim", s.prim);
+    for (int d = 0; d < 3; ++d) print_shape(("cumom" + std::to_string(d)).c_str(), s.cumom[d]);
+    for (int d = 0; d < 3; ++d) print_shape(("vel" + std::to_string(d)).c_str(), s.vel[d]);
+    print_shape("source", s.source);
+    print_shape("eta", s.eta);
+    print_shape("chi", s.chi);
+    print_shape("D", s.D);
+    for (int d = 0; d < 3; ++d) print_shape(("faceflux" + std::to_string(d)).c_str(), s.faceflux[d]);
+    print_shape("edgeflux_x0", s.edgeflux_x[0]);
+    print_shape("edgeflux_x1", s.edgeflux_x[1]);
+    print_shape("edgeflux_y1", s.edgeflux_y[1]);
+    for (int d = 0; d < 3; ++d) print_shape(("cenflux" + std::to_string(d)).c_str(), s.cenflux[d]);
+    // Array4 indexing agrees with the C-ABI layout (first and last element)
+    Array4<Real> a = s.cu.array();
+    a(-2, -2, -2, 0) = 1.0;
+    a(n + 1, n + 1, n + 1, s.nvars - 1) = 2.0;
+    const Real* p = s.cu.dataPtr();
+    std::printf("array4 %d %d\n", p[0] == 1.0 ? 1 : 0, p[s.cu.size() - 1] == 2.0 ? 1 : 0);
+    return 0;
+}
+
+static void write_all(FILE* f, const MultiFab& m) {
+    std::vector<Real> h;
+    m.copyToHost(h);
+    if (std::fwrite(h.data(), sizeof(Real), h.size(), f) != h.size()) throw std::runtime_error("short write");
+}
+
+static void step_all(State& s, double dt, int nsteps) {
+    TurbForcingComp turbforce;
+    for (int step = 0; step < nsteps; ++step)
+        RK3stepStag(s.cu, s.cumom, s.prim, s.vel, s.source, s.eta, s.zeta, s.kappa, s.chi, s.D, s.faceflux,
+                    s.edgeflux_x, s.edgeflux_y, s.edgeflux_z, s.cenflux, s.ranchem, s.geom, dt, step, turbforce);
+}
+
+static int cmd_run(const std::string& arena, int n, int nsteps, int seed, double dt, const char* out) {
+    set_argon(n, seed);
+    // initialise on the device, as the reference's GPU build does
+    State dev(n, Arena::Device, true);
+    dev.init();
+    if (arena == "device") {
+        step_all(dev, dt, nsteps);
+    } else {
+        // a CPU build's MultiFabs: state in pinned host memory, no by-products
+        State host(n, Arena::Pinned, false);
+        MultiFab::Copy(host.cu, dev.cu);
+        MultiFab::Copy(host.prim, dev.prim);
+        for (int d = 0; d < 3; ++d) {
+            MultiFab::Copy(host.cumom[d], dev.cumom[d]);
+            MultiFab::Copy(host.vel[d], dev.vel[d]);
+        }
+        step_all(host, dt, nsteps);
+        MultiFab::Copy(dev.cu, host.cu);
+        MultiFab::Copy(dev.prim, host.prim);
+        for (int d = 0; d < 3; ++d) {
+            MultiFab::Copy(dev.cumom[d], host.cumom[d]);
+            MultiFab::Copy(dev.vel[d], host.vel[d]);
+        }
+    }
+    FILE* f = std::fopen(out, "wb");
+    if (!f) return 2;
+    write_all(f, dev.cu);
+    for (int d = 0; d < 3; ++d) write_all(f, dev.cumom[d]);
+    write_all(f, dev.prim);
+    for (int d = 0; d < 3; ++d) write_all(f, dev.vel[d]);
+    std::fclose(f);
+    fhd::ref::finalize();
+    return 0;
+}
+
+static int cmd_massfrac(int n) {
+    set_argon(n, 1);
+    common::rhobar[0] = 1.0;  // species 2 absent: Y_2 = 0
+    common::rhobar[1] = 0.0;
+    fhd::ref::abort_handler = throwing_handler;
+    State s(n, Arena::Device, true);
+    try {
+        s.init();
+    } catch (const Caught& e) {
+        std::printf("caught: %s\n", e.what());
+        fhd::ref::finalize();
+        return 3;
+    }
+    fhd::ref::finalize();
+    return 0;
+}
+
+int main(int argc, char** argv) {
+    if (argc < 3) {
+        std::fprintf(stderr, "usage: %s shapes <n> | run <device|pinned> <n> <nsteps> <seed> <dt> <out> | massfrac <n>\n",
+                     argv[0]);
+        return 1;
+    }
+    const std::string cmd = argv[1];
+    try {
+        if (cmd == "shapes") return cmd_shapes(std::atoi(argv[2]));
+        if (cmd == "run" && argc == 8)
+            return cmd_run(argv[2], std::atoi(argv[3]), std::atoi(argv[4]), std::atoi(argv[5]),
+                           std::strtod(argv[6], nullptr), argv[7]);
+        if (cmd == "massfrac") return cmd_massfrac(std::atoi(argv[2]));
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "error: %s\n", e.what());
+        return 4;
+    }
+    std::fprintf(stderr, "bad arguments\n");
+    return 1;
+}

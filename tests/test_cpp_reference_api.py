@@ -1,0 +1,110 @@
+"""The C++ reference-signature layer (include/fhd/reference_api.hpp over
+include/fhd/amrex_compat.hpp): a driver that calls InitConsVarStag,
+conservedToPrimitiveStag, FillBoundary, calculateTransportCoeffs and
+RK3stepStag by the reference's names must give the same MultiFab shapes as the
+Python layer (CPU) and the same state, bit for bit, as the Python path through
+the C ABI (GPU), also when its MultiFabs live in pinned host memory."""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+import torch
+
+from fhdex_b200.params import argon, stable_dt
+from fhdex_b200.state import StagState
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIBDIR = os.path.join(ROOT, "fhdex_b200", "lib")
+CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+
+
+@pytest.fixture(scope="module")
+def driver(tmp_path_factory):
+    if not os.path.exists(os.path.join(LIBDIR, "libfhd_b200.so")):
+        pytest.skip("libfhd_b200.so not built")
+    cxx = shutil.which("g++")
+    if cxx is None:
+        pytest.skip("no g++")
+    exe = str(tmp_path_factory.mktemp("cpp") / "reference_driver")
+    cmd = [cxx, "-std=c++17", "-O2", "-Wall", "-Wextra", "-Werror", "-Wno-unused-parameter",
+           "-I", os.path.join(ROOT, "include"), "-I", os.path.join(CUDA, "include"),
+           os.path.join(ROOT, "tests", "cpp", "reference_driver.cpp"), "-o", exe,
+           "-L", LIBDIR, "-lfhd_b200", f"-Wl,-rpath,{LIBDIR}",
+           "-L", os.path.join(CUDA, "lib64"), "-lcudart", f"-Wl,-rpath,{os.path.join(CUDA, 'lib64')}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+def test_compat_shapes_match_python_layer(driver):
+    n = 6
+    r = subprocess.run([driver, "shapes", str(n)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stderr
+    rows = {}
+    for line in r.stdout.splitlines():
+        name, *v = line.split()
+        rows[name] = [int(x) for x in v]
+    assert rows.pop("array4") == [1, 1]
+    st = StagState(argon(n, dx=8e-6), "cpu")
+    names = {"cu": st.cu, "prim": st.prim, "source": st.source, "eta": st.eta, "chi": st.chi, "D": st.D,
+             "edgeflux_x0": st.edgeflux[0], "edgeflux_x1": st.edgeflux[1], "edgeflux_y1": st.edgeflux[3]}
+    for d in range(3):
+        names[f"cumom{d}"] = st.cumom[d]
+        names[f"vel{d}"] = st.vel[d]
+        names[f"faceflux{d}"] = st.faceflux[d]
+        names[f"cenflux{d}"] = st.cenflux[d]
+    for name, mf in names.items():
+        f = mf.fab()
+        want = list(f.lo) + list(f.hi) + [f.ncomp] + list(f.nodal)
+        assert rows[name] == want, (name, rows[name], want)
+
+
+def read_state(path, st):
+    """Split the driver's output into arrays shaped like the MultiFabs of `st`."""
+    raw = np.fromfile(path, dtype=np.float64)
+    off = 0
+    out = []
+    for m in [st.cu] + st.cumom + [st.prim] + st.vel:
+        k = m.arr.numel()
+        out.append(torch.from_numpy(raw[off:off + k].copy()).view(m.arr.shape))
+        off += k
+    assert off == raw.size
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("arena", ["device", "pinned"])
+def test_reference_driver_equals_c_abi_path(driver, tmp_path, arena):
+    from fhdex_b200.context import Context
+    n, nsteps, seed = 12, 3, 7
+    p = argon(n, dx=8e-6, seed=seed)
+    dt = stable_dt(p)
+    out = str(tmp_path / "state.bin")
+    r = subprocess.run([driver, "run", arena, str(n), str(nsteps), str(seed), repr(dt), out],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    ctx = Context(p)
+    st = StagState(p, "cuda", aux=False)
+    ctx.init_state(st)
+    for step in range(nsteps):
+        ctx.rk3_step(st, dt, step, aux=False)
+    torch.cuda.synchronize()
+    assert ctx.status() == 0
+    got = read_state(out, st)
+    names = ["cu", "cumom0", "cumom1", "cumom2", "prim", "vel0", "vel1", "vel2"]
+    mfs = [st.cu] + st.cumom + [st.prim] + st.vel
+    bad = [nm for nm, g, m in zip(names, got, mfs) if not torch.equal(g, m.arr.cpu())]
+    assert not bad, bad
+    # the state moved (the comparison is not between two initial states)
+    init = StagState(p, "cuda", aux=False)
+    ctx.init_state(init)
+    assert not torch.equal(init.cu.arr, st.cu.arr)
+
+
+@pytest.mark.gpu
+def test_reference_driver_reports_massfrac_through_abort_handler(driver):
+    r = subprocess.run([driver, "massfrac", "8"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 3, (r.returncode, r.stdout, r.stderr)
+    assert "calculateTransportCoeffs" in r.stdout and "mass fraction" in r.stdout.lower(), r.stdout
