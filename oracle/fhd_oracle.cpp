@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <random>
 #include <vector>
 #include <algorithm>
 
@@ -1188,6 +1189,48 @@ int orc_fill_random_normal(fhd_fab mf_, int scomp, int ncomp, double mean, doubl
                 }
     override_sync(mf);
     fill_boundary(mf);
+    return FHD_OK;
+}
+
+// Host-drawn noise for injected-noise runs: one std::mt19937_64(seed) engine
+// (the generator the C++ standard specifies), Box-Muller on 53-bit uniforms,
+// filling in a fixed order: for A then B, for d = 0..2: face[d] (all its
+// components, variance 1), edge[d] (variance 1), cen[d] (variance 2, the 3D
+// centre-noise variance of timeStepStag.cpp:219-222); valid points only, i
+// fastest, component slowest.  Each field is then OverrideSync'ed and
+// FillBoundary'ed, as MultiFabFillRandomNormal leaves it.  Deterministic and
+// serial: fixtures made from it are reproducible on any host with this libm.
+int orc_fill_noise_mt64(const fhd_noise* nz, uint64_t seed) {
+    std::mt19937_64 eng(seed);
+    bool have = false;
+    double spare = 0.0;
+    auto normal = [&]() {
+        if (have) { have = false; return spare; }
+        double u1 = ((double)(eng() >> 11) + 1.0) * (1.0 / 9007199254740992.0);  // (0,1]
+        double u2 = (double)(eng() >> 11) * (1.0 / 9007199254740992.0);          // [0,1)
+        double r = std::sqrt(-2.0 * std::log(u1));
+        double a = 2.0 * 3.14159265358979323846 * u2;
+        spare = r * std::sin(a);
+        have = true;
+        return r * std::cos(a);
+    };
+    auto fill = [&](const fhd_fab& f_, double variance) {
+        Fab f(f_);
+        const double sd = std::sqrt(variance);
+        const int* N = g.n;
+        for (int n = 0; n < f.nc; ++n)
+            for (int k = 0; k < N[2] + f.nodal[2]; ++k)
+                for (int j = 0; j < N[1] + f.nodal[1]; ++j)
+                    for (int i = 0; i < N[0] + f.nodal[0]; ++i) f(i, j, k, n) = sd * normal();
+        override_sync(f);
+        fill_boundary(f);
+    };
+    for (int s = 0; s < 2; ++s)
+        for (int d = 0; d < 3; ++d) {
+            fill(nz->face[s][d], 1.0);
+            fill(nz->edge[s][d], 1.0);
+            fill(nz->cen[s][d], 2.0);
+        }
     return FHD_OK;
 }
 

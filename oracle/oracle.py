@@ -47,6 +47,7 @@ def lib():
         L.orc_fill_random_normal.argtypes = [fab, i, i, d, d, C.c_uint64, C.c_uint64]
         L.orc_philox4x32_10.argtypes = [P(C.c_uint32), P(C.c_uint32), P(C.c_uint32)]
         L.orc_philox4x32_10.restype = None
+        L.orc_fill_noise_mt64.argtypes = [P(FhdNoise), C.c_uint64]
         L.orc_max_acoustic_cfl.argtypes = [fab, pfab, d]
         L.orc_max_acoustic_cfl.restype = d
         _lib = L
@@ -129,6 +130,15 @@ def fill_step_noise(noise, seed, step):
             fill_random_normal(noise.face[s][d], 0, ns + 1, 0.0, 1.0, seed, (step << 8) | sid); sid += 1
             fill_random_normal(noise.edge[s][d], 0, 1, 0.0, 1.0, seed, (step << 8) | sid); sid += 1
             fill_random_normal(noise.cen[s][d], 0, 1, 0.0, 2.0, seed, (step << 8) | sid); sid += 1
+
+
+def fill_noise_mt64(noise, seed=1):
+    """Injected-noise A/B fields drawn on the host from std::mt19937_64(seed) with
+    Box-Muller (faces/edges variance 1, centres variance 2), OverrideSync'ed and
+    FillBoundary'ed: the noise of the injected-noise parity runs."""
+    set_params(noise.p)
+    nz = noise.c_struct()
+    _chk(lib().orc_fill_noise_mt64(C.byref(nz), seed), "fill_noise_mt64")
 
 
 def philox4x32_10(ctr, key):
