@@ -1,0 +1,68 @@
+"""Equilibrium statistics of the CUDA step with in-kernel Philox noise, against
+the fluctuation theory the reference checks its runs with
+(params_RBtest_eq_SF.py:94-104, params_COAr_eq.py:204-210; tests/theory.py):
+variances of density, species density, momentum, energy and temperature, and a
+flat static structure factor S(k) = <|d rho_k|^2>/N_cells = <d rho^2> for every
+k != 0 (the StructFact.cpp:350, :453, :603-612 normalisation), in FP64 and in
+the mixed-precision path.  32^3 argon at dx = 8e-6 cm; 3 % on variances and on
+the k-averaged S(k), 5 % on its low-k and high-k shells."""
+import pytest
+import torch
+
+from fhdex_b200.context import Context
+from fhdex_b200.params import argon, stable_dt
+from fhdex_b200.state import StagState
+from tests.theory import equilibrium_variances
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_equilibrium_variances_and_structure_factor(precision):
+    n = 32
+    p = argon(n, dx=8e-6, precision=precision, seed=4242)
+    st = StagState(p, "cuda", aux=False)
+    ctx = Context(p)
+    ctx.init_state(st)
+    dt = stable_dt(p)
+    fields = {"rho": lambda: st.cu.valid(0), "rho0": lambda: st.cu.valid(5), "rhoE": lambda: st.cu.valid(4),
+              "T": lambda: st.prim.valid(4), "jx": lambda: st.cumom[0].valid(0)[:, :, :n],
+              "jy": lambda: st.cumom[1].valid(0)[:, :n, :], "jz": lambda: st.cumom[2].valid(0)[:n, :, :]}
+    acc = {k: torch.zeros(2, dtype=torch.float64, device="cuda") for k in fields}
+    sk = torch.zeros((n, n, n), dtype=torch.float64, device="cuda")
+    nwarm, nsamp, every = 1000, 150, 5
+    cnt = 0
+    for s in range(nwarm + nsamp * every):
+        ctx.rk3_step(st, dt, s, aux=False)
+        if s >= nwarm and (s - nwarm) % every == 0:
+            for k, f in fields.items():
+                x = f()
+                acc[k][0] += x.sum()
+                acc[k][1] += (x * x).sum()
+            d = st.cu.valid(0) - p.rho0
+            sk += torch.fft.fftn(d).abs() ** 2 / d.numel()
+            cnt += 1
+    torch.cuda.synchronize()
+    assert ctx.status() == 0
+    th = equilibrium_variances(p)
+    ratios = {}
+    for k, a in acc.items():
+        m = n ** 3 * cnt
+        mean = a[0].item() / m
+        ratios[k] = (a[1].item() / m - mean * mean) / th[k]
+    print({k: f"{v:.4f}" for k, v in ratios.items()})
+    for k, r in ratios.items():
+        assert r == pytest.approx(1.0, abs=0.03), (k, r)
+    # static structure factor of density: flat at the variance for k != 0
+    sk = (sk / cnt).cpu()
+    kk = torch.fft.fftfreq(n) * n
+    kx, ky, kz = torch.meshgrid(kk, kk, kk, indexing="ij")
+    kmag = (kx ** 2 + ky ** 2 + kz ** 2).sqrt()
+    nonzero = kmag > 0
+    whole = sk[nonzero].mean().item() / th["rho"]
+    low = sk[nonzero & (kmag <= n / 6)].mean().item() / th["rho"]
+    high = sk[kmag >= n / 3].mean().item() / th["rho"]
+    print(f"S(k)/theory: all {whole:.4f} low-k {low:.4f} high-k {high:.4f}")
+    assert whole == pytest.approx(1.0, abs=0.03)
+    assert low == pytest.approx(1.0, abs=0.05)
+    assert high == pytest.approx(1.0, abs=0.05)
