@@ -43,10 +43,12 @@ HBM_FALLBACK_GBS = 6650.0
 METRIC = "cell-updates/s (RK3 steps x cells)"
 UNIT = "cell-updates/s"
 
-# DRAM traffic (read + write bytes) of one RK stage (k_taus + 3 x k_faces +
-# k_update) per cell, from the ncu capture summarised in profiles/ (None until
-# captured for that configuration).
-STAGE_TRAFFIC_BYTES_PER_CELL = {}
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one RK stage
+# (k_cellprep + k_taus + 3 x k_faces + k_update) per cell, keyed
+# "nspecies:precision": one ncu capture of a full timed step at 128^3 (the
+# summary in profiles/stage_traffic_argon128.md), scaled to the box by the cell
+# count.  Absent for configurations not captured.
+STAGE_TRAFFIC_BYTES_PER_CELL = {"2:fp64": 1499.8, "2:mixed": 1232.5}
 
 
 def measured_peak():
@@ -245,19 +247,17 @@ def autotune(ctx, st, dt, steps=2):
 
 def run_ours(args):
     import torch
-    import torch.distributed as dist
     from fhdex_b200.context import Context
     from fhdex_b200.params import stable_dt
     from fhdex_b200.state import StagState
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from fhdex_b200 import replicas
+    env = replicas.rank_env()
+    world, rank, local = env.world, env.rank, env.local
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    p = make_params(args)
+    replicas.init(env, "nccl")
+    # replicas: every rank advances its own run (own Philox key), no data-path collective
+    p = replicas.replica_params(make_params(args), rank)
     dt = stable_dt(p)
     ctx = Context(p, local)
     st = StagState(p, f"cuda:{local}", aux=False)
@@ -274,8 +274,7 @@ def run_ours(args):
     ctx.profile(True)
     ctx.profile_read()
     clocks = ClockSampler(local)
-    if world > 1:
-        dist.barrier()
+    replicas.barrier(env)
     torch.cuda.synchronize()
     clocks.start()
     time.sleep(0.3)
@@ -285,29 +284,26 @@ def run_ours(args):
         ctx.rk3_step(st, dt, args.warmup + s, aux=False)
     e1.record()
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier(env)
     clk = clocks.stop()
     prof = ctx.profile_read()
     ctx.profile(False)
     ms = e0.elapsed_time(e1)
     status = ctx.status()
-    if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = t.item()
+    ms = replicas.max_over_ranks(ms, env, device=f"cuda:{local}")
     cells = p.n_cells[0] * p.n_cells[1] * p.n_cells[2]
-    value = cells * args.steps * world / (ms / 1e3)
+    value = replicas.whole_job_rate(cells * args.steps, env, ms)
     # every bracketed profile scope is one launch, except the face-flux scope (3 launches)
     launches = sum(v[1] for v in prof.values()) + 2 * prof["faces"][1]
 
-    # roofline of the dominant kernel group: one RK stage = k_taus + 3 x k_faces +
-    # k_update (the work of the reference's calculateFluxStag + stage update).
+    # roofline of the dominant kernel group: one RK stage = k_cellprep + k_taus +
+    # 3 x k_faces + k_update (conversion, transport coefficients, calculateFluxStag
+    # and the stage update of the reference).
     # Algorithmic bytes per stage: the conserved state S = 5 + nspecies doubles per
     # cell read once (stage 1) or twice (U^s and U^0, stages 2-3) and written once;
     # averaged over the three stages: (2 + 3 + 3)/3 * S * 8 bytes per cell.
     S = 5 + p.nspecies
-    stage_ms = prof["taus"][0] + prof["faces"][0] + prof["update"][0]
+    stage_ms = prof["cellprep"][0] + prof["taus"][0] + prof["faces"][0] + prof["update"][0]
     nstages = max(prof["taus"][1], 1)
     avg_stage_s = stage_ms / 1e3 / nstages
     alg_bytes = (2 + 3 + 3) / 3.0 * S * 8 * cells
@@ -317,7 +313,8 @@ def run_ours(args):
     traffic = STAGE_TRAFFIC_BYTES_PER_CELL.get(key)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic * cells if traffic else None, "peak_kind": peak_kind,
-            "kernel": "RK stage (k_taus + 3x k_faces + k_update), per stage",
+            "traffic_gbs": traffic * cells / avg_stage_s / 1e9 if traffic else None,
+            "kernel": "RK stage (k_cellprep + k_taus + 3x k_faces + k_update), per stage",
             "kernel_ms_per_launch": 1e3 * avg_stage_s,
             "algorithmic_bytes_per_launch": alg_bytes,
             "step_breakdown_ms": {k: v[0] / args.steps for k, v in prof.items()}}
@@ -338,17 +335,12 @@ def run_ours(args):
         torch.cuda.empty_cache()
         ctx.rk3_step_host(hs, dt, 0)  # warm
         ne = max(2, min(args.steps, 5))
-        if world > 1:
-            dist.barrier()
+        replicas.barrier(env)
         t = time.perf_counter()
         for s in range(ne):
             h2d, d2h = ctx.rk3_step_host(hs, dt, 1 + s)
-        el = time.perf_counter() - t
-        if world > 1:
-            tt = torch.tensor([el], device=f"cuda:{local}", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            el = tt.item()
-        e2e = {"value": cells * ne * world / el, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+        el = replicas.max_over_ranks(time.perf_counter() - t, env, device=f"cuda:{local}")
+        e2e = {"value": replicas.whole_job_rate(cells * ne, env, 1e3 * el), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "steps": ne, "path": "fhd_rk3_step_stag_host (pinned host fabs)"}
         ctx.close()
 
@@ -357,9 +349,7 @@ def run_ours(args):
         v, sample = cpu_oracle_rate(p)
         cpu = {"value": v, "unit": UNIT, "cores": _CORES, "kind": "port", "sample": sample}
 
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish(env)
     if rank != 0:
         return
     out = {
