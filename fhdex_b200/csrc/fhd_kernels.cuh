@@ -666,8 +666,14 @@ __global__ void __launch_bounds__(128) k_taus_b(const StageArgs<NS, R, NZ>* __re
     if (q < taus_count(a)) taus_point(a, q);
 }
 
+// Register cap of the batched face kernel: 64 registers (8 blocks of 128) for up
+// to two species, where the extra occupancy outweighs small spills; 128
+// registers (4 blocks) above, where a 64-register cap spills heavily.
+template <int NS>
+constexpr int faces_b_min_blocks() { return NS <= 2 ? 8 : 4; }
+
 template <int NS, class R, int NZ, int D>
-__global__ void __launch_bounds__(128, 8) k_faces_b(const StageArgs<NS, R, NZ>* __restrict__ args,
+__global__ void __launch_bounds__(128, faces_b_min_blocks<NS>()) k_faces_b(const StageArgs<NS, R, NZ>* __restrict__ args,
                                                    const int* __restrict__ bpref, int nmem) {
     const int m = member_of(bpref, nmem);
     const StageArgs<NS, R, NZ>& a = args[m];

@@ -7,8 +7,11 @@ temperature, dt and seed) advanced together.
 species count, number of steps, precision) arrive on a Poisson trace; a request
 is admitted as soon as its HBM footprint fits the budget, joins the batch of its
 (species count, precision) class between two step chunks, and leaves it when its
-steps are done.  Each class batch runs on its own CUDA stream, so the classes'
-kernels overlap on the device; within a class the members share every launch.
+steps are done.  Each class batch runs on its own CUDA stream and advances as
+soon as its previous chunk has finished, so the classes' kernels overlap on the
+device; within a class the members share every launch.  A request whose box
+already fills the GPU (``solo_cells``) runs the single-run step on a stream of
+its own instead of joining a batch.
 ``run_alone`` is the baseline: the same trace served one request at a time with
 the plain FP64 step.
 
@@ -102,81 +105,164 @@ def ensemble(members: int = 512, seed: int = 0, precision: int = 1, sizes=(32, 6
     return b, states, cells
 
 
+class _Class:
+    """One (species count, precision) class: its batch, stream and the chunk in flight."""
+
+    def __init__(self, ns, precision, device):
+        self.batch = Batch(ns, precision, device)
+        # small requests: high-priority stream, so they are not held back by solo runs
+        self.stream = torch.cuda.Stream(device, priority=-1)
+        self.batch.set_stream(self.stream)
+        self.event = torch.cuda.Event()
+        self.inflight = 0          # steps of the chunk in flight (0 = idle)
+        self.queue = []            # admitted requests waiting to join: (req, params, state, bytes)
+        self.active = {}           # rid -> [req, member id, remaining steps, state, bytes, params]
+
+
+class _Solo:
+    """A request large enough to fill the GPU by itself: the single-run step on a
+    stream of its own, advanced in chunks like a class batch."""
+
+    def __init__(self, req, p, st, fb, device):
+        self.req, self.p, self.st, self.fb = req, p, st, fb
+        self.ctx = Context(p, device)
+        self.stream = torch.cuda.Stream(device, priority=0)
+        self.event = torch.cuda.Event()
+        self.dt = stable_dt(p)
+        self.done_steps = 0
+        self.inflight = 0
+
+    def launch(self, k):
+        with torch.cuda.stream(self.stream):
+            for s in range(self.done_steps, self.done_steps + k):
+                self.ctx.rk3_step(self.st, self.dt, s, aux=False)
+            self.event.record(self.stream)
+        self.inflight = k
+
+
 class Server:
-    def __init__(self, device: int = 0, hbm_budget: int | None = None, chunk: int = 20):
+    """solo_cells: requests with at least this many cells run alone on their own
+    stream with the single-run kernels (batching brings nothing to a launch that
+    already fills the GPU); smaller ones join their class batch."""
+
+    def __init__(self, device: int = 0, hbm_budget: int | None = None, chunk: int = 20,
+                 solo_cells: int = 96 ** 3):
         self.device = device
         free, total = torch.cuda.mem_get_info(device)
         self.budget = hbm_budget if hbm_budget is not None else int(0.6 * free)
         self.chunk = chunk
-        self.batches: dict = {}
+        self.solo_cells = solo_cells
+        self.classes: dict = {}
+        self.solos: list = []
 
-    def _batch(self, ns, precision):
+    def _class(self, ns, precision) -> _Class:
         key = (ns, precision)
-        if key not in self.batches:
-            self.batches[key] = Batch(ns, precision, self.device)
-        return self.batches[key]
+        if key not in self.classes:
+            self.classes[key] = _Class(ns, precision, self.device)
+        return self.classes[key]
+
+    def _busy(self):
+        return bool(self.solos) or any(c.inflight or c.queue or c.active for c in self.classes.values())
 
     def run(self, trace: list[Request], keep_states: bool = False):
-        """Serve `trace` in real time; returns the requests with start/finish filled
-        and, when keep_states, {rid: StagState} of the final states."""
+        """Serve `trace` in real time; returns the requests with start/finish filled,
+        {rid: StagState} of the final states (when keep_states), the cell-updates
+        done and the elapsed seconds.
+
+        Admission is FIFO by HBM footprint.  Every class batch and every solo run
+        advances independently: when its chunk in flight has finished (CUDA event
+        query, no blocking), its completed requests leave, the requests admitted
+        since join, and the next chunk of min(chunk, fewest remaining steps) steps
+        is launched on its stream.  Members join and leave only while their class
+        is idle."""
         pending = sorted(trace, key=lambda r: r.arrival)
-        active = {}      # rid -> (req, batch, mid, remaining, state, bytes)
         used = 0
         finals = {}
         cell_updates = 0
         t0 = time.perf_counter()
-        while pending or active:
+        while pending or self._busy():
             now = time.perf_counter() - t0
             # admission: FIFO, as memory frees up
             while pending and pending[0].arrival <= now:
                 r = pending[0]
                 p = request_params(r)
                 fb = footprint_bytes(p)
-                if used + fb > self.budget and active:
+                if used + fb > self.budget and self._busy():
                     break
                 pending.pop(0)
-                b = self._batch(p.nspecies, p.precision)
-                st = StagState(p, f"cuda:{self.device}", aux=False)
-                mid = b.add(p, st, stable_dt(p))
-                r.start = time.perf_counter() - t0
-                active[r.rid] = [r, b, mid, r.steps, st, fb, p]
                 used += fb
-            if not active:
-                if pending:
-                    time.sleep(max(0.0, min(0.005, pending[0].arrival - now)))
-                continue
-            # one chunk per class batch; classes run concurrently on their streams
-            chunks = {}
-            for key, b in self.batches.items():
-                rem = [v[3] for v in active.values() if v[1] is b]
-                if rem:
-                    k = min(self.chunk, min(rem))
-                    b.step(k, graph=True)
-                    chunks[key] = k
-            for key, k in chunks.items():
-                self.batches[key].synchronize()
-            now = time.perf_counter() - t0
-            for rid in list(active):
-                v = active[rid]
-                k = chunks[(v[6].nspecies, v[6].precision)]
-                v[3] -= k
-                cell_updates += k * v[6].n_cells[0] * v[6].n_cells[1] * v[6].n_cells[2]
-                if v[3] <= 0:
-                    r, b, mid = v[0], v[1], v[2]
-                    r.status = b.status(mid)
-                    b.remove(mid)
-                    r.finish = now
-                    used -= v[5]
-                    if keep_states:
-                        finals[rid] = v[4]
-                    del active[rid]
-        elapsed = time.perf_counter() - t0
-        return trace, finals, cell_updates, elapsed
+                st = StagState(p, f"cuda:{self.device}", aux=False)
+                if p.n_cells[0] * p.n_cells[1] * p.n_cells[2] >= self.solo_cells:
+                    torch.cuda.current_stream(self.device).synchronize()
+                    s = _Solo(r, p, st, fb, self.device)
+                    s.ctx.init_state(st)
+                    torch.cuda.current_stream(self.device).synchronize()
+                    r.start = time.perf_counter() - t0
+                    self.solos.append(s)
+                else:
+                    self._class(p.nspecies, p.precision).queue.append((r, p, st, fb))
+            progressed = False
+            for s in list(self.solos):
+                if s.inflight:
+                    if not s.event.query():
+                        continue
+                    n = s.p.n_cells
+                    cell_updates += s.inflight * n[0] * n[1] * n[2]
+                    s.done_steps += s.inflight
+                    s.inflight = 0
+                    if s.done_steps >= s.req.steps:
+                        s.req.status = s.ctx.status()
+                        s.req.finish = time.perf_counter() - t0
+                        used -= s.fb
+                        if keep_states:
+                            finals[s.req.rid] = s.st
+                        s.ctx.close()
+                        self.solos.remove(s)
+                        continue
+                s.launch(min(self.chunk, s.req.steps - s.done_steps))
+                progressed = True
+            for c in self.classes.values():
+                if c.inflight:
+                    if not c.event.query():
+                        continue
+                    k, c.inflight = c.inflight, 0
+                    t = time.perf_counter() - t0
+                    for rid in list(c.active):
+                        v = c.active[rid]
+                        v[2] -= k
+                        n = v[5].n_cells
+                        cell_updates += k * n[0] * n[1] * n[2]
+                        if v[2] <= 0:
+                            r = v[0]
+                            r.status = c.batch.status(v[1])
+                            c.batch.remove(v[1])
+                            r.finish = t
+                            used -= v[4]
+                            if keep_states:
+                                finals[rid] = v[3]
+                            del c.active[rid]
+                for r, p, st, fb in c.queue:
+                    mid = c.batch.add(p, st, stable_dt(p))
+                    r.start = time.perf_counter() - t0
+                    c.active[r.rid] = [r, mid, r.steps, st, fb, p]
+                c.queue = []
+                if c.active:
+                    k = min(self.chunk, min(v[2] for v in c.active.values()))
+                    c.batch.step(k, graph=True)
+                    c.event.record(c.stream)
+                    c.inflight = k
+                    progressed = True
+            if not progressed:
+                idle = pending and not self._busy()
+                nxt = pending[0].arrival - (time.perf_counter() - t0) if idle else 0.0002
+                time.sleep(max(0.0, min(0.005, nxt)))
+        return trace, finals, cell_updates, time.perf_counter() - t0
 
     def close(self):
-        for b in self.batches.values():
-            b.close()
-        self.batches = {}
+        for c in self.classes.values():
+            c.batch.synchronize()
+            c.batch.close()
+        self.classes = {}
 
 
 def run_alone(trace: list[Request], device: int = 0, fp64: bool = True):

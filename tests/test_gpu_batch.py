@@ -94,13 +94,16 @@ def test_members_join_and_leave_between_steps():
 
 def test_server_results_match_runs_alone():
     """Requests served with continuous batching (joining and leaving batches of
-    both precisions and species counts at different times) end in exactly the
-    state they reach when run alone."""
+    both precisions and species counts at different times, and boxes of 11^3 cells
+    or more on the solo lane) end in exactly the state they reach when run alone."""
     from fhdex_b200.serve import Server, poisson_trace, request_params
-    trace = poisson_trace(6, rate=400.0, seed=3, edge=(8, 14), steps=(3, 9))
-    srv = Server(chunk=2)
+    trace = poisson_trace(8, rate=400.0, seed=3, edge=(8, 14), steps=(3, 9))
+    srv = Server(chunk=2, solo_cells=11 ** 3)
     reqs, finals, cell_updates, elapsed = srv.run(trace, keep_states=True)
     assert all(r.status == 0 for r in reqs)
+    sizes = [r.n for r in reqs]
+    assert any(n >= 11 for n in sizes) and any(n < 11 for n in sizes), sizes
+    assert cell_updates == sum(r.steps * r.n ** 3 for r in reqs)
     for r in reqs:
         p = request_params(r)
         ref = alone(p, stable_dt(p), r.steps)
