@@ -233,7 +233,7 @@ int init_uniform(const fhd_fab& cu, int ns, double rho0, double rhoE, const doub
 int num_tiles() { return kNumStageBlocks; }
 
 const char* tile_name(int t) {
-    static const char* names[] = {"b128-min4", "b256-min2", "b128-min6", "b128-min2", "b128-min8"};
+    static const char* names[] = {"b128-min4", "b256-min2", "b128-min6", "b128-min10", "b128-min8"};
     return (t >= 0 && t < num_tiles()) ? names[t] : "?";
 }
 

@@ -222,6 +222,13 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
 #pragma unroll
     for (int s = 0; s < NS; ++s) spec[s] = R(0.0);
 
+    const R un = R(F.vel[D](i, j, k));
+
+    // ---- viscous heating terms, complete (stochastic part assigned,
+    // fluxStag.cpp:298-781, then the deterministic part added, :1026-1426).  Each
+    // flux variable keeps the reference's own sequence of operations; finishing
+    // these two first only shortens the live ranges of their operands.
+    {
     const CellTaus<R> tl = tg.cell(im, jm, km);
     const CellTaus<R> th = tg.cell(i, j, k);
     // the two transverse edge families touching this face and their (lo, hi) positions
@@ -249,7 +256,19 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
         vb1h = R(vely(i, j + 1, k)); vb1l = R(vely(i, j + 1, k - 1));
         vb0h = R(vely(i, j, k));     vb0l = R(vely(i, j, k - 1));
     }
-    const R un = R(F.vel[D](i, j, k));
+    if (NZ != NZ_OFF) {
+        vdiag = R(0.5) * un * (tl.s[D] + th.s[D]);
+        R vsh = R(0.0);
+        vsh += R(0.25) * ((va1h + va1l) * ea1.s + (va0h + va0l) * ea0.s);
+        vsh += R(0.25) * ((vb1h + vb1l) * eb1.s + (vb0h + vb0l) * eb0.s);
+        vshear = vsh;
+    }
+    vdiag -= R(0.5) * un * (tl.d[D] + th.d[D]);
+    R vsh = R(0.0);
+    vsh -= R(0.25) * ((va1h + va1l) * ea1.d + (va0h + va0l) * ea0.d);
+    vsh -= R(0.25) * ((vb1h + vb1l) * eb1.d + (vb0h + vb0l) * eb0.d);
+    vshear += vsh;
+    }
 
     // ---- stochastic part (fluxStag.cpp:298-781) ----
     if (NZ != NZ_OFF) {
@@ -260,11 +279,6 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
         nz.template face_all<NS + 1>(P, D, i, j, k, wf);
         const R fw0 = dsqrt(R(P.k_B) * kp * R(P.volinv) * R(P.dtinv));
         heat = fw0 * R(wf[0]);
-        vdiag = R(0.5) * un * (tl.s[D] + th.s[D]);
-        R vsh = R(0.0);
-        vsh += R(0.25) * ((va1h + va1l) * ea1.s + (va0h + va0l) * ea0.s);
-        vsh += R(0.25) * ((vb1h + vb1l) * eb1.s + (vb0h + vb0l) * eb0.s);
-        vshear = vsh;
         R yy[NS], yyp[NS], DY[NS * NS], sqD[NS * NS], hk[NS], wien[NS];
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
@@ -318,11 +332,6 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
     // ---- diffusive part (fluxStag.cpp:1026-1426) ----
     {
         const R h = R(P.dx[D]);
-        vdiag -= R(0.5) * un * (tl.d[D] + th.d[D]);
-        R vsh = R(0.0);
-        vsh -= R(0.25) * ((va1h + va1l) * ea1.d + (va0h + va0l) * ea0.d);
-        vsh -= R(0.25) * ((vb1h + vb1l) * eb1.d + (vb0h + vb0l) * eb0.d);
-        vshear += vsh;
         const R Tl = R(F.T(im, jm, km)), Th = R(F.T(i, j, k));
         const R pl = R(F.p(im, jm, km)), ph = R(F.p(i, j, k));
         const R kp = R(0.5) * (F.kappa(im, jm, km) + F.kappa(i, j, k));

@@ -81,8 +81,15 @@ FHD_D void cellprep_point(const PrepArgs<NS, R>& a, int q) {
     for (int n = 0; n < NS * NS; ++n) a.D(i, j, k, n) = c.D[n];
 }
 
+// Register cap of the cell kernel: 64 registers up to two species (8 blocks of
+// 128, no spills); with three or four species the Giovangigli solves need ~164
+// registers in FP64 and ~93 in FP32, so cap at 128 (4 blocks, 40 B of spills in
+// FP64) and 80 (6 blocks, no spills) to raise occupancy.
 template <int NS, class R>
-__global__ void __launch_bounds__(128) k_cellprep(PrepArgs<NS, R> a) {
+constexpr int cellprep_min_blocks() { return NS <= 2 ? 8 : (sizeof(R) == 8 ? 4 : 6); }
+
+template <int NS, class R>
+__global__ void __launch_bounds__(128, cellprep_min_blocks<NS, R>()) k_cellprep(PrepArgs<NS, R> a) {
     const int tot = cellprep_count(a);
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) cellprep_point(a, q);
 }
@@ -649,7 +656,7 @@ FHD_D int member_of(const int* __restrict__ bpref, int nmem) {
 }
 
 template <int NS, class R>
-__global__ void __launch_bounds__(128) k_cellprep_b(const PrepArgs<NS, R>* __restrict__ args,
+__global__ void __launch_bounds__(128, cellprep_min_blocks<NS, R>()) k_cellprep_b(const PrepArgs<NS, R>* __restrict__ args,
                                                     const int* __restrict__ bpref, int nmem) {
     const int m = member_of(bpref, nmem);
     const PrepArgs<NS, R>& a = args[m];

@@ -87,7 +87,7 @@ int launch_cellprep(const StageCall& c) {
 // launch shapes available to the autotuner: block size of the stage kernels and
 // the register cap of the face-flux kernel (minimum resident blocks per SM)
 constexpr int kStageBlocks[] = {128, 256, 128, 128, 128};
-constexpr int kFaceMinBlocks[] = {4, 2, 6, 2, 8};
+constexpr int kFaceMinBlocks[] = {4, 2, 6, 10, 8};  // as instantiated in launch_stage_part_t
 constexpr int kNumStageBlocks = 5;
 
 template <int NS, class R, int NZ>
@@ -134,7 +134,7 @@ int launch_stage_part_t(const StageCall& c, int part) {
             case 0: FHD_FACES(128, 4) break;
             case 1: FHD_FACES(256, 2) break;
             case 2: FHD_FACES(128, 6) break;
-            case 3: FHD_FACES(128, 2) break;
+            case 3: FHD_FACES(128, 10) break;
             default: FHD_FACES(128, 8) break;
         }
 #undef FHD_FACES
