@@ -683,9 +683,13 @@ int fhd_rk3_step_stag_host(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab
     for (int q = 0; q < 8; ++q) {
         df[q] = *hf[q];
         df[q].data = p;
-        if (cudaMemcpyAsync(p, hf[q]->data, bytes[q], cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
-            return FHD_ERR_CUDA;
-        h2d += (int64_t)bytes[q];
+        // only cu and mom go up: the step derives prim and vel from them before
+        // reading either, so the input prim/vel contents are dead
+        if (q < 4) {
+            if (cudaMemcpyAsync(p, hf[q]->data, bytes[q], cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+                return FHD_ERR_CUDA;
+            h2d += (int64_t)bytes[q];
+        }
         p += bytes[q];
     }
     if (inj) {

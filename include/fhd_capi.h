@@ -191,7 +191,9 @@ int fhd_fill_step_noise(fhd_ctx* ctx, const fhd_noise* noise, int64_t step);
 /* RK3stepStag: timeStepStag.cpp:13-1245 (declared
  * compressible_functions_stag.H:113-125).  Advances cu/mom/prim/vel by one
  * SSP-RK3 step in place (ghosts refreshed, as after the reference's final
- * FillBoundary).  source: nprimvars-component cell fab (the reference's
+ * FillBoundary).  prim and vel are recomputed from cu and mom at the start of
+ * every stage (the reference reads them as given, which in its driver are
+ * always the conversion of cu and mom), so their contents on entry are not read.  source: nprimvars-component cell fab (the reference's
  * `source`, all zeros unless chemistry is on) or data == NULL for zero.
  * eta..D receive the stage-3 transport coefficients and faceflux/edgeflux/
  * cenflux the stage-3 fluxes when their data pointers are non-NULL (pass NULL
@@ -204,10 +206,11 @@ int fhd_rk3_step_stag(fhd_ctx* ctx, fhd_fab cu, const fhd_fab mom[3], fhd_fab pr
                       const fhd_noise* injected, double dt, int64_t step);
 
 /* RK3stepStag on HOST fabs (same layouts as above, host pointers; pinned memory
- * gives full copy bandwidth): copies cu/mom/prim/vel to device buffers owned by
- * the context, advances one step in place there (in-kernel noise, or injected
- * noise given as host fabs), copies the four fields back and waits for the
- * stream.  For callers whose MultiFabs live in host memory (a CPU AMReX build);
+ * gives full copy bandwidth): copies cu and mom to device buffers owned by the
+ * context, advances one step there (in-kernel noise, or injected noise given as
+ * host fabs), copies cu/mom/prim/vel back and waits for the stream.  prim and vel
+ * are outputs only: the step derives them from cu and mom before reading them
+ * (as fhd_rk3_step_stag does), so their contents on entry are not read.  For callers whose MultiFabs live in host memory (a CPU AMReX build);
  * no reference counterpart beyond RK3stepStag itself. */
 int fhd_rk3_step_stag_host(fhd_ctx* ctx, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim,
                            const fhd_fab vel[3], const fhd_noise* injected, double dt,
