@@ -125,14 +125,15 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_oracle_rate(p, target_s=15.0, max_n=None):
-    """Oracle (CPU restatement of the reference step, OpenMP over all host cores)
-    on a bounded sample: a smaller box of the same gas, enough steps for about
-    target_s seconds.  Returns (cell-updates/s, sample description)."""
+def cpu_oracle_rate(p, target_s=15.0, max_n=None, threads=0):
+    """Oracle (CPU restatement of the reference step, OpenMP over `threads` host
+    cores, 0 = all) on a bounded sample: a smaller box of the same gas, enough
+    steps for about target_s seconds.  Returns (cell-updates/s, sample description)."""
     from oracle import oracle as O
     from fhdex_b200.params import stable_dt
     from fhdex_b200.state import StagState, StepNoise
     O.build()
+    O.set_threads(threads)
     n = min(64, p.n_cells[0]) if max_n is None else max_n
     q = p.replace(n_cells=(n, n, n), prob_hi=tuple(p.dx[0] * n for _ in range(3)))
     st = StagState(q)
@@ -150,6 +151,7 @@ def cpu_oracle_rate(p, target_s=15.0, max_n=None):
         rc = O.rk3_step(st, nz, dt)
         assert rc == 0
     el = time.perf_counter() - t
+    O.set_threads(0)
     return n ** 3 * steps / el, f"{n}^3 box of the same gas, {steps} RK3 steps incl. per-step noise fill, {el:.1f} s"
 
 
@@ -347,7 +349,9 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, sample = cpu_oracle_rate(p)
-        cpu = {"value": v, "unit": UNIT, "cores": _CORES, "kind": "port", "sample": sample}
+        v1, sample1 = cpu_oracle_rate(p, target_s=8.0, max_n=32, threads=1)
+        cpu = {"value": v, "unit": UNIT, "cores": _CORES, "kind": "port", "sample": sample,
+               "single_thread": {"value": v1, "unit": UNIT, "cores": 1, "sample": sample1}}
 
     replicas.finish(env)
     if rank != 0:

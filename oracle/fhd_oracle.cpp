@@ -21,6 +21,9 @@
 #include <random>
 #include <vector>
 #include <algorithm>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 #include "../include/fhd_capi.h"
 
@@ -1009,6 +1012,20 @@ int orc_get_hc(double* hcv, double* hcp) {
 }
 
 int orc_take_status() { int s = g_status; g_status = 0; return s; }
+
+// OpenMP thread count of the oracle's parallel loops (<= 0: all host cores);
+// returns the count in effect.  Lets the CPU baseline be timed at 1 thread and
+// at all cores.
+int orc_set_threads(int n) {
+#ifdef _OPENMP
+    if (n <= 0) n = omp_get_num_procs();
+    omp_set_num_threads(n);
+    return omp_get_max_threads();
+#else
+    (void)n;
+    return 1;
+#endif
+}
 
 int orc_fill_boundary(fhd_fab f) { fill_boundary(Fab(f)); return FHD_OK; }
 int orc_override_sync(fhd_fab f) { override_sync(Fab(f)); return FHD_OK; }

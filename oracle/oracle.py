@@ -48,6 +48,8 @@ def lib():
         L.orc_philox4x32_10.argtypes = [P(C.c_uint32), P(C.c_uint32), P(C.c_uint32)]
         L.orc_philox4x32_10.restype = None
         L.orc_fill_noise_mt64.argtypes = [P(FhdNoise), C.c_uint64]
+        L.orc_set_threads.argtypes = [i]
+        L.orc_set_threads.restype = i
         L.orc_max_acoustic_cfl.argtypes = [fab, pfab, d]
         L.orc_max_acoustic_cfl.restype = d
         _lib = L
@@ -130,6 +132,11 @@ def fill_step_noise(noise, seed, step):
             fill_random_normal(noise.face[s][d], 0, ns + 1, 0.0, 1.0, seed, (step << 8) | sid); sid += 1
             fill_random_normal(noise.edge[s][d], 0, 1, 0.0, 1.0, seed, (step << 8) | sid); sid += 1
             fill_random_normal(noise.cen[s][d], 0, 1, 0.0, 2.0, seed, (step << 8) | sid); sid += 1
+
+
+def set_threads(n=0):
+    """OpenMP threads of the oracle's loops (0: all host cores); returns the count."""
+    return lib().orc_set_threads(int(n))
 
 
 def fill_noise_mt64(noise, seed=1):
