@@ -49,6 +49,10 @@ UNIT = "cell-updates/s"
 # summary in profiles/stage_traffic_argon128.md), scaled to the box by the cell
 # count.  Absent for configurations not captured.
 STAGE_TRAFFIC_BYTES_PER_CELL = {"2:fp64": 1499.8, "2:mixed": 1232.5}
+# DRAM traffic of one statistics update per cell (all flags), keyed "nspecies":
+# ncu capture of the three statistics kernels at 128^3 (the summary in
+# profiles/stats_argon128.md), scaled by the cell count.
+STATS_TRAFFIC_BYTES_PER_CELL = {"2": 1639.1}
 
 
 def measured_peak():
@@ -368,6 +372,67 @@ def run_ours(args):
     print(json.dumps(out), flush=True)
 
 
+def stats_alg_bytes_per_cell(p):
+    """Algorithmic bytes of one statistics update per cell: the state read once
+    (cu, prim, the three face momenta) and every statistic read and written once
+    (cuMeans, cuVars, primMeans, primVars, coVars, mom3, mom4 and the four
+    face-centred statistics in three directions)."""
+    nv, npv = p.nvars, p.nprimvars
+    reads = nv + npv + 3
+    stats = 2 * nv + (npv + 3) + (npv + 5) + 26 + 2 * (nv + 1) + 4 * 3
+    return 8 * (reads + 2 * stats)
+
+
+def run_stats(args):
+    """Running statistics (fhd_stats_stag, all flags) after the step, timed alone:
+    --steps updates with CUDA events on the launching stream; HBM roofline."""
+    import torch
+    from fhdex_b200 import capi
+    from fhdex_b200.context import Context
+    from fhdex_b200.params import stable_dt
+    from fhdex_b200.state import StagState
+    from fhdex_b200.stats import StatsState
+    torch.cuda.set_device(0)
+    p = make_params(args)
+    ctx = Context(p, 0)
+    st = StagState(p, "cuda:0", aux=False)
+    ctx.init_state(st)
+    dt = stable_dt(p)
+    ctx.rk3_step(st, dt, 0, aux=False)
+    stats = StatsState(p, "cuda:0")
+    flags = capi.STATS_MEANS | capi.STATS_VARS | capi.STATS_MOM3 | capi.STATS_MOM4
+    for s in range(1, args.warmup + 1):
+        ctx.stats_stag(st, stats, s, flags)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for s in range(args.steps):
+        ctx.stats_stag(st, stats, args.warmup + 1 + s, flags)
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    assert ctx.status() == 0
+    cells = p.n_cells[0] * p.n_cells[1] * p.n_cells[2]
+    alg = stats_alg_bytes_per_cell(p) * cells
+    peak, peak_kind = measured_peak()
+    achieved = alg / (ms / 1e3) / 1e9
+    traffic = STATS_TRAFFIC_BYTES_PER_CELL.get(f"{p.nspecies}")
+    print(json.dumps({"mode": "stats", "metric": "statistics updates/s (cells x updates)", "unit": "cell-updates/s",
+                      "value": cells / (ms / 1e3), "ms_per_update": ms, "steps": args.steps, "warmup": args.warmup,
+                      "dtype": "f64", "config": {"workload": f"running statistics, all flags, {p.n_cells[0]}^3, "
+                                                             f"{p.nspecies} species"},
+                      "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                                   "frac": achieved / peak, "peak_kind": peak_kind,
+                                   "traffic": traffic * cells if traffic else None,
+                                   "algorithmic_bytes_per_launch": alg,
+                                   "kernel": "k_stats_means_a + k_stats_means_b + k_stats_vars + 4 ghost fills"},
+                      "clocks": clk}), flush=True)
+
+
 def run_ensemble(args):
     """Batched ensemble: --members realisations of argon, half 32^3 and half 64^3,
     T0 ~ U(250,350) K, rho0 ~ U(1e-3,3e-3) g/cm^3, one graph replay per step."""
@@ -423,7 +488,7 @@ def run_serve(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--mode", default="step", choices=["step", "ensemble", "serve"])
+    ap.add_argument("--mode", default="step", choices=["step", "ensemble", "serve", "stats"])
     ap.add_argument("--members", type=int, default=512)
     ap.add_argument("--requests", type=int, default=48)
     ap.add_argument("--rate", type=float, default=50.0)
@@ -451,6 +516,8 @@ def main():
         run_ensemble(args)
     elif args.mode == "serve":
         run_serve(args)
+    elif args.mode == "stats":
+        run_stats(args)
     else:
         run_ours(args)
 

@@ -35,6 +35,7 @@ def _units():
     u.append(("capi", "fhd_capi.cu", ["-fmad=false"]))
     u.append(("noalloc", "fhd_noalloc.cu", ["-fmad=false"]))
     u.append(("batch", "fhd_batch.cu", ["-fmad=false"]))
+    u.append(("stats", "fhd_stats.cu", ["-fmad=false"]))
     return u
 
 

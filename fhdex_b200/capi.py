@@ -80,6 +80,17 @@ PROF_KINDS = ("cellprep", "taus", "faces", "update", "ghosts", "convert", "aux_f
 FabArr3 = FhdFab * 3
 FabArr6 = FhdFab * 6
 
+
+class FhdStats(C.Structure):
+    """fhd_stats: the reference's statistics MultiFabs (one box each)."""
+    _fields_ = [("cuMeans", FhdFab), ("cuVars", FhdFab), ("primMeans", FhdFab), ("primVars", FhdFab),
+                ("coVars", FhdFab), ("mom3", FhdFab), ("mom4", FhdFab),
+                ("velMeans", FhdFab * 3), ("velVars", FhdFab * 3), ("cumomMeans", FhdFab * 3),
+                ("cumomVars", FhdFab * 3)]
+
+
+STATS_MEANS, STATS_VARS, STATS_MOM3, STATS_MOM4 = 1, 2, 4, 8
+
 _PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG_DIR, "lib", "libfhd_b200.so")
 
@@ -120,6 +131,7 @@ def _declare(lib):
         "fhd_profile": (i, [vp, i]),
         "fhd_profile_read": (i, [vp, P(d), P(C.c_int64)]),
         "fhd_rk3_step_stag_noalloc": (i, [P(FhdParams), fab, pfab, fab, pfab, d, C.c_int64, vp, P(i)]),
+        "fhd_stats_stag": (i, [vp, fab, fab, pfab, pfab, P(FhdStats), C.c_int64, i]),
         "fhd_batch_create": (i, [P(vp), i, i, i]),
         "fhd_batch_destroy": (i, [vp]),
         "fhd_batch_set_stream": (i, [vp, vp]),

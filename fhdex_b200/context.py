@@ -148,6 +148,15 @@ class Context:
                                         *args, C.byref(nz) if nz is not None else None, dt, step)
         check(rc, "fhd_rk3_step_stag")
 
+    def stats_stag(self, st: StagState, stats, steps: int, flags: int = 15):
+        """evaluateStatsStag3D's per-cell update (fhd_stats_stag) with sample count
+        `steps` (1 for the first sample after a reset); flags = capi.STATS_*."""
+        self._stream()
+        s = stats.c_struct()
+        self._stats_struct = s
+        check(self.lib.fhd_stats_stag(self._h, st.cu.fab(), st.prim.fab(), st.vel_fabs(), st.mom_fabs(),
+                                      C.byref(s), steps, flags), "fhd_stats_stag")
+
     def init_state(self, st: StagState):
         """main_driver init: InitConsVarStag -> conservedToPrimitiveStag -> FillBoundary."""
         self.init_cons_var_stag(st)

@@ -626,6 +626,36 @@ int fhd_rk3_step_stag(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim
     return fill_ghosts(g, ng, c->prm.n_cells, c->stream);
 }
 
+int fhd_stats_stag(fhd_ctx* c, fhd_fab cu, fhd_fab prim, const fhd_fab vel[3], const fhd_fab mom[3],
+                   const fhd_stats* st, int64_t steps, int flags) {
+    (void)vel;  // the reference's per-cell statistics take vel but read only the momenta
+    if (!c || !mom || !st || steps < 1) return FHD_ERR_BAD_ARG;
+    const bool means = flags & FHD_STATS_MEANS, vars = flags & FHD_STATS_VARS;
+    if (vars && !means) return FHD_ERR_BAD_ARG;  // statsStag.cpp:38-39
+    const int ns = c->prm.nspecies, nvars = 5 + ns, nprim = 6 + 2 * ns;
+    if (!fab_ok(c, cu, CELLN, NGC, nvars, FHD_F64) || !fab_ok(c, prim, CELLN, 0, nprim, FHD_F64)) return FHD_ERR_BAD_ARG;
+    for (int d = 0; d < 3; ++d) {
+        if (!fab_ok(c, mom[d], FACEN[d], 0, 1, FHD_F64)) return FHD_ERR_BAD_ARG;
+        if (!fab_ok(c, st->velMeans[d], FACEN[d], 0, 1, FHD_F64) || !fab_ok(c, st->cumomMeans[d], FACEN[d], 0, 1, FHD_F64))
+            return FHD_ERR_BAD_ARG;
+        if (vars && (!fab_ok(c, st->velVars[d], FACEN[d], 0, 1, FHD_F64) ||
+                     !fab_ok(c, st->cumomVars[d], FACEN[d], 0, 1, FHD_F64)))
+            return FHD_ERR_BAD_ARG;
+    }
+    if (!fab_ok(c, st->cuMeans, CELLN, NGC, nvars, FHD_F64) || !fab_ok(c, st->primMeans, CELLN, 0, nprim + 3, FHD_F64))
+        return FHD_ERR_BAD_ARG;
+    if (vars) {
+        if (!fab_ok(c, st->cuVars, CELLN, 0, nvars, FHD_F64) || !fab_ok(c, st->primVars, CELLN, 0, nprim + 5, FHD_F64) ||
+            !fab_ok(c, st->coVars, CELLN, 0, 26, FHD_F64))
+            return FHD_ERR_BAD_ARG;
+        if ((flags & FHD_STATS_MOM3) && !fab_ok(c, st->mom3, CELLN, 0, nvars + 1, FHD_F64)) return FHD_ERR_BAD_ARG;
+        if ((flags & FHD_STATS_MOM4) && !fab_ok(c, st->mom4, CELLN, 0, nvars + 1, FHD_F64)) return FHD_ERR_BAD_ARG;
+    }
+    cudaSetDevice(c->device);
+    const DevParams P = make_dev(c, 1.0, 0);
+    return exact_stats(P, cu, prim, mom, *st, steps, flags, c->stream);
+}
+
 int fhd_profile(fhd_ctx* c, int enable) {
     if (!c) return FHD_ERR_BAD_ARG;
     c->prof = enable != 0;

@@ -57,6 +57,9 @@ struct GhostReq {
     int c0, nc;
 };
 int fill_ghosts(const GhostReq* reqs, int n, const int ncell[3], cudaStream_t s);
+// running statistics (fhd_stats.cu, exact TU)
+int exact_stats(const DevParams& P, const fhd_fab& cu, const fhd_fab& prim, const fhd_fab mom[3],
+                const fhd_stats& st, int64_t steps, int flags, cudaStream_t s);
 int override_sync(const fhd_fab& f, const int ncell[3], cudaStream_t s);
 int noise_fill(const DevParams& P, const fhd_fab& f, int c0, int nc, double mean, double sd, uint32_t fid0, int use_b,
                cudaStream_t s);

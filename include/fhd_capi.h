@@ -254,6 +254,37 @@ int fhd_batch_size(const fhd_batch* batch);
 int fhd_batch_member_status(fhd_batch* batch, int member);
 int fhd_batch_synchronize(fhd_batch* batch);
 
+/* ---- running statistics ----------------------------------------------------------
+ * The per-cell part of evaluateStatsStag3D (statsStag.cpp:10-77), which the
+ * reference's time loop calls after every step (main_driver.cpp:1235-1241):
+ * EvaluateStatsMeans (statsStag.cpp:200-365) and EvaluateVarsCoVarsMom3
+ * (:367-691), each followed by the reference's FillBoundary of the cell-centred
+ * means/variances.  Without surface coverage (nspec_surfcov = 0) and without
+ * the yz-averaged spatial cross-correlations (plot_cross).  Fabs have the
+ * reference's shapes (main_driver.cpp:646-714): cuMeans/cuVars nvars comps,
+ * primMeans nprimvars+3 comps, primVars nprimvars+5 comps, coVars 26 comps,
+ * mom3/mom4 nvars+1 comps, all cell-centred; velMeans/velVars/cumomMeans/
+ * cumomVars nodal in d.  cu and cuMeans need ghost width >= 2 (the density mean
+ * is also updated on two ghost layers, as the reference does); the others may
+ * have any ghost width (their ghosts are refilled periodically).  The variance
+ * fabs and mom3/mom4 may be empty when their flags are off. */
+typedef struct {
+    fhd_fab cuMeans, cuVars, primMeans, primVars, coVars, mom3, mom4;
+    fhd_fab velMeans[3], velVars[3], cumomMeans[3], cumomVars[3];
+} fhd_stats;
+
+/* flags of fhd_stats_stag (the reference's plot_means, plot_vars/plot_covars,
+ * plot_mom3, plot_mom4 inputs) */
+enum { FHD_STATS_MEANS = 1, FHD_STATS_VARS = 2, FHD_STATS_MOM3 = 4, FHD_STATS_MOM4 = 8 };
+
+/* One statistics update with sample count `steps` (the reference's statsCount,
+ * 1 for the first sample after a reset): stepsminusone = steps - 1 and
+ * stepsinv = 1/steps weight every running average.  FHD_STATS_VARS without
+ * FHD_STATS_MEANS is rejected (the reference aborts).  cu/prim/vel/mom are the
+ * state after the step, with filled ghosts. */
+int fhd_stats_stag(fhd_ctx* ctx, fhd_fab cu, fhd_fab prim, const fhd_fab vel[3], const fhd_fab mom[3],
+                   const fhd_stats* stats, int64_t steps, int flags);
+
 /* RK3stepStag without any device allocation, for callers that cannot allocate:
  * code whose device memory is owned by an arena that a stray cudaMalloc would
  * fail or fragment, framework callbacks that forbid allocation on their hot

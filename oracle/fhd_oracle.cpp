@@ -1209,6 +1209,214 @@ int orc_fill_random_normal(fhd_fab mf_, int scomp, int ncomp, double mean, doubl
     return FHD_OK;
 }
 
+// evaluateStatsStag3D's per-cell statistics (statsStag.cpp:10-77) without surface
+// coverage or spatial correlations: EvaluateStatsMeans (:200-365) then
+// FillBoundary of the cell means, EvaluateVarsCoVarsMom3 (:367-691) then
+// FillBoundary of the cell variances, each loop in the reference's order.
+// flags as fhd_stats_stag.
+int orc_stats_stag(fhd_fab cu_, fhd_fab prim_, const fhd_fab* mom_, const fhd_stats* st, int64_t steps, int flags) {
+    const int* N = g.n;
+    const int ns = g.ns, nvars = 5 + ns, nprimvars = 6 + 2 * ns;
+    Fab cu(cu_), prim(prim_), cumeans(st->cuMeans), primmeans(st->primMeans);
+    Fab mom[3] = {Fab(mom_[0]), Fab(mom_[1]), Fab(mom_[2])};
+    Fab mm[3] = {Fab(st->cumomMeans[0]), Fab(st->cumomMeans[1]), Fab(st->cumomMeans[2])};
+    Fab vm[3] = {Fab(st->velMeans[0]), Fab(st->velMeans[1]), Fab(st->velMeans[2])};
+    const double stepsminusone = steps - 1.;
+    const double stepsinv = 1. / steps;
+    const bool means = flags & FHD_STATS_MEANS, vars = flags & FHD_STATS_VARS;
+    if (vars && !means) return FHD_ERR_BAD_ARG;
+    if (means) {
+        // mean momentum on faces (:215-243)
+        for (int d = 0; d < 3; ++d)
+            for (int k = 0; k < N[2] + (d == 2); ++k)
+                for (int j = 0; j < N[1] + (d == 1); ++j)
+                    for (int i = 0; i < N[0] + (d == 0); ++i)
+                        mm[d](i, j, k) = (mm[d](i, j, k) * stepsminusone + mom[d](i, j, k)) * stepsinv;
+        // mean density on the cells grown by ngc = 2 (:245-256)
+        for (int k = -2; k < N[2] + 2; ++k)
+            for (int j = -2; j < N[1] + 2; ++j)
+                for (int i = -2; i < N[0] + 2; ++i)
+                    cumeans(i, j, k, 0) = (cumeans(i, j, k, 0) * stepsminusone + cu(i, j, k, 0)) * stepsinv;
+        // other means (:258-317)
+        for (int k = 0; k < N[2]; ++k)
+            for (int j = 0; j < N[1]; ++j)
+                for (int i = 0; i < N[0]; ++i) {
+                    double fracvec[MAXS];
+                    const Fab &mxm = mm[0], &mym = mm[1], &mzm = mm[2];
+                    cumeans(i, j, k, 1) = 0.5 * (mxm(i, j, k) + mxm(i + 1, j, k));
+                    cumeans(i, j, k, 2) = 0.5 * (mym(i, j, k) + mym(i, j + 1, k));
+                    cumeans(i, j, k, 3) = 0.5 * (mzm(i, j, k) + mzm(i, j, k + 1));
+                    cumeans(i, j, k, 4) = (cumeans(i, j, k, 4) * stepsminusone + cu(i, j, k, 4)) * stepsinv;
+                    for (int l = 5; l < nvars; ++l) {
+                        cumeans(i, j, k, l) = (cumeans(i, j, k, l) * stepsminusone + cu(i, j, k, l)) * stepsinv;
+                        fracvec[l - 5] = cumeans(i, j, k, l) / cumeans(i, j, k, 0);
+                        primmeans(i, j, k, l + 1) = fracvec[l - 5];
+                    }
+                    for (int l = 0; l < ns; ++l)
+                        primmeans(i, j, k, 6 + ns + l) =
+                            (primmeans(i, j, k, 6 + ns + l) * stepsminusone + prim(i, j, k, 6 + ns + l)) * stepsinv;
+                    double densitymeaninv = 1.0 / cumeans(i, j, k, 0);
+                    primmeans(i, j, k, 1) = densitymeaninv * 0.5 * (mxm(i, j, k) + mxm(i + 1, j, k));
+                    primmeans(i, j, k, 2) = densitymeaninv * 0.5 * (mym(i, j, k) + mym(i, j + 1, k));
+                    primmeans(i, j, k, 3) = densitymeaninv * 0.5 * (mzm(i, j, k) + mzm(i, j, k + 1));
+                    for (int c = 0; c < 3; ++c)
+                        primmeans(i, j, k, nprimvars + c) =
+                            (primmeans(i, j, k, nprimvars + c) * stepsminusone + prim(i, j, k, 1 + c)) * stepsinv;
+                    primmeans(i, j, k, 0) = cumeans(i, j, k, 0);
+                    primmeans(i, j, k, 4) = (primmeans(i, j, k, 4) * stepsminusone + prim(i, j, k, 4)) * stepsinv;
+                    GetPressureGas(primmeans(i, j, k, 5), fracvec, cumeans(i, j, k, 0), primmeans(i, j, k, 4));
+                }
+        // mean face velocities (:320-363)
+        for (int d = 0; d < 3; ++d) {
+            const int e0 = d == 0, e1 = d == 1, e2 = d == 2;
+            for (int k = 0; k < N[2] + e2; ++k)
+                for (int j = 0; j < N[1] + e1; ++j)
+                    for (int i = 0; i < N[0] + e0; ++i) {
+                        double densitymeaninv = 2.0 / (cumeans(i - e0, j - e1, k - e2, 0) + cumeans(i, j, k, 0));
+                        vm[d](i, j, k) = mm[d](i, j, k) * densitymeaninv;
+                    }
+        }
+        fill_boundary(cumeans);
+        fill_boundary(primmeans);
+    }
+    if (vars) {
+        Fab cuvars(st->cuVars), primvars(st->primVars), covars(st->coVars);
+        Fab mv[3] = {Fab(st->cumomVars[0]), Fab(st->cumomVars[1]), Fab(st->cumomVars[2])};
+        Fab vv[3] = {Fab(st->velVars[0]), Fab(st->velVars[1]), Fab(st->velVars[2])};
+        // momentum and velocity variances (:387-435)
+        for (int d = 0; d < 3; ++d) {
+            const int e0 = d == 0, e1 = d == 1, e2 = d == 2;
+            for (int k = 0; k < N[2] + e2; ++k)
+                for (int j = 0; j < N[1] + e1; ++j)
+                    for (int i = 0; i < N[0] + e0; ++i) {
+                        double delj = mom[d](i, j, k) - mm[d](i, j, k);
+                        mv[d](i, j, k) = (mv[d](i, j, k) * stepsminusone + delj * delj) * stepsinv;
+                        double densitymeaninv = 2.0 / (cumeans(i - e0, j - e1, k - e2, 0) + cumeans(i, j, k, 0));
+                        double delrho = 0.5 * (cu(i - e0, j - e1, k - e2, 0) + cu(i, j, k, 0)) -
+                                        0.5 * (cumeans(i - e0, j - e1, k - e2, 0) + cumeans(i, j, k, 0));
+                        double delvel = (delj - vm[d](i, j, k) * delrho) * densitymeaninv;
+                        vv[d](i, j, k) = (vv[d](i, j, k) * stepsminusone + delvel * delvel) * stepsinv;
+                    }
+        }
+        // cell variances and covariances (:438-613)
+        for (int k = 0; k < N[2]; ++k)
+            for (int j = 0; j < N[1]; ++j)
+                for (int i = 0; i < N[0]; ++i) {
+                    const Fab &momx = mom[0], &momy = mom[1], &momz = mom[2];
+                    const Fab &momxmeans = mm[0], &momymeans = mm[1], &momzmeans = mm[2];
+                    double delrho = cu(i, j, k, 0) - cumeans(i, j, k, 0);
+                    cuvars(i, j, k, 0) = (cuvars(i, j, k, 0) * stepsminusone + delrho * delrho) * stepsinv;
+                    double delenergy = cu(i, j, k, 4) - cumeans(i, j, k, 4);
+                    cuvars(i, j, k, 4) = (cuvars(i, j, k, 4) * stepsminusone + delenergy * delenergy) * stepsinv;
+                    for (int l = 5; l < nvars; ++l) {
+                        double delmassvec = cu(i, j, k, l) - cumeans(i, j, k, l);
+                        cuvars(i, j, k, l) = (cuvars(i, j, k, l) * stepsminusone + delmassvec * delmassvec) * stepsinv;
+                    }
+                    double delrhoYk[MAXS], Ykmean[MAXS], delYk[MAXS];
+                    for (int s = 0; s < ns; ++s) {
+                        delrhoYk[s] = cu(i, j, k, 5 + s) - cumeans(i, j, k, 5 + s);
+                        Ykmean[s] = primmeans(i, j, k, 6 + s);
+                        delYk[s] = (delrhoYk[s] - Ykmean[s] * delrho) / cumeans(i, j, k, 0);
+                        primvars(i, j, k, 6 + s) = (primvars(i, j, k, 6 + s) * stepsminusone + delYk[s] * delYk[s]) * stepsinv;
+                    }
+                    primvars(i, j, k, 0) = cuvars(i, j, k, 0);
+                    double vx = 0.5 * (vm[0](i, j, k) + vm[0](i + 1, j, k));
+                    double vy = 0.5 * (vm[1](i, j, k) + vm[1](i, j + 1, k));
+                    double vz = 0.5 * (vm[2](i, j, k) + vm[2](i, j, k + 1));
+                    double T = primmeans(i, j, k, 4);
+                    double densitymeaninv = 1.0 / cumeans(i, j, k, 0);
+                    double cv = 0.;
+                    for (int l = 0; l < ns; ++l) cv = cv + g.hcv[l] * cumeans(i, j, k, 5 + l) / cumeans(i, j, k, 0);
+                    double cvinv = 1.0 / cv;
+                    double qmean = cv * T - 0.5 * (vx * vx + vy * vy + vz * vz);
+                    double deljx = 0.5 * (momx(i, j, k) + momx(i + 1, j, k)) - 0.5 * (momxmeans(i, j, k) + momxmeans(i + 1, j, k));
+                    double deljy = 0.5 * (momy(i, j, k) + momy(i, j + 1, k)) - 0.5 * (momymeans(i, j, k) + momymeans(i, j + 1, k));
+                    double deljz = 0.5 * (momz(i, j, k) + momz(i, j, k + 1)) - 0.5 * (momzmeans(i, j, k) + momzmeans(i, j, k + 1));
+                    cuvars(i, j, k, 1) = (cuvars(i, j, k, 1) * stepsminusone + deljx * deljx) * stepsinv;
+                    cuvars(i, j, k, 2) = (cuvars(i, j, k, 2) * stepsminusone + deljy * deljy) * stepsinv;
+                    cuvars(i, j, k, 3) = (cuvars(i, j, k, 3) * stepsminusone + deljz * deljz) * stepsinv;
+                    double delvelx = (deljx - vx * delrho) * densitymeaninv;
+                    double delvely = (deljy - vy * delrho) * densitymeaninv;
+                    double delvelz = (deljz - vz * delrho) * densitymeaninv;
+                    primvars(i, j, k, 1) = (primvars(i, j, k, 1) * stepsminusone + delvelx * delvelx) * stepsinv;
+                    primvars(i, j, k, 2) = (primvars(i, j, k, 2) * stepsminusone + delvely * delvely) * stepsinv;
+                    primvars(i, j, k, 3) = (primvars(i, j, k, 3) * stepsminusone + delvelz * delvelz) * stepsinv;
+                    double delg = vx * deljx + vy * deljy + vz * deljz;
+                    const int np = nprimvars;
+                    primvars(i, j, k, np + 0) = (primvars(i, j, k, np + 0) * stepsminusone + delg * delg) * stepsinv;
+                    primvars(i, j, k, np + 1) = (primvars(i, j, k, np + 1) * stepsminusone + delg * delenergy) * stepsinv;
+                    primvars(i, j, k, np + 2) = (primvars(i, j, k, np + 2) * stepsminusone + delrho * delenergy) * stepsinv;
+                    primvars(i, j, k, np + 3) = (primvars(i, j, k, np + 3) * stepsminusone + delrho * delg) * stepsinv;
+                    primvars(i, j, k, np + 4) =
+                        (primvars(i, j, k, np + 4) * stepsminusone +
+                         cvinv * cvinv * densitymeaninv * densitymeaninv *
+                             (cuvars(i, j, k, 4) + primvars(i, j, k, np + 0) - 2 * primvars(i, j, k, np + 1) +
+                              qmean * (qmean * cuvars(i, j, k, 0) - 2 * primvars(i, j, k, np + 2) +
+                                       2 * primvars(i, j, k, np + 3)))) *
+                        stepsinv;
+                    double delT = prim(i, j, k, 4) - primmeans(i, j, k, 4);
+                    primvars(i, j, k, 4) = (primvars(i, j, k, 4) * stepsminusone + delT * delT) * stepsinv;
+                    double deltemp = delT;
+                    const double terms[26] = {
+                        delrho * deljx, delrho * deljy, delrho * deljz, deljx * deljy, deljy * deljz, deljx * deljz,
+                        delrho * delenergy, deljx * delenergy, deljy * delenergy, deljz * delenergy,
+                        delrhoYk[0] * delrhoYk[ns - 1], delrho * delvelx, delrho * delvely, delrho * delvelz,
+                        delvelx * delvely, delvely * delvelz, delvelx * delvelz, delrho * deltemp, delvelx * deltemp,
+                        delvely * deltemp, delvelz * deltemp, delYk[0] * delYk[ns - 1], delYk[0] * delvelx,
+                        delYk[ns - 1] * delvelx, delrhoYk[0] * delvelx, delrhoYk[ns - 1] * delvelx};
+                    for (int c = 0; c < 26; ++c)
+                        covars(i, j, k, c) = (covars(i, j, k, c) * stepsminusone + terms[c]) * stepsinv;
+                }
+        // third and fourth moments (:616-689)
+        const bool m3on = flags & FHD_STATS_MOM3, m4on = flags & FHD_STATS_MOM4;
+        if (m3on || m4on) {
+            Fab m3(st->mom3), m4(st->mom4);
+            for (int k = 0; k < N[2]; ++k)
+                for (int j = 0; j < N[1]; ++j)
+                    for (int i = 0; i < N[0]; ++i) {
+                        double delrho = cu(i, j, k, 0) - cumeans(i, j, k, 0);
+                        if (m3on) m3(i, j, k, 0) = (m3(i, j, k, 0) * stepsminusone + delrho * delrho * delrho) * stepsinv;
+                        if (m4on) m4(i, j, k, 0) = (m4(i, j, k, 0) * stepsminusone + delrho * delrho * delrho * delrho) * stepsinv;
+                        double delenergy = cu(i, j, k, 4) - cumeans(i, j, k, 4);
+                        if (m3on) m3(i, j, k, 4) = (m3(i, j, k, 4) * stepsminusone + delenergy * delenergy * delenergy) * stepsinv;
+                        if (m4on)
+                            m4(i, j, k, 4) =
+                                (m4(i, j, k, 4) * stepsminusone + delenergy * delenergy * delenergy * delenergy) * stepsinv;
+                        double delrhoYk[MAXS], delYk[MAXS];
+                        for (int s = 0; s < ns; ++s) {
+                            delrhoYk[s] = cu(i, j, k, 5 + s) - cumeans(i, j, k, 5 + s);
+                            double Ykmean = primmeans(i, j, k, 6 + s);
+                            delYk[s] = (delrhoYk[s] - Ykmean * delrho) / cumeans(i, j, k, 0);
+                            if (m3on) m3(i, j, k, 5 + s) = (m3(i, j, k, 5 + s) * stepsminusone + delYk[s] * delYk[s] * delYk[s]) * stepsinv;
+                            if (m4on)
+                                m4(i, j, k, 5 + s) =
+                                    (m4(i, j, k, 5 + s) * stepsminusone + delYk[s] * delYk[s] * delYk[s] * delYk[s]) * stepsinv;
+                        }
+                        double vx = 0.5 * (vm[0](i, j, k) + vm[0](i + 1, j, k));
+                        double vy = 0.5 * (vm[1](i, j, k) + vm[1](i, j + 1, k));
+                        double vz = 0.5 * (vm[2](i, j, k) + vm[2](i, j, k + 1));
+                        double densitymeaninv = 1.0 / cumeans(i, j, k, 0);
+                        double deljx = 0.5 * (mom[0](i, j, k) + mom[0](i + 1, j, k)) - 0.5 * (mm[0](i, j, k) + mm[0](i + 1, j, k));
+                        double deljy = 0.5 * (mom[1](i, j, k) + mom[1](i, j + 1, k)) - 0.5 * (mm[1](i, j, k) + mm[1](i, j + 1, k));
+                        double deljz = 0.5 * (mom[2](i, j, k) + mom[2](i, j, k + 1)) - 0.5 * (mm[2](i, j, k) + mm[2](i, j, k + 1));
+                        double dv[3] = {(deljx - vx * delrho) * densitymeaninv, (deljy - vy * delrho) * densitymeaninv,
+                                        (deljz - vz * delrho) * densitymeaninv};
+                        for (int c = 0; c < 3; ++c) {
+                            if (m3on) m3(i, j, k, 1 + c) = (m3(i, j, k, 1 + c) * stepsminusone + dv[c] * dv[c] * dv[c]) * stepsinv;
+                            if (m4on)
+                                m4(i, j, k, 1 + c) = (m4(i, j, k, 1 + c) * stepsminusone + dv[c] * dv[c] * dv[c] * dv[c]) * stepsinv;
+                        }
+                        double delT = prim(i, j, k, 4) - primmeans(i, j, k, 4);
+                        if (m3on) m3(i, j, k, 5 + ns) = (m3(i, j, k, 5 + ns) * stepsminusone + delT * delT * delT) * stepsinv;
+                        if (m4on) m4(i, j, k, 5 + ns) = (m4(i, j, k, 5 + ns) * stepsminusone + delT * delT * delT * delT) * stepsinv;
+                    }
+        }
+        fill_boundary(cuvars);
+        fill_boundary(primvars);
+    }
+    return FHD_OK;
+}
+
 // Host-drawn noise for injected-noise runs: one std::mt19937_64(seed) engine
 // (the generator the C++ standard specifies), Box-Muller on 53-bit uniforms,
 // filling in a fixed order: for A then B, for d = 0..2: face[d] (all its

@@ -11,7 +11,7 @@ import ctypes as C
 import os
 import subprocess
 
-from fhdex_b200.capi import FabArr3, FabArr6, FhdFab, FhdNoise, FhdParams
+from fhdex_b200.capi import FabArr3, FabArr6, FhdFab, FhdNoise, FhdParams, FhdStats
 from fhdex_b200.fab import fab_array
 
 _DIR = os.path.dirname(os.path.abspath(__file__))
@@ -48,6 +48,7 @@ def lib():
         L.orc_philox4x32_10.argtypes = [P(C.c_uint32), P(C.c_uint32), P(C.c_uint32)]
         L.orc_philox4x32_10.restype = None
         L.orc_fill_noise_mt64.argtypes = [P(FhdNoise), C.c_uint64]
+        L.orc_stats_stag.argtypes = [fab, fab, pfab, P(FhdStats), C.c_int64, i]
         L.orc_set_threads.argtypes = [i]
         L.orc_set_threads.restype = i
         L.orc_max_acoustic_cfl.argtypes = [fab, pfab, d]
@@ -132,6 +133,14 @@ def fill_step_noise(noise, seed, step):
             fill_random_normal(noise.face[s][d], 0, ns + 1, 0.0, 1.0, seed, (step << 8) | sid); sid += 1
             fill_random_normal(noise.edge[s][d], 0, 1, 0.0, 1.0, seed, (step << 8) | sid); sid += 1
             fill_random_normal(noise.cen[s][d], 0, 1, 0.0, 2.0, seed, (step << 8) | sid); sid += 1
+
+
+def stats_stag(st, stats, steps, flags=15):
+    """evaluateStatsStag3D's per-cell statistics (statsStag.cpp:10-77) on host
+    MultiFabs; returns the FHD_* code."""
+    set_params(st.p)
+    s = stats.c_struct()
+    return lib().orc_stats_stag(st.cu.fab(), st.prim.fab(), st.mom_fabs(), C.byref(s), steps, flags)
 
 
 def set_threads(n=0):

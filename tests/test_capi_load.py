@@ -35,13 +35,14 @@ def test_every_declared_entry_point_is_exported():
 def test_struct_layouts_match_header(tmp_path):
     src = tmp_path / "sz.c"
     src.write_text(f'#include "{HEADER}"\n#include <stdio.h>\n#include <stddef.h>\n'
-                   'int main(){printf("%zu %zu %zu %zu\\n", sizeof(fhd_fab), sizeof(fhd_params), '
-                   'sizeof(fhd_noise), offsetof(fhd_params, seed));return 0;}\n')
+                   'int main(){printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(fhd_fab), sizeof(fhd_params), '
+                   'sizeof(fhd_noise), offsetof(fhd_params, seed), sizeof(fhd_stats), '
+                   'offsetof(fhd_stats, cumomVars));return 0;}\n')
     exe = tmp_path / "sz"
     subprocess.check_call(["gcc", str(src), "-o", str(exe)])
     vals = [int(x) for x in subprocess.check_output([str(exe)]).split()]
     assert vals == [C.sizeof(capi.FhdFab), C.sizeof(capi.FhdParams), C.sizeof(capi.FhdNoise),
-                    capi.FhdParams.seed.offset]
+                    capi.FhdParams.seed.offset, C.sizeof(capi.FhdStats), capi.FhdStats.cumomVars.offset]
 
 
 def test_strerror_is_callable_without_gpu():
