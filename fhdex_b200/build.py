@@ -36,6 +36,7 @@ def _units():
     u.append(("noalloc", "fhd_noalloc.cu", ["-fmad=false"]))
     u.append(("batch", "fhd_batch.cu", ["-fmad=false"]))
     u.append(("stats", "fhd_stats.cu", ["-fmad=false"]))
+    u.append(("sf", "fhd_sf.cu", ["-fmad=false"]))
     return u
 
 
@@ -73,7 +74,9 @@ def build(verbose=False, jobs=None):
     objs = [o for o, _ in results]
     rebuilt = [n for _, n in results if n]
     if rebuilt or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs
+        cudalib = os.path.join(os.path.dirname(os.path.dirname(NVCC)), "lib64")
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-L" + cudalib, "-lcufft", "-Xlinker",
+                                                             "-rpath=" + cudalib]
         subprocess.check_call(cmd)
     return LIB
 

@@ -132,6 +132,14 @@ def _declare(lib):
         "fhd_profile_read": (i, [vp, P(d), P(C.c_int64)]),
         "fhd_rk3_step_stag_noalloc": (i, [P(FhdParams), fab, pfab, fab, pfab, d, C.c_int64, vp, P(i)]),
         "fhd_stats_stag": (i, [vp, fab, fab, pfab, pfab, P(FhdStats), C.c_int64, i]),
+        "fhd_sf_create": (i, [P(vp), P(i), i, i, P(i), P(i), P(d), i]),
+        "fhd_sf_destroy": (i, [vp]),
+        "fhd_sf_set_stream": (i, [vp, vp]),
+        "fhd_sf_synchronize": (i, [vp]),
+        "fhd_sf_ncov": (i, [vp]),
+        "fhd_sf_nsamples": (C.c_int64, [vp]),
+        "fhd_sf_fort_structure": (i, [vp, fab, i]),
+        "fhd_sf_finalize": (i, [vp, fab, fab, fab, i]),
         "fhd_batch_create": (i, [P(vp), i, i, i]),
         "fhd_batch_destroy": (i, [vp]),
         "fhd_batch_set_stream": (i, [vp, vp]),

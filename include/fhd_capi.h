@@ -285,6 +285,33 @@ enum { FHD_STATS_MEANS = 1, FHD_STATS_VARS = 2, FHD_STATS_MOM3 = 4, FHD_STATS_MO
 int fhd_stats_stag(fhd_ctx* ctx, fhd_fab cu, fhd_fab prim, const fhd_fab vel[3], const fhd_fab mom[3],
                    const fhd_stats* stats, int64_t steps, int flags);
 
+/* ---- static structure factor -------------------------------------------------------
+ * StructFact (src_analysis/StructFact.H, StructFact.cpp) for one periodic box of
+ * n_cells cells: covariances of the Fourier transforms of cell-centred
+ * variables, accumulated over samples.  Pairs (pairA[c], pairB[c]), c < ncov,
+ * index the components of the `variables` fab; pairA == NULL selects all
+ * nvar (nvar + 1) / 2 pairs (A = j, B = i for i <= j) as the reference's define
+ * without pairs does (StructFact.cpp:45-69).  var_scaling has one entry per pair
+ * (the result is divided by it).  The accumulators live in device memory owned
+ * by the object (2 x ncov doubles per cell). */
+typedef struct fhd_sf fhd_sf;
+int fhd_sf_create(fhd_sf** sf, const int n_cells[3], int nvar, int ncov, const int* pairA, const int* pairB,
+                  const double* var_scaling, int device);
+int fhd_sf_destroy(fhd_sf* sf);
+int fhd_sf_set_stream(fhd_sf* sf, void* stream);
+int fhd_sf_synchronize(fhd_sf* sf);
+int fhd_sf_ncov(const fhd_sf* sf);
+int64_t fhd_sf_nsamples(const fhd_sf* sf);
+/* StructFact::FortStructure (StructFact.cpp:231-311): one sample from the
+ * cell-centred `variables` fab (nvar components, any ghost width, device
+ * memory); reset = 1 restarts the accumulation with this sample. */
+int fhd_sf_fort_structure(fhd_sf* sf, fhd_fab variables, int reset);
+/* StructFact::CallFinalize (StructFact.cpp:598-641): the averaged covariances,
+ * zero_avg = 1 zeroes k = 0, shifted so that k = 0 sits at n_cells/2, scaled by
+ * 1/var_scaling, into cell-centred fabs of ncov components (real, imaginary,
+ * magnitude).  The accumulators are left unchanged. */
+int fhd_sf_finalize(fhd_sf* sf, fhd_fab cov_real, fhd_fab cov_imag, fhd_fab cov_mag, int zero_avg);
+
 /* RK3stepStag without any device allocation, for callers that cannot allocate:
  * code whose device memory is owned by an arena that a stray cudaMalloc would
  * fail or fragment, framework callbacks that forbid allocation on their hot
