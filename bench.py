@@ -433,6 +433,55 @@ def run_stats(args):
                       "clocks": clk}), flush=True)
 
 
+def run_sf(args):
+    """Static structure factor (fhd_sf_fort_structure): rho, rhoE, T and jx of the
+    stepped state, all 10 pairs, --steps samples timed with CUDA events."""
+    import torch
+    from fhdex_b200.context import Context
+    from fhdex_b200.fab import CELL, MultiFab
+    from fhdex_b200.params import stable_dt
+    from fhdex_b200.state import StagState
+    from fhdex_b200.structfact import StructFact
+    torch.cuda.set_device(0)
+    p = make_params(args)
+    ctx = Context(p, 0)
+    st = StagState(p, "cuda:0", aux=False)
+    ctx.init_state(st)
+    ctx.rk3_step(st, stable_dt(p), 0, aux=False)
+    nvar = 4
+    var = MultiFab(p.n_cells, CELL, nvar, 0, device="cuda:0")
+    var.valid(0).copy_(st.cu.valid(0))
+    var.valid(1).copy_(st.cu.valid(4))
+    var.valid(2).copy_(st.prim.valid(4))
+    var.valid(3).copy_(st.cu.valid(1))
+    sf = StructFact(p.n_cells, ["rho", "rhoE", "T", "jx"], [1.0] * (nvar * (nvar + 1) // 2))
+    for s in range(args.warmup):
+        sf.fort_structure(var)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for s in range(args.steps):
+        sf.fort_structure(var)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    cells = p.n_cells[0] * p.n_cells[1] * p.n_cells[2]
+    # per point: pack (read + write 8 B), FFT (read 8 B, write the 8 B half spectrum) and
+    # the accumulation's spectrum read (8 B) per variable; covariance read + write per pair
+    alg = cells * (40 * nvar + 32 * sf.ncov)
+    peak, peak_kind = measured_peak()
+    achieved = alg / (ms / 1e3) / 1e9
+    print(json.dumps({"mode": "sf", "metric": "structure-factor samples x cells / s", "unit": "cell-samples/s",
+                      "value": cells / (ms / 1e3), "ms_per_sample": ms, "steps": args.steps, "nvar": nvar,
+                      "ncov": sf.ncov, "config": {"workload": f"StructFact of 4 variables, 10 pairs, "
+                                                              f"{p.n_cells[0]}^3"},
+                      "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                                   "frac": achieved / peak, "peak_kind": peak_kind,
+                                   "algorithmic_bytes_per_launch": alg,
+                                   "kernel": "4 x (k_sf_pack + cuFFT D2Z) + k_sf_accumulate"}}), flush=True)
+    sf.close()
+
+
 def run_ensemble(args):
     """Batched ensemble: --members realisations of argon, half 32^3 and half 64^3,
     T0 ~ U(250,350) K, rho0 ~ U(1e-3,3e-3) g/cm^3, one graph replay per step."""
@@ -488,7 +537,7 @@ def run_serve(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--mode", default="step", choices=["step", "ensemble", "serve", "stats"])
+    ap.add_argument("--mode", default="step", choices=["step", "ensemble", "serve", "stats", "sf"])
     ap.add_argument("--members", type=int, default=512)
     ap.add_argument("--requests", type=int, default=48)
     ap.add_argument("--rate", type=float, default=50.0)
@@ -518,6 +567,8 @@ def main():
         run_serve(args)
     elif args.mode == "stats":
         run_stats(args)
+    elif args.mode == "sf":
+        run_sf(args)
     else:
         run_ours(args)
 
