@@ -16,6 +16,12 @@
 
 namespace fhd {
 
+// Every kernel here has internal linkage (static): the FP64 units (built with
+// -fmad=false) and the mixed units (-fmad=true) both instantiate the kernels that
+// do not depend on the precision (e.g. k_convert_b<NS>) under the same name.
+// With external linkage a launch could reach the other unit's device code, and
+// which one depends on the order the modules are loaded in.
+
 enum { ST_OK = 0, ST_MASSFRAC = 2, ST_NONFINITE = 3 };
 
 FHD_D void flag(int* status, int code) {
@@ -89,7 +95,7 @@ template <int NS, class R>
 constexpr int cellprep_min_blocks() { return NS <= 2 ? 8 : (sizeof(R) == 8 ? 4 : 6); }
 
 template <int NS, class R>
-__global__ void __launch_bounds__(128, cellprep_min_blocks<NS, R>()) k_cellprep(PrepArgs<NS, R> a) {
+static __global__ void __launch_bounds__(128, cellprep_min_blocks<NS, R>()) k_cellprep(PrepArgs<NS, R> a) {
     const int tot = cellprep_count(a);
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) cellprep_point(a, q);
 }
@@ -171,7 +177,7 @@ FHD_D void taus_point(const StageArgs<NS, R, NZ>& a, int q) {
 }
 
 template <int NS, class R, int NZ>
-__global__ void __launch_bounds__(256) k_taus(StageArgs<NS, R, NZ> a) {
+static __global__ void __launch_bounds__(256) k_taus(StageArgs<NS, R, NZ> a) {
     const int tot = taus_count(a);
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) taus_point(a, q);
 }
@@ -216,7 +222,7 @@ FHD_D void faces_point(const StageArgs<NS, R, NZ>& a, int q) {
 
 // MINB = minimum resident blocks requested from the register allocator.
 template <int NS, class R, int NZ, int D, int BS, int MINB>
-__global__ void __launch_bounds__(BS, MINB) k_faces(StageArgs<NS, R, NZ> a) {
+static __global__ void __launch_bounds__(BS, MINB) k_faces(StageArgs<NS, R, NZ> a) {
     const int tot = faces_count<NS, R, NZ, D>(a);
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x)
         faces_point<NS, R, NZ, D>(a, q);
@@ -300,7 +306,7 @@ FHD_D void update_point(const StageArgs<NS, R, NZ>& a, int q) {
 }
 
 template <int NS, class R, int NZ>
-__global__ void __launch_bounds__(256) k_update(StageArgs<NS, R, NZ> a) {
+static __global__ void __launch_bounds__(256) k_update(StageArgs<NS, R, NZ> a) {
     const int tot = update_count(a);
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) update_point(a, q);
 }
@@ -370,7 +376,7 @@ FHD_D void convert_point(const ConvArgs<NS>& a, int q) {
 }
 
 template <int NS>
-__global__ void __launch_bounds__(128) k_convert(ConvArgs<NS> a) {
+static __global__ void __launch_bounds__(128) k_convert(ConvArgs<NS> a) {
     const int tot = convert_count(a);
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) convert_point(a, q);
 }
@@ -481,7 +487,7 @@ struct TransArgs {
 };
 
 template <int NS>
-__global__ void __launch_bounds__(128) k_transport(TransArgs<NS> a) {
+static __global__ void __launch_bounds__(128) k_transport(TransArgs<NS> a) {
     const DevParams& P = a.P;
     const int g = a.ng;
     const int nx = P.n[0] + 2 * g, ny = P.n[1] + 2 * g, nz = P.n[2] + 2 * g;
@@ -527,7 +533,7 @@ struct AuxArgs {
 
 // faceflux[d] on valid faces; items enumerate the three face boxes back to back
 template <int NS, class R, int NZ>
-__global__ void __launch_bounds__(128) k_aux_faces(AuxArgs<NS, R, NZ> a) {
+static __global__ void __launch_bounds__(128) k_aux_faces(AuxArgs<NS, R, NZ> a) {
     const DevParams& P = a.P;
     const int* N = P.n;
     const int64_t nxf = (int64_t)(N[0] + 1) * N[1] * N[2], nyf = (int64_t)N[0] * (N[1] + 1) * N[2],
@@ -557,7 +563,7 @@ __global__ void __launch_bounds__(128) k_aux_faces(AuxArgs<NS, R, NZ> a) {
 
 // edge fluxes (6 fabs) on valid edges and centre fluxes on cells grown by 1
 template <int NS, class R, int NZ>
-__global__ void __launch_bounds__(128) k_aux_edges_cen(AuxArgs<NS, R, NZ> a) {
+static __global__ void __launch_bounds__(128) k_aux_edges_cen(AuxArgs<NS, R, NZ> a) {
     const DevParams& P = a.P;
     const int* N = P.n;
     const int64_t nxy = (int64_t)(N[0] + 1) * (N[1] + 1) * N[2], nxz = (int64_t)(N[0] + 1) * N[1] * (N[2] + 1),
@@ -656,7 +662,7 @@ FHD_D int member_of(const int* __restrict__ bpref, int nmem) {
 }
 
 template <int NS, class R>
-__global__ void __launch_bounds__(128, cellprep_min_blocks<NS, R>()) k_cellprep_b(const PrepArgs<NS, R>* __restrict__ args,
+static __global__ void __launch_bounds__(128, cellprep_min_blocks<NS, R>()) k_cellprep_b(const PrepArgs<NS, R>* __restrict__ args,
                                                     const int* __restrict__ bpref, int nmem) {
     const int m = member_of(bpref, nmem);
     const PrepArgs<NS, R>& a = args[m];
@@ -665,7 +671,7 @@ __global__ void __launch_bounds__(128, cellprep_min_blocks<NS, R>()) k_cellprep_
 }
 
 template <int NS, class R, int NZ>
-__global__ void __launch_bounds__(128) k_taus_b(const StageArgs<NS, R, NZ>* __restrict__ args,
+static __global__ void __launch_bounds__(128) k_taus_b(const StageArgs<NS, R, NZ>* __restrict__ args,
                                                 const int* __restrict__ bpref, int nmem) {
     const int m = member_of(bpref, nmem);
     const StageArgs<NS, R, NZ>& a = args[m];
@@ -680,7 +686,7 @@ template <int NS>
 constexpr int faces_b_min_blocks() { return NS <= 2 ? 8 : 4; }
 
 template <int NS, class R, int NZ, int D>
-__global__ void __launch_bounds__(128, faces_b_min_blocks<NS>()) k_faces_b(const StageArgs<NS, R, NZ>* __restrict__ args,
+static __global__ void __launch_bounds__(128, faces_b_min_blocks<NS>()) k_faces_b(const StageArgs<NS, R, NZ>* __restrict__ args,
                                                    const int* __restrict__ bpref, int nmem) {
     const int m = member_of(bpref, nmem);
     const StageArgs<NS, R, NZ>& a = args[m];
@@ -689,7 +695,7 @@ __global__ void __launch_bounds__(128, faces_b_min_blocks<NS>()) k_faces_b(const
 }
 
 template <int NS, class R, int NZ>
-__global__ void __launch_bounds__(128) k_update_b(const StageArgs<NS, R, NZ>* __restrict__ args,
+static __global__ void __launch_bounds__(128) k_update_b(const StageArgs<NS, R, NZ>* __restrict__ args,
                                                   const int* __restrict__ bpref, int nmem) {
     const int m = member_of(bpref, nmem);
     const StageArgs<NS, R, NZ>& a = args[m];
@@ -698,7 +704,7 @@ __global__ void __launch_bounds__(128) k_update_b(const StageArgs<NS, R, NZ>* __
 }
 
 template <int NS>
-__global__ void __launch_bounds__(128) k_convert_b(const ConvArgs<NS>* __restrict__ args,
+static __global__ void __launch_bounds__(128) k_convert_b(const ConvArgs<NS>* __restrict__ args,
                                                    const int* __restrict__ bpref, int nmem) {
     const int m = member_of(bpref, nmem);
     const ConvArgs<NS>& a = args[m];

@@ -59,7 +59,7 @@ static __global__ void __launch_bounds__(256) k_stats_means_a(StatsArgs a) {
 
 // pass B: one thread per point of [0, n]^3
 template <int NS>
-__global__ void __launch_bounds__(256) k_stats_means_b(StatsArgs a) {
+static __global__ void __launch_bounds__(256) k_stats_means_b(StatsArgs a) {
     const DevParams& P = a.P;
     const int* n = P.n;
     const int gx = n[0] + 1, gy = n[1] + 1, gz = n[2] + 1;
@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(256) k_stats_means_b(StatsArgs a) {
 // pass C: one thread per point of [0, n]^3.  As in pass B, operands are loaded in
 // groups before the stores they feed, so each thread keeps many loads in flight.
 template <int NS>
-__global__ void __launch_bounds__(256) k_stats_vars(StatsArgs a) {
+static __global__ void __launch_bounds__(256) k_stats_vars(StatsArgs a) {
     const DevParams& P = a.P;
     const int* n = P.n;
     const int gx = n[0] + 1, gy = n[1] + 1, gz = n[2] + 1;

@@ -4,7 +4,9 @@ FP64: bit for bit (the batched kernels run the same point functions in the same
 order with the member's own Philox key and step counter).  Mixed precision: the
 FP32 units are built with FMA contraction, which the compiler may apply
 differently in the batched and the single-run kernels, so members agree with the
-run alone within a norm-relative error of MIXED_TOL per field."""
+run alone within a norm-relative error of MIXED_TOL per field: FP32 rounding
+(6e-8) amplified over the steps, a tenth of the mixed path's own 1e-4 bound
+against the FP64 result."""
 import pytest
 import torch
 
@@ -27,7 +29,7 @@ def alone(p, dt, steps, first=0):
     return st
 
 
-MIXED_TOL = 1e-6
+MIXED_TOL = 1e-5
 
 
 def same(a, b, tol=0.0):
@@ -63,6 +65,30 @@ def test_batch_members_match_runs_alone(precision):
         ref = alone(p, dt, 3)
         tol = 0.0 if precision == 0 else MIXED_TOL
         assert not same(st, ref, tol), (p.n_cells, same(st, ref, tol))
+    b.close()
+
+
+def test_fp64_batch_after_mixed_runs_matches_alone():
+    """FP64 members stay bit-exact after mixed-precision work in the same process.
+    (Kernels that do not depend on the precision are instantiated by both the FP64
+    and the FMA-contracting mixed units; with external linkage a launch could run
+    the mixed unit's copy once that module was loaded.)"""
+    pm = argon(12, dx=8e-6, seed=5, precision=1)
+    alone(pm, stable_dt(pm), 2)                    # loads the mixed kernels
+    bm = Batch(2, 1)
+    sm = StagState(pm, "cuda", aux=False)
+    bm.add(pm, sm, stable_dt(pm))
+    bm.step(2, graph=True)
+    bm.synchronize()
+    bm.close()
+    p = argon(16, dx=8e-6, T_init=260.0, rho0=1.2e-3, seed=11)
+    dt = stable_dt(p)
+    b = Batch(2, 0)
+    st = StagState(p, "cuda", aux=False)
+    b.add(p, st, dt)
+    b.step(3, graph=True)
+    b.synchronize()
+    assert not same(st, alone(p, dt, 3))
     b.close()
 
 
