@@ -243,7 +243,9 @@ FHD_D bool transport_gio(const DevParams& P, R rho, R temperature, R pressure, c
     R sumYk = R(0.);
 #pragma unroll
     for (int n = 0; n < NS; ++n) {
-        if (Yraw[n] <= R(0.) || Yraw[n] >= R(1.)) ok = false;
+        // a single gas has Y = 1 by construction: the range check (transCoeffs.cpp:45-46)
+        // applies to mixtures only
+        if (NS > 1 && (Yraw[n] <= R(0.) || Yraw[n] >= R(1.))) ok = false;
         Yk[n] = clamp01(Yraw[n]);
         sumYk += Yk[n];
     }
@@ -385,10 +387,14 @@ FHD_D bool transport_gio(const DevParams& P, R rho, R temperature, R pressure, c
         for (int j = 0; j < NS; ++j) ch += row[j] * Bi[j];
         c.chi[i] = ch;
     }
-    R Dl[NS * NS];
-    D_GIO1<NS, R>(Dbin, Ykp, Xkp, Dl);
+    if constexpr (NS == 1) {
+        c.D[0] = R(0.);  // a single gas has no species diffusion
+    } else {
+        R Dl[NS * NS];
+        D_GIO1<NS, R>(Dbin, Ykp, Xkp, Dl);
 #pragma unroll
-    for (int q = 0; q < NS * NS; ++q) c.D[q] = Dl[q] * rho;
+        for (int q = 0; q < NS * NS; ++q) c.D[q] = Dl[q] * rho;
+    }
     if (P.visc_type == 3 || P.visc_type == -3) c.zeta = R(P.zeta_ratio) * c.eta;
     return ok;
 }

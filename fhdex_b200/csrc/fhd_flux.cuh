@@ -279,6 +279,8 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
         nz.template face_all<NS + 1>(P, D, i, j, k, wf);
         const R fw0 = dsqrt(R(P.k_B) * kp * R(P.volinv) * R(P.dtinv));
         heat = fw0 * R(wf[0]);
+        // species noise, Soret: mixtures only (a single gas has no species flux)
+        if constexpr (NS > 1) {
         R yy[NS], yyp[NS], DY[NS * NS], sqD[NS * NS], hk[NS], wien[NS];
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
@@ -327,6 +329,7 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
             soret += soret_s;
         }
         duf = soret;
+        }
     }
 
     // ---- diffusive part (fluxStag.cpp:1026-1426) ----
@@ -338,6 +341,8 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
         const R meanT = R(0.5) * (Tl + Th);
         const R meanP = R(0.5) * (pl + ph);
         heat -= kp * (Th - Tl) / h;
+        // species diffusion, Dufour: mixtures only
+        if constexpr (NS > 1) {
         R dk[NS], sor[NS], Fk[NS], hk[NS];
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
@@ -371,6 +376,7 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
         duf += Q5;
 #pragma unroll
         for (int s = 0; s < NS; ++s) spec[s] += Fk[s];
+        }
     }
 
     // ---- hyperbolic part (fluxStag.cpp:1508-1764), in double ----
@@ -429,6 +435,9 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
     out.aux[2] = (double)vshear;
     out.aux[3] = (double)duf;
     f4 += out.aux[0] + out.aux[1] + out.aux[2] + out.aux[3];
+    // a single gas: its species density is the density, so its flux is the mass
+    // flux exactly (rhoY stays bitwise equal to rho through the RK update)
+    if constexpr (NS == 1) fs[0] = f0;
     out.cons[0] = f0;
     out.cons[1] = f4;
 #pragma unroll

@@ -120,6 +120,17 @@ def argon(n=32, dx=1e-6, **kw) -> Params:
     return base.replace(**kw)
 
 
+def argon_single(n=32, dx=1e-6, **kw) -> Params:
+    """Argon as one species (the single-gas fast path: no species flux; the
+    reference itself cannot run nspecies = 1 and uses two identical species,
+    ``argon``).  Same gas, same stable dt as ``argon``."""
+    n3 = (n, n, n) if isinstance(n, int) else tuple(n)
+    base = Params(nspecies=1, n_cells=n3, prob_hi=tuple(dx * n3[d] for d in range(3)),
+                  molmass=(39.95,), diameter=(3.66e-8,), dof=(3.0,), e0=(0.0,), hcv=(-1.0,), hcp=(-1.0,),
+                  rhobar=(1.0,))
+    return base.replace(**kw)
+
+
 def mixture4(n=32, dx=1e-6, **kw) -> Params:
     """4-species ideal-gas mixture (Ar/Ne/Kr/He), equal mass fractions."""
     n3 = (n, n, n) if isinstance(n, int) else tuple(n)

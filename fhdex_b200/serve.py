@@ -15,9 +15,10 @@ its own instead of joining a batch.
 ``run_alone`` is the baseline: the same trace served one request at a time with
 the plain FP64 step.
 
-A one-species request runs in the reference's parity form of a single gas: two
-identical species (the reference cannot run nspecies = 1; its transport routine
-aborts on Y = 1).
+A one-species request runs the single-gas fast path (nspecies = 1: no species
+flux); the reference itself cannot run nspecies = 1 (its transport routine aborts
+on Y = 1) and models a single gas as two identical species, which two-species
+requests do.
 """
 from __future__ import annotations
 
@@ -30,7 +31,7 @@ import torch
 
 from .batch import Batch
 from .context import Context
-from .params import Params, argon, mixture4, stable_dt
+from .params import Params, argon, argon_single, mixture4, stable_dt
 from .state import StagState
 
 
@@ -50,7 +51,9 @@ class Request:
 
 
 def request_params(r: Request, dx=8e-6) -> Params:
-    if r.ns in (1, 2):
+    if r.ns == 1:
+        return argon_single(r.n, dx=dx, precision=r.precision, seed=r.seed)
+    if r.ns == 2:
         return argon(r.n, dx=dx, precision=r.precision, seed=r.seed)
     if r.ns == 4:
         return mixture4(r.n, dx=dx, precision=r.precision, seed=r.seed)
