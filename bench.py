@@ -8,10 +8,16 @@ guard trips after the first step), fully periodic, FP64, in-kernel Philox
 noise, dt from the acoustic + diffusive stability rule.  One step = one
 SSP-RK3 step of the whole box.  value = cells * steps * ranks / max-over-ranks
 device time; e2e = the same metric through the host-buffer C-ABI call
-(fhd_rk3_step_stag_host: H2D of cu/mom/prim/vel from pinned memory, step, D2H).
+(fhd_rk3_step_stag_host: H2D of cu and mom from pinned memory, step, D2H of
+cu, mom, prim and vel).
 
   python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
-                  [--n 256] [--ns 2] [--precision fp64|mixed] [--tile auto|<idx>]
+                  [--n 256] [--ns 1|2|4] [--precision fp64|mixed] [--tile auto|<idx>]
+                  [--mode step|ensemble|serve|stats|sf]
+
+--ns 1 is the single-gas fast path (no CPU baseline: the reference cannot run
+one species).  The other modes time the batched ensemble, the continuous-
+batching server, the running statistics and the structure factor.
 
 N > 1 runs one independent replica per GPU (weak scaling, no data-path
 collective; the runs do not exchange data).  --impl reference times the
@@ -65,13 +71,15 @@ def measured_peak():
 
 
 def make_params(args):
-    from fhdex_b200.params import argon, mixture4
+    from fhdex_b200.params import argon, argon_single, mixture4
     prec = 1 if args.precision == "mixed" else 0
+    if args.ns == 1:
+        return argon_single(args.n, dx=args.dx, precision=prec, seed=args.seed)
     if args.ns == 2:
         return argon(args.n, dx=args.dx, precision=prec, seed=args.seed)
     if args.ns == 4:
         return mixture4(args.n, dx=args.dx, precision=prec, seed=args.seed)
-    raise SystemExit("--ns must be 2 (argon parity form) or 4 (mixture)")
+    raise SystemExit("--ns must be 1 (single gas), 2 (argon parity form) or 4 (mixture)")
 
 
 class ClockSampler:
@@ -212,7 +220,7 @@ def run_reference(args):
 
 def config_dict(args, p, dt, tile):
     return {
-        "workload": (f"{'argon (2 identical species)' if p.nspecies == 2 else '4-species mixture'} "
+        "workload": (f"{ {1: 'argon (single gas)', 2: 'argon (2 identical species)'}.get(p.nspecies, '4-species mixture')} "
                      f"{p.n_cells[0]}^3, dx={p.dx[0]:g} cm, periodic, {args.precision}, in-kernel Philox noise"),
         "n_cells": list(p.n_cells), "nspecies": p.nspecies, "precision": args.precision, "dt_s": dt,
         "noise": "philox-4x32-10 in kernel", "tile": tile,
@@ -351,7 +359,7 @@ def run_ours(args):
         ctx.close()
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu and p.nspecies > 1:
         v, sample = cpu_oracle_rate(p)
         v1, sample1 = cpu_oracle_rate(p, target_s=8.0, max_n=32, threads=1)
         cpu = {"value": v, "unit": UNIT, "cores": _CORES, "kind": "port", "sample": sample,
