@@ -84,55 +84,7 @@ bool fab_ok(const fhd_ctx* c, const fhd_fab& f, const int nodal[3], int min_ng, 
     return true;
 }
 
-DevParams make_dev(const fhd_ctx* c, double dt, uint64_t step) {
-    const fhd_params& p = c->prm;
-    DevParams P;
-    std::memset(&P, 0, sizeof(P));
-    P.ns = p.nspecies;
-    P.nvars = 5 + p.nspecies;
-    P.nprim = 6 + 2 * p.nspecies;
-    for (int d = 0; d < 3; ++d) {
-        P.n[d] = p.n_cells[d];
-        P.dx[d] = (p.prob_hi[d] - p.prob_lo[d]) / p.n_cells[d];
-        P.grav[d] = p.grav[d];
-    }
-    P.dt = dt;
-    P.volinv = 1. / (P.dx[0] * P.dx[1] * P.dx[2]);
-    P.dtinv = 1. / dt;
-    P.k_B = p.k_B;
-    P.Runiv = p.Runiv;
-    P.zeta_ratio = p.zeta_ratio;
-    P.visc_type = p.visc_type;
-    P.advection_type = p.advection_type;
-    P.stoch = p.stoch_stress_form;
-    const double AKL = 1.0, BKL = 1.0, CKL = 1.0;
-    for (int i = 0; i < MAXS; ++i) {
-        P.molmass[i] = p.molmass[i];
-        P.hcv[i] = p.hcv[i];
-        P.hcp[i] = p.hcp[i];
-        P.e0[i] = p.e0[i];
-        P.mm[i] = p.molmass[i] * (p.k_B / p.Runiv);
-        P.mmkB[i] = P.mm[i] * p.k_B;
-    }
-    for (int i = 0; i < MAXS; ++i)
-        for (int j = 0; j < MAXS; ++j) {
-            P.diam[i][j] = 0.5 * (p.diameter[i] + p.diameter[j]);
-            P.mu[i][j] = P.mm[i] * P.mm[j] / (P.mm[i] + P.mm[j]);
-            P.msum[i][j] = P.mm[i] + P.mm[j];
-            P.vfac[i][j] = 1.0 + 0.6 * P.mm[j] / P.mm[i] * AKL;
-            P.kfac[i][j] = 7.5 * P.mm[i] / P.mm[j] + 6.25 * P.mm[j] / P.mm[i] - 3.0 * P.mm[j] / P.mm[i] * BKL + 4.0 * AKL;
-        }
-    for (int i = 0; i < MAXS; ++i) P.eta1pre[i] = 5.0 / (16.0 * P.diam[i][i] * P.diam[i][i]);
-    P.koff = 55.0 / 4.0 - 3.0 * BKL - 4.0 * AKL;
-    P.voff = 0.6 * AKL - 1.0;
-    P.cfac = 6.0 * CKL - 5.0;
-    P.sqrt2 = std::sqrt(2.0);
-    P.sqrt3 = std::sqrt(3.0);
-    P.key0 = (uint32_t)p.seed;
-    P.key1 = (uint32_t)(p.seed >> 32);
-    P.step = step;
-    return P;
-}
+DevParams make_dev(const fhd_ctx* c, double dt, uint64_t step) { return dev_params(c->prm, dt, step); }
 
 int ensure_scratch(fhd_ctx* c) {
     const int* n = c->prm.n_cells;

@@ -9,6 +9,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "fhd_div.h"
+
 #define FHD_HD __host__ __device__ __forceinline__
 #define FHD_D __device__ __forceinline__
 
@@ -60,7 +62,26 @@ struct DevParams {
     uint32_t key0, key1;             // Philox key
     uint64_t step;                   // Philox counter words 2-3
     const uint64_t* step_ptr;        // when set, the step is read here (batched graph replay)
+    // correctly rounded reciprocals (host 1.0 / x) of the constant divisors, for
+    // div_rcp; the dividend window is empty (div_span 0: plain divisions) when a
+    // divisor lies outside div_rcp's divisor window
+    double rdx[3];
+    double rmolmass[MAXS], rmm[MAXS];
+    double rmu[MAXS][MAXS], rmsum[MAXS][MAXS];
+    double rRdt;                     // 1/(Runiv*dt)
+    double rpi, r3;                  // 1/pi (the transport model's pi), 1/3
+    uint32_t div_lo, div_span;
 };
+
+// a / b for a constant divisor b with y = RN(1/b) from DevParams: bitwise a / b
+// (fhd_div.h); in single precision the plain division
+FHD_D double divc(const DevParams& P, double a, double b, double y) { return div_rcp(a, b, y, P.div_lo, P.div_span); }
+FHD_D float divc(const DevParams&, float a, float b, float) { return a / b; }
+// a / b for a cell value b used as a divisor several times, y = 1.0 / b
+FHD_D double divv(const DevParams& P, double a, double b, double y) {
+    return div_rcp_any(a, b, y, P.div_lo, P.div_span);
+}
+FHD_D float divv(const DevParams&, float a, float b, float) { return a / b; }
 
 FHD_D uint64_t noise_step(const DevParams& P) { return P.step_ptr ? *P.step_ptr : P.step; }
 
@@ -70,10 +91,10 @@ template <int NS, class R>
 FHD_D void GetMolfrac(const DevParams& P, const R (&Y)[NS], R (&X)[NS]) {
     R molmix = R(0.);
 #pragma unroll
-    for (int n = 0; n < NS; ++n) molmix += Y[n] / R(P.molmass[n]);
+    for (int n = 0; n < NS; ++n) molmix += divc(P, Y[n], R(P.molmass[n]), R(P.rmolmass[n]));
     molmix = R(1.) / molmix;
 #pragma unroll
-    for (int n = 0; n < NS; ++n) X[n] = Y[n] * molmix / R(P.molmass[n]);
+    for (int n = 0; n < NS; ++n) X[n] = divc(P, Y[n] * molmix, R(P.molmass[n]), R(P.rmolmass[n]));
 }
 
 template <int NS, class R>
@@ -91,7 +112,7 @@ template <int NS, class R>
 FHD_D R GetPressureGas(const DevParams& P, const R (&Y)[NS], R density, R temp) {
     R molmix = R(0.);
 #pragma unroll
-    for (int n = 0; n < NS; ++n) molmix += Y[n] / R(P.molmass[n]);
+    for (int n = 0; n < NS; ++n) molmix += divc(P, Y[n], R(P.molmass[n]), R(P.rmolmass[n]));
     molmix = R(1.) / molmix;
     return density * (R(P.Runiv) / molmix) * temp;
 }
@@ -140,8 +161,10 @@ FHD_D void CholeskyDecomp(R (&a)[NS * NS], R (&sqda)[NS * NS]) {
 }
 
 // D_GIO1 (compressible_functions.H:647-778).  Dout[j*NS+i] = Diff_ij(i,j)*Ykp[i].
+// rDbin: 1.0 / Dbin off the diagonal (only off-diagonal entries divide here)
 template <int NS, class R>
-FHD_D void D_GIO1(const R (&Dbin)[NS][NS], const R (&Ykp)[NS], const R (&Xkp)[NS], R (&Dout)[NS * NS]) {
+FHD_D void D_GIO1(const DevParams& P, const R (&Dbin)[NS][NS], const R (&rDbin)[NS][NS], const R (&Ykp)[NS],
+                  const R (&Xkp)[NS], R (&Dout)[NS * NS]) {
     R Diff[NS * NS], PJ[NS * NS], M2[NS * NS], Pmat[NS * NS], Jmat[NS * NS];
     R Di[NS], Minv[NS], Mmat[NS];
 #pragma unroll
@@ -149,7 +172,7 @@ FHD_D void D_GIO1(const R (&Dbin)[NS][NS], const R (&Ykp)[NS], const R (&Xkp)[NS
         R term2 = R(0.);
 #pragma unroll
         for (int j = 0; j < NS; ++j)
-            if (j != i) term2 = term2 + Xkp[j] / Dbin[i][j];
+            if (j != i) term2 = term2 + divv(P, Xkp[j], Dbin[i][j], rDbin[i][j]);
         Di[i] = (R(1.) - Ykp[i]) / term2;
     }
 #pragma unroll
@@ -175,10 +198,10 @@ FHD_D void D_GIO1(const R (&Dbin)[NS][NS], const R (&Ykp)[NS], const R (&Xkp)[NS
                 R term1 = R(0.);
 #pragma unroll
                 for (int k = 0; k < NS; ++k)
-                    if (k != i) term1 = term1 + Xkp[i] * Xkp[k] / Dbin[i][k];
+                    if (k != i) term1 = term1 + divv(P, Xkp[i] * Xkp[k], Dbin[i][k], rDbin[i][k]);
                 Deltamat = term1;
             } else {
-                Deltamat = -Xkp[i] * Xkp[j] / Dbin[i][j];
+                Deltamat = divv(P, -Xkp[i] * Xkp[j], Dbin[i][j], rDbin[i][j]);
             }
             R z = -Deltamat;
             if (i == j) z = z + Mmat[i];
@@ -255,17 +278,17 @@ FHD_D bool transport_gio(const DevParams& P, R rho, R temperature, R pressure, c
     const R pi = R(3.1415926535897932);
     R mbar = R(0.0);
 #pragma unroll
-    for (int n = 0; n < NS; ++n) mbar += Yk[n] / R(P.mm[n]);
+    for (int n = 0; n < NS; ++n) mbar += divc(P, Yk[n], R(P.mm[n]), R(P.rmm[n]));
     mbar = R(1.0) / mbar;
     R Xk[NS], Xkp[NS], Ykp[NS];
     R Xksum = R(0.0);
 #pragma unroll
     for (int n = 0; n < NS; ++n) {
-        Xk[n] = Yk[n] * mbar / R(P.mm[n]);
+        Xk[n] = divc(P, Yk[n] * mbar, R(P.mm[n]), R(P.rmm[n]));
         Xksum += Xk[n];
     }
 #pragma unroll
-    for (int n = 0; n < NS; ++n) Xkp[n] = Xk[n] + R(1.0e-16) * (Xksum / R(double(NS)) - Xk[n]);
+    for (int n = 0; n < NS; ++n) Xkp[n] = Xk[n] + R(1.0e-16) * (divc(P, Xksum, R(double(NS)), R(1.0 / double(NS))) - Xk[n]);
 #pragma unroll
     for (int n = 0; n < NS; ++n) Ykp[n] = Xkp[n] * R(P.mm[n]) / mbar;
 
@@ -277,14 +300,20 @@ FHD_D bool transport_gio(const DevParams& P, R rho, R temperature, R pressure, c
         for (int j = 0; j < NS; ++j) {
             if (j < i) { Dbin[i][j] = Dbin[j][i]; continue; }  // symmetric: bitwise equal
             const R dij = R(P.diam[i][j]);
-            Dbin[i][j] = (R(3.0) / R(16.0)) * dsqrt(R(2.0) * pi * kT * kT * kT / R(P.mu[i][j])) /
+            Dbin[i][j] = (R(3.0) / R(16.0)) * dsqrt(divc(P, R(2.0) * pi * kT * kT * kT, R(P.mu[i][j]), R(P.rmu[i][j]))) /
                          (pressure * pi * dij * dij);
         }
+    // reciprocals of the off-diagonal binary diffusivities, each a divisor ~7 times below
+    R rDbin[NS][NS];
+#pragma unroll
+    for (int i = 0; i < NS; ++i)
+#pragma unroll
+        for (int j = 0; j < NS; ++j) rDbin[i][j] = (i == j) ? R(0.) : (j < i ? rDbin[j][i] : R(1.) / Dbin[i][j]);
     // viscosity
     R amat[NS][NS], Bi[NS], rhs[NS];
 #pragma unroll
     for (int i = 0; i < NS; ++i) {
-        const R eta1 = R(P.eta1pre[i]) * dsqrt(R(P.mmkB[i]) * temperature / pi);
+        const R eta1 = R(P.eta1pre[i]) * dsqrt(divc(P, R(P.mmkB[i]) * temperature, pi, R(P.rpi)));
         rhs[i] = Xkp[i];
         Bi[i] = rhs[i];
 #pragma unroll
@@ -337,10 +366,12 @@ FHD_D bool transport_gio(const DevParams& P, R rho, R temperature, R pressure, c
 #pragma unroll
                 for (int k = 0; k < NS; ++k)
                     if (k != i)
-                        a += Xkp[i] * Xkp[k] / Dbin[i][k] * R(P.mu[i][k]) / R(P.msum[i][k]) * R(P.kfac[i][k]);
+                        a += divc(P, divv(P, Xkp[i] * Xkp[k], Dbin[i][k], rDbin[i][k]) * R(P.mu[i][k]), R(P.msum[i][k]),
+                                  R(P.rmsum[i][k])) * R(P.kfac[i][k]);
                 amat[i][i] = a;
             } else {
-                amat[i][j] = R(-1.0) * Xkp[i] * Xkp[j] / Dbin[i][j] * R(P.mu[i][j]) / R(P.msum[i][j]) * R(P.koff);
+                amat[i][j] = divc(P, divv(P, R(-1.0) * Xkp[i] * Xkp[j], Dbin[i][j], rDbin[i][j]) * R(P.mu[i][j]),
+                                  R(P.msum[i][j]), R(P.rmsum[i][j])) * R(P.koff);
             }
         }
     }
@@ -377,10 +408,13 @@ FHD_D bool transport_gio(const DevParams& P, R rho, R temperature, R pressure, c
                 R a = R(0.0);
 #pragma unroll
                 for (int k = 0; k < NS; ++k)
-                    if (k != i) a -= R(0.5) * Xkp[k] / Dbin[i][k] * R(P.mm[k]) / R(P.msum[i][k]) * R(P.cfac);
+                    if (k != i)
+                        a -= divc(P, divv(P, R(0.5) * Xkp[k], Dbin[i][k], rDbin[i][k]) * R(P.mm[k]), R(P.msum[i][k]),
+                                  R(P.rmsum[i][k])) * R(P.cfac);
                 row[j] = a;
             } else {
-                row[j] = R(0.5) * Xkp[j] / Dbin[i][j] * R(P.mm[i]) / R(P.msum[i][j]) * R(P.cfac);
+                row[j] = divc(P, divv(P, R(0.5) * Xkp[j], Dbin[i][j], rDbin[i][j]) * R(P.mm[i]), R(P.msum[i][j]),
+                              R(P.rmsum[i][j])) * R(P.cfac);
             }
         }
 #pragma unroll
@@ -391,7 +425,7 @@ FHD_D bool transport_gio(const DevParams& P, R rho, R temperature, R pressure, c
         c.D[0] = R(0.);  // a single gas has no species diffusion
     } else {
         R Dl[NS * NS];
-        D_GIO1<NS, R>(Dbin, Ykp, Xkp, Dl);
+        D_GIO1<NS, R>(P, Dbin, rDbin, Ykp, Xkp, Dl);
 #pragma unroll
         for (int q = 0; q < NS * NS; ++q) c.D[q] = Dl[q] * rho;
     }

@@ -137,8 +137,8 @@ FHD_D CellTaus<R> cell_taus(const DevParams& P, const Fields<NS, R>& F, const No
         const R fac1 = dsqrt(R(2.0) * R(P.k_B) * etaT * R(P.volinv) * R(P.dtinv));
         R fac2 = R(-1.0 / 3.0) * dsqrt(R(2.0) * R(P.k_B) * etaT * R(P.volinv) * R(P.dtinv));
         if (visc3)
-            fac2 = dsqrt(R(P.k_B) * zetaT * R(P.volinv) * R(P.dtinv) / R(3.0)) -
-                   dsqrt(R(2.0) * R(P.k_B) * etaT * R(P.volinv) * R(P.dtinv)) / R(3.0);
+            fac2 = dsqrt(divc(P, R(P.k_B) * zetaT * R(P.volinv) * R(P.dtinv), R(3.0), R(P.r3))) -
+                   divc(P, dsqrt(R(2.0) * R(P.k_B) * etaT * R(P.volinv) * R(P.dtinv)), R(3.0), R(P.r3));
         double wc[3];
         nz.cen_all(P, i, j, k, wc);
         const R w0 = R(wc[0]), w1 = R(wc[1]), w2 = R(wc[2]);
@@ -149,14 +149,15 @@ FHD_D CellTaus<R> cell_taus(const DevParams& P, const Fields<NS, R>& F, const No
     } else {
         t.s[0] = t.s[1] = t.s[2] = R(0.);
     }
-    const R u_x = (R(F.vel[0](i + 1, j, k)) - R(F.vel[0](i, j, k))) / R(P.dx[0]);
-    const R v_y = (R(F.vel[1](i, j + 1, k)) - R(F.vel[1](i, j, k))) / R(P.dx[1]);
-    const R w_z = (R(F.vel[2](i, j, k + 1)) - R(F.vel[2](i, j, k))) / R(P.dx[2]);
+    const R u_x = divc(P, R(F.vel[0](i + 1, j, k)) - R(F.vel[0](i, j, k)), R(P.dx[0]), R(P.rdx[0]));
+    const R v_y = divc(P, R(F.vel[1](i, j + 1, k)) - R(F.vel[1](i, j, k)), R(P.dx[1]), R(P.rdx[1]));
+    const R w_z = divc(P, R(F.vel[2](i, j, k + 1)) - R(F.vel[2](i, j, k)), R(P.dx[2]), R(P.rdx[2]));
     const R div = u_x + v_y + w_z;
     const R zc = visc3 ? R(F.zeta(i, j, k)) : R(0.0);
-    t.d[0] = R(2) * eta * u_x + (zc - R(2) * eta / R(3.)) * div;
-    t.d[1] = R(2) * eta * v_y + (zc - R(2) * eta / R(3.)) * div;
-    t.d[2] = R(2) * eta * w_z + (zc - R(2) * eta / R(3.)) * div;
+    const R eta23 = divc(P, R(2) * eta, R(3.), R(P.r3));
+    t.d[0] = R(2) * eta * u_x + (zc - eta23) * div;
+    t.d[1] = R(2) * eta * v_y + (zc - eta23) * div;
+    t.d[2] = R(2) * eta * w_z + (zc - eta23) * div;
     return t;
 }
 
@@ -181,14 +182,14 @@ FHD_D Taus<R> edge_taus_w(const DevParams& P, const Fields<NS, R>& F, double wno
     }
     R g1, g2;
     if (E == 0) {
-        g1 = (R(F.vel[0](i, j, k)) - R(F.vel[0](i, j - 1, k))) / R(P.dx[1]);  // u_y
-        g2 = (R(F.vel[1](i, j, k)) - R(F.vel[1](i - 1, j, k))) / R(P.dx[0]);  // v_x
+        g1 = divc(P, R(F.vel[0](i, j, k)) - R(F.vel[0](i, j - 1, k)), R(P.dx[1]), R(P.rdx[1]));  // u_y
+        g2 = divc(P, R(F.vel[1](i, j, k)) - R(F.vel[1](i - 1, j, k)), R(P.dx[0]), R(P.rdx[0]));  // v_x
     } else if (E == 1) {
-        g1 = (R(F.vel[0](i, j, k)) - R(F.vel[0](i, j, k - 1))) / R(P.dx[2]);  // u_z
-        g2 = (R(F.vel[2](i, j, k)) - R(F.vel[2](i - 1, j, k))) / R(P.dx[0]);  // w_x
+        g1 = divc(P, R(F.vel[0](i, j, k)) - R(F.vel[0](i, j, k - 1)), R(P.dx[2]), R(P.rdx[2]));  // u_z
+        g2 = divc(P, R(F.vel[2](i, j, k)) - R(F.vel[2](i - 1, j, k)), R(P.dx[0]), R(P.rdx[0]));  // w_x
     } else {
-        g1 = (R(F.vel[1](i, j, k)) - R(F.vel[1](i, j, k - 1))) / R(P.dx[2]);  // v_z
-        g2 = (R(F.vel[2](i, j, k)) - R(F.vel[2](i, j - 1, k))) / R(P.dx[1]);  // w_y
+        g1 = divc(P, R(F.vel[1](i, j, k)) - R(F.vel[1](i, j, k - 1)), R(P.dx[2]), R(P.rdx[2]));  // v_z
+        g2 = divc(P, R(F.vel[2](i, j, k)) - R(F.vel[2](i, j - 1, k)), R(P.dx[1]), R(P.rdx[1]));  // w_y
     }
     const R ei = R(0.25) * (F.eta(ai, aj, ak) + F.eta(bi, bj, bk) + F.eta(ci, cj, ck) + F.eta(i, j, k));
     t.d = ei * (g1 + g2);
@@ -296,7 +297,7 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
         R MWmix = R(0.);
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
-            MWmix = MWmix + R(0.5) * (yy[s] + yyp[s]) / R(P.molmass[s]);
+            MWmix = MWmix + divc(P, R(0.5) * (yy[s] + yyp[s]), R(P.molmass[s]), R(P.rmolmass[s]));
 #pragma unroll
             for (int ll = 0; ll < NS; ++ll)
                 DY[s * NS + ll] = R(0.5) * (F.D(im, jm, km, ll * NS + s) * yy[ll] + F.D(i, j, k, ll * NS + s) * yyp[ll] +
@@ -310,7 +311,7 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
             }
         MWmix = R(1.) / MWmix;
         CholeskyDecomp<NS, R>(DY, sqD);
-        const R fwc = dsqrt(R(P.k_B) * MWmix * R(P.volinv) / (R(P.Runiv) * R(P.dt)));
+        const R fwc = dsqrt(divc(P, R(P.k_B) * MWmix * R(P.volinv), R(P.Runiv) * R(P.dt), R(P.rRdt)));
         R zs[NS];
 #pragma unroll
         for (int ll = 0; ll < NS; ++ll) zs[ll] = R(wf[1 + ll]);
@@ -324,7 +325,7 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
         R soret = R(0.);
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
-            const R soret_s = (hk[s] + R(P.Runiv) * meanT / R(P.molmass[s]) * R(0.5) *
+            const R soret_s = (hk[s] + divc(P, R(P.Runiv) * meanT, R(P.molmass[s]), R(P.rmolmass[s])) * R(0.5) *
                                            (F.chi(im, jm, km, s) + F.chi(i, j, k, s))) * wien[s];
             soret += soret_s;
         }
@@ -334,26 +335,26 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
 
     // ---- diffusive part (fluxStag.cpp:1026-1426) ----
     {
-        const R h = R(P.dx[D]);
+        const R h = R(P.dx[D]), rh = R(P.rdx[D]);
         const R Tl = R(F.T(im, jm, km)), Th = R(F.T(i, j, k));
         const R pl = R(F.p(im, jm, km)), ph = R(F.p(i, j, k));
         const R kp = R(0.5) * (F.kappa(im, jm, km) + F.kappa(i, j, k));
         const R meanT = R(0.5) * (Tl + Th);
         const R meanP = R(0.5) * (pl + ph);
-        heat -= kp * (Th - Tl) / h;
+        heat -= divc(P, kp * (Th - Tl), h, rh);
         // species diffusion, Dufour: mixtures only
         if constexpr (NS > 1) {
         R dk[NS], sor[NS], Fk[NS], hk[NS];
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
             const R Xl = R(F.X(im, jm, km, s)), Xh = R(F.X(i, j, k, s));
-            const R term1 = (Xh - Xl) / h;
+            const R term1 = divc(P, Xh - Xl, h, rh);
             const R mX = R(0.5) * (Xl + Xh);
             const R mY = R(0.5) * (R(F.Y(im, jm, km, s)) + R(F.Y(i, j, k, s)));
-            const R term2 = (mX - mY) * (ph - pl) / h / meanP;
+            const R term2 = divc(P, (mX - mY) * (ph - pl), h, rh) / meanP;
             dk[s] = term1 + term2;
             const R ChiX = R(0.5) * (F.chi(im, jm, km, s) * Xl + F.chi(i, j, k, s) * Xh);
-            sor[s] = ChiX * (Th - Tl) / h / meanT;
+            sor[s] = divc(P, ChiX * (Th - Tl), h, rh) / meanT;
         }
 #pragma unroll
         for (int kk = 0; kk < NS; ++kk) {
@@ -371,7 +372,7 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
         for (int s = 0; s < NS; ++s) {
             // z faces use chi(i,j,k)+chi(i,j,k), fluxStag.cpp:1407 (kept from the reference)
             const R chs = (D == 2) ? (F.chi(i, j, k, s) + F.chi(i, j, k, s)) : (F.chi(im, jm, km, s) + F.chi(i, j, k, s));
-            Q5 += (hk[s] + R(0.5) * R(P.Runiv) * meanT * chs / R(P.molmass[s])) * Fk[s];
+            Q5 += (hk[s] + divc(P, R(0.5) * R(P.Runiv) * meanT * chs, R(P.molmass[s]), R(P.rmolmass[s]))) * Fk[s];
         }
         duf += Q5;
 #pragma unroll

@@ -2,6 +2,8 @@
 // translation units (fhd_exact.cu: FP64 in the reference's operation order,
 // built with -fmad=false; fhd_mixed.cu: FP32 fluxes/coefficients).
 #pragma once
+#include <cmath>
+#include <cstring>
 #include <cuda_runtime.h>
 #include "../../include/fhd_capi.h"
 #include "fhd_device.cuh"
@@ -15,6 +17,80 @@ struct NoiseFabs {
     fhd_fab ea[3], eb[3];   // xy, xz, yz edges
     fhd_fab ca[3], cb[3];   // centres
 };
+
+// Kernel parameters of a run (after GetHcGas): cell widths, the transport model's
+// cell-independent constants in the reference's own operation order
+// (compressible_functions.H:1180-1222), the Philox key and the reciprocals of the
+// constant divisors.
+inline DevParams dev_params(const fhd_params& p, double dt, uint64_t step) {
+    DevParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.ns = p.nspecies;
+    P.nvars = 5 + p.nspecies;
+    P.nprim = 6 + 2 * p.nspecies;
+    for (int d = 0; d < 3; ++d) {
+        P.n[d] = p.n_cells[d];
+        P.dx[d] = (p.prob_hi[d] - p.prob_lo[d]) / p.n_cells[d];
+        P.grav[d] = p.grav[d];
+    }
+    P.dt = dt;
+    P.volinv = 1. / (P.dx[0] * P.dx[1] * P.dx[2]);
+    P.dtinv = 1. / dt;
+    P.k_B = p.k_B;
+    P.Runiv = p.Runiv;
+    P.zeta_ratio = p.zeta_ratio;
+    P.visc_type = p.visc_type;
+    P.advection_type = p.advection_type;
+    P.stoch = p.stoch_stress_form;
+    const double AKL = 1.0, BKL = 1.0, CKL = 1.0;
+    for (int i = 0; i < MAXS; ++i) {
+        P.molmass[i] = p.molmass[i];
+        P.hcv[i] = p.hcv[i];
+        P.hcp[i] = p.hcp[i];
+        P.e0[i] = p.e0[i];
+        P.mm[i] = p.molmass[i] * (p.k_B / p.Runiv);
+        P.mmkB[i] = P.mm[i] * p.k_B;
+    }
+    for (int i = 0; i < MAXS; ++i)
+        for (int j = 0; j < MAXS; ++j) {
+            P.diam[i][j] = 0.5 * (p.diameter[i] + p.diameter[j]);
+            P.mu[i][j] = P.mm[i] * P.mm[j] / (P.mm[i] + P.mm[j]);
+            P.msum[i][j] = P.mm[i] + P.mm[j];
+            P.vfac[i][j] = 1.0 + 0.6 * P.mm[j] / P.mm[i] * AKL;
+            P.kfac[i][j] = 7.5 * P.mm[i] / P.mm[j] + 6.25 * P.mm[j] / P.mm[i] - 3.0 * P.mm[j] / P.mm[i] * BKL + 4.0 * AKL;
+        }
+    for (int i = 0; i < MAXS; ++i) P.eta1pre[i] = 5.0 / (16.0 * P.diam[i][i] * P.diam[i][i]);
+    P.koff = 55.0 / 4.0 - 3.0 * BKL - 4.0 * AKL;
+    P.voff = 0.6 * AKL - 1.0;
+    P.cfac = 6.0 * CKL - 5.0;
+    P.sqrt2 = sqrt(2.0);
+    P.sqrt3 = sqrt(3.0);
+    P.key0 = (uint32_t)p.seed;
+    P.key1 = (uint32_t)(p.seed >> 32);
+    P.step = step;
+    P.step_ptr = nullptr;
+    // reciprocals of the constant divisors for div_rcp (fhd_div.h)
+    bool in_window = true;
+    auto rcp = [&](double b) {
+        in_window = in_window && div_divisor_ok(b);
+        return 1.0 / b;
+    };
+    for (int d = 0; d < 3; ++d) P.rdx[d] = rcp(P.dx[d]);
+    for (int i = 0; i < P.ns; ++i) {
+        P.rmolmass[i] = rcp(P.molmass[i]);
+        P.rmm[i] = rcp(P.mm[i]);
+        for (int j = 0; j < P.ns; ++j) {
+            P.rmu[i][j] = rcp(P.mu[i][j]);
+            P.rmsum[i][j] = rcp(P.msum[i][j]);
+        }
+    }
+    P.rRdt = rcp(P.Runiv * P.dt);
+    P.rpi = rcp(3.1415926535897932);
+    P.r3 = rcp(3.0);
+    P.div_lo = kDivAlo;
+    P.div_span = in_window ? kDivAspan : 0u;
+    return P;
+}
 
 // Everything one stage (or one flux-operator call) reads and writes.
 struct StageCall {

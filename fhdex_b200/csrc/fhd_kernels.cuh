@@ -248,9 +248,9 @@ FHD_D void update_point(const StageArgs<NS, R, NZ>& a, int q) {
 #pragma unroll
             for (int c = 0; c < 2 + NS; ++c) {
                 const int n = (c == 0) ? 0 : 3 + c;  // conserved component index
-                const double div = (a.ff[0](i + 1, j, k, c) - a.ff[0](i, j, k, c)) / P.dx[0] +
-                                   (a.ff[1](i, j + 1, k, c) - a.ff[1](i, j, k, c)) / P.dx[1] +
-                                   (a.ff[2](i, j, k + 1, c) - a.ff[2](i, j, k, c)) / P.dx[2];
+                const double div = divc(P, a.ff[0](i + 1, j, k, c) - a.ff[0](i, j, k, c), P.dx[0], P.rdx[0]) +
+                                   divc(P, a.ff[1](i, j + 1, k, c) - a.ff[1](i, j, k, c), P.dx[1], P.rdx[1]) +
+                                   divc(P, a.ff[2](i, j, k + 1, c) - a.ff[2](i, j, k, c), P.dx[2], P.rdx[2]);
                 const double src = a.src.p ? a.src(i, j, k, n) : 0.0;
                 const double u0 = a.cons0(i, j, k, n);
                 double v;
@@ -291,13 +291,15 @@ FHD_D void update_point(const StageArgs<NS, R, NZ>& a, int q) {
             const double m0 = a.mom0[d](i, j, k);
             double v;
             if (st == 1) {
-                v = m0 - dt * t1 / P.dx[0] - dt * t2 / P.dx[1] - dt * t3 / P.dx[2] + 0.5 * dt * P.grav[d] * rsum;
+                v = m0 - divc(P, dt * t1, P.dx[0], P.rdx[0]) - divc(P, dt * t2, P.dx[1], P.rdx[1]) -
+                    divc(P, dt * t3, P.dx[2], P.rdx[2]) + 0.5 * dt * P.grav[d] * rsum;
             } else if (st == 2) {
-                v = 0.25 * 3.0 * m0 + 0.25 * F.mom[d](i, j, k) - 0.25 * dt * t1 / P.dx[0] - 0.25 * dt * t2 / P.dx[1] -
-                    0.25 * dt * t3 / P.dx[2] + 0.5 * 0.25 * dt * P.grav[d] * rsum;
+                v = 0.25 * 3.0 * m0 + 0.25 * F.mom[d](i, j, k) - divc(P, 0.25 * dt * t1, P.dx[0], P.rdx[0]) -
+                    divc(P, 0.25 * dt * t2, P.dx[1], P.rdx[1]) - divc(P, 0.25 * dt * t3, P.dx[2], P.rdx[2]) +
+                    0.5 * 0.25 * dt * P.grav[d] * rsum;
             } else {
-                v = (2. / 3.) * (0.5 * m0 + F.mom[d](i, j, k)) - (2. / 3.) * dt * t1 / P.dx[0] -
-                    (2. / 3.) * dt * t2 / P.dx[1] - (2. / 3.) * dt * t3 / P.dx[2] +
+                v = (2. / 3.) * (0.5 * m0 + F.mom[d](i, j, k)) - divc(P, (2. / 3.) * dt * t1, P.dx[0], P.rdx[0]) -
+                    divc(P, (2. / 3.) * dt * t2, P.dx[1], P.rdx[1]) - divc(P, (2. / 3.) * dt * t3, P.dx[2], P.rdx[2]) +
                     0.5 * (2. / 3.) * dt * P.grav[d] * rsum;
             }
             a.mom_o[d](i, j, k) = v;
