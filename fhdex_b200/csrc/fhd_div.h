@@ -9,8 +9,10 @@
 // theorem assumes no overflow or underflow anywhere, which holds when
 //   2^-900 <= |a| < 2^900  and  2^-100 <= |b| < 2^100
 // (then |a y| < 2^1001, |a/b| > 2^-1000 and the remainder's last bit lies above
-// 2^-1010).  Every other a (zero, subnormal, huge, inf, NaN) or b takes the plain
-// division, so the result equals a / b for all inputs.  Three FP64 operations
+// 2^-1010).  A zero dividend over a finite nonzero b gives the signed zero a*b
+// (its sign is sign(a) xor sign(b), as for a / b); every other a (subnormal, huge,
+// inf, NaN) or b takes the plain division, so the result equals a / b for all
+// inputs.  Three FP64 operations
 // replace the division's reciprocal refinement; the divisors here are constants of
 // the run (cell widths, molar masses, reduced masses) whose reciprocals the host
 // computes once, or cell values used as divisors several times.
@@ -52,11 +54,19 @@ FHD_DIV_HD bool div_in_window(double x, uint32_t lo, uint32_t span) {
 // true when b may be used as a divisor of div_rcp (host check of run constants)
 inline bool div_divisor_ok(double b) { return div_in_window(b, kDivBlo, kDivBspan); }
 
+// a / b with a short cut for a zero dividend (a*b is then the same signed zero as
+// a / b for any finite nonzero b); otherwise the plain division
+FHD_DIV_HD double div_zero_short(double a, double b) {
+    if (a == 0.0 && div_in_window(b, kDivBlo, kDivBspan)) return a * b;
+    return a / b;
+}
+
+// the inputs outside the windows, out of line (one copy per module, two arguments
+// so that call sites stay light)
 #if defined(__CUDA_ARCH__)
-// the rare inputs outside the windows: one out-of-line division per module
-static __device__ __noinline__ double div_plain(double a, double b) { return a / b; }
+static __device__ __noinline__ double div_outside(double a, double b) { return div_zero_short(a, b); }
 #else
-inline double div_plain(double a, double b) { return a / b; }
+inline double div_outside(double a, double b) { return div_zero_short(a, b); }
 #endif
 
 // a / b for a divisor b inside the b-window (checked by the caller, e.g. on the
@@ -68,17 +78,29 @@ FHD_DIV_HD double div_rcp(double a, double b, double y, uint32_t alo = kDivAlo, 
         const double q = a * y;
         return fma(fma(-q, b, a), y, q);
     }
-    return div_plain(a, b);
+    return div_outside(a, b);
+}
+
+// div_rcp with the zero dividend handled inline, for call sites where zero
+// dividends are common (no out-of-line call for them)
+FHD_DIV_HD double div_rcp_z(double a, double b, double y, uint32_t alo = kDivAlo, uint32_t aspan = kDivAspan) {
+    if (div_in_window(a, alo, aspan)) {
+        const double q = a * y;
+        return fma(fma(-q, b, a), y, q);
+    }
+    if (a == 0.0 && aspan != 0u) return a * b;  // b: a run constant inside the divisor window
+    return div_outside(a, b);
 }
 
 // a / b for any b, with y = RN(1/b) from a correctly rounded division 1.0 / b
 FHD_DIV_HD double div_rcp_any(double a, double b, double y, uint32_t alo = kDivAlo,
                                uint32_t aspan = kDivAspan) {
-    if (div_in_window(a, alo, aspan) && div_in_window(b, kDivBlo, kDivBspan)) {
+    const bool bwin = div_in_window(b, kDivBlo, kDivBspan);
+    if (div_in_window(a, alo, aspan) && bwin) {
         const double q = a * y;
         return fma(fma(-q, b, a), y, q);
     }
-    return div_plain(a, b);
+    return div_outside(a, b);
 }
 
 }  // namespace fhd

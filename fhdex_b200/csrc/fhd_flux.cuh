@@ -351,10 +351,10 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
             const R term1 = divc(P, Xh - Xl, h, rh);
             const R mX = R(0.5) * (Xl + Xh);
             const R mY = R(0.5) * (R(F.Y(im, jm, km, s)) + R(F.Y(i, j, k, s)));
-            const R term2 = divc(P, (mX - mY) * (ph - pl), h, rh) / meanP;
+            const R term2 = divz(divc0(P, (mX - mY) * (ph - pl), h, rh), meanP);
             dk[s] = term1 + term2;
             const R ChiX = R(0.5) * (F.chi(im, jm, km, s) * Xl + F.chi(i, j, k, s) * Xh);
-            sor[s] = divc(P, ChiX * (Th - Tl), h, rh) / meanT;
+            sor[s] = divz(divc0(P, ChiX * (Th - Tl), h, rh), meanT);
         }
 #pragma unroll
         for (int kk = 0; kk < NS; ++kk) {
@@ -372,7 +372,7 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
         for (int s = 0; s < NS; ++s) {
             // z faces use chi(i,j,k)+chi(i,j,k), fluxStag.cpp:1407 (kept from the reference)
             const R chs = (D == 2) ? (F.chi(i, j, k, s) + F.chi(i, j, k, s)) : (F.chi(im, jm, km, s) + F.chi(i, j, k, s));
-            Q5 += (hk[s] + divc(P, R(0.5) * R(P.Runiv) * meanT * chs, R(P.molmass[s]), R(P.rmolmass[s]))) * Fk[s];
+            Q5 += (hk[s] + divc0(P, R(0.5) * R(P.Runiv) * meanT * chs, R(P.molmass[s]), R(P.rmolmass[s]))) * Fk[s];
         }
         duf += Q5;
 #pragma unroll

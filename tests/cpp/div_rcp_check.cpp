@@ -62,12 +62,13 @@ int main(int argc, char** argv) {
     long checked = 0, bad = 0;
     auto check = [&](double a, double b, bool any) {
         const double y = 1.0 / b;
-        const double q = any ? fhd::div_rcp_any(a, b, y) : fhd::div_rcp(a, b, y);
         const double ref = a / b;
+        const double q = any ? fhd::div_rcp_any(a, b, y) : fhd::div_rcp(a, b, y);
+        const double qz = any ? q : fhd::div_rcp_z(a, b, y);
         ++checked;
-        if (!same(q, ref)) {
+        if (!same(q, ref) || !same(qz, ref)) {
             if (bad < 10)
-                std::printf("mismatch a=%a b=%a got %a want %a\n", a, b, q, ref);
+                std::printf("mismatch a=%a b=%a got %a / %a want %a\n", a, b, q, qz, ref);
             ++bad;
         }
     };
@@ -111,6 +112,30 @@ int main(int argc, char** argv) {
     for (double b : {0.0, -0.0, std::numeric_limits<double>::denorm_min(), std::numeric_limits<double>::infinity(),
                      std::numeric_limits<double>::quiet_NaN()})
         for (int r = 0; r < 1000; ++r) check(rnd(-300, 300), b, true);
+    // signed zero dividends over negative and positive divisors, and div_zero_short
+    for (long r = 0; r < n_rand / 100; ++r) {
+        const double b = rnd(-1022, 1023);
+        for (double a : {0.0, -0.0}) {
+            check(a, b, true);
+            if (fhd::div_in_window(b, fhd::kDivBlo, fhd::kDivBspan)) check(a, b, false);
+        }
+    }
+    auto check_z = [&](double a, double b) {
+        ++checked;
+        const double q = fhd::div_zero_short(a, b), ref = a / b;
+        if (!same(q, ref)) {
+            if (bad < 10) std::printf("mismatch (zero short cut) a=%a b=%a got %a want %a\n", a, b, q, ref);
+            ++bad;
+        }
+    };
+    for (double b : specials)
+        for (double a : specials) check_z(a, b);
+    for (long r = 0; r < n_rand / 10; ++r) {
+        const double b = rnd(-1022, 1023);
+        check_z(0.0, b);
+        check_z(-0.0, b);
+        check_z(rnd(-1022, 1023), b);
+    }
 
     std::printf("checked %ld mismatches %ld\n", checked, bad);
     return bad == 0 ? 0 : 1;

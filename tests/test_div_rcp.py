@@ -3,9 +3,10 @@ masses) and by cell values used several times through fhd::div_rcp /
 div_rcp_any (Markstein's correction step with a known reciprocal).  Bitwise
 parity with the oracle needs those quotients to equal the IEEE division exactly:
 this runs the same header on the host against a / b over ~1e8 dividend/divisor
-pairs, including zeros, subnormals, inf/NaN, window edges and quotients next to
-rounding midpoints, and checks that the check itself catches an uncorrected
-quotient."""
+pairs, including signed zeros over divisors of both signs, subnormals, inf/NaN,
+window edges and quotients next to rounding midpoints (and the zero-dividend
+short cut div_zero_short), and checks that the check itself catches an
+uncorrected quotient."""
 import os
 import shutil
 import subprocess
@@ -41,7 +42,7 @@ def test_check_detects_an_uncorrected_quotient(tmp_path):
     remainder correction) must report mismatches."""
     src = open(os.path.join(CSRC, "fhd_div.h")).read()
     good = "return fma(fma(-q, b, a), y, q);"
-    assert src.count(good) == 2
+    assert src.count(good) == 3, "the planted mistake targets every correction step"
     planted = tmp_path / "planted"
     planted.mkdir()
     (planted / "fhd_div.h").write_text(src.replace(good, "return q;"))
