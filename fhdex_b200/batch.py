@@ -72,3 +72,20 @@ class Batch:
 
     def __len__(self):
         return self.lib.fhd_batch_size(self._h)
+
+    # register caps of the batched face-flux kernels (registers per thread)
+    TILE_REGS = (64, 80, 128)
+
+    def set_tile(self, tile: int):
+        """Face-kernel launch shape: an index into TILE_REGS, or -1 for the default."""
+        check(self.lib.fhd_batch_set_tile(self._h, tile), "fhd_batch_set_tile")
+
+    def autotune(self, reps: int = 3):
+        """Time the batched face-flux kernels of one stage for every register cap on
+        the current members and keep the fastest (members' states do not change;
+        run after at least one step).  Returns (best tile, {regs: ms})."""
+        nt = self.lib.fhd_batch_num_tiles()
+        ms = (C.c_double * nt)()
+        best = C.c_int(-1)
+        check(self.lib.fhd_batch_autotune(self._h, reps, ms, C.byref(best)), "fhd_batch_autotune")
+        return best.value, {self.TILE_REGS[t]: round(ms[t], 4) for t in range(nt)}

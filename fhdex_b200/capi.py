@@ -149,6 +149,9 @@ def _declare(lib):
         "fhd_batch_size": (i, [vp]),
         "fhd_batch_member_status": (i, [vp, i]),
         "fhd_batch_synchronize": (i, [vp]),
+        "fhd_batch_num_tiles": (i, []),
+        "fhd_batch_set_tile": (i, [vp, i]),
+        "fhd_batch_autotune": (i, [vp, i, P(d), P(i)]),
     }
     for name, (res, args) in sigs.items():
         if hasattr(lib, name):

@@ -89,6 +89,7 @@ struct fhd_batch {
     uint64_t* dsteps = nullptr;  // inside dbuf
     int* dstatus = nullptr;      // inside dbuf, one word per member
     std::vector<Launch> plan;
+    int tile = -1;               // face-kernel register cap (batch_face_tiles(); -1 default)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
 };
@@ -332,8 +333,8 @@ int run_plan(fhd_batch* b) {
         int rc = FHD_OK;
         if (L.kind <= 6) {
             const bool mixed = (L.kind == 6) ? false : b->mixed;
-            rc = batch_launch(b->ns, mixed, L.kind, b->mode, d + L.args_off, reinterpret_cast<const int*>(d + L.bpref_off),
-                              L.nitems, L.nblocks, b->stream);
+            rc = batch_launch(b->ns, mixed, L.kind, b->mode, b->tile, d + L.args_off,
+                              reinterpret_cast<const int*>(d + L.bpref_off), L.nitems, L.nblocks, b->stream);
         } else if (L.kind == 7) {
             rc = ghost_launch_b(d + L.args_off, reinterpret_cast<const int*>(d + L.bpref_off), L.nitems, L.nblocks,
                                 b->stream);
@@ -526,6 +527,74 @@ int fhd_batch_step(fhd_batch* b, int nsteps, int use_graph) {
 }
 
 int fhd_batch_size(const fhd_batch* b) { return b ? (int)b->mem.size() : -1; }
+
+int fhd_batch_num_tiles(void) { return batch_face_tiles(); }
+
+int fhd_batch_set_tile(fhd_batch* b, int tile) {
+    if (!b || tile < -1 || tile >= batch_face_tiles()) return FHD_ERR_BAD_ARG;
+    if (tile != b->tile) {
+        b->tile = tile;
+        drop_graph(b);
+    }
+    return FHD_OK;
+}
+
+int fhd_batch_autotune(fhd_batch* b, int reps, double* ms, int* best) {
+    if (!b || reps < 1) return FHD_ERR_BAD_ARG;
+    if (b->mem.empty()) {
+        if (best) *best = b->tile;
+        return FHD_OK;
+    }
+    cudaSetDevice(b->device);
+    if (b->dirty) {
+        const int rc = rebuild(b);
+        if (rc) return rc;
+    }
+    std::vector<const Launch*> faces;  // the face launches of the first stage
+    for (const Launch& L : b->plan)
+        if (L.kind >= 2 && L.kind <= 4 && faces.size() < 3) faces.push_back(&L);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        if (e0) cudaEventDestroy(e0);
+        return cuda_ok(cudaGetLastError());
+    }
+    char* d = static_cast<char*>(b->dbuf);
+    const int nt = batch_face_tiles();
+    int bt = b->tile, rc = FHD_OK;
+    double bms = 0.0;
+    for (int t = 0; t < nt && !rc; ++t) {
+        for (int r = 0; r <= reps && !rc; ++r) {
+            if (r == 1 && cudaEventRecord(e0, b->stream) != cudaSuccess) rc = FHD_ERR_CUDA;
+            for (const Launch* L : faces)
+                if (!rc)
+                    rc = batch_launch(b->ns, b->mixed, L->kind, b->mode, t, d + L->args_off,
+                                      reinterpret_cast<const int*>(d + L->bpref_off), L->nitems, L->nblocks, b->stream);
+        }
+        float el = 0.f;
+        if (!rc && (cudaEventRecord(e1, b->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                    cudaEventElapsedTime(&el, e0, e1) != cudaSuccess))
+            rc = FHD_ERR_CUDA;
+        if (rc) break;
+        const double per = (double)el / reps;
+        if (ms) ms[t] = per;
+        if (t == 0 || per < bms) {
+            bms = per;
+            bt = t;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) {
+        cudaGetLastError();
+        return rc;
+    }
+    if (bt != b->tile) {
+        b->tile = bt;
+        drop_graph(b);
+    }
+    if (best) *best = bt;
+    return FHD_OK;
+}
 
 int fhd_batch_member_status(fhd_batch* b, int member) {
     if (!b) return FHD_ERR_BAD_ARG;

@@ -36,28 +36,28 @@ int exact_convert_ns4(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const 
 
 size_t exact_batch_args_size_ns1(int, int);
 void exact_batch_pack_ns1(int, int, const StageCall&, void*);
-int exact_batch_launch_ns1(int, int, const void*, const int*, int, int, cudaStream_t);
+int exact_batch_launch_ns1(int, int, int, const void*, const int*, int, int, cudaStream_t);
 size_t mixed_batch_args_size_ns1(int, int);
 void mixed_batch_pack_ns1(int, int, const StageCall&, void*);
-int mixed_batch_launch_ns1(int, int, const void*, const int*, int, int, cudaStream_t);
+int mixed_batch_launch_ns1(int, int, int, const void*, const int*, int, int, cudaStream_t);
 size_t exact_batch_args_size_ns2(int, int);
 void exact_batch_pack_ns2(int, int, const StageCall&, void*);
-int exact_batch_launch_ns2(int, int, const void*, const int*, int, int, cudaStream_t);
+int exact_batch_launch_ns2(int, int, int, const void*, const int*, int, int, cudaStream_t);
 size_t mixed_batch_args_size_ns2(int, int);
 void mixed_batch_pack_ns2(int, int, const StageCall&, void*);
-int mixed_batch_launch_ns2(int, int, const void*, const int*, int, int, cudaStream_t);
+int mixed_batch_launch_ns2(int, int, int, const void*, const int*, int, int, cudaStream_t);
 size_t exact_batch_args_size_ns3(int, int);
 void exact_batch_pack_ns3(int, int, const StageCall&, void*);
-int exact_batch_launch_ns3(int, int, const void*, const int*, int, int, cudaStream_t);
+int exact_batch_launch_ns3(int, int, int, const void*, const int*, int, int, cudaStream_t);
 size_t mixed_batch_args_size_ns3(int, int);
 void mixed_batch_pack_ns3(int, int, const StageCall&, void*);
-int mixed_batch_launch_ns3(int, int, const void*, const int*, int, int, cudaStream_t);
+int mixed_batch_launch_ns3(int, int, int, const void*, const int*, int, int, cudaStream_t);
 size_t exact_batch_args_size_ns4(int, int);
 void exact_batch_pack_ns4(int, int, const StageCall&, void*);
-int exact_batch_launch_ns4(int, int, const void*, const int*, int, int, cudaStream_t);
+int exact_batch_launch_ns4(int, int, int, const void*, const int*, int, int, cudaStream_t);
 size_t mixed_batch_args_size_ns4(int, int);
 void mixed_batch_pack_ns4(int, int, const StageCall&, void*);
-int mixed_batch_launch_ns4(int, int, const void*, const int*, int, int, cudaStream_t);
+int mixed_batch_launch_ns4(int, int, int, const void*, const int*, int, int, cudaStream_t);
 
 #define FHD_DISPATCH(ns, fn, ...)            \
     switch (ns) {                             \
@@ -100,11 +100,14 @@ void batch_pack(int ns, bool mixed, int kind, int mode, const StageCall& c, void
         default: break;
     }
 }
-int batch_launch(int ns, bool mixed, int kind, int mode, const void* dargs, const int* dbpref, int nmem, int nblocks,
-                 cudaStream_t s) {
-    if (mixed) { FHD_DISPATCH(ns, mixed_batch_launch_ns, kind, mode, dargs, dbpref, nmem, nblocks, s) }
-    FHD_DISPATCH(ns, exact_batch_launch_ns, kind, mode, dargs, dbpref, nmem, nblocks, s)
+int batch_launch(int ns, bool mixed, int kind, int mode, int tile, const void* dargs, const int* dbpref, int nmem,
+                 int nblocks, cudaStream_t s) {
+    if (mixed) { FHD_DISPATCH(ns, mixed_batch_launch_ns, kind, mode, tile, dargs, dbpref, nmem, nblocks, s) }
+    FHD_DISPATCH(ns, exact_batch_launch_ns, kind, mode, tile, dargs, dbpref, nmem, nblocks, s)
 }
+
+int batch_face_tiles() { return kNumBatchFaceTiles; }
+int batch_face_min_blocks(int tile) { return (tile >= 0 && tile < kNumBatchFaceTiles) ? kBatchFaceMinBlocks[tile] : 0; }
 
 int ghost_desc_size() { return (int)sizeof(GhostFab); }
 

@@ -144,8 +144,11 @@ int init_uniform(const fhd_fab& cu, int ns, double rho0, double rhoE, const doub
 // batched launches (kinds: 0 cellprep, 1 stresses, 2-4 faces, 5 update, 6 conversion)
 size_t batch_args_size(int ns, bool mixed, int kind, int mode);
 void batch_pack(int ns, bool mixed, int kind, int mode, const StageCall& c, void* dst);
-int batch_launch(int ns, bool mixed, int kind, int mode, const void* dargs, const int* dbpref, int nmem, int nblocks,
-                 cudaStream_t s);
+// tile: register cap of the face kinds (batch_face_tiles() choices; -1 the default)
+int batch_launch(int ns, bool mixed, int kind, int mode, int tile, const void* dargs, const int* dbpref, int nmem,
+                 int nblocks, cudaStream_t s);
+int batch_face_tiles();
+int batch_face_min_blocks(int tile);
 struct GhostFabDesc;  // opaque to the host code
 int ghost_desc_size();
 int64_t ghost_pack(const fhd_fab& f, int c0, int nc, const int ncell[3], void* dst);  // returns work items

@@ -30,10 +30,10 @@ void FHD_CAT(FHD_CAT(FHD_PFX, _batch_pack_ns), FHD_NS)(int kind, int mode, const
     if (mode == NM_OFF) batch_pack_t<FHD_NS, FHD_R, NZ_OFF>(kind, c, dst);
     else batch_pack_t<FHD_NS, FHD_R, NZ_PHILOX>(kind, c, dst);
 }
-int FHD_CAT(FHD_CAT(FHD_PFX, _batch_launch_ns), FHD_NS)(int kind, int mode, const void* dargs, const int* dbpref,
-                                                       int nmem, int nblocks, cudaStream_t s) {
-    return mode == NM_OFF ? batch_launch_t<FHD_NS, FHD_R, NZ_OFF>(kind, dargs, dbpref, nmem, nblocks, s)
-                          : batch_launch_t<FHD_NS, FHD_R, NZ_PHILOX>(kind, dargs, dbpref, nmem, nblocks, s);
+int FHD_CAT(FHD_CAT(FHD_PFX, _batch_launch_ns), FHD_NS)(int kind, int mode, int tile, const void* dargs,
+                                                       const int* dbpref, int nmem, int nblocks, cudaStream_t s) {
+    return mode == NM_OFF ? batch_launch_t<FHD_NS, FHD_R, NZ_OFF>(kind, tile, dargs, dbpref, nmem, nblocks, s)
+                          : batch_launch_t<FHD_NS, FHD_R, NZ_PHILOX>(kind, tile, dargs, dbpref, nmem, nblocks, s);
 }
 
 #if defined(FHD_MIXED) && FHD_MIXED

@@ -663,11 +663,26 @@ FHD_D int member_of(const int* __restrict__ bpref, int nmem) {
     return lo;
 }
 
+// The member's argument block, copied once per block into shared memory (every
+// thread of a block belongs to the same member): the bodies then read pointers,
+// strides and run constants with shared loads on demand instead of holding what
+// they read from global memory in registers.
+template <class A>
+FHD_D const A& member_args(const A* __restrict__ args, int m) {
+    static_assert(sizeof(A) % 8 == 0, "argument blocks are copied in 8-byte words");
+    __shared__ A sa;
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(args + m);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sa);
+    for (int w = threadIdx.x; w < (int)(sizeof(A) / 8); w += blockDim.x) dst[w] = src[w];
+    __syncthreads();
+    return sa;
+}
+
 template <int NS, class R>
 static __global__ void __launch_bounds__(128, cellprep_min_blocks<NS, R>()) k_cellprep_b(const PrepArgs<NS, R>* __restrict__ args,
                                                     const int* __restrict__ bpref, int nmem) {
     const int m = member_of(bpref, nmem);
-    const PrepArgs<NS, R>& a = args[m];
+    const PrepArgs<NS, R>& a = member_args(args, m);
     const int q = (blockIdx.x - bpref[m]) * blockDim.x + threadIdx.x;
     if (q < cellprep_count(a)) cellprep_point(a, q);
 }
@@ -676,22 +691,18 @@ template <int NS, class R, int NZ>
 static __global__ void __launch_bounds__(128) k_taus_b(const StageArgs<NS, R, NZ>* __restrict__ args,
                                                 const int* __restrict__ bpref, int nmem) {
     const int m = member_of(bpref, nmem);
-    const StageArgs<NS, R, NZ>& a = args[m];
+    const StageArgs<NS, R, NZ>& a = member_args(args, m);
     const int q = (blockIdx.x - bpref[m]) * blockDim.x + threadIdx.x;
     if (q < taus_count(a)) taus_point(a, q);
 }
 
-// Register cap of the batched face kernel: 64 registers (8 blocks of 128) for up
-// to two species, where the extra occupancy outweighs small spills; 128
-// registers (4 blocks) above, where a 64-register cap spills heavily.
-template <int NS>
-constexpr int faces_b_min_blocks() { return NS <= 2 ? 8 : 4; }
-
-template <int NS, class R, int NZ, int D>
-static __global__ void __launch_bounds__(128, faces_b_min_blocks<NS>()) k_faces_b(const StageArgs<NS, R, NZ>* __restrict__ args,
+// Register cap of the batched face kernel: MINB resident blocks of 128 threads
+// (8: 64 registers, 6: 80, 4: 128), picked per batch by its autotuner.
+template <int NS, class R, int NZ, int D, int MINB>
+static __global__ void __launch_bounds__(128, MINB) k_faces_b(const StageArgs<NS, R, NZ>* __restrict__ args,
                                                    const int* __restrict__ bpref, int nmem) {
     const int m = member_of(bpref, nmem);
-    const StageArgs<NS, R, NZ>& a = args[m];
+    const StageArgs<NS, R, NZ>& a = member_args(args, m);
     const int q = (blockIdx.x - bpref[m]) * blockDim.x + threadIdx.x;
     if (q < faces_count<NS, R, NZ, D>(a)) faces_point<NS, R, NZ, D>(a, q);
 }
@@ -700,7 +711,7 @@ template <int NS, class R, int NZ>
 static __global__ void __launch_bounds__(128) k_update_b(const StageArgs<NS, R, NZ>* __restrict__ args,
                                                   const int* __restrict__ bpref, int nmem) {
     const int m = member_of(bpref, nmem);
-    const StageArgs<NS, R, NZ>& a = args[m];
+    const StageArgs<NS, R, NZ>& a = member_args(args, m);
     const int q = (blockIdx.x - bpref[m]) * blockDim.x + threadIdx.x;
     if (q < update_count(a)) update_point(a, q);
 }
@@ -709,7 +720,7 @@ template <int NS>
 static __global__ void __launch_bounds__(128) k_convert_b(const ConvArgs<NS>* __restrict__ args,
                                                    const int* __restrict__ bpref, int nmem) {
     const int m = member_of(bpref, nmem);
-    const ConvArgs<NS>& a = args[m];
+    const ConvArgs<NS>& a = member_args(args, m);
     const int q = (blockIdx.x - bpref[m]) * blockDim.x + threadIdx.x;
     if (q < convert_count(a)) convert_point(a, q);
 }

@@ -211,17 +211,35 @@ void batch_pack_t(int kind, const StageCall& c, void* dst) {
     }
 }
 
+// register caps of the batched face kernel (resident blocks of 128 per SM), the
+// batch autotuner's choices; the default is the first for up to two species and
+// the last above
+constexpr int kBatchFaceMinBlocks[] = {8, 6, 4};
+constexpr int kNumBatchFaceTiles = 3;
+
+template <int NS, class R, int NZ, int MINB>
+void batch_faces_t(int kind, const StageArgs<NS, R, NZ>* sa, const int* dbpref, int nmem, int nblocks, cudaStream_t s) {
+    if (kind == 2) k_faces_b<NS, R, NZ, 0, MINB><<<nblocks, 128, 0, s>>>(sa, dbpref, nmem);
+    else if (kind == 3) k_faces_b<NS, R, NZ, 1, MINB><<<nblocks, 128, 0, s>>>(sa, dbpref, nmem);
+    else k_faces_b<NS, R, NZ, 2, MINB><<<nblocks, 128, 0, s>>>(sa, dbpref, nmem);
+}
+
 template <int NS, class R, int NZ>
-int batch_launch_t(int kind, const void* dargs, const int* dbpref, int nmem, int nblocks, cudaStream_t s) {
+int batch_launch_t(int kind, int tile, const void* dargs, const int* dbpref, int nmem, int nblocks, cudaStream_t s) {
     if (nblocks <= 0 || nmem <= 0) return FHD_OK;
     using SA = StageArgs<NS, R, NZ>;
     const SA* sa = static_cast<const SA*>(dargs);
     switch (kind) {
         case 0: k_cellprep_b<NS, R><<<nblocks, 128, 0, s>>>(static_cast<const PrepArgs<NS, R>*>(dargs), dbpref, nmem); break;
         case 1: k_taus_b<NS, R, NZ><<<nblocks, 128, 0, s>>>(sa, dbpref, nmem); break;
-        case 2: k_faces_b<NS, R, NZ, 0><<<nblocks, 128, 0, s>>>(sa, dbpref, nmem); break;
-        case 3: k_faces_b<NS, R, NZ, 1><<<nblocks, 128, 0, s>>>(sa, dbpref, nmem); break;
-        case 4: k_faces_b<NS, R, NZ, 2><<<nblocks, 128, 0, s>>>(sa, dbpref, nmem); break;
+        case 2:
+        case 3:
+        case 4:
+            if (tile < 0 || tile >= kNumBatchFaceTiles) tile = NS <= 2 ? 0 : kNumBatchFaceTiles - 1;
+            if (tile == 0) batch_faces_t<NS, R, NZ, kBatchFaceMinBlocks[0]>(kind, sa, dbpref, nmem, nblocks, s);
+            else if (tile == 1) batch_faces_t<NS, R, NZ, kBatchFaceMinBlocks[1]>(kind, sa, dbpref, nmem, nblocks, s);
+            else batch_faces_t<NS, R, NZ, kBatchFaceMinBlocks[2]>(kind, sa, dbpref, nmem, nblocks, s);
+            break;
         case 5: k_update_b<NS, R, NZ><<<nblocks, 128, 0, s>>>(sa, dbpref, nmem); break;
         case 6: k_convert_b<NS><<<nblocks, 128, 0, s>>>(static_cast<const ConvArgs<NS>*>(dargs), dbpref, nmem); break;
         default: return FHD_ERR_BAD_ARG;

@@ -253,6 +253,20 @@ int fhd_batch_size(const fhd_batch* batch);
 /* Latched device status of one member (waits for the stream). */
 int fhd_batch_member_status(fhd_batch* batch, int member);
 int fhd_batch_synchronize(fhd_batch* batch);
+/* Launch shape of the batched face-flux kernels: tile 0 .. fhd_batch_num_tiles()-1
+ * caps them at 64, 80 or 128 registers per thread (8, 6 or 4 resident blocks of
+ * 128), -1 restores the default (64 up to two species, 128 above).  Takes effect
+ * at the next step. */
+int fhd_batch_num_tiles(void);
+int fhd_batch_set_tile(fhd_batch* batch, int tile);
+/* The batch's autotuner: times the face-flux launches of one RK stage over the
+ * current members for every tile (one untimed round, then reps timed rounds,
+ * CUDA events on the batch stream) and keeps the fastest.  Those launches write
+ * only the stage's face-flux scratch, which every stage recomputes before reading
+ * it, so no member's state changes; run it after at least one step so that their
+ * inputs are the members' fields.  ms (optional, fhd_batch_num_tiles() entries)
+ * receives the mean milliseconds of each tile, *best (optional) the choice. */
+int fhd_batch_autotune(fhd_batch* batch, int reps, double* ms, int* best);
 
 /* ---- running statistics ----------------------------------------------------------
  * The per-cell part of evaluateStatsStag3D (statsStag.cpp:10-77), which the

@@ -48,3 +48,12 @@ def test_struct_layouts_match_header(tmp_path):
 def test_strerror_is_callable_without_gpu():
     lib = capi.load()
     assert lib.fhd_strerror(capi.FHD_ERR_MASSFRAC).startswith(b"mass fraction")
+
+
+def test_batch_tile_entry_points_validate_without_gpu():
+    """The batch's launch-shape choices and the argument checks of its tile calls
+    (no batch object needed, so no GPU)."""
+    lib = capi.load()
+    assert lib.fhd_batch_num_tiles() == 3
+    assert lib.fhd_batch_set_tile(None, 0) == capi.FHD_ERR_BAD_ARG
+    assert lib.fhd_batch_autotune(None, 3, None, None) == capi.FHD_ERR_BAD_ARG

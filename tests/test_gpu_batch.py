@@ -92,6 +92,36 @@ def test_fp64_batch_after_mixed_runs_matches_alone():
     b.close()
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_every_face_tile_and_the_autotuner_keep_member_results(precision):
+    """Each register cap of the batched face kernels gives the members the result
+    they get alone (FP64 bit for bit), and the autotuner, run between steps,
+    changes no member's state."""
+    ps = [argon(12, dx=8e-6, T_init=280.0, seed=31, precision=precision),
+          argon((10, 14, 8), dx=8e-6, rho0=2.2e-3, seed=32, precision=precision)]
+    dts = [stable_dt(p) for p in ps]
+    refs = [alone(p, dt, 3) for p, dt in zip(ps, dts)]
+    tol = 0.0 if precision == 0 else MIXED_TOL
+    for tile in [0, 1, 2, "auto"]:
+        b = Batch(2, precision)
+        sts = [StagState(p, "cuda", aux=False) for p in ps]
+        for p, st, dt in zip(ps, sts, dts):
+            b.add(p, st, dt)
+        if tile == "auto":
+            b.step(1, graph=True)
+            best, ms = b.autotune(reps=2)
+            assert best in (0, 1, 2) and sorted(ms) == list(Batch.TILE_REGS)
+            assert all(v > 0 for v in ms.values()), ms
+            b.step(2, graph=True)
+        else:
+            b.set_tile(tile)
+            b.step(3, graph=True)
+        b.synchronize()
+        for st, ref in zip(sts, refs):
+            assert not same(st, ref, tol), (tile, same(st, ref, tol))
+        b.close()
+
+
 def test_members_join_and_leave_between_steps():
     pa = argon(16, dx=8e-6, seed=21)
     pb = mixture4(12, dx=8e-6, seed=22)
