@@ -81,7 +81,7 @@ FHD_D float divc(const DevParams&, float a, float b, float) { return a / b; }
 FHD_D double divc0(const DevParams& P, double a, double b, double y) {
     return div_rcp_z(a, b, y, P.div_lo, P.div_span);
 }
-FHD_D float divc0(const DevParams&, float a, float b, float) { return a / b; }
+FHD_D float divc0(const DevParams&, float a, float b, float) { return div_zero_short(a, b); }
 // a / b for a cell value b used as a divisor several times, y = 1.0 / b
 FHD_D double divv(const DevParams& P, double a, double b, double y) {
     return div_rcp_any(a, b, y, P.div_lo, P.div_span);
@@ -90,7 +90,7 @@ FHD_D float divv(const DevParams&, float a, float b, float) { return a / b; }
 // a / b for a cell value b where the dividend is often exactly zero (the Soret
 // terms of identical species, whose thermal diffusion ratios vanish)
 FHD_D double divz(double a, double b) { return div_zero_short(a, b); }
-FHD_D float divz(float a, float b) { return a / b; }
+FHD_D float divz(float a, float b) { return div_zero_short(a, b); }
 
 FHD_D uint64_t noise_step(const DevParams& P) { return P.step_ptr ? *P.step_ptr : P.step; }
 

@@ -61,6 +61,22 @@ FHD_DIV_HD double div_zero_short(double a, double b) {
     return a / b;
 }
 
+// single precision: the same zero-dividend short cut for a normal b (exponent
+// field 1..254); otherwise the plain correctly rounded division
+FHD_DIV_HD uint32_t div_bits(float x) {
+#if defined(__CUDA_ARCH__)
+    return __float_as_uint(x);
+#else
+    uint32_t u;
+    std::memcpy(&u, &x, sizeof(u));
+    return u;
+#endif
+}
+FHD_DIV_HD float div_zero_short(float a, float b) {
+    if (a == 0.0f && ((div_bits(b) & 0x7fffffffu) - 0x00800000u) < 0x7f000000u) return a * b;
+    return a / b;
+}
+
 // the inputs outside the windows, out of line (one copy per module, two arguments
 // so that call sites stay light)
 #if defined(__CUDA_ARCH__)

@@ -137,6 +137,27 @@ int main(int argc, char** argv) {
         check_z(rnd(-1022, 1023), b);
     }
 
+    // single precision short cut
+    std::uniform_int_distribution<uint32_t> fbits(0u, 0xffffffffu);
+    auto fsame = [](float x, float y) {
+        uint32_t ux, uy;
+        std::memcpy(&ux, &x, 4);
+        std::memcpy(&uy, &y, 4);
+        return (std::isnan(x) && std::isnan(y)) || ux == uy;
+    };
+    for (long r = 0; r < n_rand / 10; ++r) {
+        uint32_t ub = fbits(g);
+        float b;
+        std::memcpy(&b, &ub, 4);
+        for (float a : {0.0f, -0.0f, 1.5f, -3.0e-30f}) {
+            ++checked;
+            const float q = fhd::div_zero_short(a, b), ref = a / b;
+            if (!fsame(q, ref)) {
+                if (bad < 10) std::printf("mismatch (f32 zero short cut) a=%a b=%a got %a want %a\n", a, b, q, ref);
+                ++bad;
+            }
+        }
+    }
     std::printf("checked %ld mismatches %ld\n", checked, bad);
     return bad == 0 ? 0 : 1;
 }

@@ -12,7 +12,7 @@ import torch
 from fhdex_b200.context import Context
 from fhdex_b200.params import argon, stable_dt
 from fhdex_b200.state import StagState
-from tests.theory import equilibrium_variances
+from fhdex_b200.equilibrium import equilibrium_variances
 
 pytestmark = pytest.mark.gpu
 
@@ -66,3 +66,15 @@ def test_equilibrium_variances_and_structure_factor(precision):
     assert whole == pytest.approx(1.0, abs=0.03)
     assert low == pytest.approx(1.0, abs=0.05)
     assert high == pytest.approx(1.0, abs=0.05)
+
+
+def test_batched_mixed_equilibrium_within_one_percent():
+    """The batched mixed-precision form at equilibrium (8 independent 32^3 runs,
+    dt/2, 150 snapshots): every variance within 1 % of the theory.  (At the full
+    stable dt the temperature variance carries a ~1.3 % time-discretisation excess,
+    identical in FP64 and mixed; it falls ~8x at dt/2.)"""
+    from fhdex_b200.equilibrium import batch_variance_ratios
+    ratios, _ = batch_variance_ratios(members=8, precision=1, dt_scale=0.5, warm=2000, every=10)
+    print({k: f"{v:.5f}" for k, v in ratios.items()})
+    for k, r in ratios.items():
+        assert r == pytest.approx(1.0, abs=0.01), (k, r)

@@ -11,7 +11,7 @@ from fhdex_b200.params import argon, mixture4, stable_dt
 from fhdex_b200.state import StagState
 from fhdex_b200.stats import StatsState
 from tests.helpers import perturbed_state
-from tests.theory import equilibrium_variances
+from fhdex_b200.equilibrium import equilibrium_variances
 
 pytestmark = pytest.mark.gpu
 

@@ -52,7 +52,7 @@ def test_density_structure_factor_of_the_step_is_flat():
     from fhdex_b200.context import Context
     from fhdex_b200.params import argon, stable_dt
     from fhdex_b200.state import StagState
-    from tests.theory import equilibrium_variances
+    from fhdex_b200.equilibrium import equilibrium_variances
     n = 32
     p = argon(n, dx=8e-6, seed=7)
     st = StagState(p, "cuda", aux=False)

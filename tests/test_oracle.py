@@ -14,7 +14,7 @@ import torch
 from fhdex_b200.params import argon, hard_sphere_single_gas, mixture4, parse_inputs, stable_dt
 from fhdex_b200.state import StagState, StepNoise
 from tests.helpers import perturbed_state, seeded_noise
-from tests.theory import equilibrium_variances
+from fhdex_b200.equilibrium import equilibrium_variances
 
 
 def test_gio_reduces_to_closed_form_hard_sphere(oracle):
