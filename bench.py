@@ -551,8 +551,9 @@ def run_serve(args):
     nspecies in {1,2,4}, steps U{100..2000}, precision FP64/mixed; continuous
     batching vs serving one request at a time with the plain FP64 step."""
     import torch
-    from fhdex_b200.serve import Server, latency_stats, poisson_trace, run_alone
+    from fhdex_b200.serve import Server, latency_stats, poisson_trace, run_alone, warm_kernels
     torch.cuda.set_device(0)
+    warm_kernels(0)                  # both paths start with every kernel loaded
     steps = (args.serve_min_steps, args.serve_max_steps)
     trace = poisson_trace(args.requests, rate=args.rate, seed=args.seed, steps=steps)
     srv = Server(chunk=args.chunk)

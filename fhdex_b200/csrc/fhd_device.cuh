@@ -87,6 +87,12 @@ FHD_D double divv(const DevParams& P, double a, double b, double y) {
     return div_rcp_any(a, b, y, P.div_lo, P.div_span);
 }
 FHD_D float divv(const DevParams&, float a, float b, float) { return a / b; }
+// a / Dbin with the reciprocal path for up to two species (see transport_gio)
+template <int NS, class R>
+FHD_D R div_dbin(const DevParams& P, R a, R b, R y) {
+    if constexpr (NS <= 2) return divv(P, a, b, y);
+    else return a / b;
+}
 // a / b for a cell value b where the dividend is often exactly zero (the Soret
 // terms of identical species, whose thermal diffusion ratios vanish)
 FHD_D double divz(double a, double b) { return div_zero_short(a, b); }
@@ -181,7 +187,7 @@ FHD_D void D_GIO1(const DevParams& P, const R (&Dbin)[NS][NS], const R (&rDbin)[
         R term2 = R(0.);
 #pragma unroll
         for (int j = 0; j < NS; ++j)
-            if (j != i) term2 = term2 + divv(P, Xkp[j], Dbin[i][j], rDbin[i][j]);
+            if (j != i) term2 = term2 + div_dbin<NS, R>(P, Xkp[j], Dbin[i][j], rDbin[i][j]);
         Di[i] = (R(1.) - Ykp[i]) / term2;
     }
 #pragma unroll
@@ -207,10 +213,10 @@ FHD_D void D_GIO1(const DevParams& P, const R (&Dbin)[NS][NS], const R (&rDbin)[
                 R term1 = R(0.);
 #pragma unroll
                 for (int k = 0; k < NS; ++k)
-                    if (k != i) term1 = term1 + divv(P, Xkp[i] * Xkp[k], Dbin[i][k], rDbin[i][k]);
+                    if (k != i) term1 = term1 + div_dbin<NS, R>(P, Xkp[i] * Xkp[k], Dbin[i][k], rDbin[i][k]);
                 Deltamat = term1;
             } else {
-                Deltamat = divv(P, -Xkp[i] * Xkp[j], Dbin[i][j], rDbin[i][j]);
+                Deltamat = div_dbin<NS, R>(P, -Xkp[i] * Xkp[j], Dbin[i][j], rDbin[i][j]);
             }
             R z = -Deltamat;
             if (i == j) z = z + Mmat[i];
@@ -313,11 +319,14 @@ FHD_D bool transport_gio(const DevParams& P, R rho, R temperature, R pressure, c
                          (pressure * pi * dij * dij);
         }
     // reciprocals of the off-diagonal binary diffusivities, each a divisor ~7 times below
+    // (up to two species: one reciprocal for 14 divisions; with more species the
+    // reciprocals held across the solves cost more in spills than they save)
     R rDbin[NS][NS];
 #pragma unroll
     for (int i = 0; i < NS; ++i)
 #pragma unroll
-        for (int j = 0; j < NS; ++j) rDbin[i][j] = (i == j) ? R(0.) : (j < i ? rDbin[j][i] : R(1.) / Dbin[i][j]);
+        for (int j = 0; j < NS; ++j)
+            rDbin[i][j] = (i == j || NS > 2) ? R(0.) : (j < i ? rDbin[j][i] : R(1.) / Dbin[i][j]);
     // viscosity
     R amat[NS][NS], Bi[NS], rhs[NS];
 #pragma unroll
@@ -375,11 +384,11 @@ FHD_D bool transport_gio(const DevParams& P, R rho, R temperature, R pressure, c
 #pragma unroll
                 for (int k = 0; k < NS; ++k)
                     if (k != i)
-                        a += divc(P, divv(P, Xkp[i] * Xkp[k], Dbin[i][k], rDbin[i][k]) * R(P.mu[i][k]), R(P.msum[i][k]),
+                        a += divc(P, div_dbin<NS, R>(P, Xkp[i] * Xkp[k], Dbin[i][k], rDbin[i][k]) * R(P.mu[i][k]), R(P.msum[i][k]),
                                   R(P.rmsum[i][k])) * R(P.kfac[i][k]);
                 amat[i][i] = a;
             } else {
-                amat[i][j] = divc(P, divv(P, R(-1.0) * Xkp[i] * Xkp[j], Dbin[i][j], rDbin[i][j]) * R(P.mu[i][j]),
+                amat[i][j] = divc(P, div_dbin<NS, R>(P, R(-1.0) * Xkp[i] * Xkp[j], Dbin[i][j], rDbin[i][j]) * R(P.mu[i][j]),
                                   R(P.msum[i][j]), R(P.rmsum[i][j])) * R(P.koff);
             }
         }
@@ -418,11 +427,11 @@ FHD_D bool transport_gio(const DevParams& P, R rho, R temperature, R pressure, c
 #pragma unroll
                 for (int k = 0; k < NS; ++k)
                     if (k != i)
-                        a -= divc(P, divv(P, R(0.5) * Xkp[k], Dbin[i][k], rDbin[i][k]) * R(P.mm[k]), R(P.msum[i][k]),
+                        a -= divc(P, div_dbin<NS, R>(P, R(0.5) * Xkp[k], Dbin[i][k], rDbin[i][k]) * R(P.mm[k]), R(P.msum[i][k]),
                                   R(P.rmsum[i][k])) * R(P.cfac);
                 row[j] = a;
             } else {
-                row[j] = divc(P, divv(P, R(0.5) * Xkp[j], Dbin[i][j], rDbin[i][j]) * R(P.mm[i]), R(P.msum[i][j]),
+                row[j] = divc(P, div_dbin<NS, R>(P, R(0.5) * Xkp[j], Dbin[i][j], rDbin[i][j]) * R(P.mm[i]), R(P.msum[i][j]),
                               R(P.rmsum[i][j])) * R(P.cfac);
             }
         }

@@ -75,6 +75,30 @@ def poisson_trace(nreq: int, rate: float = 50.0, seed: int = 0, edge=(16, 128), 
     return out
 
 
+def warm_kernels(device: int = 0, ns_choices=(1, 2, 4), precisions=(0, 1), n: int = 16):
+    """Loads every kernel a served trace can use before anything is timed (CUDA
+    loads a kernel's module on its first launch): per (species count, precision)
+    one n^3 member through the batched step (graph and direct launches) and one
+    single-run step, as the solo lane and the one-at-a-time baseline use."""
+    for ns in ns_choices:
+        for prec in precisions:
+            p = request_params(Request(0, 0.0, n, ns, 1, prec, seed=1))
+            dt = stable_dt(p)
+            b = Batch(ns, prec, device)
+            st = StagState(p, f"cuda:{device}", aux=False)
+            b.add(p, st, dt)
+            b.step(1, graph=True)
+            b.step(1, graph=False)
+            b.synchronize()
+            b.close()
+            ctx = Context(p, device)
+            st1 = StagState(p, f"cuda:{device}", aux=False)
+            ctx.init_state(st1)
+            ctx.rk3_step(st1, dt, 0, aux=False)
+            torch.cuda.synchronize(device)
+            ctx.close()
+
+
 def footprint_bytes(p: Params) -> int:
     """Device bytes of one run: the state MultiFabs plus the batch's stage scratch."""
     n = p.n_cells
@@ -109,12 +133,14 @@ def ensemble(members: int = 512, seed: int = 0, precision: int = 1, sizes=(32, 6
 
 
 class _Class:
-    """One (species count, precision) class: its batch, stream and the chunk in flight."""
+    """One (species count, precision, size bucket) class: its batch, stream and the
+    chunk in flight."""
 
-    def __init__(self, ns, precision, device):
+    def __init__(self, ns, precision, device, priority=-1):
         self.batch = Batch(ns, precision, device)
-        # small requests: high-priority stream, so they are not held back by solo runs
-        self.stream = torch.cuda.Stream(device, priority=-1)
+        # batched requests: higher-priority streams than the solo runs (the smaller
+        # the boxes, the higher), so short requests are not held back by long ones
+        self.stream = torch.cuda.Stream(device, priority=priority)
         self.batch.set_stream(self.stream)
         self.event = torch.cuda.Event()
         self.inflight = 0          # steps of the chunk in flight (0 = idle)
@@ -146,22 +172,31 @@ class _Solo:
 class Server:
     """solo_cells: requests with at least this many cells run alone on their own
     stream with the single-run kernels (batching brings nothing to a launch that
-    already fills the GPU); smaller ones join their class batch."""
+    already fills the GPU); smaller ones join the batch of their class (species
+    count, precision, size bucket).  small_cells splits the batched requests into
+    two size buckets (0: one bucket): a batch advances all its members together, so
+    a small box batched with a large one would move at the large one's pace.
+    Batched classes run on priority -1 streams (the small bucket on small_priority),
+    solo runs on priority 0."""
 
     def __init__(self, device: int = 0, hbm_budget: int | None = None, chunk: int = 20,
-                 solo_cells: int = 96 ** 3):
+                 solo_cells: int = 96 ** 3, small_cells: int = 40 ** 3, small_priority: int = -3):
         self.device = device
         free, total = torch.cuda.mem_get_info(device)
         self.budget = hbm_budget if hbm_budget is not None else int(0.6 * free)
         self.chunk = chunk
         self.solo_cells = solo_cells
+        self.small_cells = small_cells
+        self.small_priority = small_priority
         self.classes: dict = {}
         self.solos: list = []
 
-    def _class(self, ns, precision) -> _Class:
-        key = (ns, precision)
+    def _class(self, ns, precision, cells) -> _Class:
+        bucket = 0 if cells < self.small_cells else 1
+        key = (ns, precision, bucket)
         if key not in self.classes:
-            self.classes[key] = _Class(ns, precision, self.device)
+            self.classes[key] = _Class(ns, precision, self.device,
+                                       priority=self.small_priority if bucket == 0 else -1)
         return self.classes[key]
 
     def _busy(self):
@@ -195,7 +230,8 @@ class Server:
                 pending.pop(0)
                 used += fb
                 st = StagState(p, f"cuda:{self.device}", aux=False)
-                if p.n_cells[0] * p.n_cells[1] * p.n_cells[2] >= self.solo_cells:
+                cells = p.n_cells[0] * p.n_cells[1] * p.n_cells[2]
+                if cells >= self.solo_cells:
                     torch.cuda.current_stream(self.device).synchronize()
                     s = _Solo(r, p, st, fb, self.device)
                     s.ctx.init_state(st)
@@ -203,7 +239,7 @@ class Server:
                     r.start = time.perf_counter() - t0
                     self.solos.append(s)
                 else:
-                    self._class(p.nspecies, p.precision).queue.append((r, p, st, fb))
+                    self._class(p.nspecies, p.precision, cells).queue.append((r, p, st, fb))
             progressed = False
             for s in list(self.solos):
                 if s.inflight:

@@ -150,11 +150,12 @@ def test_members_join_and_leave_between_steps():
 
 def test_server_results_match_runs_alone():
     """Requests served with continuous batching (joining and leaving batches of
-    both precisions and species counts at different times, and boxes of 11^3 cells
-    or more on the solo lane) end in exactly the state they reach when run alone."""
+    both precisions, species counts and size buckets at different times, and boxes of
+    11^3 cells or more on the solo lane) end in exactly the state they reach when run
+    alone."""
     from fhdex_b200.serve import Server, poisson_trace, request_params
     trace = poisson_trace(8, rate=400.0, seed=3, edge=(8, 14), steps=(3, 9))
-    srv = Server(chunk=2, solo_cells=11 ** 3)
+    srv = Server(chunk=2, solo_cells=11 ** 3, small_cells=9 ** 3)
     reqs, finals, cell_updates, elapsed = srv.run(trace, keep_states=True)
     assert all(r.status == 0 for r in reqs)
     sizes = [r.n for r in reqs]
