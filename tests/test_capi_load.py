@@ -50,6 +50,33 @@ def test_strerror_is_callable_without_gpu():
     assert lib.fhd_strerror(capi.FHD_ERR_MASSFRAC).startswith(b"mass fraction")
 
 
+@pytest.mark.parametrize("change,code", [
+    (dict(nspecies=5), "FHD_ERR_UNSUPPORTED"),
+    (dict(nspecies=0), "FHD_ERR_UNSUPPORTED"),
+    (dict(n_cells=(1, 8, 8)), "FHD_ERR_BAD_ARG"),
+    (dict(n_cells=(2048, 2048, 1024)), "FHD_ERR_UNSUPPORTED"),   # 2^32 cells
+    (dict(algorithm_type=0), "FHD_ERR_UNSUPPORTED"),
+    (dict(stoch_stress_form=2), "FHD_ERR_UNSUPPORTED"),
+    (dict(advection_type=3), "FHD_ERR_UNSUPPORTED"),
+    (dict(precision=7), "FHD_ERR_BAD_ARG"),
+    (dict(visc_type=3, zeta_ratio=-1.0), "FHD_ERR_BAD_ARG"),
+])
+def test_create_rejects_out_of_scope_parameters_without_gpu(change, code):
+    """fhd_create validates the run before touching a device: out-of-scope options
+    and impossible boxes come back as error codes, never as a crash."""
+    from fhdex_b200.params import argon
+    p = argon(8, dx=8e-6)
+    for k, v in change.items():
+        setattr(p, k, v)
+    if "n_cells" in change:
+        p.prob_hi = tuple(p.prob_lo[d] + 8e-6 * p.n_cells[d] for d in range(3))
+    cp = p.to_c()
+    h = C.c_void_p()
+    lib = capi.load()
+    assert lib.fhd_create(C.byref(h), C.byref(cp), 0) == getattr(capi, code)
+    assert not h.value
+
+
 def test_batch_tile_entry_points_validate_without_gpu():
     """The batch's launch-shape choices and the argument checks of its tile calls
     (no batch object needed, so no GPU)."""

@@ -119,6 +119,26 @@ def test_in_kernel_philox_equals_injected_replay(oracle):
         assert not bad, (s, bad[:4])
 
 
+def test_large_ragged_box_in_kernel_noise_bitwise(oracle):
+    """A box large enough for every stage kernel's grid-stride loop to wrap (more
+    work items than the 4736 x 128 threads of a launch) with unequal, non-power-of-
+    two extents: one in-kernel-noise RK3 step equals the oracle fed the materialised
+    noise, bit for bit, including the stage-3 fluxes and transport coefficients."""
+    p = argon((100, 96, 90), dx=8e-6, seed=515)
+    st = perturbed_state(oracle, p, seed=8)
+    d = gpu_copy(st)
+    ctx = Context(p)
+    dt = stable_dt(p)
+    nz = StepNoise(p, "cuda")
+    ctx.fill_step_noise(nz, 0)
+    ctx.rk3_step(d, dt, 0, noise=None, aux=True)
+    torch.cuda.synchronize()
+    assert ctx.status() == 0
+    assert oracle.rk3_step(st, nz.to("cpu"), dt) == 0
+    bad, _ = compare_named(d.named(aux=True), st.named(aux=True))
+    assert not bad, bad[:8]
+
+
 def test_all_tile_shapes_identical(oracle):
     p = argon((12, 10, 9), dx=8e-6)
     st = perturbed_state(oracle, p, seed=7)
