@@ -57,6 +57,14 @@ struct Noise {
         w0 = comb(0.0 + sd * (double)z[0], 0.0 + sd * (double)z[1]);
         w1 = comb(0.0 + sd * (double)z[2], 0.0 + sd * (double)z[3]);
     }
+    // fields fid0 and fid0+1 with their own standard deviations
+    FHD_D void gauss2sd(const DevParams& P, uint32_t fid0, int i, int j, int k, double sd0, double sd1, double& w0,
+                        double& w1) const {
+        float z[4];
+        normal_quad(P.key0, P.key1, canon(P, i, j, k), fid0 >> 1, noise_step(P), z);
+        w0 = comb(0.0 + sd0 * (double)z[0], 0.0 + sd0 * (double)z[1]);
+        w1 = comb(0.0 + sd1 * (double)z[2], 0.0 + sd1 * (double)z[3]);
+    }
     FHD_D double gauss1(const DevParams& P, uint32_t fid, int i, int j, int k, double sd) const {
         float za, zb;
         normal_pair(P.key0, P.key1, canon(P, i, j, k), fid, noise_step(P), za, zb);
@@ -77,17 +85,38 @@ struct Noise {
     }
     FHD_D void cen_all(const DevParams& P, int i, int j, int k, double (&out)[3]) const {
         if (MODE == NZ_PHILOX) {
-            gauss2(P, fid_cen(0), i, j, k, P.sqrt2, out[0], out[1]);
-            out[2] = gauss1(P, fid_cen(2), i, j, k, P.sqrt2);
+            out[0] = gauss1(P, fid_cen(0), i, j, k, P.sqrt2);
+            gauss2(P, fid_cen(1), i, j, k, P.sqrt2, out[1], out[2]);
         } else {
 #pragma unroll
             for (int d = 0; d < 3; ++d) out[d] = cen(P, d, i, j, k);
         }
     }
+    // The six stress fields of point (i,j,k) in three Philox calls: the centre
+    // fields of cell (i,j,k) with, when `edges`, the yz edge field of node (i,j,k)
+    // (cen_and_yz_edge), then the xy and xz edge fields (xy_xz_edges)
+    FHD_D void cen_and_yz_edge(const DevParams& P, int i, int j, int k, bool edges, double (&wc)[3],
+                               double& we2) const {
+        if (MODE == NZ_PHILOX) {
+            gauss2sd(P, fid_edge(2), i, j, k, 1.0, P.sqrt2, we2, wc[0]);
+            gauss2(P, fid_cen(1), i, j, k, P.sqrt2, wc[1], wc[2]);
+        } else {
+            cen_all(P, i, j, k, wc);
+            if (edges) we2 = edge(P, 2, i, j, k);
+        }
+    }
+    FHD_D void xy_xz_edges(const DevParams& P, int i, int j, int k, double& we0, double& we1) const {
+        if (MODE == NZ_PHILOX) {
+            gauss2(P, fid_edge(0), i, j, k, 1.0, we0, we1);
+        } else {
+            we0 = edge(P, 0, i, j, k);
+            we1 = edge(P, 1, i, j, k);
+        }
+    }
     FHD_D void edge_all(const DevParams& P, int i, int j, int k, double (&out)[3]) const {
         if (MODE == NZ_PHILOX) {
             gauss2(P, fid_edge(0), i, j, k, 1.0, out[0], out[1]);
-            out[2] = gauss1(P, fid_edge(2), i, j, k, 1.0);
+            out[2] = gauss1(P, fid_edge(2), i, j, k, 1.0);  // (shares its call with centre x)
         } else {
 #pragma unroll
             for (int e = 0; e < 3; ++e) out[e] = edge(P, e, i, j, k);
@@ -124,9 +153,10 @@ struct CellTaus {
     R s[3], d[3];
 };
 
-// diagonal stresses at a cell: stochastic fluxStag.cpp:163-206, deterministic :872-924
+// diagonal stresses at a cell: stochastic fluxStag.cpp:163-206, deterministic :872-924;
+// wc: the three centre noise values W of the cell
 template <int NS, class R, int NZ>
-FHD_D CellTaus<R> cell_taus(const DevParams& P, const Fields<NS, R>& F, const Noise<NZ>& nz, int i, int j, int k) {
+FHD_D CellTaus<R> cell_taus_w(const DevParams& P, const Fields<NS, R>& F, const double (&wc)[3], int i, int j, int k) {
     CellTaus<R> t;
     const R eta = F.eta(i, j, k);
     const bool visc3 = (P.visc_type == 3 || P.visc_type == -3);
@@ -139,8 +169,6 @@ FHD_D CellTaus<R> cell_taus(const DevParams& P, const Fields<NS, R>& F, const No
         if (visc3)
             fac2 = dsqrt(divc(P, R(P.k_B) * zetaT * R(P.volinv) * R(P.dtinv), R(3.0), R(P.r3))) -
                    divc(P, dsqrt(R(2.0) * R(P.k_B) * etaT * R(P.volinv) * R(P.dtinv)), R(3.0), R(P.r3));
-        double wc[3];
-        nz.cen_all(P, i, j, k, wc);
         const R w0 = R(wc[0]), w1 = R(wc[1]), w2 = R(wc[2]);
         const R traceZ = w0 + w1 + w2;
         t.s[0] = (fac1 * w0) + (fac2 * traceZ);
@@ -194,6 +222,13 @@ FHD_D Taus<R> edge_taus_w(const DevParams& P, const Fields<NS, R>& F, double wno
     const R ei = R(0.25) * (F.eta(ai, aj, ak) + F.eta(bi, bj, bk) + F.eta(ci, cj, ck) + F.eta(i, j, k));
     t.d = ei * (g1 + g2);
     return t;
+}
+
+template <int NS, class R, int NZ>
+FHD_D CellTaus<R> cell_taus(const DevParams& P, const Fields<NS, R>& F, const Noise<NZ>& nz, int i, int j, int k) {
+    double wc[3] = {0.0, 0.0, 0.0};
+    if (NZ != NZ_OFF) nz.cen_all(P, i, j, k, wc);
+    return cell_taus_w<NS, R, NZ>(P, F, wc, i, j, k);
 }
 
 template <int NS, class R, int NZ, int E>

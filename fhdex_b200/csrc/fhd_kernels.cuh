@@ -137,16 +137,18 @@ FHD_D void taus_point(const StageArgs<NS, R, NZ>& a, int q) {
     const int nx = P.n[0] + 2, ny = P.n[1] + 2;
     {
         const int i = q % nx - 1, j = (q / nx) % ny - 1, k = q / (nx * ny) - 1;
-        const CellTaus<R> t = cell_taus<NS, R, NZ>(P, a.F, a.noise, i, j, k);
+        const bool edges = i >= 0 && j >= 0 && k >= 0;
+        double wc[3] = {0.0, 0.0, 0.0}, we[3] = {0.0, 0.0, 0.0};
+        if (NZ != NZ_OFF) a.noise.cen_and_yz_edge(P, i, j, k, edges, wc, we[2]);
+        const CellTaus<R> t = cell_taus_w<NS, R, NZ>(P, a.F, wc, i, j, k);
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             a.ct(i, j, k, d) = t.s[d];
             a.ct(i, j, k, 3 + d) = t.d[d];
             a.mc(i, j, k, d) = cen_total<NS, R>(P, a.F, t, d, i, j, k);
         }
-        if (i < 0 || j < 0 || k < 0) return;
-        double we[3] = {0.0, 0.0, 0.0};
-        if (NZ != NZ_OFF) a.noise.edge_all(P, i, j, k, we);
+        if (!edges) return;
+        if (NZ != NZ_OFF) a.noise.xy_xz_edges(P, i, j, k, we[0], we[1]);
         const int hadv = P.advection_type >= 0;
         double ea, eb;
         if (k < P.n[2]) {

@@ -81,9 +81,11 @@ FHD_HD uint32_t canon(const DevParams& P, int i, int j, int k) {
 }
 
 // Field ids: face d comp c (0 energy, 1.. species) -> 16 d + c; edges xy, xz, yz ->
-// 48 + e; centres -> 52 + d.  Fields 2q, 2q+1 share one Philox call.
+// 48 + e; centres -> 51 + d.  Fields 2q, 2q+1 share one Philox call, so the six
+// stress fields of a point take three calls: (edge xy, xz), (edge yz, centre x),
+// (centre y, z).
 FHD_HD uint32_t fid_face(int d, int c) { return (uint32_t)(16 * d + c); }
 FHD_HD uint32_t fid_edge(int e) { return (uint32_t)(48 + e); }
-FHD_HD uint32_t fid_cen(int d) { return (uint32_t)(52 + d); }
+FHD_HD uint32_t fid_cen(int d) { return (uint32_t)(51 + d); }
 
 }  // namespace fhd
