@@ -73,30 +73,37 @@ struct DevParams {
     uint32_t div_lo, div_span;
 };
 
+// a / b in the compute type: FP64 the correctly rounded division (the reference's
+// arithmetic); FP32 (the mixed path, held to a tolerance against FP64) the fast
+// division __fdividef (about 2 ulp; physical divisors stay far below 2^126).
+FHD_D double rdiv(double a, double b) { return a / b; }
+FHD_D float rdiv(float a, float b) { return __fdividef(a, b); }
+
 // a / b for a constant divisor b with y = RN(1/b) from DevParams: bitwise a / b
-// (fhd_div.h); in single precision the plain division
+// (fhd_div.h).  In single precision (the mixed path, held to a tolerance against
+// FP64, not to bitwise parity) the product a * y: within about one FP32 ulp of a / b.
 FHD_D double divc(const DevParams& P, double a, double b, double y) { return div_rcp(a, b, y, P.div_lo, P.div_span); }
-FHD_D float divc(const DevParams&, float a, float b, float) { return a / b; }
+FHD_D float divc(const DevParams&, float a, float, float y) { return a * y; }
 // divc for call sites whose dividend is often exactly zero (zero handled inline)
 FHD_D double divc0(const DevParams& P, double a, double b, double y) {
     return div_rcp_z(a, b, y, P.div_lo, P.div_span);
 }
-FHD_D float divc0(const DevParams&, float a, float b, float) { return div_zero_short(a, b); }
+FHD_D float divc0(const DevParams&, float a, float, float y) { return a * y; }
 // a / b for a cell value b used as a divisor several times, y = 1.0 / b
 FHD_D double divv(const DevParams& P, double a, double b, double y) {
     return div_rcp_any(a, b, y, P.div_lo, P.div_span);
 }
-FHD_D float divv(const DevParams&, float a, float b, float) { return a / b; }
+FHD_D float divv(const DevParams&, float a, float, float y) { return a * y; }
 // a / Dbin with the reciprocal path for up to two species (see transport_gio)
 template <int NS, class R>
 FHD_D R div_dbin(const DevParams& P, R a, R b, R y) {
     if constexpr (NS <= 2) return divv(P, a, b, y);
-    else return a / b;
+    else return rdiv(a, b);
 }
 // a / b for a cell value b where the dividend is often exactly zero (the Soret
 // terms of identical species, whose thermal diffusion ratios vanish)
 FHD_D double divz(double a, double b) { return div_zero_short(a, b); }
-FHD_D float divz(float a, float b) { return div_zero_short(a, b); }
+FHD_D float divz(float a, float b) { return rdiv(a, b); }
 
 FHD_D uint64_t noise_step(const DevParams& P) { return P.step_ptr ? *P.step_ptr : P.step; }
 
@@ -107,7 +114,7 @@ FHD_D void GetMolfrac(const DevParams& P, const R (&Y)[NS], R (&X)[NS]) {
     R molmix = R(0.);
 #pragma unroll
     for (int n = 0; n < NS; ++n) molmix += divc(P, Y[n], R(P.molmass[n]), R(P.rmolmass[n]));
-    molmix = R(1.) / molmix;
+    molmix = rdiv(R(1.), molmix);
 #pragma unroll
     for (int n = 0; n < NS; ++n) X[n] = divc(P, Y[n] * molmix, R(P.molmass[n]), R(P.rmolmass[n]));
 }
@@ -120,7 +127,7 @@ FHD_D R GetTemperature(const DevParams& P, R energy, const R (&Y)[NS]) {
         cvmix += Y[n] * R(P.hcv[n]);
         e0mix += Y[n] * R(P.e0[n]);
     }
-    return (energy - e0mix) / cvmix;
+    return rdiv(energy - e0mix, cvmix);
 }
 
 template <int NS, class R>
@@ -128,8 +135,8 @@ FHD_D R GetPressureGas(const DevParams& P, const R (&Y)[NS], R density, R temp) 
     R molmix = R(0.);
 #pragma unroll
     for (int n = 0; n < NS; ++n) molmix += divc(P, Y[n], R(P.molmass[n]), R(P.rmolmass[n]));
-    molmix = R(1.) / molmix;
-    return density * (R(P.Runiv) / molmix) * temp;
+    molmix = rdiv(R(1.), molmix);
+    return density * rdiv(R(P.Runiv), molmix) * temp;
 }
 
 template <int NS, class R>
@@ -165,7 +172,7 @@ FHD_D void CholeskyDecomp(R (&a)[NS * NS], R (&sqda)[NS * NS]) {
                 if (sum1 <= R(0.)) { p[i] = R(0.); ising = 1; }
                 else p[i] = dsqrt(sum1);
             }
-            if (ising == 0) a[j * NS + i] = sum1 / p[i];
+            if (ising == 0) a[j * NS + i] = rdiv(sum1, p[i]);
             else a[j * NS + i] = R(0.);
         }
     }
@@ -188,12 +195,12 @@ FHD_D void D_GIO1(const DevParams& P, const R (&Dbin)[NS][NS], const R (&rDbin)[
 #pragma unroll
         for (int j = 0; j < NS; ++j)
             if (j != i) term2 = term2 + div_dbin<NS, R>(P, Xkp[j], Dbin[i][j], rDbin[i][j]);
-        Di[i] = (R(1.) - Ykp[i]) / term2;
+        Di[i] = rdiv(R(1.) - Ykp[i], term2);
     }
 #pragma unroll
     for (int i = 0; i < NS; ++i) {
-        Mmat[i] = Xkp[i] / Di[i];
-        Minv[i] = Di[i] / Xkp[i];
+        Mmat[i] = rdiv(Xkp[i], Di[i]);
+        Minv[i] = rdiv(Di[i], Xkp[i]);
     }
 #pragma unroll
     for (int i = 0; i < NS; ++i)
@@ -288,13 +295,13 @@ FHD_D bool transport_gio(const DevParams& P, R rho, R temperature, R pressure, c
         sumYk += Yk[n];
     }
 #pragma unroll
-    for (int n = 0; n < NS; ++n) Yk[n] /= sumYk;
+    for (int n = 0; n < NS; ++n) Yk[n] = rdiv(Yk[n], sumYk);
 
     const R pi = R(3.1415926535897932);
     R mbar = R(0.0);
 #pragma unroll
     for (int n = 0; n < NS; ++n) mbar += divc(P, Yk[n], R(P.mm[n]), R(P.rmm[n]));
-    mbar = R(1.0) / mbar;
+    mbar = rdiv(R(1.0), mbar);
     R Xk[NS], Xkp[NS], Ykp[NS];
     R Xksum = R(0.0);
 #pragma unroll
@@ -305,7 +312,7 @@ FHD_D bool transport_gio(const DevParams& P, R rho, R temperature, R pressure, c
 #pragma unroll
     for (int n = 0; n < NS; ++n) Xkp[n] = Xk[n] + R(1.0e-16) * (divc(P, Xksum, R(double(NS)), R(1.0 / double(NS))) - Xk[n]);
 #pragma unroll
-    for (int n = 0; n < NS; ++n) Ykp[n] = Xkp[n] * R(P.mm[n]) / mbar;
+    for (int n = 0; n < NS; ++n) Ykp[n] = rdiv(Xkp[n] * R(P.mm[n]), mbar);
 
     const R kT = R(P.k_B) * temperature;
     R Dbin[NS][NS];
@@ -315,8 +322,8 @@ FHD_D bool transport_gio(const DevParams& P, R rho, R temperature, R pressure, c
         for (int j = 0; j < NS; ++j) {
             if (j < i) { Dbin[i][j] = Dbin[j][i]; continue; }  // symmetric: bitwise equal
             const R dij = R(P.diam[i][j]);
-            Dbin[i][j] = (R(3.0) / R(16.0)) * dsqrt(divc(P, R(2.0) * pi * kT * kT * kT, R(P.mu[i][j]), R(P.rmu[i][j]))) /
-                         (pressure * pi * dij * dij);
+            Dbin[i][j] = rdiv((R(3.0) / R(16.0)) * dsqrt(divc(P, R(2.0) * pi * kT * kT * kT, R(P.mu[i][j]), R(P.rmu[i][j]))),
+                              pressure * pi * dij * dij);
         }
     // reciprocals of the off-diagonal binary diffusivities, each a divisor ~7 times below
     // (up to two species: one reciprocal for 14 divisions; with more species the
@@ -326,7 +333,7 @@ FHD_D bool transport_gio(const DevParams& P, R rho, R temperature, R pressure, c
     for (int i = 0; i < NS; ++i)
 #pragma unroll
         for (int j = 0; j < NS; ++j)
-            rDbin[i][j] = (i == j || NS > 2) ? R(0.) : (j < i ? rDbin[j][i] : R(1.) / Dbin[i][j]);
+            rDbin[i][j] = (i == j || NS > 2) ? R(0.) : (j < i ? rDbin[j][i] : rdiv(R(1.), Dbin[i][j]));
     // viscosity
     R amat[NS][NS], Bi[NS], rhs[NS];
 #pragma unroll
@@ -337,15 +344,15 @@ FHD_D bool transport_gio(const DevParams& P, R rho, R temperature, R pressure, c
 #pragma unroll
         for (int j = 0; j < NS; ++j) {
             if (i == j) {
-                R a = Xkp[i] * Xkp[i] / eta1;
+                R a = rdiv(Xkp[i] * Xkp[i], eta1);
 #pragma unroll
                 for (int k = 0; k < NS; ++k)
                     if (k != i)
-                        a += R(2.0) * kT * Xkp[i] * Xkp[k] / (pressure * Dbin[i][k] * R(P.msum[i][k])) *
+                        a += rdiv(R(2.0) * kT * Xkp[i] * Xkp[k], pressure * Dbin[i][k] * R(P.msum[i][k])) *
                              R(P.vfac[i][k]);
                 amat[i][i] = a;
             } else {
-                amat[i][j] = R(2.0) * kT * Xkp[i] * Xkp[j] / (pressure * Dbin[i][j] * R(P.msum[i][j])) *
+                amat[i][j] = rdiv(R(2.0) * kT * Xkp[i] * Xkp[j], pressure * Dbin[i][j] * R(P.msum[i][j])) *
                              R(P.voff);
             }
         }
@@ -354,18 +361,18 @@ FHD_D bool transport_gio(const DevParams& P, R rho, R temperature, R pressure, c
     for (int j = 0; j < NS - 1; ++j)
 #pragma unroll
         for (int i = j + 1; i < NS; ++i) {
-            const R fact1 = amat[i][j] / amat[j][j];
+            const R fact1 = rdiv(amat[i][j], amat[j][j]);
 #pragma unroll
             for (int k = 0; k < NS; ++k) amat[i][k] -= fact1 * amat[j][k];
             Bi[i] -= fact1 * Bi[j];
         }
-    Bi[NS - 1] /= amat[NS - 1][NS - 1];
+    Bi[NS - 1] = rdiv(Bi[NS - 1], amat[NS - 1][NS - 1]);
 #pragma unroll
     for (int i = NS - 2; i > -1; --i) {
         R sum1 = R(0.0);
 #pragma unroll
         for (int j = NS - 1; j > i; --j) sum1 += amat[i][j] * Bi[j];
-        Bi[i] = (Bi[i] - sum1) / amat[i][i];
+        Bi[i] = rdiv(Bi[i] - sum1, amat[i][i]);
     }
     R eta = R(0.0);
 #pragma unroll
@@ -380,7 +387,7 @@ FHD_D bool transport_gio(const DevParams& P, R rho, R temperature, R pressure, c
 #pragma unroll
         for (int j = 0; j < NS; ++j) {
             if (i == j) {
-                R a = Xkp[i] * Xkp[i] / Dbin[i][j] * R(2.0) * R(1.0);
+                R a = rdiv(Xkp[i] * Xkp[i], Dbin[i][j]) * R(2.0) * R(1.0);
 #pragma unroll
                 for (int k = 0; k < NS; ++k)
                     if (k != i)
@@ -397,23 +404,23 @@ FHD_D bool transport_gio(const DevParams& P, R rho, R temperature, R pressure, c
     for (int j = 0; j < NS - 1; ++j)
 #pragma unroll
         for (int i = j + 1; i < NS; ++i) {
-            const R fact1 = amat[i][j] / amat[j][j];
+            const R fact1 = rdiv(amat[i][j], amat[j][j]);
 #pragma unroll
             for (int k = 0; k < NS; ++k) amat[i][k] -= fact1 * amat[j][k];
             Bi[i] -= fact1 * Bi[j];
         }
-    Bi[NS - 1] /= amat[NS - 1][NS - 1];
+    Bi[NS - 1] = rdiv(Bi[NS - 1], amat[NS - 1][NS - 1]);
 #pragma unroll
     for (int i = NS - 2; i > -1; --i) {
         R sum1 = R(0.0);
 #pragma unroll
         for (int j = NS - 1; j > i; --j) sum1 += amat[i][j] * Bi[j];
-        Bi[i] = (Bi[i] - sum1) / amat[i][i];
+        Bi[i] = rdiv(Bi[i] - sum1, amat[i][i]);
     }
     R kappa = R(0.0);
 #pragma unroll
     for (int i = 0; i < NS; ++i) kappa += rhs[i] * Bi[i];
-    kappa *= pressure / temperature;
+    kappa *= rdiv(pressure, temperature);
     c.kappa = kappa;
     // thermal diffusion ratios
 #pragma unroll

@@ -328,7 +328,7 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
 #pragma unroll
         for (int n = 0; n < NS; ++n) { sumy += yy[n]; sumyp += yyp[n]; }
 #pragma unroll
-        for (int n = 0; n < NS; ++n) { yy[n] /= sumy; yyp[n] /= sumyp; }
+        for (int n = 0; n < NS; ++n) { yy[n] = rdiv(yy[n], sumy); yyp[n] = rdiv(yyp[n], sumyp); }
         R MWmix = R(0.);
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
@@ -344,7 +344,7 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
 #pragma unroll
                 for (int n = 0; n < NS; ++n) { DY[s * NS + n] = R(0.); DY[n * NS + s] = R(0.); }
             }
-        MWmix = R(1.) / MWmix;
+        MWmix = rdiv(R(1.), MWmix);
         CholeskyDecomp<NS, R>(DY, sqD);
         const R fwc = dsqrt(divc(P, R(P.k_B) * MWmix * R(P.volinv), R(P.Runiv) * R(P.dt), R(P.rRdt)));
         R zs[NS];
