@@ -310,7 +310,7 @@ FHD_D void update_point(const StageArgs<NS, R, NZ>& a, int q) {
 }
 
 template <int NS, class R, int NZ>
-static __global__ void __launch_bounds__(256) k_update(StageArgs<NS, R, NZ> a) {
+static __global__ void __launch_bounds__(128, 16) k_update(StageArgs<NS, R, NZ> a) {  // HBM-bound: full occupancy
     const int tot = update_count(a);
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) update_point(a, q);
 }

@@ -139,7 +139,9 @@ int launch_stage_part_t(const StageCall& c, int part) {
         }
 #undef FHD_FACES
     } else {
-        k_update<NS, R, NZ><<<grid_for((int64_t)(N[0] + 1) * (N[1] + 1) * (N[2] + 1), b), b, 0, c.stream>>>(a);
+        // 128 threads whatever the tile: the update kernel is capped at 32 registers
+        // for full occupancy (16 blocks of 128 per SM)
+        k_update<NS, R, NZ><<<grid_for((int64_t)(N[0] + 1) * (N[1] + 1) * (N[2] + 1), 128), 128, 0, c.stream>>>(a);
     }
     return cuda_rc(cudaGetLastError());
 }
