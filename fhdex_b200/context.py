@@ -126,6 +126,12 @@ class Context:
         check(self.lib.fhd_fill_random_normal(self._h, mf.fab(), scomp, ncomp, mean, variance, int(overridesync),
                                               int(fillboundary), stream_id), "fhd_fill_random_normal")
 
+    def fill_random_uniform(self, mf, scomp, ncomp, overridesync=True, fillboundary=True, stream_id=0):
+        """MultiFabFillRandomUniform: uniforms in [0, 1) on the valid region."""
+        self._stream()
+        check(self.lib.fhd_fill_random_uniform(self._h, mf.fab(), scomp, ncomp, int(overridesync),
+                                               int(fillboundary), stream_id), "fhd_fill_random_uniform")
+
     def fill_step_noise(self, noise: StepNoise, step: int):
         self._stream()
         self._noise_struct = noise.c_struct()

@@ -442,6 +442,26 @@ int fhd_fill_random_normal(fhd_ctx* c, fhd_fab mf, int scomp, int ncomp, double 
     return rc;
 }
 
+int fhd_fill_random_uniform(fhd_ctx* c, fhd_fab mf, int scomp, int ncomp, int overridesync, int fillboundary,
+                            uint64_t stream_id) {
+    if (!c || !mf.data || scomp < 0 || ncomp < 1 || scomp + ncomp > mf.ncomp) return FHD_ERR_BAD_ARG;
+    int nodal[3] = {mf.nodal[0], mf.nodal[1], mf.nodal[2]};
+    if (!fab_ok(c, mf, nodal, 0, 1, FHD_F64)) return FHD_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    DevParams P = make_dev(c, 1.0, stream_id);
+    // counter word 1 is the field id itself here (0x2000 + comp): apart from the
+    // normal fills' field pairs and from the step noise
+    int rc = noise_fill(P, mf, scomp, ncomp, 0.0, 1.0, 0x2000u + (uint32_t)scomp, 2, c->stream);
+    if (rc) return rc;
+    if (overridesync) rc = override_sync(mf, c->prm.n_cells, c->stream);
+    if (rc) return rc;
+    if (fillboundary && -mf.lo[0] > 0) {
+        GhostReq r{mf, scomp, ncomp};
+        rc = fill_ghosts(&r, 1, c->prm.n_cells, c->stream);
+    }
+    return rc;
+}
+
 int fhd_fill_step_noise(fhd_ctx* c, const fhd_noise* nz, int64_t step) {
     if (!c || !nz) return FHD_ERR_BAD_ARG;
     if (!noise_ok(c, nz)) return FHD_ERR_BAD_ARG;

@@ -612,6 +612,9 @@ static __global__ void __launch_bounds__(128) k_aux_edges_cen(AuxArgs<NS, R, NZ>
 // MultiFabFillRandomNormal body: value = mean + sd*z on the valid region, with z
 // from the counter (canonical point, field = fid0 + comp, stream) -> periodic
 // duplicates are equal (OverrideSync); ghosts by k_ghosts afterwards.
+// MultiFabFillRandomUniform body (use_b = 2): a uniform in [0, 1) with 53 random
+// bits, 27 from the first and 26 from the second word of one Philox call on the
+// counter (canonical point, field = fid0 + comp, stream).
 struct NoiseFillArgs {
     DevParams P;
     Arr4<double> f;
@@ -619,13 +622,23 @@ struct NoiseFillArgs {
     int c0, nc;
     double mean, sd;
     uint32_t fid0;
-    int use_b;        // take z_B of the pair instead of z_A
+    int use_b;        // 0: z_A of the field's pair, 1: z_B, 2: the uniform
 };
+
+FHD_D double uniform53(uint32_t w0, uint32_t w1) {
+    return ((double)(w0 >> 5) * 67108864.0 + (double)(w1 >> 6)) * (1.0 / 9007199254740992.0);
+}
 static __global__ void k_noise_fill(NoiseFillArgs a) {
     const int64_t tot = (int64_t)a.vx * a.vy * a.vz * a.nc;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < tot; q += (int64_t)gridDim.x * blockDim.x) {
         const int i = (int)(q % a.vx), j = (int)((q / a.vx) % a.vy), k = (int)((q / ((int64_t)a.vx * a.vy)) % a.vz);
         const int c = (int)(q / ((int64_t)a.vx * a.vy * a.vz));
+        if (a.use_b == 2) {
+            uint32_t w[4] = {canon(a.P, i, j, k), a.fid0 + (uint32_t)c, (uint32_t)a.P.step, (uint32_t)(a.P.step >> 32)};
+            philox4x32_10(w, a.P.key0, a.P.key1);
+            a.f(i, j, k, a.c0 + c) = uniform53(w[0], w[1]);
+            continue;
+        }
         float za, zb;
         normal_pair(a.P.key0, a.P.key1, canon(a.P, i, j, k), a.fid0 + (uint32_t)c, a.P.step, za, zb);
         a.f(i, j, k, a.c0 + c) = a.mean + a.sd * (double)(a.use_b ? zb : za);

@@ -15,7 +15,8 @@
 //   calculateFluxStag          src_compressible_stag/compressible_functions_stag.H:127-143
 //   calculateTransportCoeffs   src_compressible/compressible_functions.H:37-39
 //   MultiFabFillRandom,
-//   MultiFabFillRandomNormal   src_rng/rng_functions.H:13-22
+//   MultiFabFillRandomNormal,
+//   MultiFabFillRandomUniform  src_rng/rng_functions.H:13-22
 //
 // As in the reference, physics parameters are process globals in namespaces
 // `common` and `compressible` (src_common/common_namespace.H,
@@ -377,6 +378,19 @@ inline void MultiFabFillRandomNormal(fhd::amrex_compat::MultiFab& mf, const int&
     check(fhd_fill_random_normal(context(), mf.fab(), scomp, ncomp, mean, variance, overridesync ? 1 : 0,
                                  fillboundary ? 1 : 0, id),
           "MultiFabFillRandomNormal");
+}
+
+// MultiFabFillRandomUniform (MultiFabFillRandom.cpp:53-66): uniforms in [0, 1) in
+// components scomp..scomp+ncomp-1 of the valid region, then OverrideSync and
+// FillBoundary when asked; independent streams per call as above.
+inline void MultiFabFillRandomUniform(fhd::amrex_compat::MultiFab& mf, const int& scomp, const int& ncomp,
+                                      const fhd::amrex_compat::Geometry& /*geom*/, bool overridesync = true,
+                                      bool fillboundary = true) {
+    using namespace fhd::ref;
+    require_device(mf, "MultiFabFillRandomUniform");
+    const uint64_t id = ++runtime().fill_calls;
+    check(fhd_fill_random_uniform(context(), mf.fab(), scomp, ncomp, overridesync ? 1 : 0, fillboundary ? 1 : 0, id),
+          "MultiFabFillRandomUniform");
 }
 
 // MultiFabFillRandom (MultiFabFillRandom.cpp:5-31): N(0, variance) in one

@@ -183,6 +183,13 @@ int fhd_fill_random_normal(fhd_ctx* ctx, fhd_fab mf, int scomp, int ncomp, doubl
                            double variance, int overridesync, int fillboundary,
                            uint64_t stream_id);
 
+/* MultiFabFillRandomUniform: MultiFabFillRandom.cpp:53-66 (declared
+ * rng_functions.H:20-22).  Uniform values in [0, 1) with 53 random bits (one
+ * Philox-4x32-10 call per point), then OverrideSync / FillBoundary when asked;
+ * `stream_id` selects an independent stream as for the normal fill. */
+int fhd_fill_random_uniform(fhd_ctx* ctx, fhd_fab mf, int scomp, int ncomp, int overridesync,
+                            int fillboundary, uint64_t stream_id);
+
 /* Fills `noise` with exactly the A/B fields the fused step generates
  * in-kernel for (seed, step): lets a caller replay an in-kernel-noise step
  * through the injected-noise path. */
