@@ -333,6 +333,20 @@ def run_ours(args):
             "algorithmic_bytes_per_launch": alg_bytes,
             "step_breakdown_ms": {k: v[0] / args.steps for k, v in prof.items()}}
 
+    # the same steps replayed from a CUDA graph the context captures once
+    # (fhd_rk3_steps_stag): what small, launch-bound boxes gain
+    side = torch.cuda.Stream(local)
+    with torch.cuda.stream(side):
+        ctx.rk3_steps(st, dt, args.warmup + args.steps, 1)   # capture + one untimed replay
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record()
+        ctx.rk3_steps(st, dt, args.warmup + args.steps + 1, args.steps)
+        g1.record()
+    side.synchronize()
+    gms = replicas.max_over_ranks(g0.elapsed_time(g1), env, device=f"cuda:{local}")
+    graph = {"ms_per_step": gms / args.steps, "value": replicas.whole_job_rate(cells * args.steps, env, gms),
+             "path": "fhd_rk3_steps_stag (one captured step replayed per step)"}
+
     # e2e through the host-buffer C-ABI call (H2D + step + D2H, pinned memory)
     ctx.close()
     del st
@@ -374,7 +388,7 @@ def run_ours(args):
         "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
         "data": "synthetic (uniform argon at rest + in-kernel Philox noise; no dataset)",
         "config": dict(config_dict(args, p, dt, tname), autotune_ms_per_step=tune),
-        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "graph_replay": graph, "gpu_launches": launches,
         "clocks": clk, "status": status,
     }
     print(json.dumps(out), flush=True)

@@ -121,6 +121,7 @@ def _declare(lib):
         "fhd_override_sync": (i, [vp, fab]),
         "fhd_fill_random_normal": (i, [vp, fab, i, i, d, d, i, i, C.c_uint64]),
         "fhd_fill_random_uniform": (i, [vp, fab, i, i, i, i, C.c_uint64]),
+        "fhd_rk3_steps_stag": (i, [vp, fab, pfab, fab, pfab, d, C.c_int64, i]),
         "fhd_fill_step_noise": (i, [vp, P(FhdNoise), C.c_int64]),
         "fhd_rk3_step_stag": (i, [vp, fab, pfab, fab, pfab, fab, fab, fab, fab, fab, fab,
                                   pfab, pfab, pfab, P(FhdNoise), d, C.c_int64]),

@@ -154,6 +154,25 @@ class Context:
                                         *args, C.byref(nz) if nz is not None else None, dt, step)
         check(rc, "fhd_rk3_step_stag")
 
+    def rk3_steps(self, st: StagState, dt: float, step0: int, nsteps: int):
+        """nsteps RK3stepStag steps with in-kernel noise (steps step0 .. step0+nsteps-1),
+        replayed from a CUDA graph the context captures and keeps (fhd_rk3_steps_stag);
+        bitwise the same as nsteps rk3_step(..., aux=False) calls.  The legacy default
+        stream cannot be captured, so from it the steps run on a side stream ordered
+        after and before the caller's stream."""
+        cur = torch.cuda.current_stream(self.device)
+        if cur.cuda_stream != 0:
+            self._stream()
+            check(self.lib.fhd_rk3_steps_stag(self._h, st.cu.fab(), st.mom_fabs(), st.prim.fab(), st.vel_fabs(), dt,
+                                              step0, nsteps), "fhd_rk3_steps_stag")
+            return
+        if getattr(self, "_side", None) is None:
+            self._side = torch.cuda.Stream(self.device)
+        self._side.wait_stream(cur)
+        with torch.cuda.stream(self._side):
+            self.rk3_steps(st, dt, step0, nsteps)
+        cur.wait_stream(self._side)
+
     def stats_stag(self, st: StagState, stats, steps: int, flags: int = 15):
         """evaluateStatsStag3D's per-cell update (fhd_stats_stag) with sample count
         `steps` (1 for the first sample after a reset); flags = capi.STATS_*."""

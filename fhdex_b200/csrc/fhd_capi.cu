@@ -34,6 +34,12 @@ struct fhd_ctx {
     // device mirrors for the host-buffer step
     double* hbuf = nullptr;
     size_t hbuf_bytes = 0;
+    // graph replay of whole steps (fhd_rk3_steps_stag): the captured step, the device
+    // word its noise reads the step number from, and what the capture was made for
+    cudaGraph_t sgraph = nullptr;
+    cudaGraphExec_t sgexec = nullptr;
+    uint64_t* d_step = nullptr;
+    std::vector<uint64_t> skey;
     // CUDA-event timing per kernel kind
     bool prof = false;
     struct Ev { cudaEvent_t a, b; int kind; };
@@ -260,6 +266,9 @@ int fhd_destroy(fhd_ctx* c) {
     if (c->hbuf) cudaFree(c->hbuf);
     for (auto& e : c->evs) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
     if (c->d_status) cudaFree(c->d_status);
+    if (c->sgexec) cudaGraphExecDestroy(c->sgexec);
+    if (c->sgraph) cudaGraphDestroy(c->sgraph);
+    if (c->d_step) cudaFree(c->d_step);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
     return FHD_OK;
@@ -482,48 +491,23 @@ int fhd_fill_step_noise(fhd_ctx* c, const fhd_noise* nz, int64_t step) {
     return fill_ghosts(g, ng, c->prm.n_cells, c->stream);
 }
 
-int fhd_rk3_step_stag(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim, const fhd_fab vel[3], fhd_fab source,
-                      fhd_fab eta, fhd_fab zeta, fhd_fab kappa, fhd_fab chi, fhd_fab D, const fhd_fab* faceflux,
-                      const fhd_fab* edgeflux, const fhd_fab* cenflux, const fhd_noise* injected, double dt,
-                      int64_t step) {
-    if (!c || !mom || !vel || !(dt > 0)) return FHD_ERR_BAD_ARG;
-    const int ns = c->prm.nspecies, nvars = 5 + ns, nprim = 6 + 2 * ns;
+// The launches of one RK3 step (after validation and scratch set-up); step_ptr,
+// when set, is the device word the Philox noise reads its step from (graph replay).
+static int step_launches(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim, const fhd_fab vel[3], fhd_fab source,
+                  fhd_fab eta, fhd_fab zeta, fhd_fab kappa, fhd_fab chi, fhd_fab D, const fhd_fab* faceflux,
+                  const fhd_fab* edgeflux, const fhd_fab* cenflux, const fhd_noise* injected, double dt, int64_t step,
+                  bool aux_coef, bool aux_flux, const uint64_t* step_ptr) {
+    const int ns = c->prm.nspecies, nprim = 6 + 2 * ns;
     const bool mixed = c->prm.precision == FHD_PREC_MIXED;
-    if (!fab_ok(c, cu, CELLN, NGC, nvars, FHD_F64) || !fab_ok(c, prim, CELLN, NGC, nprim, FHD_F64)) return FHD_ERR_BAD_ARG;
-    for (int d = 0; d < 3; ++d)
-        if (!fab_ok(c, mom[d], FACEN[d], NGC, 1, FHD_F64) || !fab_ok(c, vel[d], FACEN[d], NGC, 1, FHD_F64))
-            return FHD_ERR_BAD_ARG;
-    if (source.data && !fab_ok(c, source, CELLN, 0, nvars, FHD_F64)) return FHD_ERR_BAD_ARG;
-    const bool aux_coef = eta.data != nullptr;
-    if (aux_coef) {
-        if (mixed) return FHD_ERR_UNSUPPORTED;
-        if (!fab_ok(c, eta, CELLN, 1, 1, FHD_F64) || !fab_ok(c, zeta, CELLN, 1, 1, FHD_F64) ||
-            !fab_ok(c, kappa, CELLN, 1, 1, FHD_F64) || !fab_ok(c, chi, CELLN, 1, ns, FHD_F64) ||
-            !fab_ok(c, D, CELLN, 1, ns * ns, FHD_F64))
-            return FHD_ERR_BAD_ARG;
-    }
-    const bool aux_flux = faceflux && edgeflux && cenflux && faceflux[0].data;
-    if (aux_flux) {
-        if (mixed || !aux_coef) return FHD_ERR_UNSUPPORTED;
-        for (int d = 0; d < 3; ++d)
-            if (!fab_ok(c, faceflux[d], FACEN[d], 0, nvars + 4, FHD_F64, 0) || !fab_ok(c, cenflux[d], CELLN, 1, 1, FHD_F64, 1))
-                return FHD_ERR_BAD_ARG;
-        for (int e = 0; e < 6; ++e)
-            if (!fab_ok(c, edgeflux[e], EFLUXN[e], 0, 1, FHD_F64, 0)) return FHD_ERR_BAD_ARG;
-    }
     const bool stoch = c->prm.stoch_stress_form == 1;
-    if (stoch && injected && !noise_ok(c, injected)) return FHD_ERR_BAD_ARG;
-    cudaSetDevice(c->device);
-    int rc = ensure_scratch(c);
-    if (rc) return rc;
-    rc = ensure_coef(c, mixed ? FHD_F32 : FHD_F64);
-    if (rc) return rc;
+    int rc = FHD_OK;
     const double w[3] = {(2.0 * std::sqrt(2.0) + 1.0 * std::sqrt(3.0)) / 5.0,
                          (-4.0 * std::sqrt(2.0) + 3.0 * std::sqrt(3.0)) / 5.0,
                          (1.0 * std::sqrt(2.0) - 2.0 * std::sqrt(3.0)) / 10.0};
     StageCall sc;
     std::memset(&sc, 0, sizeof(sc));
     sc.P = make_dev(c, dt, (uint64_t)step);
+    sc.P.step_ptr = step_ptr;
     sc.mode = !stoch ? NM_OFF : (injected ? NM_AB : NM_PHILOX);
     if (injected && stoch) set_noise(sc, injected, false);
     sc.pr = prim;
@@ -596,6 +580,125 @@ int fhd_rk3_step_stag(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim
     }
     ProfScope ps(c, 4);
     return fill_ghosts(g, ng, c->prm.n_cells, c->stream);
+}
+
+
+int fhd_rk3_step_stag(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim, const fhd_fab vel[3], fhd_fab source,
+                      fhd_fab eta, fhd_fab zeta, fhd_fab kappa, fhd_fab chi, fhd_fab D, const fhd_fab* faceflux,
+                      const fhd_fab* edgeflux, const fhd_fab* cenflux, const fhd_noise* injected, double dt,
+                      int64_t step) {
+    if (!c || !mom || !vel || !(dt > 0)) return FHD_ERR_BAD_ARG;
+    const int ns = c->prm.nspecies, nvars = 5 + ns, nprim = 6 + 2 * ns;
+    const bool mixed = c->prm.precision == FHD_PREC_MIXED;
+    if (!fab_ok(c, cu, CELLN, NGC, nvars, FHD_F64) || !fab_ok(c, prim, CELLN, NGC, nprim, FHD_F64)) return FHD_ERR_BAD_ARG;
+    for (int d = 0; d < 3; ++d)
+        if (!fab_ok(c, mom[d], FACEN[d], NGC, 1, FHD_F64) || !fab_ok(c, vel[d], FACEN[d], NGC, 1, FHD_F64))
+            return FHD_ERR_BAD_ARG;
+    if (source.data && !fab_ok(c, source, CELLN, 0, nvars, FHD_F64)) return FHD_ERR_BAD_ARG;
+    const bool aux_coef = eta.data != nullptr;
+    if (aux_coef) {
+        if (mixed) return FHD_ERR_UNSUPPORTED;
+        if (!fab_ok(c, eta, CELLN, 1, 1, FHD_F64) || !fab_ok(c, zeta, CELLN, 1, 1, FHD_F64) ||
+            !fab_ok(c, kappa, CELLN, 1, 1, FHD_F64) || !fab_ok(c, chi, CELLN, 1, ns, FHD_F64) ||
+            !fab_ok(c, D, CELLN, 1, ns * ns, FHD_F64))
+            return FHD_ERR_BAD_ARG;
+    }
+    const bool aux_flux = faceflux && edgeflux && cenflux && faceflux[0].data;
+    if (aux_flux) {
+        if (mixed || !aux_coef) return FHD_ERR_UNSUPPORTED;
+        for (int d = 0; d < 3; ++d)
+            if (!fab_ok(c, faceflux[d], FACEN[d], 0, nvars + 4, FHD_F64, 0) || !fab_ok(c, cenflux[d], CELLN, 1, 1, FHD_F64, 1))
+                return FHD_ERR_BAD_ARG;
+        for (int e = 0; e < 6; ++e)
+            if (!fab_ok(c, edgeflux[e], EFLUXN[e], 0, 1, FHD_F64, 0)) return FHD_ERR_BAD_ARG;
+    }
+    const bool stoch = c->prm.stoch_stress_form == 1;
+    if (stoch && injected && !noise_ok(c, injected)) return FHD_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    int rc = ensure_scratch(c);
+    if (rc) return rc;
+    rc = ensure_coef(c, mixed ? FHD_F32 : FHD_F64);
+    if (rc) return rc;
+    return step_launches(c, cu, mom, prim, vel, source, eta, zeta, kappa, chi, D, faceflux, edgeflux, cenflux, injected,
+                         dt, step, aux_coef, aux_flux, nullptr);
+}
+
+int fhd_rk3_steps_stag(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim, const fhd_fab vel[3], double dt,
+                       int64_t step0, int nsteps) {
+    if (!c || !mom || !vel || !(dt > 0) || nsteps < 0) return FHD_ERR_BAD_ARG;
+    const int ns = c->prm.nspecies, nvars = 5 + ns, nprim = 6 + 2 * ns;
+    const bool mixed = c->prm.precision == FHD_PREC_MIXED;
+    if (!fab_ok(c, cu, CELLN, NGC, nvars, FHD_F64) || !fab_ok(c, prim, CELLN, NGC, nprim, FHD_F64)) return FHD_ERR_BAD_ARG;
+    for (int d = 0; d < 3; ++d)
+        if (!fab_ok(c, mom[d], FACEN[d], NGC, 1, FHD_F64) || !fab_ok(c, vel[d], FACEN[d], NGC, 1, FHD_F64))
+            return FHD_ERR_BAD_ARG;
+    if (nsteps == 0) return FHD_OK;
+    cudaSetDevice(c->device);
+    int rc = ensure_scratch(c);
+    if (rc) return rc;
+    rc = ensure_coef(c, mixed ? FHD_F32 : FHD_F64);
+    if (rc) return rc;
+    if (!c->d_step && cudaMalloc(&c->d_step, sizeof(uint64_t)) != cudaSuccess) {
+        cudaGetLastError();
+        c->d_step = nullptr;
+        return FHD_ERR_OOM;
+    }
+    const fhd_fab none{};
+    // what the captured launches embed: every pointer, layout, dt and the tile
+    std::vector<uint64_t> key;
+    auto add_fab = [&](const fhd_fab& f) {
+        key.push_back((uint64_t)(uintptr_t)f.data);
+        for (int d = 0; d < 3; ++d) key.push_back(((uint64_t)(uint32_t)f.lo[d] << 32) | (uint32_t)f.hi[d]);
+    };
+    add_fab(cu);
+    add_fab(prim);
+    for (int d = 0; d < 3; ++d) { add_fab(mom[d]); add_fab(vel[d]); }
+    uint64_t dtb;
+    std::memcpy(&dtb, &dt, sizeof(dtb));
+    key.push_back(dtb);
+    key.push_back((uint64_t)c->tile);
+    key.push_back((uint64_t)(uintptr_t)c->scratch);
+    key.push_back((uint64_t)(uintptr_t)c->coef);
+    bool captured = c->sgexec && key == c->skey;
+    if (!captured) {
+        if (c->sgexec) cudaGraphExecDestroy(c->sgexec);
+        if (c->sgraph) cudaGraphDestroy(c->sgraph);
+        c->sgexec = nullptr;
+        c->sgraph = nullptr;
+        c->skey.clear();
+        if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            const bool prof = c->prof;
+            c->prof = false;  // no timing events inside the graph
+            rc = step_launches(c, cu, mom, prim, vel, none, none, none, none, none, none, nullptr, nullptr, nullptr,
+                               nullptr, dt, step0, false, false, c->d_step);
+            if (!rc) rc = steps_inc(c->d_step, 1, c->stream);
+            c->prof = prof;
+            cudaGraph_t g = nullptr;
+            const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+            if (!rc && e == cudaSuccess && cudaGraphInstantiate(&c->sgexec, g, 0) == cudaSuccess) {
+                c->sgraph = g;
+                c->skey = key;
+                captured = true;
+            } else {
+                if (g) cudaGraphDestroy(g);
+                c->sgexec = nullptr;
+                cudaGetLastError();
+                if (rc) return rc;
+            }
+        } else {
+            cudaGetLastError();  // e.g. the legacy default stream: launch step by step below
+        }
+    }
+    if (!captured) {
+        for (int s = 0; s < nsteps && !rc; ++s)
+            rc = step_launches(c, cu, mom, prim, vel, none, none, none, none, none, none, nullptr, nullptr, nullptr,
+                               nullptr, dt, step0 + s, false, false, nullptr);
+        return rc;
+    }
+    rc = steps_set(c->d_step, (uint64_t)step0, c->stream);
+    for (int s = 0; s < nsteps && !rc; ++s)
+        if (cudaGraphLaunch(c->sgexec, c->stream) != cudaSuccess) { cudaGetLastError(); rc = FHD_ERR_CUDA; }
+    return rc;
 }
 
 int fhd_stats_stag(fhd_ctx* c, fhd_fab cu, fhd_fab prim, const fhd_fab vel[3], const fhd_fab mom[3],

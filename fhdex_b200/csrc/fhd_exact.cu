@@ -139,6 +139,11 @@ int ghost_launch_b(const void* dfabs, const int* dbpref, int nfab, int nblocks, 
     return cuda_rc(cudaGetLastError());
 }
 
+int steps_set(uint64_t* step, uint64_t v, cudaStream_t s) {
+    k_steps_set<<<1, 1, 0, s>>>(step, v);
+    return cuda_rc(cudaGetLastError());
+}
+
 int steps_inc(uint64_t* steps, int n, cudaStream_t s) {
     if (n <= 0) return FHD_OK;
     k_steps_inc<<<(n + 255) / 256, 256, 0, s>>>(steps, n);

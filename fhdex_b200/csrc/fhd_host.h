@@ -154,6 +154,7 @@ int ghost_desc_size();
 int64_t ghost_pack(const fhd_fab& f, int c0, int nc, const int ncell[3], void* dst);  // returns work items
 int ghost_launch_b(const void* dfabs, const int* dbpref, int nfab, int nblocks, cudaStream_t s);
 int steps_inc(uint64_t* steps, int n, cudaStream_t s);
+int steps_set(uint64_t* step, uint64_t v, cudaStream_t s);
 
 int num_tiles();
 const char* tile_name(int t);

@@ -748,6 +748,8 @@ static __global__ void __launch_bounds__(256) k_ghosts_b(const GhostFab* __restr
     if (q < f.npts * f.nc) ghost_point(f, q);
 }
 
+static __global__ void k_steps_set(uint64_t* step, uint64_t v) { *step = v; }
+
 static __global__ void k_steps_inc(uint64_t* steps, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) steps[i] += 1;

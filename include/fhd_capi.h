@@ -212,6 +212,17 @@ int fhd_rk3_step_stag(fhd_ctx* ctx, fhd_fab cu, const fhd_fab mom[3], fhd_fab pr
                       const fhd_fab* edgeflux, const fhd_fab* cenflux,
                       const fhd_noise* injected, double dt, int64_t step);
 
+/* nsteps RK3stepStag steps (no source, no by-products; in-kernel Philox noise,
+ * or none when stoch_stress_form is 0) replayed from a CUDA graph: the first
+ * call captures one step and the context keeps it while the fabs, dt and tile
+ * stay the same.  For boxes small enough that a step's 23 launches cost more
+ * than their work.  Step s of the call draws the noise of step step0 + s, so the
+ * result is bitwise that of nsteps fhd_rk3_step_stag calls with steps step0,
+ * step0 + 1, ...  On a stream that cannot be captured (the legacy default
+ * stream) the steps are launched one by one. */
+int fhd_rk3_steps_stag(fhd_ctx* ctx, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim,
+                       const fhd_fab vel[3], double dt, int64_t step0, int nsteps);
+
 /* RK3stepStag on HOST fabs (same layouts as above, host pointers; pinned memory
  * gives full copy bandwidth): copies cu and mom to device buffers owned by the
  * context, advances one step there (in-kernel noise, or injected noise given as

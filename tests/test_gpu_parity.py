@@ -276,3 +276,32 @@ def test_host_buffer_step_equals_device_step(oracle):
     up = host.cu.arr.numel() * 8 + sum(m.arr.numel() * 8 for m in host.cumom)
     assert h2d == up
     assert d2h == sum(m.arr.numel() * 8 for m in host.state_mfs())
+
+
+@pytest.mark.parametrize("precision,stoch", [(0, 1), (1, 1), (0, 0)])
+def test_graph_replayed_steps_equal_single_steps(oracle, precision, stoch):
+    """fhd_rk3_steps_stag (one captured step replayed from a CUDA graph, the step
+    number read from a device counter) gives bitwise the state of the same steps
+    launched one by one, across a second call that continues the step count and
+    after a change of fabs that forces a new capture."""
+    p = argon((12, 10, 9), dx=8e-6, seed=4321, precision=precision)
+    p.stoch_stress_form = stoch
+    st = perturbed_state(oracle, p, seed=12)
+    a = gpu_copy(st)
+    b = gpu_copy(st)
+    ctx = Context(p)
+    dt = stable_dt(p)
+    for s in range(7):
+        ctx.rk3_step(a, dt, s, aux=False)
+    ctx.rk3_steps(b, dt, 0, 4)
+    ctx.rk3_steps(b, dt, 4, 3)
+    torch.cuda.synchronize()
+    bad, _ = compare_named(b.named(), a.named())
+    assert not bad, bad[:4]
+    c = gpu_copy(st)
+    ctx.rk3_steps(c, dt, 0, 7)   # other fabs: captured anew
+    torch.cuda.synchronize()
+    bad, _ = compare_named(c.named(), a.named())
+    assert not bad, bad[:4]
+    assert ctx.status() == 0
+    ctx.close()
