@@ -163,8 +163,7 @@ class _Solo:
 
     def launch(self, k):
         with torch.cuda.stream(self.stream):
-            for s in range(self.done_steps, self.done_steps + k):
-                self.ctx.rk3_step(self.st, self.dt, s, aux=False)
+            self.ctx.rk3_steps(self.st, self.dt, self.done_steps, k)
             self.event.record(self.stream)
         self.inflight = k
 
@@ -306,7 +305,8 @@ class Server:
 
 def run_alone(trace: list[Request], device: int = 0, fp64: bool = True):
     """Baseline: the same trace served one request at a time (FIFO) with the plain
-    single-run step (FP64 unless fp64=False)."""
+    single-run step (FP64 unless fp64=False), its steps replayed from the
+    context's CUDA graph (fhd_rk3_steps_stag), the fastest single-run path."""
     reqs = sorted(trace, key=lambda r: r.arrival)
     t0 = time.perf_counter()
     cell_updates = 0
@@ -323,8 +323,7 @@ def run_alone(trace: list[Request], device: int = 0, fp64: bool = True):
         st = StagState(p, f"cuda:{device}", aux=False)
         ctx.init_state(st)
         dt = stable_dt(p)
-        for s in range(r.steps):
-            ctx.rk3_step(st, dt, s, aux=False)
+        ctx.rk3_steps(st, dt, 0, r.steps)
         torch.cuda.synchronize(device)
         r.status = ctx.status()
         r.finish = time.perf_counter() - t0
