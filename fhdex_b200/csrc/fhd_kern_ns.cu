@@ -103,7 +103,7 @@ int FHD_CAT(exact_convert_ns, FHD_NS)(const DevParams& P, fhd_fab prim, const fh
     }
     a.status = status;
     const int64_t tot = (int64_t)P.n[0] * P.n[1] * P.n[2];
-    k_convert<FHD_NS><<<grid_for(tot, 128), 128, 0, s>>>(a);
+    k_convert<FHD_NS><<<resident_grid<k_convert<FHD_NS>>(tot, 128), 128, 0, s>>>(a);
     return cuda_rc(cudaGetLastError());
 }
 #endif

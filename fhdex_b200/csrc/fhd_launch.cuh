@@ -19,6 +19,48 @@ inline Arr4<T> view(const fhd_fab& f, int comp0 = 0) {
     return a;
 }
 
+// Grid of a grid-stride kernel: as many blocks as the SMs hold at once (the kernel's
+// occupancy at this block size, queried once per kernel and block size), so that
+// every block runs from the start and all finish together instead of leaving a
+// partly filled last wave; fewer when there is less work.
+inline int device_sms() {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) {
+            cudaGetLastError();
+            sms = 148;
+        }
+    }
+    return sms;
+}
+
+template <auto K>
+inline int resident_blocks(int block) {
+    static int cache[3] = {0, 0, 0};  // block sizes 128, 256, other
+    const int slot = block == 128 ? 0 : (block == 256 ? 1 : 2);
+    if (slot == 2 || !cache[slot]) {
+        int nb = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, K, block, 0) != cudaSuccess || nb < 1) {
+            cudaGetLastError();
+            nb = 1;
+        }
+        if (slot == 2) return nb * device_sms();
+        cache[slot] = nb * device_sms();
+    }
+    return cache[slot];
+}
+
+template <auto K>
+inline int resident_grid(int64_t items, int block) {
+    int64_t g = (items + block - 1) / block;
+    const int cap = resident_blocks<K>(block);
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
 inline int grid_for(int64_t items, int block, int cap = 148 * 32) {
     int64_t g = (items + block - 1) / block;
     if (g > cap) g = cap;
@@ -80,6 +122,8 @@ int launch_cellprep(const StageCall& c) {
     a.D = view<R>(c.D);
     a.status = c.status;
     const int64_t tot = (int64_t)(c.P.n[0] + 3) * (c.P.n[1] + 3) * (c.P.n[2] + 3);
+    // (an occupancy-sized grid was measured slower here: blocks beyond the resident
+    // set rebalance this kernel's uneven per-cell cost)
     k_cellprep<NS, R><<<grid_for(tot, 128), 128, 0, c.stream>>>(a);
     return cuda_rc(cudaGetLastError());
 }
@@ -127,9 +171,12 @@ int launch_stage_part_t(const StageCall& c, int part) {
     } else if (part == 1) {
         const int t = (c.tile >= 0 && c.tile < kNumStageBlocks) ? c.tile : 0;
 #define FHD_FACES(BS, MINB)                                                                                      \
-        k_faces<NS, R, NZ, 0, BS, MINB><<<grid_for((int64_t)(N[0] + 1) * N[1] * N[2], BS), BS, 0, c.stream>>>(a); \
-        k_faces<NS, R, NZ, 1, BS, MINB><<<grid_for((int64_t)N[0] * (N[1] + 1) * N[2], BS), BS, 0, c.stream>>>(a); \
-        k_faces<NS, R, NZ, 2, BS, MINB><<<grid_for((int64_t)N[0] * N[1] * (N[2] + 1), BS), BS, 0, c.stream>>>(a);
+        k_faces<NS, R, NZ, 0, BS, MINB><<<resident_grid<k_faces<NS, R, NZ, 0, BS, MINB>>(                     \
+            (int64_t)(N[0] + 1) * N[1] * N[2], BS), BS, 0, c.stream>>>(a);                                     \
+        k_faces<NS, R, NZ, 1, BS, MINB><<<resident_grid<k_faces<NS, R, NZ, 1, BS, MINB>>(                     \
+            (int64_t)N[0] * (N[1] + 1) * N[2], BS), BS, 0, c.stream>>>(a);                                     \
+        k_faces<NS, R, NZ, 2, BS, MINB><<<resident_grid<k_faces<NS, R, NZ, 2, BS, MINB>>(                     \
+            (int64_t)N[0] * N[1] * (N[2] + 1), BS), BS, 0, c.stream>>>(a);
         switch (t) {
             case 0: FHD_FACES(128, 4) break;
             case 1: FHD_FACES(256, 2) break;
@@ -141,7 +188,8 @@ int launch_stage_part_t(const StageCall& c, int part) {
     } else {
         // 128 threads whatever the tile: the update kernel is capped at 32 registers
         // for full occupancy (16 blocks of 128 per SM)
-        k_update<NS, R, NZ><<<grid_for((int64_t)(N[0] + 1) * (N[1] + 1) * (N[2] + 1), 128), 128, 0, c.stream>>>(a);
+        k_update<NS, R, NZ><<<resident_grid<k_update<NS, R, NZ>>((int64_t)(N[0] + 1) * (N[1] + 1) * (N[2] + 1), 128),
+                               128, 0, c.stream>>>(a);
     }
     return cuda_rc(cudaGetLastError());
 }
