@@ -9,6 +9,7 @@ import ctypes as C
 import os
 
 MAX_SPECIES = 8
+MAX_REACTIONS = 8
 
 FHD_OK = 0
 FHD_ERR_BAD_ARG = 1
@@ -64,6 +65,15 @@ class FhdParams(C.Structure):
         ("stoch_stress_form", C.c_int),
         ("precision", C.c_int),
         ("seed", C.c_uint64),
+        ("nreaction", C.c_int),
+        ("reaction_type", C.c_int),
+        ("stoich_R", (C.c_int * MAX_SPECIES) * MAX_REACTIONS),
+        ("stoich_P", (C.c_int * MAX_SPECIES) * MAX_REACTIONS),
+        ("rate_const", C.c_double * MAX_REACTIONS),
+        ("alpha_param", C.c_double * MAX_REACTIONS),
+        ("beta_param", C.c_double * MAX_REACTIONS),
+        ("T0_chem", C.c_double),
+        ("avogadro", C.c_double),
     ]
 
 
@@ -72,6 +82,7 @@ class FhdNoise(C.Structure):
         ("face", (FhdFab * 3) * 2),
         ("edge", (FhdFab * 3) * 2),
         ("cen", (FhdFab * 3) * 2),
+        ("chem", FhdFab * 2),
     ]
 
 
@@ -123,6 +134,7 @@ def _declare(lib):
         "fhd_fill_random_uniform": (i, [vp, fab, i, i, i, i, C.c_uint64]),
         "fhd_rk3_steps_stag": (i, [vp, fab, pfab, fab, pfab, d, C.c_int64, i]),
         "fhd_fill_step_noise": (i, [vp, P(FhdNoise), C.c_int64]),
+        "fhd_chemistry_source_cle": (i, [vp, d, d, fab, fab, fab]),
         "fhd_rk3_step_stag": (i, [vp, fab, pfab, fab, pfab, fab, fab, fab, fab, fab, fab,
                                   pfab, pfab, pfab, P(FhdNoise), d, C.c_int64]),
         "fhd_rk3_step_stag_host": (i, [vp, fab, pfab, fab, pfab, P(FhdNoise), d, C.c_int64,

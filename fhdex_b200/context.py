@@ -132,6 +132,18 @@ class Context:
         check(self.lib.fhd_fill_random_uniform(self._h, mf.fab(), scomp, ncomp, int(overridesync),
                                                int(fillboundary), stream_id), "fhd_fill_random_uniform")
 
+    def chemistry_source_cle(self, prim, source, ranchem, dt: float, dV: float | None = None):
+        """compute_compressible_chemistry_source_CLE (chemistry_functions.cpp:128-193):
+        species comps 5.. of ``source`` from ``prim`` and the reaction noises
+        ``ranchem`` (None for reaction_type 0); dV defaults to the cell volume."""
+        self._stream()
+        if dV is None:
+            dx = self.p.dx
+            dV = dx[0] * dx[1] * dx[2]
+        rf = ranchem.fab() if ranchem is not None else capi.FhdFab()
+        check(self.lib.fhd_chemistry_source_cle(self._h, dt, dV, prim.fab(), source.fab(), rf),
+              "fhd_chemistry_source_cle")
+
     def fill_step_noise(self, noise: StepNoise, step: int):
         self._stream()
         self._noise_struct = noise.c_struct()

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "fhd_host.h"
+#include "fhd_chem.cuh"
 #include "philox.cuh"
 
 using namespace fhd;
@@ -30,6 +31,7 @@ struct fhd_ctx {
     fhd_fab ct{}, et{};          // stage stresses (coefficient precision)
     fhd_fab sff[3]{};            // stage conservative face fluxes (f64)
     fhd_fab smc{}, sme{};        // stage total centre / edge momentum fluxes (f64)
+    fhd_fab csrc{};              // zeroed source of a step given none (chemistry on)
     int tile = 0;
     // device mirrors for the host-buffer step
     double* hbuf = nullptr;
@@ -103,8 +105,10 @@ int ensure_scratch(fhd_ctx* c) {
     const int allnod[3] = {1, 1, 1};
     const int64_t npts = fab_points(make_fab(nullptr, n, allnod, 0, 1, FHD_F64));  // [0, n]^3
     const int64_t c1pts = fab_points(make_fab(nullptr, n, CELLN, 1, 1, FHD_F64));  // cells grown by 1
+    const int64_t vpts = (int64_t)n[0] * n[1] * n[2];
+    const int64_t srcpts = c->prm.nreaction > 0 ? vpts * nvars : 0;  // chemistry's source when the caller has none
     const size_t need = (size_t)(2 * cellpts * nvars + 2 * (fpts[0] + fpts[1] + fpts[2]) + 3 * npts * (2 + ns) +
-                                 3 * c1pts + 6 * npts) * sizeof(double);
+                                 3 * c1pts + 6 * npts + srcpts) * sizeof(double);
     if (c->scratch && c->scratch_bytes >= need) return FHD_OK;
     if (c->scratch) cudaFree(c->scratch);
     c->scratch = nullptr;
@@ -123,7 +127,8 @@ int ensure_scratch(fhd_ctx* c) {
         p += npts * (2 + ns);
     }
     c->smc = make_fab(p, n, CELLN, 1, 3, FHD_F64); p += c1pts * 3;
-    c->sme = make_fab(p, n, allnod, 0, 6, FHD_F64);
+    c->sme = make_fab(p, n, allnod, 0, 6, FHD_F64); p += npts * 6;
+    c->csrc = srcpts ? make_fab(p, n, CELLN, 0, nvars, FHD_F64) : fhd_fab{};
     return FHD_OK;
 }
 
@@ -181,6 +186,15 @@ int sync_rc(cudaError_t e) {
     return FHD_ERR_CUDA;
 }
 
+// the reaction noises of an injected step: required when the step's chemistry
+// draws them (nreaction > 0 and reaction_type 1)
+bool chem_noise_needed(const fhd_ctx* c) { return c->prm.nreaction > 0 && c->prm.reaction_type == 1; }
+bool chem_noise_ok(const fhd_ctx* c, const fhd_noise* nz) {
+    for (int s = 0; s < 2; ++s)
+        if (!fab_ok(c, nz->chem[s], CELLN, 0, c->prm.nreaction, FHD_F64)) return false;
+    return true;
+}
+
 bool noise_ok(const fhd_ctx* c, const fhd_noise* nz) {
     const int ns = c->prm.nspecies;
     for (int s = 0; s < 2; ++s)
@@ -235,6 +249,16 @@ int fhd_create(fhd_ctx** out, const fhd_params* params, int device) {
     if (p.advection_type < -1 || p.advection_type > 2) return FHD_ERR_UNSUPPORTED;
     if (p.precision != FHD_PREC_FP64 && p.precision != FHD_PREC_MIXED) return FHD_ERR_BAD_ARG;
     if ((p.visc_type == 3 || p.visc_type == -3) && p.zeta_ratio < 0) return FHD_ERR_BAD_ARG;
+    // chemistry (chemistry_functions.cpp:50-52, 131-135)
+    if (p.nreaction < 0 || p.nreaction > FHD_MAX_REACTIONS) return FHD_ERR_BAD_ARG;
+    if (p.nreaction > 0) {
+        if (p.reaction_type != 0 && p.reaction_type != 1) return FHD_ERR_UNSUPPORTED;
+        if (!(p.T0_chem > 0)) return FHD_ERR_BAD_ARG;
+        for (int m = 0; m < p.nreaction; ++m)
+            for (int n = 0; n < p.nspecies; ++n)
+                if (p.stoich_R[m][n] < 0 || p.stoich_R[m][n] > 16 || p.stoich_P[m][n] < 0 || p.stoich_P[m][n] > 16)
+                    return FHD_ERR_BAD_ARG;
+    }
     fhd_ctx* c = new (std::nothrow) fhd_ctx;
     if (!c) return FHD_ERR_OOM;
     c->prm = p;
@@ -471,12 +495,36 @@ int fhd_fill_random_uniform(fhd_ctx* c, fhd_fab mf, int scomp, int ncomp, int ov
     return rc;
 }
 
+int fhd_chemistry_source_cle(fhd_ctx* c, double dt, double dV, fhd_fab prim, fhd_fab source, fhd_fab ranchem) {
+    if (!c || c->prm.nreaction < 1 || !(dt > 0) || !(dV > 0)) return FHD_ERR_BAD_ARG;
+    const int ns = c->prm.nspecies, nprim = 6 + 2 * ns;
+    if (!fab_ok(c, prim, CELLN, 0, nprim, FHD_F64) || !fab_ok(c, source, CELLN, 0, 5 + ns, FHD_F64)) return FHD_ERR_BAD_ARG;
+    const bool cle = c->prm.reaction_type == 1;
+    if (cle && !fab_ok(c, ranchem, CELLN, 0, c->prm.nreaction, FHD_F64)) return FHD_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    const DevParams P = make_dev(c, dt, 0);
+    const ChemParams cp = chem_params(c->prm, dt, dV);
+    return chem_launch(P, cp, prim, source, cle ? &ranchem : nullptr, nullptr, cle ? CN_W : CN_OFF, 0.0, c->stream);
+}
+
 int fhd_fill_step_noise(fhd_ctx* c, const fhd_noise* nz, int64_t step) {
     if (!c || !nz) return FHD_ERR_BAD_ARG;
-    if (!noise_ok(c, nz)) return FHD_ERR_BAD_ARG;
+    // the stress fields (when face[0][0] is given) and the reaction fields (when
+    // chem[0] is given and the context has reactions); at least one of the two
+    const bool stress = nz->face[0][0].data != nullptr;
+    const bool chem = nz->chem[0].data != nullptr;
+    if (!stress && !chem) return FHD_ERR_BAD_ARG;
+    if (stress && !noise_ok(c, nz)) return FHD_ERR_BAD_ARG;
+    if (chem && (c->prm.nreaction < 1 || !chem_noise_ok(c, nz))) return FHD_ERR_BAD_ARG;
     cudaSetDevice(c->device);
     const int ns = c->prm.nspecies;
     DevParams P = make_dev(c, 1.0, (uint64_t)step);
+    if (chem)
+        for (int s = 0; s < 2; ++s) {
+            const int rc = noise_fill(P, nz->chem[s], 0, c->prm.nreaction, 0.0, 1.0, fid_chem(0), s, c->stream);
+            if (rc) return rc;
+        }
+    if (!stress) return FHD_OK;
     GhostReq g[6];
     int ng = 0;
     for (int s = 0; s < 2; ++s)
@@ -517,6 +565,16 @@ static int step_launches(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab p
     if (aux_coef && !mixed) { sc.eta = eta; sc.zeta = zeta; sc.kappa = kappa; sc.chi = chi; sc.D = D; }
     else { sc.eta = c->ceta; sc.zeta = c->czeta; sc.kappa = c->ckappa; sc.chi = c->cchi; sc.D = c->cD; }
     sc.src = source;
+    // chemistry source (timeStepStag.cpp:354-361): written into the caller's source,
+    // or into the context's zeroed one, after each stage's conversion
+    const bool chem = c->prm.nreaction > 0;
+    ChemParams cp;
+    int cmode = CN_OFF;
+    if (chem) {
+        if (!sc.src.data) sc.src = c->csrc;
+        cp = chem_params(c->prm, dt, sc.P.dx[0] * sc.P.dx[1] * sc.P.dx[2]);
+        if (c->prm.reaction_type == 1) cmode = injected ? CN_AB : CN_PHILOX;
+    }
     sc.status = c->d_status;
     sc.stream = c->stream;
     sc.tile = c->tile;
@@ -538,6 +596,9 @@ static int step_launches(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab p
         {
             ProfScope ps(c, 0);
             rc = mixed ? mixed_cellprep(sc) : exact_cellprep(sc);
+            if (!rc && chem)
+                rc = chem_launch(sc.P, cp, prim, sc.src, cmode == CN_AB ? &injected->chem[0] : nullptr,
+                                 cmode == CN_AB ? &injected->chem[1] : nullptr, cmode, w[s], c->stream);
         }
         if (rc) return rc;
         if (s == 2 && aux_flux) {
@@ -614,6 +675,8 @@ int fhd_rk3_step_stag(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim
     }
     const bool stoch = c->prm.stoch_stress_form == 1;
     if (stoch && injected && !noise_ok(c, injected)) return FHD_ERR_BAD_ARG;
+    if (injected && chem_noise_needed(c) && !chem_noise_ok(c, injected)) return FHD_ERR_BAD_ARG;
+    if (source.data && c->prm.nreaction > 0 && !fab_ok(c, source, CELLN, 0, nvars, FHD_F64)) return FHD_ERR_BAD_ARG;
     cudaSetDevice(c->device);
     int rc = ensure_scratch(c);
     if (rc) return rc;
@@ -766,7 +829,10 @@ int fhd_rk3_step_stag_host(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab
     const fhd_fab* hf[8] = {&cu, &mom[0], &mom[1], &mom[2], &prim, &vel[0], &vel[1], &vel[2]};
     size_t bytes[8], total = 0;
     for (int q = 0; q < 8; ++q) { bytes[q] = (size_t)fab_points(*hf[q]) * hf[q]->ncomp * sizeof(double); total += bytes[q]; }
+    // injected reaction noises are not mirrored here (in-kernel reaction noise is)
+    if (injected && chem_noise_needed(c)) return FHD_ERR_UNSUPPORTED;
     fhd_noise dn;
+    std::memset(&dn, 0, sizeof(dn));
     size_t nzb = 0;
     const bool inj = injected && c->prm.stoch_stress_form == 1;
     if (inj) {

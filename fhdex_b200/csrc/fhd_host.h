@@ -133,6 +133,11 @@ struct GhostReq {
     int c0, nc;
 };
 int fill_ghosts(const GhostReq* reqs, int n, const int ncell[3], cudaStream_t s);
+// chemistry source (fhd_chem.cu): writes species comps 5.. of `source` at the valid
+// cells from `prim`; na/nb: the A/B (mode CN_AB) or W (CN_W) noise fabs
+struct ChemParams;
+int chem_launch(const DevParams& P, const ChemParams& C, const fhd_fab& prim, const fhd_fab& source,
+                const fhd_fab* na, const fhd_fab* nb, int mode, double w, cudaStream_t s);
 // running statistics (fhd_stats.cu, exact TU)
 int exact_stats(const DevParams& P, const fhd_fab& cu, const fhd_fab& prim, const fhd_fab mom[3],
                 const fhd_stats& st, int64_t steps, int flags, cudaStream_t s);

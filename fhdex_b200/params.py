@@ -12,7 +12,7 @@ import dataclasses
 import math
 from dataclasses import dataclass, field
 
-from .capi import MAX_SPECIES, FhdParams
+from .capi import MAX_REACTIONS, MAX_SPECIES, FhdParams
 
 K_B = 1.38064852e-16
 RUNIV = 8.314462175e7
@@ -41,6 +41,17 @@ class Params:
     stoch_stress_form: int = 1
     precision: int = 0
     seed: int = 1
+    # chemistry (chemistry_functions.cpp:45-124): stoich_R/stoich_P one tuple of
+    # nspecies coefficients per reaction; avogadro <= 0 means Runiv / k_B
+    nreaction: int = 0
+    reaction_type: int = 0
+    stoich_R: tuple = ()
+    stoich_P: tuple = ()
+    rate_const: tuple = ()
+    alpha_param: tuple = ()
+    beta_param: tuple = ()
+    T0_chem: float = 0.0
+    avogadro: float = 0.0
     # initial state (prob_type 1): not part of fhd_params
     rho0: float = 1.78e-3
     T_init: float = 273.0
@@ -95,6 +106,17 @@ class Params:
         p.stoch_stress_form = self.stoch_stress_form
         p.precision = self.precision
         p.seed = self.seed & 0xFFFFFFFFFFFFFFFF
+        p.nreaction = self.nreaction
+        p.reaction_type = self.reaction_type
+        for m in range(min(self.nreaction, MAX_REACTIONS)):
+            for n in range(self.nspecies):
+                p.stoich_R[m][n] = int(self.stoich_R[m][n])
+                p.stoich_P[m][n] = int(self.stoich_P[m][n])
+            p.rate_const[m] = self.rate_const[m]
+            p.alpha_param[m] = self.alpha_param[m] if m < len(self.alpha_param) else 0.0
+            p.beta_param[m] = self.beta_param[m] if m < len(self.beta_param) else 0.0
+        p.T0_chem = self.T0_chem
+        p.avogadro = self.avogadro
         return p
 
     # -- thermodynamics on the host (for dt and theory) -------------------------------
@@ -139,6 +161,32 @@ def mixture4(n=32, dx=1e-6, **kw) -> Params:
                   diameter=(3.66e-8, 2.58e-8, 4.16e-8, 2.18e-8), dof=(3.0,) * 4,
                   e0=(0.0,) * 4, hcv=(-1.0,) * 4, hcp=(-1.0,) * 4, rhobar=(0.25,) * 4)
     return base.replace(**kw)
+
+
+def no2_dimerization(n=16, dx=1e-5, **kw) -> Params:
+    """2 NO2 <-> N2O4 with the reference's compressible chemistry: two species
+    (NO2, N2O4), reaction 1 = 2 NO2 -> N2O4, reaction 2 = N2O4 -> 2 NO2, Arrhenius
+    factors about T0 = 350 K, chemical Langevin noise (reaction_type 1); gas
+    constants and composition of exec/compressible_stag/test_NO2_dimerization_eq
+    (inputs_NO2_dimerization_eq), whose initial state is at chemical equilibrium."""
+    n3 = (n, n, n) if isinstance(n, int) else tuple(n)
+    base = Params(nspecies=2, n_cells=n3, prob_hi=tuple(dx * n3[d] for d in range(3)),
+                  molmass=(46.0055, 92.0110), diameter=(3.765e-08, 4.621e-08), dof=(7.279586, 18.049072),
+                  e0=(0.0, 0.0), hcv=(-1.0, -1.0), hcp=(-1.0, -1.0), k_B=1.38065e-16, Runiv=8.31446e7,
+                  rho0=1.858338e-03, T_init=350.0, rhobar=(0.723969, 0.276031),
+                  nreaction=2, reaction_type=1, stoich_R=((2, 0), (0, 1)), stoich_P=((0, 1), (2, 0)),
+                  rate_const=(4.065753e+11, 6.236899e+07), alpha_param=(-5.337990e+10, 5.370000e+11),
+                  beta_param=(0.644950, -1.100000), T0_chem=350.0)
+    return base.replace(**kw)
+
+
+def isomerization(p: Params) -> Params:
+    """First-order A <-> B on the species of ``p`` (stoichiometric coefficients 0/1,
+    no activation energy, no temperature power): the case in which every power and
+    exponential of the chemistry source is exact."""
+    return p.replace(nreaction=2, reaction_type=1, stoich_R=((1, 0), (0, 1)), stoich_P=((0, 1), (1, 0)),
+                     rate_const=(2.0e5, 3.0e5), alpha_param=(0.0, 0.0), beta_param=(0.0, 0.0),
+                     T0_chem=p.T_init)
 
 
 def hard_sphere_single_gas(p: Params, T=None):
@@ -207,6 +255,23 @@ def parse_inputs(text: str, base: Params | None = None) -> Params:
                 "stoch_stress_form", "seed"):
         if key in kv:
             upd[key] = int(kv[key][0])
+    # chemistry keys (chemistry_functions.cpp:45-124); avogadro overrides Runiv
+    # (common_functions.cpp:775-777)
+    nr = int(kv["nreaction"][0]) if "nreaction" in kv else 0
+    if nr > 0:
+        upd["nreaction"] = nr
+        upd["reaction_type"] = int(kv["reaction_type"][0])
+        upd["stoich_R"] = tuple(tuple(int(x) for x in kv[f"stoich_{m + 1}R"][:ns]) for m in range(nr))
+        upd["stoich_P"] = tuple(tuple(int(x) for x in kv[f"stoich_{m + 1}P"][:ns]) for m in range(nr))
+        upd["rate_const"] = tuple(float(x) for x in kv["rate_const"][:nr])
+        for key in ("alpha_param", "beta_param"):
+            vals = [float(x) for x in kv.get(key, [])[:nr]]
+            upd[key] = tuple(vals + [0.0] * (nr - len(vals)))
+        if "T0_chem" in kv:
+            upd["T0_chem"] = float(kv["T0_chem"][0])
+    if "avogadro" in kv:
+        upd["avogadro"] = float(kv["avogadro"][0])
+        upd["Runiv"] = upd.get("k_B", p.k_B) * upd["avogadro"]
     for key in ("bc_vel_lo", "bc_vel_hi", "bc_mass_lo", "bc_mass_hi", "bc_therm_lo", "bc_therm_hi"):
         if key in kv and any(int(x) != -1 for x in kv[key]):
             raise ValueError(f"{key}: only fully periodic boundaries are implemented")

@@ -105,11 +105,15 @@ class StepNoise:
         self.face = [[MultiFab(N, FACE[d], ns + 1, 0, **kw) for d in range(3)] for _ in range(2)]
         self.edge = [[MultiFab(N, EDGE[e], 1, 0, **kw) for e in range(3)] for _ in range(2)]
         self.cen = [[MultiFab(N, CELL, 1, 1, **kw) for d in range(3)] for _ in range(2)]
+        # ranchem_A / ranchem_B (nreaction comps) when the run has reactions
+        nr = getattr(p, "nreaction", 0)
+        self.chem = [MultiFab(N, CELL, nr, 0, **kw) if nr > 0 else None for _ in range(2)]
 
     def mfs(self):
         out = []
         for s in range(2):
             out += self.face[s] + self.edge[s] + self.cen[s]
+        out += [c for c in self.chem if c is not None]
         return out
 
     def c_struct(self) -> FhdNoise:
@@ -119,6 +123,8 @@ class StepNoise:
                 n.face[s][d] = self.face[s][d].fab()
                 n.edge[s][d] = self.edge[s][d].fab()
                 n.cen[s][d] = self.cen[s][d].fab()
+            if self.chem[s] is not None:
+                n.chem[s] = self.chem[s].fab()
         return n
 
     def to(self, device):

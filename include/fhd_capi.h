@@ -36,6 +36,7 @@ extern "C" {
 #endif
 
 #define FHD_MAX_SPECIES 8
+#define FHD_MAX_REACTIONS 8
 
 /* return / status codes */
 enum {
@@ -96,6 +97,19 @@ typedef struct {
     int stoch_stress_form;  /* 0 (no noise) or 1                                       */
     int precision;          /* FHD_PREC_*                                               */
     uint64_t seed;          /* key of the in-kernel Philox noise                        */
+    /* Chemistry source of the compressible step
+     * (compute_compressible_chemistry_source_CLE, chemistry_functions.cpp:128-193;
+     * deck keys chemistry_functions.cpp:45-124, stoich_<m>R / stoich_<m>P per
+     * reaction).  nreaction = 0: no chemistry. */
+    int nreaction;          /* 0 .. FHD_MAX_REACTIONS                                   */
+    int reaction_type;      /* 0 deterministic, 1 chemical Langevin (CLE)               */
+    int stoich_R[FHD_MAX_REACTIONS][FHD_MAX_SPECIES];  /* reactant coefficients >= 0   */
+    int stoich_P[FHD_MAX_REACTIONS][FHD_MAX_SPECIES];  /* product coefficients >= 0    */
+    double rate_const[FHD_MAX_REACTIONS];
+    double alpha_param[FHD_MAX_REACTIONS];  /* activation: exp(-alpha/Runiv (1/T - 1/T0)) */
+    double beta_param[FHD_MAX_REACTIONS];   /* (T/T0)^beta                                 */
+    double T0_chem;         /* > 0 when nreaction > 0                                   */
+    double avogadro;        /* <= 0: Runiv / k_B (common_functions.cpp:775)             */
 } fhd_params;
 
 /* Injected Gaussian noise for one RK3 step: the "A" and "B" white-noise fields
@@ -108,11 +122,15 @@ typedef struct {
  * stochedge_y[1]; the other three edge fields it fills are never read,
  * fluxStag.cpp:130-132).  cen[.][d]: cell-centred with 1 ghost, variance 2 in
  * 3D.  Values must already be OverrideSync'ed/FillBoundary'ed, as
- * MultiFabFillRandomNormal leaves them. */
+ * MultiFabFillRandomNormal leaves them.  chem[.]: the reaction noises
+ * ranchem_A / ranchem_B (timeStepStag.cpp:148-152, 225-229), cell-centred,
+ * nreaction components, 0 ghosts, variance 1; read only when nreaction > 0 and
+ * reaction_type is 1 (data == NULL otherwise). */
 typedef struct {
     fhd_fab face[2][3];
     fhd_fab edge[2][3];
     fhd_fab cen[2][3];
+    fhd_fab chem[2];
 } fhd_noise;
 
 typedef struct fhd_ctx fhd_ctx;
@@ -190,9 +208,21 @@ int fhd_fill_random_normal(fhd_ctx* ctx, fhd_fab mf, int scomp, int ncomp, doubl
 int fhd_fill_random_uniform(fhd_ctx* ctx, fhd_fab mf, int scomp, int ncomp, int overridesync,
                             int fillboundary, uint64_t stream_id);
 
+/* compute_compressible_chemistry_source_CLE: chemistry_functions.cpp:128-193
+ * (declared chemistry_functions.H:20-21).  For every valid cell of `prim`
+ * (nprimvars comps, >= 0 ghosts) writes components 5 .. 5+nspecies-1 of
+ * `source` (>= 5+nspecies comps, >= 0 ghosts) with the law-of-mass-action
+ * rates of the context's reactions and, for reaction_type 1, their Langevin
+ * terms driven by `ranchem` (cell-centred, nreaction comps; data == NULL is
+ * accepted for reaction_type 0).  dV = dx*dy*dz as the reference's caller
+ * passes it (timeStepStag.cpp:360).  FHD_ERR_BAD_ARG when the context has no
+ * reactions. */
+int fhd_chemistry_source_cle(fhd_ctx* ctx, double dt, double dV, fhd_fab prim, fhd_fab source,
+                             fhd_fab ranchem);
+
 /* Fills `noise` with exactly the A/B fields the fused step generates
  * in-kernel for (seed, step): lets a caller replay an in-kernel-noise step
- * through the injected-noise path. */
+ * through the injected-noise path (chem[.] too when their data is non-NULL). */
 int fhd_fill_step_noise(fhd_ctx* ctx, const fhd_noise* noise, int64_t step);
 
 /* RK3stepStag: timeStepStag.cpp:13-1245 (declared
@@ -200,8 +230,11 @@ int fhd_fill_step_noise(fhd_ctx* ctx, const fhd_noise* noise, int64_t step);
  * SSP-RK3 step in place (ghosts refreshed, as after the reference's final
  * FillBoundary).  prim and vel are recomputed from cu and mom at the start of
  * every stage (the reference reads them as given, which in its driver are
- * always the conversion of cu and mom), so their contents on entry are not read.  source: nprimvars-component cell fab (the reference's
- * `source`, all zeros unless chemistry is on) or data == NULL for zero.
+ * always the conversion of cu and mom), so their contents on entry are not read.  source: nvars-component cell fab (the reference's
+ * `source`) or data == NULL for zero.  With nreaction > 0, every stage
+ * overwrites components 5 .. 5+nspecies-1 of `source` (of a zeroed scratch
+ * source when data == NULL) with the chemistry source of the stage's state
+ * before the update adds dt * source, as timeStepStag.cpp:354-361 does.
  * eta..D receive the stage-3 transport coefficients and faceflux/edgeflux/
  * cenflux the stage-3 fluxes when their data pointers are non-NULL (pass NULL
  * arrays to skip them; the fused path then never materialises them).

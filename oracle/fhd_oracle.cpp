@@ -14,7 +14,8 @@
 // Scope: periodic boundaries (every physical-BC routine on the path is then a
 // no-op: boundaryStag.cpp:5-14, 1555-1557), 3D, algorithm_type 2,
 // transport_type 1 (Giovangigli), stoch_stress_form 0/1, advection_type 0/1/2,
-// visc_type 1/2/3, no chemistry/reservoir/membrane/turbulence forcing.
+// visc_type 1/2/3, the compressible chemistry source (reaction_type 0/1), no
+// reservoir/membrane/turbulence forcing.
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -30,6 +31,7 @@
 namespace {
 
 constexpr int MAXS = FHD_MAX_SPECIES;
+const int kCellNodal[3] = {0, 0, 0};
 
 // ---- global parameters (the reference's common::/compressible:: namespaces) ----
 struct P {
@@ -41,6 +43,11 @@ struct P {
     double grav[3] = {0, 0, 0};
     double zeta_ratio = -1;
     int visc_type = 1, advection_type = 0, algorithm_type = 2, stoch_stress_form = 1;
+    // chemistry (chemistry_namespace.H; common::avogadro)
+    int nreaction = 0, reaction_type = 0;
+    int stoich_R[FHD_MAX_REACTIONS][MAXS], stoich_PR[FHD_MAX_REACTIONS][MAXS];
+    double rate_const[FHD_MAX_REACTIONS], alpha_param[FHD_MAX_REACTIONS], beta_param[FHD_MAX_REACTIONS];
+    double T0_chem = 0, avogadro = 0;
 } g;
 
 struct Fab {
@@ -883,6 +890,45 @@ void lincomb(const Fab& dst, double a, const Fab& x, int xc, double b, const Fab
                     dst(i, j, k, dc + n) = a * x(i, j, k, xc + n) + b * y(i, j, k, yc + n);
 }
 
+// compute_compressible_chemistry_source_CLE, chemistry_functions.cpp:128-193: per
+// valid cell, the law-of-mass-action rates and (reaction_type 1) their Langevin
+// terms into source comps 5..5+ns-1
+void chem_source_cle(double dt, double dV, const Fab& prim, const Fab& source, const Fab& ranchem) {
+    const int* N = g.n;
+    const int ns = g.ns, nr = g.nreaction;
+    #pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < N[2]; ++k)
+        for (int j = 0; j < N[1]; ++j)
+            for (int i = 0; i < N[0]; ++i) {
+                double pres = prim(i, j, k, 5);
+                double T = prim(i, j, k, 4);
+                double T0 = g.T0_chem;
+                double ctot = pres / g.Runiv / T;
+                double Navo = g.avogadro;
+                double ck[MAXS];
+                for (int n = 0; n < ns; n++) ck[n] = prim(i, j, k, 6 + ns + n) * ctot;
+                double avg_react_rate[FHD_MAX_REACTIONS];
+                for (int m = 0; m < nr; m++) {
+                    avg_react_rate[m] = g.rate_const[m];
+                    avg_react_rate[m] *= std::exp(-g.alpha_param[m] / g.Runiv * (1 / T - 1 / T0));
+                    avg_react_rate[m] *= std::pow(T / T0, g.beta_param[m]);
+                    for (int n = 0; n < ns; n++) avg_react_rate[m] *= std::pow(ck[n], g.stoich_R[m][n]);
+                }
+                double sourceArr[MAXS];
+                for (int n = 0; n < ns; n++) sourceArr[n] = 0.;
+                for (int m = 0; m < nr; m++) {
+                    avg_react_rate[m] = std::max(0., avg_react_rate[m]);
+                    double W = (g.reaction_type == 1 ? ranchem(i, j, k, m) : 0.0) / std::sqrt(dt * dV);
+                    for (int n = 0; n < ns; n++) {
+                        sourceArr[n] += g.molmass[n] * g.stoich_PR[m][n] * avg_react_rate[m];
+                        if (g.reaction_type == 1)
+                            sourceArr[n] += g.molmass[n] * g.stoich_PR[m][n] * std::sqrt(avg_react_rate[m] / Navo) * W;
+                    }
+                }
+                for (int n = 0; n < ns; n++) source(i, j, k, 5 + n) = sourceArr[n];
+            }
+}
+
 // The RK3 stage update of cons and face momenta, timeStepStag.cpp:439-528 (stage 1),
 // :771-861 (stage 2), :1106-1202 (stage 3).
 void stage_update(int stage, const Fab& cu, const Fab mom[3], const Fab& cin, const Fab min_[3],
@@ -1003,6 +1049,23 @@ int orc_set_params(const fhd_params* p) {
     g.stoch_stress_form = p->stoch_stress_form;
     g.zeta_ratio = p->zeta_ratio;
     if (g.algorithm_type != 2 || p->transport_type != 1) return FHD_ERR_UNSUPPORTED;
+    // chemistry_functions.cpp:45-124; avogadro = Runiv / k_B unless given (common_functions.cpp:775)
+    if (p->nreaction < 0 || p->nreaction > FHD_MAX_REACTIONS) return FHD_ERR_BAD_ARG;
+    g.nreaction = p->nreaction;
+    g.reaction_type = p->reaction_type;
+    if (g.nreaction > 0 && g.reaction_type != 0 && g.reaction_type != 1) return FHD_ERR_UNSUPPORTED;
+    if (g.nreaction > 0 && !(p->T0_chem > 0.)) return FHD_ERR_BAD_ARG;
+    for (int m = 0; m < FHD_MAX_REACTIONS; ++m) {
+        for (int n = 0; n < MAXS; ++n) {
+            g.stoich_R[m][n] = p->stoich_R[m][n];
+            g.stoich_PR[m][n] = p->stoich_P[m][n] - p->stoich_R[m][n];
+        }
+        g.rate_const[m] = p->rate_const[m];
+        g.alpha_param[m] = p->alpha_param[m];
+        g.beta_param[m] = p->beta_param[m];
+    }
+    g.T0_chem = p->T0_chem;
+    g.avogadro = p->avogadro > 0 ? p->avogadro : g.Runiv / g.k_B;
     return FHD_OK;
 }
 
@@ -1065,6 +1128,15 @@ int orc_transport_coeffs(fhd_fab prim, fhd_fab eta, fhd_fab zeta, fhd_fab kappa,
     return orc_take_status();
 }
 
+int orc_chemistry_source_cle(double dt, double dV, fhd_fab prim, fhd_fab source, fhd_fab ranchem) {
+    if (g.nreaction < 1 || !prim.data || !source.data) return FHD_ERR_BAD_ARG;
+    if (g.reaction_type == 1 && !ranchem.data) return FHD_ERR_BAD_ARG;
+    Fab r;
+    if (ranchem.data) r = Fab(ranchem);
+    chem_source_cle(dt, dV, Fab(prim), Fab(source), r);
+    return FHD_OK;
+}
+
 int orc_flux_stag(fhd_fab cu, const fhd_fab* mom, fhd_fab prim, const fhd_fab* vel, fhd_fab eta,
                   fhd_fab zeta, fhd_fab kappa, fhd_fab chi, fhd_fab D, const fhd_fab* faceflux,
                   const fhd_fab* edgeflux, const fhd_fab* cenflux, const fhd_fab* stochface,
@@ -1092,6 +1164,13 @@ int orc_rk3_step_stag(fhd_fab cu_, const fhd_fab* mom_, fhd_fab prim_, const fhd
     Fab cu(cu_), prim(prim_), eta(eta_), zeta(zeta_), kappa(kappa_), chi(chi_), D(D_);
     Fab source;
     if (source_.data) source = Fab(source_);
+    // the reference's driver always passes a (zeroed) source; chemistry writes into it
+    OwnedFab own_source(N[0], N[1], N[2], kCellNodal, 0, g.nreaction > 0 && !source_.data ? nvars : 1);
+    if (g.nreaction > 0 && !source_.data) source = own_source.f;
+    // ranchem = 1.0*ranchem_A + w*ranchem_B per stage (timeStepStag.cpp:354-361)
+    const bool cle = g.nreaction > 0 && g.reaction_type == 1;
+    if (cle && (!noise || !noise->chem[0].data || !noise->chem[1].data)) return FHD_ERR_BAD_ARG;
+    OwnedFab ranchem(N[0], N[1], N[2], kCellNodal, 0, cle ? g.nreaction : 1);
     Fab mom[3], vel[3], ff[3], cf[3], ef[6];
     for (int d = 0; d < 3; ++d) {
         mom[d] = Fab(mom_[d]); vel[d] = Fab(vel_[d]); ff[d] = Fab(faceflux[d]); cf[d] = Fab(cenflux[d]);
@@ -1141,6 +1220,10 @@ int orc_rk3_step_stag(fhd_fab cu_, const fhd_fab* mom_, fhd_fab prim_, const fhd
         transport_coeffs(prim, eta, zeta, kappa, chi, D);
         weigh_noise(w[s]);
         flux_stag(*cins[s], mins[s], prim, vel, eta, zeta, kappa, chi, D, ff, ef, cf, sf, se, sc, dt);
+        if (g.nreaction > 0) {
+            if (cle) lincomb(ranchem.f, swgt1, Fab(noise->chem[0]), 0, w[s], Fab(noise->chem[1]), 0, 0, g.nreaction, 0);
+            chem_source_cle(dt, g.dx[0] * g.dx[1] * g.dx[2], prim, source, ranchem.f);
+        }
         stage_update(s + 1, cu, mom, *cins[s], mins[s], *couts[s], mouts[s], source, ff, ef, cf, dt);
         for (int d = 0; d < 3; ++d) fill_boundary(mouts[s][d]);
         fill_boundary(*couts[s]);

@@ -45,6 +45,7 @@ def lib():
         L.orc_rk3_step_stag.argtypes = [fab, pfab, fab, pfab, fab, fab, fab, fab, fab, fab, pfab, pfab,
                                         pfab, P(FhdNoise), d]
         L.orc_fill_random_normal.argtypes = [fab, i, i, d, d, C.c_uint64, C.c_uint64]
+        L.orc_chemistry_source_cle.argtypes = [d, d, fab, fab, fab]
         L.orc_philox4x32_10.argtypes = [P(C.c_uint32), P(C.c_uint32), P(C.c_uint32)]
         L.orc_philox4x32_10.restype = None
         L.orc_fill_noise_mt64.argtypes = [P(FhdNoise), C.c_uint64]
@@ -118,6 +119,13 @@ def rk3_step(st, noise, dt):
                                    st.cenflux_fabs(), nz, dt)
 
 
+def chemistry_source_cle(p, dt, dV, prim, source, ranchem=None):
+    """compute_compressible_chemistry_source_CLE (chemistry_functions.cpp:128-193)."""
+    set_params(p)
+    rf = ranchem.fab() if ranchem is not None else FhdFab()
+    return lib().orc_chemistry_source_cle(dt, dV, prim.fab(), source.fab(), rf)
+
+
 def fill_random_normal(mf, scomp, ncomp, mean, variance, seed, stream_id):
     _chk(lib().orc_fill_random_normal(mf.fab(), scomp, ncomp, mean, variance, seed, stream_id), "fill")
 
@@ -133,6 +141,10 @@ def fill_step_noise(noise, seed, step):
             fill_random_normal(noise.face[s][d], 0, ns + 1, 0.0, 1.0, seed, (step << 8) | sid); sid += 1
             fill_random_normal(noise.edge[s][d], 0, 1, 0.0, 1.0, seed, (step << 8) | sid); sid += 1
             fill_random_normal(noise.cen[s][d], 0, 1, 0.0, 2.0, seed, (step << 8) | sid); sid += 1
+    # ranchem_A / ranchem_B, variance 1 (timeStepStag.cpp:225-229)
+    for s in range(2):
+        if noise.chem[s] is not None:
+            fill_random_normal(noise.chem[s], 0, noise.p.nreaction, 0.0, 1.0, seed, (step << 8) | sid); sid += 1
 
 
 def stats_stag(st, stats, steps, flags=15):

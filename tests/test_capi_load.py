@@ -35,14 +35,16 @@ def test_every_declared_entry_point_is_exported():
 def test_struct_layouts_match_header(tmp_path):
     src = tmp_path / "sz.c"
     src.write_text(f'#include "{HEADER}"\n#include <stdio.h>\n#include <stddef.h>\n'
-                   'int main(){printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(fhd_fab), sizeof(fhd_params), '
+                   'int main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(fhd_fab), sizeof(fhd_params), '
                    'sizeof(fhd_noise), offsetof(fhd_params, seed), sizeof(fhd_stats), '
-                   'offsetof(fhd_stats, cumomVars));return 0;}\n')
+                   'offsetof(fhd_stats, cumomVars), offsetof(fhd_params, stoich_P), offsetof(fhd_params, avogadro), '
+                   'offsetof(fhd_noise, chem));return 0;}\n')
     exe = tmp_path / "sz"
     subprocess.check_call(["gcc", str(src), "-o", str(exe)])
     vals = [int(x) for x in subprocess.check_output([str(exe)]).split()]
     assert vals == [C.sizeof(capi.FhdFab), C.sizeof(capi.FhdParams), C.sizeof(capi.FhdNoise),
-                    capi.FhdParams.seed.offset, C.sizeof(capi.FhdStats), capi.FhdStats.cumomVars.offset]
+                    capi.FhdParams.seed.offset, C.sizeof(capi.FhdStats), capi.FhdStats.cumomVars.offset,
+                    capi.FhdParams.stoich_P.offset, capi.FhdParams.avogadro.offset, capi.FhdNoise.chem.offset]
 
 
 def test_strerror_is_callable_without_gpu():
@@ -75,6 +77,32 @@ def test_create_rejects_out_of_scope_parameters_without_gpu(change, code):
     lib = capi.load()
     assert lib.fhd_create(C.byref(h), C.byref(cp), 0) == getattr(capi, code)
     assert not h.value
+
+
+@pytest.mark.parametrize("field,value,code", [
+    ("nreaction", 9, "FHD_ERR_BAD_ARG"),
+    ("nreaction", -1, "FHD_ERR_BAD_ARG"),
+    ("reaction_type", 2, "FHD_ERR_UNSUPPORTED"),   # SSA / tau leaping (chemistry_functions.cpp:131-133)
+    ("T0_chem", 0.0, "FHD_ERR_BAD_ARG"),           # chemistry_functions.cpp:135
+    ("stoich_R", -1, "FHD_ERR_BAD_ARG"),
+])
+def test_create_rejects_bad_chemistry_without_gpu(field, value, code):
+    from fhdex_b200.params import no2_dimerization
+    cp = no2_dimerization(8).to_c()
+    if field == "stoich_R":
+        cp.stoich_R[1][0] = value
+    else:
+        setattr(cp, field, value)
+    h = C.c_void_p()
+    lib = capi.load()
+    assert lib.fhd_create(C.byref(h), C.byref(cp), 0) == getattr(capi, code)
+    assert not h.value
+
+
+def test_chemistry_operator_validates_without_gpu():
+    lib = capi.load()
+    nf = capi.FhdFab()
+    assert lib.fhd_chemistry_source_cle(None, 1e-12, 1e-15, nf, nf, nf) == capi.FHD_ERR_BAD_ARG
 
 
 def test_batch_tile_entry_points_validate_without_gpu():
