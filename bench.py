@@ -71,8 +71,10 @@ def measured_peak():
 
 
 def make_params(args):
-    from fhdex_b200.params import argon, argon_single, mixture4
+    from fhdex_b200.params import argon, argon_single, mixture4, no2_dimerization
     prec = 1 if args.precision == "mixed" else 0
+    if args.gas == "no2":
+        return no2_dimerization(args.n, dx=args.dx, precision=prec, seed=args.seed)
     if args.ns == 1:
         return argon_single(args.n, dx=args.dx, precision=prec, seed=args.seed)
     if args.ns == 2:
@@ -220,8 +222,9 @@ def run_reference(args):
 
 def config_dict(args, p, dt, tile):
     return {
-        "workload": (f"{ {1: 'argon (single gas)', 2: 'argon (2 identical species)'}.get(p.nspecies, '4-species mixture')} "
-                     f"{p.n_cells[0]}^3, dx={p.dx[0]:g} cm, periodic, {args.precision}, in-kernel Philox noise"),
+        "workload": (("2 NO2 <-> N2O4 (chemistry source, CLE)" if p.nreaction > 0 else
+                      { {1: 'argon (single gas)', 2: 'argon (2 identical species)'}.get(p.nspecies, '4-species mixture')})
+                     + f" {p.n_cells[0]}^3, dx={p.dx[0]:g} cm, periodic, {args.precision}, in-kernel Philox noise"),
         "n_cells": list(p.n_cells), "nspecies": p.nspecies, "precision": args.precision, "dt_s": dt,
         "noise": "philox-4x32-10 in kernel", "tile": tile,
         "l2": "inputs larger than L2 (state ~%.1f GB)" % (state_gb(p)),
@@ -309,6 +312,8 @@ def run_ours(args):
     value = replicas.whole_job_rate(cells * args.steps, env, ms)
     # every bracketed profile scope is one launch, except the face-flux scope (3 launches)
     launches = sum(v[1] for v in prof.values()) + 2 * prof["faces"][1]
+    if p.nreaction > 0:  # k_chem runs inside each stage's cellprep scope
+        launches += prof["cellprep"][1]
 
     # roofline of the dominant kernel group: one RK stage = k_cellprep + k_taus +
     # 3 x k_faces + k_update (conversion, transport coefficients, calculateFluxStag
@@ -346,6 +351,33 @@ def run_ours(args):
     gms = replicas.max_over_ranks(g0.elapsed_time(g1), env, device=f"cuda:{local}")
     graph = {"ms_per_step": gms / args.steps, "value": replicas.whole_job_rate(cells * args.steps, env, gms),
              "path": "fhd_rk3_steps_stag (one captured step replayed per step)"}
+
+    # the chemistry kernel alone (fhd_chemistry_source_cle on the state's prim):
+    # reads T, p and X (2 + ns doubles) and the nreaction noises, writes ns doubles
+    chem = None
+    if p.nreaction > 0:
+        from fhdex_b200.fab import CELL, MultiFab
+        src = MultiFab(p.n_cells, CELL, p.nvars, 0, device=f"cuda:{local}")
+        W = MultiFab(p.n_cells, CELL, p.nreaction, 0, device=f"cuda:{local}")
+        ctx.fill_random_normal(W, 0, p.nreaction, 0.0, 1.0, overridesync=False, fillboundary=False, stream_id=5)
+        dV = p.dx[0] * p.dx[1] * p.dx[2]
+        for _ in range(3):
+            ctx.chemistry_source_cle(st.prim, src, W, dt, dV)
+        reps = 20
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        cs = torch.cuda.current_stream(local)
+        c0.record(cs)
+        for _ in range(reps):
+            ctx.chemistry_source_cle(st.prim, src, W, dt, dV)
+        c1.record(cs)
+        torch.cuda.synchronize()
+        cms = c0.elapsed_time(c1) / reps
+        cbytes = 8.0 * cells * (2 + p.nspecies + p.nreaction + p.nspecies)
+        chem = {"kernel": "k_chem (fhd_chemistry_source_cle)", "ms_per_launch": cms,
+                "algorithmic_bytes_per_launch": cbytes, "achieved_gbs": cbytes / cms / 1e6,
+                "frac": cbytes / cms / 1e6 / peak, "peak": peak, "peak_kind": peak_kind,
+                "note": "in the step it runs once per stage inside the cellprep scope (in-kernel noise: no W reads)"}
+        del src, W
 
     # e2e through the host-buffer C-ABI call (H2D + step + D2H, pinned memory)
     ctx.close()
@@ -386,9 +418,11 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
-        "data": "synthetic (uniform argon at rest + in-kernel Philox noise; no dataset)",
+        "data": ("synthetic (uniform NO2/N2O4 at chemical equilibrium + in-kernel Philox noise; no dataset)"
+                 if p.nreaction > 0 else "synthetic (uniform argon at rest + in-kernel Philox noise; no dataset)"),
         "config": dict(config_dict(args, p, dt, tname), autotune_ms_per_step=tune),
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "graph_replay": graph, "gpu_launches": launches,
+        "chemistry": chem,
         "clocks": clk, "status": status,
     }
     print(json.dumps(out), flush=True)
@@ -604,6 +638,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--ns", type=int, default=2)
+    ap.add_argument("--gas", default="argon", choices=["argon", "no2"],
+                    help="argon: --ns selects the species form; no2: 2 NO2 <-> N2O4 with the chemistry source")
     ap.add_argument("--dx", type=float, default=8e-6)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--tile", default="auto")

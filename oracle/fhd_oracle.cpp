@@ -1539,6 +1539,8 @@ int orc_fill_noise_mt64(const fhd_noise* nz, uint64_t seed) {
             fill(nz->edge[s][d], 1.0);
             fill(nz->cen[s][d], 2.0);
         }
+    for (int s = 0; s < 2; ++s)
+        if (nz->chem[s].data) fill(nz->chem[s], 1.0);  // ranchem_A/B, variance 1
     return FHD_OK;
 }
 
