@@ -13,6 +13,11 @@
 // the reference's two reaction loops into one changes no arithmetic: each rate
 // depends only on its own reaction.
 //
+// Divisions by the run's constants (Runiv, T0, sqrt(dt dV), N_A) and the second
+// division by the cell's T (whose reciprocal the rate needs anyway) use the
+// correctly rounded reciprocal-and-correction division of fhd_div.h: the same
+// quotients as a / b, in a few instructions instead of an iterative division.
+//
 // c_n^R for the integer stoichiometric coefficients is R-1 multiplications: 1 for
 // R = 0 and c for R = 1 as pow returns them, c*c (correctly rounded, as a correctly
 // rounded pow gives) for R = 2, within an ulp of pow for R >= 3.  exp and the real
@@ -40,6 +45,8 @@ struct ChemParams {
     double T0, rT0;         // T0 and 1/T0
     double navo;            // Avogadro's number
     double sq;              // sqrt(dt * dV)
+    double rR, rnavo, rsq;  // 1/Runiv, 1/navo, 1/sq
+    uint32_t div_lo, div_span;  // dividend window of div_rcp (span 0: plain divisions)
 };
 
 // Noise of the chemistry source: none (deterministic), the per-step A/B fields
@@ -71,6 +78,12 @@ inline ChemParams chem_params(const fhd_params& p, double dt, double dV) {
     C.rT0 = 1 / p.T0_chem;
     C.navo = p.avogadro > 0 ? p.avogadro : p.Runiv / p.k_B;
     C.sq = std::sqrt(dt * dV);
+    C.rR = 1.0 / p.Runiv;
+    C.rnavo = 1.0 / C.navo;
+    C.rsq = 1.0 / C.sq;
+    const bool ok = div_divisor_ok(p.Runiv) && div_divisor_ok(C.T0) && div_divisor_ok(C.navo) && div_divisor_ok(C.sq);
+    C.div_lo = kDivAlo;
+    C.div_span = ok ? kDivAspan : 0u;
     return C;
 }
 
@@ -86,27 +99,28 @@ FHD_D double chem_ipow(double c, int r) {
 template <int NS>
 FHD_D void chem_point(const DevParams& P, const ChemParams& C, double pres, double T, const double (&X)[NS],
                       const double* W, double (&S)[NS]) {
-    const double ctot = pres / P.Runiv / T;
+    const double rT = 1 / T;
+    const double ctot = div_rcp_any(div_rcp(pres, P.Runiv, C.rR, C.div_lo, C.div_span), T, rT);
     double ck[NS];
 #pragma unroll
     for (int n = 0; n < NS; ++n) {
         ck[n] = X[n] * ctot;
         S[n] = 0.;
     }
-    const double rT = 1 / T;
 #pragma unroll 1
     for (int m = 0; m < C.nr; ++m) {
         double a = C.rate[m];
         a *= exp(C.nar[m] * (rT - C.rT0));
-        a *= pow(T / C.T0, C.beta[m]);
+        a *= pow(div_rcp(T, C.T0, C.rT0, C.div_lo, C.div_span), C.beta[m]);
 #pragma unroll
         for (int n = 0; n < NS; ++n) a *= chem_ipow(ck[n], C.sR[m][n]);
         a = (0. < a) ? a : 0.;  // std::max(0., a)
-        const double Wm = W[m] / C.sq;
+        const double Wm = div_rcp_z(W[m], C.sq, C.rsq, C.div_lo, C.div_span);
+        const double fl = C.type == 1 ? sqrt(div_rcp_z(a, C.navo, C.rnavo, C.div_lo, C.div_span)) : 0.0;
 #pragma unroll
         for (int n = 0; n < NS; ++n) {
             S[n] += P.molmass[n] * (double)C.sPR[m][n] * a;
-            if (C.type == 1) S[n] += P.molmass[n] * (double)C.sPR[m][n] * sqrt(a / C.navo) * Wm;
+            if (C.type == 1) S[n] += P.molmass[n] * (double)C.sPR[m][n] * fl * Wm;
         }
     }
 }
