@@ -17,11 +17,14 @@
 //   MultiFabFillRandom,
 //   MultiFabFillRandomNormal,
 //   MultiFabFillRandomUniform  src_rng/rng_functions.H:13-22
+//   compute_compressible_chemistry_source_CLE
+//                              src_chemistry/chemistry_functions.H:20-21
 //
 // As in the reference, physics parameters are process globals in namespaces
-// `common` and `compressible` (src_common/common_namespace.H,
-// src_compressible/compressible_namespace.H) with the reference's names and
-// defaults (common_functions.cpp:332-550, compressible_functions.cpp:15-88).
+// `common`, `compressible` and `chemistry` (src_common/common_namespace.H,
+// src_compressible/compressible_namespace.H, src_chemistry/chemistry_namespace.H)
+// with the reference's names and defaults (common_functions.cpp:332-550,
+// compressible_functions.cpp:15-88, chemistry_functions.cpp:45-124).
 // The first call builds one fhd_ctx from them on `fhd::ref::device`; after
 // changing a global call fhd::ref::reinitialize().
 //
@@ -83,6 +86,29 @@ inline int transport_type = 1;
 inline Real zeta_ratio = -1.0;
 }  // namespace compressible
 
+namespace common {
+// <= 0: Runiv / k_B, as InitializeCommonNamespace derives it (common_functions.cpp:775)
+inline fhd::amrex_compat::Real avogadro = 0.0;
+}  // namespace common
+
+namespace chemistry {
+using fhd::amrex_compat::GpuArray;
+using fhd::amrex_compat::Real;
+// Array2D<int, 0, MAX_REACTION, 0, MAX_SPECIES> of the reference, indexed (reaction, species)
+struct StoichTable {
+    int v[FHD_MAX_REACTIONS][FHD_MAX_SPECIES] = {};
+    int& operator()(int m, int n) { return v[m][n]; }
+    int operator()(int m, int n) const { return v[m][n]; }
+};
+inline int nreaction = 0;
+inline int reaction_type = 0;  // 0 deterministic, 1 CLE (the only two the compressible source takes)
+inline StoichTable stoich_coeffs_R, stoich_coeffs_P;
+inline GpuArray<Real, FHD_MAX_REACTIONS> rate_const{};
+inline GpuArray<Real, FHD_MAX_REACTIONS> alpha_param{};
+inline GpuArray<Real, FHD_MAX_REACTIONS> beta_param{};
+inline Real T0_chem = 0.0;
+}  // namespace chemistry
+
 namespace fhd {
 namespace ref {
 
@@ -142,6 +168,19 @@ inline fhd_params params_from_globals() {
     p.stoch_stress_form = common::stoch_stress_form;
     p.precision = precision;
     p.seed = uint64_t(int64_t(common::seed));
+    p.nreaction = chemistry::nreaction;
+    p.reaction_type = chemistry::reaction_type;
+    for (int m = 0; m < FHD_MAX_REACTIONS; ++m) {
+        for (int n = 0; n < FHD_MAX_SPECIES; ++n) {
+            p.stoich_R[m][n] = chemistry::stoich_coeffs_R(m, n);
+            p.stoich_P[m][n] = chemistry::stoich_coeffs_P(m, n);
+        }
+        p.rate_const[m] = chemistry::rate_const[m];
+        p.alpha_param[m] = chemistry::alpha_param[m];
+        p.beta_param[m] = chemistry::beta_param[m];
+    }
+    p.T0_chem = chemistry::T0_chem;
+    p.avogadro = common::avogadro;
     return p;
 }
 
@@ -253,6 +292,26 @@ inline void conservedToPrimitiveStag(fhd::amrex_compat::MultiFab& prim_in,
     fabs_of(momStag_in, mom);
     check(fhd_conserved_to_primitive_stag(context(), prim_in.fab(), vel, cons_in.fab(), mom),
           "conservedToPrimitiveStag");
+}
+
+// compute_compressible_chemistry_source_CLE (chemistry_functions.cpp:128-193):
+// species components 5.. of `source` from `prim` and the reaction noises
+// `ranchem` (read for reaction_type 1 only).
+inline void compute_compressible_chemistry_source_CLE(fhd::amrex_compat::Real dt, fhd::amrex_compat::Real dV,
+                                                      fhd::amrex_compat::MultiFab& prim,
+                                                      fhd::amrex_compat::MultiFab& source,
+                                                      fhd::amrex_compat::MultiFab& ranchem) {
+    using namespace fhd::ref;
+    require_device(prim, "compute_compressible_chemistry_source_CLE");
+    require_device(source, "compute_compressible_chemistry_source_CLE");
+    fhd_fab rf;
+    std::memset(&rf, 0, sizeof(rf));
+    if (chemistry::reaction_type == 1) {
+        require_device(ranchem, "compute_compressible_chemistry_source_CLE");
+        rf = ranchem.fab();
+    }
+    check(fhd_chemistry_source_cle(context(), dt, dV, prim.fab(), source.fab(), rf),
+          "compute_compressible_chemistry_source_CLE");
 }
 
 // calculateTransportCoeffs (transCoeffs.cpp:7-90).  A bad mass fraction is

@@ -6,9 +6,10 @@
 //
 //   reference_driver shapes <n>
 //       print the Array4 bounds of every MultiFab kind (host arena, no GPU)
-//   reference_driver run <device|pinned> <n> <nsteps> <seed> <dt> <out.bin>
+//   reference_driver run <device|pinned> <n> <nsteps> <seed> <dt> <out.bin> [argon|no2]
 //       run nsteps RK3 steps (steps 0..nsteps-1) and write cu, cumom[0..2],
-//       prim, vel[0..2] (whole buffers, ghosts included) to out.bin
+//       prim, vel[0..2] (whole buffers, ghosts included) to out.bin; no2: the
+//       2 NO2 <-> N2O4 gas with the chemistry source (chemistry:: globals)
 //   reference_driver massfrac <n>
 //       start from a state with a zero mass fraction: calculateTransportCoeffs
 //       must report it through the abort handler (exit code 3)
@@ -49,6 +50,37 @@ static void set_argon(int n, int seed) {
     common::advection_type = 2;
     common::stoch_stress_form = 1;
     common::seed = seed;
+}
+
+// 2 NO2 <-> N2O4 with chemical Langevin noise (the reference's NO2 dimerization
+// deck's gas and reactions)
+static void set_no2(int n, int seed) {
+    set_argon(n, seed);
+    const double mm[2] = {46.0055, 92.0110}, di[2] = {3.765e-08, 4.621e-08}, dof[2] = {7.279586, 18.049072},
+                 rb[2] = {0.723969, 0.276031};
+    for (int s = 0; s < 2; ++s) {
+        common::molmass[s] = mm[s];
+        common::diameter[s] = di[s];
+        common::dof[s] = dof[s];
+        common::rhobar[s] = rb[s];
+        common::T_init[s] = 350.0;
+    }
+    common::rho0 = 1.858338e-03;
+    common::k_B = 1.38065e-16;
+    common::Runiv = 8.31446e7;
+    chemistry::nreaction = 2;
+    chemistry::reaction_type = 1;
+    chemistry::stoich_coeffs_R(0, 0) = 2;  // 2 NO2 -> N2O4
+    chemistry::stoich_coeffs_P(0, 1) = 1;
+    chemistry::stoich_coeffs_R(1, 1) = 1;  // N2O4 -> 2 NO2
+    chemistry::stoich_coeffs_P(1, 0) = 2;
+    chemistry::rate_const[0] = 4.065753e+11;
+    chemistry::rate_const[1] = 6.236899e+07;
+    chemistry::alpha_param[0] = -5.337990e+10;
+    chemistry::alpha_param[1] = 5.370000e+11;
+    chemistry::beta_param[0] = 0.644950;
+    chemistry::beta_param[1] = -1.100000;
+    chemistry::T0_chem = 350.0;
 }
 
 struct State {
@@ -152,8 +184,12 @@ static void step_all(State& s, double dt, int nsteps) {
                     s.edgeflux_x, s.edgeflux_y, s.edgeflux_z, s.cenflux, s.ranchem, s.geom, dt, step, turbforce);
 }
 
-static int cmd_run(const std::string& arena, int n, int nsteps, int seed, double dt, const char* out) {
-    set_argon(n, seed);
+static int cmd_run(const std::string& arena, int n, int nsteps, int seed, double dt, const char* out,
+                   const std::string& gas) {
+    if (gas == "no2")
+        set_no2(n, seed);
+    else
+        set_argon(n, seed);
     // initialise on the device, as the reference's GPU build does
     State dev(n, Arena::Device, true);
     dev.init();
@@ -213,9 +249,9 @@ int main(int argc, char** argv) {
     const std::string cmd = argv[1];
     try {
         if (cmd == "shapes") return cmd_shapes(std::atoi(argv[2]));
-        if (cmd == "run" && argc == 8)
+        if (cmd == "run" && (argc == 8 || argc == 9))
             return cmd_run(argv[2], std::atoi(argv[3]), std::atoi(argv[4]), std::atoi(argv[5]),
-                           std::strtod(argv[6], nullptr), argv[7]);
+                           std::strtod(argv[6], nullptr), argv[7], argc == 9 ? argv[8] : "argon");
         if (cmd == "massfrac") return cmd_massfrac(std::atoi(argv[2]));
     } catch (const std::exception& e) {
         std::fprintf(stderr, "error: %s\n", e.what());

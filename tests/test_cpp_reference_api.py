@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 import torch
 
-from fhdex_b200.params import argon, stable_dt
+from fhdex_b200.params import argon, no2_dimerization, stable_dt
 from fhdex_b200.state import StagState
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -75,14 +75,17 @@ def read_state(path, st):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("arena", ["device", "pinned"])
-def test_reference_driver_equals_c_abi_path(driver, tmp_path, arena):
+@pytest.mark.parametrize("arena,gas", [("device", "argon"), ("pinned", "argon"), ("device", "no2"), ("pinned", "no2")])
+def test_reference_driver_equals_c_abi_path(driver, tmp_path, arena, gas):
+    """The reference-named API (RK3stepStag over the compat MultiFabs, parameters in
+    the common::/compressible::/chemistry:: globals) equals the C ABI bit for bit;
+    no2 runs the chemistry source inside every stage."""
     from fhdex_b200.context import Context
     n, nsteps, seed = 12, 3, 7
-    p = argon(n, dx=8e-6, seed=seed)
+    p = no2_dimerization(n, dx=8e-6, seed=seed) if gas == "no2" else argon(n, dx=8e-6, seed=seed)
     dt = stable_dt(p)
     out = str(tmp_path / "state.bin")
-    r = subprocess.run([driver, "run", arena, str(n), str(nsteps), str(seed), repr(dt), out],
+    r = subprocess.run([driver, "run", arena, str(n), str(nsteps), str(seed), repr(dt), out, gas],
                        capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     ctx = Context(p)
