@@ -38,6 +38,7 @@ def _units():
     u.append(("stats", "fhd_stats.cu", ["-fmad=false"]))
     u.append(("sf", "fhd_sf.cu", ["-fmad=false"]))
     u.append(("chem", "fhd_chem.cu", ["-fmad=false"]))
+    u.append(("plot", "fhd_plot.cu", ["-fmad=false"]))
     return u
 
 

@@ -135,6 +135,12 @@ def _declare(lib):
         "fhd_rk3_steps_stag": (i, [vp, fab, pfab, fab, pfab, d, C.c_int64, i]),
         "fhd_fill_step_noise": (i, [vp, P(FhdNoise), C.c_int64]),
         "fhd_chemistry_source_cle": (i, [vp, d, d, fab, fab, fab]),
+        "fhd_plotfile_ncomp": (i, [P(FhdParams), i]),
+        "fhd_plotfile_varname": (i, [P(FhdParams), i, i, C.c_char_p, i]),
+        "fhd_plotfile_write_host": (i, [P(FhdParams), C.c_char_p, P(d), i, d, i]),
+        "fhd_plotfile_pack": (i, [vp, i, fab, fab, pfab, fab, pfab, fab, fab, fab, P(FhdStats)]),
+        "fhd_write_plotfile_stag": (i, [vp, C.c_char_p, i, d, i, fab, pfab, fab, pfab, fab, fab, fab,
+                                        P(FhdStats)]),
         "fhd_rk3_step_stag": (i, [vp, fab, pfab, fab, pfab, fab, fab, fab, fab, fab, fab,
                                   pfab, pfab, pfab, P(FhdNoise), d, C.c_int64]),
         "fhd_rk3_step_stag_host": (i, [vp, fab, pfab, fab, pfab, P(FhdNoise), d, C.c_int64,

@@ -495,6 +495,113 @@ int fhd_fill_random_uniform(fhd_ctx* c, fhd_fab mf, int scomp, int ncomp, int ov
     return rc;
 }
 
+static bool device_accessible(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return false; }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged || a.type == cudaMemoryTypeHost;
+}
+
+static bool plot_inputs_accessible(int flags, const fhd_fab& cu, const fhd_fab* cumom, const fhd_fab& prim,
+                                   const fhd_fab* vel, const fhd_fab& eta, const fhd_fab& kappa, const fhd_fab& zeta,
+                                   const fhd_stats* st, int visc3) {
+    std::vector<const void*> ptrs = {cu.data, prim.data, eta.data, kappa.data};
+    if (visc3) ptrs.push_back(zeta.data);
+    for (int d = 0; d < 3; ++d) { ptrs.push_back(cumom[d].data); ptrs.push_back(vel[d].data); }
+    if (flags & FHD_PLOT_MEANS) {
+        ptrs.push_back(st->cuMeans.data);
+        ptrs.push_back(st->primMeans.data);
+        for (int d = 0; d < 3; ++d) { ptrs.push_back(st->cumomMeans[d].data); ptrs.push_back(st->velMeans[d].data); }
+    }
+    if (flags & FHD_PLOT_VARS) {
+        ptrs.push_back(st->cuVars.data);
+        ptrs.push_back(st->primVars.data);
+        for (int d = 0; d < 3; ++d) { ptrs.push_back(st->cumomVars[d].data); ptrs.push_back(st->velVars[d].data); }
+    }
+    if (flags & FHD_PLOT_COVARS) ptrs.push_back(st->coVars.data);
+    if (flags & FHD_PLOT_MOM3) ptrs.push_back(st->mom3.data);
+    if (flags & FHD_PLOT_MOM4) ptrs.push_back(st->mom4.data);
+    for (const void* p : ptrs)
+        if (!p || !device_accessible(p)) return false;
+    return true;
+}
+
+static bool plot_params_ok(const fhd_params* p) {
+    if (!p || p->nspecies < 1 || p->nspecies > 4) return false;
+    for (int d = 0; d < 3; ++d)
+        if (p->n_cells[d] < 1) return false;
+    return true;
+}
+
+int fhd_plotfile_ncomp(const fhd_params* p, int flags) {
+    if (!plot_params_ok(p) || flags < 0 || flags > 31) return -FHD_ERR_BAD_ARG;
+    std::vector<std::string> names;
+    const int rc = plot_names(*p, flags, names);
+    return rc ? -rc : (int)names.size();
+}
+
+int fhd_plotfile_varname(const fhd_params* p, int flags, int comp, char* buf, int buflen) {
+    if (!plot_params_ok(p) || !buf || buflen < 1 || flags < 0 || flags > 31) return FHD_ERR_BAD_ARG;
+    std::vector<std::string> names;
+    const int rc = plot_names(*p, flags, names);
+    if (rc) return rc;
+    if (comp < 0 || comp >= (int)names.size() || (int)names[comp].size() >= buflen) return FHD_ERR_BAD_ARG;
+    std::memcpy(buf, names[comp].c_str(), names[comp].size() + 1);
+    return FHD_OK;
+}
+
+int fhd_plotfile_write_host(const fhd_params* p, const char* dir, const double* data, int flags, double time,
+                            int step) {
+    if (!plot_params_ok(p) || !dir || !data || flags < 0 || flags > 31) return FHD_ERR_BAD_ARG;
+    std::vector<std::string> names;
+    const int rc = plot_names(*p, flags, names);
+    if (rc) return rc;
+    return plot_write(*p, dir, data, names, time, step);
+}
+
+int fhd_plotfile_pack(fhd_ctx* c, int flags, fhd_fab out, fhd_fab cu, const fhd_fab cumom[3], fhd_fab prim,
+                      const fhd_fab vel[3], fhd_fab eta, fhd_fab kappa, fhd_fab zeta, const fhd_stats* stats) {
+    if (!c || !cumom || !vel || flags < 0 || flags > 31 || (flags && !stats)) return FHD_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    const int visc3 = c->prm.visc_type == 3 || c->prm.visc_type == -3;
+    if (!out.data || !device_accessible(out.data) ||
+        !plot_inputs_accessible(flags, cu, cumom, prim, vel, eta, kappa, zeta, stats, visc3))
+        return FHD_ERR_BAD_ARG;
+    return plot_pack(c->prm, flags, out, cu, cumom, prim, vel, eta, kappa, zeta, stats, c->stream);
+}
+
+int fhd_write_plotfile_stag(fhd_ctx* c, const char* plot_base_name, int step, double time, int flags, fhd_fab cu,
+                            const fhd_fab cumom[3], fhd_fab prim, const fhd_fab vel[3], fhd_fab eta, fhd_fab kappa,
+                            fhd_fab zeta, const fhd_stats* stats) {
+    if (!c || !plot_base_name || step < 0) return FHD_ERR_BAD_ARG;
+    const int nc = fhd_plotfile_ncomp(&c->prm, flags);
+    if (nc <= 0) return nc < 0 ? -nc : FHD_ERR_BAD_ARG;
+    std::vector<std::string> names;
+    int rc = plot_names(c->prm, flags, names);
+    if (rc) return rc;
+    cudaSetDevice(c->device);
+    const int* n = c->prm.n_cells;
+    const size_t cells = (size_t)n[0] * n[1] * n[2];
+    double* dbuf = nullptr;
+    if (cudaMalloc(&dbuf, cells * nc * sizeof(double)) != cudaSuccess) { cudaGetLastError(); return FHD_ERR_OOM; }
+    const fhd_fab out = make_fab(dbuf, n, CELLN, 0, nc, FHD_F64);
+    rc = fhd_plotfile_pack(c, flags, out, cu, cumom, prim, vel, eta, kappa, zeta, stats);
+    std::vector<double> host;
+    if (!rc) {
+        host.resize(cells * nc);
+        if (cudaMemcpyAsync(host.data(), dbuf, cells * nc * sizeof(double), cudaMemcpyDeviceToHost, c->stream) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(c->stream) != cudaSuccess)
+            rc = FHD_ERR_CUDA;
+    }
+    cudaFree(dbuf);
+    if (rc) return rc;
+    // amrex::Concatenate(plot_base_name, step, 9)
+    char num[32];
+    std::snprintf(num, sizeof(num), "%09d", step);
+    const std::string dir = std::string(plot_base_name) + num;
+    return plot_write(c->prm, dir.c_str(), host.data(), names, time, step);
+}
+
 int fhd_chemistry_source_cle(fhd_ctx* c, double dt, double dV, fhd_fab prim, fhd_fab source, fhd_fab ranchem) {
     if (!c || c->prm.nreaction < 1 || !(dt > 0) || !(dV > 0)) return FHD_ERR_BAD_ARG;
     const int ns = c->prm.nspecies, nprim = 6 + 2 * ns;

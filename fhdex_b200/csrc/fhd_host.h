@@ -4,6 +4,8 @@
 #pragma once
 #include <cmath>
 #include <cstring>
+#include <string>
+#include <vector>
 #include <cuda_runtime.h>
 #include "../../include/fhd_capi.h"
 #include "fhd_device.cuh"
@@ -136,6 +138,13 @@ int fill_ghosts(const GhostReq* reqs, int n, const int ncell[3], cudaStream_t s)
 // chemistry source (fhd_chem.cu): writes species comps 5.. of `source` at the valid
 // cells from `prim`; na/nb: the A/B (mode CN_AB) or W (CN_W) noise fabs
 struct ChemParams;
+// plotfiles (fhd_plot.cu)
+int plot_pack(const fhd_params& prm, int flags, fhd_fab out, const fhd_fab& cu, const fhd_fab* cumom,
+              const fhd_fab& prim, const fhd_fab* vel, const fhd_fab& eta, const fhd_fab& kappa, const fhd_fab& zeta,
+              const fhd_stats* st, cudaStream_t s);
+int plot_names(const fhd_params& prm, int flags, std::vector<std::string>& names);
+int plot_write(const fhd_params& prm, const char* dir, const double* host, const std::vector<std::string>& names,
+               double time, int step);
 int chem_launch(const DevParams& P, const ChemParams& C, const fhd_fab& prim, const fhd_fab& source,
                 const fhd_fab* na, const fhd_fab* nb, int mode, double w, cudaStream_t s);
 // running statistics (fhd_stats.cu, exact TU)

@@ -1,0 +1,240 @@
+// fhd_plot.cu — WritePlotFileStag (writePlotFileStag.cpp:7-527): the plotfile
+// MultiFab the reference assembles from the state, the transport coefficients and
+// the running statistics, and its AMReX plotfile on disk.
+//
+// Composition: every plotfile component is a copy of one component of one source
+// MultiFab (MultiFab::Copy for cell fields, ShiftFaceToCC for face fields, which
+// copies face (i,j,k) to cell (i,j,k), ConvertStag.cpp:167-191), in the order and
+// under the names of writePlotFileStag.cpp:111-447.  One gather kernel writes all
+// of them: thread (cell, component) reads its source element through a table of
+// per-component views and writes the packed fab; reads and writes run along x.
+// Not covered: surface coverage (nspec_surfcov = 0) and plot_deltaY_dir.
+//
+// On disk (AMReX's single-level plotfile layout, as WriteSingleLevelPlotfile
+// writes it for one box): <dir>/Header (text: "HyperCLaw-V1.1", component count
+// and names, dimension, time, finest level 0, prob_lo, prob_hi, an empty
+// refinement-ratio line, the domain box, the step, the cell sizes, coordinate
+// system 0, boundary width 0, then the level's box list in physical coordinates
+// and the path "Level_0/Cell"), <dir>/Level_0/Cell_H (the VisMF header of the
+// one-box MultiFab with its per-component minima and maxima) and
+// <dir>/Level_0/Cell_D_00000 (one FAB: a text descriptor line for little-endian
+// IEEE doubles, then the data, components slowest, x fastest).
+#include <cerrno>
+#include <cstdio>
+#include <string>
+#include <sys/stat.h>
+#include <vector>
+
+#include "fhd_launch.cuh"
+
+namespace fhd {
+
+constexpr int kPlotMax = 224;  // components of the largest composition (4 species, every flag)
+
+struct PlotArgs {
+    Arr4<const double> src[kPlotMax];  // per output component, pre-offset to its source component
+    Arr4<double> out;
+    int n[3];
+    int ncomp;
+};
+
+static __global__ void __launch_bounds__(256) k_plot_pack(PlotArgs a) {
+    const int64_t cells = (int64_t)a.n[0] * a.n[1] * a.n[2];
+    const int64_t tot = cells * a.ncomp;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < tot; q += (int64_t)gridDim.x * blockDim.x) {
+        const int c = (int)(q / cells);
+        const int64_t r = q - (int64_t)c * cells;
+        const int i = (int)(r % a.n[0]), j = (int)((r / a.n[0]) % a.n[1]), k = (int)(r / ((int64_t)a.n[0] * a.n[1]));
+        a.out(i, j, k, c) = a.src[c](i, j, k);
+    }
+}
+
+struct PlotComp {
+    fhd_fab fab;
+    int comp;
+    std::string name;
+};
+
+static std::string numbered(const char* base, int i) { return std::string(base) + char('0' + i); }
+
+// the composition of writePlotFileStag.cpp:111-311 with the names of :313-447
+static bool plot_layout(const fhd_params& prm, int flags, const fhd_fab& cu, const fhd_fab* cumom, const fhd_fab& prim,
+                        const fhd_fab* vel, const fhd_fab& eta, const fhd_fab& kappa, const fhd_fab& zeta,
+                        const fhd_stats* st, std::vector<PlotComp>& out) {
+    const int ns = prm.nspecies, nvars = 5 + ns, nprim = 6 + 2 * ns;
+    const bool visc3 = prm.visc_type == 3 || prm.visc_type == -3;
+    const char* xyz[3] = {"x", "y", "z"};
+    auto add = [&](const fhd_fab& f, int c, const std::string& nm) { out.push_back(PlotComp{f, c, nm}); };
+    const fhd_fab none{};
+    auto S = [&](const fhd_fab fhd_stats::*m) -> fhd_fab { return st ? st->*m : none; };
+    // instantaneous
+    add(cu, 0, "rhoInstant");
+    for (int d = 0; d < 3; ++d) add(cu, 1 + d, std::string("j") + xyz[d] + "InstantCC");
+    add(cu, 4, "rhoEInstant");
+    for (int s = 0; s < ns; ++s) add(cu, 5 + s, numbered("rhoYkInstant_", s));
+    for (int d = 0; d < 3; ++d) add(cumom ? cumom[d] : none, 0, std::string("j") + xyz[d] + "InstantFACE");
+    for (int d = 0; d < 3; ++d) add(prim, 1 + d, std::string("u") + xyz[d] + "InstantCC");
+    add(prim, 4, "tInstant");
+    add(prim, 5, "pInstant");
+    for (int s = 0; s < ns; ++s) add(prim, 6 + s, numbered("YkInstant_", s));
+    for (int s = 0; s < ns; ++s) add(prim, 6 + ns + s, numbered("XkInstant_", s));
+    for (int d = 0; d < 3; ++d) add(vel ? vel[d] : none, 0, std::string("u") + xyz[d] + "InstantFACE");
+    add(eta, 0, "eta");
+    add(kappa, 0, "kappa");
+    if (visc3) add(zeta, 0, "zeta");
+    if (flags & FHD_PLOT_MEANS) {
+        const fhd_fab cm = S(&fhd_stats::cuMeans), pm = S(&fhd_stats::primMeans);
+        add(cm, 0, "rhoMean");
+        for (int d = 0; d < 3; ++d) add(cm, 1 + d, std::string("j") + xyz[d] + "MeanCC");
+        add(cm, 4, "rhoEMean");
+        for (int s = 0; s < ns; ++s) add(cm, 5 + s, numbered("rhoYkMean_", s));
+        for (int d = 0; d < 3; ++d) add(st ? st->cumomMeans[d] : none, 0, std::string("j") + xyz[d] + "MeanFACE");
+        for (int d = 0; d < 3; ++d) add(pm, 1 + d, std::string("u") + xyz[d] + "MeanCC");
+        add(pm, 4, "tMean");
+        add(pm, 5, "pMean");
+        for (int s = 0; s < ns; ++s) add(pm, 6 + s, numbered("YkMean_", s));
+        for (int s = 0; s < ns; ++s) add(pm, 6 + ns + s, numbered("XkMean_", s));
+        for (int d = 0; d < 3; ++d) add(st ? st->velMeans[d] : none, 0, std::string("u") + xyz[d] + "MeanFACE");
+        for (int d = 0; d < 3; ++d) add(pm, nprim + d, std::string("u") + xyz[d] + "MeanCOM");
+    }
+    if (flags & FHD_PLOT_VARS) {
+        const fhd_fab cv = S(&fhd_stats::cuVars), pv = S(&fhd_stats::primVars);
+        add(cv, 0, "rhoVar");
+        for (int d = 0; d < 3; ++d) add(cv, 1 + d, std::string("j") + xyz[d] + "VarCC");
+        add(cv, 4, "rhoEVar");
+        for (int s = 0; s < ns; ++s) add(cv, 5 + s, numbered("rhoYkVar_", s));
+        for (int d = 0; d < 3; ++d) add(st ? st->cumomVars[d] : none, 0, std::string("j") + xyz[d] + "VarFACE");
+        for (int d = 0; d < 3; ++d) add(pv, 1 + d, std::string("u") + xyz[d] + "VarCC");
+        add(pv, 4, "TVarDirect");
+        for (int s = 0; s < ns; ++s) add(pv, 6 + s, numbered("YkVar_", s));
+        const char* extra[5] = {"g-g", "g-energy", "rho-energy", "rho-g", "TVar"};
+        for (int e = 0; e < 5; ++e) add(pv, nprim + e, extra[e]);
+        for (int d = 0; d < 3; ++d) add(st ? st->velVars[d] : none, 0, std::string("u") + xyz[d] + "VarFACE");
+    }
+    if (flags & FHD_PLOT_COVARS) {
+        const char* cov[26] = {"rho-jx", "rho-jy", "rho-jz", "jx-jy", "jy-jz", "jx-jz", "rho-rhoE", "rhoE-jx",
+                               "rhoE-jy", "rhoE-jz", "rhoL-rhoH", "rho-vx", "rho-vy", "rho-vz", "vx-vy", "vy-vz",
+                               "vx-vz", "rho-T", "vx-T", "vy-T", "vz-T", "YkL-YkH", "YkL-vx", "YkH-vx",
+                               "rhoYkL-vx", "rhoYkH-vx"};
+        for (int e = 0; e < 26; ++e) add(S(&fhd_stats::coVars), e, cov[e]);
+    }
+    for (int q = 0; q < 2; ++q) {
+        if (!(flags & (q == 0 ? FHD_PLOT_MOM3 : FHD_PLOT_MOM4))) continue;
+        const fhd_fab m = S(q == 0 ? &fhd_stats::mom3 : &fhd_stats::mom4);
+        const std::string sfx = q == 0 ? "mom3" : "mom4";
+        add(m, 0, "rho" + sfx);
+        for (int d = 0; d < 3; ++d) add(m, 1 + d, std::string("vel") + xyz[d] + sfx);
+        add(m, 4, "rhoE" + sfx);
+        for (int s = 0; s < ns; ++s) add(m, 5 + s, numbered(("Yk" + sfx + "_").c_str(), s));
+        add(m, 5 + ns, "T" + sfx);
+    }
+    return (int)out.size() <= kPlotMax;
+}
+
+// a source fab must exist, cover the domain's valid region and hold the component
+static bool plot_src_ok(const fhd_params& prm, const PlotComp& pc) {
+    const fhd_fab& f = pc.fab;
+    if (!f.data || f.dtype != FHD_F64 || pc.comp >= f.ncomp) return false;
+    for (int d = 0; d < 3; ++d)
+        if (f.lo[d] > 0 || f.hi[d] < prm.n_cells[d] - 1) return false;
+    return true;
+}
+
+int plot_pack(const fhd_params& prm, int flags, fhd_fab out, const fhd_fab& cu, const fhd_fab* cumom,
+              const fhd_fab& prim, const fhd_fab* vel, const fhd_fab& eta, const fhd_fab& kappa, const fhd_fab& zeta,
+              const fhd_stats* st, cudaStream_t s) {
+    std::vector<PlotComp> L;
+    if (!plot_layout(prm, flags, cu, cumom, prim, vel, eta, kappa, zeta, st, L)) return FHD_ERR_UNSUPPORTED;
+    if (!out.data || out.dtype != FHD_F64 || out.ncomp < (int)L.size()) return FHD_ERR_BAD_ARG;
+    for (int d = 0; d < 3; ++d)
+        if (out.lo[d] > 0 || out.hi[d] < prm.n_cells[d] - 1 || out.nodal[d]) return FHD_ERR_BAD_ARG;
+    for (const PlotComp& pc : L)
+        if (!plot_src_ok(prm, pc)) return FHD_ERR_BAD_ARG;
+    PlotArgs a;
+    std::memset(&a, 0, sizeof(a));
+    for (size_t c = 0; c < L.size(); ++c) a.src[c] = view<const double>(L[c].fab, L[c].comp);
+    a.out = view<double>(out);
+    for (int d = 0; d < 3; ++d) a.n[d] = prm.n_cells[d];
+    a.ncomp = (int)L.size();
+    const int64_t tot = (int64_t)a.n[0] * a.n[1] * a.n[2] * a.ncomp;
+    k_plot_pack<<<grid_for(tot, 256), 256, 0, s>>>(a);
+    return cuda_rc(cudaGetLastError());
+}
+
+int plot_names(const fhd_params& prm, int flags, std::vector<std::string>& names) {
+    std::vector<PlotComp> L;
+    const fhd_fab none{};
+    fhd_fab three[3] = {none, none, none};
+    fhd_stats st;
+    std::memset(&st, 0, sizeof(st));
+    if (!plot_layout(prm, flags, none, three, none, three, none, none, none, &st, L)) return FHD_ERR_UNSUPPORTED;
+    names.clear();
+    for (const PlotComp& pc : L) names.push_back(pc.name);
+    return FHD_OK;
+}
+
+static bool make_dir(const std::string& p) { return mkdir(p.c_str(), 0755) == 0 || errno == EEXIST; }
+
+// AMReX's text form of a cell box: ((lo) (hi) (type))
+static std::string box_text(const int n[3]) {
+    char b[160];
+    std::snprintf(b, sizeof(b), "((0,0,0) (%d,%d,%d) (0,0,0))", n[0] - 1, n[1] - 1, n[2] - 1);
+    return b;
+}
+
+// Writes the packed host data (ncomp components of the valid box, x fastest,
+// components slowest) as a single-level, single-box AMReX plotfile.
+int plot_write(const fhd_params& prm, const char* dir, const double* host, const std::vector<std::string>& names,
+               double time, int step) {
+    const int nc = (int)names.size();
+    const int* n = prm.n_cells;
+    const int64_t cells = (int64_t)n[0] * n[1] * n[2];
+    const std::string root(dir);
+    if (!make_dir(root) || !make_dir(root + "/Level_0")) return FHD_ERR_BAD_ARG;
+    double dx[3];
+    for (int d = 0; d < 3; ++d) dx[d] = (prm.prob_hi[d] - prm.prob_lo[d]) / n[d];
+    FILE* h = std::fopen((root + "/Header").c_str(), "w");
+    if (!h) return FHD_ERR_BAD_ARG;
+    std::fprintf(h, "HyperCLaw-V1.1\n%d\n", nc);
+    for (const std::string& s : names) std::fprintf(h, "%s\n", s.c_str());
+    std::fprintf(h, "3\n%.17g\n0\n", time);
+    std::fprintf(h, "%.17g %.17g %.17g \n", prm.prob_lo[0], prm.prob_lo[1], prm.prob_lo[2]);
+    std::fprintf(h, "%.17g %.17g %.17g \n", prm.prob_hi[0], prm.prob_hi[1], prm.prob_hi[2]);
+    std::fprintf(h, "\n%s \n%d \n", box_text(n).c_str(), step);
+    std::fprintf(h, "%.17g %.17g %.17g \n", dx[0], dx[1], dx[2]);
+    std::fprintf(h, "0\n0\n");
+    std::fprintf(h, "0 1 %.17g\n%d\n", time, step);
+    for (int d = 0; d < 3; ++d) std::fprintf(h, "%.17g %.17g\n", prm.prob_lo[d], prm.prob_hi[d]);
+    std::fprintf(h, "Level_0/Cell\n");
+    const bool hok = std::fclose(h) == 0;
+    // Cell_D_00000: one FAB
+    FILE* f = std::fopen((root + "/Level_0/Cell_D_00000").c_str(), "wb");
+    if (!f) return FHD_ERR_BAD_ARG;
+    std::fprintf(f, "FAB ((8, (64 11 52 0 1 12 0 1023)),(8, (1 2 3 4 5 6 7 8)))%s %d\n", box_text(n).c_str(), nc);
+    const size_t cnt = (size_t)cells * nc;
+    const bool dok = std::fwrite(host, sizeof(double), cnt, f) == cnt;
+    const bool fok = std::fclose(f) == 0;
+    // Cell_H: VisMF header of the one-box MultiFab, with per-component min / max
+    FILE* v = std::fopen((root + "/Level_0/Cell_H").c_str(), "w");
+    if (!v) return FHD_ERR_BAD_ARG;
+    std::fprintf(v, "1\n1\n%d\n0\n(1 0\n%s\n)\n1\nFabOnDisk: Cell_D_00000 0\n\n1,%d\n", nc, box_text(n).c_str(), nc);
+    std::vector<double> mn(nc), mx(nc);
+    for (int c = 0; c < nc; ++c) {
+        const double* p = host + (size_t)c * cells;
+        double a = p[0], b = p[0];
+        for (int64_t q = 1; q < cells; ++q) {
+            a = p[q] < a ? p[q] : a;
+            b = p[q] > b ? p[q] : b;
+        }
+        mn[c] = a;
+        mx[c] = b;
+    }
+    for (int c = 0; c < nc; ++c) std::fprintf(v, "%.17g,", mn[c]);
+    std::fprintf(v, "\n\n1,%d\n", nc);
+    for (int c = 0; c < nc; ++c) std::fprintf(v, "%.17g,", mx[c]);
+    std::fprintf(v, "\n");
+    const bool vok = std::fclose(v) == 0;
+    return (hok && dok && fok && vok) ? FHD_OK : FHD_ERR_BAD_ARG;
+}
+
+}  // namespace fhd

@@ -338,6 +338,34 @@ typedef struct {
     fhd_fab velMeans[3], velVars[3], cumomMeans[3], cumomVars[3];
 } fhd_stats;
 
+/* ---- plotfiles --------------------------------------------------------------------
+ * WritePlotFileStag (writePlotFileStag.cpp:7-527, declared
+ * compressible_functions_stag.H): the cell-centred plotfile MultiFab the
+ * reference assembles (instantaneous cu, face momenta shifted to cells, prim
+ * components 1.., face velocities shifted to cells, eta, kappa, zeta when
+ * |visc_type| == 3; then, by flag, the means, variances, covariances and third /
+ * fourth moments of fhd_stats), under the reference's variable names, and its
+ * single-level AMReX plotfile <plot_base_name><step, 9 digits>/ (Header,
+ * Level_0/Cell_H, Level_0/Cell_D_00000).  Surface coverage and plot_deltaY_dir
+ * are not covered.  Source fabs must be device-accessible (device, managed or
+ * pinned host memory) and cover the valid region. */
+enum { FHD_PLOT_MEANS = 1, FHD_PLOT_VARS = 2, FHD_PLOT_COVARS = 4, FHD_PLOT_MOM3 = 8, FHD_PLOT_MOM4 = 16 };
+/* number of plotfile components for `flags` (negative: -error code); no device */
+int fhd_plotfile_ncomp(const fhd_params* params, int flags);
+/* name of component `comp` into buf (NUL-terminated, at most buflen bytes) */
+int fhd_plotfile_varname(const fhd_params* params, int flags, int comp, char* buf, int buflen);
+/* writes the plotfile directory `dir` from packed host data (fhd_plotfile_ncomp
+ * components of the valid box, x fastest, components slowest); no device */
+int fhd_plotfile_write_host(const fhd_params* params, const char* dir, const double* data, int flags,
+                            double time, int step);
+/* the plotfile MultiFab into `out` (cell-centred, >= fhd_plotfile_ncomp comps) */
+int fhd_plotfile_pack(fhd_ctx* ctx, int flags, fhd_fab out, fhd_fab cu, const fhd_fab cumom[3], fhd_fab prim,
+                      const fhd_fab vel[3], fhd_fab eta, fhd_fab kappa, fhd_fab zeta, const fhd_stats* stats);
+/* pack, copy to the host and write the plotfile directory (blocks on the stream) */
+int fhd_write_plotfile_stag(fhd_ctx* ctx, const char* plot_base_name, int step, double time, int flags, fhd_fab cu,
+                            const fhd_fab cumom[3], fhd_fab prim, const fhd_fab vel[3], fhd_fab eta, fhd_fab kappa,
+                            fhd_fab zeta, const fhd_stats* stats);
+
 /* flags of fhd_stats_stag (the reference's plot_means, plot_vars/plot_covars,
  * plot_mom3, plot_mom4 inputs) */
 enum { FHD_STATS_MEANS = 1, FHD_STATS_VARS = 2, FHD_STATS_MOM3 = 4, FHD_STATS_MOM4 = 8 };
