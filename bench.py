@@ -489,6 +489,80 @@ def run_stats(args):
                       "clocks": clk}), flush=True)
 
 
+def run_plot(args):
+    """WritePlotFileStag: the GPU composition of the plotfile MultiFab (all
+    statistics flags) timed over --steps launches with CUDA events (HBM roofline:
+    every component read once and written once), and one plotfile written to disk
+    at 64^3 (wall clock, pack + copy + file writes)."""
+    import shutil
+    import tempfile
+    import torch
+    from fhdex_b200.context import Context
+    from fhdex_b200.params import stable_dt
+    from fhdex_b200.plotfile import COVARS, MEANS, MOM3, MOM4, VARS, pack, plotfile_names, write_plotfile_stag
+    from fhdex_b200.state import StagState
+    from fhdex_b200.stats import StatsState
+    flags = MEANS | VARS | COVARS | MOM3 | MOM4
+
+    def prepared(p):
+        ctx = Context(p, 0)
+        st = StagState(p, "cuda:0", aux=True)
+        ctx.init_state(st)
+        ctx.rk3_step(st, stable_dt(p), 0, aux=True)
+        stats = StatsState(p, "cuda:0")
+        ctx.stats_stag(st, stats, 1, 15)
+        return ctx, st, stats
+
+    torch.cuda.set_device(0)
+    p = make_params(args)
+    ctx, st, stats = prepared(p)
+    out = pack(ctx, st, stats, flags)
+    for _ in range(args.warmup):
+        pack(ctx, st, stats, flags, out=out)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        pack(ctx, st, stats, flags, out=out)
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    assert ctx.status() == 0
+    ncomp = out.ncomp
+    cells = p.n_cells[0] * p.n_cells[1] * p.n_cells[2]
+    alg = 2 * 8 * ncomp * cells
+    peak, peak_kind = measured_peak()
+    achieved = alg / (ms / 1e3) / 1e9
+    ctx.close()
+    del st, stats, out
+    torch.cuda.empty_cache()
+    # one plotfile on disk at 64^3
+    q = p.replace(n_cells=(64, 64, 64), prob_hi=tuple(p.dx[0] * 64 for _ in range(3)))
+    ctx, st, stats = prepared(q)
+    tmp = tempfile.mkdtemp(prefix="fhdplt")
+    t = time.perf_counter()
+    path = write_plotfile_stag(ctx, os.path.join(tmp, "plt"), 1, 0.0, st, stats, flags)
+    wall = time.perf_counter() - t
+    nbytes = sum(os.path.getsize(os.path.join(dp, f)) for dp, _, fs in os.walk(path) for f in fs)
+    shutil.rmtree(tmp, ignore_errors=True)
+    ctx.close()
+    print(json.dumps({"mode": "plot", "metric": "plotfile components packed/s (cells x components)",
+                      "unit": "cell-components/s", "value": cells * ncomp / (ms / 1e3), "ms_per_pack": ms,
+                      "steps": args.steps, "warmup": args.warmup, "dtype": "f64",
+                      "config": {"workload": f"WritePlotFileStag composition, all statistics flags, "
+                                             f"{p.n_cells[0]}^3, {p.nspecies} species, {ncomp} components"},
+                      "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                                   "frac": achieved / peak, "peak_kind": peak_kind,
+                                   "algorithmic_bytes_per_launch": alg, "kernel": "k_plot_pack"},
+                      "write_64": {"seconds": wall, "bytes": nbytes, "names": len(plotfile_names(q, flags)),
+                                   "path": "fhd_write_plotfile_stag (pack + D2H + Header/Cell_H/Cell_D files)"},
+                      "clocks": clk}), flush=True)
+
+
 def run_sf(args):
     """Static structure factor (fhd_sf_fort_structure): rho, rhoE, T and jx of the
     stepped state, all 10 pairs, --steps samples timed with CUDA events."""
@@ -623,7 +697,7 @@ def run_serve(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--mode", default="step", choices=["step", "ensemble", "serve", "stats", "sf"])
+    ap.add_argument("--mode", default="step", choices=["step", "ensemble", "serve", "stats", "sf", "plot"])
     ap.add_argument("--members", type=int, default=512)
     ap.add_argument("--requests", type=int, default=48)
     ap.add_argument("--rate", type=float, default=50.0)
@@ -659,6 +733,8 @@ def main():
         run_stats(args)
     elif args.mode == "sf":
         run_sf(args)
+    elif args.mode == "plot":
+        run_plot(args)
     else:
         run_ours(args)
 

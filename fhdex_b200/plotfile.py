@@ -54,12 +54,14 @@ def _args(st, stats, flags):
     return (st.cu.fab(), st.mom_fabs(), st.prim.fab(), st.vel_fabs(), st.eta.fab(), st.kappa.fab(), zeta), sp
 
 
-def pack(ctx, st, stats=None, flags: int = 0) -> MultiFab:
-    """The plotfile MultiFab (cell-centred, no ghosts) on the state's device.  ``st``
-    needs its transport coefficients (a StagState with aux=True)."""
+def pack(ctx, st, stats=None, flags: int = 0, out: MultiFab | None = None) -> MultiFab:
+    """The plotfile MultiFab (cell-centred, no ghosts) on the state's device, into
+    ``out`` when given.  ``st`` needs its transport coefficients (a StagState with
+    aux=True)."""
     ctx._stream()
-    n = len(plotfile_names(ctx.p, flags))
-    out = MultiFab(st.cu.n_cells, CELL, n, 0, device=st.cu.arr.device)
+    if out is None:
+        n = len(plotfile_names(ctx.p, flags))
+        out = MultiFab(st.cu.n_cells, CELL, n, 0, device=st.cu.arr.device)
     a, sp = _args(st, stats, flags)
     check(ctx.lib.fhd_plotfile_pack(ctx._h, flags, out.fab(), *a, sp), "fhd_plotfile_pack")
     return out
