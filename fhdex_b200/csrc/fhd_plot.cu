@@ -6,8 +6,9 @@
 // MultiFab (MultiFab::Copy for cell fields, ShiftFaceToCC for face fields, which
 // copies face (i,j,k) to cell (i,j,k), ConvertStag.cpp:167-191), in the order and
 // under the names of writePlotFileStag.cpp:111-447.  One gather kernel writes all
-// of them: thread (cell, component) reads its source element through a table of
-// per-component views and writes the packed fab; reads and writes run along x.
+// of them through a table of per-component source views: block (z-plane,
+// component) copies the plane's rows, threads along x, so reads and writes are
+// contiguous and the indexing is 32-bit with no divisions.
 // Not covered: surface coverage (nspec_surfcov = 0) and plot_deltaY_dir.
 //
 // On disk (AMReX's single-level plotfile layout, as WriteSingleLevelPlotfile
@@ -38,15 +39,16 @@ struct PlotArgs {
     int ncomp;
 };
 
+// blockIdx.y: output component; blockIdx.x: z-planes (grid-stride)
 static __global__ void __launch_bounds__(256) k_plot_pack(PlotArgs a) {
-    const int64_t cells = (int64_t)a.n[0] * a.n[1] * a.n[2];
-    const int64_t tot = cells * a.ncomp;
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < tot; q += (int64_t)gridDim.x * blockDim.x) {
-        const int c = (int)(q / cells);
-        const int64_t r = q - (int64_t)c * cells;
-        const int i = (int)(r % a.n[0]), j = (int)((r / a.n[0]) % a.n[1]), k = (int)(r / ((int64_t)a.n[0] * a.n[1]));
-        a.out(i, j, k, c) = a.src[c](i, j, k);
-    }
+    const int c = blockIdx.y;
+    const Arr4<const double> s = a.src[c];
+    for (int k = blockIdx.x; k < a.n[2]; k += gridDim.x)
+        for (int j = 0; j < a.n[1]; ++j) {
+            const double* __restrict__ sp = &s(0, j, k);
+            double* __restrict__ dp = &a.out(0, j, k, c);
+            for (int i = threadIdx.x; i < a.n[0]; i += blockDim.x) dp[i] = sp[i];
+        }
 }
 
 struct PlotComp {
@@ -61,7 +63,7 @@ static std::string numbered(const char* base, int i) { return std::string(base) 
 static bool plot_layout(const fhd_params& prm, int flags, const fhd_fab& cu, const fhd_fab* cumom, const fhd_fab& prim,
                         const fhd_fab* vel, const fhd_fab& eta, const fhd_fab& kappa, const fhd_fab& zeta,
                         const fhd_stats* st, std::vector<PlotComp>& out) {
-    const int ns = prm.nspecies, nvars = 5 + ns, nprim = 6 + 2 * ns;
+    const int ns = prm.nspecies, nprim = 6 + 2 * ns;
     const bool visc3 = prm.visc_type == 3 || prm.visc_type == -3;
     const char* xyz[3] = {"x", "y", "z"};
     auto add = [&](const fhd_fab& f, int c, const std::string& nm) { out.push_back(PlotComp{f, c, nm}); };
@@ -156,8 +158,9 @@ int plot_pack(const fhd_params& prm, int flags, fhd_fab out, const fhd_fab& cu, 
     a.out = view<double>(out);
     for (int d = 0; d < 3; ++d) a.n[d] = prm.n_cells[d];
     a.ncomp = (int)L.size();
-    const int64_t tot = (int64_t)a.n[0] * a.n[1] * a.n[2] * a.ncomp;
-    k_plot_pack<<<grid_for(tot, 256), 256, 0, s>>>(a);
+    // every block of the (plane, component) grid copies at least a whole plane
+    const dim3 grid((unsigned)a.n[2], (unsigned)a.ncomp);
+    k_plot_pack<<<grid, 256, 0, s>>>(a);
     return cuda_rc(cudaGetLastError());
 }
 
