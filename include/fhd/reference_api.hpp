@@ -19,6 +19,7 @@
 //   MultiFabFillRandomUniform  src_rng/rng_functions.H:13-22
 //   compute_compressible_chemistry_source_CLE
 //                              src_chemistry/chemistry_functions.H:20-21
+//   WritePlotFileStag          src_compressible_stag/compressible_functions_stag.H:15-39
 //
 // As in the reference, physics parameters are process globals in namespaces
 // `common`, `compressible` and `chemistry` (src_common/common_namespace.H,
@@ -89,6 +90,13 @@ inline Real zeta_ratio = -1.0;
 namespace common {
 // <= 0: Runiv / k_B, as InitializeCommonNamespace derives it (common_functions.cpp:775)
 inline fhd::amrex_compat::Real avogadro = 0.0;
+// plotfile inputs (common_functions.cpp:390, 614-618)
+inline std::string plot_base_name = "plt";
+inline int plot_means = 0;
+inline int plot_vars = 0;
+inline int plot_covars = 0;
+inline int plot_mom3 = 0;
+inline int plot_mom4 = 0;
 }  // namespace common
 
 namespace chemistry {
@@ -450,6 +458,55 @@ inline void MultiFabFillRandomUniform(fhd::amrex_compat::MultiFab& mf, const int
     const uint64_t id = ++runtime().fill_calls;
     check(fhd_fill_random_uniform(context(), mf.fab(), scomp, ncomp, overridesync ? 1 : 0, fillboundary ? 1 : 0, id),
           "MultiFabFillRandomUniform");
+}
+
+// WritePlotFileStag (writePlotFileStag.cpp:7-527): the plotfile
+// <plot_base_name><step, 9 digits>/ with the common::plot_means / plot_vars /
+// plot_covars / plot_mom3 / plot_mom4 selections.  The surface-coverage
+// MultiFabs are accepted and ignored (no surface chemistry on this path).
+inline void WritePlotFileStag(int step, const fhd::amrex_compat::Real time, const fhd::amrex_compat::Geometry& /*geom*/,
+                              const fhd::amrex_compat::MultiFab& cu, const fhd::amrex_compat::MultiFab& cuMeans,
+                              const fhd::amrex_compat::MultiFab& cuVars,
+                              const std::array<fhd::amrex_compat::MultiFab, 3>& cumom,
+                              const std::array<fhd::amrex_compat::MultiFab, 3>& cumomMeans,
+                              const std::array<fhd::amrex_compat::MultiFab, 3>& cumomVars,
+                              const fhd::amrex_compat::MultiFab& prim, const fhd::amrex_compat::MultiFab& primMeans,
+                              const fhd::amrex_compat::MultiFab& primVars,
+                              const std::array<fhd::amrex_compat::MultiFab, 3>& vel,
+                              const std::array<fhd::amrex_compat::MultiFab, 3>& velMeans,
+                              const std::array<fhd::amrex_compat::MultiFab, 3>& velVars,
+                              const fhd::amrex_compat::MultiFab& coVars, const fhd::amrex_compat::MultiFab& mom3,
+                              const fhd::amrex_compat::MultiFab& mom4, const fhd::amrex_compat::MultiFab& /*surfcov*/,
+                              const fhd::amrex_compat::MultiFab& /*surfcovMeans*/,
+                              const fhd::amrex_compat::MultiFab& /*surfcovVars*/,
+                              const fhd::amrex_compat::MultiFab& /*surfcovcoVars*/,
+                              const fhd::amrex_compat::MultiFab& eta, const fhd::amrex_compat::MultiFab& kappa,
+                              const fhd::amrex_compat::MultiFab& zeta) {
+    using namespace fhd::ref;
+    const int flags = (common::plot_means == 1 ? FHD_PLOT_MEANS : 0) | (common::plot_vars == 1 ? FHD_PLOT_VARS : 0) |
+                      (common::plot_covars == 1 ? FHD_PLOT_COVARS : 0) | (common::plot_mom3 ? FHD_PLOT_MOM3 : 0) |
+                      (common::plot_mom4 ? FHD_PLOT_MOM4 : 0);
+    fhd_stats st;
+    std::memset(&st, 0, sizeof(st));
+    st.cuMeans = cuMeans.fab();
+    st.cuVars = cuVars.fab();
+    st.primMeans = primMeans.fab();
+    st.primVars = primVars.fab();
+    st.coVars = coVars.fab();
+    st.mom3 = mom3.fab();
+    st.mom4 = mom4.fab();
+    for (int d = 0; d < 3; ++d) {
+        st.velMeans[d] = velMeans[d].fab();
+        st.velVars[d] = velVars[d].fab();
+        st.cumomMeans[d] = cumomMeans[d].fab();
+        st.cumomVars[d] = cumomVars[d].fab();
+    }
+    fhd_fab mom[3], vl[3];
+    fabs_of(cumom, mom);
+    fabs_of(vel, vl);
+    check(fhd_write_plotfile_stag(context(), common::plot_base_name.c_str(), step, time, flags, cu.fab(), mom,
+                                  prim.fab(), vl, eta.fab(), kappa.fab(), zeta.fab(), &st),
+          "WritePlotFileStag");
 }
 
 // MultiFabFillRandom (MultiFabFillRandom.cpp:5-31): N(0, variance) in one

@@ -10,6 +10,9 @@
 //       run nsteps RK3 steps (steps 0..nsteps-1) and write cu, cumom[0..2],
 //       prim, vel[0..2] (whole buffers, ghosts included) to out.bin; no2: the
 //       2 NO2 <-> N2O4 gas with the chemistry source (chemistry:: globals)
+//   reference_driver plot <n> <nsteps> <seed> <dt> <plot_base_name>
+//       run nsteps RK3 steps on device MultiFabs and WritePlotFileStag (step
+//       nsteps, time nsteps*dt, no statistics)
 //   reference_driver massfrac <n>
 //       start from a state with a zero mass fraction: calculateTransportCoeffs
 //       must report it through the abort handler (exit code 3)
@@ -223,6 +226,20 @@ static int cmd_run(const std::string& arena, int n, int nsteps, int seed, double
     return 0;
 }
 
+static int cmd_plot(int n, int nsteps, int seed, double dt, const char* base) {
+    set_argon(n, seed);
+    State s(n, Arena::Device, true);
+    s.init();
+    step_all(s, dt, nsteps);
+    MultiFab none;
+    std::array<MultiFab, 3> none3;
+    common::plot_base_name = base;
+    WritePlotFileStag(nsteps, nsteps * dt, s.geom, s.cu, none, none, s.cumom, none3, none3, s.prim, none, none, s.vel,
+                      none3, none3, none, none, none, none, none, none, none, s.eta, s.kappa, s.zeta);
+    fhd::ref::finalize();
+    return 0;
+}
+
 static int cmd_massfrac(int n) {
     set_argon(n, 1);
     common::rhobar[0] = 1.0;  // species 2 absent: Y_2 = 0
@@ -253,6 +270,9 @@ int main(int argc, char** argv) {
             return cmd_run(argv[2], std::atoi(argv[3]), std::atoi(argv[4]), std::atoi(argv[5]),
                            std::strtod(argv[6], nullptr), argv[7], argc == 9 ? argv[8] : "argon");
         if (cmd == "massfrac") return cmd_massfrac(std::atoi(argv[2]));
+        if (cmd == "plot" && argc == 7)
+            return cmd_plot(std::atoi(argv[2]), std::atoi(argv[3]), std::atoi(argv[4]), std::strtod(argv[5], nullptr),
+                            argv[6]);
     } catch (const std::exception& e) {
         std::fprintf(stderr, "error: %s\n", e.what());
         return 4;

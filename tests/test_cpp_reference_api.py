@@ -111,3 +111,29 @@ def test_reference_driver_reports_massfrac_through_abort_handler(driver):
     r = subprocess.run([driver, "massfrac", "8"], capture_output=True, text=True, timeout=120)
     assert r.returncode == 3, (r.returncode, r.stdout, r.stderr)
     assert "calculateTransportCoeffs" in r.stdout and "mass fraction" in r.stdout.lower(), r.stdout
+
+
+@pytest.mark.gpu
+def test_reference_driver_plotfile_equals_c_abi_plotfile(driver, tmp_path):
+    """WritePlotFileStag through the reference-named layer writes the same files,
+    byte for byte, as fhd_write_plotfile_stag on the same steps."""
+    from fhdex_b200.context import Context
+    from fhdex_b200.plotfile import write_plotfile_stag
+    n, nsteps, seed = 8, 2, 5
+    p = argon(n, dx=8e-6, seed=seed)
+    dt = stable_dt(p)
+    base = str(tmp_path / "ref_plt")
+    r = subprocess.run([driver, "plot", str(n), str(nsteps), str(seed), repr(dt), base],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    ctx = Context(p)
+    st = StagState(p, "cuda")
+    ctx.init_state(st)
+    for step in range(nsteps):
+        ctx.rk3_step(st, dt, step, aux=True)
+    ours = write_plotfile_stag(ctx, str(tmp_path / "abi_plt"), nsteps, nsteps * dt, st)
+    theirs = base + f"{nsteps:09d}"
+    for rel in ("Header", "Level_0/Cell_H", "Level_0/Cell_D_00000"):
+        a = open(os.path.join(ours, rel), "rb").read()
+        b = open(os.path.join(theirs, rel), "rb").read()
+        assert a == b, rel
