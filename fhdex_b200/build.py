@@ -23,7 +23,7 @@ BASE = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contr
                "-Xptxas", "-v", f"-I{CSRC}", f"-I{os.path.join(ROOT, 'include')}"]
 SPECIES = (1, 2, 3, 4)
 
-HEADERS = ["fhd_div.h", "fhd_device.cuh", "philox.cuh", "fhd_flux.cuh", "fhd_kernels.cuh", "fhd_launch.cuh", "fhd_host.h", "fhd_chem.cuh"]
+HEADERS = ["fhd_div.h", "fhd_device.cuh", "philox.cuh", "fhd_flux.cuh", "fhd_kernels.cuh", "fhd_launch.cuh", "fhd_host.h", "fhd_chem.cuh", "fhd_vismf.h"]
 
 
 def _units():
@@ -39,6 +39,7 @@ def _units():
     u.append(("sf", "fhd_sf.cu", ["-fmad=false"]))
     u.append(("chem", "fhd_chem.cu", ["-fmad=false"]))
     u.append(("plot", "fhd_plot.cu", ["-fmad=false"]))
+    u.append(("chk", "fhd_chk.cu", []))
     return u
 
 

@@ -138,6 +138,9 @@ def _declare(lib):
         "fhd_plotfile_ncomp": (i, [P(FhdParams), i]),
         "fhd_plotfile_varname": (i, [P(FhdParams), i, i, C.c_char_p, i]),
         "fhd_plotfile_write_host": (i, [P(FhdParams), C.c_char_p, P(d), i, d, i]),
+        "fhd_write_checkpoint": (i, [P(FhdParams), C.c_char_p, i, d, i, fab, pfab, fab, pfab, P(FhdStats)]),
+        "fhd_read_checkpoint": (i, [P(FhdParams), C.c_char_p, i, P(i), P(d), P(i), fab, pfab, fab, pfab,
+                                    P(FhdStats)]),
         "fhd_plotfile_pack": (i, [vp, i, fab, fab, pfab, fab, pfab, fab, fab, fab, P(FhdStats)]),
         "fhd_write_plotfile_stag": (i, [vp, C.c_char_p, i, d, i, fab, pfab, fab, pfab, fab, fab, fab,
                                         P(FhdStats)]),

@@ -1,0 +1,194 @@
+// fhd_chk.cu — WriteCheckPoint / ReadCheckPoint (Checkpoint.cpp:28-257, 259-575)
+// for one periodic box: chk<step, 9 digits>/Header (title line, step, time,
+// statsCount, the BoxArray) and Level_0/<name>_H, <name>_D_00000 for every
+// MultiFab the reference saves, under its names (cu, cuMeans, cuVars, prim,
+// primMeans, primVars, velx..z, velmeanx..z, velvarx..z, cumomx..z,
+// cumommeanx..z, cumomvarx..z, coVars, mom3, mom4), whole fabs with their ghost
+// cells as VisMF writes them.
+//
+// The reference also saves its C++ random engines' states (rng files); the noise
+// here is a function of (seed, step) alone, so the restart step is all the
+// generator needs.  Host code: device fabs are copied with cudaMemcpy after a
+// device synchronisation, host fabs with memcpy (no GPU needed for those).
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/fhd_capi.h"
+#include "fhd_vismf.h"
+
+namespace fhd {
+
+namespace {
+
+bool on_device(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+int64_t fab_elems(const fhd_fab& f) {
+    int64_t n = f.ncomp;
+    for (int d = 0; d < 3; ++d) n *= (int64_t)(f.hi[d] - f.lo[d] + 1);
+    return n;
+}
+
+bool copy_bytes(void* dst, const void* src, size_t bytes, bool dev) {
+    if (!dev) {
+        std::memcpy(dst, src, bytes);
+        return true;
+    }
+    if (cudaMemcpy(dst, src, bytes, cudaMemcpyDefault) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return true;
+}
+
+struct Entry {
+    std::string name;
+    fhd_fab fab;
+};
+
+// the MultiFabs of Checkpoint.cpp:172-239 that the caller supplied
+std::vector<Entry> entries(fhd_fab cu, const fhd_fab* cumom, fhd_fab prim, const fhd_fab* vel, const fhd_stats* st) {
+    const char* xyz = "xyz";
+    std::vector<Entry> e;
+    auto add = [&](const std::string& n, const fhd_fab& f) {
+        if (f.data) e.push_back(Entry{n, f});
+    };
+    add("cu", cu);
+    if (st) {
+        add("cuMeans", st->cuMeans);
+        add("cuVars", st->cuVars);
+    }
+    add("prim", prim);
+    if (st) {
+        add("primMeans", st->primMeans);
+        add("primVars", st->primVars);
+    }
+    for (int d = 0; d < 3; ++d) add(std::string("vel") + xyz[d], vel[d]);
+    if (st) {
+        for (int d = 0; d < 3; ++d) add(std::string("velmean") + xyz[d], st->velMeans[d]);
+        for (int d = 0; d < 3; ++d) add(std::string("velvar") + xyz[d], st->velVars[d]);
+    }
+    for (int d = 0; d < 3; ++d) add(std::string("cumom") + xyz[d], cumom[d]);
+    if (st) {
+        for (int d = 0; d < 3; ++d) add(std::string("cumommean") + xyz[d], st->cumomMeans[d]);
+        for (int d = 0; d < 3; ++d) add(std::string("cumomvar") + xyz[d], st->cumomVars[d]);
+        add("coVars", st->coVars);
+        add("mom3", st->mom3);
+        add("mom4", st->mom4);
+    }
+    return e;
+}
+
+// a one-box fab of the domain: uniform ghost width, valid box = the domain (+ nodal)
+bool geometry(const fhd_params& p, const fhd_fab& f, int vlo[3], int vhi[3], int type[3], int* ng) {
+    if (f.dtype != FHD_F64 || f.ncomp < 1) return false;
+    *ng = -f.lo[0];
+    for (int d = 0; d < 3; ++d) {
+        type[d] = f.nodal[d] ? 1 : 0;
+        vlo[d] = 0;
+        vhi[d] = p.n_cells[d] - 1 + type[d];
+        if (f.lo[d] != -*ng || f.hi[d] != vhi[d] + *ng) return false;
+    }
+    return *ng >= 0;
+}
+
+std::string chk_dir(const char* base, int step) {
+    char num[32];
+    std::snprintf(num, sizeof(num), "%09d", step);
+    return std::string(base) + num;
+}
+
+}  // namespace
+}  // namespace fhd
+
+using namespace fhd;
+
+extern "C" int fhd_write_checkpoint(const fhd_params* params, const char* chk_base, int step, double time,
+                                    int stats_count, fhd_fab cu, const fhd_fab cumom[3], fhd_fab prim,
+                                    const fhd_fab vel[3], const fhd_stats* stats) {
+    if (!params || !chk_base || !cumom || !vel || step < 0 || !cu.data || !prim.data) return FHD_ERR_BAD_ARG;
+    const std::vector<Entry> E = entries(cu, cumom, prim, vel, stats);
+    bool dev = false;
+    for (const Entry& e : E) {
+        int vlo[3], vhi[3], type[3], ng;
+        if (!geometry(*params, e.fab, vlo, vhi, type, &ng)) return FHD_ERR_BAD_ARG;
+        dev = dev || on_device(e.fab.data);
+    }
+    if (dev && cudaDeviceSynchronize() != cudaSuccess) {
+        cudaGetLastError();
+        return FHD_ERR_CUDA;
+    }
+    const std::string dir = chk_dir(chk_base, step);
+    if (!vismf_mkdir(dir) || !vismf_mkdir(dir + "/Level_0")) return FHD_ERR_BAD_ARG;
+    FILE* h = std::fopen((dir + "/Header").c_str(), "w");
+    if (!h) return FHD_ERR_BAD_ARG;
+    const int lo[3] = {0, 0, 0}, hi[3] = {params->n_cells[0] - 1, params->n_cells[1] - 1, params->n_cells[2] - 1},
+              cc[3] = {0, 0, 0};
+    std::fprintf(h, "Checkpoint file for FHDeX/compressStag\n%d\n%.17g\n%d\n(1 0\n%s\n)\n\n", step, time, stats_count,
+                 vismf_box(lo, hi, cc).c_str());
+    if (std::fclose(h) != 0) return FHD_ERR_BAD_ARG;
+    std::vector<double> buf;
+    for (const Entry& e : E) {
+        int vlo[3], vhi[3], type[3], ng;
+        geometry(*params, e.fab, vlo, vhi, type, &ng);
+        buf.resize((size_t)fab_elems(e.fab));
+        if (!copy_bytes(buf.data(), e.fab.data, buf.size() * sizeof(double), on_device(e.fab.data)))
+            return FHD_ERR_CUDA;
+        if (!vismf_write(dir + "/Level_0", e.name, buf.data(), vlo, vhi, type, e.fab.ncomp, ng)) return FHD_ERR_BAD_ARG;
+    }
+    return FHD_OK;
+}
+
+extern "C" int fhd_read_checkpoint(const fhd_params* params, const char* chk_base, int restart, int* step,
+                                   double* time, int* stats_count, fhd_fab cu, const fhd_fab cumom[3], fhd_fab prim,
+                                   const fhd_fab vel[3], const fhd_stats* stats) {
+    if (!params || !chk_base || !cumom || !vel || restart < 0 || !step || !time || !stats_count || !cu.data ||
+        !prim.data)
+        return FHD_ERR_BAD_ARG;
+    const std::string dir = chk_dir(chk_base, restart);
+    FILE* h = std::fopen((dir + "/Header").c_str(), "r");
+    if (!h) return FHD_ERR_BAD_ARG;
+    char title[256];
+    int s = 0, sc = 0;
+    double t = 0;
+    const bool hok = std::fgets(title, sizeof(title), h) && std::fscanf(h, "%d %lf %d", &s, &t, &sc) == 3;
+    std::fclose(h);
+    if (!hok || std::strncmp(title, "Checkpoint file for FHDeX/compressStag", 38) != 0) return FHD_ERR_BAD_ARG;
+    const std::vector<Entry> E = entries(cu, cumom, prim, vel, stats);
+    std::vector<double> buf;
+    bool synced = false;
+    for (const Entry& e : E) {
+        int vlo[3], vhi[3], type[3], ng;
+        if (!geometry(*params, e.fab, vlo, vhi, type, &ng)) return FHD_ERR_BAD_ARG;
+        int glo[3], ghi[3];
+        for (int d = 0; d < 3; ++d) {
+            glo[d] = vlo[d] - ng;
+            ghi[d] = vhi[d] + ng;
+        }
+        if (!vismf_read(dir + "/Level_0", e.name, glo, ghi, type, e.fab.ncomp, buf)) return FHD_ERR_BAD_ARG;
+        const bool dev = on_device(e.fab.data);
+        if (dev && !synced) {
+            if (cudaDeviceSynchronize() != cudaSuccess) {
+                cudaGetLastError();
+                return FHD_ERR_CUDA;
+            }
+            synced = true;
+        }
+        if (!copy_bytes(e.fab.data, buf.data(), buf.size() * sizeof(double), dev)) return FHD_ERR_CUDA;
+    }
+    // ReadCheckPoint resumes at the step after the saved one (Checkpoint.cpp:328-329)
+    *step = s + 1;
+    *time = t;
+    *stats_count = sc;
+    return FHD_OK;
+}

@@ -20,13 +20,12 @@
 // one-box MultiFab with its per-component minima and maxima) and
 // <dir>/Level_0/Cell_D_00000 (one FAB: a text descriptor line for little-endian
 // IEEE doubles, then the data, components slowest, x fastest).
-#include <cerrno>
 #include <cstdio>
 #include <string>
-#include <sys/stat.h>
 #include <vector>
 
 #include "fhd_launch.cuh"
+#include "fhd_vismf.h"
 
 namespace fhd {
 
@@ -176,13 +175,9 @@ int plot_names(const fhd_params& prm, int flags, std::vector<std::string>& names
     return FHD_OK;
 }
 
-static bool make_dir(const std::string& p) { return mkdir(p.c_str(), 0755) == 0 || errno == EEXIST; }
-
-// AMReX's text form of a cell box: ((lo) (hi) (type))
 static std::string box_text(const int n[3]) {
-    char b[160];
-    std::snprintf(b, sizeof(b), "((0,0,0) (%d,%d,%d) (0,0,0))", n[0] - 1, n[1] - 1, n[2] - 1);
-    return b;
+    const int lo[3] = {0, 0, 0}, hi[3] = {n[0] - 1, n[1] - 1, n[2] - 1}, type[3] = {0, 0, 0};
+    return vismf_box(lo, hi, type);
 }
 
 // Writes the packed host data (ncomp components of the valid box, x fastest,
@@ -191,9 +186,8 @@ int plot_write(const fhd_params& prm, const char* dir, const double* host, const
                double time, int step) {
     const int nc = (int)names.size();
     const int* n = prm.n_cells;
-    const int64_t cells = (int64_t)n[0] * n[1] * n[2];
     const std::string root(dir);
-    if (!make_dir(root) || !make_dir(root + "/Level_0")) return FHD_ERR_BAD_ARG;
+    if (!vismf_mkdir(root) || !vismf_mkdir(root + "/Level_0")) return FHD_ERR_BAD_ARG;
     double dx[3];
     for (int d = 0; d < 3; ++d) dx[d] = (prm.prob_hi[d] - prm.prob_lo[d]) / n[d];
     FILE* h = std::fopen((root + "/Header").c_str(), "w");
@@ -210,34 +204,10 @@ int plot_write(const fhd_params& prm, const char* dir, const double* host, const
     for (int d = 0; d < 3; ++d) std::fprintf(h, "%.17g %.17g\n", prm.prob_lo[d], prm.prob_hi[d]);
     std::fprintf(h, "Level_0/Cell\n");
     const bool hok = std::fclose(h) == 0;
-    // Cell_D_00000: one FAB
-    FILE* f = std::fopen((root + "/Level_0/Cell_D_00000").c_str(), "wb");
-    if (!f) return FHD_ERR_BAD_ARG;
-    std::fprintf(f, "FAB ((8, (64 11 52 0 1 12 0 1023)),(8, (1 2 3 4 5 6 7 8)))%s %d\n", box_text(n).c_str(), nc);
-    const size_t cnt = (size_t)cells * nc;
-    const bool dok = std::fwrite(host, sizeof(double), cnt, f) == cnt;
-    const bool fok = std::fclose(f) == 0;
-    // Cell_H: VisMF header of the one-box MultiFab, with per-component min / max
-    FILE* v = std::fopen((root + "/Level_0/Cell_H").c_str(), "w");
-    if (!v) return FHD_ERR_BAD_ARG;
-    std::fprintf(v, "1\n1\n%d\n0\n(1 0\n%s\n)\n1\nFabOnDisk: Cell_D_00000 0\n\n1,%d\n", nc, box_text(n).c_str(), nc);
-    std::vector<double> mn(nc), mx(nc);
-    for (int c = 0; c < nc; ++c) {
-        const double* p = host + (size_t)c * cells;
-        double a = p[0], b = p[0];
-        for (int64_t q = 1; q < cells; ++q) {
-            a = p[q] < a ? p[q] : a;
-            b = p[q] > b ? p[q] : b;
-        }
-        mn[c] = a;
-        mx[c] = b;
-    }
-    for (int c = 0; c < nc; ++c) std::fprintf(v, "%.17g,", mn[c]);
-    std::fprintf(v, "\n\n1,%d\n", nc);
-    for (int c = 0; c < nc; ++c) std::fprintf(v, "%.17g,", mx[c]);
-    std::fprintf(v, "\n");
-    const bool vok = std::fclose(v) == 0;
-    return (hok && dok && fok && vok) ? FHD_OK : FHD_ERR_BAD_ARG;
+    // Level_0/Cell_H and Cell_D_00000: the one-box MultiFab, no ghosts
+    const int lo[3] = {0, 0, 0}, hi[3] = {n[0] - 1, n[1] - 1, n[2] - 1}, type[3] = {0, 0, 0};
+    const bool cok = vismf_write(root + "/Level_0", "Cell", host, lo, hi, type, nc, 0);
+    return (hok && cok) ? FHD_OK : FHD_ERR_BAD_ARG;
 }
 
 }  // namespace fhd
