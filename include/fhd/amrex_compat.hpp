@@ -107,6 +107,14 @@ struct RealBox {
     std::array<Real, 3> lo{{0, 0, 0}}, hi{{1, 1, 1}};
 };
 
+// One-box BoxArray and its (trivial) distribution, for the signatures that carry
+// them (ReadCheckPoint): the box is the cell-centred domain.
+struct BoxArray {
+    Box box;
+    void define(const Box& b) { box = b; }
+};
+struct DistributionMapping {};
+
 // Every direction periodic: the only boundary the drop-in step implements.
 struct Periodicity {
     IntVect period;

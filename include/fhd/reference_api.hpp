@@ -20,6 +20,8 @@
 //   compute_compressible_chemistry_source_CLE
 //                              src_chemistry/chemistry_functions.H:20-21
 //   WritePlotFileStag          src_compressible_stag/compressible_functions_stag.H:15-39
+//   WriteCheckPoint,
+//   ReadCheckPoint             src_compressible_stag/compressible_functions_stag.H:188-243
 //
 // As in the reference, physics parameters are process globals in namespaces
 // `common`, `compressible` and `chemistry` (src_common/common_namespace.H,
@@ -90,6 +92,8 @@ inline Real zeta_ratio = -1.0;
 namespace common {
 // <= 0: Runiv / k_B, as InitializeCommonNamespace derives it (common_functions.cpp:775)
 inline fhd::amrex_compat::Real avogadro = 0.0;
+// checkpoint to restart from, < 0: none (common_functions.cpp; ReadCheckPoint reads chk<restart>)
+inline int restart = -1;
 // plotfile inputs (common_functions.cpp:390, 614-618)
 inline std::string plot_base_name = "plt";
 inline int plot_means = 0;
@@ -507,6 +511,125 @@ inline void WritePlotFileStag(int step, const fhd::amrex_compat::Real time, cons
     check(fhd_write_plotfile_stag(context(), common::plot_base_name.c_str(), step, time, flags, cu.fab(), mom,
                                   prim.fab(), vl, eta.fab(), kappa.fab(), zeta.fab(), &st),
           "WritePlotFileStag");
+}
+
+// WriteCheckPoint (Checkpoint.cpp:28-257): chk<step, 9 digits>/ in the working
+// directory with the state and every defined statistics MultiFab.  The
+// surface-coverage, cross-correlation and turbulence-forcing records are not
+// written (none of them exists on this path); the noise needs no generator state.
+inline void WriteCheckPoint(int step, const fhd::amrex_compat::Real time, int statsCount,
+                            const fhd::amrex_compat::Geometry& /*geom*/, const fhd::amrex_compat::MultiFab& cu,
+                            const fhd::amrex_compat::MultiFab& cuMeans, const fhd::amrex_compat::MultiFab& cuVars,
+                            const fhd::amrex_compat::MultiFab& prim, const fhd::amrex_compat::MultiFab& primMeans,
+                            const fhd::amrex_compat::MultiFab& primVars,
+                            const std::array<fhd::amrex_compat::MultiFab, 3>& cumom,
+                            const std::array<fhd::amrex_compat::MultiFab, 3>& cumomMeans,
+                            const std::array<fhd::amrex_compat::MultiFab, 3>& cumomVars,
+                            const std::array<fhd::amrex_compat::MultiFab, 3>& vel,
+                            const std::array<fhd::amrex_compat::MultiFab, 3>& velMeans,
+                            const std::array<fhd::amrex_compat::MultiFab, 3>& velVars,
+                            const fhd::amrex_compat::MultiFab& coVars, const fhd::amrex_compat::MultiFab& mom3,
+                            const fhd::amrex_compat::MultiFab& mom4, const fhd::amrex_compat::MultiFab& /*surfcov*/,
+                            const fhd::amrex_compat::MultiFab& /*surfcovMeans*/,
+                            const fhd::amrex_compat::MultiFab& /*surfcovVars*/,
+                            const fhd::amrex_compat::MultiFab& /*surfcovcoVars*/,
+                            const fhd::amrex_compat::MultiFab& /*spatialCrossMF*/,
+                            const fhd::amrex_compat::Vector<fhd::amrex_compat::Real>& /*spatialCrossVec*/,
+                            int /*ncross*/, TurbForcingComp& /*turbforce*/) {
+    using namespace fhd::ref;
+    fhd_stats st;
+    std::memset(&st, 0, sizeof(st));
+    st.cuMeans = cuMeans.fab();
+    st.cuVars = cuVars.fab();
+    st.primMeans = primMeans.fab();
+    st.primVars = primVars.fab();
+    st.coVars = coVars.fab();
+    st.mom3 = mom3.fab();
+    st.mom4 = mom4.fab();
+    for (int d = 0; d < 3; ++d) {
+        st.velMeans[d] = velMeans[d].fab();
+        st.velVars[d] = velVars[d].fab();
+        st.cumomMeans[d] = cumomMeans[d].fab();
+        st.cumomVars[d] = cumomVars[d].fab();
+    }
+    fhd_fab mom[3], vl[3];
+    fabs_of(cumom, mom);
+    fabs_of(vel, vl);
+    const fhd_params p = params_from_globals();
+    check(fhd_write_checkpoint(&p, "chk", step, time, statsCount, cu.fab(), mom, prim.fab(), vl, &st),
+          "WriteCheckPoint");
+}
+
+// ReadCheckPoint (Checkpoint.cpp:259-575): defines every MultiFab with the
+// reference's shapes on `domain` (device memory, 2 ghost cells for the state and
+// the cell-centred means/variances, none for the others; mom3 / mom4 only with
+// plot_mom3 / plot_mom4), reads chk<common::restart, 9 digits>/ into them and sets
+// step to the saved step + 1, time and statsCount.
+inline void ReadCheckPoint(int& step, fhd::amrex_compat::Real& time, int& statsCount,
+                           fhd::amrex_compat::Geometry& /*geom*/, const fhd::amrex_compat::Box& domain,
+                           fhd::amrex_compat::MultiFab& cu, fhd::amrex_compat::MultiFab& cuMeans,
+                           fhd::amrex_compat::MultiFab& cuVars, fhd::amrex_compat::MultiFab& prim,
+                           fhd::amrex_compat::MultiFab& primMeans, fhd::amrex_compat::MultiFab& primVars,
+                           std::array<fhd::amrex_compat::MultiFab, 3>& cumom,
+                           std::array<fhd::amrex_compat::MultiFab, 3>& cumomMeans,
+                           std::array<fhd::amrex_compat::MultiFab, 3>& cumomVars,
+                           std::array<fhd::amrex_compat::MultiFab, 3>& vel,
+                           std::array<fhd::amrex_compat::MultiFab, 3>& velMeans,
+                           std::array<fhd::amrex_compat::MultiFab, 3>& velVars,
+                           fhd::amrex_compat::MultiFab& coVars, fhd::amrex_compat::MultiFab& mom3,
+                           fhd::amrex_compat::MultiFab& mom4, fhd::amrex_compat::MultiFab& /*surfcov*/,
+                           fhd::amrex_compat::MultiFab& /*surfcovMeans*/, fhd::amrex_compat::MultiFab& /*surfcovVars*/,
+                           fhd::amrex_compat::MultiFab& /*surfcovcoVars*/,
+                           fhd::amrex_compat::MultiFab& /*spatialCrossMF*/,
+                           fhd::amrex_compat::Vector<fhd::amrex_compat::Real>& /*spatialCrossVec*/, int /*ncross*/,
+                           TurbForcingComp& /*turbforce*/, fhd::amrex_compat::BoxArray& ba,
+                           fhd::amrex_compat::DistributionMapping& /*dmap*/) {
+    using namespace fhd::ref;
+    using fhd::amrex_compat::convert;
+    using fhd::amrex_compat::face_nodal;
+    const int ns = common::nspecies, nvars = 5 + ns, nprim = 6 + 2 * ns, ngc = 2;
+    ba.define(domain);
+    cu.define(domain, nvars, ngc);
+    cuMeans.define(domain, nvars, ngc);
+    cuVars.define(domain, nvars, ngc);
+    prim.define(domain, nprim, ngc);
+    primMeans.define(domain, nprim + 3, ngc);
+    primVars.define(domain, nprim + 5, ngc);
+    for (int d = 0; d < 3; ++d) {
+        const fhd::amrex_compat::Box fb = convert(domain, face_nodal(d));
+        vel[d].define(fb, 1, ngc);
+        cumom[d].define(fb, 1, ngc);
+        velMeans[d].define(fb, 1, 0);
+        cumomMeans[d].define(fb, 1, 0);
+        velVars[d].define(fb, 1, 0);
+        cumomVars[d].define(fb, 1, 0);
+    }
+    coVars.define(domain, 26, 0);
+    if (common::plot_mom3) mom3.define(domain, nvars + 1, 0);
+    if (common::plot_mom4) mom4.define(domain, nvars + 1, 0);
+    fhd_stats st;
+    std::memset(&st, 0, sizeof(st));
+    st.cuMeans = cuMeans.fab();
+    st.cuVars = cuVars.fab();
+    st.primMeans = primMeans.fab();
+    st.primVars = primVars.fab();
+    st.coVars = coVars.fab();
+    st.mom3 = mom3.fab();
+    st.mom4 = mom4.fab();
+    for (int d = 0; d < 3; ++d) {
+        st.velMeans[d] = velMeans[d].fab();
+        st.velVars[d] = velVars[d].fab();
+        st.cumomMeans[d] = cumomMeans[d].fab();
+        st.cumomVars[d] = cumomVars[d].fab();
+    }
+    fhd_fab mom[3], vl[3];
+    fabs_of(cumom, mom);
+    fabs_of(vel, vl);
+    const fhd_params p = params_from_globals();
+    double t = 0.0;
+    check(fhd_read_checkpoint(&p, "chk", common::restart, &step, &t, &statsCount, cu.fab(), mom, prim.fab(), vl, &st),
+          "ReadCheckPoint");
+    time = t;
 }
 
 // MultiFabFillRandom (MultiFabFillRandom.cpp:5-31): N(0, variance) in one

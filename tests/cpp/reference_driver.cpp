@@ -13,6 +13,10 @@
 //   reference_driver plot <n> <nsteps> <seed> <dt> <plot_base_name>
 //       run nsteps RK3 steps on device MultiFabs and WritePlotFileStag (step
 //       nsteps, time nsteps*dt, no statistics)
+//   reference_driver chk <n> <n1> <n2> <seed> <dt> <out.bin>
+//       n1 steps, WriteCheckPoint (chk<n1-1> in the working directory, with
+//       zeroed statistics MultiFabs), ReadCheckPoint into new MultiFabs, steps
+//       n1..n1+n2-1 on them; writes the final state as `run` does
 //   reference_driver massfrac <n>
 //       start from a state with a zero mass fraction: calculateTransportCoeffs
 //       must report it through the abort handler (exit code 3)
@@ -240,6 +244,53 @@ static int cmd_plot(int n, int nsteps, int seed, double dt, const char* base) {
     return 0;
 }
 
+static int cmd_chk(int n, int n1, int n2, int seed, double dt, const char* out) {
+    set_argon(n, seed);
+    State s(n, Arena::Device, true);
+    s.init();
+    step_all(s, dt, n1);
+    const Box dom(IntVect(0, 0, 0), IntVect(n - 1, n - 1, n - 1));
+    const int nv = s.nvars, np = s.nprimvars;
+    MultiFab cuMeans(dom, nv, 2), cuVars(dom, nv, 2), primMeans(dom, np + 3, 2), primVars(dom, np + 5, 2),
+        coVars(dom, 26, 0), none;
+    std::array<MultiFab, 3> cmm, cmv, vm, vv, none3;
+    for (int d = 0; d < 3; ++d) {
+        cmm[d].define(convert(dom, face_nodal(d)), 1, 0);
+        cmv[d].define(convert(dom, face_nodal(d)), 1, 0);
+        vm[d].define(convert(dom, face_nodal(d)), 1, 0);
+        vv[d].define(convert(dom, face_nodal(d)), 1, 0);
+    }
+    Vector<Real> cross;
+    TurbForcingComp turb;
+    WriteCheckPoint(n1 - 1, n1 * dt, 0, s.geom, s.cu, cuMeans, cuVars, s.prim, primMeans, primVars, s.cumom, cmm, cmv,
+                    s.vel, vm, vv, coVars, none, none, none, none, none, none, none, cross, 0, turb);
+    // restart into fresh MultiFabs
+    State r(n, Arena::Device, false);
+    MultiFab rcm, rcv, rpm, rpv, rco, rm3, rm4, sc0, sc1, sc2, sc3, scross;
+    std::array<MultiFab, 3> rcmm, rcmv, rvm, rvv;
+    BoxArray ba;
+    DistributionMapping dm;
+    int step = -1, count = -1;
+    Real time = -1.0;
+    common::restart = n1 - 1;
+    ReadCheckPoint(step, time, count, r.geom, dom, r.cu, rcm, rcv, r.prim, rpm, rpv, r.cumom, rcmm, rcmv, r.vel, rvm,
+                   rvv, rco, rm3, rm4, sc0, sc1, sc2, sc3, scross, cross, 0, turb, ba, dm);
+    if (step != n1 || count != 0 || time != n1 * dt) return 5;
+    TurbForcingComp turbforce;
+    for (int st = step; st < n1 + n2; ++st)
+        RK3stepStag(r.cu, r.cumom, r.prim, r.vel, r.source, r.eta, r.zeta, r.kappa, r.chi, r.D, r.faceflux,
+                    r.edgeflux_x, r.edgeflux_y, r.edgeflux_z, r.cenflux, r.ranchem, r.geom, dt, st, turbforce);
+    FILE* f = std::fopen(out, "wb");
+    if (!f) return 2;
+    write_all(f, r.cu);
+    for (int d = 0; d < 3; ++d) write_all(f, r.cumom[d]);
+    write_all(f, r.prim);
+    for (int d = 0; d < 3; ++d) write_all(f, r.vel[d]);
+    std::fclose(f);
+    fhd::ref::finalize();
+    return 0;
+}
+
 static int cmd_massfrac(int n) {
     set_argon(n, 1);
     common::rhobar[0] = 1.0;  // species 2 absent: Y_2 = 0
@@ -270,6 +321,9 @@ int main(int argc, char** argv) {
             return cmd_run(argv[2], std::atoi(argv[3]), std::atoi(argv[4]), std::atoi(argv[5]),
                            std::strtod(argv[6], nullptr), argv[7], argc == 9 ? argv[8] : "argon");
         if (cmd == "massfrac") return cmd_massfrac(std::atoi(argv[2]));
+        if (cmd == "chk" && argc == 8)
+            return cmd_chk(std::atoi(argv[2]), std::atoi(argv[3]), std::atoi(argv[4]), std::atoi(argv[5]),
+                           std::strtod(argv[6], nullptr), argv[7]);
         if (cmd == "plot" && argc == 7)
             return cmd_plot(std::atoi(argv[2]), std::atoi(argv[3]), std::atoi(argv[4]), std::strtod(argv[5], nullptr),
                             argv[6]);

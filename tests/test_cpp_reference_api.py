@@ -137,3 +137,29 @@ def test_reference_driver_plotfile_equals_c_abi_plotfile(driver, tmp_path):
         a = open(os.path.join(ours, rel), "rb").read()
         b = open(os.path.join(theirs, rel), "rb").read()
         assert a == b, rel
+
+
+@pytest.mark.gpu
+def test_reference_driver_checkpoint_restart_equals_uninterrupted_run(driver, tmp_path):
+    """WriteCheckPoint, ReadCheckPoint into new MultiFabs and the remaining steps,
+    all through the reference-named layer, end bitwise where n1 + n2 uninterrupted
+    C-ABI steps end."""
+    from fhdex_b200.context import Context
+    n, n1, n2, seed = 10, 2, 3, 11
+    p = argon(n, dx=8e-6, seed=seed)
+    dt = stable_dt(p)
+    out = str(tmp_path / "state.bin")
+    r = subprocess.run([driver, "chk", str(n), str(n1), str(n2), str(seed), repr(dt), out],
+                       capture_output=True, text=True, timeout=300, cwd=str(tmp_path))
+    assert r.returncode == 0, (r.returncode, r.stderr)
+    assert os.path.isdir(tmp_path / f"chk{n1 - 1:09d}")
+    ctx = Context(p)
+    st = StagState(p, "cuda", aux=False)
+    ctx.init_state(st)
+    for step in range(n1 + n2):
+        ctx.rk3_step(st, dt, step, aux=False)
+    torch.cuda.synchronize()
+    got = read_state(out, st)
+    mfs = [st.cu] + st.cumom + [st.prim] + st.vel
+    bad = [k for k, (g, m) in enumerate(zip(got, mfs)) if not torch.equal(g, m.arr.cpu())]
+    assert not bad, bad
