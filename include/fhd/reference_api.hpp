@@ -22,6 +22,7 @@
 //   WritePlotFileStag          src_compressible_stag/compressible_functions_stag.H:15-39
 //   WriteCheckPoint,
 //   ReadCheckPoint             src_compressible_stag/compressible_functions_stag.H:188-243
+//   evaluateStatsStag3D        src_compressible_stag/compressible_functions_stag.H:257-273
 //
 // As in the reference, physics parameters are process globals in namespaces
 // `common`, `compressible` and `chemistry` (src_common/common_namespace.H,
@@ -511,6 +512,55 @@ inline void WritePlotFileStag(int step, const fhd::amrex_compat::Real time, cons
     check(fhd_write_plotfile_stag(context(), common::plot_base_name.c_str(), step, time, flags, cu.fab(), mom,
                                   prim.fab(), vl, eta.fab(), kappa.fab(), zeta.fab(), &st),
           "WritePlotFileStag");
+}
+
+// evaluateStatsStag3D (statsStag.cpp:10-77): the running means (plot_means) and
+// the variances, covariances and third / fourth moments (plot_vars or
+// plot_covars; plot_mom3 / plot_mom4) with sample count `steps`, each followed by
+// the reference's FillBoundary.  Without surface coverage (theta*) and without
+// the yz-averaged spatial cross-correlations (plot_cross), which are not on this
+// path: those arguments are accepted and left untouched.
+inline void evaluateStatsStag3D(fhd::amrex_compat::MultiFab& cons, fhd::amrex_compat::MultiFab& consMean,
+                                fhd::amrex_compat::MultiFab& consVar, fhd::amrex_compat::MultiFab& prim_in,
+                                fhd::amrex_compat::MultiFab& primMean, fhd::amrex_compat::MultiFab& primVar,
+                                const std::array<fhd::amrex_compat::MultiFab, 3>& vel,
+                                std::array<fhd::amrex_compat::MultiFab, 3>& velMean,
+                                std::array<fhd::amrex_compat::MultiFab, 3>& velVar,
+                                const std::array<fhd::amrex_compat::MultiFab, 3>& cumom,
+                                std::array<fhd::amrex_compat::MultiFab, 3>& cumomMean,
+                                std::array<fhd::amrex_compat::MultiFab, 3>& cumomVar,
+                                fhd::amrex_compat::MultiFab& coVar, fhd::amrex_compat::MultiFab& mom3,
+                                fhd::amrex_compat::MultiFab& mom4, fhd::amrex_compat::MultiFab& /*theta*/,
+                                fhd::amrex_compat::MultiFab& /*thetaMean*/, fhd::amrex_compat::MultiFab& /*thetaVar*/,
+                                fhd::amrex_compat::MultiFab& /*thetacoVar*/,
+                                fhd::amrex_compat::Vector<fhd::amrex_compat::Real>& /*dataSliceMeans_xcross*/,
+                                fhd::amrex_compat::Vector<fhd::amrex_compat::Real>& /*spatialCross3D*/,
+                                const int /*ncross*/, const fhd::amrex_compat::Box& /*domain*/, const int steps,
+                                const fhd::amrex_compat::Geometry& /*geom*/) {
+    using namespace fhd::ref;
+    const int flags = (common::plot_means ? FHD_STATS_MEANS : 0) |
+                      ((common::plot_vars || common::plot_covars) ? FHD_STATS_VARS : 0) |
+                      (common::plot_mom3 ? FHD_STATS_MOM3 : 0) | (common::plot_mom4 ? FHD_STATS_MOM4 : 0);
+    if (!flags) return;
+    fhd_stats st;
+    std::memset(&st, 0, sizeof(st));
+    st.cuMeans = consMean.fab();
+    st.cuVars = consVar.fab();
+    st.primMeans = primMean.fab();
+    st.primVars = primVar.fab();
+    st.coVars = coVar.fab();
+    st.mom3 = mom3.fab();
+    st.mom4 = mom4.fab();
+    for (int d = 0; d < 3; ++d) {
+        st.velMeans[d] = velMean[d].fab();
+        st.velVars[d] = velVar[d].fab();
+        st.cumomMeans[d] = cumomMean[d].fab();
+        st.cumomVars[d] = cumomVar[d].fab();
+    }
+    fhd_fab vl[3], mom[3];
+    fabs_of(vel, vl);
+    fabs_of(cumom, mom);
+    check(fhd_stats_stag(context(), cons.fab(), prim_in.fab(), vl, mom, &st, steps, flags), "evaluateStatsStag3D");
 }
 
 // WriteCheckPoint (Checkpoint.cpp:28-257): chk<step, 9 digits>/ in the working

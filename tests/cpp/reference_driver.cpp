@@ -17,6 +17,10 @@
 //       n1 steps, WriteCheckPoint (chk<n1-1> in the working directory, with
 //       zeroed statistics MultiFabs), ReadCheckPoint into new MultiFabs, steps
 //       n1..n1+n2-1 on them; writes the final state as `run` does
+//   reference_driver stats <n> <nsteps> <seed> <dt> <out.bin>
+//       nsteps RK3 steps, evaluateStatsStag3D after each (plot_means, plot_vars,
+//       plot_mom3, plot_mom4); writes cuMeans, cuVars, primMeans, primVars,
+//       coVars, mom3, mom4, velMeans, velVars, cumomMeans, cumomVars
 //   reference_driver massfrac <n>
 //       start from a state with a zero mass fraction: calculateTransportCoeffs
 //       must report it through the abort handler (exit code 3)
@@ -291,6 +295,42 @@ static int cmd_chk(int n, int n1, int n2, int seed, double dt, const char* out) 
     return 0;
 }
 
+static int cmd_stats(int n, int nsteps, int seed, double dt, const char* out) {
+    set_argon(n, seed);
+    common::plot_means = common::plot_vars = common::plot_mom3 = common::plot_mom4 = 1;
+    State s(n, Arena::Device, true);
+    s.init();
+    const Box dom(IntVect(0, 0, 0), IntVect(n - 1, n - 1, n - 1));
+    const int nv = s.nvars, np = s.nprimvars;
+    MultiFab cuMeans(dom, nv, 2), cuVars(dom, nv, 2), primMeans(dom, np + 3, 2), primVars(dom, np + 5, 2),
+        coVars(dom, 26, 0), mom3(dom, nv + 1, 0), mom4(dom, nv + 1, 0), theta;
+    std::array<MultiFab, 3> vm, vv, cmm, cmv;
+    for (int d = 0; d < 3; ++d) {
+        vm[d].define(convert(dom, face_nodal(d)), 1, 0);
+        vv[d].define(convert(dom, face_nodal(d)), 1, 0);
+        cmm[d].define(convert(dom, face_nodal(d)), 1, 0);
+        cmv[d].define(convert(dom, face_nodal(d)), 1, 0);
+    }
+    Vector<Real> slice, cross;
+    TurbForcingComp turb;
+    for (int step = 0; step < nsteps; ++step) {
+        RK3stepStag(s.cu, s.cumom, s.prim, s.vel, s.source, s.eta, s.zeta, s.kappa, s.chi, s.D, s.faceflux,
+                    s.edgeflux_x, s.edgeflux_y, s.edgeflux_z, s.cenflux, s.ranchem, s.geom, dt, step, turb);
+        evaluateStatsStag3D(s.cu, cuMeans, cuVars, s.prim, primMeans, primVars, s.vel, vm, vv, s.cumom, cmm, cmv,
+                            coVars, mom3, mom4, theta, theta, theta, theta, slice, cross, 0, dom, step + 1, s.geom);
+    }
+    FILE* f = std::fopen(out, "wb");
+    if (!f) return 2;
+    for (const MultiFab* m : {&cuMeans, &cuVars, &primMeans, &primVars, &coVars, &mom3, &mom4}) write_all(f, *m);
+    for (int d = 0; d < 3; ++d) write_all(f, vm[d]);
+    for (int d = 0; d < 3; ++d) write_all(f, vv[d]);
+    for (int d = 0; d < 3; ++d) write_all(f, cmm[d]);
+    for (int d = 0; d < 3; ++d) write_all(f, cmv[d]);
+    std::fclose(f);
+    fhd::ref::finalize();
+    return 0;
+}
+
 static int cmd_massfrac(int n) {
     set_argon(n, 1);
     common::rhobar[0] = 1.0;  // species 2 absent: Y_2 = 0
@@ -321,6 +361,9 @@ int main(int argc, char** argv) {
             return cmd_run(argv[2], std::atoi(argv[3]), std::atoi(argv[4]), std::atoi(argv[5]),
                            std::strtod(argv[6], nullptr), argv[7], argc == 9 ? argv[8] : "argon");
         if (cmd == "massfrac") return cmd_massfrac(std::atoi(argv[2]));
+        if (cmd == "stats" && argc == 7)
+            return cmd_stats(std::atoi(argv[2]), std::atoi(argv[3]), std::atoi(argv[4]), std::strtod(argv[5], nullptr),
+                             argv[6]);
         if (cmd == "chk" && argc == 8)
             return cmd_chk(std::atoi(argv[2]), std::atoi(argv[3]), std::atoi(argv[4]), std::atoi(argv[5]),
                            std::strtod(argv[6], nullptr), argv[7]);

@@ -163,3 +163,40 @@ def test_reference_driver_checkpoint_restart_equals_uninterrupted_run(driver, tm
     mfs = [st.cu] + st.cumom + [st.prim] + st.vel
     bad = [k for k, (g, m) in enumerate(zip(got, mfs)) if not torch.equal(g, m.arr.cpu())]
     assert not bad, bad
+
+
+@pytest.mark.gpu
+def test_reference_driver_statistics_equal_c_abi_statistics(driver, tmp_path):
+    """evaluateStatsStag3D through the reference-named layer (plot_means, plot_vars,
+    plot_mom3, plot_mom4) after every step equals fhd_stats_stag bit for bit."""
+    from fhdex_b200.context import Context
+    from fhdex_b200.stats import StatsState
+    n, nsteps, seed = 8, 3, 13
+    p = argon(n, dx=8e-6, seed=seed)
+    dt = stable_dt(p)
+    out = str(tmp_path / "stats.bin")
+    r = subprocess.run([driver, "stats", str(n), str(nsteps), str(seed), repr(dt), out],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, (r.returncode, r.stderr)
+    ctx = Context(p)
+    st = StagState(p, "cuda")
+    ctx.init_state(st)
+    stats = StatsState(p, "cuda")
+    for step in range(nsteps):
+        ctx.rk3_step(st, dt, step, aux=True)
+        ctx.stats_stag(st, stats, step + 1, 15)
+    torch.cuda.synchronize()
+    mfs = [stats.cuMeans, stats.cuVars, stats.primMeans, stats.primVars, stats.coVars, stats.mom3, stats.mom4]
+    mfs += stats.velMeans + stats.velVars + stats.cumomMeans + stats.cumomVars
+    raw = np.fromfile(out, dtype=np.float64)
+    off = 0
+    bad = []
+    for k, m in enumerate(mfs):
+        size = m.arr.numel()
+        got = torch.from_numpy(raw[off:off + size].copy()).view(m.arr.shape)
+        off += size
+        if not torch.equal(got, m.arr.cpu()):
+            bad.append(k)
+    assert off == raw.size
+    assert not bad, bad
+    assert stats.cuVars.arr.abs().max().item() > 0
