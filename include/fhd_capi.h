@@ -367,7 +367,9 @@ int fhd_plotfile_pack(fhd_ctx* ctx, int flags, fhd_fab out, fhd_fab cu, const fh
  * statsCount, the BoxArray) and Level_0/<name>_H + <name>_D_00000 for cu, prim,
  * vel, cumom and, when `stats` is given, every non-empty statistics fab, under
  * the reference's names, whole fabs with ghost cells.  Fabs may be device or
- * host memory (no device needed for host fabs).  The read fills fabs of the same
+ * host memory (no device needed for host fabs; with device fabs the call
+ * synchronises the device before copying, so pending work on any stream is
+ * finished first).  The read fills fabs of the same
  * shapes and returns step = saved step + 1, the time and statsCount, as the
  * reference's restart does; the in-kernel noise needs no saved generator state
  * (it is a function of seed and step). */
@@ -378,7 +380,8 @@ int fhd_read_checkpoint(const fhd_params* params, const char* chk_base, int rest
                         int* stats_count, fhd_fab cu, const fhd_fab cumom[3], fhd_fab prim, const fhd_fab vel[3],
                         const fhd_stats* stats);
 
-/* pack, copy to the host and write the plotfile directory (blocks on the stream) */
+/* pack, copy to the host and write the plotfile directory (blocks on the stream;
+ * allocates and frees a temporary device buffer of the packed size) */
 int fhd_write_plotfile_stag(fhd_ctx* ctx, const char* plot_base_name, int step, double time, int flags, fhd_fab cu,
                             const fhd_fab cumom[3], fhd_fab prim, const fhd_fab vel[3], fhd_fab eta, fhd_fab kappa,
                             fhd_fab zeta, const fhd_stats* stats);
