@@ -18,7 +18,15 @@
 
 namespace fhd {
 
-inline bool vismf_mkdir(const std::string& p) { return mkdir(p.c_str(), 0755) == 0 || errno == EEXIST; }
+// creates the directory and any missing parents (as AMReX builds a plotfile's or
+// checkpoint's directory hierarchy)
+inline bool vismf_mkdir(const std::string& p) {
+    for (size_t s = p.find('/', 1); s != std::string::npos; s = p.find('/', s + 1)) {
+        const std::string part = p.substr(0, s);
+        if (mkdir(part.c_str(), 0755) != 0 && errno != EEXIST) return false;
+    }
+    return mkdir(p.c_str(), 0755) == 0 || errno == EEXIST;
+}
 
 // AMReX's text form of a box: ((lo) (hi) (index type))
 inline std::string vismf_box(const int lo[3], const int hi[3], const int type[3]) {

@@ -58,3 +58,11 @@ def test_bad_flags_are_rejected():
     import ctypes as C
     cp = argon(4).to_c()
     assert capi.load().fhd_plotfile_ncomp(C.byref(cp), 32) == -capi.FHD_ERR_BAD_ARG
+
+
+def test_plotfile_directory_parents_are_created(tmp_path):
+    p = argon((3, 3, 3), dx=8e-6)
+    data = torch.zeros((len(plotfile_names(p, 0)), 3, 3, 3), dtype=torch.float64)
+    d = str(tmp_path / "runs" / "case1" / "plt000000000")
+    write_plotfile_host(p, d, data, 0, 0.0, 0)
+    assert read_header(d)["names"] == plotfile_names(p, 0)
