@@ -189,6 +189,19 @@ def isomerization(p: Params) -> Params:
                      T0_chem=p.T_init)
 
 
+def exchange_network(p: Params) -> Params:
+    """A + B <-> C + D and A <-> C on the first four species of ``p`` (coefficients
+    0/1, no activation energy, no temperature power): a four-species reaction
+    network whose powers and exponentials are all exact.  A parity case for the
+    four-species kernel, not a chemical system: the molar masses of the species it
+    is applied to need not balance."""
+    return p.replace(nreaction=3, reaction_type=1,
+                     stoich_R=((1, 1, 0, 0), (0, 0, 1, 1), (1, 0, 0, 0)),
+                     stoich_P=((0, 0, 1, 1), (1, 1, 0, 0), (0, 0, 1, 0)),
+                     rate_const=(3.0e9, 2.0e9, 5.0e4), alpha_param=(0.0, 0.0, 0.0), beta_param=(0.0, 0.0, 0.0),
+                     T0_chem=p.T_init)
+
+
 def hard_sphere_single_gas(p: Params, T=None):
     """Closed-form first Chapman-Enskog hard-sphere viscosity and conductivity of a
     pure gas: eta = 5/(16 d^2) sqrt(m k T / pi), kappa = (75/64)(k/d^2) sqrt(kT/(pi m)).

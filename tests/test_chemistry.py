@@ -16,7 +16,7 @@ import pytest
 import torch
 
 from fhdex_b200.fab import CELL, MultiFab
-from fhdex_b200.params import isomerization, no2_dimerization, parse_inputs
+from fhdex_b200.params import exchange_network, isomerization, mixture4, no2_dimerization, parse_inputs
 from tests.helpers import perturbed_state
 
 
@@ -70,7 +70,8 @@ def cell_volume(p):
 
 @pytest.mark.parametrize("make", [lambda: no2_dimerization((5, 4, 3)),
                                   lambda: isomerization(no2_dimerization((4, 3, 5))),
-                                  lambda: no2_dimerization((3, 4, 4), reaction_type=0)])
+                                  lambda: no2_dimerization((3, 4, 4), reaction_type=0),
+                                  lambda: exchange_network(mixture4((4, 3, 3), dx=8e-6))])
 def test_oracle_matches_python_transcription_bitwise(oracle, make):
     p = make()
     st, W, src = chem_inputs(oracle, p, seed=3)
