@@ -1,5 +1,5 @@
 """Generates the golden fixtures of the injected-noise RK3 step (run from the
-repository root: ``python -m tests.golden.make_golden``).
+repository root: ``python -m tests.golden.make_golden [case ...]``).
 
 The reference holds no stored outputs for this path (its regression decks have
 no golden files and it cannot be built here), so the fixtures freeze the CPU
@@ -28,7 +28,9 @@ import os
 
 import numpy as np
 
-from fhdex_b200.params import Params, argon, mixture4, stable_dt
+import sys
+
+from fhdex_b200.params import Params, argon, isomerization, mixture4, no2_dimerization, stable_dt
 from fhdex_b200.state import StepNoise
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -41,6 +43,9 @@ CASES = {
                                                 advection_type=1), 12, 2),
     "argon_6x4x5_adv0_grav": (lambda: argon((6, 4, 5), dx=8e-6, advection_type=0,
                                             grav=(0.0, 0.0, -981.0)), 13, 3),
+    # NO2 / N2O4 gas with a first-order CLE reaction pair: the chemistry source inside
+    # every stage, its reaction noises stored with the rest (h<s>)
+    "iso_no2_5x4x4_chem": (lambda: isomerization(no2_dimerization((5, 4, 4), dx=8e-6)), 14, 4),
 }
 
 
@@ -51,11 +56,15 @@ def noise_arrays(nz: StepNoise):
             out[f"f{s}{d}"] = nz.face[s][d].arr
             out[f"e{s}{d}"] = nz.edge[s][d].arr
             out[f"c{s}{d}"] = nz.cen[s][d].arr
+        if nz.chem[s] is not None:
+            out[f"h{s}"] = nz.chem[s].arr
     return out
 
 
 def params_from_json(d: dict) -> Params:
-    return Params(**{k: tuple(v) if isinstance(v, list) else v for k, v in d.items()})
+    def tup(v):
+        return tuple(tup(x) for x in v) if isinstance(v, list) else v
+    return Params(**{k: tup(v) for k, v in d.items()})
 
 
 def make_case(O, name):
@@ -94,11 +103,13 @@ def load_manifest():
         return json.load(f)
 
 
-def main():
+def main(names=None):
+    """Writes the fixtures of `names` (all cases when None) and their manifest
+    entries, keeping the other cases' entries."""
     from oracle import oracle as O
     O.build()
-    manifest = {}
-    for name in CASES:
+    manifest = load_manifest() if os.path.exists(os.path.join(HERE, "MANIFEST.json")) else {}
+    for name in names or CASES:
         meta, arrays = make_case(O, name)
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), meta=np.array(json.dumps(meta)), **arrays)
         manifest[name] = {k: sha(a) for k, a in sorted(arrays.items())}
@@ -108,4 +119,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or None)
