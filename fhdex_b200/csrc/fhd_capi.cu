@@ -525,6 +525,13 @@ static bool plot_inputs_accessible(int flags, const fhd_fab& cu, const fhd_fab* 
     return true;
 }
 
+// FHD_PLOT_* bits, at most one of the three deltaY directions
+static bool plot_flags_ok(int flags) {
+    if (flags < 0 || flags > 255) return false;
+    const int dy = (flags >> 5) & 7;
+    return dy == 0 || dy == 1 || dy == 2 || dy == 4;
+}
+
 static bool plot_params_ok(const fhd_params* p) {
     if (!p || p->nspecies < 1 || p->nspecies > 4) return false;
     for (int d = 0; d < 3; ++d)
@@ -533,14 +540,14 @@ static bool plot_params_ok(const fhd_params* p) {
 }
 
 int fhd_plotfile_ncomp(const fhd_params* p, int flags) {
-    if (!plot_params_ok(p) || flags < 0 || flags > 31) return -FHD_ERR_BAD_ARG;
+    if (!plot_params_ok(p) || !plot_flags_ok(flags)) return -FHD_ERR_BAD_ARG;
     std::vector<std::string> names;
     const int rc = plot_names(*p, flags, names);
     return rc ? -rc : (int)names.size();
 }
 
 int fhd_plotfile_varname(const fhd_params* p, int flags, int comp, char* buf, int buflen) {
-    if (!plot_params_ok(p) || !buf || buflen < 1 || flags < 0 || flags > 31) return FHD_ERR_BAD_ARG;
+    if (!plot_params_ok(p) || !buf || buflen < 1 || !plot_flags_ok(flags)) return FHD_ERR_BAD_ARG;
     std::vector<std::string> names;
     const int rc = plot_names(*p, flags, names);
     if (rc) return rc;
@@ -551,7 +558,7 @@ int fhd_plotfile_varname(const fhd_params* p, int flags, int comp, char* buf, in
 
 int fhd_plotfile_write_host(const fhd_params* p, const char* dir, const double* data, int flags, double time,
                             int step) {
-    if (!plot_params_ok(p) || !dir || !data || flags < 0 || flags > 31) return FHD_ERR_BAD_ARG;
+    if (!plot_params_ok(p) || !dir || !data || !plot_flags_ok(flags)) return FHD_ERR_BAD_ARG;
     std::vector<std::string> names;
     const int rc = plot_names(*p, flags, names);
     if (rc) return rc;
@@ -560,7 +567,7 @@ int fhd_plotfile_write_host(const fhd_params* p, const char* dir, const double* 
 
 int fhd_plotfile_pack(fhd_ctx* c, int flags, fhd_fab out, fhd_fab cu, const fhd_fab cumom[3], fhd_fab prim,
                       const fhd_fab vel[3], fhd_fab eta, fhd_fab kappa, fhd_fab zeta, const fhd_stats* stats) {
-    if (!c || !cumom || !vel || flags < 0 || flags > 31 || (flags && !stats)) return FHD_ERR_BAD_ARG;
+    if (!c || !cumom || !vel || !plot_flags_ok(flags) || ((flags & 31) && !stats)) return FHD_ERR_BAD_ARG;
     cudaSetDevice(c->device);
     const int visc3 = c->prm.visc_type == 3 || c->prm.visc_type == -3;
     if (!out.data || !device_accessible(out.data) ||

@@ -9,7 +9,11 @@
 // of them through a table of per-component source views: block (z-plane,
 // component) copies the plane's rows, threads along x, so reads and writes are
 // contiguous and the indexing is 32-bit with no divisions.
-// Not covered: surface coverage (nspec_surfcov = 0) and plot_deltaY_dir.
+// plot_deltaY_dir (writePlotFileStag.cpp:282-290) appends Y_k minus its plane
+// average (WriteHorizontalAverageToMF, ComputeAverages.cpp:96-190): one thread per
+// (plane, species) sums the plane in the reference's loop order (k, j, i) so the
+// average is bitwise the reference's, then (-average) + Y_k is written, as
+// Ybar.mult(-1) and MultiFab::Add leave it.  Not covered: surface coverage.
 //
 // On disk (AMReX's single-level plotfile layout, as WriteSingleLevelPlotfile
 // writes it for one box): <dir>/Header (text: "HyperCLaw-V1.1", component count
@@ -37,6 +41,50 @@ struct PlotArgs {
     int n[3];
     int ncomp;
 };
+
+// plane averages of Y_k for plot_deltaY_dir: thread (r, n) sums the cells with
+// coordinate r along `dir` in the order k, j, i, then divides by the plane's cell count
+struct HAvgArgs {
+    Arr4<const double> y;  // prim, pre-offset to Y_0
+    double* avg;           // [r * ns + n]
+    int n[3], dir, ns;
+};
+static __global__ void __launch_bounds__(128) k_plot_havg(HAvgArgs a) {
+    const int npts = a.n[a.dir];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= npts * a.ns) return;
+    const int r = t / a.ns, c = t % a.ns;
+    double s = 0.0;
+    if (a.dir == 2) {
+        for (int j = 0; j < a.n[1]; ++j)
+            for (int i = 0; i < a.n[0]; ++i) s += a.y(i, j, r, c);
+    } else if (a.dir == 1) {
+        for (int k = 0; k < a.n[2]; ++k)
+            for (int i = 0; i < a.n[0]; ++i) s += a.y(i, r, k, c);
+    } else {
+        for (int k = 0; k < a.n[2]; ++k)
+            for (int j = 0; j < a.n[1]; ++j) s += a.y(r, j, k, c);
+    }
+    const int navg = a.dir == 0 ? a.n[1] * a.n[2] : (a.dir == 1 ? a.n[0] * a.n[2] : a.n[0] * a.n[1]);
+    a.avg[r * a.ns + c] = s / navg;
+}
+
+// out component c0 + n = (-average) + Y_n, block (z-plane, species) as the pack
+struct DeltaYArgs {
+    Arr4<const double> y;
+    Arr4<double> out;
+    const double* avg;
+    int n[3], dir, ns, c0;
+};
+static __global__ void __launch_bounds__(256) k_plot_deltay(DeltaYArgs a) {
+    const int c = blockIdx.y;
+    for (int k = blockIdx.x; k < a.n[2]; k += gridDim.x)
+        for (int j = 0; j < a.n[1]; ++j)
+            for (int i = threadIdx.x; i < a.n[0]; i += blockDim.x) {
+                const int r = a.dir == 0 ? i : (a.dir == 1 ? j : k);
+                a.out(i, j, k, a.c0 + c) = (-a.avg[r * a.ns + c]) + a.y(i, j, k, c);
+            }
+}
 
 // blockIdx.y: output component; blockIdx.x: z-planes (grid-stride)
 static __global__ void __launch_bounds__(256) k_plot_pack(PlotArgs a) {
@@ -129,13 +177,17 @@ static bool plot_layout(const fhd_params& prm, int flags, const fhd_fab& cu, con
         for (int s = 0; s < ns; ++s) add(m, 5 + s, numbered(("Yk" + sfx + "_").c_str(), s));
         add(m, 5 + ns, "T" + sfx);
     }
+    // plot_deltaY_dir: computed, not copied (comp -1 marks them)
+    if (flags & (FHD_PLOT_DELTAY_X | FHD_PLOT_DELTAY_Y | FHD_PLOT_DELTAY_Z))
+        for (int s = 0; s < ns; ++s) out.push_back(PlotComp{prim, -1, numbered("deltaYk_", s)});
     return (int)out.size() <= kPlotMax;
 }
 
 // a source fab must exist, cover the domain's valid region and hold the component
 static bool plot_src_ok(const fhd_params& prm, const PlotComp& pc) {
     const fhd_fab& f = pc.fab;
-    if (!f.data || f.dtype != FHD_F64 || pc.comp >= f.ncomp) return false;
+    const int need = pc.comp >= 0 ? pc.comp : 6 + prm.nspecies - 1;  // deltaY reads Y_0..Y_{ns-1} of prim
+    if (!f.data || f.dtype != FHD_F64 || need >= f.ncomp) return false;
     for (int d = 0; d < 3; ++d)
         if (f.lo[d] > 0 || f.hi[d] < prm.n_cells[d] - 1) return false;
     return true;
@@ -151,16 +203,46 @@ int plot_pack(const fhd_params& prm, int flags, fhd_fab out, const fhd_fab& cu, 
         if (out.lo[d] > 0 || out.hi[d] < prm.n_cells[d] - 1 || out.nodal[d]) return FHD_ERR_BAD_ARG;
     for (const PlotComp& pc : L)
         if (!plot_src_ok(prm, pc)) return FHD_ERR_BAD_ARG;
+    int ncopy = 0;
+    while (ncopy < (int)L.size() && L[ncopy].comp >= 0) ++ncopy;  // copies first, deltaY last
     PlotArgs a;
     std::memset(&a, 0, sizeof(a));
-    for (size_t c = 0; c < L.size(); ++c) a.src[c] = view<const double>(L[c].fab, L[c].comp);
+    for (int c = 0; c < ncopy; ++c) a.src[c] = view<const double>(L[c].fab, L[c].comp);
     a.out = view<double>(out);
     for (int d = 0; d < 3; ++d) a.n[d] = prm.n_cells[d];
-    a.ncomp = (int)L.size();
+    a.ncomp = ncopy;
     // every block of the (plane, component) grid copies at least a whole plane
     const dim3 grid((unsigned)a.n[2], (unsigned)a.ncomp);
     k_plot_pack<<<grid, 256, 0, s>>>(a);
-    return cuda_rc(cudaGetLastError());
+    int rc = cuda_rc(cudaGetLastError());
+    if (rc || ncopy == (int)L.size()) return rc;
+    // plot_deltaY_dir
+    const int dir = (flags & FHD_PLOT_DELTAY_X) ? 0 : ((flags & FHD_PLOT_DELTAY_Y) ? 1 : 2);
+    const int ns = prm.nspecies, npts = prm.n_cells[dir];
+    double* avg = nullptr;
+    if (cudaMallocAsync(reinterpret_cast<void**>(&avg), sizeof(double) * npts * ns, s) != cudaSuccess) {
+        cudaGetLastError();
+        return FHD_ERR_OOM;
+    }
+    HAvgArgs h;
+    h.y = view<const double>(prim, 6);
+    h.avg = avg;
+    for (int d = 0; d < 3; ++d) h.n[d] = prm.n_cells[d];
+    h.dir = dir;
+    h.ns = ns;
+    k_plot_havg<<<(npts * ns + 127) / 128, 128, 0, s>>>(h);
+    DeltaYArgs dy;
+    dy.y = h.y;
+    dy.out = a.out;
+    dy.avg = avg;
+    for (int d = 0; d < 3; ++d) dy.n[d] = prm.n_cells[d];
+    dy.dir = dir;
+    dy.ns = ns;
+    dy.c0 = ncopy;
+    k_plot_deltay<<<dim3((unsigned)dy.n[2], (unsigned)ns), 256, 0, s>>>(dy);
+    rc = cuda_rc(cudaGetLastError());
+    cudaFreeAsync(avg, s);
+    return rc;
 }
 
 int plot_names(const fhd_params& prm, int flags, std::vector<std::string>& names) {

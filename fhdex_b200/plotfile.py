@@ -15,11 +15,14 @@ from .capi import check
 from .fab import CELL, MultiFab
 
 MEANS, VARS, COVARS, MOM3, MOM4 = 1, 2, 4, 8, 16
+DELTAY = (32, 64, 128)   # plot_deltaY_dir = 0, 1, 2
 
 
-def flags_of(plot_means=False, plot_vars=False, plot_covars=False, plot_mom3=False, plot_mom4=False) -> int:
+def flags_of(plot_means=False, plot_vars=False, plot_covars=False, plot_mom3=False, plot_mom4=False,
+             plot_deltaY_dir=-1) -> int:
     return ((MEANS if plot_means else 0) | (VARS if plot_vars else 0) | (COVARS if plot_covars else 0)
-            | (MOM3 if plot_mom3 else 0) | (MOM4 if plot_mom4 else 0))
+            | (MOM3 if plot_mom3 else 0) | (MOM4 if plot_mom4 else 0)
+            | (DELTAY[plot_deltaY_dir] if plot_deltaY_dir in (0, 1, 2) else 0))
 
 
 def plotfile_names(p, flags: int = 0) -> list[str]:

@@ -102,6 +102,7 @@ inline int plot_vars = 0;
 inline int plot_covars = 0;
 inline int plot_mom3 = 0;
 inline int plot_mom4 = 0;
+inline int plot_deltaY_dir = -1;  // common_functions.cpp:620
 }  // namespace common
 
 namespace chemistry {
@@ -467,7 +468,7 @@ inline void MultiFabFillRandomUniform(fhd::amrex_compat::MultiFab& mf, const int
 
 // WritePlotFileStag (writePlotFileStag.cpp:7-527): the plotfile
 // <plot_base_name><step, 9 digits>/ with the common::plot_means / plot_vars /
-// plot_covars / plot_mom3 / plot_mom4 selections.  The surface-coverage
+// plot_covars / plot_mom3 / plot_mom4 / plot_deltaY_dir selections.  The surface-coverage
 // MultiFabs are accepted and ignored (no surface chemistry on this path).
 inline void WritePlotFileStag(int step, const fhd::amrex_compat::Real time, const fhd::amrex_compat::Geometry& /*geom*/,
                               const fhd::amrex_compat::MultiFab& cu, const fhd::amrex_compat::MultiFab& cuMeans,
@@ -490,7 +491,8 @@ inline void WritePlotFileStag(int step, const fhd::amrex_compat::Real time, cons
     using namespace fhd::ref;
     const int flags = (common::plot_means == 1 ? FHD_PLOT_MEANS : 0) | (common::plot_vars == 1 ? FHD_PLOT_VARS : 0) |
                       (common::plot_covars == 1 ? FHD_PLOT_COVARS : 0) | (common::plot_mom3 ? FHD_PLOT_MOM3 : 0) |
-                      (common::plot_mom4 ? FHD_PLOT_MOM4 : 0);
+                      (common::plot_mom4 ? FHD_PLOT_MOM4 : 0) |
+                      (common::plot_deltaY_dir >= 0 && common::plot_deltaY_dir < 3 ? (FHD_PLOT_DELTAY_X << common::plot_deltaY_dir) : 0);
     fhd_stats st;
     std::memset(&st, 0, sizeof(st));
     st.cuMeans = cuMeans.fab();

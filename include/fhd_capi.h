@@ -346,10 +346,15 @@ typedef struct {
  * |visc_type| == 3; then, by flag, the means, variances, covariances and third /
  * fourth moments of fhd_stats), under the reference's variable names, and its
  * single-level AMReX plotfile <plot_base_name><step, 9 digits>/ (Header,
- * Level_0/Cell_H, Level_0/Cell_D_00000).  Surface coverage and plot_deltaY_dir
- * are not covered.  Source fabs must be device-accessible (device, managed or
- * pinned host memory) and cover the valid region. */
-enum { FHD_PLOT_MEANS = 1, FHD_PLOT_VARS = 2, FHD_PLOT_COVARS = 4, FHD_PLOT_MOM3 = 8, FHD_PLOT_MOM4 = 16 };
+ * Level_0/Cell_H, Level_0/Cell_D_00000).  FHD_PLOT_DELTAY_X/Y/Z (at most one)
+ * append plot_deltaY_dir's components, Y_k minus its average over the planes
+ * normal to that direction (writePlotFileStag.cpp:282-290; WriteHorizontalAverageToMF,
+ * ComputeAverages.cpp:96-190); these take a small stream-ordered device buffer
+ * for the averages.  Surface coverage is not covered.  Source fabs must be
+ * device-accessible (device, managed or pinned host memory) and cover the valid
+ * region. */
+enum { FHD_PLOT_MEANS = 1, FHD_PLOT_VARS = 2, FHD_PLOT_COVARS = 4, FHD_PLOT_MOM3 = 8, FHD_PLOT_MOM4 = 16,
+       FHD_PLOT_DELTAY_X = 32, FHD_PLOT_DELTAY_Y = 64, FHD_PLOT_DELTAY_Z = 128 };
 /* number of plotfile components for `flags` (negative: -error code); no device */
 int fhd_plotfile_ncomp(const fhd_params* params, int flags);
 /* name of component `comp` into buf (NUL-terminated, at most buflen bytes) */

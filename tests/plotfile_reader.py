@@ -66,7 +66,7 @@ def read_cell_h(path):
     return nc, mins, maxs
 
 
-def reference_names(p, means=False, varz=False, covars=False, mom3=False, mom4=False):
+def reference_names(p, means=False, varz=False, covars=False, mom3=False, mom4=False, deltay=-1):
     """writePlotFileStag.cpp:313-447, as the reference builds its varNames."""
     ns = p.nspecies
     sp = lambda base: [base + chr(48 + i) for i in range(ns)]
@@ -93,6 +93,8 @@ def reference_names(p, means=False, varz=False, covars=False, mom3=False, mom4=F
         if on:
             v += ["rho" + sfx, "velx" + sfx, "vely" + sfx, "velz" + sfx, "rhoE" + sfx] + sp("Yk" + sfx + "_")
             v += ["T" + sfx]
+    if deltay != -1:
+        v += sp("deltaYk_")
     # nplot of writePlotFileStag.cpp:37-99
     nvars = 5 + ns
     nplot = nvars + 3 + 5 + 2 * ns + 3 + 2 + (1 if abs(p.visc_type) == 3 else 0)
@@ -100,11 +102,13 @@ def reference_names(p, means=False, varz=False, covars=False, mom3=False, mom4=F
     nplot += (nvars + 3 + 9 + ns + 3) if varz else 0
     nplot += 26 if covars else 0
     nplot += (nvars + 1) * (int(mom3) + int(mom4))
+    nplot += ns if deltay != -1 else 0
     assert len(v) == nplot
     return v
 
 
-def reference_composition(p, st, stats=None, means=False, varz=False, covars=False, mom3=False, mom4=False):
+def reference_composition(p, st, stats=None, means=False, varz=False, covars=False, mom3=False, mom4=False,
+                          deltay=-1):
     """writePlotFileStag.cpp:111-281 on the valid box: list of (ncomp, nz, ny, nx) arrays
     (MultiFab::Copy of cell components; ShiftFaceToCC copies face (i,j,k) to cell (i,j,k))."""
     ns = p.nspecies
@@ -138,4 +142,18 @@ def reference_composition(p, st, stats=None, means=False, varz=False, covars=Fal
         out += [cell(stats.mom3, c) for c in range(6 + ns)]
     if mom4:
         out += [cell(stats.mom4, c) for c in range(6 + ns)]
+    if deltay != -1:
+        # WriteHorizontalAverageToMF (ComputeAverages.cpp:96-190): per plane r the
+        # sequential sum in loop order k, j, i (np.cumsum adds one term at a time),
+        # divided by the plane's cell count; then (-average) + Y_k
+        for c in range(ns):
+            y = cell(st.prim, 6 + c)                      # (z, y, x)
+            avg = np.empty(N[deltay])
+            for r in range(N[deltay]):
+                plane = (y[:, :, r] if deltay == 0 else (y[:, r, :] if deltay == 1 else y[r, :, :])).ravel()
+                navg = plane.size
+                avg[r] = np.cumsum(plane)[-1] / navg
+            shape = [1, 1, 1]
+            shape[2 - deltay] = N[deltay]
+            out.append((-avg).reshape(shape) + y)
     return np.stack(out)

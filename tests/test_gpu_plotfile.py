@@ -33,14 +33,19 @@ def evolved(oracle, p, nsteps=3):
 
 @pytest.mark.parametrize("make,flags", [(lambda: argon((6, 5, 4), dx=8e-6), 0),
                                         (lambda: argon((6, 5, 4), dx=8e-6), ALL),
-                                        (lambda: mixture4((5, 4, 6), dx=8e-6, visc_type=3, zeta_ratio=1.0), ALL)])
+                                        (lambda: mixture4((5, 4, 6), dx=8e-6, visc_type=3, zeta_ratio=1.0), ALL),
+                                        (lambda: argon((6, 5, 4), dx=8e-6), ALL | 32),
+                                        (lambda: mixture4((7, 5, 6), dx=8e-6), MEANS | 64),
+                                        (lambda: mixture4((5, 6, 7), dx=8e-6), 128)])
 def test_pack_is_the_references_composition(oracle, make, flags):
     p = make()
     ctx, st, stats = evolved(oracle, p)
     out = pack(ctx, st, stats, flags)
     torch.cuda.synchronize()
+    dy = {32: 0, 64: 1, 128: 2}.get(flags & 224, -1)
     want = reference_composition(p, st, stats, means=bool(flags & MEANS), varz=bool(flags & VARS),
-                                 covars=bool(flags & COVARS), mom3=bool(flags & MOM3), mom4=bool(flags & MOM4))
+                                 covars=bool(flags & COVARS), mom3=bool(flags & MOM3), mom4=bool(flags & MOM4),
+                                 deltay=dy)
     got = out.arr.cpu().numpy()
     assert got.shape == want.shape
     assert np.array_equal(got, want)

@@ -20,13 +20,15 @@ CASES = [
     (argon(4), MEANS | VARS),
     (mixture4((5, 4, 3)), MEANS | VARS | COVARS | MOM3 | MOM4),
     (mixture4((3, 3, 3), visc_type=3, zeta_ratio=1.0), COVARS | MOM4),
+    (argon(4), MEANS | 64),
 ]
 
 
 @pytest.mark.parametrize("p,flags", CASES)
 def test_names_are_the_references(p, flags):
+    dy = {32: 0, 64: 1, 128: 2}.get(flags & 224, -1)
     want = reference_names(p, means=bool(flags & MEANS), varz=bool(flags & VARS), covars=bool(flags & COVARS),
-                           mom3=bool(flags & MOM3), mom4=bool(flags & MOM4))
+                           mom3=bool(flags & MOM3), mom4=bool(flags & MOM4), deltay=dy)
     assert plotfile_names(p, flags) == want
 
 
@@ -57,7 +59,8 @@ def test_bad_flags_are_rejected():
     from fhdex_b200 import capi
     import ctypes as C
     cp = argon(4).to_c()
-    assert capi.load().fhd_plotfile_ncomp(C.byref(cp), 32) == -capi.FHD_ERR_BAD_ARG
+    assert capi.load().fhd_plotfile_ncomp(C.byref(cp), 256) == -capi.FHD_ERR_BAD_ARG
+    assert capi.load().fhd_plotfile_ncomp(C.byref(cp), 32 | 64) == -capi.FHD_ERR_BAD_ARG  # two deltaY directions
 
 
 def test_plotfile_directory_parents_are_created(tmp_path):
