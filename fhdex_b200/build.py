@@ -40,6 +40,7 @@ def _units():
     u.append(("chem", "fhd_chem.cu", ["-fmad=false"]))
     u.append(("plot", "fhd_plot.cu", ["-fmad=false"]))
     u.append(("chk", "fhd_chk.cu", []))
+    u.append(("peak", "fhd_peak.cu", []))
     return u
 
 

@@ -153,6 +153,7 @@ def _declare(lib):
         "fhd_tile_name": (C.c_char_p, [i]),
         "fhd_profile": (i, [vp, i]),
         "fhd_profile_read": (i, [vp, P(d), P(C.c_int64)]),
+        "fhd_measure_fma_peak": (i, [i, i, P(d)]),
         "fhd_rk3_step_stag_noalloc": (i, [P(FhdParams), fab, pfab, fab, pfab, d, C.c_int64, vp, P(i)]),
         "fhd_stats_stag": (i, [vp, fab, fab, pfab, pfab, P(FhdStats), C.c_int64, i]),
         "fhd_sf_create": (i, [P(vp), P(i), i, i, P(i), P(i), P(d), i]),

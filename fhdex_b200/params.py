@@ -73,6 +73,10 @@ class Params:
     def replace(self, **kw):
         return dataclasses.replace(self, **kw)
 
+    def to_inputs(self) -> str:
+        """This parameter set as an FHDeX inputs deck (see ``to_inputs``)."""
+        return to_inputs(self)
+
     def hc(self):
         """(hcv, hcp) as GetHcGas derives them (compressible_functions.cpp:91-100)."""
         hcv, hcp = [], []
@@ -231,6 +235,49 @@ def stable_dt(p: Params, cfl=0.2, diff=0.1):
         eta, kappa = hard_sphere_single_gas(q)
         dmax = max(dmax, eta / p.rho0, kappa / (p.rho0 * cv))
     return min(cfl * dx / c, diff * dx * dx / dmax)
+
+
+def _fmt(v) -> str:
+    return repr(float(v)) if isinstance(v, float) else str(v)
+
+
+def to_inputs(p: "Params") -> str:
+    """``p`` as an FHDeX inputs deck with the reference's key names
+    (common_functions.cpp:257-1010, compressible_functions.cpp:15-88,
+    chemistry_functions.cpp:45-124): fully periodic, two ghost cells,
+    prob_type 1, nvars / nprimvars as main_driver.cpp:47-53 requires them.
+    Floats are written in their shortest round-trip form, so a reader that
+    parses decimal to the nearest double gets every value back exactly;
+    ``parse_inputs`` reads the deck back into the same parameters."""
+    ns = p.nspecies
+
+    def row(key, vals):
+        return f"{key} = " + " ".join(_fmt(float(x)) if not isinstance(x, int) else str(x) for x in vals)
+
+    lines = [f"nspecies = {ns}", row("n_cells", [int(x) for x in p.n_cells]), row("prob_lo", p.prob_lo),
+             row("prob_hi", p.prob_hi), f"ngc = {p.ngc} {p.ngc} {p.ngc}", f"nvars = {p.nvars}",
+             f"nprimvars = {p.nprimvars}", row("molmass", p.molmass[:ns]), row("diameter", p.diameter[:ns]),
+             row("dof", p.dof[:ns]), row("e0", p.e0[:ns]), row("hcv", p.hcv[:ns]), row("hcp", p.hcp[:ns]),
+             row("rhobar", p.rhobar[:ns]), f"rho0 = {_fmt(float(p.rho0))}", f"T_init = {_fmt(float(p.T_init))}",
+             f"k_B = {_fmt(float(p.k_B))}", f"Runiv = {_fmt(float(p.Runiv))}", row("grav", p.grav),
+             f"algorithm_type = {p.algorithm_type}", f"visc_type = {p.visc_type}",
+             f"advection_type = {p.advection_type}", f"transport_type = {p.transport_type}",
+             f"stoch_stress_form = {p.stoch_stress_form}", f"seed = {p.seed}", "prob_type = 1"]
+    if p.zeta_ratio >= 0:
+        lines.append(f"zeta_ratio = {_fmt(float(p.zeta_ratio))}")
+    for key in ("bc_vel_lo", "bc_vel_hi", "bc_mass_lo", "bc_mass_hi", "bc_therm_lo", "bc_therm_hi"):
+        lines.append(f"{key} = -1 -1 -1")
+    if p.nreaction > 0:
+        nr = p.nreaction
+        lines += [f"nreaction = {nr}", f"reaction_type = {p.reaction_type}"]
+        for m in range(nr):
+            lines.append(row(f"stoich_{m + 1}R", [int(x) for x in p.stoich_R[m][:ns]]))
+            lines.append(row(f"stoich_{m + 1}P", [int(x) for x in p.stoich_P[m][:ns]]))
+        lines += [row("rate_const", p.rate_const[:nr]), row("alpha_param", (list(p.alpha_param) + [0.0] * nr)[:nr]),
+                  row("beta_param", (list(p.beta_param) + [0.0] * nr)[:nr]), f"T0_chem = {_fmt(float(p.T0_chem))}"]
+    if p.avogadro > 0:
+        lines.append(f"avogadro = {_fmt(float(p.avogadro))}")
+    return "\n".join(lines) + "\n"
 
 
 _LIST_KEYS = ("n_cells", "prob_lo", "prob_hi", "molmass", "diameter", "dof", "e0", "hcv",

@@ -278,6 +278,13 @@ int fhd_rk3_step_stag_host(fhd_ctx* ctx, fhd_fab cu, const fhd_fab mom[3], fhd_f
 int fhd_profile(fhd_ctx* ctx, int enable);
 int fhd_profile_read(fhd_ctx* ctx, double* ms, int64_t* launches);
 
+/* FMA throughput of `device` in TFLOP/s (2 flops per fma), FP64 (fp64 != 0) or
+ * FP32: the best of five timed launches of independent fma chains over a whole
+ * number of waves (CUDA events).  The compute denominator of the step's
+ * roofline beside the measured HBM bandwidth.  Changes no device setting.  No
+ * reference counterpart. */
+int fhd_measure_fma_peak(int device, int fp64, double* tflops);
+
 /* ---- ensembles and served runs (no reference counterpart: the reference runs one
  * simulation per process) ------------------------------------------------------
  * A batch advances many independent runs of one species count and precision
@@ -440,10 +447,12 @@ int fhd_sf_finalize(fhd_sf* sf, fhd_fab cov_real, fhd_fab cov_imag, fhd_fab cov_
  *
  * Same step as fhd_rk3_step_stag with FP64 precision, in-kernel Philox noise
  * (or none when stoch_stress_form == 0) and no by-product outputs, on the
- * caller's stream (NULL = legacy default stream).  Its stage scratch is a
+ * caller's stream (NULL = legacy default stream).  cu, mom, prim and vel must
+ * be device memory of the CURRENT device (checked: FHD_ERR_BAD_ARG otherwise),
+ * with one ghost width >= 2 per fab, as fhd_rk3_step_stag accepts.  Its stage scratch is a
  * file-scope 16 MiB device array held by every GPU that loads the library until
- * the process exits; boxes whose scratch does not fit (about 28^3 cells with 2
- * species, 24^3 with 4) return FHD_ERR_TOO_LARGE before any GPU work.  The first
+ * the process exits; boxes whose scratch does not fit (the largest cubes that fit: 29^3
+ * cells with 2 species, 26^3 with 4) return FHD_ERR_TOO_LARGE before any GPU work.  The first
  * call on a device looks up the array's device address (cudaGetSymbolAddress,
  * that device current): make it before any stream capture.  Calls share the
  * array and it keeps the last call's contents, so calls whose GPU work overlaps

@@ -6,10 +6,12 @@
 // single fully periodic box, following the reference operator by operator and
 // keeping its floating-point operation order (build with -ffp-contract=off so
 // a*b+c is never fused).  Every function cites the reference lines it follows.
-// The reference itself needs AMReX (not vendored, no network) and cannot be
-// built here; the oracle is pinned instead by the reference's known-answer
-// formulas (closed-form hard-sphere transport, exact conservation, equilibrium
-// variances) in tests/.
+// The reference application needs AMReX (not vendored, no network), but its
+// hot-path sources compile unmodified against the host-only AMReX stand-in in
+// oracle/amrex_host (oracle/_ref, recipe in oracle/Makefile); tests/
+// test_reference_pin.py holds this restatement bit for bit to that build, and
+// tests/ also check it against the reference's known-answer formulas
+// (closed-form hard-sphere transport, exact conservation, equilibrium variances).
 //
 // Scope: periodic boundaries (every physical-BC routine on the path is then a
 // no-op: boundaryStag.cpp:5-14, 1555-1557), 3D, algorithm_type 2,

@@ -1,0 +1,229 @@
+"""ctypes front end of oracle/_ref/libfhd_ref.so (TEST INFRASTRUCTURE ONLY).
+
+The library is FHDeX's own hot-path sources (timeStepStag.cpp, fluxStag.cpp,
+conservedPrimitiveConversionsStag.cpp, transCoeffs.cpp, boundaryStag.cpp,
+compressible_functions*.cpp, MultiFabFillRandom.cpp, chemistry_functions.cpp,
+common_functions.cpp, reservoirStag.cpp) compiled unmodified against the
+host-only AMReX stand-in in ``oracle/amrex_host`` (recipe: ``make -C oracle
+ref``), with ``oracle/ref_driver.cpp`` as its C ABI.  The tests run it beside
+the restated oracle (``oracle/fhd_oracle.cpp``) on the same inputs to pin the
+restatement to the reference's code.  It is built where the reference tree
+exists; the built library travels with the repository to machines without it.
+
+Functions take host MultiFabs from ``fhdex_b200.state`` (the geometry the
+reference's main_driver gives them) and a ``Params`` whose ``to_inputs()`` deck
+the reference's own namespace initialisers read.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+import subprocess
+
+import torch
+
+_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(_DIR, "_ref", "libfhd_ref.so")
+REF_TREE = os.environ.get("FHD_REFERENCE_TREE", "/root/reference")
+_lib = None
+_params = None
+
+
+def build():
+    """Compile the reference sources where the reference tree exists."""
+    if os.path.isdir(REF_TREE):
+        subprocess.check_call(["make", "-s", "-C", _DIR, "ref", f"REF={REF_TREE}", f"-j{os.cpu_count() or 4}"])
+
+
+def available() -> bool:
+    return os.path.exists(LIB)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        P = C.POINTER
+        d, i, vp = C.c_double, C.c_int, C.c_void_p
+        pp = P(vp)
+        L.fhdref_error.restype = C.c_char_p
+        L.fhdref_init.argtypes = [C.c_char_p]
+        L.fhdref_globals.argtypes = [P(i), P(i), P(i), P(i), P(d), P(d), P(i)]
+        L.fhdref_init_cons_var_stag.argtypes = [vp, pp]
+        L.fhdref_conserved_to_primitive.argtypes = [vp, pp, vp, pp]
+        L.fhdref_set_bc.argtypes = [vp, vp, pp, pp]
+        L.fhdref_transport.argtypes = [vp] * 6
+        L.fhdref_flux.argtypes = [vp, pp, vp, pp, vp, vp, vp, vp, vp, pp, pp, pp, pp, pp, pp, d, d, d]
+        L.fhdref_rk3_step.argtypes = [vp, pp, vp, pp, vp, vp, vp, vp, vp, vp, pp, pp, pp, vp, pp, pp, d, i]
+        L.fhdref_noise_log.argtypes = [P(i), P(i), P(d), i]
+        L.fhdref_chemistry_source.argtypes = [d, d, vp, vp, vp]
+        L.fhdref_max_acoustic_cfl.argtypes = [vp, pp, d, P(d)]
+        _lib = L
+    return _lib
+
+
+def _chk(rc, what):
+    if rc != 0:
+        raise RuntimeError(f"reference {what}: {lib().fhdref_error().decode()}")
+
+
+def _ptr(t: torch.Tensor):
+    assert t.device.type == "cpu" and t.dtype == torch.float64 and t.is_contiguous()
+    return C.c_void_p(t.data_ptr())
+
+
+def _ptrs(tensors):
+    arr = (C.c_void_p * len(tensors))()
+    for q, t in enumerate(tensors):
+        arr[q] = None if t is None else _ptr(t).value
+    return arr
+
+
+def init(p):
+    """Read ``p``'s deck through the reference's namespace initialisers."""
+    global _params
+    if _params is not p:
+        _chk(lib().fhdref_init(p.to_inputs().encode()), "init")
+        _params = p
+
+
+def globals_(p):
+    """(nspecies, nvars, nprimvars, ngc, hcv[:ns], hcp[:ns], nreaction) as the
+    reference derives them (GetHcGas, compressible_functions.cpp:91-100)."""
+    init(p)
+    ns, nv, npv, ng, nr = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    hv = (C.c_double * 8)()
+    hp = (C.c_double * 8)()
+    _chk(lib().fhdref_globals(C.byref(ns), C.byref(nv), C.byref(npv), C.byref(ng), hv, hp, C.byref(nr)), "globals")
+    return ns.value, nv.value, npv.value, ng.value, list(hv[:ns.value]), list(hp[:ns.value]), nr.value
+
+
+def init_cons_var_stag(st):
+    init(st.p)
+    _chk(lib().fhdref_init_cons_var_stag(_ptr(st.cu.arr), _ptrs([m.arr for m in st.cumom])), "InitConsVarStag")
+
+
+def conserved_to_primitive(st):
+    init(st.p)
+    _chk(lib().fhdref_conserved_to_primitive(_ptr(st.prim.arr), _ptrs([m.arr for m in st.vel]), _ptr(st.cu.arr),
+                                             _ptrs([m.arr for m in st.cumom])), "conservedToPrimitiveStag")
+
+
+def set_bc(st):
+    init(st.p)
+    _chk(lib().fhdref_set_bc(_ptr(st.prim.arr), _ptr(st.cu.arr), _ptrs([m.arr for m in st.cumom]),
+                             _ptrs([m.arr for m in st.vel])), "setBCStag")
+
+
+def transport(st):
+    init(st.p)
+    _chk(lib().fhdref_transport(_ptr(st.prim.arr), _ptr(st.eta.arr), _ptr(st.zeta.arr), _ptr(st.kappa.arr),
+                                _ptr(st.chi.arr), _ptr(st.D.arr)), "calculateTransportCoeffs")
+
+
+def _ref_edges(e3):
+    """The reference's six edge MultiFabs (edgeflux_x = {xy, xz}, _y = {xy, yz},
+    _z = {xz, yz}) from the three distinct noise fields xy, xz, yz.  The
+    reference's flux reads only x[0], x[1] and y[1]; the other three get the
+    negated fields, so that a read of them would show as a mismatch."""
+    xy, xz, yz = e3
+    return [xy, xz, (-xy).contiguous(), yz, (-xz).contiguous(), (-yz).contiguous()]
+
+
+def flux(st, sf, se, sc, dt, w1=1.0, w2=0.0):
+    """calculateFluxStag with the weighted noise W: sf[3] face fields (nspecies+1
+    comps: energy, species), se[3] edge fields (xy, xz, yz), sc[3] centre fields
+    (one ghost), host MultiFabs in the layout of fhdex_b200.state.StepNoise.
+    The reference's face noise MultiFab has nvars components with the energy at
+    component 4; the first four are left zero."""
+    init(st.p)
+    nv = st.p.nvars
+    faces = []
+    for d in range(3):
+        f = torch.zeros((nv,) + tuple(sf[d].arr.shape[1:]), dtype=torch.float64)
+        f[4:] = sf[d].arr
+        faces.append(f)
+    edges = _ref_edges([m.arr for m in se])
+    _chk(lib().fhdref_flux(_ptr(st.cu.arr), _ptrs([m.arr for m in st.cumom]), _ptr(st.prim.arr),
+                           _ptrs([m.arr for m in st.vel]), _ptr(st.eta.arr), _ptr(st.zeta.arr), _ptr(st.kappa.arr),
+                           _ptr(st.chi.arr), _ptr(st.D.arr), _ptrs([m.arr for m in st.faceflux]),
+                           _ptrs([m.arr for m in st.edgeflux]), _ptrs([m.arr for m in st.cenflux]), _ptrs(faces),
+                           _ptrs(edges), _ptrs([m.arr for m in sc]), w1, w2, dt), "calculateFluxStag")
+
+
+def step_normals(noise):
+    """The 24 fields of RK3stepStag's MultiFabFillRandomNormal calls, in the
+    reference's order (timeStepStag.cpp:183-222), from a StepNoise (face[s][d]:
+    energy + species comps; edge[s][e]: xy, xz, yz; cen[s][d]: one ghost)."""
+    out = []
+    for d in range(3):
+        out += [noise.face[0][d].arr, noise.face[1][d].arr]
+    eA = _ref_edges([m.arr for m in noise.edge[0]])
+    eB = _ref_edges([m.arr for m in noise.edge[1]])
+    for i in range(2):
+        for e in (i, 2 + i, 4 + i):  # stochedge_x[i], _y[i], _z[i]
+            out += [eA[e], eB[e]]
+    for d in range(3):
+        out += [noise.cen[0][d].arr, noise.cen[1][d].arr]
+    return out
+
+
+def rk3_step(st, noise, dt, step=0):
+    """RK3stepStag with the step's noise injected from ``noise`` (StepNoise).
+    Returns the log of the 24 noise fills: (scomp, ncomp, mean, stddev, nodal)."""
+    init(st.p)
+    normals = step_normals(noise)
+    chem = []
+    nr = st.p.nreaction
+    for m in range(nr):
+        for s in range(2):
+            chem.append(noise.chem[s].arr[m].contiguous())
+    _chk(lib().fhdref_rk3_step(_ptr(st.cu.arr), _ptrs([m.arr for m in st.cumom]), _ptr(st.prim.arr),
+                               _ptrs([m.arr for m in st.vel]), _ptr(st.source.arr), _ptr(st.eta.arr),
+                               _ptr(st.zeta.arr), _ptr(st.kappa.arr), _ptr(st.chi.arr), _ptr(st.D.arr),
+                               _ptrs([m.arr for m in st.faceflux]), _ptrs([m.arr for m in st.edgeflux]),
+                               _ptrs([m.arr for m in st.cenflux]),
+                               _ptr(noise_ranchem(st)) if nr > 0 else None, _ptrs(normals),
+                               _ptrs(chem) if nr > 0 else None, dt, step), "RK3stepStag")
+    return noise_log()
+
+
+def noise_ranchem(st):
+    """The caller's ranchem MultiFab (nreaction comps, ngc ghosts), as main_driver.cpp:1006-1007 defines it."""
+    if getattr(st, "_ref_ranchem", None) is None:
+        from fhdex_b200.fab import CELL, MultiFab
+        st._ref_ranchem = MultiFab(st.p.n_cells, CELL, st.p.nreaction, st.p.ngc).arr
+    return st._ref_ranchem
+
+
+def noise_log():
+    n = C.c_int()
+    ints = (C.c_int * (11 * 64))()
+    reals = (C.c_double * (2 * 64))()
+    lib().fhdref_noise_log(C.byref(n), ints, reals, 64)
+    out = []
+    for q in range(n.value):
+        o = ints[11 * q: 11 * q + 11]
+        out.append(dict(scomp=o[0], ncomp=o[1], lo=tuple(o[2:5]), hi=tuple(o[5:8]), nodal=tuple(o[8:11]),
+                        mean=reals[2 * q], stddev=reals[2 * q + 1]))
+    return out
+
+
+def chemistry_source(p, dt, dV, prim, source, ranchem):
+    init(p)
+    _chk(lib().fhdref_chemistry_source(dt, dV, _ptr(prim.arr), _ptr(source.arr), _ptr(ranchem.arr)),
+         "compute_compressible_chemistry_source_CLE")
+
+
+def max_acoustic_cfl(st, dt):
+    init(st.p)
+    out = C.c_double()
+    _chk(lib().fhdref_max_acoustic_cfl(_ptr(st.prim.arr), _ptrs([m.arr for m in st.vel]), dt, C.byref(out)),
+         "GetMaxAcousticCFL")
+    return out.value
+
+
+SQRT2 = math.sqrt(2.0)

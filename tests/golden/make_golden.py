@@ -2,8 +2,8 @@
 repository root: ``python -m tests.golden.make_golden [case ...]``).
 
 The reference holds no stored outputs for this path (its regression decks have
-no golden files and it cannot be built here), so the fixtures freeze the CPU
-oracle's results on small boxes, with noise drawn on the host from
+no golden files), so the fixtures freeze the CPU oracle's results on small
+boxes, with noise drawn on the host from
 std::mt19937_64 and Box-Muller (``oracle.fill_noise_mt64``):
 
   * ``<case>.npz``: parameters and dt (``meta``, JSON), the input state
@@ -14,8 +14,10 @@ std::mt19937_64 and Box-Muller (``oracle.fill_noise_mt64``):
   * ``MANIFEST.json``: SHA-256 of every array, so a changed fixture or a
     drifted oracle is caught.
 
-The oracle itself is pinned by the reference's known answers (closed-form GIO
-coefficients, equilibrium variances, conservation) in tests/test_oracle.py; the
+The reference's own hot-path sources, compiled unmodified into oracle/_ref,
+reproduce every fixture bit for bit (tests/test_reference_pin.py); the oracle
+is also checked against the reference's known answers (closed-form GIO
+coefficients, equilibrium variances, conservation) in tests/test_oracle.py.  The
 fixtures let the GPU tests check the CUDA path without running the oracle and
 guard the oracle against silent drift.
 """
