@@ -27,7 +27,8 @@ using namespace fhd;
 
 namespace {
 
-// 16 MiB: room for a 24^3 box with 4 species or a 28^3 box with 2 species.
+// 16 MiB: room for a 26^3 box with 4 species or a 29^3 box with 2 species
+// (30x30x29 with 2 species leaves 48 KiB unused).
 constexpr size_t kNoallocBytes = (size_t)16 << 20;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
 
@@ -73,11 +74,23 @@ fhd_fab box(const int n[3], const int nodal[3], int ng, int nc, int dtype) {
     return f;
 }
 
-bool same_geometry(const fhd_fab& f, const int n[3], const int nodal[3], int ng, int min_nc) {
+// A caller's fab: FP64, at least min_nc components, the same ghost width g >= min_ng
+// on every side (the kernels take each fab's own lo, as fhd_rk3_step_stag does).
+bool same_geometry(const fhd_fab& f, const int n[3], const int nodal[3], int min_ng, int min_nc) {
     if (!f.data || f.dtype != FHD_F64 || f.ncomp < min_nc) return false;
+    const int g = -f.lo[0];
+    if (g < min_ng) return false;
     for (int d = 0; d < 3; ++d)
-        if (f.lo[d] != -ng || f.hi[d] != n[d] - 1 + nodal[d] + ng || f.nodal[d] != nodal[d]) return false;
+        if (f.lo[d] != -g || f.hi[d] != n[d] - 1 + nodal[d] + g || f.nodal[d] != nodal[d]) return false;
     return points(f) * f.ncomp < ((int64_t)1 << 31);
+}
+
+// Every caller fab must be device memory of the current device: the kernels
+// run there and would otherwise mix two devices' memory.
+bool on_current_device(const fhd_fab& f, int dev) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, f.data) != cudaSuccess) { cudaGetLastError(); return false; }
+    return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == dev;
 }
 
 // carves fabs out of the static scratch, 256-byte aligned
@@ -115,6 +128,13 @@ extern "C" int fhd_rk3_step_stag_noalloc(const fhd_params* params, fhd_fab cu, c
     for (int d = 0; d < 3; ++d)
         if (!same_geometry(mom[d], n, face[d], 2, 1) || !same_geometry(vel[d], n, face[d], 2, 1))
             return FHD_ERR_BAD_ARG;
+    {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return FHD_ERR_CUDA; }
+        const fhd_fab* own[8] = {&cu, &prim, &mom[0], &mom[1], &mom[2], &vel[0], &vel[1], &vel[2]};
+        for (const fhd_fab* f : own)
+            if (!on_current_device(*f, dev)) return FHD_ERR_BAD_ARG;
+    }
 
     // scratch layout (sizes only first: reject what does not fit before touching the GPU)
     fhd_fab st = box(n, cell, 0, 1, FHD_F64);   // status word
