@@ -86,7 +86,7 @@ class FhdNoise(C.Structure):
     ]
 
 
-PROF_KINDS = ("cellprep", "taus", "faces", "update", "ghosts", "convert", "aux_fluxes")
+PROF_KINDS = ("cellprep", "taus", "faces", "update", "ghosts", "convert", "aux_fluxes", "fused")
 
 FabArr3 = FhdFab * 3
 FabArr6 = FhdFab * 6

@@ -722,9 +722,14 @@ static int step_launches(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab p
             rc = exact_aux_fluxes(sc);
             if (rc) return rc;
         }
-        for (int part = 0; part < 3 && !rc; ++part) {
-            ProfScope ps(c, 1 + part);
-            rc = mixed ? mixed_stage_part(sc, part) : exact_stage_part(sc, part);
+        if (tile_fused(c->tile)) {
+            ProfScope ps(c, 7);
+            rc = mixed ? mixed_stage_part(sc, 3) : exact_stage_part(sc, 3);
+        } else {
+            for (int part = 0; part < 3 && !rc; ++part) {
+                ProfScope ps(c, 1 + part);
+                rc = mixed ? mixed_stage_part(sc, part) : exact_stage_part(sc, part);
+            }
         }
         if (rc) return rc;
         GhostReq g[5] = {{*outs[s], 0, 1}, {*outs[s], 4, 1 + ns}, {outsm[s][0], 0, 1}, {outsm[s][1], 0, 1},

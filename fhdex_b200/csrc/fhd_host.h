@@ -119,7 +119,7 @@ struct StageCall {
 
 // exact (FP64) translation unit
 int exact_cellprep(const StageCall& c);
-int exact_stage_part(const StageCall& c, int part);  // 0 stresses, 1 face fluxes, 2 update
+int exact_stage_part(const StageCall& c, int part);  // 0 stresses, 1 face fluxes, 2 update, 3 fused (all three)
 int exact_aux_fluxes(const StageCall& c);
 int exact_transport(const DevParams& P, fhd_fab prim, fhd_fab eta, fhd_fab zeta, fhd_fab kappa, fhd_fab chi,
                     fhd_fab D, int* status, cudaStream_t s);
@@ -172,5 +172,6 @@ int steps_set(uint64_t* step, uint64_t v, cudaStream_t s);
 
 int num_tiles();
 const char* tile_name(int t);
+bool tile_fused(int t);  // the tile selects the fused stage kernel (stage part 3)
 
 }  // namespace fhd

@@ -2,6 +2,7 @@
 #pragma once
 #include "fhd_host.h"
 #include "fhd_kernels.cuh"
+#include "fhd_fused.cuh"
 
 namespace fhd {
 
@@ -133,6 +134,13 @@ int launch_cellprep(const StageCall& c) {
 constexpr int kStageBlocks[] = {128, 256, 128, 128, 128};
 constexpr int kFaceMinBlocks[] = {4, 2, 6, 10, 8};  // as instantiated in launch_stage_part_t
 constexpr int kNumStageBlocks = 5;
+// the fused stage kernel (k_stage_zm): tile of 16 x 8 cells; per fused tile the
+// block size (128, 256 or 384 threads over the same tile) and the z-chunk depth
+constexpr int kZmTX = 16, kZmTY = 8;
+constexpr int kZmThreads[] = {128, 256, 256, 384};
+constexpr int kZmChunks[] = {32, 32, 64, 32};
+constexpr int kNumZmTiles = 4;
+inline bool tile_is_fused(int t) { return t >= kNumStageBlocks && t < kNumStageBlocks + kNumZmTiles; }
 
 template <int NS, class R, int NZ>
 StageArgs<NS, R, NZ> make_stage_args(const StageCall& c) {
@@ -194,8 +202,58 @@ int launch_stage_part_t(const StageCall& c, int part) {
     return cuda_rc(cudaGetLastError());
 }
 
+// resident blocks per SM asked of the register allocator: the shared memory of a
+// 16 x 8 tile (56-80 KB) holds 2-4 blocks per SM
+template <int NS, class R>
+constexpr int zm_min_blocks(int bt) {
+    return bt == 128 ? (sizeof(R) == 8 ? (NS <= 2 ? 3 : 2) : (NS <= 2 ? 4 : 3)) : (bt == 256 ? (NS <= 2 ? 3 : 2) : 2);
+}
+
+template <int NS, class R, int NZ, int BT>
+int launch_stage_zm_bt(const StageCall& c, int zc) {
+    constexpr int TX = kZmTX, TY = kZmTY;
+    constexpr size_t smem = ZmSmem<NS, R, TX, TY>::bytes;
+    auto kern = k_stage_zm<NS, R, NZ, TX, TY, BT, zm_min_blocks<NS, R>(BT)>;
+    // the dynamic shared memory above 48 KiB is opted into per device, once
+    static bool set[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return FHD_ERR_CUDA; }
+    if (dev < 0 || dev >= 64) return FHD_ERR_UNSUPPORTED;
+    if (!set[dev]) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+            cudaGetLastError();
+            return FHD_ERR_CUDA;
+        }
+        set[dev] = true;
+    }
+    const StageArgs<NS, R, NZ> a = make_stage_args<NS, R, NZ>(c);
+    const int* N = c.P.n;
+    const dim3 grid((N[0] + TX - 1) / TX, (N[1] + TY - 1) / TY, (N[2] + zc - 1) / zc);
+    kern<<<grid, BT, smem, c.stream>>>(a, zc);
+    return cuda_rc(cudaGetLastError());
+}
+
+template <int NS, class R, int NZ>
+int launch_stage_zm_t(const StageCall& c) {
+    const int t = tile_is_fused(c.tile) ? c.tile - kNumStageBlocks : 0;
+    switch (kZmThreads[t]) {
+        case 256: return launch_stage_zm_bt<NS, R, NZ, 256>(c, kZmChunks[t]);
+        case 384: return launch_stage_zm_bt<NS, R, NZ, 384>(c, kZmChunks[t]);
+        default: return launch_stage_zm_bt<NS, R, NZ, 128>(c, kZmChunks[t]);
+    }
+}
+
+// part: 0 stresses, 1 face fluxes, 2 update, 3 the fused kernel (all three)
 template <int NS, class R>
 int launch_stage_part(const StageCall& c, int part) {
+    if (part == 3) {
+        switch (c.mode) {
+            case NM_OFF: return launch_stage_zm_t<NS, R, NZ_OFF>(c);
+            case NM_AB: return launch_stage_zm_t<NS, R, NZ_AB>(c);
+            case NM_PHILOX: return launch_stage_zm_t<NS, R, NZ_PHILOX>(c);
+            default: return FHD_ERR_BAD_ARG;
+        }
+    }
     switch (c.mode) {
         case NM_OFF: return launch_stage_part_t<NS, R, NZ_OFF>(c, part);
         case NM_AB: return launch_stage_part_t<NS, R, NZ_AB>(c, part);

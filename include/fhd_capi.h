@@ -271,10 +271,11 @@ int fhd_rk3_step_stag_host(fhd_ctx* ctx, fhd_fab cu, const fhd_fab mom[3], fhd_f
  * (tracing aid in place of the reference's TinyProfiler regions).  Kinds:
  * 0 cellprep (conversion + transport), 1 stresses, 2 face fluxes (the three
  * per-direction launches together), 3 divergence/RK update, 4 ghost fill,
- * 5 final conversion, 6 by-product fluxes.  fhd_profile_read synchronizes, sums
- * the elapsed times (ms) and bracketed launches per kind since the last read,
- * and resets. */
-#define FHD_PROF_KINDS 7
+ * 5 final conversion, 6 by-product fluxes, 7 the fused stage kernel (stresses,
+ * face fluxes and update in one launch, when the tile selects it).
+ * fhd_profile_read synchronizes, sums the elapsed times (ms) and bracketed
+ * launches per kind since the last read, and resets. */
+#define FHD_PROF_KINDS 8
 int fhd_profile(fhd_ctx* ctx, int enable);
 int fhd_profile_read(fhd_ctx* ctx, double* ms, int64_t* launches);
 
