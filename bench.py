@@ -52,14 +52,17 @@ UNIT = "cell-updates/s"
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one RK stage
 # (k_cellprep + k_taus + 3 x k_faces + k_update) per cell, keyed
-# "nspecies:precision": one ncu capture of a full timed step at 128^3 (the
-# summary in profiles/stage_traffic_argon128.md), scaled to the box by the cell
-# count.  Absent for configurations not captured.
-STAGE_TRAFFIC_BYTES_PER_CELL = {"2:fp64": 1499.8, "2:mixed": 1232.5}
+# "nspecies:precision": ncu, 128^3, one full timed step captured, scaled to the
+# box by the cell count (every operand exceeds L2 at both sizes).  Absent for
+# configurations not captured.
+STAGE_TRAFFIC_BYTES_PER_CELL = {"2:fp64": 1592.1, "2:mixed": 1232.5}
 # DRAM traffic of one statistics update per cell (all flags), keyed "nspecies":
-# ncu capture of the three statistics kernels at 128^3 (the summary in
-# profiles/stats_argon128.md), scaled by the cell count.
+# ncu, 128^3, the three statistics kernels captured, scaled by the cell count.
 STATS_TRAFFIC_BYTES_PER_CELL = {"2": 1639.1}
+# FP64 flops of one RK stage per cell (dadd + dmul + 2 x dfma thread instructions
+# of k_cellprep, k_taus, 3 x k_faces and k_update; ncu at 128^3, divided by the
+# cells), keyed "nspecies:precision".
+STAGE_FP64_FLOPS_PER_CELL = {"2:fp64": 3042.4}
 
 
 def measured_peak():
@@ -329,6 +332,160 @@ def autotune(ctx, st, dt, steps=2):
     return best[0], best[1], best[2], table
 
 
+def fma_peaks(device):
+    """FP64 / FP32 FMA throughput of this GPU, measured now (fhd_measure_fma_peak),
+    with the committed measurement (MEASURED_FMA.json) beside it."""
+    from fhdex_b200.peaks import measure_fma_peaks
+    try:
+        live = measure_fma_peaks(device)
+    except Exception as e:  # pragma: no cover - reported, not fatal
+        live = {"error": repr(e)}
+    committed = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_FMA.json")) as f:
+            committed = json.load(f)
+    except Exception:
+        pass
+    return live, committed
+
+
+def step_extras(args, p, dt, local, peak, peak_kind):
+    """The forms the benchmark's metric compares, measured in the same call after
+    the headline step (untimed for the headline): the 256^3 step in the mixed
+    precision, the FP64 step with its by-products (aux), the batched ensemble and
+    the continuous-batching server, each against the plain FP64 one-at-a-time
+    path of the same call, and the batched mixed form's equilibrium variances."""
+    import torch
+    from fhdex_b200.context import Context
+    from fhdex_b200.state import StagState
+    out = {}
+    cells = p.n_cells[0] * p.n_cells[1] * p.n_cells[2]
+    S = 5 + p.nspecies
+
+    def timed(ctx, st, nsteps, aux=False):
+        for s in range(2):
+            ctx.rk3_step(st, dt, s, aux=aux)
+        torch.cuda.synchronize()
+        ctx.profile(True)
+        ctx.profile_read()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for s in range(nsteps):
+            ctx.rk3_step(st, dt, 2 + s, aux=aux)
+        e1.record()
+        torch.cuda.synchronize()
+        prof = ctx.profile_read()
+        ctx.profile(False)
+        return e0.elapsed_time(e1) / nsteps, prof
+
+    # the same step with the by-products RK3stepStag writes (coefficients, fluxes)
+    ctx = Context(p, local)
+    st = StagState(p, f"cuda:{local}", aux=True)
+    ctx.init_state(st)
+    t, _, tname, _ = autotune(ctx, st, dt)
+    ms_aux, _ = timed(ctx, st, 3, aux=True)
+    out["aux_true"] = {"ms_per_step": ms_aux, "value": cells / (ms_aux / 1e3), "tile": tname,
+                       "writes": "stage-3 eta, zeta, kappa, chi, D, face/edge/centre fluxes (the reference's "
+                                 "RK3stepStag outputs besides the state)"}
+    ctx.close()
+    del st
+    torch.cuda.empty_cache()
+
+    # the mixed-precision step on the same box
+    pm = p.replace(precision=1)
+    ctx = Context(pm, local)
+    st = StagState(pm, f"cuda:{local}", aux=False)
+    ctx.init_state(st)
+    t, _, tname, _ = autotune(ctx, st, dt)
+    ms_mx, prof = timed(ctx, st, max(3, min(args.steps, 10)))
+    stage_ms = sum(prof[k][0] for k in ("cellprep", "taus", "faces", "update", "fused"))
+    nst = max(prof["taus"][1] + prof["fused"][1], 1)
+    ach = (2 + 3 + 3) / 3.0 * S * 8 * cells / (stage_ms / 1e3 / nst) / 1e9
+    out["mixed"] = {"ms_per_step": ms_mx, "value": cells / (ms_mx / 1e3), "tile": tname,
+                    "dtype": "f32 fluxes/coefficients + f64 state", "status": ctx.status(),
+                    "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                                 "peak_kind": peak_kind, "kernel_ms_per_launch": stage_ms / nst}}
+    ctx.close()
+    del st
+    torch.cuda.empty_cache()
+
+    # batched ensemble (reduced: --members members x --bench-batch-steps steps)
+    from fhdex_b200.params import stable_dt
+    from fhdex_b200.serve import ensemble, latency_stats, poisson_trace, run_alone, Server, warm_kernels
+    nb = args.bench_batch_steps
+    batched = {"config": {"members": args.members, "sizes": "half 32^3, half 64^3", "gas": "argon (2 species)",
+                          "T0": "U(250, 350) K", "rho0": "U(1e-3, 3e-3) g/cm^3", "steps": nb,
+                          "launch": "23 batched kernels per step, one CUDA graph replay per step"}}
+    members = None
+    for prec, key in ((0, "fp64"), (1, "mixed")):
+        b, states, bcells = ensemble(args.members, seed=args.seed, precision=prec)
+        members = [q for q, _ in states]
+        s_ = torch.cuda.Stream(local)
+        b.set_stream(s_)
+        b.step(3, graph=True)
+        b.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(s_):
+            e0.record()
+        b.step(nb, graph=True)
+        with torch.cuda.stream(s_):
+            e1.record()
+        b.synchronize()
+        ms = e0.elapsed_time(e1)
+        bad = sum(1 for mid in list(b.members) if b.status(mid) != 0)
+        b.close()
+        del states
+        torch.cuda.empty_cache()
+        batched[key] = {"value": bcells * nb / (ms / 1e3), "ms_per_step": ms / nb, "members_with_status": bad}
+    # the plain FP64 path, one member at a time (graph replay of its own step)
+    tot = 0.0
+    acells = 0
+    for q in members:
+        q = q.replace(precision=0)
+        c = Context(q, local)
+        st = StagState(q, f"cuda:{local}", aux=False)
+        c.init_state(st)
+        qdt = stable_dt(q)
+        c.rk3_steps(st, qdt, 0, 1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        c.rk3_steps(st, qdt, 1, nb)
+        torch.cuda.synchronize()
+        tot += time.perf_counter() - t0
+        acells += q.n_cells[0] * q.n_cells[1] * q.n_cells[2]
+        c.close()
+        del st
+    batched["alone_fp64"] = {"value": acells * nb / tot, "elapsed_s": tot,
+                             "path": "each member alone: fhd_rk3_steps_stag (graph replay), FP64, one after another"}
+    from fhdex_b200.equilibrium import batch_variance_ratios
+    ratios, m = batch_variance_ratios(members=8, precision=1, dt_scale=0.5, warm=2000, every=10)
+    batched["equilibrium_mixed"] = {"members": 8, "n": 32, "dt": "stable_dt/2", "samples_per_field": m,
+                                    "variance_over_theory": {k: round(v, 5) for k, v in ratios.items()},
+                                    "max_abs_error": round(max(abs(v - 1.0) for v in ratios.values()), 5)}
+    out["batched"] = batched
+
+    # continuous-batching server against one request at a time (plain FP64)
+    warm_kernels(local)
+    steps = (args.serve_min_steps, args.bench_serve_max_steps)
+    trace = poisson_trace(args.bench_requests, rate=args.rate, seed=args.seed, steps=steps)
+    srv = Server(device=local, chunk=args.chunk)
+    reqs, _, cu_b, el_b = srv.run(trace)
+    srv.close()
+    torch.cuda.empty_cache()
+    trace2 = poisson_trace(args.bench_requests, rate=args.rate, seed=args.seed, steps=steps)
+    reqs2, cu_a, el_a = run_alone(trace2, device=local)
+    out["served"] = {
+        "config": {"requests": args.bench_requests, "arrivals": f"Poisson, {args.rate:g} per s",
+                   "box_edge": "log-uniform 16-128", "nspecies": "{1, 2, 4}", "steps": f"U{{{steps[0]}..{steps[1]}}}",
+                   "precision": "FP64 or mixed per request", "chunk_steps": args.chunk},
+        "served": {"value": cu_b / el_b, "elapsed_s": el_b, **latency_stats(reqs),
+                   "bad_status": sum(1 for r in reqs if r.status)},
+        "alone_fp64": {"value": cu_a / el_a, "elapsed_s": el_a, **latency_stats(reqs2),
+                       "bad_status": sum(1 for r in reqs2 if r.status)},
+    }
+    return out
+
+
 def run_ours(args):
     import torch
     from fhdex_b200.context import Context
@@ -396,9 +553,10 @@ def run_ours(args):
     peak, peak_kind = measured_peak()
     achieved = alg_bytes / avg_stage_s / 1e9
     key = f"{p.nspecies}:{args.precision}"
-    traffic = STAGE_TRAFFIC_BYTES_PER_CELL.get(key)
+    traffic = None if prof["fused"][1] else STAGE_TRAFFIC_BYTES_PER_CELL.get(key)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic * cells if traffic else None, "peak_kind": peak_kind,
+            "traffic_source": "ncu, 128^3, one timed step, per cell, scaled to this box" if traffic else None,
             "traffic_gbs": traffic * cells / avg_stage_s / 1e9 if traffic else None,
             "kernel": ("RK stage (k_cellprep + k_stage_zm), per stage" if prof["fused"][1] else
                        "RK stage (k_cellprep + k_taus + 3x k_faces + k_update), per stage"),
@@ -486,9 +644,26 @@ def run_ours(args):
         cpu = {"value": v, "unit": UNIT, "cores": _CORES, "kind": kind, "sample": sample,
                "single_core": {"value": v1, "unit": UNIT, "cores": 1, "sample": sample1}}
 
+    extras = None
+    fma = None
+    if rank == 0 and world == 1:
+        fma_live, fma_file = fma_peaks(local)
+        fma = {"measured_now": fma_live, "committed": fma_file}
+        if not args.no_extras:
+            extras = step_extras(args, p, dt, local, peak, peak_kind)
     replicas.finish(env)
     if rank != 0:
         return
+    if fma and "fp64_tflops" in fma["measured_now"]:
+        # FP64 denominator: FP64 flops per cell per stage counted by ncu (dadd +
+        # dmul + 2 dfma, split pipeline, argon, in-kernel noise), over the stage time
+        fl = STAGE_FP64_FLOPS_PER_CELL.get(f"{p.nspecies}:{args.precision}")
+        if fl:
+            tf = fl * cells / avg_stage_s / 1e12
+            pk = fma["measured_now"]["fp64_tflops"]
+            roof["fp64"] = {"achieved": tf, "peak": pk, "unit": "TFLOP/s", "frac": tf / pk,
+                            "flops_per_cell_stage": fl, "peak_kind": "measured (fhd_measure_fma_peak)",
+                            "flops_source": "ncu instruction count of one stage at 128^3, per cell"}
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -497,9 +672,11 @@ def run_ours(args):
                  if p.nreaction > 0 else "synthetic (uniform argon at rest + in-kernel Philox noise; no dataset)"),
         "config": dict(config_dict(args, p, dt, tname), autotune_ms_per_step=tune),
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "graph_replay": graph, "gpu_launches": launches,
-        "chemistry": chem,
+        "chemistry": chem, "aux": False, "fma_peaks": fma,
         "clocks": clk, "status": status,
     }
+    if extras:
+        out.update(extras)
     print(json.dumps(out), flush=True)
 
 
@@ -795,6 +972,11 @@ def main():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the mixed / aux / batched / served objects of the step line")
+    ap.add_argument("--bench-batch-steps", type=int, default=20)
+    ap.add_argument("--bench-requests", type=int, default=50)
+    ap.add_argument("--bench-serve-max-steps", type=int, default=600)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
