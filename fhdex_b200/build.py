@@ -23,7 +23,7 @@ BASE = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contr
                "-Xptxas", "-v", f"-I{CSRC}", f"-I{os.path.join(ROOT, 'include')}"]
 SPECIES = (1, 2, 3, 4)
 
-HEADERS = ["fhd_div.h", "fhd_device.cuh", "philox.cuh", "fhd_flux.cuh", "fhd_kernels.cuh", "fhd_launch.cuh", "fhd_fused.cuh", "fhd_host.h", "fhd_chem.cuh", "fhd_vismf.h"]
+HEADERS = ["fhd_div.h", "fhd_device.cuh", "philox.cuh", "fhd_flux.cuh", "fhd_kernels.cuh", "fhd_launch.cuh", "fhd_fused.cuh", "fhd_host.h", "fhd_chem.cuh", "fhd_vismf.h", "fhd_walls.cuh"]
 
 
 def _units():

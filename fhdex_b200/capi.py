@@ -74,6 +74,19 @@ class FhdParams(C.Structure):
         ("beta_param", C.c_double * MAX_REACTIONS),
         ("T0_chem", C.c_double),
         ("avogadro", C.c_double),
+        ("walls", C.c_int),
+        ("bc_vel_lo", C.c_int * 3),
+        ("bc_vel_hi", C.c_int * 3),
+        ("bc_mass_lo", C.c_int * 3),
+        ("bc_mass_hi", C.c_int * 3),
+        ("bc_therm_lo", C.c_int * 3),
+        ("bc_therm_hi", C.c_int * 3),
+        ("t_lo", C.c_double * 3),
+        ("t_hi", C.c_double * 3),
+        ("bc_Yk_lo", (C.c_double * MAX_SPECIES) * 3),
+        ("bc_Yk_hi", (C.c_double * MAX_SPECIES) * 3),
+        ("bc_Xk_lo", (C.c_double * MAX_SPECIES) * 3),
+        ("bc_Xk_hi", (C.c_double * MAX_SPECIES) * 3),
     ]
 
 
@@ -130,6 +143,7 @@ def _declare(lib):
                               pfab, pfab, pfab, pfab, pfab, pfab, d]),
         "fhd_fill_boundary": (i, [vp, fab]),
         "fhd_override_sync": (i, [vp, fab]),
+        "fhd_set_bc_stag": (i, [vp, fab, fab, pfab, pfab]),
         "fhd_fill_random_normal": (i, [vp, fab, i, i, d, d, i, i, C.c_uint64]),
         "fhd_fill_random_uniform": (i, [vp, fab, i, i, i, i, C.c_uint64]),
         "fhd_rk3_steps_stag": (i, [vp, fab, pfab, fab, pfab, d, C.c_int64, i]),

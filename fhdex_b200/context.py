@@ -116,6 +116,13 @@ class Context:
         self._stream()
         check(self.lib.fhd_fill_boundary(self._h, mf.fab()), "fhd_fill_boundary")
 
+    def set_bc(self, st: StagState, cu=None, mom=None):
+        """setBCStag on (prim, cu, cumom, vel); nothing on a fully periodic box."""
+        cu = cu or st.cu
+        mom = mom or st.cumom
+        mf = FabArr3(*[m.fab() for m in mom])
+        check(self.lib.fhd_set_bc_stag(self._h, st.prim.fab(), cu.fab(), mf, st.vel_fabs()), "fhd_set_bc_stag")
+
     def override_sync(self, mf):
         self._stream()
         check(self.lib.fhd_override_sync(self._h, mf.fab()), "fhd_override_sync")
@@ -195,8 +202,11 @@ class Context:
                                       C.byref(s), steps, flags), "fhd_stats_stag")
 
     def init_state(self, st: StagState):
-        """main_driver init: InitConsVarStag -> conservedToPrimitiveStag -> FillBoundary."""
+        """main_driver init: InitConsVarStag -> conservedToPrimitiveStag ->
+        FillBoundary -> setBCStag (main_driver.cpp:766-780)."""
         self.init_cons_var_stag(st)
         self.conserved_to_primitive(st)
         for m in [st.cu, st.prim] + st.cumom + st.vel:
             self.fill_boundary(m)
+        if self.p.walls:
+            self.set_bc(st)

@@ -33,6 +33,10 @@ struct fhd_ctx {
     fhd_fab smc{}, sme{};        // stage total centre / edge momentum fluxes (f64)
     fhd_fab csrc{};              // zeroed source of a step given none (chemistry on)
     int tile = 0;
+    // physical boundaries: the periodic directions and the walls' values
+    int per[3] = {1, 1, 1};
+    bool walls = false;
+    WallParams wall{};
     // device mirrors for the host-buffer step
     double* hbuf = nullptr;
     size_t hbuf_bytes = 0;
@@ -93,6 +97,15 @@ bool fab_ok(const fhd_ctx* c, const fhd_fab& f, const int nodal[3], int min_ng, 
 }
 
 DevParams make_dev(const fhd_ctx* c, double dt, uint64_t step) { return dev_params(c->prm, dt, step); }
+
+// With walls the state has the reference's ghost width exactly (the conditions
+// fill every ghost layer, as the stage buffers have NGC of them)
+bool walls_ghosts_ok(const fhd_fab& cu, const fhd_fab* mom, const fhd_fab& prim, const fhd_fab* vel) {
+    if (-cu.lo[0] != NGC || -prim.lo[0] != NGC) return false;
+    for (int d = 0; d < 3; ++d)
+        if (-mom[d].lo[0] != NGC || -vel[d].lo[0] != NGC) return false;
+    return true;
+}
 
 int ensure_scratch(fhd_ctx* c) {
     const int* n = c->prm.n_cells;
@@ -236,6 +249,61 @@ const char* fhd_strerror(int code) {
     }
 }
 
+// Wall settings (boundaryStag.cpp SetupBCStag / SetupCWallStag): a direction is
+// periodic when both sides have bc_vel -1; otherwise both are walls with slip or
+// no-slip velocity, adiabatic or isothermal temperature and impermeable or
+// concentration mass conditions.  The concentration walls' Y and X follow from
+// whichever of the two sums to 1 (GetMassfrac / GetMolfrac,
+// compressible_functions.H:139-167).  Reservoirs (bc_mass >= 3) are not handled.
+int setup_walls(const fhd_params& p, int per[3], WallParams& W) {
+    std::memset(&W, 0, sizeof(W));
+    const int ns = p.nspecies;
+    for (int d = 0; d < 3; ++d) {
+        per[d] = 1;
+        if (!p.walls) continue;
+        const bool plo = p.bc_vel_lo[d] == -1, phi = p.bc_vel_hi[d] == -1;
+        if (plo && phi) continue;
+        if (plo != phi) return FHD_ERR_BAD_ARG;
+        per[d] = 0;
+        if (p.n_cells[d] < NGC) return FHD_ERR_BAD_ARG;
+        for (int h = 0; h < 2; ++h) {
+            const int s = 2 * d + h;
+            const int v = h ? p.bc_vel_hi[d] : p.bc_vel_lo[d];
+            const int m = h ? p.bc_mass_hi[d] : p.bc_mass_lo[d];
+            const int t = h ? p.bc_therm_hi[d] : p.bc_therm_lo[d];
+            if (m >= 3) return FHD_ERR_UNSUPPORTED;
+            if ((v != 1 && v != 2) || (m != 1 && m != 2) || (t != 1 && t != 2)) return FHD_ERR_BAD_ARG;
+            W.t[s] = h ? p.t_hi[d] : p.t_lo[d];
+            if (t == 2 && !(W.t[s] > 0)) return FHD_ERR_BAD_ARG;
+            const double* Yk = h ? p.bc_Yk_hi[d] : p.bc_Yk_lo[d];
+            const double* Xk = h ? p.bc_Xk_hi[d] : p.bc_Xk_lo[d];
+            for (int n = 0; n < ns; ++n) {
+                W.Yk[s][n] = Yk[n];
+                W.Xk[s][n] = Xk[n];
+            }
+            if (m != 2) continue;
+            double sumx = 0., sumy = 0.;
+            for (int n = 0; n < ns; ++n) {
+                sumx = sumx + Xk[n];
+                sumy = sumy + Yk[n];
+            }
+            if (std::fabs(sumx - 1) < 1.e-10) {
+                double molmix = 0.;
+                for (int n = 0; n < ns; ++n) molmix += W.Xk[s][n] * p.molmass[n];
+                for (int n = 0; n < ns; ++n) W.Yk[s][n] = W.Xk[s][n] * p.molmass[n] / molmix;
+            } else if (std::fabs(sumy - 1) < 1.e-10) {
+                double molmix = 0.;
+                for (int n = 0; n < ns; ++n) molmix += W.Yk[s][n] / p.molmass[n];
+                molmix = 1. / molmix;
+                for (int n = 0; n < ns; ++n) W.Xk[s][n] = W.Yk[s][n] * molmix / p.molmass[n];
+            } else {
+                return FHD_ERR_BAD_ARG;
+            }
+        }
+    }
+    return FHD_OK;
+}
+
 int fhd_create(fhd_ctx** out, const fhd_params* params, int device) {
     if (!out || !params) return FHD_ERR_BAD_ARG;
     *out = nullptr;
@@ -259,9 +327,26 @@ int fhd_create(fhd_ctx** out, const fhd_params* params, int device) {
                 if (p.stoich_R[m][n] < 0 || p.stoich_R[m][n] > 16 || p.stoich_P[m][n] < 0 || p.stoich_P[m][n] > 16)
                     return FHD_ERR_BAD_ARG;
     }
+    int per[3];
+    WallParams wall;
+    if (const int rc = setup_walls(p, per, wall)) return rc;
+    const bool walls = !(per[0] && per[1] && per[2]);
+    if (walls && p.precision != FHD_PREC_FP64) return FHD_ERR_UNSUPPORTED;
     fhd_ctx* c = new (std::nothrow) fhd_ctx;
     if (!c) return FHD_ERR_OOM;
     c->prm = p;
+    c->prm.walls = walls ? 1 : 0;
+    // the effective wall compositions (after SetupCWallStag)
+    for (int d = 0; d < 3 && walls; ++d)
+        for (int n = 0; n < p.nspecies; ++n) {
+            c->prm.bc_Yk_lo[d][n] = wall.Yk[2 * d][n];
+            c->prm.bc_Xk_lo[d][n] = wall.Xk[2 * d][n];
+            c->prm.bc_Yk_hi[d][n] = wall.Yk[2 * d + 1][n];
+            c->prm.bc_Xk_hi[d][n] = wall.Xk[2 * d + 1][n];
+        }
+    for (int d = 0; d < 3; ++d) c->per[d] = per[d];
+    c->walls = walls;
+    c->wall = wall;
     // GetHcGas, compressible_functions.cpp:91-100
     for (int i = 0; i < p.nspecies; ++i) {
         if (c->prm.hcv[i] < 0.) c->prm.hcv[i] = 0.5 * p.dof[i] * p.Runiv / p.molmass[i];
@@ -445,7 +530,29 @@ int fhd_fill_boundary(fhd_ctx* c, fhd_fab f) {
     if (!fab_ok(c, f, nodal, 0, 1, FHD_F64)) return FHD_ERR_BAD_ARG;
     cudaSetDevice(c->device);
     GhostReq r{f, 0, f.ncomp};
-    return fill_ghosts(&r, 1, c->prm.n_cells, c->stream);
+    return fill_ghosts(&r, 1, c->prm.n_cells, c->stream, c->per, 0);
+}
+
+int fhd_set_bc_stag(fhd_ctx* c, fhd_fab prim, fhd_fab cu, const fhd_fab cumom[3], const fhd_fab vel[3]) {
+    if (!c || !cumom || !vel) return FHD_ERR_BAD_ARG;
+    const int ns = c->prm.nspecies;
+    if (!fab_ok(c, prim, CELLN, 0, 6 + 2 * ns, FHD_F64)) return FHD_ERR_BAD_ARG;
+    const int g = -prim.lo[0];
+    if (!fab_ok(c, cu, CELLN, g, 5 + ns, FHD_F64, g)) return FHD_ERR_BAD_ARG;
+    const int gm = -cumom[0].lo[0];
+    // BCRhoRhoE reads the face momenta around every ghost cell of prim
+    if (gm < g) return FHD_ERR_BAD_ARG;
+    for (int d = 0; d < 3; ++d)
+        if (!fab_ok(c, cumom[d], FACEN[d], gm, 1, FHD_F64, gm) || !fab_ok(c, vel[d], FACEN[d], gm, 1, FHD_F64, gm))
+            return FHD_ERR_BAD_ARG;
+    if (!c->walls) return FHD_OK;
+    for (int d = 0; d < 3; ++d)
+        if (!c->per[d] && (c->prm.n_cells[d] < g || c->prm.n_cells[d] < gm)) return FHD_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    const DevParams P = make_dev(c, 1.0, 0);
+    int rc = bc_mom(P, cumom, vel, c->stream);
+    if (!rc) rc = exact_bc_prim(P, c->wall, prim, cu, cumom, c->stream);
+    return rc;
 }
 
 int fhd_override_sync(fhd_ctx* c, fhd_fab f) {
@@ -453,7 +560,7 @@ int fhd_override_sync(fhd_ctx* c, fhd_fab f) {
     int nodal[3] = {f.nodal[0], f.nodal[1], f.nodal[2]};
     if (!fab_ok(c, f, nodal, 0, 1, FHD_F64)) return FHD_ERR_BAD_ARG;
     cudaSetDevice(c->device);
-    return override_sync(f, c->prm.n_cells, c->stream);
+    return override_sync(f, c->prm.n_cells, c->stream, c->per);
 }
 
 int fhd_fill_random_normal(fhd_ctx* c, fhd_fab mf, int scomp, int ncomp, double mean, double variance,
@@ -466,11 +573,11 @@ int fhd_fill_random_normal(fhd_ctx* c, fhd_fab mf, int scomp, int ncomp, double 
     // field ids above the step-noise range keep these streams apart from the step's noise
     int rc = noise_fill(P, mf, scomp, ncomp, mean, std::sqrt(variance), 0x1000u + (uint32_t)scomp, 0, c->stream);
     if (rc) return rc;
-    if (overridesync) rc = override_sync(mf, c->prm.n_cells, c->stream);
+    if (overridesync) rc = override_sync(mf, c->prm.n_cells, c->stream, c->per);
     if (rc) return rc;
     if (fillboundary && -mf.lo[0] > 0) {
         GhostReq r{mf, scomp, ncomp};
-        rc = fill_ghosts(&r, 1, c->prm.n_cells, c->stream);
+        rc = fill_ghosts(&r, 1, c->prm.n_cells, c->stream, c->per, 0);
     }
     return rc;
 }
@@ -486,11 +593,11 @@ int fhd_fill_random_uniform(fhd_ctx* c, fhd_fab mf, int scomp, int ncomp, int ov
     // normal fills' field pairs and from the step noise
     int rc = noise_fill(P, mf, scomp, ncomp, 0.0, 1.0, 0x2000u + (uint32_t)scomp, 2, c->stream);
     if (rc) return rc;
-    if (overridesync) rc = override_sync(mf, c->prm.n_cells, c->stream);
+    if (overridesync) rc = override_sync(mf, c->prm.n_cells, c->stream, c->per);
     if (rc) return rc;
     if (fillboundary && -mf.lo[0] > 0) {
         GhostReq r{mf, scomp, ncomp};
-        rc = fill_ghosts(&r, 1, c->prm.n_cells, c->stream);
+        rc = fill_ghosts(&r, 1, c->prm.n_cells, c->stream, c->per, 0);
     }
     return rc;
 }
@@ -646,11 +753,120 @@ int fhd_fill_step_noise(fhd_ctx* c, const fhd_noise* nz, int64_t step) {
             const fhd_fab& f = nz->face[s][d];
             int rc = noise_fill(P, f, f.ncomp - (ns + 1), ns + 1, 0.0, 1.0, fid_face(d, 0), s, c->stream);
             if (!rc) rc = noise_fill(P, nz->edge[s][d], 0, 1, 0.0, 1.0, fid_edge(d), s, c->stream);
-            if (!rc) rc = noise_fill(P, nz->cen[s][d], 0, 1, 0.0, std::sqrt(2.0), fid_cen(d), s, c->stream);
+            // the centre noise is read on the cells grown by 1: in a wall direction
+            // its ghost layer holds values of its own
+            if (!rc) rc = noise_fill(P, nz->cen[s][d], 0, 1, 0.0, std::sqrt(2.0), fid_cen(d), s, c->stream, 1);
             if (rc) return rc;
             g[ng++] = GhostReq{nz->cen[s][d], 0, 1};
         }
-    return fill_ghosts(g, ng, c->prm.n_cells, c->stream);
+    return fill_ghosts(g, ng, c->prm.n_cells, c->stream, c->per, 1);
+}
+
+// One RK3 step of a box with physical walls (timeStepStag.cpp with setBCStag):
+// per stage the coefficients on the whole grown box from the stage's prim, the
+// wall variants of the stresses and fluxes, the update, then BCMomNormal /
+// BCMomTrans on the new face momenta, FillBoundary of the periodic directions,
+// conservedToPrimitiveStag on the valid region, FillBoundary again and setBCStag
+// (the conditions of boundaryStag.cpp on every ghost of the wall directions).
+// The state's prim and vel carry each stage's primitive fields, as in the
+// reference.  (The reference also runs BCMassTempPress on the previous stage's
+// prim before the conversion; setBCStag rewrites every value that pass writes
+// from the new prim, so it is left out.)
+static int walls_step_launches(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim, const fhd_fab vel[3],
+                               fhd_fab source, fhd_fab eta, fhd_fab zeta, fhd_fab kappa, fhd_fab chi, fhd_fab D,
+                               const fhd_fab* faceflux, const fhd_fab* edgeflux, const fhd_fab* cenflux,
+                               const fhd_noise* injected, double dt, int64_t step, bool aux_coef, bool aux_flux,
+                               const uint64_t* step_ptr) {
+    const int ns = c->prm.nspecies, nvars = 5 + ns, nprim = 6 + 2 * ns;
+    const bool stoch = c->prm.stoch_stress_form == 1;
+    int rc = FHD_OK;
+    const double w[3] = {(2.0 * std::sqrt(2.0) + 1.0 * std::sqrt(3.0)) / 5.0,
+                         (-4.0 * std::sqrt(2.0) + 3.0 * std::sqrt(3.0)) / 5.0,
+                         (1.0 * std::sqrt(2.0) - 2.0 * std::sqrt(3.0)) / 10.0};
+    StageCall sc;
+    std::memset(&sc, 0, sizeof(sc));
+    sc.P = make_dev(c, dt, (uint64_t)step);
+    sc.P.step_ptr = step_ptr;
+    sc.mode = !stoch ? NM_OFF : (injected ? NM_AB : NM_PHILOX);
+    if (injected && stoch) set_noise(sc, injected, false);
+    sc.pr = prim;
+    sc.pT = 4;
+    for (int d = 0; d < 3; ++d) { sc.vel[d] = vel[d]; sc.mom0[d] = mom[d]; }
+    sc.cons0 = cu;
+    sc.src = source;
+    const bool chem = c->prm.nreaction > 0;
+    ChemParams cp;
+    int cmode = CN_OFF;
+    if (chem) {
+        if (!sc.src.data) sc.src = c->csrc;
+        cp = chem_params(c->prm, dt, sc.P.dx[0] * sc.P.dx[1] * sc.P.dx[2]);
+        if (c->prm.reaction_type == 1) cmode = injected ? CN_AB : CN_PHILOX;
+    }
+    sc.status = c->d_status;
+    sc.stream = c->stream;
+    sc.ct = c->ct;
+    sc.et = c->et;
+    sc.smc = c->smc;
+    sc.sme = c->sme;
+    for (int d = 0; d < 3; ++d) sc.sff[d] = c->sff[d];
+    const fhd_fab* ins[3] = {&cu, &c->cup, &c->cup2};
+    const fhd_fab* insm[3] = {mom, c->cupm, c->cup2m};
+    const fhd_fab* outs[3] = {&c->cup, &c->cup2, &cu};
+    const fhd_fab* outsm[3] = {c->cupm, c->cup2m, mom};
+    for (int s = 0; s < 3; ++s) {
+        sc.stage = s + 1;
+        sc.w = w[s];
+        sc.cons_s = *ins[s];
+        sc.cons_o = *outs[s];
+        for (int d = 0; d < 3; ++d) { sc.mom_s[d] = insm[s][d]; sc.mom_o[d] = outsm[s][d]; }
+        // calculateTransportCoeffs on the grown box (the caller's fabs at stage 3)
+        if (s == 2 && aux_coef) { sc.eta = eta; sc.zeta = zeta; sc.kappa = kappa; sc.chi = chi; sc.D = D; }
+        else { sc.eta = c->ceta; sc.zeta = c->czeta; sc.kappa = c->ckappa; sc.chi = c->cchi; sc.D = c->cD; }
+        {
+            ProfScope ps(c, 0);
+            rc = exact_transport(sc.P, prim, sc.eta, sc.zeta, sc.kappa, sc.chi, sc.D, c->d_status, c->stream);
+            if (!rc && chem)
+                rc = chem_launch(sc.P, cp, prim, sc.src, cmode == CN_AB ? &injected->chem[0] : nullptr,
+                                 cmode == CN_AB ? &injected->chem[1] : nullptr, cmode, w[s], c->stream);
+        }
+        if (rc) return rc;
+        if (s == 2 && aux_flux) {
+            for (int d = 0; d < 3; ++d) { sc.ff[d] = faceflux[d]; sc.cf[d] = cenflux[d]; }
+            for (int e = 0; e < 6; ++e) sc.ef[e] = edgeflux[e];
+            ProfScope ps(c, 6);
+            rc = exact_aux_fluxes(sc);
+            if (rc) return rc;
+        }
+        for (int part = 0; part < 3 && !rc; ++part) {
+            ProfScope ps(c, 1 + part);
+            rc = exact_walls_part(sc, part);
+        }
+        if (rc) return rc;
+        {
+            ProfScope ps(c, 4);
+            // wall faces of the new momenta (the conversion reads them), then the
+            // periodic ghosts that the conversion and the conditions read
+            rc = bc_mom(sc.P, outsm[s], vel, c->stream);
+            GhostReq g[5] = {{*outs[s], 0, 1}, {*outs[s], 4, 1 + ns}, {outsm[s][0], 0, 1}, {outsm[s][1], 0, 1},
+                             {outsm[s][2], 0, 1}};
+            if (!rc) rc = fill_ghosts(g, 5, c->prm.n_cells, c->stream, c->per, 0);
+        }
+        if (rc) return rc;
+        {
+            ProfScope ps(c, 5);
+            rc = exact_convert(sc.P, prim, vel, *outs[s], outsm[s], c->d_status, c->stream);
+        }
+        if (rc) return rc;
+        {
+            ProfScope ps(c, 4);
+            GhostReq g[5] = {{*outs[s], 0, nvars}, {prim, 0, nprim}, {vel[0], 0, 1}, {vel[1], 0, 1}, {vel[2], 0, 1}};
+            rc = fill_ghosts(g, 5, c->prm.n_cells, c->stream, c->per, 0);
+            if (!rc) rc = bc_mom(sc.P, outsm[s], vel, c->stream);
+            if (!rc) rc = exact_bc_prim(sc.P, c->wall, prim, *outs[s], outsm[s], c->stream);
+        }
+        if (rc) return rc;
+    }
+    return FHD_OK;
 }
 
 // The launches of one RK3 step (after validation and scratch set-up); step_ptr,
@@ -659,6 +875,9 @@ static int step_launches(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab p
                   fhd_fab eta, fhd_fab zeta, fhd_fab kappa, fhd_fab chi, fhd_fab D, const fhd_fab* faceflux,
                   const fhd_fab* edgeflux, const fhd_fab* cenflux, const fhd_noise* injected, double dt, int64_t step,
                   bool aux_coef, bool aux_flux, const uint64_t* step_ptr) {
+    if (c->walls)
+        return walls_step_launches(c, cu, mom, prim, vel, source, eta, zeta, kappa, chi, D, faceflux, edgeflux,
+                                   cenflux, injected, dt, step, aux_coef, aux_flux, step_ptr);
     const int ns = c->prm.nspecies, nprim = 6 + 2 * ns;
     const bool mixed = c->prm.precision == FHD_PREC_MIXED;
     const bool stoch = c->prm.stoch_stress_form == 1;
@@ -775,6 +994,7 @@ int fhd_rk3_step_stag(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim
         if (!fab_ok(c, mom[d], FACEN[d], NGC, 1, FHD_F64) || !fab_ok(c, vel[d], FACEN[d], NGC, 1, FHD_F64))
             return FHD_ERR_BAD_ARG;
     if (source.data && !fab_ok(c, source, CELLN, 0, nvars, FHD_F64)) return FHD_ERR_BAD_ARG;
+    if (c->walls && !walls_ghosts_ok(cu, mom, prim, vel)) return FHD_ERR_BAD_ARG;
     const bool aux_coef = eta.data != nullptr;
     if (aux_coef) {
         if (mixed) return FHD_ERR_UNSUPPORTED;
@@ -814,6 +1034,7 @@ int fhd_rk3_steps_stag(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab pri
     for (int d = 0; d < 3; ++d)
         if (!fab_ok(c, mom[d], FACEN[d], NGC, 1, FHD_F64) || !fab_ok(c, vel[d], FACEN[d], NGC, 1, FHD_F64))
             return FHD_ERR_BAD_ARG;
+    if (c->walls && !walls_ghosts_ok(cu, mom, prim, vel)) return FHD_ERR_BAD_ARG;
     if (nsteps == 0) return FHD_OK;
     cudaSetDevice(c->device);
     int rc = ensure_scratch(c);

@@ -44,6 +44,11 @@ struct DevParams {
     double grav[3];
     double zeta_ratio;
     int visc_type, advection_type, stoch;
+    // physical boundaries; side s = 2 d + (0 lo, 1 hi); -1 on periodic sides
+    int walls;                       // any wall
+    int periodic[3];
+    int bc_vel[6], bc_mass[6], bc_therm[6];
+    double hdx[3], rhdx[3];          // 0.5*dx and RN(1/(0.5*dx)) (the wall faces' half-cell divisor)
     double molmass[MAXS], hcv[MAXS], hcp[MAXS], e0[MAXS];
     // Giovangigli model constants (compressible_functions.H:1180-1222)
     double mm[MAXS];                 // molmass*(k_B/Runiv)
@@ -106,6 +111,34 @@ FHD_D double divz(double a, double b) { return div_zero_short(a, b); }
 FHD_D float divz(float a, float b) { return rdiv(a, b); }
 
 FHD_D uint64_t noise_step(const DevParams& P) { return P.step_ptr ? *P.step_ptr : P.step; }
+
+// ---- physical boundaries ---------------------------------------------------------------
+// wall values per side s = 2 d + (0 lo, 1 hi) (after SetupCWallStag)
+struct WallParams {
+    double t[6];
+    double Yk[6][MAXS], Xk[6][MAXS];
+};
+
+// the reference's is_<lo|hi>_<d>_dirichlet_mass (fluxStag.cpp:84-89): a side whose
+// bc_mass is neither -1 (periodic) nor 3
+FHD_HD bool dirichlet_side(const DevParams& P, int side) {
+    const int b = P.bc_mass[side];
+    return b != -1 && b != 3;
+}
+// the wall side (0 lo, 1 hi) of the face plane idx of direction d, or -1: the
+// reference's (i == 0 and is_lo_x_dirichlet_mass) / (i == n_cells[0] and
+// is_hi_x_dirichlet_mass) tests
+FHD_HD int wall_face(const DevParams& P, int d, int idx) {
+    if (idx == 0 && dirichlet_side(P, 2 * d)) return 0;
+    if (idx == P.n[d] && dirichlet_side(P, 2 * d + 1)) return 1;
+    return -1;
+}
+// StochFluxStag's factors (boundaryStag.cpp:2086-3009) on a wall side: 0 for an
+// impermeable / adiabatic / slip wall (type 1), sqrt(2) for a concentration /
+// isothermal / no-slip wall (type 2), 1 otherwise
+FHD_HD double stoch_factor(const DevParams& P, int type) {
+    return type == 1 ? 0. : (type == 2 ? P.sqrt2 : 1.0);
+}
 
 // ---- EOS helpers (compressible_functions.H:138-219, 1497-1520) ----------------------
 

@@ -12,6 +12,8 @@ int mixed_cellprep_ns1(const StageCall&);
 int mixed_stage_ns1(const StageCall&, int);
 int exact_transport_ns1(const DevParams&, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, int*, cudaStream_t);
 int exact_convert_ns1(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const fhd_fab*, int*, cudaStream_t);
+int exact_walls_ns1(const StageCall&, int);
+int exact_bc_prim_ns1(const DevParams&, const WallParams&, fhd_fab, fhd_fab, const fhd_fab*, cudaStream_t);
 int exact_cellprep_ns2(const StageCall&);
 int exact_stage_ns2(const StageCall&, int);
 int exact_aux_ns2(const StageCall&);
@@ -19,6 +21,8 @@ int mixed_cellprep_ns2(const StageCall&);
 int mixed_stage_ns2(const StageCall&, int);
 int exact_transport_ns2(const DevParams&, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, int*, cudaStream_t);
 int exact_convert_ns2(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const fhd_fab*, int*, cudaStream_t);
+int exact_walls_ns2(const StageCall&, int);
+int exact_bc_prim_ns2(const DevParams&, const WallParams&, fhd_fab, fhd_fab, const fhd_fab*, cudaStream_t);
 int exact_cellprep_ns3(const StageCall&);
 int exact_stage_ns3(const StageCall&, int);
 int exact_aux_ns3(const StageCall&);
@@ -26,6 +30,8 @@ int mixed_cellprep_ns3(const StageCall&);
 int mixed_stage_ns3(const StageCall&, int);
 int exact_transport_ns3(const DevParams&, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, int*, cudaStream_t);
 int exact_convert_ns3(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const fhd_fab*, int*, cudaStream_t);
+int exact_walls_ns3(const StageCall&, int);
+int exact_bc_prim_ns3(const DevParams&, const WallParams&, fhd_fab, fhd_fab, const fhd_fab*, cudaStream_t);
 int exact_cellprep_ns4(const StageCall&);
 int exact_stage_ns4(const StageCall&, int);
 int exact_aux_ns4(const StageCall&);
@@ -33,6 +39,8 @@ int mixed_cellprep_ns4(const StageCall&);
 int mixed_stage_ns4(const StageCall&, int);
 int exact_transport_ns4(const DevParams&, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, int*, cudaStream_t);
 int exact_convert_ns4(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const fhd_fab*, int*, cudaStream_t);
+int exact_walls_ns4(const StageCall&, int);
+int exact_bc_prim_ns4(const DevParams&, const WallParams&, fhd_fab, fhd_fab, const fhd_fab*, cudaStream_t);
 
 size_t exact_batch_args_size_ns1(int, int);
 void exact_batch_pack_ns1(int, int, const StageCall&, void*);
@@ -82,6 +90,39 @@ int exact_convert(const DevParams& P, fhd_fab prim, const fhd_fab vel[3], fhd_fa
     FHD_DISPATCH(P.ns, exact_convert_ns, P, prim, vel, cons, mom, status, s)
 }
 
+int exact_walls_part(const StageCall& c, int part) { FHD_DISPATCH(c.P.ns, exact_walls_ns, c, part) }
+int exact_bc_prim(const DevParams& P, const WallParams& W, fhd_fab prim, fhd_fab cons, const fhd_fab mom[3],
+                  cudaStream_t s) {
+    FHD_DISPATCH(P.ns, exact_bc_prim_ns, P, W, prim, cons, mom, s)
+}
+
+int bc_mom(const DevParams& P, const fhd_fab mom[3], const fhd_fab vel[3], cudaStream_t s) {
+    BcMomArgs a;
+    a.P = P;
+    int64_t most = 0;
+    for (int d = 0; d < 3; ++d) {
+        a.mom[d] = view<double>(mom[d]);
+        a.vel[d] = view<double>(vel[d]);
+        const int g = -mom[d].lo[0];
+        int blo[3], bhi[3], clo[3], chi[3];
+        for (int e = 0; e < 3; ++e) {
+            const int nod = e == d;
+            blo[e] = -g;
+            bhi[e] = P.n[e] - 1 + nod + g;
+            const bool w = P.walls && !P.periodic[e];
+            // the core no condition touches: inside the walls (the wall faces of
+            // the nodal direction included in the conditions)
+            clo[e] = w ? nod : blo[e];
+            chi[e] = w ? P.n[e] - 1 : bhi[e];
+        }
+        a.sh[d] = make_shell(blo, bhi, clo, chi);
+        if (a.sh[d].n > most) most = a.sh[d].n;
+    }
+    if (most == 0) return FHD_OK;
+    k_bc_mom<<<dim3(grid_for(most, 256, 148 * 8), 3), 256, 0, s>>>(a);
+    return cuda_rc(cudaGetLastError());
+}
+
 size_t batch_args_size(int ns, bool mixed, int kind, int mode) {
     switch (ns) {
         case 1: return mixed ? mixed_batch_args_size_ns1(kind, mode) : exact_batch_args_size_ns1(kind, mode);
@@ -127,6 +168,8 @@ int64_t ghost_pack(const fhd_fab& f, int c0, int nc, const int ncell[3], void* d
     g.sn = ext[0] * ext[1] * ext[2];
     g.c0 = c0;
     g.nc = nc;
+    for (int d = 0; d < 3; ++d) g.per[d] = 1;
+    g.mode = 0;
     const int64_t VY = g.vhi[1] + 1, VZ = g.vhi[2] + 1;
     g.npts = gw == 0 ? 0 : 2 * gw * ext[0] * ext[1] + 2 * gw * ext[0] * VZ + 2 * gw * VY * VZ;
     memcpy(dst, &g, sizeof(g));
@@ -150,7 +193,7 @@ int steps_inc(uint64_t* steps, int n, cudaStream_t s) {
     return cuda_rc(cudaGetLastError());
 }
 
-int fill_ghosts(const GhostReq* reqs, int n, const int ncell[3], cudaStream_t s) {
+int fill_ghosts(const GhostReq* reqs, int n, const int ncell[3], cudaStream_t s, const int* periodic, int mode) {
     for (int base = 0; base < n; base += 16) {
         GhostArgs a;
         a.nf = 0;
@@ -171,7 +214,11 @@ int fill_ghosts(const GhostReq* reqs, int n, const int ncell[3], cudaStream_t s)
             g.sn = ext[0] * ext[1] * ext[2];
             g.c0 = reqs[q].c0;
             g.nc = reqs[q].nc;
-            for (int d = 0; d < 3; ++d) g.n[d] = ncell[d];
+            for (int d = 0; d < 3; ++d) {
+                g.n[d] = ncell[d];
+                g.per[d] = periodic ? periodic[d] : 1;
+            }
+            g.mode = mode;
             const int64_t VX = g.vhi[0] + 1, VY = g.vhi[1] + 1, VZ = g.vhi[2] + 1;
             g.npts = 2 * gw * ext[0] * ext[1] + 2 * gw * ext[0] * VZ + 2 * gw * VY * VZ;
             (void)VX;
@@ -187,13 +234,13 @@ int fill_ghosts(const GhostReq* reqs, int n, const int ncell[3], cudaStream_t s)
     return FHD_OK;
 }
 
-int override_sync(const fhd_fab& f, const int ncell[3], cudaStream_t s) {
+int override_sync(const fhd_fab& f, const int ncell[3], cudaStream_t s, const int* periodic) {
     SyncArgs a;
     a.p = static_cast<double*>(f.data);
     a.lo = f.lo[0];
     int64_t ext[3];
     for (int d = 0; d < 3; ++d) {
-        a.nodal[d] = f.nodal[d];
+        a.nodal[d] = f.nodal[d] && (!periodic || periodic[d]);
         a.n[d] = ncell[d];
         ext[d] = f.hi[d] - f.lo[d] + 1;
     }
@@ -201,19 +248,30 @@ int override_sync(const fhd_fab& f, const int ncell[3], cudaStream_t s) {
     a.sz = ext[0] * ext[1];
     a.sn = ext[0] * ext[1] * ext[2];
     a.nc = f.ncomp;
-    const int64_t tot = (int64_t)(ncell[0] + f.nodal[0]) * (ncell[1] + f.nodal[1]) * (ncell[2] + f.nodal[2]) * f.ncomp;
+    const int64_t tot = (int64_t)(ncell[0] + a.nodal[0]) * (ncell[1] + a.nodal[1]) * (ncell[2] + a.nodal[2]) * f.ncomp;
+    if (!a.nodal[0] && !a.nodal[1] && !a.nodal[2]) return FHD_OK;
     k_override_sync<<<grid_for(tot, 256), 256, 0, s>>>(a);
     return cuda_rc(cudaGetLastError());
 }
 
 int noise_fill(const DevParams& P, const fhd_fab& f, int c0, int nc, double mean, double sd, uint32_t fid0, int use_b,
-               cudaStream_t s) {
+               cudaStream_t s, int wall_ghosts) {
     NoiseFillArgs a;
     a.P = P;
     a.f = view<double>(f);
-    a.vx = P.n[0] + f.nodal[0];
-    a.vy = P.n[1] + f.nodal[1];
-    a.vz = P.n[2] + f.nodal[2];
+    int ext[3], org[3];
+    for (int d = 0; d < 3; ++d) {
+        // a wall direction of a field with ghosts: its first ghost layer too
+        const bool g = wall_ghosts && P.walls && !P.periodic[d] && -f.lo[d] >= 1;
+        ext[d] = P.n[d] + f.nodal[d] + (g ? 2 : 0);
+        org[d] = g ? -1 : 0;
+    }
+    a.vx = ext[0];
+    a.vy = ext[1];
+    a.vz = ext[2];
+    a.ox = org[0];
+    a.oy = org[1];
+    a.oz = org[2];
     a.c0 = c0;
     a.nc = nc;
     a.mean = mean;

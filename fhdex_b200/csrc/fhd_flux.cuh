@@ -192,7 +192,11 @@ FHD_D CellTaus<R> cell_taus_w(const DevParams& P, const Fields<NS, R>& F, const 
 // off-diagonal stress at an edge E (0 xy, 1 xz, 2 yz): stochastic fluxStag.cpp:209-295,
 // deterministic :927-1023.  The four cells around the edge are c00, c01, c10, c11
 // in the reference's summation order.
-template <int NS, class R, int NZ, int E>
+// WL: walls; an edge on a wall plane averages only the two cells on the wall's
+// ghost side for its stochastic amplitude and its viscosity, and differences the
+// velocity across the wall over the half cell (fluxStag.cpp:221-232, 250-261,
+// 279-290, 939-1019: the first direction's wall is tested last and wins a corner).
+template <int NS, class R, int NZ, int E, bool WL = false>
 FHD_D Taus<R> edge_taus_w(const DevParams& P, const Fields<NS, R>& F, double wnoise, int i, int j, int k) {
     // cells: (a) low-low, (b) low-high, (c) high-low, (d) high-high in the edge's two directions
     int ai, aj, ak, bi, bj, bk, ci, cj, ck;
@@ -201,8 +205,20 @@ FHD_D Taus<R> edge_taus_w(const DevParams& P, const Fields<NS, R>& F, double wno
     else { ai = i; aj = j - 1; ak = k - 1; bi = i; bj = j - 1; bk = k; ci = i; cj = j; ck = k - 1; }
     Taus<R> t;
     if (NZ != NZ_OFF) {
-        const R etaT = R(0.25) * (F.eta(ai, aj, ak) * R(F.T(ai, aj, ak)) + F.eta(bi, bj, bk) * R(F.T(bi, bj, bk)) +
-                                  F.eta(ci, cj, ck) * R(F.T(ci, cj, ck)) + F.eta(i, j, k) * R(F.T(i, j, k)));
+        R etaT = R(0.25) * (F.eta(ai, aj, ak) * R(F.T(ai, aj, ak)) + F.eta(bi, bj, bk) * R(F.T(bi, bj, bk)) +
+                            F.eta(ci, cj, ck) * R(F.T(ci, cj, ck)) + F.eta(i, j, k) * R(F.T(i, j, k)));
+        if (WL) {
+            // cells a (lo, lo), b (lo, hi), c (hi, lo), d = (i, j, k) in the edge's
+            // (first, second) directions; the wall of the second direction is tested first
+            const int d1 = E == 2 ? 1 : 0, d2 = E == 0 ? 1 : 2;
+            const int x1 = d1 == 0 ? i : j, x2 = d2 == 1 ? j : k;
+            const R ta = F.eta(ai, aj, ak) * R(F.T(ai, aj, ak)), tb = F.eta(bi, bj, bk) * R(F.T(bi, bj, bk));
+            const R tc = F.eta(ci, cj, ck) * R(F.T(ci, cj, ck)), td = F.eta(i, j, k) * R(F.T(i, j, k));
+            if (x2 == 0 && dirichlet_side(P, 2 * d2)) etaT = R(0.5) * (ta + tc);
+            if (x2 == P.n[d2] && dirichlet_side(P, 2 * d2 + 1)) etaT = R(0.5) * (tb + td);
+            if (x1 == 0 && dirichlet_side(P, 2 * d1)) etaT = R(0.5) * (ta + tb);
+            if (x1 == P.n[d1] && dirichlet_side(P, 2 * d1 + 1)) etaT = R(0.5) * (tc + td);
+        }
         const R fac = dsqrt(R(2.0) * R(P.k_B) * etaT * R(P.volinv) * R(P.dtinv));
         t.s = fac * R(wnoise);
     } else {
@@ -219,7 +235,42 @@ FHD_D Taus<R> edge_taus_w(const DevParams& P, const Fields<NS, R>& F, double wno
         g1 = divc(P, R(F.vel[1](i, j, k)) - R(F.vel[1](i, j, k - 1)), R(P.dx[2]), R(P.rdx[2]));  // v_z
         g2 = divc(P, R(F.vel[2](i, j, k)) - R(F.vel[2](i, j - 1, k)), R(P.dx[1]), R(P.rdx[1]));  // w_y
     }
-    const R ei = R(0.25) * (F.eta(ai, aj, ak) + F.eta(bi, bj, bk) + F.eta(ci, cj, ck) + F.eta(i, j, k));
+    R ei = R(0.25) * (F.eta(ai, aj, ak) + F.eta(bi, bj, bk) + F.eta(ci, cj, ck) + F.eta(i, j, k));
+    if (WL) {
+        // a wall plane: the gradient across it over the half cell to the wall value,
+        // eta from the two ghost-side cells (fluxStag.cpp:939-954, 971-986, 1004-1019);
+        // g1 is the gradient across the second direction, g2 across the first
+        const int d1 = E == 2 ? 1 : 0, d2 = E == 0 ? 1 : 2;
+        const int x1 = d1 == 0 ? i : j, x2 = d2 == 1 ? j : k;
+        const R ea = F.eta(ai, aj, ak), eb = F.eta(bi, bj, bk), ec = F.eta(ci, cj, ck), ed = F.eta(i, j, k);
+        R n1, n2;  // numerators of g1, g2
+        if (E == 0) {
+            n1 = R(F.vel[0](i, j, k)) - R(F.vel[0](i, j - 1, k));
+            n2 = R(F.vel[1](i, j, k)) - R(F.vel[1](i - 1, j, k));
+        } else if (E == 1) {
+            n1 = R(F.vel[0](i, j, k)) - R(F.vel[0](i, j, k - 1));
+            n2 = R(F.vel[2](i, j, k)) - R(F.vel[2](i - 1, j, k));
+        } else {
+            n1 = R(F.vel[1](i, j, k)) - R(F.vel[1](i, j, k - 1));
+            n2 = R(F.vel[2](i, j, k)) - R(F.vel[2](i, j - 1, k));
+        }
+        if (x2 == 0 && dirichlet_side(P, 2 * d2)) {
+            g1 = divc(P, n1, R(P.hdx[d2]), R(P.rhdx[d2]));
+            ei = R(0.5) * (ea + ec);
+        }
+        if (x2 == P.n[d2] && dirichlet_side(P, 2 * d2 + 1)) {
+            g1 = divc(P, n1, R(P.hdx[d2]), R(P.rhdx[d2]));
+            ei = R(0.5) * (eb + ed);
+        }
+        if (x1 == 0 && dirichlet_side(P, 2 * d1)) {
+            g2 = divc(P, n2, R(P.hdx[d1]), R(P.rhdx[d1]));
+            ei = R(0.5) * (ea + eb);
+        }
+        if (x1 == P.n[d1] && dirichlet_side(P, 2 * d1 + 1)) {
+            g2 = divc(P, n2, R(P.hdx[d1]), R(P.rhdx[d1]));
+            ei = R(0.5) * (ec + ed);
+        }
+    }
     t.d = ei * (g1 + g2);
     return t;
 }
@@ -231,9 +282,9 @@ FHD_D CellTaus<R> cell_taus(const DevParams& P, const Fields<NS, R>& F, const No
     return cell_taus_w<NS, R, NZ>(P, F, wc, i, j, k);
 }
 
-template <int NS, class R, int NZ, int E>
+template <int NS, class R, int NZ, int E, bool WL = false>
 FHD_D Taus<R> edge_taus(const DevParams& P, const Fields<NS, R>& F, const Noise<NZ>& nz, int i, int j, int k) {
-    return edge_taus_w<NS, R, NZ, E>(P, F, NZ != NZ_OFF ? nz.edge(P, E, i, j, k) : 0.0, i, j, k);
+    return edge_taus_w<NS, R, NZ, E, WL>(P, F, NZ != NZ_OFF ? nz.edge(P, E, i, j, k) : 0.0, i, j, k);
 }
 
 // ---- face fluxes ---------------------------------------------------------------------
@@ -243,8 +294,15 @@ struct FaceFlux {
     double aux[4];        // comps nvars .. nvars+3 (heat, visc. heating diag/shear, Dufour)
 };
 
-// TauGet: .cell(i,j,k) -> CellTaus, .edge<E>(i,j,k) -> Taus
-template <int NS, class R, int NZ, int D, class TauGet>
+// TauGet: .cell(i,j,k) -> CellTaus, .edge<E>(i,j,k) -> Taus.
+// WL: the box has physical walls.  A face on a wall plane (the reference's
+// "(i == 0) and is_lo_x_dirichlet_mass" faces) then takes the wall values from the
+// cell on the wall's ghost side with half-cell differences (fluxStag.cpp's
+// Dirichlet branches), StochFluxStag's factors on its stochastic heat, species,
+// Dufour and shear-heating parts (boundaryStag.cpp:2086-3009),
+// BCWallReservoirFluxStag's zero species / Dufour fluxes on impermeable walls
+// (boundaryStag.cpp:300-580) and no advective flux (fluxStag.cpp:1511-1529).
+template <int NS, class R, int NZ, int D, class TauGet, bool WL = false>
 FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const Noise<NZ>& nz, const TauGet& tg,
                              int i, int j, int k) {
     constexpr int e0 = D == 0, e1 = D == 1, e2 = D == 2;
@@ -252,6 +310,10 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
     const Arr4<const double>& velx = F.vel[0];
     const Arr4<const double>& vely = F.vel[1];
     const Arr4<const double>& velz = F.vel[2];
+    // wall side of this face (0 lo, 1 hi, -1 none) and the cell holding the wall values
+    const int ws = WL ? wall_face(P, D, D == 0 ? i : (D == 1 ? j : k)) : -1;
+    const int gi = ws == 0 ? im : i, gj = ws == 0 ? jm : j, gk = ws == 0 ? km : k;
+    const int wside = 2 * D + (ws == 1 ? 1 : 0);
     // flux components in the reference's accumulation order
     R heat = R(0.0), vdiag = R(0.0), vshear = R(0.0), duf = R(0.0);
     R spec[NS];
@@ -295,26 +357,53 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
     if (NZ != NZ_OFF) {
         vdiag = R(0.5) * un * (tl.s[D] + th.s[D]);
         R vsh = R(0.0);
-        vsh += R(0.25) * ((va1h + va1l) * ea1.s + (va0h + va0l) * ea0.s);
-        vsh += R(0.25) * ((vb1h + vb1l) * eb1.s + (vb0h + vb0l) * eb0.s);
+        if (WL && ws == 0) {
+            vsh += R(0.5) * (va1l * ea1.s + va0l * ea0.s);
+            vsh += R(0.5) * (vb1l * eb1.s + vb0l * eb0.s);
+        } else if (WL && ws == 1) {
+            vsh += R(0.5) * (va1h * ea1.s + va0h * ea0.s);
+            vsh += R(0.5) * (vb1h * eb1.s + vb0h * eb0.s);
+        } else {
+            vsh += R(0.25) * ((va1h + va1l) * ea1.s + (va0h + va0l) * ea0.s);
+            vsh += R(0.25) * ((vb1h + vb1l) * eb1.s + (vb0h + vb0l) * eb0.s);
+        }
         vshear = vsh;
+        // StochFluxStag: velocity walls scale the stochastic shear heating
+        if (WL && ws >= 0 && (P.bc_vel[wside] == 1 || P.bc_vel[wside] == 2))
+            vshear *= R(stoch_factor(P, P.bc_vel[wside]));
     }
     vdiag -= R(0.5) * un * (tl.d[D] + th.d[D]);
     R vsh = R(0.0);
-    vsh -= R(0.25) * ((va1h + va1l) * ea1.d + (va0h + va0l) * ea0.d);
-    vsh -= R(0.25) * ((vb1h + vb1l) * eb1.d + (vb0h + vb0l) * eb0.d);
+    if (WL && ws == 0) {
+        vsh -= R(0.5) * (va1l * ea1.d + va0l * ea0.d);
+        vsh -= R(0.5) * (vb1l * eb1.d + vb0l * eb0.d);
+    } else if (WL && ws == 1) {
+        vsh -= R(0.5) * (va1h * ea1.d + va0h * ea0.d);
+        vsh -= R(0.5) * (vb1h * eb1.d + vb0h * eb0.d);
+    } else {
+        vsh -= R(0.25) * ((va1h + va1l) * ea1.d + (va0h + va0l) * ea0.d);
+        vsh -= R(0.25) * ((vb1h + vb1l) * eb1.d + (vb0h + vb0l) * eb0.d);
+    }
     vshear += vsh;
     }
 
     // ---- stochastic part (fluxStag.cpp:298-781) ----
     if (NZ != NZ_OFF) {
         const R Th = R(F.T(i, j, k)), Tl = R(F.T(im, jm, km));
-        const R kp = (F.kappa(i, j, k) * Th * Th + F.kappa(im, jm, km) * Tl * Tl);
-        const R meanT = R(0.5) * (Th + Tl);
+        R kp = (F.kappa(i, j, k) * Th * Th + F.kappa(im, jm, km) * Tl * Tl);
+        R meanT = R(0.5) * (Th + Tl);
+        if (WL && ws >= 0) {
+            const R Tg = R(F.T(gi, gj, gk));
+            kp = R(2.0) * F.kappa(gi, gj, gk) * Tg * Tg;
+            meanT = Tg;
+        }
         double wf[NS + 1];
         nz.template face_all<NS + 1>(P, D, i, j, k, wf);
         const R fw0 = dsqrt(R(P.k_B) * kp * R(P.volinv) * R(P.dtinv));
         heat = fw0 * R(wf[0]);
+        // StochFluxStag: thermal walls scale the stochastic heat flux
+        if (WL && ws >= 0 && (P.bc_therm[wside] == 1 || P.bc_therm[wside] == 2))
+            heat *= R(stoch_factor(P, P.bc_therm[wside]));
         // species noise, Soret: mixtures only (a single gas has no species flux)
         if constexpr (NS > 1) {
         R yy[NS], yyp[NS], DY[NS * NS], sqD[NS * NS], hk[NS], wien[NS];
@@ -323,6 +412,8 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
             wien[s] = R(0.);
             yy[s] = clamp01(R(F.Y(im, jm, km, s)));
             yyp[s] = clamp01(R(F.Y(i, j, k, s)));
+            if (WL && ws == 0) yyp[s] = clamp01(R(F.Y(im, jm, km, s)));
+            if (WL && ws == 1) yy[s] = clamp01(R(F.Y(i, j, k, s)));
         }
         R sumy = R(0.), sumyp = R(0.);
 #pragma unroll
@@ -334,9 +425,14 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
         for (int s = 0; s < NS; ++s) {
             MWmix = MWmix + divc(P, R(0.5) * (yy[s] + yyp[s]), R(P.molmass[s]), R(P.rmolmass[s]));
 #pragma unroll
-            for (int ll = 0; ll < NS; ++ll)
-                DY[s * NS + ll] = R(0.5) * (F.D(im, jm, km, ll * NS + s) * yy[ll] + F.D(i, j, k, ll * NS + s) * yyp[ll] +
-                                            (F.D(im, jm, km, s * NS + ll) * yy[s] + F.D(i, j, k, s * NS + ll) * yyp[s]));
+            for (int ll = 0; ll < NS; ++ll) {
+                if (WL && ws >= 0)
+                    DY[s * NS + ll] = R(0.5) * (F.D(gi, gj, gk, ll * NS + s) * yy[ll] + F.D(gi, gj, gk, ll * NS + s) * yyp[ll] +
+                                                (F.D(gi, gj, gk, s * NS + ll) * yy[s] + F.D(gi, gj, gk, s * NS + ll) * yyp[s]));
+                else
+                    DY[s * NS + ll] = R(0.5) * (F.D(im, jm, km, ll * NS + s) * yy[ll] + F.D(i, j, k, ll * NS + s) * yyp[ll] +
+                                                (F.D(im, jm, km, s * NS + ll) * yy[s] + F.D(i, j, k, s * NS + ll) * yyp[s]));
+            }
         }
 #pragma unroll
         for (int s = 0; s < NS; ++s)
@@ -360,22 +456,41 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
         R soret = R(0.);
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
-            const R soret_s = (hk[s] + divc(P, R(P.Runiv) * meanT, R(P.molmass[s]), R(P.rmolmass[s])) * R(0.5) *
-                                           (F.chi(im, jm, km, s) + F.chi(i, j, k, s))) * wien[s];
+            R soret_s;
+            if (WL && ws >= 0)
+                soret_s = (hk[s] + divc(P, R(P.Runiv) * meanT, R(P.molmass[s]), R(P.rmolmass[s])) *
+                                       F.chi(gi, gj, gk, s)) * wien[s];
+            else
+                soret_s = (hk[s] + divc(P, R(P.Runiv) * meanT, R(P.molmass[s]), R(P.rmolmass[s])) * R(0.5) *
+                                       (F.chi(im, jm, km, s) + F.chi(i, j, k, s))) * wien[s];
             soret += soret_s;
         }
         duf = soret;
+        // StochFluxStag: mass walls scale the stochastic species and Dufour fluxes
+        if (WL && ws >= 0 && (P.bc_mass[wside] == 1 || P.bc_mass[wside] == 2)) {
+            const R f = R(stoch_factor(P, P.bc_mass[wside]));
+#pragma unroll
+            for (int s = 0; s < NS; ++s) spec[s] *= f;
+            duf *= f;
+        }
         }
     }
 
     // ---- diffusive part (fluxStag.cpp:1026-1426) ----
     {
-        const R h = R(P.dx[D]), rh = R(P.rdx[D]);
+        // wall faces difference over the half cell to the wall value
+        const R h = (WL && ws >= 0) ? R(P.hdx[D]) : R(P.dx[D]);
+        const R rh = (WL && ws >= 0) ? R(P.rhdx[D]) : R(P.rdx[D]);
         const R Tl = R(F.T(im, jm, km)), Th = R(F.T(i, j, k));
         const R pl = R(F.p(im, jm, km)), ph = R(F.p(i, j, k));
-        const R kp = R(0.5) * (F.kappa(im, jm, km) + F.kappa(i, j, k));
-        const R meanT = R(0.5) * (Tl + Th);
-        const R meanP = R(0.5) * (pl + ph);
+        R kp = R(0.5) * (F.kappa(im, jm, km) + F.kappa(i, j, k));
+        R meanT = R(0.5) * (Tl + Th);
+        R meanP = R(0.5) * (pl + ph);
+        if (WL && ws >= 0) {
+            kp = F.kappa(gi, gj, gk);
+            meanT = R(F.T(gi, gj, gk));
+            meanP = R(F.p(gi, gj, gk));
+        }
         heat -= divc(P, kp * (Th - Tl), h, rh);
         // species diffusion, Dufour: mixtures only
         if constexpr (NS > 1) {
@@ -384,11 +499,16 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
         for (int s = 0; s < NS; ++s) {
             const R Xl = R(F.X(im, jm, km, s)), Xh = R(F.X(i, j, k, s));
             const R term1 = divc(P, Xh - Xl, h, rh);
-            const R mX = R(0.5) * (Xl + Xh);
-            const R mY = R(0.5) * (R(F.Y(im, jm, km, s)) + R(F.Y(i, j, k, s)));
+            R mX = R(0.5) * (Xl + Xh);
+            R mY = R(0.5) * (R(F.Y(im, jm, km, s)) + R(F.Y(i, j, k, s)));
+            if (WL && ws >= 0) {
+                mX = R(F.X(gi, gj, gk, s));
+                mY = R(F.Y(gi, gj, gk, s));
+            }
             const R term2 = divz(divc0(P, (mX - mY) * (ph - pl), h, rh), meanP);
             dk[s] = term1 + term2;
-            const R ChiX = R(0.5) * (F.chi(im, jm, km, s) * Xl + F.chi(i, j, k, s) * Xh);
+            R ChiX = R(0.5) * (F.chi(im, jm, km, s) * Xl + F.chi(i, j, k, s) * Xh);
+            if (WL && ws >= 0) ChiX = F.chi(gi, gj, gk, s) * R(F.X(gi, gj, gk, s));
             sor[s] = divz(divc0(P, ChiX * (Th - Tl), h, rh), meanT);
         }
 #pragma unroll
@@ -396,7 +516,9 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
             R f = R(0.);
 #pragma unroll
             for (int ll = 0; ll < NS; ++ll) {
-                const R Fks = R(0.5) * (F.D(im, jm, km, ll * NS + kk) + F.D(i, j, k, ll * NS + kk)) * (dk[ll] + sor[ll]);
+                R Fks;
+                if (WL && ws >= 0) Fks = F.D(gi, gj, gk, ll * NS + kk) * (dk[ll] + sor[ll]);
+                else Fks = R(0.5) * (F.D(im, jm, km, ll * NS + kk) + F.D(i, j, k, ll * NS + kk)) * (dk[ll] + sor[ll]);
                 f -= Fks;
             }
             Fk[kk] = f;
@@ -405,13 +527,24 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
         R Q5 = R(0.);
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
-            // z faces use chi(i,j,k)+chi(i,j,k), fluxStag.cpp:1407 (kept from the reference)
-            const R chs = (D == 2) ? (F.chi(i, j, k, s) + F.chi(i, j, k, s)) : (F.chi(im, jm, km, s) + F.chi(i, j, k, s));
-            Q5 += (hk[s] + divc0(P, R(0.5) * R(P.Runiv) * meanT * chs, R(P.molmass[s]), R(P.rmolmass[s]))) * Fk[s];
+            if (WL && ws >= 0) {
+                Q5 += (hk[s] + divc0(P, R(P.Runiv) * meanT * F.chi(gi, gj, gk, s), R(P.molmass[s]), R(P.rmolmass[s]))) *
+                      Fk[s];
+            } else {
+                // z faces use chi(i,j,k)+chi(i,j,k), fluxStag.cpp:1407 (kept from the reference)
+                const R chs = (D == 2) ? (F.chi(i, j, k, s) + F.chi(i, j, k, s)) : (F.chi(im, jm, km, s) + F.chi(i, j, k, s));
+                Q5 += (hk[s] + divc0(P, R(0.5) * R(P.Runiv) * meanT * chs, R(P.molmass[s]), R(P.rmolmass[s]))) * Fk[s];
+            }
         }
         duf += Q5;
 #pragma unroll
         for (int s = 0; s < NS; ++s) spec[s] += Fk[s];
+        }
+        // BCWallReservoirFluxStag: impermeable walls carry no species or Dufour flux
+        if (WL && ws >= 0 && P.bc_mass[wside] == 1) {
+#pragma unroll
+            for (int s = 0; s < NS; ++s) spec[s] = R(0.);
+            duf = R(0.);
         }
     }
 
@@ -422,7 +555,13 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
 #pragma unroll
     for (int s = 0; s < NS; ++s) fs[s] = (double)spec[s];
     const int adv = P.advection_type;
-    if (adv >= 0) {
+    if (WL && ws >= 0) {
+        // no advection through a wall face (fluxStag.cpp:1511-1529)
+        f0 += 0.0;
+        f4 += 0.0;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) fs[s] += 0.0;
+    } else if (adv >= 0) {
         const double m = F.mom[D](i, j, k);
         const double u = F.vel[D](i, j, k);
         f0 += m;
@@ -484,20 +623,38 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
 // ---- momentum fluxes --------------------------------------------------------------
 // advective edge terms (fluxStag.cpp:1767-1845): returns the two fluxes of edge E:
 // E=0 xy: (edgey_u, edgex_v); E=1 xz: (edgez_u, edgex_w); E=2 yz: (edgez_v, edgey_w)
-template <int NS, class R, int E>
+// WL: walls; an edge on a wall plane takes the momentum / velocity of its wall
+// side only (fluxStag.cpp:1774-1789, 1797-1812, 1820-1835: the second
+// direction's wall is tested first, the first direction's wins a corner).
+template <int NS, class R, int E, bool WL = false>
 FHD_D void edge_adv(const DevParams& P, const Fields<NS, R>& F, int i, int j, int k, double& a, double& b) {
     const Arr4<const double>&mx = F.mom[0], &my = F.mom[1], &mz = F.mom[2];
     const Arr4<const double>&vx = F.vel[0], &vy = F.vel[1], &vz = F.vel[2];
     if (P.advection_type < 0) { a = b = 0.0; return; }
+    // edge of directions (p, q) = xy, xz or yz: a carries the p-momentum along q
+    // (m0, m1 the p-face momenta on the q-1 / q sides, u0, u1 the q-face velocities
+    // on the p-1 / p sides), b the q-momentum along p (n0, n1 on the p sides, w0,
+    // w1 the p-face velocities on the q sides)
+    double m0, m1, u0, u1, n0, n1, w0, w1;
     if (E == 0) {
-        a = 0.25 * (mx(i, j - 1, k) + mx(i, j, k)) * (vy(i - 1, j, k) + vy(i, j, k));
-        b = 0.25 * (my(i - 1, j, k) + my(i, j, k)) * (vx(i, j - 1, k) + vx(i, j, k));
+        m0 = mx(i, j - 1, k); m1 = mx(i, j, k); u0 = vy(i - 1, j, k); u1 = vy(i, j, k);
+        n0 = my(i - 1, j, k); n1 = my(i, j, k); w0 = vx(i, j - 1, k); w1 = vx(i, j, k);
     } else if (E == 1) {
-        a = 0.25 * (mx(i, j, k - 1) + mx(i, j, k)) * (vz(i - 1, j, k) + vz(i, j, k));
-        b = 0.25 * (mz(i - 1, j, k) + mz(i, j, k)) * (vx(i, j, k - 1) + vx(i, j, k));
+        m0 = mx(i, j, k - 1); m1 = mx(i, j, k); u0 = vz(i - 1, j, k); u1 = vz(i, j, k);
+        n0 = mz(i - 1, j, k); n1 = mz(i, j, k); w0 = vx(i, j, k - 1); w1 = vx(i, j, k);
     } else {
-        a = 0.25 * (my(i, j, k - 1) + my(i, j, k)) * (vz(i, j - 1, k) + vz(i, j, k));
-        b = 0.25 * (mz(i, j - 1, k) + mz(i, j, k)) * (vy(i, j, k - 1) + vy(i, j, k));
+        m0 = my(i, j, k - 1); m1 = my(i, j, k); u0 = vz(i, j - 1, k); u1 = vz(i, j, k);
+        n0 = mz(i, j - 1, k); n1 = mz(i, j, k); w0 = vy(i, j, k - 1); w1 = vy(i, j, k);
+    }
+    a = 0.25 * (m0 + m1) * (u0 + u1);
+    b = 0.25 * (n0 + n1) * (w0 + w1);
+    if (WL) {
+        const int dp = E == 2 ? 1 : 0, dq = E == 0 ? 1 : 2;
+        const int xp = dp == 0 ? i : j, xq = dq == 1 ? j : k;
+        if (xq == 0 && dirichlet_side(P, 2 * dq)) { a = 0.5 * (m0) * (u0 + u1); b = 0.5 * (n0 + n1) * (w0); }
+        if (xq == P.n[dq] && dirichlet_side(P, 2 * dq + 1)) { a = 0.5 * (m1) * (u0 + u1); b = 0.5 * (n0 + n1) * (w1); }
+        if (xp == 0 && dirichlet_side(P, 2 * dp)) { a = 0.5 * (m0 + m1) * (u0); b = 0.5 * (n0) * (w0 + w1); }
+        if (xp == P.n[dp] && dirichlet_side(P, 2 * dp + 1)) { a = 0.5 * (m0 + m1) * (u1); b = 0.5 * (n1) * (w0 + w1); }
     }
 }
 
@@ -505,6 +662,28 @@ FHD_D void edge_adv(const DevParams& P, const Fields<NS, R>& F, int i, int j, in
 template <class R>
 FHD_D double edge_total(const Taus<R>& t, double adv, int has_adv) {
     double v = (double)t.s;
+    v -= (double)t.d;
+    if (has_adv) v += adv;
+    return v;
+}
+
+// the same with walls: StochFluxStag's velocity-wall factors on the stochastic part
+// of an edge of type E lying on wall planes, in its order (lo x, hi x, lo y, hi y,
+// lo z, hi z; boundaryStag.cpp:2456-3009)
+template <class R, int E>
+FHD_D double edge_total_w(const DevParams& P, const Taus<R>& t, double adv, int has_adv, int i, int j, int k) {
+    double v = (double)t.s;
+    const int x[3] = {i, j, k};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const bool along = (E == 0) ? (d != 2) : (E == 1) ? (d != 1) : (d != 0);  // the edge is nodal in d
+        if (!along) continue;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int side = 2 * d + h, b = P.bc_vel[side];
+            if ((b == 1 || b == 2) && x[d] == (h ? P.n[d] : 0)) v *= stoch_factor(P, b);
+        }
+    }
     v -= (double)t.d;
     if (has_adv) v += adv;
     return v;

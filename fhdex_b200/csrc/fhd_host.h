@@ -20,6 +20,15 @@ struct NoiseFabs {
     fhd_fab ca[3], cb[3];   // centres
 };
 
+// a box with a physical wall in some direction (both sides of a periodic
+// direction have bc_vel -1)
+inline bool has_walls(const fhd_params& p) {
+    if (!p.walls) return false;
+    for (int d = 0; d < 3; ++d)
+        if (p.bc_vel_lo[d] != -1 || p.bc_vel_hi[d] != -1) return true;
+    return false;
+}
+
 // Kernel parameters of a run (after GetHcGas): cell widths, the transport model's
 // cell-independent constants in the reference's own operation order
 // (compressible_functions.H:1180-1222), the Philox key and the reciprocals of the
@@ -67,6 +76,18 @@ inline DevParams dev_params(const fhd_params& p, double dt, uint64_t step) {
     P.cfac = 6.0 * CKL - 5.0;
     P.sqrt2 = sqrt(2.0);
     P.sqrt3 = sqrt(3.0);
+    P.walls = p.walls ? 1 : 0;
+    for (int d = 0; d < 3; ++d) {
+        P.periodic[d] = !P.walls || (p.bc_vel_lo[d] == -1 && p.bc_vel_hi[d] == -1);
+        const int* lo[3] = {p.bc_vel_lo, p.bc_mass_lo, p.bc_therm_lo};
+        const int* hi[3] = {p.bc_vel_hi, p.bc_mass_hi, p.bc_therm_hi};
+        int* dst[3] = {P.bc_vel, P.bc_mass, P.bc_therm};
+        for (int q = 0; q < 3; ++q) {
+            dst[q][2 * d] = P.periodic[d] ? -1 : lo[q][d];
+            dst[q][2 * d + 1] = P.periodic[d] ? -1 : hi[q][d];
+        }
+        P.hdx[d] = 0.5 * P.dx[d];
+    }
     P.key0 = (uint32_t)p.seed;
     P.key1 = (uint32_t)(p.seed >> 32);
     P.step = step;
@@ -88,6 +109,7 @@ inline DevParams dev_params(const fhd_params& p, double dt, uint64_t step) {
     }
     P.rRdt = rcp(P.Runiv * P.dt);
     P.rpi = rcp(3.1415926535897932);
+    for (int d = 0; d < 3; ++d) P.rhdx[d] = rcp(P.hdx[d]);
     P.r3 = rcp(3.0);
     P.div_lo = kDivAlo;
     P.div_span = in_window ? kDivAspan : 0u;
@@ -125,6 +147,13 @@ int exact_transport(const DevParams& P, fhd_fab prim, fhd_fab eta, fhd_fab zeta,
                     fhd_fab D, int* status, cudaStream_t s);
 int exact_convert(const DevParams& P, fhd_fab prim, const fhd_fab vel[3], fhd_fab cons, const fhd_fab mom[3],
                   int* status, cudaStream_t s);
+// boxes with physical walls (FP64): the stage parts (0 stresses, 1 face fluxes, 2
+// update), BCMassTempPress + BCRhoRhoE on prim / cons, BCMomNormal + BCMomTrans on
+// the face momenta and velocities
+int exact_walls_part(const StageCall& c, int part);
+int exact_bc_prim(const DevParams& P, const WallParams& W, fhd_fab prim, fhd_fab cons, const fhd_fab mom[3],
+                  cudaStream_t s);
+int bc_mom(const DevParams& P, const fhd_fab mom[3], const fhd_fab vel[3], cudaStream_t s);
 // mixed translation unit (coefficient fabs are f32)
 int mixed_cellprep(const StageCall& c);
 int mixed_stage_part(const StageCall& c, int part);
@@ -134,7 +163,10 @@ struct GhostReq {
     fhd_fab f;
     int c0, nc;
 };
-int fill_ghosts(const GhostReq* reqs, int n, const int ncell[3], cudaStream_t s);
+// periodic: the periodic directions (nullptr: all); mode 0 FillBoundary, 1 noise
+// fields with wall ghosts of their own (k_ghosts)
+int fill_ghosts(const GhostReq* reqs, int n, const int ncell[3], cudaStream_t s, const int* periodic = nullptr,
+                int mode = 0);
 // chemistry source (fhd_chem.cu): writes species comps 5.. of `source` at the valid
 // cells from `prim`; na/nb: the A/B (mode CN_AB) or W (CN_W) noise fabs
 struct ChemParams;
@@ -150,9 +182,10 @@ int chem_launch(const DevParams& P, const ChemParams& C, const fhd_fab& prim, co
 // running statistics (fhd_stats.cu, exact TU)
 int exact_stats(const DevParams& P, const fhd_fab& cu, const fhd_fab& prim, const fhd_fab mom[3],
                 const fhd_stats& st, int64_t steps, int flags, cudaStream_t s);
-int override_sync(const fhd_fab& f, const int ncell[3], cudaStream_t s);
+int override_sync(const fhd_fab& f, const int ncell[3], cudaStream_t s, const int* periodic = nullptr);
+// wall_ghosts: also fill the first ghost layer of the wall directions (centre noise)
 int noise_fill(const DevParams& P, const fhd_fab& f, int c0, int nc, double mean, double sd, uint32_t fid0, int use_b,
-               cudaStream_t s);
+               cudaStream_t s, int wall_ghosts = 0);
 int init_uniform(const fhd_fab& cu, int ns, double rho0, double rhoE, const double* rhoY, cudaStream_t s);
 
 // batched launches (kinds: 0 cellprep, 1 stresses, 2-4 faces, 5 update, 6 conversion)

@@ -43,7 +43,7 @@ int FHD_CAT(mixed_stage_ns, FHD_NS)(const StageCall& c, int part) { return launc
 int FHD_CAT(exact_cellprep_ns, FHD_NS)(const StageCall& c) { return launch_cellprep<FHD_NS, double>(c); }
 int FHD_CAT(exact_stage_ns, FHD_NS)(const StageCall& c, int part) { return launch_stage_part<FHD_NS, double>(c, part); }
 
-template <int NS, int NZ>
+template <int NS, int NZ, bool WL>
 int launch_aux_t(const StageCall& c) {
     AuxArgs<NS, double, NZ> a;
     a.P = c.P;
@@ -59,19 +59,29 @@ int launch_aux_t(const StageCall& c) {
                        (int64_t)N[0] * N[1] * (N[2] + 1);
     const int64_t ne = (int64_t)(N[0] + 1) * (N[1] + 1) * N[2] + (int64_t)(N[0] + 1) * N[1] * (N[2] + 1) +
                        (int64_t)N[0] * (N[1] + 1) * (N[2] + 1) + (int64_t)(N[0] + 2) * (N[1] + 2) * (N[2] + 2);
-    if (c.ff[0].data) k_aux_faces<NS, double, NZ><<<grid_for(nf, 128), 128, 0, c.stream>>>(a);
-    if (c.ef[0].data) k_aux_edges_cen<NS, double, NZ><<<grid_for(ne, 128), 128, 0, c.stream>>>(a);
+    if (c.ff[0].data) k_aux_faces<NS, double, NZ, WL><<<grid_for(nf, 128), 128, 0, c.stream>>>(a);
+    if (c.ef[0].data) k_aux_edges_cen<NS, double, NZ, WL><<<grid_for(ne, 128), 128, 0, c.stream>>>(a);
     return cuda_rc(cudaGetLastError());
 }
 
-int FHD_CAT(exact_aux_ns, FHD_NS)(const StageCall& c) {
+template <bool WL>
+int aux_mode(const StageCall& c) {
     switch (c.mode) {
-        case NM_OFF: return launch_aux_t<FHD_NS, NZ_OFF>(c);
-        case NM_W: return launch_aux_t<FHD_NS, NZ_W>(c);
-        case NM_AB: return launch_aux_t<FHD_NS, NZ_AB>(c);
-        case NM_PHILOX: return launch_aux_t<FHD_NS, NZ_PHILOX>(c);
+        case NM_OFF: return launch_aux_t<FHD_NS, NZ_OFF, WL>(c);
+        case NM_W: return launch_aux_t<FHD_NS, NZ_W, WL>(c);
+        case NM_AB: return launch_aux_t<FHD_NS, NZ_AB, WL>(c);
+        case NM_PHILOX: return launch_aux_t<FHD_NS, NZ_PHILOX, WL>(c);
         default: return FHD_ERR_BAD_ARG;
     }
+}
+
+int FHD_CAT(exact_aux_ns, FHD_NS)(const StageCall& c) { return c.P.walls ? aux_mode<true>(c) : aux_mode<false>(c); }
+
+int FHD_CAT(exact_walls_ns, FHD_NS)(const StageCall& c, int part) { return launch_walls_part<FHD_NS>(c, part); }
+
+int FHD_CAT(exact_bc_prim_ns, FHD_NS)(const DevParams& P, const WallParams& W, fhd_fab prim, fhd_fab cons,
+                                      const fhd_fab* mom, cudaStream_t s) {
+    return launch_bc_prim<FHD_NS>(P, W, prim, cons, mom, s);
 }
 
 int FHD_CAT(exact_transport_ns, FHD_NS)(const DevParams& P, fhd_fab prim, fhd_fab eta, fhd_fab zeta, fhd_fab kappa,
@@ -84,7 +94,10 @@ int FHD_CAT(exact_transport_ns, FHD_NS)(const DevParams& P, fhd_fab prim, fhd_fa
     a.kappa = view<double>(kappa);
     a.chi = view<double>(chi);
     a.D = view<double>(D);
-    a.ng = -prim.lo[0];
+    // the grown box that every coefficient fab and prim cover
+    int g = -prim.lo[0];
+    for (const fhd_fab* f : {&eta, &zeta, &kappa, &chi, &D}) g = -f->lo[0] < g ? -f->lo[0] : g;
+    a.ng = g;
     a.status = status;
     const int64_t tot = (int64_t)(P.n[0] + 2 * a.ng) * (P.n[1] + 2 * a.ng) * (P.n[2] + 2 * a.ng);
     k_transport<FHD_NS><<<grid_for(tot, 128), 128, 0, s>>>(a);

@@ -131,7 +131,9 @@ struct StageArgs {
 template <int NS, class R, int NZ>
 FHD_D int taus_count(const StageArgs<NS, R, NZ>& a) { return (a.P.n[0] + 2) * (a.P.n[1] + 2) * (a.P.n[2] + 2); }
 
-template <int NS, class R, int NZ>
+// WL: walls (the wall variants of the edge stresses, advective edge fluxes and
+// StochFluxStag's factors on the edge totals)
+template <int NS, class R, int NZ, bool WL = false>
 FHD_D void taus_point(const StageArgs<NS, R, NZ>& a, int q) {
     const DevParams& P = a.P;
     const int nx = P.n[0] + 2, ny = P.n[1] + 2;
@@ -152,36 +154,37 @@ FHD_D void taus_point(const StageArgs<NS, R, NZ>& a, int q) {
         const int hadv = P.advection_type >= 0;
         double ea, eb;
         if (k < P.n[2]) {
-            const Taus<R> e = edge_taus_w<NS, R, NZ, 0>(P, a.F, we[0], i, j, k);
+            const Taus<R> e = edge_taus_w<NS, R, NZ, 0, WL>(P, a.F, we[0], i, j, k);
             a.et(i, j, k, 0) = e.s;
             a.et(i, j, k, 1) = e.d;
-            edge_adv<NS, R, 0>(P, a.F, i, j, k, ea, eb);
-            a.me(i, j, k, 2) = edge_total<R>(e, ea, hadv);  // edgey_u
-            a.me(i, j, k, 0) = edge_total<R>(e, eb, hadv);  // edgex_v
+            edge_adv<NS, R, 0, WL>(P, a.F, i, j, k, ea, eb);
+            a.me(i, j, k, 2) = WL ? edge_total_w<R, 0>(P, e, ea, hadv, i, j, k) : edge_total<R>(e, ea, hadv);  // edgey_u
+            a.me(i, j, k, 0) = WL ? edge_total_w<R, 0>(P, e, eb, hadv, i, j, k) : edge_total<R>(e, eb, hadv);  // edgex_v
         }
         if (j < P.n[1]) {
-            const Taus<R> e = edge_taus_w<NS, R, NZ, 1>(P, a.F, we[1], i, j, k);
+            const Taus<R> e = edge_taus_w<NS, R, NZ, 1, WL>(P, a.F, we[1], i, j, k);
             a.et(i, j, k, 2) = e.s;
             a.et(i, j, k, 3) = e.d;
-            edge_adv<NS, R, 1>(P, a.F, i, j, k, ea, eb);
-            a.me(i, j, k, 4) = edge_total<R>(e, ea, hadv);  // edgez_u
-            a.me(i, j, k, 1) = edge_total<R>(e, eb, hadv);  // edgex_w
+            edge_adv<NS, R, 1, WL>(P, a.F, i, j, k, ea, eb);
+            a.me(i, j, k, 4) = WL ? edge_total_w<R, 1>(P, e, ea, hadv, i, j, k) : edge_total<R>(e, ea, hadv);  // edgez_u
+            a.me(i, j, k, 1) = WL ? edge_total_w<R, 1>(P, e, eb, hadv, i, j, k) : edge_total<R>(e, eb, hadv);  // edgex_w
         }
         if (i < P.n[0]) {
-            const Taus<R> e = edge_taus_w<NS, R, NZ, 2>(P, a.F, we[2], i, j, k);
+            const Taus<R> e = edge_taus_w<NS, R, NZ, 2, WL>(P, a.F, we[2], i, j, k);
             a.et(i, j, k, 4) = e.s;
             a.et(i, j, k, 5) = e.d;
-            edge_adv<NS, R, 2>(P, a.F, i, j, k, ea, eb);
-            a.me(i, j, k, 5) = edge_total<R>(e, ea, hadv);  // edgez_v
-            a.me(i, j, k, 3) = edge_total<R>(e, eb, hadv);  // edgey_w
+            edge_adv<NS, R, 2, WL>(P, a.F, i, j, k, ea, eb);
+            a.me(i, j, k, 5) = WL ? edge_total_w<R, 2>(P, e, ea, hadv, i, j, k) : edge_total<R>(e, ea, hadv);  // edgez_v
+            a.me(i, j, k, 3) = WL ? edge_total_w<R, 2>(P, e, eb, hadv, i, j, k) : edge_total<R>(e, eb, hadv);  // edgey_w
         }
     }
 }
 
-template <int NS, class R, int NZ>
+template <int NS, class R, int NZ, bool WL = false>
 static __global__ void __launch_bounds__(256) k_taus(StageArgs<NS, R, NZ> a) {
     const int tot = taus_count(a);
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) taus_point(a, q);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x)
+        taus_point<NS, R, NZ, WL>(a, q);
 }
 
 template <class R>
@@ -211,23 +214,23 @@ FHD_D int faces_count(const StageArgs<NS, R, NZ>& a) {
     return (a.P.n[0] + (D == 0)) * (a.P.n[1] + (D == 1)) * (a.P.n[2] + (D == 2));
 }
 
-template <int NS, class R, int NZ, int D>
+template <int NS, class R, int NZ, int D, bool WL = false>
 FHD_D void faces_point(const StageArgs<NS, R, NZ>& a, int q) {
     const DevParams& P = a.P;
     const int nx = P.n[0] + (D == 0), ny = P.n[1] + (D == 1);
     const GlobalTaus<R> tg{a.ct, a.et};
     const int i = q % nx, j = (q / nx) % ny, k = q / (nx * ny);
-    const FaceFlux<NS> f = face_flux<NS, R, NZ, D>(P, a.F, a.noise, tg, i, j, k);
+    const FaceFlux<NS> f = face_flux<NS, R, NZ, D, GlobalTaus<R>, WL>(P, a.F, a.noise, tg, i, j, k);
 #pragma unroll
     for (int c = 0; c < 2 + NS; ++c) a.ff[D](i, j, k, c) = f.cons[c];
 }
 
 // MINB = minimum resident blocks requested from the register allocator.
-template <int NS, class R, int NZ, int D, int BS, int MINB>
+template <int NS, class R, int NZ, int D, int BS, int MINB, bool WL = false>
 static __global__ void __launch_bounds__(BS, MINB) k_faces(StageArgs<NS, R, NZ> a) {
     const int tot = faces_count<NS, R, NZ, D>(a);
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x)
-        faces_point<NS, R, NZ, D>(a, q);
+        faces_point<NS, R, NZ, D, WL>(a, q);
 }
 
 // RK3 stage combination (timeStepStag.cpp:439-528, 771-861, 1106-1202): one thread
@@ -395,6 +398,12 @@ struct GhostFab {
     int c0, nc;       // component range
     int64_t npts;     // ghost points of one component
     int n[3];         // cells of the box (period)
+    // periodic directions (walls elsewhere).  mode 0 (FillBoundary): a ghost point
+    // is filled only when it lies outside the valid box in periodic directions
+    // alone; mode 1 (noise fields whose wall ghosts hold their own values): the
+    // periodic coordinates are wrapped and the wall coordinates kept.
+    int per[3];
+    int mode;
 };
 struct GhostArgs {
     GhostFab f[16];
@@ -430,13 +439,21 @@ FHD_D void ghost_point(const GhostFab& f, int64_t q) {
             k = (int)(r / VY); j = (int)(r % VY);
             i = ii < g ? ii - g : VX + (ii - g);
         }
-        int si = i, sj = j, sk = k;
-        while (si < 0) si += f.n[0];
-        while (si > f.vhi[0]) si -= f.n[0];
-        while (sj < 0) sj += f.n[1];
-        while (sj > f.vhi[1]) sj -= f.n[1];
-        while (sk < 0) sk += f.n[2];
-        while (sk > f.vhi[2]) sk -= f.n[2];
+        int s[3] = {i, j, k};
+        bool wrapped = false;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            if (s[d] >= 0 && s[d] <= f.vhi[d]) continue;
+            if (!f.per[d]) {
+                if (f.mode == 0) return;
+                continue;
+            }
+            wrapped = true;
+            while (s[d] < 0) s[d] += f.n[d];
+            while (s[d] > f.vhi[d]) s[d] -= f.n[d];
+        }
+        if (!wrapped) return;
+        const int si = s[0], sj = s[1], sk = s[2];
         const int64_t base = (int64_t)c * f.sn;
         f.p[base + (i + g) + (j + g) * f.sy + (k + g) * f.sz] = f.p[base + (si + g) + (sj + g) * f.sy + (sk + g) * f.sz];
     }
@@ -455,7 +472,7 @@ static __global__ void __launch_bounds__(256) k_ghosts(GhostArgs a) {
 struct SyncArgs {
     double* p;
     int lo;
-    int nodal[3];
+    int nodal[3];   // nodal and periodic (a wall direction has no duplicate points)
     int n[3];
     int64_t sy, sz, sn;
     int nc;
@@ -515,14 +532,14 @@ static __global__ void __launch_bounds__(128) k_transport(TransArgs<NS> a) {
 }
 
 // stresses recomputed on the fly (operator path)
-template <int NS, class R, int NZ>
+template <int NS, class R, int NZ, bool WL = false>
 struct DirectTaus {
     const DevParams* P;
     const Fields<NS, R>* F;
     const Noise<NZ>* nz;
     FHD_D CellTaus<R> cell(int i, int j, int k) const { return cell_taus<NS, R, NZ>(*P, *F, *nz, i, j, k); }
     template <int E>
-    FHD_D Taus<R> edge(int i, int j, int k) const { return edge_taus<NS, R, NZ, E>(*P, *F, *nz, i, j, k); }
+    FHD_D Taus<R> edge(int i, int j, int k) const { return edge_taus<NS, R, NZ, E, WL>(*P, *F, *nz, i, j, k); }
 };
 
 template <int NS, class R, int NZ>
@@ -536,22 +553,23 @@ struct AuxArgs {
 };
 
 // faceflux[d] on valid faces; items enumerate the three face boxes back to back
-template <int NS, class R, int NZ>
+template <int NS, class R, int NZ, bool WL = false>
 static __global__ void __launch_bounds__(128) k_aux_faces(AuxArgs<NS, R, NZ> a) {
     const DevParams& P = a.P;
     const int* N = P.n;
     const int64_t nxf = (int64_t)(N[0] + 1) * N[1] * N[2], nyf = (int64_t)N[0] * (N[1] + 1) * N[2],
                   nzf = (int64_t)N[0] * N[1] * (N[2] + 1);
-    const DirectTaus<NS, R, NZ> tg{&P, &a.F, &a.noise};
+    const DirectTaus<NS, R, NZ, WL> tg{&P, &a.F, &a.noise};
+    using TG = DirectTaus<NS, R, NZ, WL>;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nxf + nyf + nzf; q += (int64_t)gridDim.x * blockDim.x) {
         int d, i, j, k;
         if (q < nxf) { d = 0; i = (int)(q % (N[0] + 1)); j = (int)((q / (N[0] + 1)) % N[1]); k = (int)(q / ((int64_t)(N[0] + 1) * N[1])); }
         else if (q < nxf + nyf) { const int64_t r = q - nxf; d = 1; i = (int)(r % N[0]); j = (int)((r / N[0]) % (N[1] + 1)); k = (int)(r / ((int64_t)N[0] * (N[1] + 1))); }
         else { const int64_t r = q - nxf - nyf; d = 2; i = (int)(r % N[0]); j = (int)((r / N[0]) % N[1]); k = (int)(r / ((int64_t)N[0] * N[1])); }
         FaceFlux<NS> f;
-        if (d == 0) f = face_flux<NS, R, NZ, 0>(P, a.F, a.noise, tg, i, j, k);
-        else if (d == 1) f = face_flux<NS, R, NZ, 1>(P, a.F, a.noise, tg, i, j, k);
-        else f = face_flux<NS, R, NZ, 2>(P, a.F, a.noise, tg, i, j, k);
+        if (d == 0) f = face_flux<NS, R, NZ, 0, TG, WL>(P, a.F, a.noise, tg, i, j, k);
+        else if (d == 1) f = face_flux<NS, R, NZ, 1, TG, WL>(P, a.F, a.noise, tg, i, j, k);
+        else f = face_flux<NS, R, NZ, 2, TG, WL>(P, a.F, a.noise, tg, i, j, k);
         const Arr4<double>& o = a.ff[d];
         o(i, j, k, 0) = f.cons[0];
         o(i, j, k, 1) = 0.0;
@@ -566,7 +584,7 @@ static __global__ void __launch_bounds__(128) k_aux_faces(AuxArgs<NS, R, NZ> a) 
 }
 
 // edge fluxes (6 fabs) on valid edges and centre fluxes on cells grown by 1
-template <int NS, class R, int NZ>
+template <int NS, class R, int NZ, bool WL = false>
 static __global__ void __launch_bounds__(128) k_aux_edges_cen(AuxArgs<NS, R, NZ> a) {
     const DevParams& P = a.P;
     const int* N = P.n;
@@ -577,24 +595,24 @@ static __global__ void __launch_bounds__(128) k_aux_edges_cen(AuxArgs<NS, R, NZ>
         double ea, eb;
         if (q < nxy) {
             const int i = (int)(q % (N[0] + 1)), j = (int)((q / (N[0] + 1)) % (N[1] + 1)), k = (int)(q / ((int64_t)(N[0] + 1) * (N[1] + 1)));
-            const Taus<R> t = edge_taus<NS, R, NZ, 0>(P, a.F, a.noise, i, j, k);
-            edge_adv<NS, R, 0>(P, a.F, i, j, k, ea, eb);
-            a.ef[2](i, j, k) = edge_total<R>(t, ea, hadv);  // edgey_u
-            a.ef[0](i, j, k) = edge_total<R>(t, eb, hadv);  // edgex_v
+            const Taus<R> t = edge_taus<NS, R, NZ, 0, WL>(P, a.F, a.noise, i, j, k);
+            edge_adv<NS, R, 0, WL>(P, a.F, i, j, k, ea, eb);
+            a.ef[2](i, j, k) = WL ? edge_total_w<R, 0>(P, t, ea, hadv, i, j, k) : edge_total<R>(t, ea, hadv);  // edgey_u
+            a.ef[0](i, j, k) = WL ? edge_total_w<R, 0>(P, t, eb, hadv, i, j, k) : edge_total<R>(t, eb, hadv);  // edgex_v
         } else if (q < nxy + nxz) {
             const int64_t r = q - nxy;
             const int i = (int)(r % (N[0] + 1)), j = (int)((r / (N[0] + 1)) % N[1]), k = (int)(r / ((int64_t)(N[0] + 1) * N[1]));
-            const Taus<R> t = edge_taus<NS, R, NZ, 1>(P, a.F, a.noise, i, j, k);
-            edge_adv<NS, R, 1>(P, a.F, i, j, k, ea, eb);
-            a.ef[4](i, j, k) = edge_total<R>(t, ea, hadv);  // edgez_u
-            a.ef[1](i, j, k) = edge_total<R>(t, eb, hadv);  // edgex_w
+            const Taus<R> t = edge_taus<NS, R, NZ, 1, WL>(P, a.F, a.noise, i, j, k);
+            edge_adv<NS, R, 1, WL>(P, a.F, i, j, k, ea, eb);
+            a.ef[4](i, j, k) = WL ? edge_total_w<R, 1>(P, t, ea, hadv, i, j, k) : edge_total<R>(t, ea, hadv);  // edgez_u
+            a.ef[1](i, j, k) = WL ? edge_total_w<R, 1>(P, t, eb, hadv, i, j, k) : edge_total<R>(t, eb, hadv);  // edgex_w
         } else if (q < nxy + nxz + nyz) {
             const int64_t r = q - nxy - nxz;
             const int i = (int)(r % N[0]), j = (int)((r / N[0]) % (N[1] + 1)), k = (int)(r / ((int64_t)N[0] * (N[1] + 1)));
-            const Taus<R> t = edge_taus<NS, R, NZ, 2>(P, a.F, a.noise, i, j, k);
-            edge_adv<NS, R, 2>(P, a.F, i, j, k, ea, eb);
-            a.ef[5](i, j, k) = edge_total<R>(t, ea, hadv);  // edgez_v
-            a.ef[3](i, j, k) = edge_total<R>(t, eb, hadv);  // edgey_w
+            const Taus<R> t = edge_taus<NS, R, NZ, 2, WL>(P, a.F, a.noise, i, j, k);
+            edge_adv<NS, R, 2, WL>(P, a.F, i, j, k, ea, eb);
+            a.ef[5](i, j, k) = WL ? edge_total_w<R, 2>(P, t, ea, hadv, i, j, k) : edge_total<R>(t, ea, hadv);  // edgez_v
+            a.ef[3](i, j, k) = WL ? edge_total_w<R, 2>(P, t, eb, hadv, i, j, k) : edge_total<R>(t, eb, hadv);  // edgey_w
         } else {
             const int64_t r = q - nxy - nxz - nyz;
             const int i = (int)(r % (N[0] + 2)) - 1, j = (int)((r / (N[0] + 2)) % (N[1] + 2)) - 1,
@@ -618,7 +636,8 @@ static __global__ void __launch_bounds__(128) k_aux_edges_cen(AuxArgs<NS, R, NZ>
 struct NoiseFillArgs {
     DevParams P;
     Arr4<double> f;
-    int vx, vy, vz;   // valid extents
+    int vx, vy, vz;   // extents of the filled box
+    int ox, oy, oz;   // its low corner (0, or -1 to take the ghost layer of a wall direction)
     int c0, nc;
     double mean, sd;
     uint32_t fid0;
@@ -631,7 +650,8 @@ FHD_D double uniform53(uint32_t w0, uint32_t w1) {
 static __global__ void k_noise_fill(NoiseFillArgs a) {
     const int64_t tot = (int64_t)a.vx * a.vy * a.vz * a.nc;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < tot; q += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(q % a.vx), j = (int)((q / a.vx) % a.vy), k = (int)((q / ((int64_t)a.vx * a.vy)) % a.vz);
+        const int i = (int)(q % a.vx) + a.ox, j = (int)((q / a.vx) % a.vy) + a.oy,
+                  k = (int)((q / ((int64_t)a.vx * a.vy)) % a.vz) + a.oz;
         const int c = (int)(q / ((int64_t)a.vx * a.vy * a.vz));
         if (a.use_b == 2) {
             uint32_t w[4] = {canon(a.P, i, j, k), a.fid0 + (uint32_t)c, (uint32_t)a.P.step, (uint32_t)(a.P.step >> 32)};

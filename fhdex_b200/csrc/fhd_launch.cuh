@@ -3,6 +3,7 @@
 #include "fhd_host.h"
 #include "fhd_kernels.cuh"
 #include "fhd_fused.cuh"
+#include "fhd_walls.cuh"
 
 namespace fhd {
 
@@ -241,6 +242,63 @@ int launch_stage_zm_t(const StageCall& c) {
         case 384: return launch_stage_zm_bt<NS, R, NZ, 384>(c, kZmChunks[t]);
         default: return launch_stage_zm_bt<NS, R, NZ, 128>(c, kZmChunks[t]);
     }
+}
+
+// the stage parts of a box with physical walls (FP64, one launch shape): the wall
+// variants of the stresses and face fluxes, and the common update
+template <int NS, int NZ>
+int launch_walls_part_t(const StageCall& c, int part) {
+    const StageArgs<NS, double, NZ> a = make_stage_args<NS, double, NZ>(c);
+    const int* N = c.P.n;
+    if (part == 0) {
+        k_taus<NS, double, NZ, true><<<grid_for((int64_t)(N[0] + 2) * (N[1] + 2) * (N[2] + 2), 128), 128, 0, c.stream>>>(a);
+    } else if (part == 1) {
+        k_faces<NS, double, NZ, 0, 128, 4, true><<<resident_grid<k_faces<NS, double, NZ, 0, 128, 4, true>>(
+            (int64_t)(N[0] + 1) * N[1] * N[2], 128), 128, 0, c.stream>>>(a);
+        k_faces<NS, double, NZ, 1, 128, 4, true><<<resident_grid<k_faces<NS, double, NZ, 1, 128, 4, true>>(
+            (int64_t)N[0] * (N[1] + 1) * N[2], 128), 128, 0, c.stream>>>(a);
+        k_faces<NS, double, NZ, 2, 128, 4, true><<<resident_grid<k_faces<NS, double, NZ, 2, 128, 4, true>>(
+            (int64_t)N[0] * N[1] * (N[2] + 1), 128), 128, 0, c.stream>>>(a);
+    } else {
+        k_update<NS, double, NZ><<<resident_grid<k_update<NS, double, NZ>>(
+            (int64_t)(N[0] + 1) * (N[1] + 1) * (N[2] + 1), 128), 128, 0, c.stream>>>(a);
+    }
+    return cuda_rc(cudaGetLastError());
+}
+
+template <int NS>
+int launch_walls_part(const StageCall& c, int part) {
+    switch (c.mode) {
+        case NM_OFF: return launch_walls_part_t<NS, NZ_OFF>(c, part);
+        case NM_AB: return launch_walls_part_t<NS, NZ_AB>(c, part);
+        case NM_PHILOX: return launch_walls_part_t<NS, NZ_PHILOX>(c, part);
+        default: return FHD_ERR_BAD_ARG;
+    }
+}
+
+// BCMassTempPress + BCRhoRhoE on the ghost cells of the wall directions
+template <int NS>
+int launch_bc_prim(const DevParams& P, const WallParams& W, const fhd_fab& prim, const fhd_fab& cons,
+                   const fhd_fab mom[3], cudaStream_t s) {
+    BcPrimArgs<NS> a;
+    a.P = P;
+    a.W = W;
+    a.prim = view<double>(prim);
+    a.cons = view<double>(cons);
+    for (int d = 0; d < 3; ++d) a.mom[d] = view<const double>(mom[d]);
+    const int g = -prim.lo[0];
+    int blo[3], bhi[3], clo[3], chi[3];
+    for (int d = 0; d < 3; ++d) {
+        blo[d] = -g;
+        bhi[d] = P.n[d] - 1 + g;
+        const bool w = P.walls && !P.periodic[d];
+        clo[d] = w ? 0 : blo[d];
+        chi[d] = w ? P.n[d] - 1 : bhi[d];
+    }
+    a.sh = make_shell(blo, bhi, clo, chi);
+    if (a.sh.n == 0) return FHD_OK;
+    k_bc_prim<NS><<<grid_for(a.sh.n, 128), 128, 0, s>>>(a);
+    return cuda_rc(cudaGetLastError());
 }
 
 // part: 0 stresses, 1 face fluxes, 2 update, 3 the fused kernel (all three)

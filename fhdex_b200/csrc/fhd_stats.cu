@@ -356,13 +356,13 @@ static int stats_launch(const StatsArgs& a, bool means, bool vars, const fhd_fab
         k_stats_means_a<<<grid_for(ga, 256), 256, 0, s>>>(a);
         k_stats_means_b<NS><<<grid_for(gb, 256), 256, 0, s>>>(a);
         const GhostReq g[2] = {{cuMeans, 0, cuMeans.ncomp}, {primMeans, 0, primMeans.ncomp}};
-        const int rc = fill_ghosts(g, 2, n, s);
+        const int rc = fill_ghosts(g, 2, n, s, a.P.periodic, 0);
         if (rc) return rc;
     }
     if (vars) {
         k_stats_vars<NS><<<grid_for(gb, 256), 256, 0, s>>>(a);
         const GhostReq g[2] = {{cuVars, 0, cuVars.ncomp}, {primVars, 0, primVars.ncomp}};
-        const int rc = fill_ghosts(g, 2, n, s);
+        const int rc = fill_ghosts(g, 2, n, s, a.P.periodic, 0);
         if (rc) return rc;
     }
     return cuda_rc(cudaGetLastError());

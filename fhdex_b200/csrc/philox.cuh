@@ -78,9 +78,19 @@ FHD_D void normal_pair(uint32_t key0, uint32_t key1, uint32_t pidx, uint32_t fid
 // canonical periodic index of a point within one period of the box
 FHD_HD int wrap1(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
+// Directions with walls are not periodic: there a point keeps its own index,
+// shifted by one so that the ghost cell -1 and the cell/node n are distinct
+// (n + 2 indices: cells -1..n, nodes 0..n), as the reference's wall directions
+// neither OverrideSync nor FillBoundary their noise.
+FHD_HD uint32_t canon1(const DevParams& P, int d, int i) {
+    return P.periodic[d] ? (uint32_t)wrap1(i, P.n[d]) : (uint32_t)(i + 1);
+}
 FHD_HD uint32_t canon(const DevParams& P, int i, int j, int k) {
-    return (uint32_t)wrap1(i, P.n[0]) +
-           (uint32_t)P.n[0] * ((uint32_t)wrap1(j, P.n[1]) + (uint32_t)P.n[1] * (uint32_t)wrap1(k, P.n[2]));
+    if (!P.walls)
+        return (uint32_t)wrap1(i, P.n[0]) +
+               (uint32_t)P.n[0] * ((uint32_t)wrap1(j, P.n[1]) + (uint32_t)P.n[1] * (uint32_t)wrap1(k, P.n[2]));
+    const uint32_t sx = P.periodic[0] ? P.n[0] : P.n[0] + 2, sy = P.periodic[1] ? P.n[1] : P.n[1] + 2;
+    return canon1(P, 0, i) + sx * (canon1(P, 1, j) + sy * canon1(P, 2, k));
 }
 
 // Field ids: face d comp c (0 energy, 1.. species) -> 16 d + c; edges xy, xz, yz ->

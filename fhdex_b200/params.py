@@ -52,6 +52,24 @@ class Params:
     beta_param: tuple = ()
     T0_chem: float = 0.0
     avogadro: float = 0.0
+    # physical boundaries (boundaryStag.cpp; the reference's deck keys): walls = 0
+    # fully periodic; else a direction with bc_vel_lo == bc_vel_hi == -1 is
+    # periodic and the others have walls on both sides (bc_vel 1 slip / 2 no-slip,
+    # bc_therm 1 adiabatic / 2 isothermal at t_lo / t_hi, bc_mass 1 impermeable /
+    # 2 wall composition bc_Yk or bc_Xk, one tuple of nspecies values per direction)
+    walls: int = 0
+    bc_vel_lo: tuple = (-1, -1, -1)
+    bc_vel_hi: tuple = (-1, -1, -1)
+    bc_mass_lo: tuple = (-1, -1, -1)
+    bc_mass_hi: tuple = (-1, -1, -1)
+    bc_therm_lo: tuple = (-1, -1, -1)
+    bc_therm_hi: tuple = (-1, -1, -1)
+    t_lo: tuple = (0.0, 0.0, 0.0)
+    t_hi: tuple = (0.0, 0.0, 0.0)
+    bc_Yk_lo: tuple = ((), (), ())
+    bc_Yk_hi: tuple = ((), (), ())
+    bc_Xk_lo: tuple = ((), (), ())
+    bc_Xk_hi: tuple = ((), (), ())
     # initial state (prob_type 1): not part of fhd_params
     rho0: float = 1.78e-3
     T_init: float = 273.0
@@ -121,6 +139,15 @@ class Params:
             p.beta_param[m] = self.beta_param[m] if m < len(self.beta_param) else 0.0
         p.T0_chem = self.T0_chem
         p.avogadro = self.avogadro
+        p.walls = 1 if self.walls else 0
+        for d in range(3):
+            for name in ("bc_vel_lo", "bc_vel_hi", "bc_mass_lo", "bc_mass_hi", "bc_therm_lo", "bc_therm_hi",
+                         "t_lo", "t_hi"):
+                getattr(p, name)[d] = getattr(self, name)[d]
+            for name in ("bc_Yk_lo", "bc_Yk_hi", "bc_Xk_lo", "bc_Xk_hi"):
+                vals = getattr(self, name)[d]
+                for i in range(MAX_SPECIES):
+                    getattr(p, name)[d][i] = vals[i] if i < len(vals) else -1.0
         return p
 
     # -- thermodynamics on the host (for dt and theory) -------------------------------
@@ -219,6 +246,30 @@ def hard_sphere_single_gas(p: Params, T=None):
     return eta, kappa
 
 
+def with_walls(p: Params, **dirs) -> Params:
+    """``p`` with physical walls on the directions named x, y, z (both sides),
+    each a dict: vel (1 slip, 2 no-slip), therm (1 adiabatic, 2 isothermal), mass
+    (1 impermeable, 2 held at a wall composition), t = (t_lo, t_hi) for isothermal
+    walls, Yk or Xk = (lo, hi) compositions for concentration walls.  The other
+    directions stay periodic."""
+    vl, vh, ml, mh, tl, th = ([-1] * 3 for _ in range(6))
+    Tl, Th = [0.0] * 3, [0.0] * 3
+    comp = {k: [(), (), ()] for k in ("bc_Yk_lo", "bc_Yk_hi", "bc_Xk_lo", "bc_Xk_hi")}
+    for ax, spec in dirs.items():
+        d = "xyz".index(ax)
+        vl[d] = vh[d] = int(spec.get("vel", 2))
+        ml[d] = mh[d] = int(spec.get("mass", 1))
+        tl[d] = th[d] = int(spec.get("therm", 1))
+        Tl[d], Th[d] = (float(v) for v in spec.get("t", (p.T_init, p.T_init)))
+        for key in ("Yk", "Xk"):
+            if key in spec:
+                comp[f"bc_{key}_lo"][d] = tuple(float(v) for v in spec[key][0])
+                comp[f"bc_{key}_hi"][d] = tuple(float(v) for v in spec[key][1])
+    return p.replace(walls=1, bc_vel_lo=tuple(vl), bc_vel_hi=tuple(vh), bc_mass_lo=tuple(ml),
+                     bc_mass_hi=tuple(mh), bc_therm_lo=tuple(tl), bc_therm_hi=tuple(th), t_lo=tuple(Tl),
+                     t_hi=tuple(Th), **{k: tuple(v) for k, v in comp.items()})
+
+
 def stable_dt(p: Params, cfl=0.2, diff=0.1):
     """dt = min(cfl*dx/(c+|u|), diff*dx^2/max(nu, chi)) at the initial state (|u| = 0).
     The configured acoustic CFL 0.2 alone violates the explicit diffusive limit at
@@ -266,7 +317,16 @@ def to_inputs(p: "Params") -> str:
     if p.zeta_ratio >= 0:
         lines.append(f"zeta_ratio = {_fmt(float(p.zeta_ratio))}")
     for key in ("bc_vel_lo", "bc_vel_hi", "bc_mass_lo", "bc_mass_hi", "bc_therm_lo", "bc_therm_hi"):
-        lines.append(f"{key} = -1 -1 -1")
+        vals = getattr(p, key) if p.walls else (-1, -1, -1)
+        lines.append(row(key, [int(x) for x in vals]))
+    if p.walls:
+        lines += [row("t_lo", p.t_lo), row("t_hi", p.t_hi)]
+        for name, key in (("bc_Yk_lo", "bc_Yk_{}_lo"), ("bc_Yk_hi", "bc_Yk_{}_hi"), ("bc_Xk_lo", "bc_Xk_{}_lo"),
+                          ("bc_Xk_hi", "bc_Xk_{}_hi")):
+            for d, ax in enumerate("xyz"):
+                vals = getattr(p, name)[d]
+                if len(vals):
+                    lines.append(row(key.format(ax), [float(v) for v in vals]))
     if p.nreaction > 0:
         nr = p.nreaction
         lines += [f"nreaction = {nr}", f"reaction_type = {p.reaction_type}"]
@@ -286,8 +346,8 @@ _LIST_KEYS = ("n_cells", "prob_lo", "prob_hi", "molmass", "diameter", "dof", "e0
 
 def parse_inputs(text: str, base: Params | None = None) -> Params:
     """Parse an FHDeX inputs deck (reference key names) into Params.  Keys outside
-    this path (plot_int, struct_fact_int, bc_*, ...) are ignored; only fully
-    periodic decks are accepted."""
+    this path (plot_int, struct_fact_int, ...) are ignored; reservoir boundaries
+    are rejected."""
     kv = {}
     for line in text.splitlines():
         line = line.split("#", 1)[0].strip()
@@ -332,9 +392,23 @@ def parse_inputs(text: str, base: Params | None = None) -> Params:
     if "avogadro" in kv:
         upd["avogadro"] = float(kv["avogadro"][0])
         upd["Runiv"] = upd.get("k_B", p.k_B) * upd["avogadro"]
-    for key in ("bc_vel_lo", "bc_vel_hi", "bc_mass_lo", "bc_mass_hi", "bc_therm_lo", "bc_therm_hi"):
-        if key in kv and any(int(x) != -1 for x in kv[key]):
-            raise ValueError(f"{key}: only fully periodic boundaries are implemented")
+    # physical boundaries (boundaryStag.cpp): walls on the directions whose bc_vel is
+    # not -1; reservoirs (bc_mass >= 3) are outside the implemented scope
+    bck = ("bc_vel_lo", "bc_vel_hi", "bc_mass_lo", "bc_mass_hi", "bc_therm_lo", "bc_therm_hi")
+    if any(k in kv and any(int(x) != -1 for x in kv[k]) for k in bck):
+        upd["walls"] = 1
+        for key in bck:
+            if key in kv:
+                upd[key] = tuple(int(x) for x in kv[key][:3])
+        for key in ("bc_mass_lo", "bc_mass_hi"):
+            if any(v >= 3 for v in upd.get(key, ())):
+                raise ValueError(f"{key}: reservoir boundaries (bc_mass >= 3) are not implemented")
+        for key in ("t_lo", "t_hi"):
+            if key in kv:
+                upd[key] = tuple(float(x) for x in kv[key][:3])
+        for name, pat in (("bc_Yk_lo", "bc_Yk_{}_lo"), ("bc_Yk_hi", "bc_Yk_{}_hi"), ("bc_Xk_lo", "bc_Xk_{}_lo"),
+                          ("bc_Xk_hi", "bc_Xk_{}_hi")):
+            upd[name] = tuple(tuple(float(x) for x in kv.get(pat.format(ax), [])[:ns]) for ax in "xyz")
     if "dof" in upd and "hcv" not in upd:
         upd["hcv"] = (-1.0,) * ns
         upd["hcp"] = (-1.0,) * ns

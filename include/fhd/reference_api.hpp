@@ -103,6 +103,22 @@ inline int plot_covars = 0;
 inline int plot_mom3 = 0;
 inline int plot_mom4 = 0;
 inline int plot_deltaY_dir = -1;  // common_functions.cpp:620
+// Physical boundaries (common_namespace.H:150-185, read at common_functions.cpp:800-900).
+// A direction whose bc_vel_lo and bc_vel_hi are both -1 is periodic (the default
+// here; the staggered decks set every bc_vel); otherwise both sides are walls:
+// bc_vel 1 slip / 2 no-slip, bc_therm 1 adiabatic / 2 isothermal at t_lo / t_hi,
+// bc_mass 1 impermeable / 2 at the wall composition bc_Yk_* or bc_Xk_* (the one
+// that sums to 1).  Reservoirs (bc_mass >= 3) are refused.
+inline GpuArray<int, 3> bc_vel_lo{{-1, -1, -1}}, bc_vel_hi{{-1, -1, -1}};
+inline GpuArray<int, 3> bc_mass_lo{{-1, -1, -1}}, bc_mass_hi{{-1, -1, -1}};
+inline GpuArray<int, 3> bc_therm_lo{{-1, -1, -1}}, bc_therm_hi{{-1, -1, -1}};
+inline GpuArray<Real, 3> t_lo{{0., 0., 0.}}, t_hi{{0., 0., 0.}};
+inline GpuArray<Real, MAX_SPECIES> bc_Yk_x_lo{{-1, -1, -1, -1, -1, -1, -1, -1}}, bc_Yk_x_hi{{-1, -1, -1, -1, -1, -1, -1, -1}};
+inline GpuArray<Real, MAX_SPECIES> bc_Yk_y_lo{{-1, -1, -1, -1, -1, -1, -1, -1}}, bc_Yk_y_hi{{-1, -1, -1, -1, -1, -1, -1, -1}};
+inline GpuArray<Real, MAX_SPECIES> bc_Yk_z_lo{{-1, -1, -1, -1, -1, -1, -1, -1}}, bc_Yk_z_hi{{-1, -1, -1, -1, -1, -1, -1, -1}};
+inline GpuArray<Real, MAX_SPECIES> bc_Xk_x_lo{{-1, -1, -1, -1, -1, -1, -1, -1}}, bc_Xk_x_hi{{-1, -1, -1, -1, -1, -1, -1, -1}};
+inline GpuArray<Real, MAX_SPECIES> bc_Xk_y_lo{{-1, -1, -1, -1, -1, -1, -1, -1}}, bc_Xk_y_hi{{-1, -1, -1, -1, -1, -1, -1, -1}};
+inline GpuArray<Real, MAX_SPECIES> bc_Xk_z_lo{{-1, -1, -1, -1, -1, -1, -1, -1}}, bc_Xk_z_hi{{-1, -1, -1, -1, -1, -1, -1, -1}};
 }  // namespace common
 
 namespace chemistry {
@@ -195,6 +211,27 @@ inline fhd_params params_from_globals() {
     }
     p.T0_chem = chemistry::T0_chem;
     p.avogadro = common::avogadro;
+    const amrex_compat::GpuArray<Real, MAX_SPECIES>* yk[2][3] = {{&common::bc_Yk_x_lo, &common::bc_Yk_y_lo, &common::bc_Yk_z_lo},
+                                                   {&common::bc_Yk_x_hi, &common::bc_Yk_y_hi, &common::bc_Yk_z_hi}};
+    const amrex_compat::GpuArray<Real, MAX_SPECIES>* xk[2][3] = {{&common::bc_Xk_x_lo, &common::bc_Xk_y_lo, &common::bc_Xk_z_lo},
+                                                   {&common::bc_Xk_x_hi, &common::bc_Xk_y_hi, &common::bc_Xk_z_hi}};
+    for (int d = 0; d < 3; ++d) {
+        if (common::bc_vel_lo[d] != -1 || common::bc_vel_hi[d] != -1) p.walls = 1;
+        p.bc_vel_lo[d] = common::bc_vel_lo[d];
+        p.bc_vel_hi[d] = common::bc_vel_hi[d];
+        p.bc_mass_lo[d] = common::bc_mass_lo[d];
+        p.bc_mass_hi[d] = common::bc_mass_hi[d];
+        p.bc_therm_lo[d] = common::bc_therm_lo[d];
+        p.bc_therm_hi[d] = common::bc_therm_hi[d];
+        p.t_lo[d] = common::t_lo[d];
+        p.t_hi[d] = common::t_hi[d];
+        for (int s = 0; s < FHD_MAX_SPECIES; ++s) {
+            p.bc_Yk_lo[d][s] = (*yk[0][d])[s];
+            p.bc_Yk_hi[d][s] = (*yk[1][d])[s];
+            p.bc_Xk_lo[d][s] = (*xk[0][d])[s];
+            p.bc_Xk_hi[d][s] = (*xk[1][d])[s];
+        }
+    }
     return p;
 }
 
@@ -291,6 +328,25 @@ inline void InitConsVarStag(fhd::amrex_compat::MultiFab& cons,
     check(fhd_init_cons_var_stag(context(), cons.fab(), mom, common::rho0, common::T_init[0],
                                  common::rhobar.data()),
           "InitConsVarStag");
+}
+
+// setBCStag (boundaryStag.cpp:268-298): the wall conditions on every ghost of a
+// wall direction and the wall faces; nothing on a fully periodic box.
+inline void setBCStag(fhd::amrex_compat::MultiFab& prim_in, fhd::amrex_compat::MultiFab& cons_in,
+                      std::array<fhd::amrex_compat::MultiFab, 3>& cumom_in,
+                      std::array<fhd::amrex_compat::MultiFab, 3>& vel_in,
+                      const fhd::amrex_compat::Geometry& /*geom*/) {
+    using namespace fhd::ref;
+    require_device(prim_in, "setBCStag");
+    require_device(cons_in, "setBCStag");
+    fhd_fab mom[3], vel[3];
+    for (int d = 0; d < 3; ++d) {
+        require_device(cumom_in[d], "setBCStag");
+        require_device(vel_in[d], "setBCStag");
+    }
+    fabs_of(cumom_in, mom);
+    fabs_of(vel_in, vel);
+    check(fhd_set_bc_stag(context(), prim_in.fab(), cons_in.fab(), mom, vel), "setBCStag");
 }
 
 // conservedToPrimitiveStag (conservedPrimitiveConversionsStag.cpp:5-144).

@@ -110,6 +110,24 @@ typedef struct {
     double beta_param[FHD_MAX_REACTIONS];   /* (T/T0)^beta                                 */
     double T0_chem;         /* > 0 when nreaction > 0                                   */
     double avogadro;        /* <= 0: Runiv / k_B (common_functions.cpp:775)             */
+    /* Physical boundaries (boundaryStag.cpp; deck keys bc_vel_lo/hi, bc_mass_lo/hi,
+     * bc_therm_lo/hi, t_lo/hi, bc_Yk_<x|y|z>_lo/hi, bc_Xk_<x|y|z>_lo/hi).  walls = 0:
+     * fully periodic and the fields below are ignored.  walls = 1: direction d is
+     * periodic when bc_vel_lo[d] == bc_vel_hi[d] == -1; otherwise both of its sides
+     * are walls with bc_vel 1 (slip) or 2 (no-slip), bc_therm 1 (adiabatic) or 2
+     * (isothermal at t_lo[d] / t_hi[d]) and bc_mass 1 (impermeable) or 2 (species
+     * held at the wall composition bc_Yk / bc_Xk, of which the one summing to 1
+     * defines the other, as SetupCWallStag does; fhd_get_params returns both).
+     * Reservoirs (bc_mass >= 3) are outside the implemented scope.  FP64 only;
+     * the state's ghost width is then exactly 2 in fhd_rk3_step_stag(s), and
+     * the batched and no-allocation steps return FHD_ERR_UNSUPPORTED. */
+    int walls;
+    int bc_vel_lo[3], bc_vel_hi[3];
+    int bc_mass_lo[3], bc_mass_hi[3];
+    int bc_therm_lo[3], bc_therm_hi[3];
+    double t_lo[3], t_hi[3];
+    double bc_Yk_lo[3][FHD_MAX_SPECIES], bc_Yk_hi[3][FHD_MAX_SPECIES];
+    double bc_Xk_lo[3][FHD_MAX_SPECIES], bc_Xk_hi[3][FHD_MAX_SPECIES];
 } fhd_params;
 
 /* Injected Gaussian noise for one RK3 step: the "A" and "B" white-noise fields
@@ -147,7 +165,7 @@ int fhd_set_stream(fhd_ctx* ctx, void* stream);
 int fhd_synchronize(fhd_ctx* ctx);
 /* Reads and clears the device status word (blocks on the stream). */
 int fhd_status(fhd_ctx* ctx);
-/* Effective parameters (after GetHcGas). */
+/* Effective parameters (after GetHcGas and SetupCWallStag). */
 int fhd_get_params(const fhd_ctx* ctx, fhd_params* out);
 /* Launch shape of the stage kernels (index into fhd_tile_name's list); the
  * autotuner in the host layer times them and sets the fastest.  No reference
@@ -187,12 +205,23 @@ int fhd_flux_stag(fhd_ctx* ctx, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim,
                   const fhd_fab stochface[3], const fhd_fab stochedge[3],
                   const fhd_fab stochcen[3], double dt);
 
-/* MultiFab::FillBoundary(periodicity) for a fully periodic single box:
- * ghosts <- periodic images of valid points; valid points untouched. */
+/* MultiFab::FillBoundary(periodicity) for a single box: ghosts <- periodic
+ * images of valid points; valid points untouched.  With walls only the ghosts
+ * outside the box in periodic directions alone are filled (AMReX fills no ghost
+ * that is outside the domain in a non-periodic direction). */
 int fhd_fill_boundary(fhd_ctx* ctx, fhd_fab f);
 /* MultiFab::OverrideSync(periodicity): periodic duplicates of nodal points take
- * the value of the low-side owner (point n_cells[d] <- point 0). */
+ * the value of the low-side owner (point n_cells[d] <- point 0); wall directions
+ * have no duplicates. */
 int fhd_override_sync(fhd_ctx* ctx, fhd_fab f);
+
+/* setBCStag: boundaryStag.cpp:268-298 (declared compressible_functions_stag.H).
+ * BCMassTempPress, BCMomNormal, BCMomTrans of every direction, then BCRhoRhoE:
+ * on a box with walls, sets the wall faces' normal momentum and velocity to 0
+ * and every ghost of a wall direction of prim (rho, T, p, Y, X), cu (rho, rho E,
+ * rho Y), cumom and vel.  prim and cu have one ghost width, cumom and vel all
+ * the same one; a fully periodic context does nothing. */
+int fhd_set_bc_stag(fhd_ctx* ctx, fhd_fab prim, fhd_fab cu, const fhd_fab cumom[3], const fhd_fab vel[3]);
 
 /* MultiFabFillRandomNormal: MultiFabFillRandom.cpp:34-50 (declared
  * rng_functions.H:13-22).  Philox-4x32-10 normals; `stream_id` selects an

@@ -61,6 +61,8 @@ def lib():
         L.fhdref_noise_log.argtypes = [P(i), P(i), P(d), i]
         L.fhdref_chemistry_source.argtypes = [d, d, vp, vp, vp]
         L.fhdref_max_acoustic_cfl.argtypes = [vp, pp, d, P(d)]
+        L.fhdref_fill_boundary.argtypes = [vp, P(i), i, i, i]
+        L.fhdref_wall_composition.argtypes = [i, P(d), P(d)]
         _lib = L
     return _lib
 
@@ -216,6 +218,78 @@ def chemistry_source(p, dt, dV, prim, source, ranchem):
     init(p)
     _chk(lib().fhdref_chemistry_source(dt, dV, _ptr(prim.arr), _ptr(source.arr), _ptr(ranchem.arr)),
          "compute_compressible_chemistry_source_CLE")
+
+
+def fill_boundary(p, mf, override_sync=False):
+    """The stand-in's FillBoundary (and OverrideSync) of one host MultiFab with p's
+    periodicity: ghost points of wall directions are left alone."""
+    init(p)
+    nod = (C.c_int * 3)(*mf.nodal)
+    _chk(lib().fhdref_fill_boundary(_ptr(mf.arr), nod, mf.ncomp, mf.ngrow, int(override_sync)), "FillBoundary")
+
+
+def wall_composition(p, side):
+    """(Yk, Xk) of wall side 2 d + hi after SetupCWallStag."""
+    init(p)
+    y = (C.c_double * 8)()
+    x = (C.c_double * 8)()
+    _chk(lib().fhdref_wall_composition(side, y, x), "SetupCWallStag")
+    return list(y[:p.nspecies]), list(x[:p.nspecies])
+
+
+def state_from_reference(p, seed=0, amp=0.02, vel_amp=0.05):
+    """A perturbed physical state made with the reference's own operators, valid
+    for walls: InitConsVarStag, random perturbations of the valid density,
+    composition, energy and face momenta, then conservedToPrimitiveStag,
+    FillBoundary (periodic directions) and setBCStag, main_driver's init sequence
+    (main_driver.cpp:757-794)."""
+    from fhdex_b200.state import StagState
+    st = StagState(p)
+    init(p)
+    init_cons_var_stag(st)
+    g = torch.Generator().manual_seed(seed)
+    ns = p.nspecies
+    vc = st.cu.valid()
+    shp = vc.shape[1:]
+    rho = vc[0].clone()
+    frac = torch.stack([vc[5 + s] / rho for s in range(ns)])
+    frac = frac * (1.0 + amp * (2 * torch.rand((ns,) + shp, generator=g, dtype=torch.float64) - 1))
+    frac = frac / frac.sum(0)
+    rho_new = rho * (1.0 + amp * (2 * torch.rand(shp, generator=g, dtype=torch.float64) - 1))
+    vc[0] = rho_new
+    for s in range(ns):
+        vc[5 + s] = rho_new * frac[s]
+    vc[4] = vc[4] * (1.0 + 0.5 * amp * (2 * torch.rand(shp, generator=g, dtype=torch.float64) - 1))
+    c = p.sound_speed()
+    for d in range(3):
+        mv = st.cumom[d].valid(0)
+        mv.copy_(p.rho0 * vel_amp * c * (2 * torch.rand(mv.shape, generator=g, dtype=torch.float64) - 1))
+        fill_boundary(p, st.cumom[d], override_sync=True)
+    fill_boundary(p, st.cu)
+    conserved_to_primitive(st)
+    for m in [st.cu, st.prim] + st.vel:
+        fill_boundary(p, m)
+    set_bc(st)
+    return st
+
+
+def step_noise(p, seed):
+    """A/B noise of one step as the reference's fills leave it: standard normals
+    (faces, edges) and normals of variance 2 (centres, one ghost) at every point of
+    each field's storage, then OverrideSync and FillBoundary with p's periodicity
+    (wall directions keep their own values, ghosts included)."""
+    import math as _m
+    from fhdex_b200.state import StepNoise
+    nz = StepNoise(p)
+    g = torch.Generator().manual_seed(seed)
+    for s_ in range(2):
+        for d in range(3):
+            for mf, var in ((nz.face[s_][d], 1.0), (nz.edge[s_][d], 1.0), (nz.cen[s_][d], 2.0)):
+                mf.arr.copy_(_m.sqrt(var) * torch.randn(mf.arr.shape, generator=g, dtype=torch.float64))
+                fill_boundary(p, mf, override_sync=True)
+        if nz.chem[s_] is not None:
+            nz.chem[s_].arr.copy_(torch.randn(nz.chem[s_].arr.shape, generator=g, dtype=torch.float64))
+    return nz
 
 
 def max_acoustic_cfl(st, dt):

@@ -112,6 +112,7 @@ int fhdref_init(const char* inputs) {
                 is_periodic[i] = 1;
             }
         SetupBCStag();
+        if (algorithm_type == 2) SetupCWallStag();  // main_driver.cpp:147-151
         Box domain(IntVect(0, 0, 0), IntVect(n_cells[0] - 1, n_cells[1] - 1, n_cells[2] - 1));
         RealBox real_box({prob_lo[0], prob_lo[1], prob_lo[2]}, {prob_hi[0], prob_hi[1], prob_hi[2]});
         g_geom.define(domain, real_box, 0, is_periodic);
@@ -123,6 +124,33 @@ int fhdref_init(const char* inputs) {
         g_ready = false;
         return 1;
     }
+}
+
+// FillBoundary / OverrideSync of one MultiFab (the stand-in's, with the run's
+// periodicity: wall directions are left alone), for the harness's initial states
+// and noise fields.
+int fhdref_fill_boundary(double* p, const int* nodal, int nc, int ng, int override_sync) {
+    return guarded([&] {
+        MultiFab m;
+        wrap(m, p, IntVect(nodal[0], nodal[1], nodal[2]), nc, ng);
+        if (override_sync) m.OverrideSync(g_geom.periodicity());
+        m.FillBoundary(g_geom.periodicity());
+    });
+}
+
+// Wall compositions after SetupCWallStag (bc_Yk / bc_Xk of side s = 2 d + hi).
+int fhdref_wall_composition(int s, double* yk, double* xk) {
+    return guarded([&] {
+        const int d = s / 2, hi = s % 2;
+        const GpuArray<Real, MAX_SPECIES>* Y[6] = {&bc_Yk_x_lo, &bc_Yk_x_hi, &bc_Yk_y_lo, &bc_Yk_y_hi, &bc_Yk_z_lo,
+                                                   &bc_Yk_z_hi};
+        const GpuArray<Real, MAX_SPECIES>* X[6] = {&bc_Xk_x_lo, &bc_Xk_x_hi, &bc_Xk_y_lo, &bc_Xk_y_hi, &bc_Xk_z_lo,
+                                                   &bc_Xk_z_hi};
+        for (int n = 0; n < nspecies; ++n) {
+            yk[n] = (*Y[2 * d + hi])[n];
+            xk[n] = (*X[2 * d + hi])[n];
+        }
+    });
 }
 
 // Derived globals after GetHcGas, for the harness's consistency checks.
