@@ -415,28 +415,32 @@ def step_extras(args, p, dt, local, peak, peak_kind):
     nb = args.bench_batch_steps
     batched = {"config": {"members": args.members, "sizes": "half 32^3, half 64^3", "gas": "argon (2 species)",
                           "T0": "U(250, 350) K", "rho0": "U(1e-3, 3e-3) g/cm^3", "steps": nb,
-                          "launch": "23 batched kernels per step, one CUDA graph replay per step"}}
+                          "launch": "fp64 / mixed: 23 batched kernels per step, one CUDA graph replay per step; "
+                                    "*_persistent: one persistent launch per step (k_batch_persist), graph replay"}}
     members = None
     for prec, key in ((0, "fp64"), (1, "mixed")):
         b, states, bcells = ensemble(args.members, seed=args.seed, precision=prec)
         members = [q for q, _ in states]
         s_ = torch.cuda.Stream(local)
         b.set_stream(s_)
-        b.step(3, graph=True)
-        b.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        with torch.cuda.stream(s_):
-            e0.record()
-        b.step(nb, graph=True)
-        with torch.cuda.stream(s_):
-            e1.record()
-        b.synchronize()
-        ms = e0.elapsed_time(e1)
-        bad = sum(1 for mid in list(b.members) if b.status(mid) != 0)
+        for form in ("", "_persistent"):
+            b.set_persistent(form == "_persistent")
+            b.step(3, graph=True)
+            b.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(s_):
+                e0.record()
+            b.step(nb, graph=True)
+            with torch.cuda.stream(s_):
+                e1.record()
+            b.synchronize()
+            ms = e0.elapsed_time(e1)
+            bad = sum(1 for mid in list(b.members) if b.status(mid) != 0)
+            batched[key + form] = {"value": bcells * nb / (ms / 1e3), "ms_per_step": ms / nb,
+                                   "members_with_status": bad}
         b.close()
         del states
         torch.cuda.empty_cache()
-        batched[key] = {"value": bcells * nb / (ms / 1e3), "ms_per_step": ms / nb, "members_with_status": bad}
     # the plain FP64 path, one member at a time (graph replay of its own step)
     tot = 0.0
     acells = 0
@@ -899,6 +903,8 @@ def run_ensemble(args):
     b.synchronize()
     # the batch's autotuner picks the face kernels' register cap on these members
     tile, tune_ms = b.autotune()
+    if args.persistent:
+        b.set_persistent(True)
     b.step(1, graph=True)            # re-capture the step graph with the chosen shape (untimed)
     b.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -916,7 +922,8 @@ def run_ensemble(args):
                       "members": args.members, "cells_total": cells, "steps": args.steps, "ms_per_step": ms / args.steps,
                       "precision": args.precision, "members_with_status": bad,
                       "face_tile_regs": b.TILE_REGS[tile], "autotune_face_ms_per_stage": tune_ms,
-                      "launch": "23 batched kernels per step, one CUDA graph replay per step",
+                      "launch": ("one persistent launch per step (k_batch_persist), graph replay" if args.persistent
+                                 else "23 batched kernels per step, one CUDA graph replay per step"),
                       "equilibrium": eq}), flush=True)
 
 
@@ -974,6 +981,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the mixed / aux / batched / served objects of the step line")
+    ap.add_argument("--persistent", action="store_true",
+                    help="ensemble mode: one persistent launch per step instead of the per-kind launches")
     ap.add_argument("--bench-batch-steps", type=int, default=20)
     ap.add_argument("--bench-requests", type=int, default=50)
     ap.add_argument("--bench-serve-max-steps", type=int, default=600)

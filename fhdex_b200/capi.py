@@ -185,6 +185,8 @@ def _declare(lib):
         "fhd_batch_remove": (i, [vp, i]),
         "fhd_batch_step": (i, [vp, i, i]),
         "fhd_batch_size": (i, [vp]),
+        "fhd_batch_set_persistent": (i, [vp, i]),
+        "fhd_batch_set_wait_limit": (i, [vp, d, i]),
         "fhd_batch_member_status": (i, [vp, i]),
         "fhd_batch_synchronize": (i, [vp]),
         "fhd_batch_num_tiles": (i, []),

@@ -118,6 +118,7 @@ class Context:
 
     def set_bc(self, st: StagState, cu=None, mom=None):
         """setBCStag on (prim, cu, cumom, vel); nothing on a fully periodic box."""
+        self._stream()
         cu = cu or st.cu
         mom = mom or st.cumom
         mf = FabArr3(*[m.fab() for m in mom])

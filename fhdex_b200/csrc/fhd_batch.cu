@@ -67,7 +67,12 @@ struct Launch {
     size_t bpref_off;  // offset of the block-prefix array
     int nitems;        // members (or fabs)
     int nblocks;
+    size_t stride;     // bytes of one member's (fab's) argument block
+    std::vector<int64_t> items;  // work items per member (fab)
 };
+
+// items per chunk of the persistent step (k_batch_persist)
+const int kPersistChunk = 2048;
 
 const double kW[3] = {(2.0 * std::sqrt(2.0) + 1.0 * std::sqrt(3.0)) / 5.0,
                       (-4.0 * std::sqrt(2.0) + 3.0 * std::sqrt(3.0)) / 5.0,
@@ -90,6 +95,12 @@ struct fhd_batch {
     int* dstatus = nullptr;      // inside dbuf, one word per member
     std::vector<Launch> plan;
     int tile = -1;               // face-kernel register cap (batch_face_tiles(); -1 default)
+    // the persistent step: one launch per RK3 step over a work-unit table in dbuf
+    bool persistent = false;
+    PersistArgs pargs{};
+    size_t counters_bytes = 0;   // next, abort, done[] (zeroed before each launch)
+    double wait_limit_s = 1.0;
+    int hold_phase = -1;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
 };
@@ -223,6 +234,11 @@ int rebuild(fhd_batch* b) {
     add(sizeof(int) * (M + 1));
     add((size_t)ghost_sz * 5 * M);
     add(sizeof(int) * (5 * M + 1));
+    // persistent step: 24 phases; 11 units per member and stage, 7 for the end
+    const int kPhases = 24;
+    add(sizeof(PUnit) * (size_t)40 * M);
+    add(sizeof(unsigned int) * (size_t)kPhases * M);
+    add(sizeof(unsigned int) * ((size_t)kPhases * M + 2));
     need += 4096;
     if (!b->dbuf || b->dbuf_bytes < need) {
         if (b->dbuf) cudaFreeAsync(b->dbuf, b->stream);
@@ -254,10 +270,10 @@ int rebuild(fhd_batch* b) {
         }
         return off;
     };
-    auto push_ghosts = [&](int s, int& nfab, int& nblocks) {
+    auto push_ghosts = [&](int s, int& nfab, int& nblocks, std::vector<int64_t>& items) {
         const size_t off = align(256);
         host.resize(off + (size_t)ghost_sz * 5 * M);
-        std::vector<int64_t> items;
+        items.clear();
         int f = 0;
         for (int q = 0; q < M; ++q) {
             const Member& m = b->mem[q];
@@ -275,10 +291,10 @@ int rebuild(fhd_batch* b) {
         const size_t bpo = push_bpref(items, 256, nblocks);
         return std::make_pair(off, bpo);
     };
-    auto push_final_ghosts = [&](int& nfab, int& nblocks) {
+    auto push_final_ghosts = [&](int& nfab, int& nblocks, std::vector<int64_t>& items) {
         const size_t off = align(256);
         host.resize(off + (size_t)ghost_sz * 5 * M);
-        std::vector<int64_t> items;
+        items.clear();
         int f = 0;
         for (int q = 0; q < M; ++q) {
             const Member& m = b->mem[q];
@@ -300,11 +316,13 @@ int rebuild(fhd_batch* b) {
             for (const Member& m : b->mem) items.push_back(kind_items(kind, m.prm.n_cells));
             int nb = 0;
             const size_t bpo = push_bpref(items, 128, nb);
-            b->plan.push_back(Launch{kind, kind == 0 ? prep : stg, bpo, M, nb});
+            b->plan.push_back(Launch{kind, kind == 0 ? prep : stg, bpo, M, nb,
+                                     batch_args_size(b->ns, b->mixed, kind == 0 ? 0 : 1, b->mode), items});
         }
         int nfab = 0, nb = 0;
-        auto g = push_ghosts(s, nfab, nb);
-        b->plan.push_back(Launch{7, g.first, g.second, nfab, nb});
+        std::vector<int64_t> gitems;
+        auto g = push_ghosts(s, nfab, nb, gitems);
+        b->plan.push_back(Launch{7, g.first, g.second, nfab, nb, (size_t)ghost_sz, gitems});
     }
     {
         const size_t conv = push_args(6, false, 2);
@@ -312,11 +330,61 @@ int rebuild(fhd_batch* b) {
         for (const Member& m : b->mem) items.push_back(kind_items(6, m.prm.n_cells));
         int nb = 0;
         const size_t bpo = push_bpref(items, 128, nb);
-        b->plan.push_back(Launch{6, conv, bpo, M, nb});
+        b->plan.push_back(Launch{6, conv, bpo, M, nb, batch_args_size(b->ns, false, 6, b->mode), items});
         int nfab = 0;
-        auto g = push_final_ghosts(nfab, nb);
-        b->plan.push_back(Launch{7, g.first, g.second, nfab, nb});
-        b->plan.push_back(Launch{8, 0, 0, M, 0});
+        std::vector<int64_t> gitems;
+        auto g = push_final_ghosts(nfab, nb, gitems);
+        b->plan.push_back(Launch{7, g.first, g.second, nfab, nb, (size_t)ghost_sz, gitems});
+        b->plan.push_back(Launch{8, 0, 0, M, 0, 0, std::vector<int64_t>(M, 1)});
+    }
+    // the persistent step's work units, phase-major over members, with each
+    // member's chunk count per phase and the zeroed counters
+    {
+        const int nph = (int)b->plan.size();
+        std::vector<PUnit> units;
+        std::vector<unsigned int> needv((size_t)nph * M, 0);
+        int64_t first = 0;
+        for (int ph = 0; ph < nph; ++ph) {
+            const Launch& L = b->plan[ph];
+            const int per = L.kind == 7 ? 5 : 1;  // ghost fabs per member
+            for (size_t u = 0; u < L.items.size(); ++u) {
+                PUnit pu;
+                pu.args = L.kind == 8 ? nullptr : dbase + L.args_off + L.stride * u;
+                pu.first = first;
+                pu.items = L.items[u];
+                pu.member = (int)(u / per);
+                pu.phase = ph;
+                pu.kind = L.kind;
+                pu.pad = 0;
+                const int64_t nch = (pu.items + kPersistChunk - 1) / kPersistChunk;
+                first += nch;
+                needv[(size_t)pu.member * nph + ph] += (unsigned int)nch;
+                units.push_back(pu);
+            }
+        }
+        const size_t uoff = align(256);
+        host.resize(uoff + sizeof(PUnit) * units.size());
+        memcpy(host.data() + uoff, units.data(), sizeof(PUnit) * units.size());
+        const size_t noff = align(256);
+        host.resize(noff + sizeof(unsigned int) * needv.size());
+        memcpy(host.data() + noff, needv.data(), sizeof(unsigned int) * needv.size());
+        const size_t coff = align(256);
+        b->counters_bytes = sizeof(unsigned int) * (needv.size() + 2);
+        host.resize(coff + b->counters_bytes, 0);
+        PersistArgs& a = b->pargs;
+        a.units = reinterpret_cast<const PUnit*>(dbase + uoff);
+        a.nunits = (int)units.size();
+        a.nphase = nph;
+        a.total = first;
+        a.chunk = kPersistChunk;
+        a.next = reinterpret_cast<unsigned int*>(dbase + coff);
+        a.abort = reinterpret_cast<int*>(dbase + coff + sizeof(unsigned int));
+        a.done = reinterpret_cast<unsigned int*>(dbase + coff + 2 * sizeof(unsigned int));
+        a.need = reinterpret_cast<const unsigned int*>(dbase + noff);
+        a.status = b->dstatus;
+        a.steps = b->dsteps;
+        a.limit_ns = (unsigned long long)(b->wait_limit_s * 1e9);
+        a.hold_phase = b->hold_phase;
     }
     if (host.size() > b->dbuf_bytes) return FHD_ERR_OOM;
     if (cudaMemcpyAsync(b->dbuf, host.data(), host.size(), cudaMemcpyHostToDevice, b->stream) != cudaSuccess)
@@ -328,6 +396,12 @@ int rebuild(fhd_batch* b) {
 }
 
 int run_plan(fhd_batch* b) {
+    if (b->persistent) {
+        // zero the dispenser, the abort flag and the per-phase counters, then one launch
+        if (cudaMemsetAsync(b->pargs.next, 0, b->counters_bytes, b->stream) != cudaSuccess)
+            return cuda_ok(cudaGetLastError());
+        return batch_persist(b->ns, b->mixed, b->mode, b->pargs, b->stream);
+    }
     char* d = static_cast<char*>(b->dbuf);
     for (const Launch& L : b->plan) {
         int rc = FHD_OK;
@@ -528,6 +602,25 @@ int fhd_batch_step(fhd_batch* b, int nsteps, int use_graph) {
 }
 
 int fhd_batch_size(const fhd_batch* b) { return b ? (int)b->mem.size() : -1; }
+
+int fhd_batch_set_persistent(fhd_batch* b, int enable) {
+    if (!b) return FHD_ERR_BAD_ARG;
+    if ((enable != 0) != b->persistent) {
+        b->persistent = enable != 0;
+        drop_graph(b);
+    }
+    return FHD_OK;
+}
+
+int fhd_batch_set_wait_limit(fhd_batch* b, double seconds, int hold_phase) {
+    if (!b || !(seconds > 0) || seconds > 60 || hold_phase < -1 || hold_phase >= 24) return FHD_ERR_BAD_ARG;
+    b->wait_limit_s = seconds;
+    b->hold_phase = hold_phase;
+    b->pargs.limit_ns = (unsigned long long)(seconds * 1e9);
+    b->pargs.hold_phase = hold_phase;
+    drop_graph(b);
+    return FHD_OK;
+}
 
 int fhd_batch_num_tiles(void) { return batch_face_tiles(); }
 

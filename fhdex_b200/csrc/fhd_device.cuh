@@ -112,6 +112,32 @@ FHD_D float divz(float a, float b) { return rdiv(a, b); }
 
 FHD_D uint64_t noise_step(const DevParams& P) { return P.step_ptr ? *P.step_ptr : P.step; }
 
+// ---- persistent batched step: work units and run descriptor (k_batch_persist) -----------
+enum { PK_PREP = 0, PK_TAUS = 1, PK_FACEX = 2, PK_FACEY = 3, PK_FACEZ = 4, PK_UPDATE = 5, PK_CONVERT = 6,
+       PK_GHOST = 7, PK_STEP = 8 };
+
+struct PUnit {
+    const void* args;   // the unit's argument block (PrepArgs, StageArgs, ConvArgs or GhostFab)
+    int64_t first;      // global index of the unit's first chunk
+    int64_t items;      // work items (points; points x components for a ghost fab)
+    int member, phase, kind, pad;
+};
+
+struct PersistArgs {
+    const PUnit* units;
+    int nunits, nphase;
+    int64_t total;              // chunks of the step
+    int chunk;                  // items per chunk
+    unsigned int* next;         // chunk dispenser
+    unsigned int* done;         // [member][phase] finished chunks
+    const unsigned int* need;   // [member][phase] chunks
+    int* status;                // per member
+    int* abort;
+    uint64_t* steps;            // per-member step counters
+    unsigned long long limit_ns;
+    int hold_phase;             // failure-injection hook: this phase's completions are never published (-1: none)
+};
+
 // ---- physical boundaries ---------------------------------------------------------------
 // wall values per side s = 2 d + (0 lo, 1 hi) (after SetupCWallStag)
 struct WallParams {
@@ -141,6 +167,14 @@ FHD_HD double stoch_factor(const DevParams& P, int type) {
 }
 
 // ---- EOS helpers (compressible_functions.H:138-219, 1497-1520) ----------------------
+// Products summed in double go through mul_rn / add_rn, which are never fused into
+// an FMA: the conversion then gives the same bits in the FP64 units (built without
+// contraction) and in the mixed units (built with it), where the persistent batched
+// step converts the state.  FP32 code keeps the compiler's contraction.
+FHD_D double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+FHD_D double add_rn(double a, double b) { return __dadd_rn(a, b); }
+FHD_D float mul_rn(float a, float b) { return a * b; }
+FHD_D float add_rn(float a, float b) { return a + b; }
 
 template <int NS, class R>
 FHD_D void GetMolfrac(const DevParams& P, const R (&Y)[NS], R (&X)[NS]) {
@@ -157,8 +191,8 @@ FHD_D R GetTemperature(const DevParams& P, R energy, const R (&Y)[NS]) {
     R cvmix = R(0.), e0mix = R(0.);
 #pragma unroll
     for (int n = 0; n < NS; ++n) {
-        cvmix += Y[n] * R(P.hcv[n]);
-        e0mix += Y[n] * R(P.e0[n]);
+        cvmix = add_rn(cvmix, mul_rn(Y[n], R(P.hcv[n])));
+        e0mix = add_rn(e0mix, mul_rn(Y[n], R(P.e0[n])));
     }
     return rdiv(energy - e0mix, cvmix);
 }
@@ -503,9 +537,9 @@ template <int NS>
 FHD_D bool cons_to_prim(const DevParams& P, double rho, double rhoE, const double (&rhoY)[NS], double mxl,
                         double mxh, double myl, double myh, double mzl, double mzh, Prim<NS>& q) {
     double kin = 0.;
-    kin += (mxh + mxl) * (mxh + mxl);
-    kin += (myh + myl) * (myh + myl);
-    kin += (mzh + mzl) * (mzh + mzl);
+    kin = add_rn(kin, mul_rn(mxh + mxl, mxh + mxl));
+    kin = add_rn(kin, mul_rn(myh + myl, myh + myl));
+    kin = add_rn(kin, mul_rn(mzh + mzl, mzh + mzl));
     kin *= (0.125 / rho);
     const double intenergy = (rhoE - kin) / rho;
     double Yf[NS];

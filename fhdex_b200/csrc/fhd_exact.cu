@@ -48,24 +48,32 @@ int exact_batch_launch_ns1(int, int, int, const void*, const int*, int, int, cud
 size_t mixed_batch_args_size_ns1(int, int);
 void mixed_batch_pack_ns1(int, int, const StageCall&, void*);
 int mixed_batch_launch_ns1(int, int, int, const void*, const int*, int, int, cudaStream_t);
+int exact_batch_persist_ns1(int, const PersistArgs&, cudaStream_t);
+int mixed_batch_persist_ns1(int, const PersistArgs&, cudaStream_t);
 size_t exact_batch_args_size_ns2(int, int);
 void exact_batch_pack_ns2(int, int, const StageCall&, void*);
 int exact_batch_launch_ns2(int, int, int, const void*, const int*, int, int, cudaStream_t);
 size_t mixed_batch_args_size_ns2(int, int);
 void mixed_batch_pack_ns2(int, int, const StageCall&, void*);
 int mixed_batch_launch_ns2(int, int, int, const void*, const int*, int, int, cudaStream_t);
+int exact_batch_persist_ns2(int, const PersistArgs&, cudaStream_t);
+int mixed_batch_persist_ns2(int, const PersistArgs&, cudaStream_t);
 size_t exact_batch_args_size_ns3(int, int);
 void exact_batch_pack_ns3(int, int, const StageCall&, void*);
 int exact_batch_launch_ns3(int, int, int, const void*, const int*, int, int, cudaStream_t);
 size_t mixed_batch_args_size_ns3(int, int);
 void mixed_batch_pack_ns3(int, int, const StageCall&, void*);
 int mixed_batch_launch_ns3(int, int, int, const void*, const int*, int, int, cudaStream_t);
+int exact_batch_persist_ns3(int, const PersistArgs&, cudaStream_t);
+int mixed_batch_persist_ns3(int, const PersistArgs&, cudaStream_t);
 size_t exact_batch_args_size_ns4(int, int);
 void exact_batch_pack_ns4(int, int, const StageCall&, void*);
 int exact_batch_launch_ns4(int, int, int, const void*, const int*, int, int, cudaStream_t);
 size_t mixed_batch_args_size_ns4(int, int);
 void mixed_batch_pack_ns4(int, int, const StageCall&, void*);
 int mixed_batch_launch_ns4(int, int, int, const void*, const int*, int, int, cudaStream_t);
+int exact_batch_persist_ns4(int, const PersistArgs&, cudaStream_t);
+int mixed_batch_persist_ns4(int, const PersistArgs&, cudaStream_t);
 
 #define FHD_DISPATCH(ns, fn, ...)            \
     switch (ns) {                             \
@@ -145,6 +153,11 @@ int batch_launch(int ns, bool mixed, int kind, int mode, int tile, const void* d
                  int nblocks, cudaStream_t s) {
     if (mixed) { FHD_DISPATCH(ns, mixed_batch_launch_ns, kind, mode, tile, dargs, dbpref, nmem, nblocks, s) }
     FHD_DISPATCH(ns, exact_batch_launch_ns, kind, mode, tile, dargs, dbpref, nmem, nblocks, s)
+}
+
+int batch_persist(int ns, bool mixed, int mode, const PersistArgs& a, cudaStream_t s) {
+    if (mixed) { FHD_DISPATCH(ns, mixed_batch_persist_ns, mode, a, s) }
+    FHD_DISPATCH(ns, exact_batch_persist_ns, mode, a, s)
 }
 
 int batch_face_tiles() { return kNumBatchFaceTiles; }

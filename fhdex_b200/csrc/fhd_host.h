@@ -195,6 +195,8 @@ void batch_pack(int ns, bool mixed, int kind, int mode, const StageCall& c, void
 int batch_launch(int ns, bool mixed, int kind, int mode, int tile, const void* dargs, const int* dbpref, int nmem,
                  int nblocks, cudaStream_t s);
 int batch_face_tiles();
+// the persistent batched step (k_batch_persist): one launch per RK3 step
+int batch_persist(int ns, bool mixed, int mode, const PersistArgs& a, cudaStream_t s);
 int batch_face_min_blocks(int tile);
 struct GhostFabDesc;  // opaque to the host code
 int ghost_desc_size();

@@ -36,6 +36,10 @@ int FHD_CAT(FHD_CAT(FHD_PFX, _batch_launch_ns), FHD_NS)(int kind, int mode, int 
                           : batch_launch_t<FHD_NS, FHD_R, NZ_PHILOX>(kind, tile, dargs, dbpref, nmem, nblocks, s);
 }
 
+int FHD_CAT(FHD_CAT(FHD_PFX, _batch_persist_ns), FHD_NS)(int mode, const PersistArgs& a, cudaStream_t s) {
+    return mode == NM_OFF ? batch_persist_t<FHD_NS, FHD_R, NZ_OFF>(a, s) : batch_persist_t<FHD_NS, FHD_R, NZ_PHILOX>(a, s);
+}
+
 #if defined(FHD_MIXED) && FHD_MIXED
 int FHD_CAT(mixed_cellprep_ns, FHD_NS)(const StageCall& c) { return launch_cellprep<FHD_NS, float>(c); }
 int FHD_CAT(mixed_stage_ns, FHD_NS)(const StageCall& c, int part) { return launch_stage_part<FHD_NS, float>(c, part); }

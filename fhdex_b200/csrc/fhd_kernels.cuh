@@ -22,7 +22,7 @@ namespace fhd {
 // With external linkage a launch could reach the other unit's device code, and
 // which one depends on the order the modules are loaded in.
 
-enum { ST_OK = 0, ST_MASSFRAC = 2, ST_NONFINITE = 3 };
+enum { ST_OK = 0, ST_MASSFRAC = 2, ST_NONFINITE = 3, ST_TIMEOUT = 5 };
 
 FHD_D void flag(int* status, int code) {
     if (status) atomicCAS(status, 0, code);
@@ -766,6 +766,143 @@ static __global__ void __launch_bounds__(256) k_ghosts_b(const GhostFab* __restr
     const GhostFab& f = fabs[m];
     const int64_t q = (int64_t)(blockIdx.x - bpref[m]) * blockDim.x + threadIdx.x;
     if (q < f.npts * f.nc) ghost_point(f, q);
+}
+
+// ===================================================================================
+// persistent batched step: one launch runs every phase of one RK3 step for every
+// member.  Phases per member: for each stage cellprep, stresses, faces x / y / z,
+// update, ghost fill; then the conversion, its ghost fill and the step counter.
+// Work is cut into chunks of `chunk` items; a unit is one member's (or one ghost
+// fab's) part of a phase.  Blocks take chunks in order from one counter (phase-
+// major over members) and, before working on a chunk of phase p > 0, wait until
+// every chunk of the member's phase p - 1 is done.  A block only ever waits on
+// chunks taken before its own, by blocks that are running, so the order cannot
+// deadlock; every wait is still bounded in time (limit_ns): on expiry the block
+// marks the member FHD_ERR_TIMEOUT, raises the abort flag and all blocks stop
+// taking work.
+// ===================================================================================
+FHD_D unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// bounded wait for every chunk of member m's phase p; 1 when done, 0 on abort or expiry
+FHD_D int wait_phase(const PersistArgs& a, int m, int p) {
+    volatile const unsigned int* d = a.done + (size_t)m * a.nphase + p;
+    const unsigned int target = a.need[(size_t)m * a.nphase + p];
+    const unsigned long long t0 = global_ns();
+    for (;;) {
+        if (*d >= target) {
+            __threadfence();
+            return 1;
+        }
+        if (*reinterpret_cast<volatile int*>(a.abort)) return 0;
+        if (global_ns() - t0 > a.limit_ns) {
+            atomicCAS(a.status + m, 0, ST_TIMEOUT);
+            atomicExch(a.abort, 1);
+            return 0;
+        }
+        __nanosleep(256);
+    }
+}
+
+template <int NS, class R, int NZ>
+struct PersistBytes {
+    static constexpr size_t a = sizeof(PrepArgs<NS, R>), b = sizeof(StageArgs<NS, R, NZ>), c = sizeof(ConvArgs<NS>),
+                            d = sizeof(GhostFab);
+    static constexpr size_t m1 = a > b ? a : b, m2 = c > d ? c : d;
+    static constexpr size_t value = ((m1 > m2 ? m1 : m2) + 7) / 8 * 8;
+};
+
+template <int NS, class R, int NZ, int MINB>
+static __global__ void __launch_bounds__(128, MINB) k_batch_persist(PersistArgs a) {
+    __shared__ unsigned long long sbuf[PersistBytes<NS, R, NZ>::value / 8];
+    __shared__ int s_unit, s_go, s_end;
+    __shared__ long long s_chunk;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            long long I = -1;
+            if (!*reinterpret_cast<volatile int*>(a.abort)) I = (long long)atomicAdd(a.next, 1u);
+            const int end = I < 0 || I >= a.total;
+            int u = 0, go = 0;
+            if (!end) {
+                int lo = 0, hi = a.nunits;
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (a.units[mid].first <= I) lo = mid;
+                    else hi = mid;
+                }
+                u = lo;
+                const PUnit& pu = a.units[u];
+                go = pu.phase == 0 ? 1 : wait_phase(a, pu.member, pu.phase - 1);
+                s_chunk = I - pu.first;
+            }
+            s_unit = u;
+            s_go = go;
+            s_end = end;
+        }
+        __syncthreads();
+        if (s_end) break;
+        const PUnit& pu = a.units[s_unit];
+        const int kind = pu.kind;
+        if (s_go) {
+            if (kind != PK_STEP) {
+                const size_t bytes = kind == PK_PREP ? sizeof(PrepArgs<NS, R>)
+                                     : kind == PK_CONVERT ? sizeof(ConvArgs<NS>)
+                                     : kind == PK_GHOST ? sizeof(GhostFab) : sizeof(StageArgs<NS, R, NZ>);
+                const unsigned long long* src = static_cast<const unsigned long long*>(pu.args);
+                for (int w = threadIdx.x; w < (int)((bytes + 7) / 8); w += blockDim.x) sbuf[w] = src[w];
+            }
+            __syncthreads();
+            const int64_t q0 = s_chunk * a.chunk;
+            const int64_t q1 = q0 + a.chunk < pu.items ? q0 + a.chunk : pu.items;
+            const int64_t q = q0 + threadIdx.x;
+            const int st = blockDim.x;
+            switch (kind) {
+                case PK_PREP: {
+                    const auto& A = *reinterpret_cast<const PrepArgs<NS, R>*>(sbuf);
+                    for (int64_t x = q; x < q1; x += st) cellprep_point(A, (int)x);
+                } break;
+                case PK_TAUS: {
+                    const auto& A = *reinterpret_cast<const StageArgs<NS, R, NZ>*>(sbuf);
+                    for (int64_t x = q; x < q1; x += st) taus_point(A, (int)x);
+                } break;
+                case PK_FACEX: {
+                    const auto& A = *reinterpret_cast<const StageArgs<NS, R, NZ>*>(sbuf);
+                    for (int64_t x = q; x < q1; x += st) faces_point<NS, R, NZ, 0>(A, (int)x);
+                } break;
+                case PK_FACEY: {
+                    const auto& A = *reinterpret_cast<const StageArgs<NS, R, NZ>*>(sbuf);
+                    for (int64_t x = q; x < q1; x += st) faces_point<NS, R, NZ, 1>(A, (int)x);
+                } break;
+                case PK_FACEZ: {
+                    const auto& A = *reinterpret_cast<const StageArgs<NS, R, NZ>*>(sbuf);
+                    for (int64_t x = q; x < q1; x += st) faces_point<NS, R, NZ, 2>(A, (int)x);
+                } break;
+                case PK_UPDATE: {
+                    const auto& A = *reinterpret_cast<const StageArgs<NS, R, NZ>*>(sbuf);
+                    for (int64_t x = q; x < q1; x += st) update_point(A, (int)x);
+                } break;
+                case PK_CONVERT: {
+                    const auto& A = *reinterpret_cast<const ConvArgs<NS>*>(sbuf);
+                    for (int64_t x = q; x < q1; x += st) convert_point(A, (int)x);
+                } break;
+                case PK_GHOST: {
+                    const auto& G = *reinterpret_cast<const GhostFab*>(sbuf);
+                    for (int64_t x = q; x < q1; x += st) ghost_point(G, x);
+                } break;
+                default:
+                    if (threadIdx.x == 0) a.steps[pu.member] += 1;
+                    break;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && s_go && pu.phase != a.hold_phase) {
+            __threadfence();
+            atomicAdd(a.done + (size_t)pu.member * a.nphase + pu.phase, 1u);
+        }
+    }
 }
 
 static __global__ void k_steps_set(uint64_t* step, uint64_t v) { *step = v; }

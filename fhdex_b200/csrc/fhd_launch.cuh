@@ -413,6 +413,15 @@ int batch_launch_t(int kind, int tile, const void* dargs, const int* dbpref, int
     return cuda_rc(cudaGetLastError());
 }
 
+// the persistent batched step: grid = the blocks that fit on the GPU at once
+template <int NS, class R, int NZ>
+int batch_persist_t(const PersistArgs& a, cudaStream_t s) {
+    constexpr int MINB = sizeof(R) == 8 ? 4 : 6;
+    const int grid = resident_blocks<k_batch_persist<NS, R, NZ, MINB>>(128);
+    k_batch_persist<NS, R, NZ, MINB><<<grid, 128, 0, s>>>(a);
+    return cuda_rc(cudaGetLastError());
+}
+
 #define FHD_NS_SWITCH(ns, CALL) \
     switch (ns) {                \
         case 1: return CALL(1);  \

@@ -338,6 +338,19 @@ int fhd_batch_remove(fhd_batch* batch, int member);
 /* Advances every member by nsteps RK3 steps (use_graph: replay a captured graph). */
 int fhd_batch_step(fhd_batch* batch, int nsteps, int use_graph);
 int fhd_batch_size(const fhd_batch* batch);
+/* Run each step of the batch as ONE persistent launch (k_batch_persist) instead of
+ * the 23 per-kind launches: blocks take chunks of every member's phases (per stage:
+ * cellprep, stresses, faces x/y/z, update, ghost fill; then the conversion, its
+ * ghost fill and the step counter) from one device counter in phase-major order
+ * and wait, bounded in time, for the member's previous phase.  Results are bitwise
+ * those of the per-kind launches.  Replayed from a graph like them. */
+int fhd_batch_set_persistent(fhd_batch* batch, int enable);
+/* Time limit of each wait of the persistent step (default 1 s; at most 60 s).  On
+ * expiry the member's status becomes FHD_ERR_TIMEOUT and every block stops taking
+ * work for that step.  hold_phase >= 0 (0 .. 23) is a failure-injection hook for
+ * tests: that phase's completions are never published, so the next phase's wait
+ * runs out; -1 turns it off. */
+int fhd_batch_set_wait_limit(fhd_batch* batch, double seconds, int hold_phase);
 /* Latched device status of one member (waits for the stream). */
 int fhd_batch_member_status(fhd_batch* batch, int member);
 int fhd_batch_synchronize(fhd_batch* batch);

@@ -167,3 +167,63 @@ def test_server_results_match_runs_alone():
         tol = 0.0 if p.precision == 0 else MIXED_TOL
         assert not same(finals[r.rid], ref, tol), (r, same(finals[r.rid], ref, tol))
     srv.close()
+
+
+@pytest.mark.parametrize("precision,ns", [(0, 2), (1, 2), (0, 4)])
+def test_persistent_step_equals_the_per_kind_launches(precision, ns):
+    """One persistent launch per step (k_batch_persist: chunks of every member's
+    phases from one device counter, bounded waits on the member's previous phase)
+    gives the per-kind launches' results bit for bit, with and without graph
+    replay, on members of different sizes."""
+    mk = argon if ns == 2 else mixture4
+    ps = [mk(16, dx=8e-6, T_init=260.0, rho0=1.2e-3, seed=21, precision=precision),
+          mk((20, 12, 8), dx=8e-6, T_init=330.0, rho0=2.5e-3, seed=22, precision=precision),
+          mk((9, 7, 13), dx=8e-6, seed=23, precision=precision)]
+    dts = [stable_dt(p) for p in ps]
+    out = []
+    for persistent in (False, True):
+        b = Batch(ns, precision)
+        b.set_persistent(persistent)
+        sts = [StagState(p, "cuda", aux=False) for p in ps]
+        ids = [b.add(p, st, dt) for p, st, dt in zip(ps, sts, dts)]
+        b.step(2, graph=False)
+        b.step(2, graph=True)
+        b.synchronize()
+        assert all(b.status(i) == 0 for i in ids)
+        out.append(sts)
+        b.close()
+    for a, r in zip(out[1], out[0]):
+        assert not same(a, r), same(a, r)
+
+
+def test_persistent_wait_runs_out_and_the_batch_stays_usable():
+    """The failure path of the persistent step's waits: with the completions of
+    phase 3 (the x face fluxes of stage 1) never published, the wait of phase 4
+    runs out after the 50 ms limit, the member's status reads FHD_ERR_TIMEOUT and
+    the launch ends; afterwards the batch steps normally again."""
+    from fhdex_b200 import capi
+    ps = [argon(12, dx=8e-6, seed=31), argon(10, dx=8e-6, seed=32)]
+    b = Batch(2, 0)
+    b.set_persistent(True)
+    sts = [StagState(p, "cuda", aux=False) for p in ps]
+    ids = [b.add(p, st, stable_dt(p)) for p, st in zip(ps, sts)]
+    b.set_wait_limit(0.05, hold_phase=3)
+    b.step(1, graph=False)
+    b.synchronize()
+    codes = [b.status(i) for i in ids]
+    assert capi.FHD_ERR_TIMEOUT in codes and all(c in (0, capi.FHD_ERR_TIMEOUT) for c in codes)
+    b.set_wait_limit(1.0, hold_phase=-1)
+    # a fresh batch of the same members' sizes steps cleanly after the timeout
+    b2 = Batch(2, 0)
+    b2.set_persistent(True)
+    st2 = StagState(ps[0], "cuda", aux=False)
+    i2 = b2.add(ps[0], st2, stable_dt(ps[0]))
+    b2.step(2, graph=True)
+    b2.synchronize()
+    assert b2.status(i2) == 0
+    ref = alone(ps[0], stable_dt(ps[0]), 2)
+    assert not same(st2, ref)
+    b.step(1, graph=False)
+    b.synchronize()
+    b.close()
+    b2.close()
