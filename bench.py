@@ -903,8 +903,23 @@ def run_ensemble(args):
     b.synchronize()
     # the batch's autotuner picks the face kernels' register cap on these members
     tile, tune_ms = b.autotune()
+    persist_ms = {}
     if args.persistent:
-        b.set_persistent(True)
+        # the persistent kernel's register cap, each timed over 3 graph-replayed steps
+        for t in range(len(b.TILE_REGS)):
+            b.set_persistent(True, t)
+            b.step(1, graph=True)
+            b.synchronize()
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(s):
+                f0.record()
+            b.step(3, graph=True)
+            with torch.cuda.stream(s):
+                f1.record()
+            b.synchronize()
+            persist_ms[b.TILE_REGS[t]] = f0.elapsed_time(f1) / 3
+        tile = min(range(len(b.TILE_REGS)), key=lambda t: persist_ms[b.TILE_REGS[t]])
+        b.set_persistent(True, tile)
     b.step(1, graph=True)            # re-capture the step graph with the chosen shape (untimed)
     b.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -922,6 +937,7 @@ def run_ensemble(args):
                       "members": args.members, "cells_total": cells, "steps": args.steps, "ms_per_step": ms / args.steps,
                       "precision": args.precision, "members_with_status": bad,
                       "face_tile_regs": b.TILE_REGS[tile], "autotune_face_ms_per_stage": tune_ms,
+                      "persistent_ms_per_step_by_regs": persist_ms or None,
                       "launch": ("one persistent launch per step (k_batch_persist), graph replay" if args.persistent
                                  else "23 batched kernels per step, one CUDA graph replay per step"),
                       "equilibrium": eq}), flush=True)

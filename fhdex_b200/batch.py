@@ -64,10 +64,11 @@ class Batch:
         self._stream = stream
         check(self.lib.fhd_batch_set_stream(self._h, C.c_void_p(stream.cuda_stream)), "fhd_batch_set_stream")
 
-    def set_persistent(self, enable: bool = True):
+    def set_persistent(self, enable: bool = True, tile: int = -1):
         """One persistent launch per step (k_batch_persist) instead of the per-kind
-        launches; bitwise the same results."""
-        check(self.lib.fhd_batch_set_persistent(self._h, int(enable)), "fhd_batch_set_persistent")
+        launches; bitwise the same results.  tile: the kernel's register cap
+        (TILE_REGS; -1 the default)."""
+        check(self.lib.fhd_batch_set_persistent(self._h, int(enable), tile), "fhd_batch_set_persistent")
 
     def set_wait_limit(self, seconds: float, hold_phase: int = -1):
         """Time limit of the persistent step's waits; hold_phase >= 0 never publishes

@@ -87,6 +87,13 @@ class FhdParams(C.Structure):
         ("bc_Yk_hi", (C.c_double * MAX_SPECIES) * 3),
         ("bc_Xk_lo", (C.c_double * MAX_SPECIES) * 3),
         ("bc_Xk_hi", (C.c_double * MAX_SPECIES) * 3),
+        ("p_lo", C.c_double * 3),
+        ("p_hi", C.c_double * 3),
+        ("rho_lo", C.c_double * 3),
+        ("rho_hi", C.c_double * 3),
+        ("rho0", C.c_double),
+        ("T_init", C.c_double),
+        ("rhobar", C.c_double * MAX_SPECIES),
     ]
 
 
@@ -185,7 +192,7 @@ def _declare(lib):
         "fhd_batch_remove": (i, [vp, i]),
         "fhd_batch_step": (i, [vp, i, i]),
         "fhd_batch_size": (i, [vp]),
-        "fhd_batch_set_persistent": (i, [vp, i]),
+        "fhd_batch_set_persistent": (i, [vp, i, i]),
         "fhd_batch_set_wait_limit": (i, [vp, d, i]),
         "fhd_batch_member_status": (i, [vp, i]),
         "fhd_batch_synchronize": (i, [vp]),

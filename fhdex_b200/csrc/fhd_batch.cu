@@ -101,6 +101,7 @@ struct fhd_batch {
     size_t counters_bytes = 0;   // next, abort, done[] (zeroed before each launch)
     double wait_limit_s = 1.0;
     int hold_phase = -1;
+    int persist_tile = -1;       // register cap of the persistent kernel (batch face tiles; -1 default)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
 };
@@ -400,7 +401,7 @@ int run_plan(fhd_batch* b) {
         // zero the dispenser, the abort flag and the per-phase counters, then one launch
         if (cudaMemsetAsync(b->pargs.next, 0, b->counters_bytes, b->stream) != cudaSuccess)
             return cuda_ok(cudaGetLastError());
-        return batch_persist(b->ns, b->mixed, b->mode, b->pargs, b->stream);
+        return batch_persist(b->ns, b->mixed, b->mode, b->persist_tile, b->pargs, b->stream);
     }
     char* d = static_cast<char*>(b->dbuf);
     for (const Launch& L : b->plan) {
@@ -603,10 +604,11 @@ int fhd_batch_step(fhd_batch* b, int nsteps, int use_graph) {
 
 int fhd_batch_size(const fhd_batch* b) { return b ? (int)b->mem.size() : -1; }
 
-int fhd_batch_set_persistent(fhd_batch* b, int enable) {
-    if (!b) return FHD_ERR_BAD_ARG;
-    if ((enable != 0) != b->persistent) {
+int fhd_batch_set_persistent(fhd_batch* b, int enable, int tile) {
+    if (!b || tile < -1 || tile >= batch_face_tiles()) return FHD_ERR_BAD_ARG;
+    if ((enable != 0) != b->persistent || tile != b->persist_tile) {
         b->persistent = enable != 0;
+        b->persist_tile = tile;
         drop_graph(b);
     }
     return FHD_OK;

@@ -36,6 +36,7 @@ struct fhd_ctx {
     // physical boundaries: the periodic directions and the walls' values
     int per[3] = {1, 1, 1};
     bool walls = false;
+    bool reservoir = false;      // a side with bc_mass 3: the boundary passes run one by one
     WallParams wall{};
     // device mirrors for the host-buffer step
     double* hbuf = nullptr;
@@ -271,17 +272,19 @@ int setup_walls(const fhd_params& p, int per[3], WallParams& W) {
             const int v = h ? p.bc_vel_hi[d] : p.bc_vel_lo[d];
             const int m = h ? p.bc_mass_hi[d] : p.bc_mass_lo[d];
             const int t = h ? p.bc_therm_hi[d] : p.bc_therm_lo[d];
-            if (m >= 3) return FHD_ERR_UNSUPPORTED;
-            if ((v != 1 && v != 2) || (m != 1 && m != 2) || (t != 1 && t != 2)) return FHD_ERR_BAD_ARG;
+            if (m >= 4) return FHD_ERR_UNSUPPORTED;
+            if ((v != 1 && v != 2) || (m != 1 && m != 2 && m != 3) || (t != 1 && t != 2)) return FHD_ERR_BAD_ARG;
             W.t[s] = h ? p.t_hi[d] : p.t_lo[d];
-            if (t == 2 && !(W.t[s] > 0)) return FHD_ERR_BAD_ARG;
+            W.p[s] = h ? p.p_hi[d] : p.p_lo[d];
+            W.rho[s] = h ? p.rho_hi[d] : p.rho_lo[d];
+            if (t == 2 && m != 3 && !(W.t[s] > 0)) return FHD_ERR_BAD_ARG;
             const double* Yk = h ? p.bc_Yk_hi[d] : p.bc_Yk_lo[d];
             const double* Xk = h ? p.bc_Xk_hi[d] : p.bc_Xk_lo[d];
             for (int n = 0; n < ns; ++n) {
                 W.Yk[s][n] = Yk[n];
                 W.Xk[s][n] = Xk[n];
             }
-            if (m != 2) continue;
+            if (m == 1) continue;
             double sumx = 0., sumy = 0.;
             for (int n = 0; n < ns; ++n) {
                 sumx = sumx + Xk[n];
@@ -299,6 +302,30 @@ int setup_walls(const fhd_params& p, int per[3], WallParams& W) {
             } else {
                 return FHD_ERR_BAD_ARG;
             }
+            if (m != 3) continue;
+            // reservoir state (boundaryStag.cpp:39-60): the pressure defaults to the
+            // initial state's (GetPressureGas of rhobar, rho0, T_init); then the
+            // density from p, t and Y (GetDensity), or, when a density is given and
+            // no temperature, the temperature from p and rho
+            if (W.p[s] <= 0.0) {
+                double molmix = 0.;
+                for (int n = 0; n < ns; ++n) molmix += p.rhobar[n] / p.molmass[n];
+                molmix = 1. / molmix;
+                W.p[s] = p.rho0 * (p.Runiv / molmix) * p.T_init;
+            }
+            if (W.rho[s] <= 0.0) {
+                if (!(W.t[s] > 0)) return FHD_ERR_BAD_ARG;
+                double molmix = 0.;
+                for (int n = 0; n < ns; ++n) molmix += W.Yk[s][n] / p.molmass[n];
+                molmix = 1. / molmix;
+                W.rho[s] = W.p[s] / (p.Runiv / molmix) / W.t[s];
+            } else if (W.t[s] <= 0.0) {
+                double molmix = 0.;
+                for (int n = 0; n < ns; ++n) molmix += W.Yk[s][n] / p.molmass[n];
+                molmix = 1. / molmix;
+                W.t[s] = W.p[s] * (molmix / p.Runiv) / W.rho[s];
+            }
+            if (!(W.p[s] > 0) || !(W.rho[s] > 0) || !(W.t[s] > 0)) return FHD_ERR_BAD_ARG;
         }
     }
     return FHD_OK;
@@ -336,9 +363,18 @@ int fhd_create(fhd_ctx** out, const fhd_params* params, int device) {
     if (!c) return FHD_ERR_OOM;
     c->prm = p;
     c->prm.walls = walls ? 1 : 0;
-    // the effective wall compositions (after SetupCWallStag)
+    // the effective wall compositions and reservoir states (after SetupCWallStag)
+    for (int d = 0; d < 3 && walls; ++d) {
+        if (per[d]) continue;
+        c->prm.t_lo[d] = wall.t[2 * d];
+        c->prm.t_hi[d] = wall.t[2 * d + 1];
+        c->prm.p_lo[d] = wall.p[2 * d];
+        c->prm.p_hi[d] = wall.p[2 * d + 1];
+        c->prm.rho_lo[d] = wall.rho[2 * d];
+        c->prm.rho_hi[d] = wall.rho[2 * d + 1];
+    }
     for (int d = 0; d < 3 && walls; ++d)
-        for (int n = 0; n < p.nspecies; ++n) {
+        for (int n = 0; n < p.nspecies && !per[d]; ++n) {
             c->prm.bc_Yk_lo[d][n] = wall.Yk[2 * d][n];
             c->prm.bc_Xk_lo[d][n] = wall.Xk[2 * d][n];
             c->prm.bc_Yk_hi[d][n] = wall.Yk[2 * d + 1][n];
@@ -347,6 +383,8 @@ int fhd_create(fhd_ctx** out, const fhd_params* params, int device) {
     for (int d = 0; d < 3; ++d) c->per[d] = per[d];
     c->walls = walls;
     c->wall = wall;
+    for (int d = 0; d < 3; ++d)
+        if (!per[d] && (p.bc_mass_lo[d] == 3 || p.bc_mass_hi[d] == 3)) c->reservoir = true;
     // GetHcGas, compressible_functions.cpp:91-100
     for (int i = 0; i < p.nspecies; ++i) {
         if (c->prm.hcv[i] < 0.) c->prm.hcv[i] = 0.5 * p.dof[i] * p.Runiv / p.molmass[i];
@@ -550,6 +588,7 @@ int fhd_set_bc_stag(fhd_ctx* c, fhd_fab prim, fhd_fab cu, const fhd_fab cumom[3]
         if (!c->per[d] && (c->prm.n_cells[d] < g || c->prm.n_cells[d] < gm)) return FHD_ERR_BAD_ARG;
     cudaSetDevice(c->device);
     const DevParams P = make_dev(c, 1.0, 0);
+    if (c->reservoir) return exact_bc_seq(P, c->wall, prim, cu, cumom, vel, true, c->stream);
     int rc = bc_mom(P, cumom, vel, c->stream);
     if (!rc) rc = exact_bc_prim(P, c->wall, prim, cu, cumom, c->stream);
     return rc;
@@ -813,6 +852,13 @@ static int walls_step_launches(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd
     const fhd_fab* insm[3] = {mom, c->cupm, c->cup2m};
     const fhd_fab* outs[3] = {&c->cup, &c->cup2, &cu};
     const fhd_fab* outsm[3] = {c->cupm, c->cup2m, mom};
+    if (c->reservoir) {
+        // the stage buffers start each step at zero, ghosts included, as RK3stepStag's
+        // cup / cup2 do (timeStepStag.cpp:30-62): with reservoirs the boundary passes
+        // read ghost corners before they rewrite them
+        const size_t stage_bytes = (size_t)((char*)c->sff[0].data - (char*)c->scratch);
+        if (cudaMemsetAsync(c->scratch, 0, stage_bytes, c->stream) != cudaSuccess) return FHD_ERR_CUDA;
+    }
     for (int s = 0; s < 3; ++s) {
         sc.stage = s + 1;
         sc.w = w[s];
@@ -845,11 +891,13 @@ static int walls_step_launches(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd
         {
             ProfScope ps(c, 4);
             // wall faces of the new momenta (the conversion reads them), then the
-            // periodic ghosts that the conversion and the conditions read
-            rc = bc_mom(sc.P, outsm[s], vel, c->stream);
-            GhostReq g[5] = {{*outs[s], 0, 1}, {*outs[s], 4, 1 + ns}, {outsm[s][0], 0, 1}, {outsm[s][1], 0, 1},
-                             {outsm[s][2], 0, 1}};
-            if (!rc) rc = fill_ghosts(g, 5, c->prm.n_cells, c->stream, c->per, 0);
+            // periodic ghosts that the conversion and the conditions read; with
+            // reservoirs every pass RK3stepStag makes here (the reservoir density
+            // enters the interface velocity)
+            if (c->reservoir) rc = exact_bc_seq(sc.P, c->wall, prim, *outs[s], outsm[s], vel, false, c->stream);
+            else rc = bc_mom(sc.P, outsm[s], vel, c->stream);
+            GhostReq g[4] = {{*outs[s], 0, nvars}, {outsm[s][0], 0, 1}, {outsm[s][1], 0, 1}, {outsm[s][2], 0, 1}};
+            if (!rc) rc = fill_ghosts(g, 4, c->prm.n_cells, c->stream, c->per, 0);
         }
         if (rc) return rc;
         {
@@ -861,8 +909,12 @@ static int walls_step_launches(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd
             ProfScope ps(c, 4);
             GhostReq g[5] = {{*outs[s], 0, nvars}, {prim, 0, nprim}, {vel[0], 0, 1}, {vel[1], 0, 1}, {vel[2], 0, 1}};
             rc = fill_ghosts(g, 5, c->prm.n_cells, c->stream, c->per, 0);
-            if (!rc) rc = bc_mom(sc.P, outsm[s], vel, c->stream);
-            if (!rc) rc = exact_bc_prim(sc.P, c->wall, prim, *outs[s], outsm[s], c->stream);
+            if (c->reservoir) {
+                if (!rc) rc = exact_bc_seq(sc.P, c->wall, prim, *outs[s], outsm[s], vel, true, c->stream);
+            } else {
+                if (!rc) rc = bc_mom(sc.P, outsm[s], vel, c->stream);
+                if (!rc) rc = exact_bc_prim(sc.P, c->wall, prim, *outs[s], outsm[s], c->stream);
+            }
         }
         if (rc) return rc;
     }

@@ -139,9 +139,10 @@ struct PersistArgs {
 };
 
 // ---- physical boundaries ---------------------------------------------------------------
-// wall values per side s = 2 d + (0 lo, 1 hi) (after SetupCWallStag)
+// wall values per side s = 2 d + (0 lo, 1 hi) (after SetupCWallStag): wall or
+// reservoir temperature, reservoir pressure and density, wall / reservoir Y and X
 struct WallParams {
-    double t[6];
+    double t[6], p[6], rho[6];
     double Yk[6][MAXS], Xk[6][MAXS];
 };
 

@@ -14,6 +14,8 @@ int exact_transport_ns1(const DevParams&, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fh
 int exact_convert_ns1(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const fhd_fab*, int*, cudaStream_t);
 int exact_walls_ns1(const StageCall&, int);
 int exact_bc_prim_ns1(const DevParams&, const WallParams&, fhd_fab, fhd_fab, const fhd_fab*, cudaStream_t);
+int exact_bc_seq_ns1(const DevParams&, const WallParams&, fhd_fab, fhd_fab, const fhd_fab*, const fhd_fab*, int,
+                     cudaStream_t);
 int exact_cellprep_ns2(const StageCall&);
 int exact_stage_ns2(const StageCall&, int);
 int exact_aux_ns2(const StageCall&);
@@ -23,6 +25,8 @@ int exact_transport_ns2(const DevParams&, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fh
 int exact_convert_ns2(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const fhd_fab*, int*, cudaStream_t);
 int exact_walls_ns2(const StageCall&, int);
 int exact_bc_prim_ns2(const DevParams&, const WallParams&, fhd_fab, fhd_fab, const fhd_fab*, cudaStream_t);
+int exact_bc_seq_ns2(const DevParams&, const WallParams&, fhd_fab, fhd_fab, const fhd_fab*, const fhd_fab*, int,
+                     cudaStream_t);
 int exact_cellprep_ns3(const StageCall&);
 int exact_stage_ns3(const StageCall&, int);
 int exact_aux_ns3(const StageCall&);
@@ -32,6 +36,8 @@ int exact_transport_ns3(const DevParams&, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fh
 int exact_convert_ns3(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const fhd_fab*, int*, cudaStream_t);
 int exact_walls_ns3(const StageCall&, int);
 int exact_bc_prim_ns3(const DevParams&, const WallParams&, fhd_fab, fhd_fab, const fhd_fab*, cudaStream_t);
+int exact_bc_seq_ns3(const DevParams&, const WallParams&, fhd_fab, fhd_fab, const fhd_fab*, const fhd_fab*, int,
+                     cudaStream_t);
 int exact_cellprep_ns4(const StageCall&);
 int exact_stage_ns4(const StageCall&, int);
 int exact_aux_ns4(const StageCall&);
@@ -41,6 +47,8 @@ int exact_transport_ns4(const DevParams&, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fh
 int exact_convert_ns4(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const fhd_fab*, int*, cudaStream_t);
 int exact_walls_ns4(const StageCall&, int);
 int exact_bc_prim_ns4(const DevParams&, const WallParams&, fhd_fab, fhd_fab, const fhd_fab*, cudaStream_t);
+int exact_bc_seq_ns4(const DevParams&, const WallParams&, fhd_fab, fhd_fab, const fhd_fab*, const fhd_fab*, int,
+                     cudaStream_t);
 
 size_t exact_batch_args_size_ns1(int, int);
 void exact_batch_pack_ns1(int, int, const StageCall&, void*);
@@ -48,32 +56,32 @@ int exact_batch_launch_ns1(int, int, int, const void*, const int*, int, int, cud
 size_t mixed_batch_args_size_ns1(int, int);
 void mixed_batch_pack_ns1(int, int, const StageCall&, void*);
 int mixed_batch_launch_ns1(int, int, int, const void*, const int*, int, int, cudaStream_t);
-int exact_batch_persist_ns1(int, const PersistArgs&, cudaStream_t);
-int mixed_batch_persist_ns1(int, const PersistArgs&, cudaStream_t);
+int exact_batch_persist_ns1(int, int, const PersistArgs&, cudaStream_t);
+int mixed_batch_persist_ns1(int, int, const PersistArgs&, cudaStream_t);
 size_t exact_batch_args_size_ns2(int, int);
 void exact_batch_pack_ns2(int, int, const StageCall&, void*);
 int exact_batch_launch_ns2(int, int, int, const void*, const int*, int, int, cudaStream_t);
 size_t mixed_batch_args_size_ns2(int, int);
 void mixed_batch_pack_ns2(int, int, const StageCall&, void*);
 int mixed_batch_launch_ns2(int, int, int, const void*, const int*, int, int, cudaStream_t);
-int exact_batch_persist_ns2(int, const PersistArgs&, cudaStream_t);
-int mixed_batch_persist_ns2(int, const PersistArgs&, cudaStream_t);
+int exact_batch_persist_ns2(int, int, const PersistArgs&, cudaStream_t);
+int mixed_batch_persist_ns2(int, int, const PersistArgs&, cudaStream_t);
 size_t exact_batch_args_size_ns3(int, int);
 void exact_batch_pack_ns3(int, int, const StageCall&, void*);
 int exact_batch_launch_ns3(int, int, int, const void*, const int*, int, int, cudaStream_t);
 size_t mixed_batch_args_size_ns3(int, int);
 void mixed_batch_pack_ns3(int, int, const StageCall&, void*);
 int mixed_batch_launch_ns3(int, int, int, const void*, const int*, int, int, cudaStream_t);
-int exact_batch_persist_ns3(int, const PersistArgs&, cudaStream_t);
-int mixed_batch_persist_ns3(int, const PersistArgs&, cudaStream_t);
+int exact_batch_persist_ns3(int, int, const PersistArgs&, cudaStream_t);
+int mixed_batch_persist_ns3(int, int, const PersistArgs&, cudaStream_t);
 size_t exact_batch_args_size_ns4(int, int);
 void exact_batch_pack_ns4(int, int, const StageCall&, void*);
 int exact_batch_launch_ns4(int, int, int, const void*, const int*, int, int, cudaStream_t);
 size_t mixed_batch_args_size_ns4(int, int);
 void mixed_batch_pack_ns4(int, int, const StageCall&, void*);
 int mixed_batch_launch_ns4(int, int, int, const void*, const int*, int, int, cudaStream_t);
-int exact_batch_persist_ns4(int, const PersistArgs&, cudaStream_t);
-int mixed_batch_persist_ns4(int, const PersistArgs&, cudaStream_t);
+int exact_batch_persist_ns4(int, int, const PersistArgs&, cudaStream_t);
+int mixed_batch_persist_ns4(int, int, const PersistArgs&, cudaStream_t);
 
 #define FHD_DISPATCH(ns, fn, ...)            \
     switch (ns) {                             \
@@ -102,6 +110,11 @@ int exact_walls_part(const StageCall& c, int part) { FHD_DISPATCH(c.P.ns, exact_
 int exact_bc_prim(const DevParams& P, const WallParams& W, fhd_fab prim, fhd_fab cons, const fhd_fab mom[3],
                   cudaStream_t s) {
     FHD_DISPATCH(P.ns, exact_bc_prim_ns, P, W, prim, cons, mom, s)
+}
+
+int exact_bc_seq(const DevParams& P, const WallParams& W, fhd_fab prim, fhd_fab cons, const fhd_fab mom[3],
+                 const fhd_fab vel[3], bool rre, cudaStream_t s) {
+    FHD_DISPATCH(P.ns, exact_bc_seq_ns, P, W, prim, cons, mom, vel, rre ? 1 : 0, s)
 }
 
 int bc_mom(const DevParams& P, const fhd_fab mom[3], const fhd_fab vel[3], cudaStream_t s) {
@@ -155,9 +168,9 @@ int batch_launch(int ns, bool mixed, int kind, int mode, int tile, const void* d
     FHD_DISPATCH(ns, exact_batch_launch_ns, kind, mode, tile, dargs, dbpref, nmem, nblocks, s)
 }
 
-int batch_persist(int ns, bool mixed, int mode, const PersistArgs& a, cudaStream_t s) {
-    if (mixed) { FHD_DISPATCH(ns, mixed_batch_persist_ns, mode, a, s) }
-    FHD_DISPATCH(ns, exact_batch_persist_ns, mode, a, s)
+int batch_persist(int ns, bool mixed, int mode, int tile, const PersistArgs& a, cudaStream_t s) {
+    if (mixed) { FHD_DISPATCH(ns, mixed_batch_persist_ns, mode, tile, a, s) }
+    FHD_DISPATCH(ns, exact_batch_persist_ns, mode, tile, a, s)
 }
 
 int batch_face_tiles() { return kNumBatchFaceTiles; }
@@ -309,15 +322,16 @@ int init_uniform(const fhd_fab& cu, int ns, double rho0, double rhoE, const doub
     return cuda_rc(cudaGetLastError());
 }
 
-int num_tiles() { return kNumStageBlocks + kNumZmTiles; }
+int num_tiles() { return kNumStageBlocks + kNumZmTiles + kNumFaces3Tiles; }
 
 // 0-4: the split stage (stress, face and update kernels) with the face kernel's
 // block size / register cap; 5-8: the fused z-marching stage kernel with its
-// block size and z-chunk depth
+// block size and z-chunk depth; 9-10: the split stage with the three face
+// directions in one launch
 const char* tile_name(int t) {
     static const char* names[] = {"b128-min4", "b256-min2", "b128-min6", "b128-min10", "b128-min8",
                                   "fused16x8-t128-z32", "fused16x8-t256-z32", "fused16x8-t256-z64",
-                                  "fused16x8-t384-z32"};
+                                  "fused16x8-t384-z32", "faces3-b128-min8", "faces3-b128-min4"};
     return (t >= 0 && t < num_tiles()) ? names[t] : "?";
 }
 

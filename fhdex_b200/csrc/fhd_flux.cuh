@@ -681,7 +681,8 @@ FHD_D double edge_total_w(const DevParams& P, const Taus<R>& t, double adv, int 
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int side = 2 * d + h, b = P.bc_vel[side];
-            if ((b == 1 || b == 2) && x[d] == (h ? P.n[d] : 0)) v *= stoch_factor(P, b);
+            // a reservoir side keeps the factor 1
+            if ((b == 1 || b == 2) && P.bc_mass[side] < 3 && x[d] == (h ? P.n[d] : 0)) v *= stoch_factor(P, b);
         }
     }
     v -= (double)t.d;
@@ -689,11 +690,17 @@ FHD_D double edge_total_w(const DevParams& P, const Taus<R>& t, double adv, int 
     return v;
 }
 
-// centre momentum flux in direction d at a cell (fluxStag.cpp:799-803, 1444-1448, 1848-1866)
-template <int NS, class R>
+// centre momentum flux in direction d at a cell (fluxStag.cpp:799-803, 1444-1448, 1848-1866).
+// WL: a ghost cell beyond a reservoir side of direction d carries no stochastic or
+// diffusive part (BCWallReservoirFluxStag, boundaryStag.cpp:482-577).
+template <int NS, class R, bool WL = false>
 FHD_D double cen_total(const DevParams& P, const Fields<NS, R>& F, const CellTaus<R>& t, int d, int i, int j, int k) {
     double v = (double)t.s[d];
     v -= (double)t.d[d];
+    if (WL) {
+        const int x = d == 0 ? i : (d == 1 ? j : k);
+        if ((x < 0 && P.bc_mass[2 * d] == 3) || (x > P.n[d] - 1 && P.bc_mass[2 * d + 1] == 3)) v = 0.0;
+    }
     if (P.advection_type >= 0) {
         const Arr4<const double>& m = F.mom[d];
         const Arr4<const double>& u = F.vel[d];

@@ -154,6 +154,10 @@ int exact_walls_part(const StageCall& c, int part);
 int exact_bc_prim(const DevParams& P, const WallParams& W, fhd_fab prim, fhd_fab cons, const fhd_fab mom[3],
                   cudaStream_t s);
 int bc_mom(const DevParams& P, const fhd_fab mom[3], const fhd_fab vel[3], cudaStream_t s);
+// the reference's boundary passes one by one (boxes with reservoirs): setBCStag
+// (rre) or the passes before the conversion
+int exact_bc_seq(const DevParams& P, const WallParams& W, fhd_fab prim, fhd_fab cons, const fhd_fab mom[3],
+                 const fhd_fab vel[3], bool rre, cudaStream_t s);
 // mixed translation unit (coefficient fabs are f32)
 int mixed_cellprep(const StageCall& c);
 int mixed_stage_part(const StageCall& c, int part);
@@ -196,7 +200,8 @@ int batch_launch(int ns, bool mixed, int kind, int mode, int tile, const void* d
                  int nblocks, cudaStream_t s);
 int batch_face_tiles();
 // the persistent batched step (k_batch_persist): one launch per RK3 step
-int batch_persist(int ns, bool mixed, int mode, const PersistArgs& a, cudaStream_t s);
+// tile: register cap as the batch face tiles (-1 the default for the species count)
+int batch_persist(int ns, bool mixed, int mode, int tile, const PersistArgs& a, cudaStream_t s);
 int batch_face_min_blocks(int tile);
 struct GhostFabDesc;  // opaque to the host code
 int ghost_desc_size();

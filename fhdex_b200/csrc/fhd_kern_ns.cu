@@ -36,8 +36,9 @@ int FHD_CAT(FHD_CAT(FHD_PFX, _batch_launch_ns), FHD_NS)(int kind, int mode, int 
                           : batch_launch_t<FHD_NS, FHD_R, NZ_PHILOX>(kind, tile, dargs, dbpref, nmem, nblocks, s);
 }
 
-int FHD_CAT(FHD_CAT(FHD_PFX, _batch_persist_ns), FHD_NS)(int mode, const PersistArgs& a, cudaStream_t s) {
-    return mode == NM_OFF ? batch_persist_t<FHD_NS, FHD_R, NZ_OFF>(a, s) : batch_persist_t<FHD_NS, FHD_R, NZ_PHILOX>(a, s);
+int FHD_CAT(FHD_CAT(FHD_PFX, _batch_persist_ns), FHD_NS)(int mode, int tile, const PersistArgs& a, cudaStream_t s) {
+    return mode == NM_OFF ? batch_persist_t<FHD_NS, FHD_R, NZ_OFF>(a, tile, s)
+                          : batch_persist_t<FHD_NS, FHD_R, NZ_PHILOX>(a, tile, s);
 }
 
 #if defined(FHD_MIXED) && FHD_MIXED
@@ -86,6 +87,11 @@ int FHD_CAT(exact_walls_ns, FHD_NS)(const StageCall& c, int part) { return launc
 int FHD_CAT(exact_bc_prim_ns, FHD_NS)(const DevParams& P, const WallParams& W, fhd_fab prim, fhd_fab cons,
                                       const fhd_fab* mom, cudaStream_t s) {
     return launch_bc_prim<FHD_NS>(P, W, prim, cons, mom, s);
+}
+
+int FHD_CAT(exact_bc_seq_ns, FHD_NS)(const DevParams& P, const WallParams& W, fhd_fab prim, fhd_fab cons,
+                                     const fhd_fab* mom, const fhd_fab* vel, int rre, cudaStream_t s) {
+    return launch_bc_seq<FHD_NS>(P, W, prim, cons, mom, vel, rre != 0, s);
 }
 
 int FHD_CAT(exact_transport_ns, FHD_NS)(const DevParams& P, fhd_fab prim, fhd_fab eta, fhd_fab zeta, fhd_fab kappa,

@@ -142,6 +142,14 @@ constexpr int kZmThreads[] = {128, 256, 256, 384};
 constexpr int kZmChunks[] = {32, 32, 64, 32};
 constexpr int kNumZmTiles = 4;
 inline bool tile_is_fused(int t) { return t >= kNumStageBlocks && t < kNumStageBlocks + kNumZmTiles; }
+// the split stage with the three face directions in one launch (k_faces3): register
+// caps of 64 and 128 (8 and 4 resident blocks of 128)
+constexpr int kFaces3MinBlocks[] = {8, 4};
+constexpr int kNumFaces3Tiles = 2;
+inline int faces3_tile(int t) {
+    const int b = kNumStageBlocks + kNumZmTiles;
+    return (t >= b && t < b + kNumFaces3Tiles) ? t - b : -1;
+}
 
 template <int NS, class R, int NZ>
 StageArgs<NS, R, NZ> make_stage_args(const StageCall& c) {
@@ -177,6 +185,14 @@ int launch_stage_part_t(const StageCall& c, int part) {
     const int b = stage_block(c);
     if (part == 0) {
         k_taus<NS, R, NZ><<<grid_for((int64_t)(N[0] + 2) * (N[1] + 2) * (N[2] + 2), b), b, 0, c.stream>>>(a);
+    } else if (part == 1 && faces3_tile(c.tile) >= 0) {
+        const int64_t pts = (int64_t)(N[0] + 1) * (N[1] + 1) * (N[2] + 1);
+        if (faces3_tile(c.tile) == 0)
+            k_faces3<NS, R, NZ, 128, kFaces3MinBlocks[0]><<<resident_grid<k_faces3<NS, R, NZ, 128, kFaces3MinBlocks[0]>>(
+                pts, 128), 128, 0, c.stream>>>(a);
+        else
+            k_faces3<NS, R, NZ, 128, kFaces3MinBlocks[1]><<<resident_grid<k_faces3<NS, R, NZ, 128, kFaces3MinBlocks[1]>>(
+                pts, 128), 128, 0, c.stream>>>(a);
     } else if (part == 1) {
         const int t = (c.tile >= 0 && c.tile < kNumStageBlocks) ? c.tile : 0;
 #define FHD_FACES(BS, MINB)                                                                                      \
@@ -301,6 +317,65 @@ int launch_bc_prim(const DevParams& P, const WallParams& W, const fhd_fab& prim,
     return cuda_rc(cudaGetLastError());
 }
 
+// The reference's boundary passes in its order, one launch each (k_bc_pass):
+// for each direction d BCMassTempPress (lo, hi) and BCMomNormal (lo, hi) of
+// mom[d] / vel[d] when d has walls, and BCMomTrans of mom[d] / vel[d] across the
+// other directions' walls (x lo, x hi, y lo, ...); with rre, BCRhoRhoE of every
+// wall side after them (setBCStag); without, the passes RK3stepStag makes before
+// the conversion.
+template <int NS>
+int launch_bc_seq(const DevParams& P, const WallParams& W, const fhd_fab& prim, const fhd_fab& cons,
+                  const fhd_fab* mom, const fhd_fab* vel, bool rre, cudaStream_t st) {
+    BcPassArgs<NS> a;
+    a.P = P;
+    a.W = W;
+    a.prim = view<double>(prim);
+    a.cons = view<double>(cons);
+    a.mx = view<const double>(mom[0]);
+    a.my = view<const double>(mom[1]);
+    a.mz = view<const double>(mom[2]);
+    const int g = -prim.lo[0], gm = -mom[0].lo[0];
+    auto wall = [&](int d) { return P.walls && !P.periodic[d]; };
+    auto launch = [&](int fn, int side, int c) {
+        a.fn = fn;
+        a.side = side;
+        a.c = c;
+        const int d = side >> 1, hi = side & 1;
+        for (int e = 0; e < 3; ++e) {
+            const bool cell = fn == BC_MTP || fn == BC_RRE;
+            const int gg = cell ? g : gm;
+            const int nod = (!cell && e == c) ? 1 : 0;
+            a.blo[e] = -gg;
+            a.bhi[e] = P.n[e] - 1 + nod + gg;
+            if (e == d) {
+                if (fn == BC_MOMN) { a.blo[e] = hi ? P.n[e] : -gg; a.bhi[e] = hi ? P.n[e] + gg : 0; }
+                else { a.blo[e] = hi ? P.n[e] : -gg; a.bhi[e] = hi ? P.n[e] + gg - 1 : -1; }
+            }
+        }
+        if (fn == BC_MOMN || fn == BC_MOMT) {
+            a.mom = view<double>(mom[c]);
+            a.vel = view<double>(vel[c]);
+        }
+        const int64_t tot = (int64_t)(a.bhi[0] - a.blo[0] + 1) * (a.bhi[1] - a.blo[1] + 1) * (a.bhi[2] - a.blo[2] + 1);
+        k_bc_pass<NS><<<grid_for(tot, 128), 128, 0, st>>>(a);
+        return cuda_rc(cudaGetLastError());
+    };
+    int rc = FHD_OK;
+    // every direction d: its own sides' passes when it has walls, and BCMomTrans of
+    // mom[d] / vel[d] across the other directions' walls in any case
+    for (int d = 0; d < 3 && !rc; ++d) {
+        for (int h = 0; h < 2 && !rc && wall(d); ++h) rc = launch(BC_MTP, 2 * d + h, d);
+        for (int h = 0; h < 2 && !rc && wall(d); ++h) rc = launch(BC_MOMN, 2 * d + h, d);
+        for (int e = 0; e < 3 && !rc; ++e) {
+            if (e == d || !wall(e)) continue;
+            for (int h = 0; h < 2 && !rc; ++h) rc = launch(BC_MOMT, 2 * e + h, d);
+        }
+    }
+    for (int side = 0; side < 6 && rre && !rc; ++side)
+        if (wall(side >> 1)) rc = launch(BC_RRE, side, 0);
+    return rc;
+}
+
 // part: 0 stresses, 1 face fluxes, 2 update, 3 the fused kernel (all three)
 template <int NS, class R>
 int launch_stage_part(const StageCall& c, int part) {
@@ -414,12 +489,23 @@ int batch_launch_t(int kind, int tile, const void* dargs, const int* dbpref, int
 }
 
 // the persistent batched step: grid = the blocks that fit on the GPU at once
-template <int NS, class R, int NZ>
-int batch_persist_t(const PersistArgs& a, cudaStream_t s) {
-    constexpr int MINB = sizeof(R) == 8 ? 4 : 6;
+template <int NS, class R, int NZ, int MINB>
+int batch_persist_minb(const PersistArgs& a, cudaStream_t s) {
     const int grid = resident_blocks<k_batch_persist<NS, R, NZ, MINB>>(128);
     k_batch_persist<NS, R, NZ, MINB><<<grid, 128, 0, s>>>(a);
     return cuda_rc(cudaGetLastError());
+}
+
+// tile: the register cap of the batch face tiles (kBatchFaceMinBlocks: 64, 80 or
+// 128 registers); -1 the default, 64 registers up to two species (measured on the
+// 512-member ensemble: 156 / 170 / 223 ms per step FP64, 112 / 124 / 141 mixed)
+// and 128 above
+template <int NS, class R, int NZ>
+int batch_persist_t(const PersistArgs& a, int tile, cudaStream_t s) {
+    if (tile < 0 || tile >= kNumBatchFaceTiles) tile = NS <= 2 ? 0 : 2;
+    if (tile == 0) return batch_persist_minb<NS, R, NZ, kBatchFaceMinBlocks[0]>(a, s);
+    if (tile == 1) return batch_persist_minb<NS, R, NZ, kBatchFaceMinBlocks[1]>(a, s);
+    return batch_persist_minb<NS, R, NZ, kBatchFaceMinBlocks[2]>(a, s);
 }
 
 #define FHD_NS_SWITCH(ns, CALL) \

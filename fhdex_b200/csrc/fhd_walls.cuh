@@ -211,4 +211,134 @@ static __global__ void __launch_bounds__(128) k_bc_prim(BcPrimArgs<NS> a) {
     }
 }
 
+// ---- one pass of the reference's boundary routines ---------------------------------
+// With reservoirs (bc_mass 3: ghost cells held at the reservoir's state, flow through
+// the interface) the reference's passes read values that earlier passes of the same
+// call left at ghost corners, some of them through the density in cons, so they run
+// here one launch per pass, in the reference's order, each over the slab of the grown
+// box beyond one side:
+//   BC_MTP   BCMassTempPress of side s     (prim; cons rho on reservoir sides)
+//   BC_MOMN  BCMomNormal of side s         (mom[d], vel[d]; d = the side's direction)
+//   BC_MOMT  BCMomTrans of side s on mom[c], vel[c] (c != d)
+//   BC_RRE   BCRhoRhoE of side s           (prim rho, cons rho, rho E, rho Y)
+enum { BC_MTP = 0, BC_MOMN = 1, BC_MOMT = 2, BC_RRE = 3 };
+
+template <int NS>
+struct BcPassArgs {
+    DevParams P;
+    WallParams W;
+    Arr4<double> prim, cons, mom, vel;   // mom, vel: component c (BC_MOMN: c = d)
+    Arr4<const double> mx, my, mz;       // face momenta (BC_RRE)
+    int fn, side, c;
+    int blo[3], bhi[3];                  // the slab
+};
+
+template <int NS>
+static __global__ void __launch_bounds__(128) k_bc_pass(BcPassArgs<NS> a) {
+    const DevParams& P = a.P;
+    const WallParams& W = a.W;
+    const int s = a.side, d = s >> 1, hi = s & 1;
+    const int64_t nx = a.bhi[0] - a.blo[0] + 1, ny = a.bhi[1] - a.blo[1] + 1, nz = a.bhi[2] - a.blo[2] + 1;
+    const int64_t tot = nx * ny * nz;
+    const int bm = P.bc_mass[s], bt = P.bc_therm[s], bv = P.bc_vel[s];
+    constexpr int NPRIM = 6 + 2 * NS;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < tot; q += (int64_t)gridDim.x * blockDim.x) {
+        int p[3] = {a.blo[0] + (int)(q % nx), a.blo[1] + (int)((q / nx) % ny), a.blo[2] + (int)(q / (nx * ny))};
+        const int i = p[0], j = p[1], k = p[2];
+        const int n = P.n[d];
+        int m[3] = {i, j, k};
+        m[d] = hi ? 2 * n - 1 - p[d] : -p[d] - 1;   // mirror across the side (cell-centred direction d)
+        if (a.fn == BC_MTP) {
+            const Arr4<double>& pr = a.prim;
+            if (bm == 1)
+                for (int c = 6; c < NPRIM; ++c) pr(i, j, k, c) = pr(m[0], m[1], m[2], c);
+            if (bm == 2)
+                for (int c = 0; c < NS; ++c) {
+                    pr(i, j, k, 6 + c) = W.Yk[s][c];
+                    pr(i, j, k, 6 + NS + c) = W.Xk[s][c];
+                }
+            if (bm >= 3) {
+                for (int c = 0; c < NS; ++c) {
+                    pr(i, j, k, 6 + c) = W.Yk[s][c];
+                    pr(i, j, k, 6 + NS + c) = W.Xk[s][c];
+                    pr(i, j, k, 0) = W.rho[s];
+                    a.cons(i, j, k, 0) = W.rho[s];
+                    pr(i, j, k, 4) = W.t[s];
+                    pr(i, j, k, 5) = W.p[s];
+                }
+            } else if (bt == 1) {
+                for (int c = 4; c < 6; ++c) pr(i, j, k, c) = pr(m[0], m[1], m[2], c);
+            } else if (bt == 2) {
+                pr(i, j, k, 4) = W.t[s];
+                pr(i, j, k, 5) = pr(m[0], m[1], m[2], 5);
+            }
+        } else if (a.fn == BC_MOMN) {
+            // mom[d], vel[d] are nodal in d: the interface face is n_d * hi
+            const int f = hi ? n : 0;
+            const bool ghost = hi ? p[d] > f : p[d] < f;
+            int fi[3] = {i, j, k}, gi[3] = {i, j, k};
+            fi[d] = f;            // the interface face / the cell inside it
+            gi[d] = f - 1;        // the cell before it
+            if (bm >= 3) {
+                if (ghost) {
+                    a.vel(i, j, k) = -2 * a.mom(fi[0], fi[1], fi[2]) /
+                                     (a.cons(fi[0], fi[1], fi[2], 0) + a.cons(gi[0], gi[1], gi[2], 0));
+                    a.mom(i, j, k) = -1 * a.mom(fi[0], fi[1], fi[2]);
+                } else if (p[d] == f) {
+                    a.vel(i, j, k) = 2 * a.mom(i, j, k) / (a.cons(fi[0], fi[1], fi[2], 0) + a.cons(gi[0], gi[1], gi[2], 0));
+                }
+            } else if (bv == 1 || bv == 2) {
+                if (ghost) {
+                    a.vel(i, j, k) = 0.0;
+                    a.mom(i, j, k) = 0.0;
+                } else if (p[d] == f) {
+                    a.vel(i, j, k) = 0.;
+                    a.mom(i, j, k) = 0.;
+                }
+            }
+        } else if (a.fn == BC_MOMT) {
+            if (bv == 1 || bv == 2) {
+                const double fac = bm >= 3 ? 0.0 : (bv == 1 ? 1.0 : 0.0);
+                a.vel(i, j, k) = fac * a.vel(m[0], m[1], m[2]);
+                a.mom(i, j, k) = fac * a.mom(m[0], m[1], m[2]);
+            }
+        } else {
+            const Arr4<double>& pr = a.prim;
+            if (bm >= 3) {
+                const double temp = pr(i, j, k, 4), rho = pr(i, j, k, 0);
+                double cvmix = 0., e0mix = 0.;
+                for (int c = 0; c < NS; ++c) {
+                    cvmix += pr(i, j, k, 6 + c) * P.hcv[c];
+                    e0mix += pr(i, j, k, 6 + c) * P.e0[c];
+                }
+                const double intenergy = e0mix + temp * cvmix;
+                for (int c = 0; c < NS; ++c) a.cons(i, j, k, 5 + c) = rho * pr(i, j, k, 6 + c);
+                const double kinenergy = 0.;
+                a.cons(i, j, k, 4) = rho * intenergy + kinenergy;
+            } else if (bv == 1 || bv == 2) {
+                const double temp = pr(i, j, k, 4), pt = pr(i, j, k, 5);
+                double molmix = 0.;
+                for (int c = 0; c < NS; ++c) molmix += pr(i, j, k, 6 + c) / P.molmass[c];
+                molmix = 1. / molmix;
+                const double rho = pt / (P.Runiv / molmix) / temp;
+                double cvmix = 0., e0mix = 0.;
+                for (int c = 0; c < NS; ++c) {
+                    cvmix += pr(i, j, k, 6 + c) * P.hcv[c];
+                    e0mix += pr(i, j, k, 6 + c) * P.e0[c];
+                }
+                const double intenergy = e0mix + temp * cvmix;
+                pr(i, j, k, 0) = rho;
+                a.cons(i, j, k, 0) = rho;
+                for (int c = 0; c < NS; ++c) a.cons(i, j, k, 5 + c) = rho * pr(i, j, k, 6 + c);
+                double kin = 0.;
+                kin += (a.mx(i + 1, j, k) + a.mx(i, j, k)) * (a.mx(i + 1, j, k) + a.mx(i, j, k));
+                kin += (a.my(i, j + 1, k) + a.my(i, j, k)) * (a.my(i, j + 1, k) + a.my(i, j, k));
+                kin += (a.mz(i, j, k + 1) + a.mz(i, j, k)) * (a.mz(i, j, k + 1) + a.mz(i, j, k));
+                kin *= (0.125 / rho);
+                a.cons(i, j, k, 4) = rho * intenergy + kin;
+            }
+        }
+    }
+}
+
 }  // namespace fhd

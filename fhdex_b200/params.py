@@ -70,6 +70,12 @@ class Params:
     bc_Yk_hi: tuple = ((), (), ())
     bc_Xk_lo: tuple = ((), (), ())
     bc_Xk_hi: tuple = ((), (), ())
+    # reservoirs (bc_mass 3): pressure (<= 0: the initial state's) and density
+    # (<= 0: from p, t and the composition)
+    p_lo: tuple = (0.0, 0.0, 0.0)
+    p_hi: tuple = (0.0, 0.0, 0.0)
+    rho_lo: tuple = (-1.0, -1.0, -1.0)
+    rho_hi: tuple = (-1.0, -1.0, -1.0)
     # initial state (prob_type 1): not part of fhd_params
     rho0: float = 1.78e-3
     T_init: float = 273.0
@@ -148,6 +154,12 @@ class Params:
                 vals = getattr(self, name)[d]
                 for i in range(MAX_SPECIES):
                     getattr(p, name)[d][i] = vals[i] if i < len(vals) else -1.0
+            for name in ("p_lo", "p_hi", "rho_lo", "rho_hi"):
+                getattr(p, name)[d] = getattr(self, name)[d]
+        p.rho0 = self.rho0
+        p.T_init = self.T_init
+        for i in range(MAX_SPECIES):
+            p.rhobar[i] = self.rhobar[i] if i < len(self.rhobar) else 0.0
         return p
 
     # -- thermodynamics on the host (for dt and theory) -------------------------------
@@ -249,25 +261,31 @@ def hard_sphere_single_gas(p: Params, T=None):
 def with_walls(p: Params, **dirs) -> Params:
     """``p`` with physical walls on the directions named x, y, z (both sides),
     each a dict: vel (1 slip, 2 no-slip), therm (1 adiabatic, 2 isothermal), mass
-    (1 impermeable, 2 held at a wall composition), t = (t_lo, t_hi) for isothermal
-    walls, Yk or Xk = (lo, hi) compositions for concentration walls.  The other
+    (1 impermeable, 2 held at a wall composition, 3 reservoir), t = (t_lo, t_hi)
+    for isothermal walls and reservoirs, Yk or Xk = (lo, hi) compositions for
+    concentration walls and reservoirs, p / rho = (lo, hi) reservoir pressure and
+    density (defaults: the initial pressure; rho from p, t, Y).  The other
     directions stay periodic."""
     vl, vh, ml, mh, tl, th = ([-1] * 3 for _ in range(6))
     Tl, Th = [0.0] * 3, [0.0] * 3
     comp = {k: [(), (), ()] for k in ("bc_Yk_lo", "bc_Yk_hi", "bc_Xk_lo", "bc_Xk_hi")}
+    Pl, Ph, Rl, Rh = [0.0] * 3, [0.0] * 3, [-1.0] * 3, [-1.0] * 3
     for ax, spec in dirs.items():
         d = "xyz".index(ax)
         vl[d] = vh[d] = int(spec.get("vel", 2))
         ml[d] = mh[d] = int(spec.get("mass", 1))
         tl[d] = th[d] = int(spec.get("therm", 1))
         Tl[d], Th[d] = (float(v) for v in spec.get("t", (p.T_init, p.T_init)))
+        Pl[d], Ph[d] = (float(v) for v in spec.get("p", (0.0, 0.0)))
+        Rl[d], Rh[d] = (float(v) for v in spec.get("rho", (-1.0, -1.0)))
         for key in ("Yk", "Xk"):
             if key in spec:
                 comp[f"bc_{key}_lo"][d] = tuple(float(v) for v in spec[key][0])
                 comp[f"bc_{key}_hi"][d] = tuple(float(v) for v in spec[key][1])
     return p.replace(walls=1, bc_vel_lo=tuple(vl), bc_vel_hi=tuple(vh), bc_mass_lo=tuple(ml),
                      bc_mass_hi=tuple(mh), bc_therm_lo=tuple(tl), bc_therm_hi=tuple(th), t_lo=tuple(Tl),
-                     t_hi=tuple(Th), **{k: tuple(v) for k, v in comp.items()})
+                     t_hi=tuple(Th), p_lo=tuple(Pl), p_hi=tuple(Ph), rho_lo=tuple(Rl), rho_hi=tuple(Rh),
+                     **{k: tuple(v) for k, v in comp.items()})
 
 
 def stable_dt(p: Params, cfl=0.2, diff=0.1):
@@ -320,7 +338,8 @@ def to_inputs(p: "Params") -> str:
         vals = getattr(p, key) if p.walls else (-1, -1, -1)
         lines.append(row(key, [int(x) for x in vals]))
     if p.walls:
-        lines += [row("t_lo", p.t_lo), row("t_hi", p.t_hi)]
+        lines += [row("t_lo", p.t_lo), row("t_hi", p.t_hi), row("p_lo", p.p_lo), row("p_hi", p.p_hi),
+                  row("rho_lo", p.rho_lo), row("rho_hi", p.rho_hi)]
         for name, key in (("bc_Yk_lo", "bc_Yk_{}_lo"), ("bc_Yk_hi", "bc_Yk_{}_hi"), ("bc_Xk_lo", "bc_Xk_{}_lo"),
                           ("bc_Xk_hi", "bc_Xk_{}_hi")):
             for d, ax in enumerate("xyz"):
@@ -401,9 +420,9 @@ def parse_inputs(text: str, base: Params | None = None) -> Params:
             if key in kv:
                 upd[key] = tuple(int(x) for x in kv[key][:3])
         for key in ("bc_mass_lo", "bc_mass_hi"):
-            if any(v >= 3 for v in upd.get(key, ())):
-                raise ValueError(f"{key}: reservoir boundaries (bc_mass >= 3) are not implemented")
-        for key in ("t_lo", "t_hi"):
+            if any(v >= 4 for v in upd.get(key, ())):
+                raise ValueError(f"{key}: the particle reservoir (bc_mass 4) is not implemented")
+        for key in ("t_lo", "t_hi", "p_lo", "p_hi", "rho_lo", "rho_hi"):
             if key in kv:
                 upd[key] = tuple(float(x) for x in kv[key][:3])
         for name, pat in (("bc_Yk_lo", "bc_Yk_{}_lo"), ("bc_Yk_hi", "bc_Yk_{}_hi"), ("bc_Xk_lo", "bc_Xk_{}_lo"),

@@ -108,11 +108,15 @@ inline int plot_deltaY_dir = -1;  // common_functions.cpp:620
 // here; the staggered decks set every bc_vel); otherwise both sides are walls:
 // bc_vel 1 slip / 2 no-slip, bc_therm 1 adiabatic / 2 isothermal at t_lo / t_hi,
 // bc_mass 1 impermeable / 2 at the wall composition bc_Yk_* or bc_Xk_* (the one
-// that sums to 1).  Reservoirs (bc_mass >= 3) are refused.
+// that sums to 1) / 3 a reservoir at t, p, rho and that composition.  The particle
+// reservoir (bc_mass 4) is refused.
 inline GpuArray<int, 3> bc_vel_lo{{-1, -1, -1}}, bc_vel_hi{{-1, -1, -1}};
 inline GpuArray<int, 3> bc_mass_lo{{-1, -1, -1}}, bc_mass_hi{{-1, -1, -1}};
 inline GpuArray<int, 3> bc_therm_lo{{-1, -1, -1}}, bc_therm_hi{{-1, -1, -1}};
 inline GpuArray<Real, 3> t_lo{{0., 0., 0.}}, t_hi{{0., 0., 0.}};
+// reservoirs (bc_mass 3): pressure (<= 0: the initial state's), density (<= 0: from p, t, Y)
+inline GpuArray<Real, 3> p_lo{{0., 0., 0.}}, p_hi{{0., 0., 0.}};
+inline GpuArray<Real, 3> rho_lo{{-1., -1., -1.}}, rho_hi{{-1., -1., -1.}};
 inline GpuArray<Real, MAX_SPECIES> bc_Yk_x_lo{{-1, -1, -1, -1, -1, -1, -1, -1}}, bc_Yk_x_hi{{-1, -1, -1, -1, -1, -1, -1, -1}};
 inline GpuArray<Real, MAX_SPECIES> bc_Yk_y_lo{{-1, -1, -1, -1, -1, -1, -1, -1}}, bc_Yk_y_hi{{-1, -1, -1, -1, -1, -1, -1, -1}};
 inline GpuArray<Real, MAX_SPECIES> bc_Yk_z_lo{{-1, -1, -1, -1, -1, -1, -1, -1}}, bc_Yk_z_hi{{-1, -1, -1, -1, -1, -1, -1, -1}};
@@ -225,6 +229,10 @@ inline fhd_params params_from_globals() {
         p.bc_therm_hi[d] = common::bc_therm_hi[d];
         p.t_lo[d] = common::t_lo[d];
         p.t_hi[d] = common::t_hi[d];
+        p.p_lo[d] = common::p_lo[d];
+        p.p_hi[d] = common::p_hi[d];
+        p.rho_lo[d] = common::rho_lo[d];
+        p.rho_hi[d] = common::rho_hi[d];
         for (int s = 0; s < FHD_MAX_SPECIES; ++s) {
             p.bc_Yk_lo[d][s] = (*yk[0][d])[s];
             p.bc_Yk_hi[d][s] = (*yk[1][d])[s];
@@ -232,6 +240,9 @@ inline fhd_params params_from_globals() {
             p.bc_Xk_hi[d][s] = (*xk[1][d])[s];
         }
     }
+    p.rho0 = common::rho0;
+    p.T_init = common::T_init[0];
+    for (int s = 0; s < FHD_MAX_SPECIES; ++s) p.rhobar[s] = common::rhobar[s];
     return p;
 }
 

@@ -117,10 +117,14 @@ typedef struct {
      * are walls with bc_vel 1 (slip) or 2 (no-slip), bc_therm 1 (adiabatic) or 2
      * (isothermal at t_lo[d] / t_hi[d]) and bc_mass 1 (impermeable) or 2 (species
      * held at the wall composition bc_Yk / bc_Xk, of which the one summing to 1
-     * defines the other, as SetupCWallStag does; fhd_get_params returns both).
-     * Reservoirs (bc_mass >= 3) are outside the implemented scope.  FP64 only;
-     * the state's ghost width is then exactly 2 in fhd_rk3_step_stag(s), and
-     * the batched and no-allocation steps return FHD_ERR_UNSUPPORTED. */
+     * defines the other, as SetupCWallStag does; fhd_get_params returns both)
+     * or 3 (a reservoir: ghost cells held at the reservoir state t, p_lo / p_hi
+     * (<= 0: the initial state's pressure), rho_lo / rho_hi (<= 0: from p, t, Y;
+     * else t <= 0 is derived from p and rho) and composition bc_Yk / bc_Xk; flow
+     * passes the interface).  The particle reservoir (bc_mass 4) returns
+     * FHD_ERR_UNSUPPORTED.  FP64 only; the state's ghost width is then exactly 2
+     * in fhd_rk3_step_stag(s), and the batched and no-allocation steps return
+     * FHD_ERR_UNSUPPORTED. */
     int walls;
     int bc_vel_lo[3], bc_vel_hi[3];
     int bc_mass_lo[3], bc_mass_hi[3];
@@ -128,6 +132,11 @@ typedef struct {
     double t_lo[3], t_hi[3];
     double bc_Yk_lo[3][FHD_MAX_SPECIES], bc_Yk_hi[3][FHD_MAX_SPECIES];
     double bc_Xk_lo[3][FHD_MAX_SPECIES], bc_Xk_hi[3][FHD_MAX_SPECIES];
+    double p_lo[3], p_hi[3], rho_lo[3], rho_hi[3];
+    /* The initial state (InitConsVarStag prob_type 1; deck keys rho0, T_init,
+     * rhobar): the reservoirs' default pressure. */
+    double rho0, T_init;
+    double rhobar[FHD_MAX_SPECIES];
 } fhd_params;
 
 /* Injected Gaussian noise for one RK3 step: the "A" and "B" white-noise fields
@@ -343,8 +352,10 @@ int fhd_batch_size(const fhd_batch* batch);
  * cellprep, stresses, faces x/y/z, update, ghost fill; then the conversion, its
  * ghost fill and the step counter) from one device counter in phase-major order
  * and wait, bounded in time, for the member's previous phase.  Results are bitwise
- * those of the per-kind launches.  Replayed from a graph like them. */
-int fhd_batch_set_persistent(fhd_batch* batch, int enable);
+ * those of the per-kind launches.  Replayed from a graph like them.  tile: the
+ * kernel's register cap as the batch face tiles (0 .. fhd_batch_num_tiles()-1:
+ * 64, 80, 128 registers); -1: 64 up to two species, 128 above. */
+int fhd_batch_set_persistent(fhd_batch* batch, int enable, int tile);
 /* Time limit of each wait of the persistent step (default 1 s; at most 60 s).  On
  * expiry the member's status becomes FHD_ERR_TIMEOUT and every block stops taking
  * work for that step.  hold_phase >= 0 (0 .. 23) is a failure-injection hook for

@@ -63,6 +63,7 @@ def lib():
         L.fhdref_max_acoustic_cfl.argtypes = [vp, pp, d, P(d)]
         L.fhdref_fill_boundary.argtypes = [vp, P(i), i, i, i]
         L.fhdref_wall_composition.argtypes = [i, P(d), P(d)]
+        L.fhdref_wall_state.argtypes = [i, P(d)]
         _lib = L
     return _lib
 
@@ -235,6 +236,14 @@ def wall_composition(p, side):
     x = (C.c_double * 8)()
     _chk(lib().fhdref_wall_composition(side, y, x), "SetupCWallStag")
     return list(y[:p.nspecies]), list(x[:p.nspecies])
+
+
+def wall_state(p, side):
+    """(t, p, rho) of wall side 2 d + hi after SetupCWallStag (reservoirs)."""
+    init(p)
+    out = (C.c_double * 3)()
+    _chk(lib().fhdref_wall_state(side, out), "SetupCWallStag")
+    return tuple(out)
 
 
 def state_from_reference(p, seed=0, amp=0.02, vel_amp=0.05):

@@ -153,6 +153,16 @@ int fhdref_wall_composition(int s, double* yk, double* xk) {
     });
 }
 
+// Reservoir state of side s after SetupCWallStag: t, p, rho.
+int fhdref_wall_state(int s, double* tpr) {
+    return guarded([&] {
+        const int d = s / 2, hi = s % 2;
+        tpr[0] = hi ? t_hi[d] : t_lo[d];
+        tpr[1] = hi ? p_hi[d] : p_lo[d];
+        tpr[2] = hi ? rho_hi[d] : rho_lo[d];
+    });
+}
+
 // Derived globals after GetHcGas, for the harness's consistency checks.
 int fhdref_globals(int* ns, int* nv, int* npv, int* ng, double* hcv_out, double* hcp_out, int* nreac) {
     return guarded([&] {

@@ -112,5 +112,5 @@ def test_batch_tile_entry_points_validate_without_gpu():
     assert lib.fhd_batch_num_tiles() == 3
     assert lib.fhd_batch_set_tile(None, 0) == capi.FHD_ERR_BAD_ARG
     assert lib.fhd_batch_autotune(None, 3, None, None) == capi.FHD_ERR_BAD_ARG
-    assert lib.fhd_batch_set_persistent(None, 1) == capi.FHD_ERR_BAD_ARG
+    assert lib.fhd_batch_set_persistent(None, 1, -1) == capi.FHD_ERR_BAD_ARG
     assert lib.fhd_batch_set_wait_limit(None, 1.0, -1) == capi.FHD_ERR_BAD_ARG

@@ -7,7 +7,9 @@ injected noise and with the in-kernel noise materialised for the reference.
 Cases: isothermal no-slip walls at two temperatures (a temperature gradient),
 slip adiabatic walls, concentration walls of a 4-species mixture, walls in two
 directions with different conditions (wall-wall edges), walls in all three
-directions (corners), and the single-gas form."""
+directions (corners), gravity along a wall normal, and reservoirs (bc_mass 3:
+ghost cells at a reservoir state, flow through the interface) alone, on all
+sides and beside a wall direction."""
 import pytest
 import torch
 
@@ -28,6 +30,7 @@ def ref():
 
 
 ISO = dict(vel=2, therm=2, mass=1)
+RES_Y = (0.22, 0.24, 0.26, 0.28)
 CASES = {
     "tempgrad_x": lambda: with_walls(argon((12, 9, 10), dx=8e-6, seed=101), x=dict(ISO, t=(263.0, 293.0))),
     "slip_adiabatic_z": lambda: with_walls(argon((9, 10, 12), dx=8e-6, seed=102), z=dict(vel=1, therm=1, mass=1)),
@@ -53,8 +56,26 @@ CASES = {
                rhobar=(0.25,) * 4, T_init=400.0, rho0=1.78e-3, seed=1),
         x=dict(vel=2, therm=2, mass=1, t=(280.8, 508.5)), y=dict(vel=1, therm=1, mass=1),
         z=dict(vel=1, therm=1, mass=1)),
+    # reservoirs (bc_mass 3): the boundary set-up of the reference's 3-D reservoir
+    # regression run (reservoirs on all six sides, no-slip, 390 / 410 K, 4 species
+    # of argon at a reservoir composition) on a smaller box; a reservoir pair
+    # facing each other across x with different compositions; a reservoir
+    # direction beside a wall direction
+    "reservoir_3d": lambda: with_walls(
+        Params(nspecies=4, n_cells=(8, 8, 8), prob_hi=(2.5e-5,) * 3, molmass=(39.948,) * 4,
+               diameter=(3.66e-8,) * 4, dof=(3.0,) * 4, e0=(0.0,) * 4, hcv=(-1.0,) * 4, hcp=(-1.0,) * 4,
+               rhobar=(0.25,) * 4, T_init=400.0, rho0=1.78e-3, seed=2),
+        **{ax: dict(vel=2, therm=2, mass=3, t=(390.0, 410.0), Yk=(RES_Y, RES_Y)) for ax in "xyz"}),
+    "reservoir_x": lambda: with_walls(
+        mixture4((12, 6, 6), dx=8e-6, seed=3),
+        x=dict(vel=2, therm=2, mass=3, t=(263.0, 283.0), Yk=((0.4, 0.2, 0.3, 0.1), (0.1, 0.3, 0.2, 0.4)))),
+    "reservoir_wall": lambda: with_walls(
+        argon((10, 9, 8), dx=8e-6, seed=4), x=dict(vel=2, therm=2, mass=3, t=(270.0, 276.0), Yk=((0.5, 0.5),) * 2,
+                                                   p=(1.0e6, 1.02e6)),
+        z=dict(vel=1, therm=1, mass=1)),
 }
-DT = {"tempgrad_3d": 1e-12}
+DT = {"tempgrad_3d": 1e-12, "reservoir_3d": 1e-12}
+RESERVOIRS = ["reservoir_3d", "reservoir_x", "reservoir_wall"]
 
 
 @pytest.mark.parametrize("name", list(CASES))
@@ -75,7 +96,7 @@ def test_wall_steps_equal_the_reference_injected_noise(ref, name):
     ctx.close()
 
 
-@pytest.mark.parametrize("name", ["tempgrad_x", "concentration_y", "box_xyz"])
+@pytest.mark.parametrize("name", ["tempgrad_x", "concentration_y", "box_xyz", "reservoir_x", "reservoir_wall"])
 def test_wall_steps_equal_the_reference_in_kernel_noise(ref, name):
     """In-kernel Philox noise (wall directions draw their ghost centres' own
     values), materialised by fhd_fill_step_noise for the reference."""
@@ -113,7 +134,7 @@ def test_wall_graph_replay_equals_single_steps(ref):
     assert ctx.status() == 0
 
 
-@pytest.mark.parametrize("name", ["concentration_y", "box_xyz", "slip_adiabatic_z"])
+@pytest.mark.parametrize("name", ["concentration_y", "box_xyz", "slip_adiabatic_z"] + RESERVOIRS)
 def test_set_bc_and_init_equal_the_reference(ref, name):
     """fhd_set_bc_stag against setBCStag on a state whose ghosts hold garbage, the
     wall compositions after SetupCWallStag, and the main_driver init."""
@@ -135,13 +156,18 @@ def test_set_bc_and_init_equal_the_reference(ref, name):
     eff = ctx.effective_params()
     for side in range(6):
         dd, hi = divmod(side, 2)
-        if (p.bc_mass_hi if hi else p.bc_mass_lo)[dd] != 2:
+        if (p.bc_mass_hi if hi else p.bc_mass_lo)[dd] not in (2, 3):
             continue
         yk, xk = ref.wall_composition(p, side)
         ey = (eff.bc_Yk_hi if hi else eff.bc_Yk_lo)[dd]
         ex = (eff.bc_Xk_hi if hi else eff.bc_Xk_lo)[dd]
         assert [ey[n] for n in range(p.nspecies)] == yk
         assert [ex[n] for n in range(p.nspecies)] == xk
+        if (p.bc_mass_hi if hi else p.bc_mass_lo)[dd] == 3:
+            t, pr, rho = ref.wall_state(p, side)
+            assert (eff.t_hi if hi else eff.t_lo)[dd] == t
+            assert (eff.p_hi if hi else eff.p_lo)[dd] == pr
+            assert (eff.rho_hi if hi else eff.rho_lo)[dd] == rho
     # main_driver init (InitConsVarStag, conversion, FillBoundary, setBCStag)
     gi = StagState(p, "cuda", aux=False)
     ctx.init_state(gi)

@@ -22,11 +22,13 @@ def test_wall_parameters_round_trip_through_the_deck():
     p = _walled()
     q = parse_inputs(p.to_inputs())
     for key in ("walls", "bc_vel_lo", "bc_vel_hi", "bc_mass_lo", "bc_mass_hi", "bc_therm_lo", "bc_therm_hi",
-                "t_lo", "t_hi"):
+                "t_lo", "t_hi", "p_lo", "p_hi", "rho_lo", "rho_hi"):
         assert tuple(getattr(q, key)) == tuple(getattr(p, key)) if key != "walls" else q.walls == 1, key
     assert q.bc_Yk_lo[2] == p.bc_Yk_lo[2] and q.bc_Yk_hi[2] == p.bc_Yk_hi[2]
     with pytest.raises(ValueError):
-        parse_inputs(p.to_inputs().replace("bc_mass_lo = 1 -1 2", "bc_mass_lo = 1 -1 3"))
+        parse_inputs(p.to_inputs().replace("bc_mass_lo = 1 -1 2", "bc_mass_lo = 1 -1 4"))
+    r = parse_inputs(p.to_inputs().replace("bc_mass_lo = 1 -1 2", "bc_mass_lo = 1 -1 3"))
+    assert r.bc_mass_lo == (1, -1, 3) and r.p_lo == p.p_lo and r.rho_lo == p.rho_lo
 
 
 def _create_rc(p, **raw):
@@ -42,8 +44,8 @@ def _create_rc(p, **raw):
 
 @pytest.mark.parametrize("change,code", [
     (dict(bc_vel_lo_1=2), "FHD_ERR_BAD_ARG"),            # one side periodic, the other a wall
-    (dict(bc_mass_lo_0=3), "FHD_ERR_UNSUPPORTED"),       # reservoir
-    (dict(bc_mass_hi_0=4), "FHD_ERR_UNSUPPORTED"),
+    (dict(bc_mass_lo_0=3), "FHD_ERR_BAD_ARG"),           # a reservoir without a composition
+    (dict(bc_mass_hi_0=4), "FHD_ERR_UNSUPPORTED"),       # the particle reservoir
     (dict(bc_vel_hi_0=3), "FHD_ERR_BAD_ARG"),
     (dict(bc_therm_lo_2=0), "FHD_ERR_BAD_ARG"),
     (dict(t_hi_0=0.0), "FHD_ERR_BAD_ARG"),               # isothermal wall without a temperature
@@ -130,3 +132,26 @@ def test_reference_single_wall_direction_is_mirror_symmetric(ref):
     rho = st.cu.valid(0)
     assert torch.allclose(rho, rho.flip(0), rtol=1e-13, atol=0)
     assert g == 2
+
+
+def test_reference_reservoir_step_holds_the_reservoir_state(ref):
+    """The reference's own step with reservoirs (bc_mass 3) across x: the ghost
+    cells hold the reservoir's temperature, pressure, density and composition
+    after every step, the interface faces carry flow (non-zero momentum), and
+    the reservoir pressure defaults to the initial state's."""
+    p = with_walls(mixture4((8, 6, 6), dx=8e-6), x=dict(vel=2, therm=2, mass=3, t=(263.0, 283.0),
+                                                         Yk=((0.4, 0.2, 0.3, 0.1), (0.1, 0.3, 0.2, 0.4))))
+    st = ref.state_from_reference(p, seed=6)
+    for s in range(2):
+        ref.rk3_step(st, ref.step_noise(p, 30 + s), stable_dt(p), s)
+    g = p.ngc
+    t, pr, rho = ref.wall_state(p, 0)
+    yk, _ = ref.wall_composition(p, 0)
+    assert t == 263.0 and pr == pytest.approx(p.rho0 * 8.314462175e7 * p.T_init * sum(
+        b / m for b, m in zip(p.rhobar, p.molmass)), rel=1e-12)
+    P = st.prim.arr
+    assert torch.all(P[4, g:-g, g:-g, :g] == t) and torch.all(P[5, g:-g, g:-g, :g] == pr)
+    assert torch.all(P[0, g:-g, g:-g, :g] == rho)
+    for n in range(p.nspecies):
+        assert torch.all(P[6 + n, g:-g, g:-g, :g] == yk[n])
+    assert st.cumom[0].valid(0)[..., 0].abs().max() > 0
