@@ -78,14 +78,32 @@ def make_params(args):
     from fhdex_b200.params import argon, argon_single, mixture4, no2_dimerization
     prec = 1 if args.precision == "mixed" else 0
     if args.gas == "no2":
-        return no2_dimerization(args.n, dx=args.dx, precision=prec, seed=args.seed)
-    if args.ns == 1:
-        return argon_single(args.n, dx=args.dx, precision=prec, seed=args.seed)
-    if args.ns == 2:
-        return argon(args.n, dx=args.dx, precision=prec, seed=args.seed)
-    if args.ns == 4:
-        return mixture4(args.n, dx=args.dx, precision=prec, seed=args.seed)
-    raise SystemExit("--ns must be 1 (single gas), 2 (argon parity form) or 4 (mixture)")
+        p = no2_dimerization(args.n, dx=args.dx, precision=prec, seed=args.seed)
+    elif args.ns == 1:
+        p = argon_single(args.n, dx=args.dx, precision=prec, seed=args.seed)
+    elif args.ns == 2:
+        p = argon(args.n, dx=args.dx, precision=prec, seed=args.seed)
+    elif args.ns == 4:
+        p = mixture4(args.n, dx=args.dx, precision=prec, seed=args.seed)
+    else:
+        raise SystemExit("--ns must be 1 (single gas), 2 (argon parity form) or 4 (mixture)")
+    return with_bench_walls(p, getattr(args, "walls", "none"))
+
+
+def with_bench_walls(p, kind):
+    """The boundary set-ups of the reference's regression runs on the bench box:
+    tempgrad (no-slip isothermal x walls at 0.9 / 1.1 T0, slip adiabatic y and z
+    walls, all impermeable) and reservoir (reservoirs of the initial composition
+    on all six sides, no-slip, at 0.95 / 1.05 T0)."""
+    from fhdex_b200.params import with_walls
+    if kind == "tempgrad":
+        slip = dict(vel=1, therm=1, mass=1)
+        return with_walls(p, x=dict(vel=2, therm=2, mass=1, t=(0.9 * p.T_init, 1.1 * p.T_init)), y=slip, z=slip)
+    if kind == "reservoir":
+        y = tuple(p.rhobar[:p.nspecies])
+        res = dict(vel=2, therm=2, mass=3, t=(0.95 * p.T_init, 1.05 * p.T_init), Yk=(y, y))
+        return with_walls(p, x=res, y=res, z=res)
+    return p
 
 
 class ClockSampler:
@@ -294,7 +312,7 @@ def config_dict(args, p, dt, tile):
     return {
         "workload": (("2 NO2 <-> N2O4 (chemistry source, CLE)" if p.nreaction > 0 else
                       {1: "argon (single gas)", 2: "argon (2 identical species)"}.get(p.nspecies, "4-species mixture"))
-                     + f" {p.n_cells[0]}^3, dx={p.dx[0]:g} cm, periodic, {args.precision}, in-kernel Philox noise"),
+                     + f" {p.n_cells[0]}^3, dx={p.dx[0]:g} cm, {'periodic' if args.walls == 'none' else args.walls + ' walls'}, {args.precision}, in-kernel Philox noise"),
         "n_cells": list(p.n_cells), "nspecies": p.nspecies, "precision": args.precision, "dt_s": dt,
         "noise": "philox-4x32-10 in kernel", "tile": tile,
         "l2": "inputs larger than L2 (state ~%.1f GB)" % (state_gb(p)),
@@ -788,6 +806,22 @@ def run_plot(args):
     clk = clocks.stop()
     ms = e0.elapsed_time(e1) / args.steps
     assert ctx.status() == 0
+    # plot_deltaY_dir: the same pack with Y_k minus its plane average in each direction
+    # (one thread per plane and species sums the plane in the reference's order)
+    from fhdex_b200.plotfile import DELTAY
+    deltay_ms = {}
+    for d, fl in enumerate(DELTAY):
+        o2 = pack(ctx, st, stats, flags | fl)
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        for _ in range(args.steps):
+            pack(ctx, st, stats, flags | fl, out=o2)
+        f1.record()
+        torch.cuda.synchronize()
+        deltay_ms["xyz"[d]] = f0.elapsed_time(f1) / args.steps
+        del o2
+    assert ctx.status() == 0
     ncomp = out.ncomp
     cells = p.n_cells[0] * p.n_cells[1] * p.n_cells[2]
     alg = 2 * 8 * ncomp * cells
@@ -808,6 +842,7 @@ def run_plot(args):
     ctx.close()
     print(json.dumps({"mode": "plot", "metric": "plotfile components packed/s (cells x components)",
                       "unit": "cell-components/s", "value": cells * ncomp / (ms / 1e3), "ms_per_pack": ms,
+                      "deltaY_ms_per_pack": deltay_ms,
                       "steps": args.steps, "warmup": args.warmup, "dtype": "f64",
                       "config": {"workload": f"WritePlotFileStag composition, all statistics flags, "
                                              f"{p.n_cells[0]}^3, {p.nspecies} species, {ncomp} components"},
@@ -987,6 +1022,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--ns", type=int, default=2)
+    ap.add_argument("--walls", default="none", choices=["none", "tempgrad", "reservoir"],
+                    help="step mode: physical boundaries of the reference's regression runs (FP64)")
     ap.add_argument("--gas", default="argon", choices=["argon", "no2"],
                     help="argon: --ns selects the species form; no2: 2 NO2 <-> N2O4 with the chemistry source")
     ap.add_argument("--dx", type=float, default=8e-6)

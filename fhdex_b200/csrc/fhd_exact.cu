@@ -322,16 +322,15 @@ int init_uniform(const fhd_fab& cu, int ns, double rho0, double rhoE, const doub
     return cuda_rc(cudaGetLastError());
 }
 
-int num_tiles() { return kNumStageBlocks + kNumZmTiles + kNumFaces3Tiles; }
+int num_tiles() { return kNumStageBlocks + kNumZmTiles; }
 
 // 0-4: the split stage (stress, face and update kernels) with the face kernel's
 // block size / register cap; 5-8: the fused z-marching stage kernel with its
-// block size and z-chunk depth; 9-10: the split stage with the three face
-// directions in one launch
+// block size and z-chunk depth
 const char* tile_name(int t) {
     static const char* names[] = {"b128-min4", "b256-min2", "b128-min6", "b128-min10", "b128-min8",
                                   "fused16x8-t128-z32", "fused16x8-t256-z32", "fused16x8-t256-z64",
-                                  "fused16x8-t384-z32", "faces3-b128-min8", "faces3-b128-min4"};
+                                  "fused16x8-t384-z32"};
     return (t >= 0 && t < num_tiles()) ? names[t] : "?";
 }
 

@@ -226,39 +226,6 @@ FHD_D void faces_point(const StageArgs<NS, R, NZ>& a, int q) {
 }
 
 // MINB = minimum resident blocks requested from the register allocator.
-// the three low faces of a point of [0, n]^3 in one thread (the x face when j < n
-// and k < n, and so on): one launch for all directions, so that a cell's fields,
-// read for its x face, are still in L1 for its y and z faces
-template <int NS, class R, int NZ, bool WL = false>
-FHD_D void faces3_point(const StageArgs<NS, R, NZ>& a, int q) {
-    const DevParams& P = a.P;
-    const int nx = P.n[0] + 1, ny = P.n[1] + 1;
-    const GlobalTaus<R> tg{a.ct, a.et};
-    const int i = q % nx, j = (q / nx) % ny, k = q / (nx * ny);
-    if (j < P.n[1] && k < P.n[2]) {
-        const FaceFlux<NS> f = face_flux<NS, R, NZ, 0, GlobalTaus<R>, WL>(P, a.F, a.noise, tg, i, j, k);
-#pragma unroll
-        for (int c = 0; c < 2 + NS; ++c) a.ff[0](i, j, k, c) = f.cons[c];
-    }
-    if (i < P.n[0] && k < P.n[2]) {
-        const FaceFlux<NS> f = face_flux<NS, R, NZ, 1, GlobalTaus<R>, WL>(P, a.F, a.noise, tg, i, j, k);
-#pragma unroll
-        for (int c = 0; c < 2 + NS; ++c) a.ff[1](i, j, k, c) = f.cons[c];
-    }
-    if (i < P.n[0] && j < P.n[1]) {
-        const FaceFlux<NS> f = face_flux<NS, R, NZ, 2, GlobalTaus<R>, WL>(P, a.F, a.noise, tg, i, j, k);
-#pragma unroll
-        for (int c = 0; c < 2 + NS; ++c) a.ff[2](i, j, k, c) = f.cons[c];
-    }
-}
-
-template <int NS, class R, int NZ, int BS, int MINB>
-static __global__ void __launch_bounds__(BS, MINB) k_faces3(StageArgs<NS, R, NZ> a) {
-    const int tot = (a.P.n[0] + 1) * (a.P.n[1] + 1) * (a.P.n[2] + 1);
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x)
-        faces3_point<NS, R, NZ>(a, q);
-}
-
 template <int NS, class R, int NZ, int D, int BS, int MINB, bool WL = false>
 static __global__ void __launch_bounds__(BS, MINB) k_faces(StageArgs<NS, R, NZ> a) {
     const int tot = faces_count<NS, R, NZ, D>(a);

@@ -142,14 +142,6 @@ constexpr int kZmThreads[] = {128, 256, 256, 384};
 constexpr int kZmChunks[] = {32, 32, 64, 32};
 constexpr int kNumZmTiles = 4;
 inline bool tile_is_fused(int t) { return t >= kNumStageBlocks && t < kNumStageBlocks + kNumZmTiles; }
-// the split stage with the three face directions in one launch (k_faces3): register
-// caps of 64 and 128 (8 and 4 resident blocks of 128)
-constexpr int kFaces3MinBlocks[] = {8, 4};
-constexpr int kNumFaces3Tiles = 2;
-inline int faces3_tile(int t) {
-    const int b = kNumStageBlocks + kNumZmTiles;
-    return (t >= b && t < b + kNumFaces3Tiles) ? t - b : -1;
-}
 
 template <int NS, class R, int NZ>
 StageArgs<NS, R, NZ> make_stage_args(const StageCall& c) {
@@ -185,14 +177,6 @@ int launch_stage_part_t(const StageCall& c, int part) {
     const int b = stage_block(c);
     if (part == 0) {
         k_taus<NS, R, NZ><<<grid_for((int64_t)(N[0] + 2) * (N[1] + 2) * (N[2] + 2), b), b, 0, c.stream>>>(a);
-    } else if (part == 1 && faces3_tile(c.tile) >= 0) {
-        const int64_t pts = (int64_t)(N[0] + 1) * (N[1] + 1) * (N[2] + 1);
-        if (faces3_tile(c.tile) == 0)
-            k_faces3<NS, R, NZ, 128, kFaces3MinBlocks[0]><<<resident_grid<k_faces3<NS, R, NZ, 128, kFaces3MinBlocks[0]>>(
-                pts, 128), 128, 0, c.stream>>>(a);
-        else
-            k_faces3<NS, R, NZ, 128, kFaces3MinBlocks[1]><<<resident_grid<k_faces3<NS, R, NZ, 128, kFaces3MinBlocks[1]>>(
-                pts, 128), 128, 0, c.stream>>>(a);
     } else if (part == 1) {
         const int t = (c.tile >= 0 && c.tile < kNumStageBlocks) ? c.tile : 0;
 #define FHD_FACES(BS, MINB)                                                                                      \
