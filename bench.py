@@ -312,7 +312,7 @@ def config_dict(args, p, dt, tile):
     return {
         "workload": (("2 NO2 <-> N2O4 (chemistry source, CLE)" if p.nreaction > 0 else
                       {1: "argon (single gas)", 2: "argon (2 identical species)"}.get(p.nspecies, "4-species mixture"))
-                     + f" {p.n_cells[0]}^3, dx={p.dx[0]:g} cm, {'periodic' if args.walls == 'none' else args.walls + ' walls'}, {args.precision}, in-kernel Philox noise"),
+                     + f" {p.n_cells[0]}^3, dx={p.dx[0]:g} cm, {'periodic' if getattr(args, 'walls', 'none') == 'none' else args.walls + ' walls'}, {args.precision}, in-kernel Philox noise"),
         "n_cells": list(p.n_cells), "nspecies": p.nspecies, "precision": args.precision, "dt_s": dt,
         "noise": "philox-4x32-10 in kernel", "tile": tile,
         "l2": "inputs larger than L2 (state ~%.1f GB)" % (state_gb(p)),
