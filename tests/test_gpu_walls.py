@@ -9,12 +9,13 @@ slip adiabatic walls, concentration walls of a 4-species mixture, walls in two
 directions with different conditions (wall-wall edges), walls in all three
 directions (corners), gravity along a wall normal, and reservoirs (bc_mass 3:
 ghost cells at a reservoir state, flow through the interface) alone, on all
-sides and beside a wall direction."""
+sides and beside a wall direction, and the chemistry source with concentration
+walls."""
 import pytest
 import torch
 
 from fhdex_b200.context import Context
-from fhdex_b200.params import Params, argon, mixture4, stable_dt, with_walls
+from fhdex_b200.params import Params, argon, isomerization, mixture4, no2_dimerization, stable_dt, with_walls
 from fhdex_b200.state import StagState, StepNoise
 from tests.helpers import compare_named
 
@@ -73,6 +74,11 @@ CASES = {
         argon((10, 9, 8), dx=8e-6, seed=4), x=dict(vel=2, therm=2, mass=3, t=(270.0, 276.0), Yk=((0.5, 0.5),) * 2,
                                                    p=(1.0e6, 1.02e6)),
         z=dict(vel=1, therm=1, mass=1)),
+    # the chemistry source of the compressible step (first-order A <-> B on the NO2 /
+    # N2O4 gas) with concentration walls in y
+    "chem_walls_y": lambda: with_walls(
+        isomerization(no2_dimerization((6, 8, 5), dx=8e-6, seed=5)),
+        y=dict(vel=2, therm=2, mass=2, t=(340.0, 360.0), Yk=((0.6, 0.4), (0.3, 0.7)))),
 }
 DT = {"tempgrad_3d": 1e-12, "reservoir_3d": 1e-12}
 RESERVOIRS = ["reservoir_3d", "reservoir_x", "reservoir_wall"]
@@ -96,7 +102,8 @@ def test_wall_steps_equal_the_reference_injected_noise(ref, name):
     ctx.close()
 
 
-@pytest.mark.parametrize("name", ["tempgrad_x", "concentration_y", "box_xyz", "reservoir_x", "reservoir_wall"])
+@pytest.mark.parametrize("name", ["tempgrad_x", "concentration_y", "box_xyz", "reservoir_x", "reservoir_wall",
+                                  "chem_walls_y"])
 def test_wall_steps_equal_the_reference_in_kernel_noise(ref, name):
     """In-kernel Philox noise (wall directions draw their ghost centres' own
     values), materialised by fhd_fill_step_noise for the reference."""
