@@ -26,7 +26,7 @@
 void InitializeChemistryNamespace();
 
 // The step only names TurbForcingComp in its signature (the forcing itself is
-// compiled in with -DTURB, which this build does not set); an empty object
+// compiled in with -DTURB, which oracle/Makefile does not set); an empty object
 // stands in for the one main_driver would construct.
 TurbForcingComp::TurbForcingComp() {}
 
