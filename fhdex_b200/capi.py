@@ -151,6 +151,7 @@ def _declare(lib):
         "fhd_fill_boundary": (i, [vp, fab]),
         "fhd_override_sync": (i, [vp, fab]),
         "fhd_set_bc_stag": (i, [vp, fab, fab, pfab, pfab]),
+        "fhd_set_reservoir_record": (i, [vp, vp, i]),
         "fhd_fill_random_normal": (i, [vp, fab, i, i, d, d, i, i, C.c_uint64]),
         "fhd_fill_random_uniform": (i, [vp, fab, i, i, i, i, C.c_uint64]),
         "fhd_rk3_steps_stag": (i, [vp, fab, pfab, fab, pfab, d, C.c_int64, i]),

@@ -124,6 +124,13 @@ class Context:
         mf = FabArr3(*[m.fab() for m in mom])
         check(self.lib.fhd_set_bc_stag(self._h, st.prim.fab(), cu.fab(), mf, st.vel_fabs()), "fhd_set_bc_stag")
 
+    def set_reservoir_record(self, buf=None, cap: int = 0):
+        """Test hook: record the particle reservoir's draws of the next steps into buf
+        (a CUDA float64 tensor of 3 x interface faces x cap values); None stops it."""
+        ptr = C.c_void_p(buf.data_ptr()) if buf is not None else None
+        check(self.lib.fhd_set_reservoir_record(self._h, ptr, cap if buf is not None else 0),
+              "fhd_set_reservoir_record")
+
     def override_sync(self, mf):
         self._stream()
         check(self.lib.fhd_override_sync(self._h, mf.fab()), "fhd_override_sync")

@@ -36,7 +36,11 @@ struct fhd_ctx {
     // physical boundaries: the periodic directions and the walls' values
     int per[3] = {1, 1, 1};
     bool walls = false;
-    bool reservoir = false;      // a side with bc_mass 3: the boundary passes run one by one
+    bool reservoir = false;      // a side with bc_mass 3 or 4: the boundary passes run one by one
+    bool res4 = false;           // a particle reservoir side (bc_mass 4)
+    ResBuffers res{};
+    double* res_rec = nullptr;   // test hook: the particle reservoir's draws
+    int res_cap = 0;
     WallParams wall{};
     // device mirrors for the host-buffer step
     double* hbuf = nullptr;
@@ -143,6 +147,34 @@ int ensure_scratch(fhd_ctx* c) {
     c->smc = make_fab(p, n, CELLN, 1, 3, FHD_F64); p += c1pts * 3;
     c->sme = make_fab(p, n, allnod, 0, 6, FHD_F64); p += npts * 6;
     c->csrc = srcpts ? make_fab(p, n, CELLN, 0, nvars, FHD_F64) : fhd_fab{};
+    return FHD_OK;
+}
+
+// the particle reservoir's faceflux_res / cumom_res (reference layout: the faces of
+// each direction, no ghosts; nvars comps / one comp)
+int ensure_res(fhd_ctx* c) {
+    if (!c->res4 || c->res.base) return FHD_OK;
+    const int* n = c->prm.n_cells;
+    const int nvars = 5 + c->prm.nspecies;
+    size_t tot = 0;
+    int64_t pts[3];
+    for (int d = 0; d < 3; ++d) {
+        c->res.sy[d] = n[0] + (d == 0);
+        c->res.sz[d] = c->res.sy[d] * (n[1] + (d == 1));
+        c->res.sn[d] = c->res.sz[d] * (n[2] + (d == 2));
+        pts[d] = c->res.sn[d];
+        tot += (size_t)pts[d] * (nvars + 1);
+    }
+    void* b = nullptr;
+    if (cudaMalloc(&b, tot * sizeof(double)) != cudaSuccess) { cudaGetLastError(); return FHD_ERR_OOM; }
+    c->res.base = b;
+    c->res.bytes = tot * sizeof(double);
+    double* q = static_cast<double*>(b);
+    for (int d = 0; d < 3; ++d) { c->res.f[d] = q; q += pts[d] * nvars; }
+    for (int d = 0; d < 3; ++d) { c->res.m[d] = q; q += pts[d]; }
+    // particle masses molmass / avogadro (reservoirStag.cpp:24-27)
+    const double navo = c->prm.avogadro > 0 ? c->prm.avogadro : c->prm.Runiv / c->prm.k_B;
+    for (int i = 0; i < MAXS; ++i) c->res.mass[i] = i < c->prm.nspecies ? c->prm.molmass[i] / navo : 0.0;
     return FHD_OK;
 }
 
@@ -272,12 +304,12 @@ int setup_walls(const fhd_params& p, int per[3], WallParams& W) {
             const int v = h ? p.bc_vel_hi[d] : p.bc_vel_lo[d];
             const int m = h ? p.bc_mass_hi[d] : p.bc_mass_lo[d];
             const int t = h ? p.bc_therm_hi[d] : p.bc_therm_lo[d];
-            if (m >= 4) return FHD_ERR_UNSUPPORTED;
-            if ((v != 1 && v != 2) || (m != 1 && m != 2 && m != 3) || (t != 1 && t != 2)) return FHD_ERR_BAD_ARG;
+            if (m >= 5) return FHD_ERR_UNSUPPORTED;
+            if ((v != 1 && v != 2) || (m < 1 || m > 4) || (t != 1 && t != 2)) return FHD_ERR_BAD_ARG;
             W.t[s] = h ? p.t_hi[d] : p.t_lo[d];
             W.p[s] = h ? p.p_hi[d] : p.p_lo[d];
             W.rho[s] = h ? p.rho_hi[d] : p.rho_lo[d];
-            if (t == 2 && m != 3 && !(W.t[s] > 0)) return FHD_ERR_BAD_ARG;
+            if (t == 2 && m < 3 && !(W.t[s] > 0)) return FHD_ERR_BAD_ARG;
             const double* Yk = h ? p.bc_Yk_hi[d] : p.bc_Yk_lo[d];
             const double* Xk = h ? p.bc_Xk_hi[d] : p.bc_Xk_lo[d];
             for (int n = 0; n < ns; ++n) {
@@ -302,7 +334,7 @@ int setup_walls(const fhd_params& p, int per[3], WallParams& W) {
             } else {
                 return FHD_ERR_BAD_ARG;
             }
-            if (m != 3) continue;
+            if (m < 3) continue;
             // reservoir state (boundaryStag.cpp:39-60): the pressure defaults to the
             // initial state's (GetPressureGas of rhobar, rho0, T_init); then the
             // density from p, t and Y (GetDensity), or, when a density is given and
@@ -383,8 +415,10 @@ int fhd_create(fhd_ctx** out, const fhd_params* params, int device) {
     for (int d = 0; d < 3; ++d) c->per[d] = per[d];
     c->walls = walls;
     c->wall = wall;
-    for (int d = 0; d < 3; ++d)
-        if (!per[d] && (p.bc_mass_lo[d] == 3 || p.bc_mass_hi[d] == 3)) c->reservoir = true;
+    for (int d = 0; d < 3; ++d) {
+        if (!per[d] && (p.bc_mass_lo[d] >= 3 || p.bc_mass_hi[d] >= 3)) c->reservoir = true;
+        if (!per[d] && (p.bc_mass_lo[d] == 4 || p.bc_mass_hi[d] == 4)) c->res4 = true;
+    }
     // GetHcGas, compressible_functions.cpp:91-100
     for (int i = 0; i < p.nspecies; ++i) {
         if (c->prm.hcv[i] < 0.) c->prm.hcv[i] = 0.5 * p.dof[i] * p.Runiv / p.molmass[i];
@@ -410,6 +444,7 @@ int fhd_destroy(fhd_ctx* c) {
     cudaStreamSynchronize(c->stream);
     if (c->scratch) cudaFree(c->scratch);
     if (c->coef) cudaFree(c->coef);
+    if (c->res.base) cudaFree(c->res.base);
     if (c->hbuf) cudaFree(c->hbuf);
     for (auto& e : c->evs) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
     if (c->d_status) cudaFree(c->d_status);
@@ -592,6 +627,19 @@ int fhd_set_bc_stag(fhd_ctx* c, fhd_fab prim, fhd_fab cu, const fhd_fab cumom[3]
     int rc = bc_mom(P, cumom, vel, c->stream);
     if (!rc) rc = exact_bc_prim(P, c->wall, prim, cu, cumom, c->stream);
     return rc;
+}
+
+int fhd_set_reservoir_record(fhd_ctx* c, void* buf, int cap) {
+    if (!c || cap < 0 || (buf && cap == 0)) return FHD_ERR_BAD_ARG;
+    c->res_rec = static_cast<double*>(buf);
+    c->res_cap = buf ? cap : 0;
+    // the captured step graph embeds the hook
+    if (c->sgexec) cudaGraphExecDestroy(c->sgexec);
+    if (c->sgraph) cudaGraphDestroy(c->sgraph);
+    c->sgexec = nullptr;
+    c->sgraph = nullptr;
+    c->skey.clear();
+    return FHD_OK;
 }
 
 int fhd_override_sync(fhd_ctx* c, fhd_fab f) {
@@ -874,6 +922,13 @@ static int walls_step_launches(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd
             if (!rc && chem)
                 rc = chem_launch(sc.P, cp, prim, sc.src, cmode == CN_AB ? &injected->chem[0] : nullptr,
                                  cmode == CN_AB ? &injected->chem[1] : nullptr, cmode, w[s], c->stream);
+            // the particle reservoir's fluxes from the stage's input (ComputeFluxMomReservoir
+            // with dt, dt / 4, 2 dt / 3: timeStepStag.cpp:341-350, 667-676, 1000-1009)
+            if (!rc && c->res4) {
+                const double dts = s == 0 ? dt : (s == 1 ? 0.25 * dt : (2.0 / 3.0) * dt);
+                rc = exact_reservoir(sc.P, c->res, *ins[s], prim, vel, dts, s, c->res_rec, c->res_cap, c->d_status,
+                                     c->stream);
+            }
         }
         if (rc) return rc;
         if (s == 2 && aux_flux) {
@@ -881,11 +936,14 @@ static int walls_step_launches(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd
             for (int e = 0; e < 6; ++e) sc.ef[e] = edgeflux[e];
             ProfScope ps(c, 6);
             rc = exact_aux_fluxes(sc);
+            if (!rc && c->res4) rc = exact_res_reset(sc.P, c->res, faceflux, 0, 4, 5, edgeflux, -1, c->stream);
             if (rc) return rc;
         }
         for (int part = 0; part < 3 && !rc; ++part) {
             ProfScope ps(c, 1 + part);
-            rc = exact_walls_part(sc, part);
+            // ResetReservoirFluxes between the fluxes and the update
+            if (part == 2 && c->res4) rc = exact_res_reset(sc.P, c->res, c->sff, 0, 1, 2, &c->sme, 0, c->stream);
+            if (!rc) rc = exact_walls_part(sc, part);
         }
         if (rc) return rc;
         {
@@ -896,6 +954,8 @@ static int walls_step_launches(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd
             // enters the interface velocity)
             if (c->reservoir) rc = exact_bc_seq(sc.P, c->wall, prim, *outs[s], outsm[s], vel, false, c->stream);
             else rc = bc_mom(sc.P, outsm[s], vel, c->stream);
+            // ResetReservoirMom (timeStepStag.cpp:538-540, 871-873, 1212-1214)
+            if (!rc && c->res4) rc = exact_res_mom(sc.P, c->res, outsm[s], c->stream);
             GhostReq g[4] = {{*outs[s], 0, nvars}, {outsm[s][0], 0, 1}, {outsm[s][1], 0, 1}, {outsm[s][2], 0, 1}};
             if (!rc) rc = fill_ghosts(g, 4, c->prm.n_cells, c->stream, c->per, 0);
         }
@@ -1073,6 +1133,8 @@ int fhd_rk3_step_stag(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim
     if (rc) return rc;
     rc = ensure_coef(c, mixed ? FHD_F32 : FHD_F64);
     if (rc) return rc;
+    rc = ensure_res(c);
+    if (rc) return rc;
     return step_launches(c, cu, mom, prim, vel, source, eta, zeta, kappa, chi, D, faceflux, edgeflux, cenflux, injected,
                          dt, step, aux_coef, aux_flux, nullptr);
 }
@@ -1092,6 +1154,8 @@ int fhd_rk3_steps_stag(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab pri
     int rc = ensure_scratch(c);
     if (rc) return rc;
     rc = ensure_coef(c, mixed ? FHD_F32 : FHD_F64);
+    if (rc) return rc;
+    rc = ensure_res(c);
     if (rc) return rc;
     if (!c->d_step && cudaMalloc(&c->d_step, sizeof(uint64_t)) != cudaSuccess) {
         cudaGetLastError();

@@ -13,6 +13,8 @@ int mixed_stage_ns1(const StageCall&, int);
 int exact_transport_ns1(const DevParams&, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, int*, cudaStream_t);
 int exact_convert_ns1(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const fhd_fab*, int*, cudaStream_t);
 int exact_walls_ns1(const StageCall&, int);
+int exact_reservoir_ns1(const ResArgs&, cudaStream_t);
+int exact_res_reset_ns1(const ResResetArgs&, cudaStream_t);
 int exact_bc_prim_ns1(const DevParams&, const WallParams&, fhd_fab, fhd_fab, const fhd_fab*, cudaStream_t);
 int exact_bc_seq_ns1(const DevParams&, const WallParams&, fhd_fab, fhd_fab, const fhd_fab*, const fhd_fab*, int,
                      cudaStream_t);
@@ -24,6 +26,8 @@ int mixed_stage_ns2(const StageCall&, int);
 int exact_transport_ns2(const DevParams&, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, int*, cudaStream_t);
 int exact_convert_ns2(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const fhd_fab*, int*, cudaStream_t);
 int exact_walls_ns2(const StageCall&, int);
+int exact_reservoir_ns2(const ResArgs&, cudaStream_t);
+int exact_res_reset_ns2(const ResResetArgs&, cudaStream_t);
 int exact_bc_prim_ns2(const DevParams&, const WallParams&, fhd_fab, fhd_fab, const fhd_fab*, cudaStream_t);
 int exact_bc_seq_ns2(const DevParams&, const WallParams&, fhd_fab, fhd_fab, const fhd_fab*, const fhd_fab*, int,
                      cudaStream_t);
@@ -35,6 +39,8 @@ int mixed_stage_ns3(const StageCall&, int);
 int exact_transport_ns3(const DevParams&, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, int*, cudaStream_t);
 int exact_convert_ns3(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const fhd_fab*, int*, cudaStream_t);
 int exact_walls_ns3(const StageCall&, int);
+int exact_reservoir_ns3(const ResArgs&, cudaStream_t);
+int exact_res_reset_ns3(const ResResetArgs&, cudaStream_t);
 int exact_bc_prim_ns3(const DevParams&, const WallParams&, fhd_fab, fhd_fab, const fhd_fab*, cudaStream_t);
 int exact_bc_seq_ns3(const DevParams&, const WallParams&, fhd_fab, fhd_fab, const fhd_fab*, const fhd_fab*, int,
                      cudaStream_t);
@@ -46,6 +52,8 @@ int mixed_stage_ns4(const StageCall&, int);
 int exact_transport_ns4(const DevParams&, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, fhd_fab, int*, cudaStream_t);
 int exact_convert_ns4(const DevParams&, fhd_fab, const fhd_fab*, fhd_fab, const fhd_fab*, int*, cudaStream_t);
 int exact_walls_ns4(const StageCall&, int);
+int exact_reservoir_ns4(const ResArgs&, cudaStream_t);
+int exact_res_reset_ns4(const ResResetArgs&, cudaStream_t);
 int exact_bc_prim_ns4(const DevParams&, const WallParams&, fhd_fab, fhd_fab, const fhd_fab*, cudaStream_t);
 int exact_bc_seq_ns4(const DevParams&, const WallParams&, fhd_fab, fhd_fab, const fhd_fab*, const fhd_fab*, int,
                      cudaStream_t);
@@ -115,6 +123,99 @@ int exact_bc_prim(const DevParams& P, const WallParams& W, fhd_fab prim, fhd_fab
 int exact_bc_seq(const DevParams& P, const WallParams& W, fhd_fab prim, fhd_fab cons, const fhd_fab mom[3],
                  const fhd_fab vel[3], bool rre, cudaStream_t s) {
     FHD_DISPATCH(P.ns, exact_bc_seq_ns, P, W, prim, cons, mom, vel, rre ? 1 : 0, s)
+}
+
+// the particle reservoir (bc_mass 4) of one stage: its fluxes and momenta into res,
+// the resets of the stage's flux scratch / the caller's flux fabs / the momenta
+int exact_reservoir(const DevParams& P, const ResBuffers& r, const fhd_fab& cons, const fhd_fab& prim,
+                    const fhd_fab vel[3], double dt, int stage, double* rec, int rec_cap, int* status,
+                    cudaStream_t s) {
+    ResArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.P = P;
+    a.cons0 = view<const double>(cons);
+    a.prim0 = view<const double>(prim);
+    for (int d = 0; d < 3; ++d) {
+        a.vel[d] = view<const double>(vel[d]);
+        a.fres[d] = r.f[d];
+        a.mres[d] = r.m[d];
+        a.fsy[d] = r.sy[d];
+        a.fsz[d] = r.sz[d];
+        a.fsn[d] = r.sn[d];
+    }
+    for (int n = 0; n < MAXS; ++n) a.mass[n] = r.mass[n];
+    a.dt = dt;
+    a.stage = stage;
+    a.nsides = 0;
+    a.face_pref[0] = 0;
+    for (int side = 0; side < 6; ++side) {
+        if (P.bc_mass[side] != 4) continue;
+        const int d = side >> 1, e1 = d == 0 ? 1 : 0, e2 = d == 2 ? 1 : 2;
+        a.sides[a.nsides] = side;
+        a.face_pref[a.nsides + 1] = a.face_pref[a.nsides] + (int64_t)P.n[e1] * P.n[e2];
+        ++a.nsides;
+    }
+    a.rec = rec;
+    a.rec_cap = rec_cap;
+    a.status = status;
+    if (cudaMemsetAsync(r.base, 0, r.bytes, s) != cudaSuccess) return FHD_ERR_CUDA;
+    FHD_DISPATCH(P.ns, exact_reservoir_ns, a, s)
+}
+
+int exact_res_reset(const DevParams& P, const ResBuffers& r, const fhd_fab* ff, int fc_rho, int fc_rhoE, int fc_Y,
+                    const fhd_fab* ef, int ef_comp_base, cudaStream_t s) {
+    for (int side = 0; side < 6; ++side) {
+        if (P.bc_mass[side] != 4) continue;
+        ResResetArgs a;
+        std::memset(&a, 0, sizeof(a));
+        a.P = P;
+        for (int d = 0; d < 3; ++d) {
+            a.fres[d] = r.f[d];
+            a.fsy[d] = r.sy[d];
+            a.fsz[d] = r.sz[d];
+            a.fsn[d] = r.sn[d];
+            if (ff) a.ff[d] = view<double>(ff[d]);
+        }
+        a.fc_rho = fc_rho;
+        a.fc_rhoE = fc_rhoE;
+        a.fc_Y = fc_Y;
+        // ef: six one-component fabs, or (ef_comp_base >= 0) one six-component fab
+        for (int e = 0; e < 6; ++e) {
+            if (!ef) continue;
+            a.ef[e] = ef_comp_base >= 0 ? view<double>(ef[0], ef_comp_base + e) : view<double>(ef[e]);
+        }
+        a.side = side;
+        int rc;
+        switch (P.ns) {
+            case 1: rc = exact_res_reset_ns1(a, s); break;
+            case 2: rc = exact_res_reset_ns2(a, s); break;
+            case 3: rc = exact_res_reset_ns3(a, s); break;
+            case 4: rc = exact_res_reset_ns4(a, s); break;
+            default: rc = FHD_ERR_UNSUPPORTED;
+        }
+        if (rc) return rc;
+    }
+    return FHD_OK;
+}
+
+int exact_res_mom(const DevParams& P, const ResBuffers& r, const fhd_fab mom[3], cudaStream_t s) {
+    for (int side = 0; side < 6; ++side) {
+        if (P.bc_mass[side] != 4) continue;
+        ResMomArgs a;
+        std::memset(&a, 0, sizeof(a));
+        a.P = P;
+        for (int d = 0; d < 3; ++d) {
+            a.mres[d] = r.m[d];
+            a.fsy[d] = r.sy[d];
+            a.fsz[d] = r.sz[d];
+            a.mom[d] = view<double>(mom[d]);
+        }
+        a.side = side;
+        const int d = side >> 1, e1 = d == 0 ? 1 : 0, e2 = d == 2 ? 1 : 2;
+        k_res_mom<<<grid_for((int64_t)P.n[e1] * P.n[e2], 128), 128, 0, s>>>(a);
+        if (cudaGetLastError() != cudaSuccess) return FHD_ERR_CUDA;
+    }
+    return FHD_OK;
 }
 
 int bc_mom(const DevParams& P, const fhd_fab mom[3], const fhd_fab vel[3], cudaStream_t s) {

@@ -368,8 +368,9 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
             vsh += R(0.25) * ((vb1h + vb1l) * eb1.s + (vb0h + vb0l) * eb0.s);
         }
         vshear = vsh;
-        // StochFluxStag: velocity walls scale the stochastic shear heating
-        if (WL && ws >= 0 && (P.bc_vel[wside] == 1 || P.bc_vel[wside] == 2))
+        // StochFluxStag: velocity walls scale the stochastic shear heating (a
+        // reservoir side keeps the factor 1)
+        if (WL && ws >= 0 && (P.bc_vel[wside] == 1 || P.bc_vel[wside] == 2) && P.bc_mass[wside] < 3)
             vshear *= R(stoch_factor(P, P.bc_vel[wside]));
     }
     vdiag -= R(0.5) * un * (tl.d[D] + th.d[D]);
@@ -401,8 +402,9 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
         nz.template face_all<NS + 1>(P, D, i, j, k, wf);
         const R fw0 = dsqrt(R(P.k_B) * kp * R(P.volinv) * R(P.dtinv));
         heat = fw0 * R(wf[0]);
-        // StochFluxStag: thermal walls scale the stochastic heat flux
-        if (WL && ws >= 0 && (P.bc_therm[wside] == 1 || P.bc_therm[wside] == 2))
+        // StochFluxStag: thermal walls scale the stochastic heat flux (a reservoir
+        // side keeps the factor 1)
+        if (WL && ws >= 0 && (P.bc_therm[wside] == 1 || P.bc_therm[wside] == 2) && P.bc_mass[wside] < 3)
             heat *= R(stoch_factor(P, P.bc_therm[wside]));
         // species noise, Soret: mixtures only (a single gas has no species flux)
         if constexpr (NS > 1) {
@@ -691,15 +693,22 @@ FHD_D double edge_total_w(const DevParams& P, const Taus<R>& t, double adv, int 
 }
 
 // centre momentum flux in direction d at a cell (fluxStag.cpp:799-803, 1444-1448, 1848-1866).
-// WL: a ghost cell beyond a reservoir side of direction d carries no stochastic or
-// diffusive part (BCWallReservoirFluxStag, boundaryStag.cpp:482-577).
+// WL: the stochastic and diffusive part of a ghost cell beyond a reservoir side of
+// direction d is 0 (bc_mass 3) or, given as `inner` (bc_mass 4), that of the cell
+// inside it (BCWallReservoirFluxStag, boundaryStag.cpp:482-577).
 template <int NS, class R, bool WL = false>
-FHD_D double cen_total(const DevParams& P, const Fields<NS, R>& F, const CellTaus<R>& t, int d, int i, int j, int k) {
+FHD_D double cen_total(const DevParams& P, const Fields<NS, R>& F, const CellTaus<R>& t, int d, int i, int j, int k,
+                       const CellTaus<R>* inner = nullptr) {
     double v = (double)t.s[d];
     v -= (double)t.d[d];
     if (WL) {
         const int x = d == 0 ? i : (d == 1 ? j : k);
-        if ((x < 0 && P.bc_mass[2 * d] == 3) || (x > P.n[d] - 1 && P.bc_mass[2 * d + 1] == 3)) v = 0.0;
+        const int side = x < 0 ? 2 * d : (x > P.n[d] - 1 ? 2 * d + 1 : -1);
+        if (side >= 0 && P.bc_mass[side] == 3) v = 0.0;
+        if (side >= 0 && P.bc_mass[side] == 4 && inner) {
+            v = (double)inner->s[d];
+            v -= (double)inner->d[d];
+        }
     }
     if (P.advection_type >= 0) {
         const Arr4<const double>& m = F.mom[d];

@@ -154,6 +154,24 @@ int exact_walls_part(const StageCall& c, int part);
 int exact_bc_prim(const DevParams& P, const WallParams& W, fhd_fab prim, fhd_fab cons, const fhd_fab mom[3],
                   cudaStream_t s);
 int bc_mom(const DevParams& P, const fhd_fab mom[3], const fhd_fab vel[3], cudaStream_t s);
+// the particle reservoir's buffers: faceflux_res[d] (nvars comps) and cumom_res[d] in
+// the reference's layout (faces of direction d, no ghost cells), particle masses
+struct ResBuffers {
+    void* base;
+    size_t bytes;
+    double* f[3];
+    double* m[3];
+    int sy[3], sz[3], sn[3];
+    double mass[MAXS];
+};
+int exact_reservoir(const DevParams& P, const ResBuffers& r, const fhd_fab& cons, const fhd_fab& prim,
+                    const fhd_fab vel[3], double dt, int stage, double* rec, int rec_cap, int* status,
+                    cudaStream_t s);
+// ff: three face-flux fabs with the conserved comps 0 / 4 / 5.. at fc_rho / fc_rhoE / fc_Y;
+// ef: six edge-flux fabs, or one fab of six comps from ef_comp_base (-1: six fabs)
+int exact_res_reset(const DevParams& P, const ResBuffers& r, const fhd_fab* ff, int fc_rho, int fc_rhoE, int fc_Y,
+                    const fhd_fab* ef, int ef_comp_base, cudaStream_t s);
+int exact_res_mom(const DevParams& P, const ResBuffers& r, const fhd_fab mom[3], cudaStream_t s);
 // the reference's boundary passes one by one (boxes with reservoirs): setBCStag
 // (rre) or the passes before the conversion
 int exact_bc_seq(const DevParams& P, const WallParams& W, fhd_fab prim, fhd_fab cons, const fhd_fab mom[3],

@@ -89,6 +89,9 @@ int FHD_CAT(exact_bc_prim_ns, FHD_NS)(const DevParams& P, const WallParams& W, f
     return launch_bc_prim<FHD_NS>(P, W, prim, cons, mom, s);
 }
 
+int FHD_CAT(exact_reservoir_ns, FHD_NS)(const ResArgs& a, cudaStream_t s) { return launch_reservoir<FHD_NS>(a, s); }
+int FHD_CAT(exact_res_reset_ns, FHD_NS)(const ResResetArgs& a, cudaStream_t s) { return launch_res_reset<FHD_NS>(a, s); }
+
 int FHD_CAT(exact_bc_seq_ns, FHD_NS)(const DevParams& P, const WallParams& W, fhd_fab prim, fhd_fab cons,
                                      const fhd_fab* mom, const fhd_fab* vel, int rre, cudaStream_t s) {
     return launch_bc_seq<FHD_NS>(P, W, prim, cons, mom, vel, rre != 0, s);

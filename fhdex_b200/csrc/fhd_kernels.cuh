@@ -100,6 +100,25 @@ static __global__ void __launch_bounds__(128, cellprep_min_blocks<NS, R>()) k_ce
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += gridDim.x * blockDim.x) cellprep_point(a, q);
 }
 
+// centre momentum flux with the particle reservoir's rule: a ghost cell beyond a
+// bc_mass 4 side of direction d takes the stochastic and diffusive part of the cell
+// inside it (recomputed here with that cell's own noise)
+template <int NS, class R, int NZ, bool WL>
+FHD_D double cen_total_res(const DevParams& P, const Fields<NS, R>& F, const Noise<NZ>& nz, const CellTaus<R>& t,
+                           int d, int i, int j, int k) {
+    if (WL) {
+        const int x = d == 0 ? i : (d == 1 ? j : k);
+        const int side = x < 0 ? 2 * d : (x > P.n[d] - 1 ? 2 * d + 1 : -1);
+        if (side >= 0 && P.bc_mass[side] == 4) {
+            int c[3] = {i, j, k};
+            c[d] += (side & 1) ? -1 : 1;
+            const CellTaus<R> tin = cell_taus<NS, R, NZ>(P, F, nz, c[0], c[1], c[2]);
+            return cen_total<NS, R, WL>(P, F, t, d, i, j, k, &tin);
+        }
+    }
+    return cen_total<NS, R, WL>(P, F, t, d, i, j, k);
+}
+
 // ===================================================================================
 // stage pipeline: k_taus -> k_faces<D> (x3) -> k_update
 // ===================================================================================
@@ -147,7 +166,7 @@ FHD_D void taus_point(const StageArgs<NS, R, NZ>& a, int q) {
         for (int d = 0; d < 3; ++d) {
             a.ct(i, j, k, d) = t.s[d];
             a.ct(i, j, k, 3 + d) = t.d[d];
-            a.mc(i, j, k, d) = cen_total<NS, R, WL>(P, a.F, t, d, i, j, k);
+            a.mc(i, j, k, d) = cen_total_res<NS, R, NZ, WL>(P, a.F, a.noise, t, d, i, j, k);
         }
         if (!edges) return;
         if (NZ != NZ_OFF) a.noise.xy_xz_edges(P, i, j, k, we[0], we[1]);
@@ -619,7 +638,7 @@ static __global__ void __launch_bounds__(128) k_aux_edges_cen(AuxArgs<NS, R, NZ>
                       k = (int)(r / ((int64_t)(N[0] + 2) * (N[1] + 2))) - 1;
             const CellTaus<R> t = cell_taus<NS, R, NZ>(P, a.F, a.noise, i, j, k);
 #pragma unroll
-            for (int d = 0; d < 3; ++d) a.cf[d](i, j, k) = cen_total<NS, R, WL>(P, a.F, t, d, i, j, k);
+            for (int d = 0; d < 3; ++d) a.cf[d](i, j, k) = cen_total_res<NS, R, NZ, WL>(P, a.F, a.noise, t, d, i, j, k);
         }
     }
 }

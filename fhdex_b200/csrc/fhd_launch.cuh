@@ -360,6 +360,24 @@ int launch_bc_seq(const DevParams& P, const WallParams& W, const fhd_fab& prim, 
     return rc;
 }
 
+// the particle reservoir's fluxes and momenta (k_reservoir), the flux reset of one
+// reservoir side (k_res_reset)
+template <int NS>
+int launch_reservoir(const ResArgs& a, cudaStream_t s) {
+    if (a.face_pref[a.nsides] == 0) return FHD_OK;
+    k_reservoir<NS><<<grid_for(a.face_pref[a.nsides], 128), 128, 0, s>>>(a);
+    return cuda_rc(cudaGetLastError());
+}
+
+template <int NS>
+int launch_res_reset(const ResResetArgs& a, cudaStream_t s) {
+    const int d = a.side >> 1, e1 = d == 0 ? 1 : 0, e2 = d == 2 ? 1 : 2;
+    const int64_t n = (int64_t)a.P.n[e1] * a.P.n[e2] + (int64_t)(a.P.n[e1] + 1) * a.P.n[e2] +
+                      (int64_t)a.P.n[e1] * (a.P.n[e2] + 1);
+    k_res_reset<NS><<<grid_for(n, 128), 128, 0, s>>>(a);
+    return cuda_rc(cudaGetLastError());
+}
+
 // part: 0 stresses, 1 face fluxes, 2 update, 3 the fused kernel (all three)
 template <int NS, class R>
 int launch_stage_part(const StageCall& c, int part) {

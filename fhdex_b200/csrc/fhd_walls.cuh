@@ -18,6 +18,7 @@
 // writes.  Factors (slip 1, no-slip 0) multiply in the passes' order.
 #pragma once
 #include "fhd_device.cuh"
+#include "philox.cuh"
 
 namespace fhd {
 
@@ -212,8 +213,8 @@ static __global__ void __launch_bounds__(128) k_bc_prim(BcPrimArgs<NS> a) {
 }
 
 // ---- one pass of the reference's boundary routines ---------------------------------
-// With reservoirs (bc_mass 3: ghost cells held at the reservoir's state, flow through
-// the interface) the reference's passes read values that earlier passes of the same
+// With reservoirs (bc_mass 3 / 4: ghost cells held at the reservoir's state, flow
+// through the interface) the reference's passes read values that earlier passes of the same
 // call left at ghost corners, some of them through the density in cons, so they run
 // here one launch per pass, in the reference's order, each over the slab of the grown
 // box beyond one side:
@@ -281,10 +282,15 @@ static __global__ void __launch_bounds__(128) k_bc_pass(BcPassArgs<NS> a) {
             gi[d] = f - 1;        // the cell before it
             if (bm >= 3) {
                 if (ghost) {
-                    a.vel(i, j, k) = -2 * a.mom(fi[0], fi[1], fi[2]) /
-                                     (a.cons(fi[0], fi[1], fi[2], 0) + a.cons(gi[0], gi[1], gi[2], 0));
-                    a.mom(i, j, k) = -1 * a.mom(fi[0], fi[1], fi[2]);
-                } else if (p[d] == f) {
+                    if (bm == 3) {
+                        a.vel(i, j, k) = -2 * a.mom(fi[0], fi[1], fi[2]) /
+                                         (a.cons(fi[0], fi[1], fi[2], 0) + a.cons(gi[0], gi[1], gi[2], 0));
+                        a.mom(i, j, k) = -1 * a.mom(fi[0], fi[1], fi[2]);
+                    } else if (bm == 4) {
+                        a.vel(i, j, k) = -1 * a.vel(fi[0], fi[1], fi[2]);
+                        a.mom(i, j, k) = -1 * a.mom(fi[0], fi[1], fi[2]);
+                    }
+                } else if (p[d] == f && bm == 3) {
                     a.vel(i, j, k) = 2 * a.mom(i, j, k) / (a.cons(fi[0], fi[1], fi[2], 0) + a.cons(gi[0], gi[1], gi[2], 0));
                 }
             } else if (bv == 1 || bv == 2) {
@@ -338,6 +344,339 @@ static __global__ void __launch_bounds__(128) k_bc_pass(BcPassArgs<NS> a) {
                 a.cons(i, j, k, 4) = rho * intenergy + kin;
             }
         }
+    }
+}
+
+// ---- the particle reservoir (bc_mass 4): ComputeFluxMomReservoir ---------------------
+// (reservoirStag.cpp:11-869, reservoirStag_K.H).  Per face of a reservoir interface two
+// Poisson processes of particles crossing in a stage's dt: from the reservoir (the ghost
+// cell's temperature and rho Y, at rest) and to it (the inside cell's temperature, rho Y
+// and velocity), each particle with a random normal velocity (rejection sampling of the
+// flux-weighted Maxwellian) and two tangential ones; their mass, species mass, energy and
+// momenta become the face's flux (faceflux_res) and normal momentum (cumom_res).  The
+// random numbers come from Philox per (face, stage, side, draw); a test can record every
+// draw to replay them into the reference.
+struct ResArgs {
+    DevParams P;
+    Arr4<const double> cons0, prim0, vel[3];
+    double* fres[3];          // faceflux_res[d]: the reference's layout (no ghosts, nvars comps)
+    double* mres[3];          // cumom_res[d]
+    int fsy[3], fsz[3], fsn[3];
+    double mass[MAXS];
+    double dt;                // the stage's dt (dt, dt / 4, 2 dt / 3)
+    int stage;
+    int sides[6], nsides;
+    int64_t face_pref[7];     // faces of the listed sides, prefix sums
+    double* rec;              // test hook: draws of (stage, listed side, face), rec_cap each, or nullptr
+    int rec_cap;
+    int* status;
+};
+
+struct ResRng {
+    uint32_t k0, k1, c0, c1, c3;
+    uint32_t n;
+    double* rec;
+    int cap;
+    FHD_D uint64_t bits() {
+        uint32_t w[4] = {c0, c1, n, c3};
+        philox4x32_10(w, k0, k1);
+        return ((uint64_t)w[0] << 32) | w[1];
+    }
+    FHD_D void keep(double v) {
+        if (rec && (int)n < cap) rec[n] = v;
+        ++n;
+    }
+    // uniform in (0, 1]: the top 53 bits + 1, over 2^53
+    FHD_D double U() {
+        const double v = (double)((bits() >> 11) + 1) * (1.0 / 9007199254740992.0);
+        keep(v);
+        return v;
+    }
+    // standard normal (Box-Muller on two such uniforms of one Philox call)
+    FHD_D double Z() {
+        uint32_t w[4] = {c0, c1, n, c3};
+        philox4x32_10(w, k0, k1);
+        const double u1 = (double)(((((uint64_t)w[0] << 32) | w[1]) >> 11) + 1) * (1.0 / 9007199254740992.0);
+        const double u2 = (double)(((((uint64_t)w[2] << 32) | w[3]) >> 11) + 1) * (1.0 / 9007199254740992.0);
+        const double v = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+        keep(v);
+        return v;
+    }
+};
+
+constexpr int kResMaxTries = 1 << 16;      // rejection-sampling attempts per velocity
+constexpr int kResMaxParticles = 1 << 22;  // particles per process
+
+// random_cross_vel (reservoirStag_K.H:10-57); ok = 0 when the attempts run out
+FHD_D double res_cross_vel(double a, double vT, bool tangential, double Vt, ResRng& g, int& ok) {
+    const double sqrtPI = 1.77245385091;
+    const double small_number = 1.0e-13;
+    double v = 0.0;
+    if (!tangential) {
+        double z = 0.0;
+        if (a > small_number) {
+            bool stop = false;
+            for (int t = 0; !stop; ++t) {
+                if (t >= kResMaxTries) { ok = 0; break; }
+                const double u = g.U();
+                if ((a * sqrtPI) / (a * sqrtPI + 1.0 + a * a) > u) {
+                    z = -1.0 * fabs(0.0 + sqrt(0.5) * g.Z());
+                    stop = true;
+                } else if ((a * sqrtPI + 1.0) / (a * sqrtPI + 1.0 + a * a) > u) {
+                    z = -1.0 * sqrt(-1.0 * log(g.U()));
+                    stop = true;
+                } else {
+                    z = a * (1.0 - sqrt(g.U()));
+                    if (exp(1.0 * z * z) > g.U()) stop = true;
+                }
+            }
+            v = (a - z) * vT;
+        } else if (a < -1.0 * small_number) {
+            bool stop = false;
+            for (int t = 0; !stop; ++t) {
+                if (t >= kResMaxTries) { ok = 0; break; }
+                z = -1.0 * sqrt(a * a - log(g.U()));
+                if (a > z * (1.0 - g.U())) stop = true;
+            }
+            v = (a - z) * vT;
+        } else {
+            v = vT * sqrt(-1.0 * log(g.U()));
+        }
+    } else {
+        v = Vt + vT * (0.0 + sqrt(0.5) * g.Z());
+    }
+    return v;
+}
+
+// poisson_process_reservoir (reservoirStag_K.H:59-166), three dimensions
+template <int NS>
+FHD_D int res_poisson(const ResArgs& a, const double (&rhoYk)[NS], double T, double Vn, double area, double VT1,
+                      double VT2, ResRng& g, double& mass_cross, double (&mom_cross)[3], double& en_cross,
+                      double (&spec)[NS]) {
+    const double sqrtPI = 1.77245385091;
+    const double small_number = 1.0e-13;
+    const double kB = a.P.k_B;
+    mass_cross = 0.0;
+    en_cross = 0.0;
+    for (int c = 0; c < 3; ++c) mom_cross[c] = 0.0;
+    for (int n = 0; n < NS; ++n) spec[n] = 0.0;
+    double rate[NS], timer[NS], vth[NS], ratio[NS];
+    bool stopf[NS];
+    for (int n = 0; n < NS; ++n) {
+        vth[n] = sqrt(2.0 * kB * T / a.mass[n]);
+        ratio[n] = Vn / vth[n];
+        const double num_density = rhoYk[n] / a.mass[n];
+        if (fabs(ratio[n]) > small_number)
+            rate[n] = (1.0 / (2.0 * sqrtPI)) * num_density * area * vth[n] *
+                      (exp(-1.0 * ratio[n] * ratio[n]) + ratio[n] * sqrtPI * (1.0 + erf(ratio[n])));
+        else
+            rate[n] = (1.0 / (2.0 * sqrtPI)) * num_density * area * vth[n];
+        timer[n] = 0.0;
+        stopf[n] = false;
+    }
+    int ok = 1;
+    bool stop = false;
+    for (int it = 0; !stop; ++it) {
+        if (it >= kResMaxParticles) return 0;
+        for (int n = 0; n < NS; ++n) {
+            if (stopf[n]) continue;
+            mass_cross += a.mass[n];
+            spec[n] += a.mass[n];
+            double v = res_cross_vel(ratio[n], vth[n], false, 0.0, g, ok);
+            mom_cross[0] += a.mass[n] * v;
+            en_cross += 0.5 * a.mass[n] * (v) * (v);
+            v = res_cross_vel(ratio[n], vth[n], true, VT1, g, ok);
+            mom_cross[1] += a.mass[n] * v;
+            en_cross += 0.5 * a.mass[n] * (v) * (v);
+            v = res_cross_vel(ratio[n], vth[n], true, VT2, g, ok);
+            mom_cross[2] += a.mass[n] * v;
+            en_cross += 0.5 * a.mass[n] * (v) * (v);
+        }
+        stop = true;
+        for (int n = 0; n < NS; ++n) {
+            if (!stopf[n]) {
+                const double rn = g.U();
+                timer[n] = timer[n] - log(rn) / (rate[n]);
+                if (timer[n] >= a.dt) stopf[n] = true;
+            }
+            stop = stop && stopf[n];
+        }
+        if (!ok) return 0;
+    }
+    return ok;
+}
+
+// one thread per face of a reservoir interface: both processes, into faceflux_res / cumom_res
+template <int NS>
+static __global__ void __launch_bounds__(128) k_reservoir(ResArgs a) {
+    const DevParams& P = a.P;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < a.face_pref[a.nsides];
+         q += (int64_t)gridDim.x * blockDim.x) {
+        int li = 0;
+        while (q >= a.face_pref[li + 1]) ++li;
+        const int s = a.sides[li], d = s >> 1, hi = s & 1;
+        const int64_t f = q - a.face_pref[li];
+        const int e1 = d == 0 ? 1 : 0, e2 = d == 2 ? 1 : 2;  // the tangential directions, in order
+        int x[3];
+        x[d] = hi ? P.n[d] : 0;
+        x[e1] = (int)(f % P.n[e1]);
+        x[e2] = (int)(f / P.n[e1]);
+        int in[3] = {x[0], x[1], x[2]}, gh[3] = {x[0], x[1], x[2]};
+        in[d] = hi ? P.n[d] - 1 : 0;       // the cell inside the interface
+        gh[d] = hi ? P.n[d] : -1;          // the reservoir's ghost cell
+        const double area = P.dx[e1] * P.dx[e2];
+        const double vol = P.dx[0] * P.dx[1] * P.dx[2];
+        ResRng g;
+        g.k0 = P.key0;
+        g.k1 = P.key1;
+        g.c0 = (uint32_t)f;
+        g.c1 = 0x40000000u | ((uint32_t)a.stage << 8) | (uint32_t)s;
+        g.c3 = (uint32_t)noise_step(P);
+        g.n = 0;
+        g.rec = a.rec ? a.rec + ((int64_t)a.stage * a.face_pref[a.nsides] + q) * a.rec_cap : nullptr;
+        g.cap = a.rec_cap;
+        double* fl = a.fres[d];
+        const int64_t fidx = x[0] + (int64_t)x[1] * a.fsy[d] + (int64_t)x[2] * a.fsz[d];
+        const int64_t fsn = a.fsn[d];
+        double& mom = a.mres[d][fidx];
+        // particles in the inside cell (for the correction of the incoming fluxes)
+        double N = 0.0;
+        for (int n = 0; n < NS; ++n) N += vol * (a.cons0(in[0], in[1], in[2], 5 + n) / a.mass[n]);
+        double rhoYk[NS], spec[NS], mc[3], mass_cross, en_cross;
+        // from the reservoir (at rest, at the ghost cell's state)
+        for (int n = 0; n < NS; ++n) rhoYk[n] = a.cons0(gh[0], gh[1], gh[2], 5 + n);
+        int ok = res_poisson<NS>(a, rhoYk, a.prim0(gh[0], gh[1], gh[2], 4), 0.0, area, 0.0, 0.0, g, mass_cross, mc,
+                                 en_cross, spec);
+        if (!hi) {
+            fl[fidx] += (1.0 - (1.0 / (12.0 * N))) * mass_cross / (a.dt * area);
+            fl[fidx + 4 * fsn] += (1.0 + (1.0 / (4.0 * N))) * en_cross / (a.dt * area);
+            for (int n = 0; n < NS; ++n) fl[fidx + (5 + n) * fsn] += (1.0 - (1.0 / (12.0 * N))) * spec[n] / (a.dt * area);
+            mom += mc[0] / vol;
+            fl[fidx + fsn] += mc[1] / a.dt / area;
+            fl[fidx + 2 * fsn] += mc[2] / a.dt / area;
+        } else {
+            fl[fidx] -= (1.0 - (1.0 / (12.0 * N))) * mass_cross / (a.dt * area);
+            fl[fidx + 4 * fsn] -= (1.0 + (1.0 / (4.0 * N))) * en_cross / (a.dt * area);
+            for (int n = 0; n < NS; ++n) fl[fidx + (5 + n) * fsn] -= (1.0 - (1.0 / (12.0 * N))) * spec[n] / (a.dt * area);
+            mom -= mc[0] / vol;
+            fl[fidx + fsn] -= mc[1] / a.dt / area;
+            fl[fidx + 2 * fsn] -= mc[2] / a.dt / area;
+        }
+        // to the reservoir (the inside cell's state and velocity)
+        const Arr4<const double>& vx = a.vel[0];
+        const Arr4<const double>& vy = a.vel[1];
+        const Arr4<const double>& vz = a.vel[2];
+        const int i = in[0], j = in[1], k = in[2];
+        double V[3];
+        V[0] = 0.5 * (vx(i, j, k) + vx(i + 1, j, k));
+        V[1] = 0.5 * (vy(i, j, k) + vy(i, j + 1, k));
+        V[2] = 0.5 * (vz(i, j, k) + vz(i, j, k + 1));
+        if (!hi) V[d] = -0.5 * (a.vel[d](i, j, k) + a.vel[d](i + (d == 0), j + (d == 1), k + (d == 2)));
+        for (int n = 0; n < NS; ++n) rhoYk[n] = a.cons0(i, j, k, 5 + n);
+        ok &= res_poisson<NS>(a, rhoYk, a.prim0(i, j, k, 4), V[d], area, V[e1], V[e2], g, mass_cross, mc, en_cross,
+                              spec);
+        if (!hi) {
+            fl[fidx] -= mass_cross / (a.dt * area);
+            fl[fidx + 4 * fsn] -= en_cross / (a.dt * area);
+            for (int n = 0; n < NS; ++n) fl[fidx + (5 + n) * fsn] -= spec[n] / (a.dt * area);
+            mom -= mc[0] / vol;
+            fl[fidx + fsn] -= mc[1] / a.dt / area;
+            fl[fidx + 2 * fsn] -= mc[2] / a.dt / area;
+        } else {
+            fl[fidx] += mass_cross / (a.dt * area);
+            fl[fidx + 4 * fsn] += en_cross / (a.dt * area);
+            for (int n = 0; n < NS; ++n) fl[fidx + (5 + n) * fsn] += spec[n] / (a.dt * area);
+            mom += mc[0] / vol;
+            fl[fidx + fsn] += mc[1] / a.dt / area;
+            fl[fidx + 2 * fsn] += mc[2] / a.dt / area;
+        }
+        if (!ok && a.status) atomicCAS(a.status, 0, 5);  // FHD_ERR_TIMEOUT: a sampling loop ran out of attempts
+    }
+}
+
+// ResetReservoirFluxes (reservoirStag.cpp:871-1394) on the stage's flux scratch (or on
+// the caller's flux MultiFabs): the interface faces take the reservoir's mass, energy and
+// species fluxes, the interface edges the average of two tangential reservoir fluxes.
+// The reference reads those pairs from faceflux_res, which has no ghost cells, at index
+// -1 and n of the edge's other direction as well; Array4 then addresses the neighbouring
+// row, plane or component of the same allocation, and so does the flat index here.
+struct ResResetArgs {
+    DevParams P;
+    const double* fres[3];
+    int fsy[3], fsz[3], fsn[3];
+    Arr4<double> ff[3];       // face fluxes: comps cons 0, 4, 5.. at fcomp[0], [1], [2]..
+    int fc_rho, fc_rhoE, fc_Y;
+    Arr4<double> ef[6];       // edge fluxes: edgex_v, edgex_w, edgey_u, edgey_w, edgez_u, edgez_v
+    int side;
+};
+
+template <int NS>
+static __global__ void __launch_bounds__(128) k_res_reset(ResResetArgs a) {
+    const DevParams& P = a.P;
+    const int s = a.side, d = s >> 1, hi = s & 1;
+    const int e1 = d == 0 ? 1 : 0, e2 = d == 2 ? 1 : 2;
+    const int plane = hi ? P.n[d] : 0;
+    // items: the interface faces, then the (e1-nodal) edges, then the (e2-nodal) edges
+    const int64_t nf = (int64_t)P.n[e1] * P.n[e2];
+    const int64_t ne1 = (int64_t)(P.n[e1] + 1) * P.n[e2], ne2 = (int64_t)P.n[e1] * (P.n[e2] + 1);
+    const double* fr = a.fres[d];
+    const int64_t sy = a.fsy[d], sz = a.fsz[d], sn = a.fsn[d];
+    auto flat = [&](int i, int j, int k, int c) { return (int64_t)i + j * sy + k * sz + c * sn; };
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nf + ne1 + ne2;
+         q += (int64_t)gridDim.x * blockDim.x) {
+        int x[3];
+        x[d] = plane;
+        if (q < nf) {
+            x[e1] = (int)(q % P.n[e1]);
+            x[e2] = (int)(q / P.n[e1]);
+            const Arr4<double>& f = a.ff[d];
+            if (!f.p) continue;
+            f(x[0], x[1], x[2], a.fc_rho) = fr[flat(x[0], x[1], x[2], 0)];
+            f(x[0], x[1], x[2], a.fc_rhoE) = fr[flat(x[0], x[1], x[2], 4)];
+            for (int n = 0; n < NS; ++n) f(x[0], x[1], x[2], a.fc_Y + n) = fr[flat(x[0], x[1], x[2], 5 + n)];
+            continue;
+        }
+        // an edge nodal in d and in e (e1: the first tangential direction, comp 1 of
+        // faceflux_res; e2: the second, comp 2), averaged over the two faces beside it in e
+        const bool first = q < nf + ne1;
+        const int64_t r = first ? q - nf : q - nf - ne1;
+        const int e = first ? e1 : e2, o = first ? e2 : e1;
+        const int ce = first ? 1 : 2;
+        x[e] = (int)(r % (P.n[e] + 1));
+        x[o] = (int)(r / (P.n[e] + 1));
+        int y[3] = {x[0], x[1], x[2]};
+        y[e] -= 1;
+        const double v = 0.5 * (fr[flat(x[0], x[1], x[2], ce)] + fr[flat(y[0], y[1], y[2], ce)]);
+        // which edge flux: the momentum component e carried in direction d
+        int slot;
+        if (d == 0) slot = e == 1 ? 0 : 1;        // edgex_v (xy), edgex_w (xz)
+        else if (d == 1) slot = e == 0 ? 2 : 3;   // edgey_u (xy), edgey_w (yz)
+        else slot = e == 0 ? 4 : 5;               // edgez_u (xz), edgez_v (yz)
+        const Arr4<double>& ef = a.ef[slot];
+        if (ef.p) ef(x[0], x[1], x[2]) = v;
+    }
+}
+
+// ResetReservoirMom (reservoirStag.cpp:1396-1625): the interface faces' normal momentum
+struct ResMomArgs {
+    DevParams P;
+    const double* mres[3];
+    int fsy[3], fsz[3];
+    Arr4<double> mom[3];
+    int side;
+};
+
+static __global__ void __launch_bounds__(128) k_res_mom(ResMomArgs a) {
+    const DevParams& P = a.P;
+    const int s = a.side, d = s >> 1, hi = s & 1;
+    const int e1 = d == 0 ? 1 : 0, e2 = d == 2 ? 1 : 2;
+    const int64_t nf = (int64_t)P.n[e1] * P.n[e2];
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nf; q += (int64_t)gridDim.x * blockDim.x) {
+        int x[3];
+        x[d] = hi ? P.n[d] : 0;
+        x[e1] = (int)(q % P.n[e1]);
+        x[e2] = (int)(q / P.n[e1]);
+        a.mom[d](x[0], x[1], x[2]) = a.mres[d][x[0] + (int64_t)x[1] * a.fsy[d] + (int64_t)x[2] * a.fsz[d]];
     }
 }
 

@@ -261,7 +261,8 @@ def hard_sphere_single_gas(p: Params, T=None):
 def with_walls(p: Params, **dirs) -> Params:
     """``p`` with physical walls on the directions named x, y, z (both sides),
     each a dict: vel (1 slip, 2 no-slip), therm (1 adiabatic, 2 isothermal), mass
-    (1 impermeable, 2 held at a wall composition, 3 reservoir), t = (t_lo, t_hi)
+    (1 impermeable, 2 held at a wall composition, 3 reservoir, 4 particle
+    reservoir), t = (t_lo, t_hi)
     for isothermal walls and reservoirs, Yk or Xk = (lo, hi) compositions for
     concentration walls and reservoirs, p / rho = (lo, hi) reservoir pressure and
     density (defaults: the initial pressure; rho from p, t, Y).  The other
@@ -420,8 +421,8 @@ def parse_inputs(text: str, base: Params | None = None) -> Params:
             if key in kv:
                 upd[key] = tuple(int(x) for x in kv[key][:3])
         for key in ("bc_mass_lo", "bc_mass_hi"):
-            if any(v >= 4 for v in upd.get(key, ())):
-                raise ValueError(f"{key}: the particle reservoir (bc_mass 4) is not implemented")
+            if any(v >= 5 for v in upd.get(key, ())):
+                raise ValueError(f"{key}: bc_mass values above 4 are not boundary conditions of this step")
         for key in ("t_lo", "t_hi", "p_lo", "p_hi", "rho_lo", "rho_hi"):
             if key in kv:
                 upd[key] = tuple(float(x) for x in kv[key][:3])

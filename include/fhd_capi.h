@@ -121,10 +121,11 @@ typedef struct {
      * or 3 (a reservoir: ghost cells held at the reservoir state t, p_lo / p_hi
      * (<= 0: the initial state's pressure), rho_lo / rho_hi (<= 0: from p, t, Y;
      * else t <= 0 is derived from p and rho) and composition bc_Yk / bc_Xk; flow
-     * passes the interface).  The particle reservoir (bc_mass 4) returns
-     * FHD_ERR_UNSUPPORTED.  FP64 only; the state's ghost width is then exactly 2
-     * in fhd_rk3_step_stag(s), and the batched and no-allocation steps return
-     * FHD_ERR_UNSUPPORTED. */
+     * passes the interface) or 4 (the same reservoir, its interface fluxes and
+     * momenta from the particles crossing it: ComputeFluxMomReservoir, with Philox
+     * draws under the context's seed).  FP64 only; the state's ghost width is then
+     * exactly 2 in fhd_rk3_step_stag(s), and the batched and no-allocation steps
+     * return FHD_ERR_UNSUPPORTED. */
     int walls;
     int bc_vel_lo[3], bc_vel_hi[3];
     int bc_mass_lo[3], bc_mass_hi[3];
@@ -231,6 +232,14 @@ int fhd_override_sync(fhd_ctx* ctx, fhd_fab f);
  * rho Y), cumom and vel.  prim and cu have one ghost width, cumom and vel all
  * the same one; a fully periodic context does nothing. */
 int fhd_set_bc_stag(fhd_ctx* ctx, fhd_fab prim, fhd_fab cu, const fhd_fab cumom[3], const fhd_fab vel[3]);
+
+/* Test hook of the particle reservoir (bc_mass 4): record every random number the
+ * reservoir's Poisson processes draw (ComputeFluxMomReservoir), so that a harness can
+ * feed the same numbers to the reference.  buf: device memory of
+ * 3 x (interface faces of the bc_mass-4 sides, x lo .. z hi) x cap doubles, entry
+ * (stage, face, n) the n-th draw of that face in that stage of the next step (draws
+ * beyond cap are not recorded); NULL turns recording off. */
+int fhd_set_reservoir_record(fhd_ctx* ctx, void* buf, int cap);
 
 /* MultiFabFillRandomNormal: MultiFabFillRandom.cpp:34-50 (declared
  * rng_functions.H:13-22).  Philox-4x32-10 normals; `stream_id` selects an

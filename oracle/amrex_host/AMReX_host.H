@@ -484,6 +484,9 @@ struct NoiseSource {
     std::function<void(MultiFab& mf, int scomp, int ncomp, Real mean, Real stddev)> fill_normal;
     // one ParallelForRNG launch: z at (i, j, k) of launch `launch`
     std::function<Real(long launch, int i, int j, int k)> point_normal;
+    // when set, every draw of a ParallelForRNG body instead: the n-th draw at (i, j, k)
+    // of launch `launch`, a uniform (normal = 0) or a standard normal (normal = 1)
+    std::function<Real(long launch, int i, int j, int k, long n, int normal)> stream;
     long launches = 0;
 };
 inline NoiseSource& noise_source() {
@@ -494,14 +497,19 @@ inline NoiseSource& noise_source() {
 struct RandomEngine {
     long launch;
     int i, j, k;
+    mutable long n = 0;   // draws made so far at this point
 };
 inline Real RandomNormal(Real mean, Real stddev, const RandomEngine& e) {
+    if (noise_source().stream) return mean + stddev * noise_source().stream(e.launch, e.i, e.j, e.k, e.n++, 1);
     if (!noise_source().point_normal) Abort("RandomNormal: no injected noise source");
     return mean + stddev * noise_source().point_normal(e.launch, e.i, e.j, e.k);
 }
 inline Real RandomNormal(Real, Real) { Abort("RandomNormal: host-RNG draws are not injected"); }
 inline Real Random() { Abort("amrex::Random: uniform draws are not injected"); }
-inline Real Random(const RandomEngine&) { Abort("amrex::Random: uniform draws are not injected"); }
+inline Real Random(const RandomEngine& e) {
+    if (noise_source().stream) return noise_source().stream(e.launch, e.i, e.j, e.k, e.n++, 0);
+    Abort("amrex::Random: uniform draws are not injected");
+}
 inline unsigned int RandomPoisson(Real, const RandomEngine&) { Abort("amrex::RandomPoisson: not injected"); }
 inline unsigned int Random_int(unsigned int, const RandomEngine&) { Abort("amrex::Random_int: not injected"); }
 
@@ -756,7 +764,7 @@ inline void ParallelFor(Long n, F&& f) { for (Long q = 0; q < n; ++q) f(q); }
 template <class F>
 inline void ParallelForRNG(const Box& b, F&& f) {
     const long launch = noise_source().launches++;
-    LoopBox(b, [&](int i, int j, int k) { f(i, j, k, RandomEngine{launch, i, j, k}); });
+    LoopBox(b, [&](int i, int j, int k) { f(i, j, k, RandomEngine{launch, i, j, k, 0}); });
 }
 
 inline void FillRandomNormal(MultiFab& mf, int scomp, int ncomp, Real mean, Real stddev) {

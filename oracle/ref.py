@@ -64,6 +64,7 @@ def lib():
         L.fhdref_fill_boundary.argtypes = [vp, P(i), i, i, i]
         L.fhdref_wall_composition.argtypes = [i, P(d), P(d)]
         L.fhdref_wall_state.argtypes = [i, P(d)]
+        L.fhdref_set_reservoir_draws.argtypes = [vp, i]
         _lib = L
     return _lib
 
@@ -236,6 +237,17 @@ def wall_composition(p, side):
     x = (C.c_double * 8)()
     _chk(lib().fhdref_wall_composition(side, y, x), "SetupCWallStag")
     return list(y[:p.nspecies]), list(x[:p.nspecies])
+
+
+def set_reservoir_draws(rec, cap):
+    """Feed the particle reservoir's draws (a contiguous float64 CPU tensor laid out as
+    fhd_set_reservoir_record writes them) to the next rk3_step; None turns it off."""
+    lib()
+    if rec is None:
+        _chk(lib().fhdref_set_reservoir_draws(None, 0), "reservoir draws")
+        return
+    assert rec.dtype == torch.float64 and rec.is_contiguous() and rec.device.type == "cpu"
+    _chk(lib().fhdref_set_reservoir_draws(C.c_void_p(rec.data_ptr()), cap), "reservoir draws")
 
 
 def wall_state(p, side):

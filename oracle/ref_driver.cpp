@@ -153,6 +153,21 @@ int fhdref_wall_composition(int s, double* yk, double* xk) {
     });
 }
 
+// Draws of the particle reservoir (bc_mass 4) for the next fhdref_rk3_step: rec holds
+// 3 x (interface faces of the bc_mass-4 sides, x lo .. z hi) x cap values, entry
+// (stage, face, n) the n-th draw at that face in that stage, as fhd_set_reservoir_record
+// lays them out; the step's ParallelForRNG launches are then the reservoir's (one per
+// such side and stage, in that order), so the step must have no chemistry noise.
+static const double* g_res_rec = nullptr;
+static int g_res_cap = 0;
+
+int fhdref_set_reservoir_draws(const double* rec, int cap) {
+    return guarded([&] {
+        g_res_rec = rec;
+        g_res_cap = cap;
+    });
+}
+
 // Reservoir state of side s after SetupCWallStag: t, p, rho.
 int fhdref_wall_state(int s, double* tpr) {
     return guarded([&] {
@@ -315,10 +330,34 @@ int fhdref_rk3_step(double* cu, double* const* mom, double* prim, double* const*
             const Long nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1;
             return chem[launch][(i - lo[0]) + (j - lo[1]) * nx + (kk - lo[2]) * nx * ny];
         };
+        if (g_res_rec) {
+            int sides[6], ns4 = 0;
+            long pref[7] = {0};
+            const int* lo = bc_mass_lo.data();
+            const int* hi = bc_mass_hi.data();
+            for (int side = 0; side < 6; ++side) {
+                const int dd = side / 2;
+                if ((side % 2 ? hi[dd] : lo[dd]) != 4) continue;
+                const int e1 = dd == 0 ? 1 : 0, e2 = dd == 2 ? 1 : 2;
+                sides[ns4] = side;
+                pref[ns4 + 1] = pref[ns4] + (long)n_cells[e1] * n_cells[e2];
+                ++ns4;
+            }
+            src.stream = [&, sides, ns4, pref](long launch, int i, int j, int kk, long n, int) -> Real {
+                if (ns4 == 0 || launch >= 3L * ns4) throw std::runtime_error("unexpected reservoir launch");
+                const int stage = (int)(launch / ns4), li = (int)(launch % ns4), dd = sides[li] / 2;
+                const int e1 = dd == 0 ? 1 : 0, e2 = dd == 2 ? 1 : 2;
+                const int x[3] = {i, j, kk};
+                const long q = pref[li] + x[e1] + (long)n_cells[e1] * x[e2];
+                if (n >= g_res_cap) throw std::runtime_error("reservoir draws beyond the recorded capacity");
+                return g_res_rec[((long)stage * pref[ns4] + q) * g_res_cap + n];
+            };
+        }
         TurbForcingComp turb;
         RK3stepStag(c, m, p, v, s, e, z, k, ch, d, ff, ex, ey, ez, cf, rc, g_geom, dt, step, turb);
         src.fill_normal = nullptr;
         src.point_normal = nullptr;
+        src.stream = nullptr;
         if (call != 24) throw std::runtime_error("RK3stepStag made an unexpected number of noise fills");
     });
 }

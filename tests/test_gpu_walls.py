@@ -210,3 +210,64 @@ def test_walls_conserve_mass_and_hold_the_wall_faces(ref):
     mx = d.cumom[0].valid(0)  # (z, y, x): the x wall faces are x = 0 and x = n
     assert torch.all(mx[..., 0] == 0) and torch.all(mx[..., -1] == 0)
     ctx.close()
+
+
+# the particle reservoir (bc_mass 4): the interface fluxes and momenta come from the
+# particles crossing it (ComputeFluxMomReservoir, ResetReservoirFluxes / Mom)
+PARTICLE = {
+    "particle_reservoir_x": lambda: with_walls(
+        argon((8, 4, 4), dx=8e-6, seed=13), x=dict(vel=2, therm=2, mass=4, t=(273.0, 280.0), Yk=((0.5, 0.5),) * 2)),
+    "particle_reservoir_wall": lambda: with_walls(
+        mixture4((6, 5, 4), dx=8e-6, seed=14),
+        y=dict(vel=2, therm=2, mass=4, t=(270.0, 276.0), Yk=((0.4, 0.2, 0.3, 0.1), (0.1, 0.3, 0.2, 0.4))),
+        z=dict(vel=1, therm=1, mass=1)),
+}
+
+
+def reservoir_faces(p):
+    n = p.n_cells
+    tot = 0
+    for d in range(3):
+        for m in (p.bc_mass_lo[d], p.bc_mass_hi[d]):
+            if m == 4:
+                e = [q for q in range(3) if q != d]
+                tot += n[e[0]] * n[e[1]]
+    return tot
+
+
+@pytest.mark.parametrize("name", list(PARTICLE))
+def test_particle_reservoir_steps_match_the_reference(ref, name):
+    """The GPU records every random number its reservoir processes draw; the
+    reference, fed the same numbers in its own call order, gives the same step.
+    The processes' rates and velocities go through exp, erf and log, which CUDA and
+    the host's libm may round differently in the last bit, so the state and the
+    stage-3 by-products agree within 1e-12 of each field's norm (everything away
+    from the interface is bit-identical)."""
+    p = PARTICLE[name]()
+    st = ref.state_from_reference(p, seed=7)
+    d = st.clone(device="cuda")
+    ctx = Context(p)
+    dt = stable_dt(p)
+    cap = 32768
+    rec = torch.full((3 * reservoir_faces(p) * cap,), float("nan"), dtype=torch.float64, device="cuda")
+    ctx.set_reservoir_record(rec, cap)
+    for s in range(2):
+        nz = ref.step_noise(p, seed=70 + s)
+        ctx.rk3_step(d, dt, s, noise=nz.to("cuda"), aux=True)
+        torch.cuda.synchronize()
+        assert ctx.status() == 0
+        drawn = rec.cpu().contiguous()
+        ref.set_reservoir_draws(drawn, cap)
+        try:
+            ref.rk3_step(st, nz, dt, s)
+        finally:
+            ref.set_reservoir_draws(None, 0)
+        bad, worst = compare_named(d.named(aux=True), st.named(aux=True), tol=1e-12)
+        assert not bad, (s, bad[:6])
+    # the interface carries flow: its normal momentum is the particles' (non-zero)
+    dd = [q for q in range(3) if 4 in (p.bc_mass_lo[q], p.bc_mass_hi[q])][0]
+    mv = d.cumom[dd].valid(0)
+    face = mv[..., 0] if dd == 0 else (mv[:, 0, :] if dd == 1 else mv[0])
+    assert face.abs().max() > 0
+    ctx.set_reservoir_record(None)
+    ctx.close()

@@ -157,11 +157,11 @@ def test_parse_inputs_reference_keys():
     assert p.n_cells == (16, 16, 16) and p.nspecies == 2 and p.seed == 7
     assert p.dx[0] == pytest.approx(8e-6)
     assert p.hcv == (-1.0, -1.0)
-    # walls and reservoirs are read; the particle reservoir (bc_mass 4) is refused
+    # walls and reservoirs are read; bc_mass above 4 is refused
     w = parse_inputs(deck + "\nbc_vel_lo = 1 -1 -1\nbc_vel_hi = 1 -1 -1\nbc_mass_lo = 1 -1 -1\n")
     assert w.walls == 1 and w.bc_vel_lo == (1, -1, -1) and w.bc_mass_lo == (1, -1, -1)
     with pytest.raises(ValueError):
-        parse_inputs(deck + "\nbc_vel_lo = 1 -1 -1\nbc_mass_lo = 4 -1 -1\n")
+        parse_inputs(deck + "\nbc_vel_lo = 1 -1 -1\nbc_mass_lo = 5 -1 -1\n")
 
 
 def test_dt_rule_respects_diffusive_limit():

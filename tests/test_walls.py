@@ -26,7 +26,7 @@ def test_wall_parameters_round_trip_through_the_deck():
         assert tuple(getattr(q, key)) == tuple(getattr(p, key)) if key != "walls" else q.walls == 1, key
     assert q.bc_Yk_lo[2] == p.bc_Yk_lo[2] and q.bc_Yk_hi[2] == p.bc_Yk_hi[2]
     with pytest.raises(ValueError):
-        parse_inputs(p.to_inputs().replace("bc_mass_lo = 1 -1 2", "bc_mass_lo = 1 -1 4"))
+        parse_inputs(p.to_inputs().replace("bc_mass_lo = 1 -1 2", "bc_mass_lo = 1 -1 5"))
     r = parse_inputs(p.to_inputs().replace("bc_mass_lo = 1 -1 2", "bc_mass_lo = 1 -1 3"))
     assert r.bc_mass_lo == (1, -1, 3) and r.p_lo == p.p_lo and r.rho_lo == p.rho_lo
 
@@ -45,7 +45,7 @@ def _create_rc(p, **raw):
 @pytest.mark.parametrize("change,code", [
     (dict(bc_vel_lo_1=2), "FHD_ERR_BAD_ARG"),            # one side periodic, the other a wall
     (dict(bc_mass_lo_0=3), "FHD_ERR_BAD_ARG"),           # a reservoir without a composition
-    (dict(bc_mass_hi_0=4), "FHD_ERR_UNSUPPORTED"),       # the particle reservoir
+    (dict(bc_mass_hi_0=5), "FHD_ERR_UNSUPPORTED"),       # no such boundary
     (dict(bc_vel_hi_0=3), "FHD_ERR_BAD_ARG"),
     (dict(bc_therm_lo_2=0), "FHD_ERR_BAD_ARG"),
     (dict(t_hi_0=0.0), "FHD_ERR_BAD_ARG"),               # isothermal wall without a temperature
