@@ -108,8 +108,8 @@ inline int plot_deltaY_dir = -1;  // common_functions.cpp:620
 // here; the staggered decks set every bc_vel); otherwise both sides are walls:
 // bc_vel 1 slip / 2 no-slip, bc_therm 1 adiabatic / 2 isothermal at t_lo / t_hi,
 // bc_mass 1 impermeable / 2 at the wall composition bc_Yk_* or bc_Xk_* (the one
-// that sums to 1) / 3 a reservoir at t, p, rho and that composition.  The particle
-// reservoir (bc_mass 4) is refused.
+// that sums to 1) / 3 a reservoir at t, p, rho and that composition / 4 the same
+// reservoir with the interface fluxes of the particles crossing it.
 inline GpuArray<int, 3> bc_vel_lo{{-1, -1, -1}}, bc_vel_hi{{-1, -1, -1}};
 inline GpuArray<int, 3> bc_mass_lo{{-1, -1, -1}}, bc_mass_hi{{-1, -1, -1}};
 inline GpuArray<int, 3> bc_therm_lo{{-1, -1, -1}}, bc_therm_hi{{-1, -1, -1}};

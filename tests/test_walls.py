@@ -1,9 +1,9 @@
-"""Physical walls without a GPU: parameter handling (the deck keys of
-boundaryStag.cpp round-trip through to_inputs / parse_inputs), fhd_create's
+"""Physical walls and reservoirs without a GPU: parameter handling (the deck keys
+of boundaryStag.cpp round-trip through to_inputs / parse_inputs), fhd_create's
 validation of wall settings before it touches a device, the entry points that
-refuse walls, and the reference's own wall step (oracle/_ref) on the cases the
-GPU tests compare against: mass conserved, wall faces at rest, ghost cells at
-the wall values."""
+refuse walls, and the reference's own wall and reservoir steps (oracle/_ref) on
+the cases the GPU tests compare against: mass conserved, wall faces at rest,
+ghost cells at the wall and reservoir values."""
 import ctypes as C
 
 import pytest
