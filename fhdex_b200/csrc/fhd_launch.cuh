@@ -253,11 +253,14 @@ int launch_walls_part_t(const StageCall& c, int part) {
     if (part == 0) {
         k_taus<NS, double, NZ, true><<<grid_for((int64_t)(N[0] + 2) * (N[1] + 2) * (N[2] + 2), 128), 128, 0, c.stream>>>(a);
     } else if (part == 1) {
-        k_faces<NS, double, NZ, 0, 128, 4, true><<<resident_grid<k_faces<NS, double, NZ, 0, 128, 4, true>>(
+        // register cap: 64 up to two species (the periodic autotuner's choice at 256^3;
+        // 128 was measured twice as slow for the wall variant), 128 above
+        constexpr int MB = NS <= 2 ? 8 : 4;
+        k_faces<NS, double, NZ, 0, 128, MB, true><<<resident_grid<k_faces<NS, double, NZ, 0, 128, MB, true>>(
             (int64_t)(N[0] + 1) * N[1] * N[2], 128), 128, 0, c.stream>>>(a);
-        k_faces<NS, double, NZ, 1, 128, 4, true><<<resident_grid<k_faces<NS, double, NZ, 1, 128, 4, true>>(
+        k_faces<NS, double, NZ, 1, 128, MB, true><<<resident_grid<k_faces<NS, double, NZ, 1, 128, MB, true>>(
             (int64_t)N[0] * (N[1] + 1) * N[2], 128), 128, 0, c.stream>>>(a);
-        k_faces<NS, double, NZ, 2, 128, 4, true><<<resident_grid<k_faces<NS, double, NZ, 2, 128, 4, true>>(
+        k_faces<NS, double, NZ, 2, 128, MB, true><<<resident_grid<k_faces<NS, double, NZ, 2, 128, MB, true>>(
             (int64_t)N[0] * N[1] * (N[2] + 1), 128), 128, 0, c.stream>>>(a);
     } else {
         k_update<NS, double, NZ><<<resident_grid<k_update<NS, double, NZ>>(
