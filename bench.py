@@ -729,10 +729,10 @@ def run_stats(args):
     ctx.init_state(st)
     dt = stable_dt(p)
     ctx.rk3_step(st, dt, 0, aux=False)
-    stats = StatsState(p, "cuda:0")
+    stats = StatsState(p, "cuda:0", cross=True)
     flags = capi.STATS_MEANS | capi.STATS_VARS | capi.STATS_MOM3 | capi.STATS_MOM4
     for s in range(1, args.warmup + 1):
-        ctx.stats_stag(st, stats, s, flags)
+        ctx.stats_stag(st, stats, s, flags | capi.STATS_CROSS)
     torch.cuda.synchronize()
     clocks = ClockSampler(0)
     clocks.start()
@@ -742,12 +742,21 @@ def run_stats(args):
     for s in range(args.steps):
         ctx.stats_stag(st, stats, args.warmup + 1 + s, flags)
     e1.record()
+    # the same updates with the yz-averaged spatial cross-correlations (plot_cross)
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record()
+    for s in range(args.steps):
+        ctx.stats_stag(st, stats, args.warmup + args.steps + 1 + s, flags | capi.STATS_CROSS)
+    e3.record()
     torch.cuda.synchronize()
     clk = clocks.stop()
     ms = e0.elapsed_time(e1) / args.steps
+    ms_cross = e2.elapsed_time(e3) / args.steps - ms
     assert ctx.status() == 0
     cells = p.n_cells[0] * p.n_cells[1] * p.n_cells[2]
     alg = stats_alg_bytes_per_cell(p) * cells
+    # k_sum_to_line streams cu, cuMeans (nvars each) and nspecies+4 components of prim and primMeans once
+    line_bytes = 8 * (2 * p.nvars + 2 * (p.nspecies + 4)) * cells
     peak, peak_kind = measured_peak()
     achieved = alg / (ms / 1e3) / 1e9
     traffic = STATS_TRAFFIC_BYTES_PER_CELL.get(f"{p.nspecies}")
@@ -760,6 +769,10 @@ def run_stats(args):
                                    "traffic": traffic * cells if traffic else None,
                                    "algorithmic_bytes_per_launch": alg,
                                    "kernel": "k_stats_means_a + k_stats_means_b + k_stats_vars + 4 ghost fills"},
+                      "cross": {"ms_per_update": ms_cross, "kernels": "k_sum_to_line + k_spatial_cross",
+                                "algorithmic_bytes": line_bytes,
+                                "achieved_GBs": line_bytes / (ms_cross / 1e3) / 1e9,
+                                "frac": line_bytes / (ms_cross / 1e3) / 1e9 / peak},
                       "clocks": clk}), flush=True)
 
 

@@ -94,6 +94,7 @@ class FhdParams(C.Structure):
         ("rho0", C.c_double),
         ("T_init", C.c_double),
         ("rhobar", C.c_double * MAX_SPECIES),
+        ("cross_cell", C.c_int),
     ]
 
 
@@ -117,10 +118,10 @@ class FhdStats(C.Structure):
     _fields_ = [("cuMeans", FhdFab), ("cuVars", FhdFab), ("primMeans", FhdFab), ("primVars", FhdFab),
                 ("coVars", FhdFab), ("mom3", FhdFab), ("mom4", FhdFab),
                 ("velMeans", FhdFab * 3), ("velVars", FhdFab * 3), ("cumomMeans", FhdFab * 3),
-                ("cumomVars", FhdFab * 3)]
+                ("cumomVars", FhdFab * 3), ("spatialCross", C.c_void_p), ("dataSliceMeans_xcross", C.c_void_p)]
 
 
-STATS_MEANS, STATS_VARS, STATS_MOM3, STATS_MOM4 = 1, 2, 4, 8
+STATS_MEANS, STATS_VARS, STATS_MOM3, STATS_MOM4, STATS_CROSS = 1, 2, 4, 8, 16
 
 _PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG_DIR, "lib", "libfhd_b200.so")
@@ -178,6 +179,9 @@ def _declare(lib):
         "fhd_measure_fma_peak": (i, [i, i, P(d)]),
         "fhd_rk3_step_stag_noalloc": (i, [P(FhdParams), fab, pfab, fab, pfab, d, C.c_int64, vp, P(i)]),
         "fhd_stats_stag": (i, [vp, fab, fab, pfab, pfab, P(FhdStats), C.c_int64, i]),
+        "fhd_spatial_cross_ncross": (i, [i]),
+        "fhd_spatial_cross_nstats": (i, [i]),
+        "fhd_write_spatial_cross": (i, [P(FhdParams), C.c_char_p, i, vp]),
         "fhd_sf_create": (i, [P(vp), P(i), i, i, P(i), P(i), P(d), i]),
         "fhd_sf_destroy": (i, [vp]),
         "fhd_sf_set_stream": (i, [vp, vp]),

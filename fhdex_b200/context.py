@@ -201,8 +201,9 @@ class Context:
         cur.wait_stream(self._side)
 
     def stats_stag(self, st: StagState, stats, steps: int, flags: int = 15):
-        """evaluateStatsStag3D's per-cell update (fhd_stats_stag) with sample count
-        `steps` (1 for the first sample after a reset); flags = capi.STATS_*."""
+        """evaluateStatsStag3D's update (fhd_stats_stag) with sample count `steps`
+        (1 for the first sample after a reset); flags = capi.STATS_* (STATS_CROSS
+        needs a StatsState made with cross=True and uses Params.cross_cell)."""
         self._stream()
         s = stats.c_struct()
         self._stats_struct = s

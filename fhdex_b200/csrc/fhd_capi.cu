@@ -42,6 +42,9 @@ struct fhd_ctx {
     double* res_rec = nullptr;   // test hook: the particle reservoir's draws
     int res_cap = 0;
     WallParams wall{};
+    // x-line scratch of the spatial cross-correlations (fhd_stats_stag, FHD_STATS_CROSS)
+    double* lines = nullptr;
+    size_t lines_bytes = 0;
     // device mirrors for the host-buffer step
     double* hbuf = nullptr;
     size_t hbuf_bytes = 0;
@@ -444,6 +447,7 @@ int fhd_destroy(fhd_ctx* c) {
     cudaStreamSynchronize(c->stream);
     if (c->scratch) cudaFree(c->scratch);
     if (c->coef) cudaFree(c->coef);
+    if (c->lines) cudaFree(c->lines);
     if (c->res.base) cudaFree(c->res.base);
     if (c->hbuf) cudaFree(c->hbuf);
     for (auto& e : c->evs) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
@@ -1245,9 +1249,35 @@ int fhd_stats_stag(fhd_ctx* c, fhd_fab cu, fhd_fab prim, const fhd_fab vel[3], c
         if ((flags & FHD_STATS_MOM3) && !fab_ok(c, st->mom3, CELLN, 0, nvars + 1, FHD_F64)) return FHD_ERR_BAD_ARG;
         if ((flags & FHD_STATS_MOM4) && !fab_ok(c, st->mom4, CELLN, 0, nvars + 1, FHD_F64)) return FHD_ERR_BAD_ARG;
     }
+    const bool cross = flags & FHD_STATS_CROSS;
+    if (cross) {
+        // main_driver.cpp:249-251
+        if (c->prm.cross_cell < 0 || c->prm.cross_cell > c->prm.n_cells[0] - 1) return FHD_ERR_BAD_ARG;
+        if (!st->spatialCross || !st->dataSliceMeans_xcross) return FHD_ERR_BAD_ARG;
+    }
     cudaSetDevice(c->device);
+    if (cross) {
+        const size_t need = (size_t)stats_line_doubles(ns, c->prm.n_cells[0]) * sizeof(double);
+        if (c->lines_bytes < need) {
+            if (c->lines) {
+                if (cudaStreamSynchronize(c->stream) != cudaSuccess) { cudaGetLastError(); return FHD_ERR_CUDA; }
+                cudaFree(c->lines);
+                c->lines = nullptr;
+                c->lines_bytes = 0;
+            }
+            if (cudaMalloc(&c->lines, need) != cudaSuccess) { cudaGetLastError(); return FHD_ERR_OOM; }
+            c->lines_bytes = need;
+        }
+    }
     const DevParams P = make_dev(c, 1.0, 0);
-    return exact_stats(P, cu, prim, mom, *st, steps, flags, c->stream);
+    return exact_stats(P, cu, prim, mom, *st, steps, flags, c->prm.cross_cell, c->lines, c->stream);
+}
+
+int fhd_spatial_cross_ncross(int nspecies) {
+    return nspecies < 1 || nspecies > FHD_MAX_SPECIES ? FHD_ERR_BAD_ARG : 37 + nspecies + 3;
+}
+int fhd_spatial_cross_nstats(int nspecies) {
+    return nspecies < 1 || nspecies > FHD_MAX_SPECIES ? FHD_ERR_BAD_ARG : 2 * (5 + nspecies) + 8 + 2 * nspecies;
 }
 
 int fhd_profile(fhd_ctx* c, int enable) {

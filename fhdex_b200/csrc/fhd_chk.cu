@@ -6,6 +6,11 @@
 // cumommeanx..z, cumomvarx..z, coVars, mom3, mom4), whole fabs with their ghost
 // cells as VisMF writes them.
 //
+// With plot_cross (fhd_stats.spatialCross non-NULL) the Header also carries
+// spatialCrossVec after the BoxArray, one value per line at 16 significant digits
+// (Checkpoint.cpp:112-118, read back at :343-358).  fhd_write_spatial_cross writes
+// WriteSpatialCross3D's text file (writePlotFileStag.cpp:528-549).
+//
 // The reference also saves its C++ random engines' states (rng files); the noise
 // here is a function of (seed, step) alone, so the restart step is all the
 // generator needs.  Host code: device fabs are copied with cudaMemcpy after a
@@ -102,6 +107,14 @@ bool geometry(const fhd_params& p, const fhd_fab& f, int vlo[3], int vhi[3], int
     return *ng >= 0;
 }
 
+int ncross_of(const fhd_params& p) { return 37 + p.nspecies + 3; }
+
+// spatialCross (host or device) into a host vector
+bool cross_to_host(const fhd_params& p, const double* src, std::vector<double>& out) {
+    out.resize((size_t)p.n_cells[0] * ncross_of(p));
+    return copy_bytes(out.data(), src, out.size() * sizeof(double), on_device(src));
+}
+
 std::string chk_dir(const char* base, int step) {
     char num[32];
     std::snprintf(num, sizeof(num), "%09d", step);
@@ -124,10 +137,14 @@ extern "C" int fhd_write_checkpoint(const fhd_params* params, const char* chk_ba
         if (!geometry(*params, e.fab, vlo, vhi, type, &ng)) return FHD_ERR_BAD_ARG;
         dev = dev || on_device(e.fab.data);
     }
+    const bool cross = stats && stats->spatialCross;
+    if (cross) dev = dev || on_device(stats->spatialCross);
     if (dev && cudaDeviceSynchronize() != cudaSuccess) {
         cudaGetLastError();
         return FHD_ERR_CUDA;
     }
+    std::vector<double> sc;
+    if (cross && !cross_to_host(*params, stats->spatialCross, sc)) return FHD_ERR_CUDA;
     const std::string dir = chk_dir(chk_base, step);
     if (!vismf_mkdir(dir) || !vismf_mkdir(dir + "/Level_0")) return FHD_ERR_BAD_ARG;
     FILE* h = std::fopen((dir + "/Header").c_str(), "w");
@@ -136,6 +153,7 @@ extern "C" int fhd_write_checkpoint(const fhd_params* params, const char* chk_ba
               cc[3] = {0, 0, 0};
     std::fprintf(h, "Checkpoint file for FHDeX/compressStag\n%d\n%.17g\n%d\n(1 0\n%s\n)\n\n", step, time, stats_count,
                  vismf_box(lo, hi, cc).c_str());
+    for (double v : sc) std::fprintf(h, "%.16g\n", v);
     if (std::fclose(h) != 0) return FHD_ERR_BAD_ARG;
     std::vector<double> buf;
     for (const Entry& e : E) {
@@ -161,7 +179,16 @@ extern "C" int fhd_read_checkpoint(const fhd_params* params, const char* chk_bas
     char title[256];
     int s = 0, sc = 0;
     double t = 0;
-    const bool hok = std::fgets(title, sizeof(title), h) && std::fscanf(h, "%d %lf %d", &s, &t, &sc) == 3;
+    bool hok = std::fgets(title, sizeof(title), h) && std::fscanf(h, "%d %lf %d", &s, &t, &sc) == 3;
+    // spatialCrossVec: the values after the BoxArray's closing ")" line
+    std::vector<double> cross;
+    if (hok && stats && stats->spatialCross) {
+        char line[512];
+        bool end = false;
+        while (!end && std::fgets(line, sizeof(line), h)) end = line[0] == ')';
+        cross.resize((size_t)params->n_cells[0] * ncross_of(*params));
+        for (double& v : cross) hok = hok && end && std::fscanf(h, "%lf", &v) == 1;
+    }
     std::fclose(h);
     if (!hok || std::strncmp(title, "Checkpoint file for FHDeX/compressStag", 38) != 0) return FHD_ERR_BAD_ARG;
     const std::vector<Entry> E = entries(cu, cumom, prim, vel, stats);
@@ -186,9 +213,45 @@ extern "C" int fhd_read_checkpoint(const fhd_params* params, const char* chk_bas
         }
         if (!copy_bytes(e.fab.data, buf.data(), buf.size() * sizeof(double), dev)) return FHD_ERR_CUDA;
     }
+    if (!cross.empty()) {
+        const bool dev = on_device(stats->spatialCross);
+        if (dev && !synced && cudaDeviceSynchronize() != cudaSuccess) {
+            cudaGetLastError();
+            return FHD_ERR_CUDA;
+        }
+        if (!copy_bytes(stats->spatialCross, cross.data(), cross.size() * sizeof(double), dev)) return FHD_ERR_CUDA;
+    }
     // ReadCheckPoint resumes at the step after the saved one (Checkpoint.cpp:328-329)
     *step = s + 1;
     *time = t;
     *stats_count = sc;
     return FHD_OK;
+}
+
+// WriteSpatialCross3D (writePlotFileStag.cpp:528-549): <base><step, 9 digits>, one
+// line per x cell: the cell centre prob_lo[0] + (i+0.5)*dx[0], then the ncross
+// entries, each followed by a space.  The reference sets 16 significant digits
+// only before the first entry, so the first line's centre keeps the stream's
+// default 6 (every later number has 16).
+extern "C" int fhd_write_spatial_cross(const fhd_params* params, const char* base, int step,
+                                       const double* spatial_cross) {
+    if (!params || !base || !spatial_cross || step < 0 || params->nspecies < 1 ||
+        params->nspecies > FHD_MAX_SPECIES || params->n_cells[0] < 1)
+        return FHD_ERR_BAD_ARG;
+    std::vector<double> sc;
+    if (on_device(spatial_cross) && cudaDeviceSynchronize() != cudaSuccess) {
+        cudaGetLastError();
+        return FHD_ERR_CUDA;
+    }
+    if (!cross_to_host(*params, spatial_cross, sc)) return FHD_ERR_CUDA;
+    FILE* f = std::fopen(chk_dir(base, step).c_str(), "w");
+    if (!f) return FHD_ERR_BAD_ARG;
+    const int nc = ncross_of(*params);
+    const double h = (params->prob_hi[0] - params->prob_lo[0]) / params->n_cells[0];
+    for (int i = 0; i < params->n_cells[0]; ++i) {
+        std::fprintf(f, i == 0 ? "%g " : "%.16g ", params->prob_lo[0] + (i + 0.5) * h);
+        for (int n = 0; n < nc; ++n) std::fprintf(f, "%.16g ", sc[(size_t)i * nc + n]);
+        std::fputc('\n', f);
+    }
+    return std::fclose(f) == 0 ? FHD_OK : FHD_ERR_BAD_ARG;
 }

@@ -202,8 +202,10 @@ int plot_write(const fhd_params& prm, const char* dir, const double* host, const
 int chem_launch(const DevParams& P, const ChemParams& C, const fhd_fab& prim, const fhd_fab& source,
                 const fhd_fab* na, const fhd_fab* nb, int mode, double w, cudaStream_t s);
 // running statistics (fhd_stats.cu, exact TU)
+// lines: device scratch of stats_line_doubles(ns, n_cells[0]) doubles (FHD_STATS_CROSS only)
 int exact_stats(const DevParams& P, const fhd_fab& cu, const fhd_fab& prim, const fhd_fab mom[3],
-                const fhd_stats& st, int64_t steps, int flags, cudaStream_t s);
+                const fhd_stats& st, int64_t steps, int flags, int cross_cell, double* lines, cudaStream_t s);
+int64_t stats_line_doubles(int ns, int nx);
 int override_sync(const fhd_fab& f, const int ncell[3], cudaStream_t s, const int* periodic = nullptr);
 // wall_ghosts: also fill the first ghost layer of the wall directions (centre noise)
 int noise_fill(const DevParams& P, const fhd_fab& f, int c0, int nc, double mean, double sd, uint32_t fid0, int use_b,

@@ -15,6 +15,8 @@
 //                    variances and covariances (:438-613) and the third/fourth
 //                    moments (:616-689)
 //   [FillBoundary of cuVars and primVars]
+//   k_sum_to_line, k_spatial_cross (FHD_STATS_CROSS): the yz-averaged spatial
+//                    cross-correlations (statsStag.cpp:46-76)
 // Every pass reads and writes each operand once per point: it is bound by HBM.
 #include "fhd_launch.cuh"
 
@@ -368,8 +370,251 @@ static int stats_launch(const StatsArgs& a, bool means, bool vars, const fhd_fab
     return cuda_rc(cudaGetLastError());
 }
 
+// ---- plot_cross: the yz-averaged spatial cross-correlations ------------------------------
+// evaluateStatsStag3D's x-line averages (statsStag.cpp:46-74) and
+// EvaluateSpatialCorrelations3D (:868-1105), after the means and variances.
+//
+// k_sum_to_line: the four sumToLine results (cu and cuMeans components 0..nvars-1,
+// prim and primMeans components 1..nspecies+4), each entry (i, n) divided by
+// n_cells[1]*n_cells[2].  An entry is its y-z plane summed from 0.0 with k outer and
+// j inner, the order of a serial one-box sumToLine, so the sum is one dependent
+// chain: one thread owns one entry and adds in that order.  A warp takes 32
+// consecutive i of one component, so every row it reads is one coalesced 256-byte
+// segment, and each thread issues kLineDepth row loads ahead of its additions: the
+// kernel streams every source component once and is bound by HBM when enough rows
+// are in flight.
+constexpr int kMaxLineJobs = 2 * (5 + MAXS) + 2 * (MAXS + 4);
+constexpr int kLineDepth = 32;
+struct LineJob {
+    const double* src;   // component n of the source at valid cell (0, 0, 0)
+    double* dst;         // line entry (0, n)
+    int64_t sy, sz;      // source strides of j and k (doubles)
+    int dstride;         // line entries per i (the source's component count)
+};
+struct LineArgs {
+    LineJob job[kMaxLineJobs];
+    int njobs, nxp, nx, ny, nz;
+};
+
+static __global__ void __launch_bounds__(128) k_sum_to_line(const __grid_constant__ LineArgs a) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = t / a.nxp, i = t - c * a.nxp;
+    if (c >= a.njobs || i >= a.nx) return;
+    const LineJob& J = a.job[c];
+    const double* p = J.src + i;
+    const int64_t rows = (int64_t)a.ny * a.nz, wrap = J.sz - (int64_t)a.ny * J.sy;
+    double acc = 0.0;
+    int j = 0;
+    int64_t off = 0;   // offset of row (j, k): k*sz + j*sy
+    for (int64_t r0 = 0; r0 < rows; r0 += kLineDepth) {
+        double v[kLineDepth];
+#pragma unroll
+        for (int u = 0; u < kLineDepth; ++u) {
+            if (r0 + u < rows) v[u] = __ldg(p + off);
+            off += J.sy;
+            if (++j == a.ny) { j = 0; off += wrap; }
+        }
+#pragma unroll
+        for (int u = 0; u < kLineDepth; ++u)
+            if (r0 + u < rows) acc += v[u];
+    }
+    J.dst[(int64_t)i * J.dstride] = acc / (double)rows;
+}
+
+// k_spatial_cross: one thread per x cell i updates spatialCross(i, 0..ncross-1) in
+// the reference's statement order (a later entry reads the earlier entries' new
+// values); every thread derives the x* quantities from the same line entries, and
+// thread 0 also stores them as dataSliceMeans_xcross.  The reference's "Y_k" of the
+// lines is entry 4+k of the prim line, i.e. prim component 5+k (pressure for k = 0);
+// the update of entries 37+nspecies+1 and +2 re-applies the running-average update
+// to entries 37 and 37+nspecies-1 that were already updated this step.  Both kept.
+struct CrossArgs {
+    const double *cu, *cum, *pr, *pm;   // lines: cu/cuMeans nvars per i, prim/primMeans nspecies+4 per i
+    double* S;                          // spatialCross, ncross per i
+    double* xcross;                     // dataSliceMeans_xcross (nstats)
+    double hcv[MAXS];
+    int nx, cc, ncross;
+    double sm1, sinv;                   // stepsminusone, stepsinv
+};
+
+template <int NS>
+static __global__ void __launch_bounds__(128) k_spatial_cross(CrossArgs a) {
+    constexpr int NV = 5 + NS, NP = NS + 4, H = NS - 1;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nx) return;
+    // data_xcross (statsStag.cpp:886-911)
+    double dx[18 + 4 * NS];
+    {
+        const double *cu = a.cu + (int64_t)NV * a.cc, *cm = a.cum + (int64_t)NV * a.cc;
+        const double *pr = a.pr + (int64_t)NP * a.cc, *pm = a.pm + (int64_t)NP * a.cc;
+        dx[0] = cu[0];  dx[1] = cm[0];  dx[2] = cu[4];  dx[3] = cm[4];
+        dx[4] = cu[1];  dx[5] = cm[1];  dx[6] = cu[2];  dx[7] = cm[2];
+        dx[8] = cu[3];  dx[9] = cm[3];
+        dx[10] = pr[0]; dx[11] = pm[0]; dx[12] = pr[1]; dx[13] = pm[1];
+        dx[14] = pr[2]; dx[15] = pm[2]; dx[16] = pr[3]; dx[17] = pm[3];
+#pragma unroll
+        for (int n = 0; n < NS; ++n) {
+            dx[18 + 4 * n + 0] = cu[5 + n];
+            dx[18 + 4 * n + 1] = cm[5 + n];
+            dx[18 + 4 * n + 2] = pr[4 + n];
+            dx[18 + 4 * n + 3] = pm[4 + n];
+        }
+    }
+    if (i == 0)
+        for (int q = 0; q < 18 + 4 * NS; ++q) a.xcross[q] = dx[q];
+    // the x* quantities (:913-958)
+    const double meanrhocross = dx[1], meanuxcross = dx[11];
+    double meanYkcross[NS], delrhoYkcross[NS], delYkcross[NS];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+        meanYkcross[n] = dx[18 + 4 * n + 3];
+        delrhoYkcross[n] = dx[18 + 4 * n + 0] - dx[18 + 4 * n + 1];
+        delYkcross[n] = dx[18 + 4 * n + 2] - dx[18 + 4 * n + 3];
+    }
+    const double delrhocross = dx[0] - dx[1], delKcross = dx[2] - dx[3];
+    const double deljxcross = dx[4] - dx[5], deljycross = dx[6] - dx[7], deljzcross = dx[8] - dx[9];
+    const double delTcross = dx[16] - dx[17], delvxcross = dx[10] - dx[11];
+    double cvcross = 0.;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) cvcross = cvcross + a.hcv[l] * dx[18 + 4 * l + 1] / dx[1];
+    const double cvinvcross = 1.0 / cvcross;
+    const double qmeancross = cvcross * dx[17] - 0.5 * (dx[11] * dx[11] + dx[13] * dx[13] + dx[15] * dx[15]);
+    const double delGcross = dx[11] * (dx[4] - dx[5]) + dx[13] * (dx[6] - dx[7]) + dx[15] * (dx[8] - dx[9]);
+
+    // the quantities at x = i (:966-1004)
+    const double *cu = a.cu + (int64_t)NV * i, *cm = a.cum + (int64_t)NV * i;
+    const double *pr = a.pr + (int64_t)NP * i, *pm = a.pm + (int64_t)NP * i;
+    const double meanrho = cm[0];
+    double meanYk[NS], delrhoYk[NS], delYk[NS];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+        meanYk[n] = pm[4 + n];
+        delrhoYk[n] = cu[5 + n] - cm[5 + n];
+        delYk[n] = pr[4 + n] - pm[4 + n];
+    }
+    const double delrho = cu[0] - cm[0], delK = cu[4] - cm[4];
+    const double deljx = cu[1] - cm[1], deljy = cu[2] - cm[2], deljz = cu[3] - cm[3];
+    const double delT = pr[3] - pm[3], delvx = pr[0] - pm[0];
+    double cv = 0.;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) cv = cv + a.hcv[l] * cm[5 + l] / cm[0];
+    const double cvinv = 1.0 / cv;
+    const double qmean = cv * pm[3] - 0.5 * (pm[0] * pm[0] + pm[1] * pm[1] + pm[2] * pm[2]);
+    const double delG = pm[0] * deljx + pm[1] * deljy + pm[2] * deljz;
+
+    double* S = a.S + (int64_t)a.ncross * i;
+    const double sm1 = a.sm1, sinv = a.sinv;
+    auto upd = [&](int q, double x) { S[q] = (S[q] * sm1 + x) * sinv; };
+    // (:1007-1027)
+    upd(0, delrhocross * delrho);
+    upd(1, delKcross * delK);
+    upd(2, deljxcross * deljx);
+    upd(3, deljycross * deljy);
+    upd(4, deljzcross * deljz);
+    upd(5, deljxcross * delrho);
+    upd(6, deljxcross * delrhoYk[0]);
+    upd(7, deljxcross * delrhoYk[H]);
+    upd(8, delrhocross * delrhoYk[0]);
+    upd(9, delrhocross * delrhoYk[H]);
+    upd(10, delrhoYkcross[0] * delrho);
+    upd(11, delrhoYkcross[H] * delrho);
+    upd(12, delGcross * delG);
+    upd(13, delGcross * delK);
+    upd(14, delKcross * delG);
+    upd(15, delrhocross * delK);
+    upd(16, delKcross * delrho);
+    upd(17, delrhocross * delG);
+    upd(18, delGcross * delrho);
+    // derived correlations (:1032-1056)
+    S[19] = (cvinvcross * cvinv / (meanrhocross * meanrho)) *
+            (S[1] + S[12] - S[13] - S[14] + qmean * qmeancross * S[0] - qmeancross * S[15] - qmean * S[16] +
+             qmeancross * S[17] + qmean * S[18]);
+    S[20] = (cvinvcross / meanrhocross) * (S[16] - S[18] - qmeancross * S[0]);
+    S[21] = (1.0 / meanrhocross) * (S[5] - meanuxcross * S[0]);
+    S[22] = (1.0 / meanrhocross) * (S[6] - meanuxcross * S[8]);
+    S[23] = (1.0 / meanrhocross) * (S[7] - meanuxcross * S[9]);
+    S[24] = (1.0 / (meanrho * meanrhocross)) *
+            (S[6] - meanuxcross * S[8] - meanYk[0] * S[5] + meanuxcross * meanYk[0] * S[0]);
+    S[25] = (1.0 / (meanrho * meanrhocross)) *
+            (S[7] - meanuxcross * S[9] - meanYk[H] * S[5] + meanuxcross * meanYk[H] * S[0]);
+    // direct correlations (:1059-1093)
+    upd(26, delTcross * delT);
+    upd(27, delTcross * delrho);
+    upd(28, delTcross * delvx);
+    upd(29, delvxcross * delrho);
+    upd(30, delvxcross * delYk[0]);
+    upd(31, delvxcross * delYk[H]);
+    upd(32, delvxcross * delrhoYk[0]);
+    upd(33, delvxcross * delrhoYk[H]);
+    upd(34, delYkcross[0] * delYk[0]);
+    upd(35, delYkcross[H] * delYk[H]);
+    upd(36, delYkcross[0] * delYk[H]);
+#pragma unroll
+    for (int n = 0; n < NS; ++n) upd(37 + n, delrhoYkcross[n] * delrhoYk[n]);
+    upd(37 + NS, delrhoYkcross[H] * delrhoYk[0]);
+    // (:1096-1104)
+    double dd = (S[37] * sm1 + delrhoYkcross[0] * delrhoYk[0]) * sinv;
+    S[37 + NS + 1] = (1.0 / (meanrho * meanrhocross)) *
+                     (dd - meanYkcross[0] * S[8] - meanYk[0] * S[10] + meanYkcross[0] * meanYk[0] * S[0]);
+    dd = (S[37 + H] * sm1 + delrhoYkcross[H] * delrhoYk[H]) * sinv;
+    S[37 + NS + 2] = (1.0 / (meanrho * meanrhocross)) *
+                     (dd - meanYkcross[H] * S[9] - meanYk[H] * S[11] + meanYkcross[H] * meanYk[H] * S[0]);
+}
+
+static LineJob line_job(const fhd_fab& f, int comp, double* dst, int dstride) {
+    const int64_t sx = f.hi[0] - f.lo[0] + 1, sy = sx * (f.hi[1] - f.lo[1] + 1);
+    const int64_t sc = sy * (f.hi[2] - f.lo[2] + 1);
+    LineJob J;
+    J.src = static_cast<const double*>(f.data) + comp * sc - f.lo[2] * sy - f.lo[1] * sx - f.lo[0];
+    J.dst = dst;
+    J.sy = sx;
+    J.sz = sy;
+    J.dstride = dstride;
+    return J;
+}
+
+template <int NS>
+static int cross_launch(const DevParams& P, const fhd_fab& cu, const fhd_fab& prim, const fhd_stats& st,
+                        int cross_cell, double sm1, double sinv, double* lines, cudaStream_t s) {
+    constexpr int NV = 5 + NS, NP = NS + 4;
+    const int nx = P.n[0];
+    LineArgs la;
+    double* L[4] = {lines, lines + (int64_t)NV * nx, lines + (int64_t)2 * NV * nx,
+                    lines + (int64_t)(2 * NV + NP) * nx};
+    int q = 0;
+    for (int n = 0; n < NV; ++n) la.job[q++] = line_job(cu, n, L[0] + n, NV);
+    for (int n = 0; n < NV; ++n) la.job[q++] = line_job(st.cuMeans, n, L[1] + n, NV);
+    for (int n = 0; n < NP; ++n) la.job[q++] = line_job(prim, 1 + n, L[2] + n, NP);
+    for (int n = 0; n < NP; ++n) la.job[q++] = line_job(st.primMeans, 1 + n, L[3] + n, NP);
+    la.njobs = q;
+    la.nxp = (nx + 31) & ~31;
+    la.nx = nx;
+    la.ny = P.n[1];
+    la.nz = P.n[2];
+    const int64_t threads = (int64_t)la.nxp * q;
+    k_sum_to_line<<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(la);
+    CrossArgs ca;
+    ca.cu = L[0];
+    ca.cum = L[1];
+    ca.pr = L[2];
+    ca.pm = L[3];
+    ca.S = st.spatialCross;
+    ca.xcross = st.dataSliceMeans_xcross;
+    for (int n = 0; n < MAXS; ++n) ca.hcv[n] = n < NS ? P.hcv[n] : 0.0;
+    ca.nx = nx;
+    ca.cc = cross_cell;
+    ca.ncross = 37 + NS + 3;
+    ca.sm1 = sm1;
+    ca.sinv = sinv;
+    k_spatial_cross<NS><<<(nx + 127) / 128, 128, 0, s>>>(ca);
+    return cuda_rc(cudaGetLastError());
+}
+
+// doubles of the x-line scratch of FHD_STATS_CROSS
+int64_t stats_line_doubles(int ns, int nx) { return (int64_t)(2 * (5 + ns) + 2 * (ns + 4)) * nx; }
+
 int exact_stats(const DevParams& P, const fhd_fab& cu, const fhd_fab& prim, const fhd_fab mom[3],
-                const fhd_stats& st, int64_t steps, int flags, cudaStream_t s) {
+                const fhd_stats& st, int64_t steps, int flags, int cross_cell, double* lines, cudaStream_t s) {
     StatsArgs a;
     a.P = P;
     a.cu = view<const double>(cu);
@@ -394,12 +639,20 @@ int exact_stats(const DevParams& P, const fhd_fab& cu, const fhd_fab& prim, cons
     const bool means = flags & FHD_STATS_MEANS, vars = flags & FHD_STATS_VARS;
     a.mom3 = vars && (flags & FHD_STATS_MOM3);
     a.mom4 = vars && (flags & FHD_STATS_MOM4);
+    int rc;
     switch (P.ns) {
-        case 1: return stats_launch<1>(a, means, vars, st.cuMeans, st.primMeans, st.cuVars, st.primVars, s);
-        case 2: return stats_launch<2>(a, means, vars, st.cuMeans, st.primMeans, st.cuVars, st.primVars, s);
-        case 3: return stats_launch<3>(a, means, vars, st.cuMeans, st.primMeans, st.cuVars, st.primVars, s);
-        case 4: return stats_launch<4>(a, means, vars, st.cuMeans, st.primMeans, st.cuVars, st.primVars, s);
+        case 1: rc = stats_launch<1>(a, means, vars, st.cuMeans, st.primMeans, st.cuVars, st.primVars, s); break;
+        case 2: rc = stats_launch<2>(a, means, vars, st.cuMeans, st.primMeans, st.cuVars, st.primVars, s); break;
+        case 3: rc = stats_launch<3>(a, means, vars, st.cuMeans, st.primMeans, st.cuVars, st.primVars, s); break;
+        case 4: rc = stats_launch<4>(a, means, vars, st.cuMeans, st.primMeans, st.cuVars, st.primVars, s); break;
         default: return FHD_ERR_UNSUPPORTED;
+    }
+    if (rc || !(flags & FHD_STATS_CROSS)) return rc;
+    switch (P.ns) {
+        case 1: return cross_launch<1>(P, cu, prim, st, cross_cell, a.sm1, a.sinv, lines, s);
+        case 2: return cross_launch<2>(P, cu, prim, st, cross_cell, a.sm1, a.sinv, lines, s);
+        case 3: return cross_launch<3>(P, cu, prim, st, cross_cell, a.sm1, a.sinv, lines, s);
+        default: return cross_launch<4>(P, cu, prim, st, cross_cell, a.sm1, a.sinv, lines, s);
     }
 }
 

@@ -81,6 +81,8 @@ class Params:
     T_init: float = 273.0
     rhobar: tuple = (0.5, 0.5)
     ngc: int = 2
+    # plot_cross's cell x* (common::cross_cell; statsStag.cpp:868-1105)
+    cross_cell: int = 0
 
     @property
     def nvars(self):
@@ -158,6 +160,7 @@ class Params:
                 getattr(p, name)[d] = getattr(self, name)[d]
         p.rho0 = self.rho0
         p.T_init = self.T_init
+        p.cross_cell = self.cross_cell
         for i in range(MAX_SPECIES):
             p.rhobar[i] = self.rhobar[i] if i < len(self.rhobar) else 0.0
         return p
@@ -332,7 +335,8 @@ def to_inputs(p: "Params") -> str:
              f"k_B = {_fmt(float(p.k_B))}", f"Runiv = {_fmt(float(p.Runiv))}", row("grav", p.grav),
              f"algorithm_type = {p.algorithm_type}", f"visc_type = {p.visc_type}",
              f"advection_type = {p.advection_type}", f"transport_type = {p.transport_type}",
-             f"stoch_stress_form = {p.stoch_stress_form}", f"seed = {p.seed}", "prob_type = 1"]
+             f"stoch_stress_form = {p.stoch_stress_form}", f"seed = {p.seed}", "prob_type = 1",
+             f"cross_cell = {p.cross_cell}"]
     if p.zeta_ratio >= 0:
         lines.append(f"zeta_ratio = {_fmt(float(p.zeta_ratio))}")
     for key in ("bc_vel_lo", "bc_vel_hi", "bc_mass_lo", "bc_mass_hi", "bc_therm_lo", "bc_therm_hi"):
@@ -392,7 +396,7 @@ def parse_inputs(text: str, base: Params | None = None) -> Params:
         if key in kv:
             upd[key] = float(kv[key][0])
     for key in ("algorithm_type", "visc_type", "advection_type", "transport_type",
-                "stoch_stress_form", "seed"):
+                "stoch_stress_form", "seed", "cross_cell"):
         if key in kv:
             upd[key] = int(kv[key][0])
     # chemistry keys (chemistry_functions.cpp:45-124); avogadro overrides Runiv

@@ -103,6 +103,11 @@ inline int plot_covars = 0;
 inline int plot_mom3 = 0;
 inline int plot_mom4 = 0;
 inline int plot_deltaY_dir = -1;  // common_functions.cpp:620
+// yz-averaged spatial cross-correlations at x = cross_cell (common_functions.cpp:345, 619)
+inline int plot_cross = 0;
+inline int cross_cell = 0;
+// a restart zeroes the statistics instead of reading them (Checkpoint.cpp:346, 500)
+inline int reset_stats = 0;
 // Physical boundaries (common_namespace.H:150-185, read at common_functions.cpp:800-900).
 // A direction whose bc_vel_lo and bc_vel_hi are both -1 is periodic (the default
 // here; the staggered decks set every bc_vel); otherwise both sides are walls:
@@ -243,14 +248,19 @@ inline fhd_params params_from_globals() {
     p.rho0 = common::rho0;
     p.T_init = common::T_init[0];
     for (int s = 0; s < FHD_MAX_SPECIES; ++s) p.rhobar[s] = common::rhobar[s];
+    p.cross_cell = common::cross_cell;
     return p;
 }
 
 struct Runtime {
     fhd_ctx* ctx = nullptr;
     uint64_t fill_calls = 0;  // stream ids of successive MultiFabFillRandom* calls
+    // device mirror of the host vectors spatialCross3D and dataSliceMeans_xcross
+    double* cross = nullptr;
+    size_t cross_doubles = 0;
     ~Runtime() {
         if (ctx) fhd_destroy(ctx);
+        if (cross) cudaFree(cross);
     }
 };
 inline Runtime& runtime() {
@@ -262,6 +272,9 @@ inline void finalize() {
     Runtime& r = runtime();
     if (r.ctx) fhd_destroy(r.ctx);
     r.ctx = nullptr;
+    if (r.cross) cudaFree(r.cross);
+    r.cross = nullptr;
+    r.cross_doubles = 0;
 }
 
 // The process-wide context, created from the globals on first use.
@@ -586,9 +599,12 @@ inline void WritePlotFileStag(int step, const fhd::amrex_compat::Real time, cons
 // evaluateStatsStag3D (statsStag.cpp:10-77): the running means (plot_means) and
 // the variances, covariances and third / fourth moments (plot_vars or
 // plot_covars; plot_mom3 / plot_mom4) with sample count `steps`, each followed by
-// the reference's FillBoundary.  Without surface coverage (theta*) and without
-// the yz-averaged spatial cross-correlations (plot_cross), which are not on this
-// path: those arguments are accepted and left untouched.
+// the reference's FillBoundary, then with plot_cross the yz-averaged spatial
+// cross-correlations at x = cross_cell into the host vectors spatialCross3D
+// (n_cells[0] * ncross) and dataSliceMeans_xcross (2*nvars + 8 + 2*nspecies),
+// through a device mirror (copied in and out on the context's stream; the call
+// then waits for the stream).  Without surface coverage (theta*): those
+// arguments are accepted and left untouched.
 inline void evaluateStatsStag3D(fhd::amrex_compat::MultiFab& cons, fhd::amrex_compat::MultiFab& consMean,
                                 fhd::amrex_compat::MultiFab& consVar, fhd::amrex_compat::MultiFab& prim_in,
                                 fhd::amrex_compat::MultiFab& primMean, fhd::amrex_compat::MultiFab& primVar,
@@ -602,15 +618,37 @@ inline void evaluateStatsStag3D(fhd::amrex_compat::MultiFab& cons, fhd::amrex_co
                                 fhd::amrex_compat::MultiFab& mom4, fhd::amrex_compat::MultiFab& /*theta*/,
                                 fhd::amrex_compat::MultiFab& /*thetaMean*/, fhd::amrex_compat::MultiFab& /*thetaVar*/,
                                 fhd::amrex_compat::MultiFab& /*thetacoVar*/,
-                                fhd::amrex_compat::Vector<fhd::amrex_compat::Real>& /*dataSliceMeans_xcross*/,
-                                fhd::amrex_compat::Vector<fhd::amrex_compat::Real>& /*spatialCross3D*/,
-                                const int /*ncross*/, const fhd::amrex_compat::Box& /*domain*/, const int steps,
+                                fhd::amrex_compat::Vector<fhd::amrex_compat::Real>& dataSliceMeans_xcross,
+                                fhd::amrex_compat::Vector<fhd::amrex_compat::Real>& spatialCross3D,
+                                const int ncross, const fhd::amrex_compat::Box& /*domain*/, const int steps,
                                 const fhd::amrex_compat::Geometry& /*geom*/) {
     using namespace fhd::ref;
     const int flags = (common::plot_means ? FHD_STATS_MEANS : 0) |
                       ((common::plot_vars || common::plot_covars) ? FHD_STATS_VARS : 0) |
-                      (common::plot_mom3 ? FHD_STATS_MOM3 : 0) | (common::plot_mom4 ? FHD_STATS_MOM4 : 0);
+                      (common::plot_mom3 ? FHD_STATS_MOM3 : 0) | (common::plot_mom4 ? FHD_STATS_MOM4 : 0) |
+                      (common::plot_cross ? FHD_STATS_CROSS : 0);
     if (!flags) return;
+    const size_t nsc = (size_t)common::n_cells[0] * ncross, nxc = dataSliceMeans_xcross.size();
+    if (common::plot_cross) {
+        if (ncross != fhd_spatial_cross_ncross(common::nspecies) || spatialCross3D.size() < nsc ||
+            (int)nxc < fhd_spatial_cross_nstats(common::nspecies))
+            fail("evaluateStatsStag3D", FHD_ERR_BAD_ARG);
+        Runtime& r = runtime();
+        if (r.cross_doubles < nsc + nxc) {
+            if (r.cross) cudaFree(r.cross);
+            r.cross = nullptr;
+            r.cross_doubles = 0;
+            if (cudaMalloc(reinterpret_cast<void**>(&r.cross), (nsc + nxc) * sizeof(double)) != cudaSuccess) {
+                cudaGetLastError();
+                fail("evaluateStatsStag3D", FHD_ERR_OOM);
+            }
+            r.cross_doubles = nsc + nxc;
+        }
+        const cudaStream_t cs = static_cast<cudaStream_t>(stream);
+        if (cudaMemcpyAsync(r.cross, spatialCross3D.data(), nsc * sizeof(double), cudaMemcpyHostToDevice, cs) !=
+            cudaSuccess)
+            fail("evaluateStatsStag3D", FHD_ERR_CUDA);
+    }
     fhd_stats st;
     std::memset(&st, 0, sizeof(st));
     st.cuMeans = consMean.fab();
@@ -626,16 +664,41 @@ inline void evaluateStatsStag3D(fhd::amrex_compat::MultiFab& cons, fhd::amrex_co
         st.cumomMeans[d] = cumomMean[d].fab();
         st.cumomVars[d] = cumomVar[d].fab();
     }
+    if (common::plot_cross) {
+        st.spatialCross = runtime().cross;
+        st.dataSliceMeans_xcross = runtime().cross + nsc;
+    }
     fhd_fab vl[3], mom[3];
     fabs_of(vel, vl);
     fabs_of(cumom, mom);
     check(fhd_stats_stag(context(), cons.fab(), prim_in.fab(), vl, mom, &st, steps, flags), "evaluateStatsStag3D");
+    if (common::plot_cross) {
+        const cudaStream_t cs = static_cast<cudaStream_t>(stream);
+        if (cudaMemcpyAsync(spatialCross3D.data(), st.spatialCross, nsc * sizeof(double), cudaMemcpyDeviceToHost,
+                            cs) != cudaSuccess ||
+            cudaMemcpyAsync(dataSliceMeans_xcross.data(), st.dataSliceMeans_xcross, nxc * sizeof(double),
+                            cudaMemcpyDeviceToHost, cs) != cudaSuccess ||
+            cudaStreamSynchronize(cs) != cudaSuccess)
+            fail("evaluateStatsStag3D", FHD_ERR_CUDA);
+    }
+}
+
+// WriteSpatialCross3D (writePlotFileStag.cpp:528-549): spatialCross<step, 9 digits>
+// in the working directory.
+inline void WriteSpatialCross3D(const fhd::amrex_compat::Vector<fhd::amrex_compat::Real>& spatialCross, int step,
+                                const fhd::amrex_compat::Geometry& /*geom*/, const int ncross) {
+    using namespace fhd::ref;
+    const fhd_params p = params_from_globals();
+    if (ncross != fhd_spatial_cross_ncross(p.nspecies) || spatialCross.size() < (size_t)p.n_cells[0] * ncross)
+        fail("WriteSpatialCross3D", FHD_ERR_BAD_ARG);
+    check(fhd_write_spatial_cross(&p, "spatialCross", step, spatialCross.data()), "WriteSpatialCross3D");
 }
 
 // WriteCheckPoint (Checkpoint.cpp:28-257): chk<step, 9 digits>/ in the working
-// directory with the state and every defined statistics MultiFab.  The
-// surface-coverage, cross-correlation and turbulence-forcing records are not
-// written (none of them exists on this path); the noise needs no generator state.
+// directory with the state, every defined statistics MultiFab and, with
+// plot_cross, spatialCrossVec in the Header.  The surface-coverage, 1-D / 2-D
+// cross-correlation and turbulence-forcing records are not written (none of
+// them exists on this path); the noise needs no generator state.
 inline void WriteCheckPoint(int step, const fhd::amrex_compat::Real time, int statsCount,
                             const fhd::amrex_compat::Geometry& /*geom*/, const fhd::amrex_compat::MultiFab& cu,
                             const fhd::amrex_compat::MultiFab& cuMeans, const fhd::amrex_compat::MultiFab& cuVars,
@@ -653,8 +716,8 @@ inline void WriteCheckPoint(int step, const fhd::amrex_compat::Real time, int st
                             const fhd::amrex_compat::MultiFab& /*surfcovVars*/,
                             const fhd::amrex_compat::MultiFab& /*surfcovcoVars*/,
                             const fhd::amrex_compat::MultiFab& /*spatialCrossMF*/,
-                            const fhd::amrex_compat::Vector<fhd::amrex_compat::Real>& /*spatialCrossVec*/,
-                            int /*ncross*/, TurbForcingComp& /*turbforce*/) {
+                            const fhd::amrex_compat::Vector<fhd::amrex_compat::Real>& spatialCrossVec,
+                            int ncross, TurbForcingComp& /*turbforce*/) {
     using namespace fhd::ref;
     fhd_stats st;
     std::memset(&st, 0, sizeof(st));
@@ -675,6 +738,11 @@ inline void WriteCheckPoint(int step, const fhd::amrex_compat::Real time, int st
     fabs_of(cumom, mom);
     fabs_of(vel, vl);
     const fhd_params p = params_from_globals();
+    if (common::plot_cross) {
+        if (ncross != fhd_spatial_cross_ncross(p.nspecies) || spatialCrossVec.size() < (size_t)p.n_cells[0] * ncross)
+            fail("WriteCheckPoint", FHD_ERR_BAD_ARG);
+        st.spatialCross = const_cast<double*>(spatialCrossVec.data());
+    }
     check(fhd_write_checkpoint(&p, "chk", step, time, statsCount, cu.fab(), mom, prim.fab(), vl, &st),
           "WriteCheckPoint");
 }
@@ -683,7 +751,10 @@ inline void WriteCheckPoint(int step, const fhd::amrex_compat::Real time, int st
 // reference's shapes on `domain` (device memory, 2 ghost cells for the state and
 // the cell-centred means/variances, none for the others; mom3 / mom4 only with
 // plot_mom3 / plot_mom4), reads chk<common::restart, 9 digits>/ into them and sets
-// step to the saved step + 1, time and statsCount.
+// step to the saved step + 1, time and statsCount.  With plot_cross the Header's
+// spatialCrossVec is read into spatialCrossVec (n_cells[0] * ncross entries); with
+// reset_stats the statistics and spatialCrossVec are zeroed instead of read
+// (Checkpoint.cpp:343-358, 498-519).
 inline void ReadCheckPoint(int& step, fhd::amrex_compat::Real& time, int& statsCount,
                            fhd::amrex_compat::Geometry& /*geom*/, const fhd::amrex_compat::Box& domain,
                            fhd::amrex_compat::MultiFab& cu, fhd::amrex_compat::MultiFab& cuMeans,
@@ -700,7 +771,7 @@ inline void ReadCheckPoint(int& step, fhd::amrex_compat::Real& time, int& statsC
                            fhd::amrex_compat::MultiFab& /*surfcovMeans*/, fhd::amrex_compat::MultiFab& /*surfcovVars*/,
                            fhd::amrex_compat::MultiFab& /*surfcovcoVars*/,
                            fhd::amrex_compat::MultiFab& /*spatialCrossMF*/,
-                           fhd::amrex_compat::Vector<fhd::amrex_compat::Real>& /*spatialCrossVec*/, int /*ncross*/,
+                           fhd::amrex_compat::Vector<fhd::amrex_compat::Real>& spatialCrossVec, int ncross,
                            TurbForcingComp& /*turbforce*/, fhd::amrex_compat::BoxArray& ba,
                            fhd::amrex_compat::DistributionMapping& /*dmap*/) {
     using namespace fhd::ref;
@@ -745,10 +816,30 @@ inline void ReadCheckPoint(int& step, fhd::amrex_compat::Real& time, int& statsC
     fabs_of(cumom, mom);
     fabs_of(vel, vl);
     const fhd_params p = params_from_globals();
+    const bool reset = common::reset_stats == 1;
+    if (common::plot_cross) {
+        if (ncross != fhd_spatial_cross_ncross(ns)) fail("ReadCheckPoint", FHD_ERR_BAD_ARG);
+        spatialCrossVec.resize((size_t)common::n_cells[0] * ncross);
+        if (!reset) st.spatialCross = spatialCrossVec.data();
+    }
     double t = 0.0;
-    check(fhd_read_checkpoint(&p, "chk", common::restart, &step, &t, &statsCount, cu.fab(), mom, prim.fab(), vl, &st),
+    check(fhd_read_checkpoint(&p, "chk", common::restart, &step, &t, &statsCount, cu.fab(), mom, prim.fab(), vl,
+                              reset ? nullptr : &st),
           "ReadCheckPoint");
     time = t;
+    if (reset) {
+        for (fhd::amrex_compat::MultiFab* m : {&cuMeans, &cuVars, &primMeans, &primVars, &coVars})
+            m->setVal(0.0);
+        for (int d = 0; d < 3; ++d) {
+            velMeans[d].setVal(0.0);
+            velVars[d].setVal(0.0);
+            cumomMeans[d].setVal(0.0);
+            cumomVars[d].setVal(0.0);
+        }
+        if (common::plot_mom3) mom3.setVal(0.0);
+        if (common::plot_mom4) mom4.setVal(0.0);
+        if (common::plot_cross) spatialCrossVec.assign(spatialCrossVec.size(), 0.0);
+    }
 }
 
 // MultiFabFillRandom (MultiFabFillRandom.cpp:5-31): N(0, variance) in one

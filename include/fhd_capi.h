@@ -138,6 +138,10 @@ typedef struct {
      * rhobar): the reservoirs' default pressure. */
     double rho0, T_init;
     double rhobar[FHD_MAX_SPECIES];
+    /* The cell x* of the yz-averaged spatial cross-correlations (deck key cross_cell,
+     * 0 <= cross_cell < n_cells[0] when fhd_stats_stag is given FHD_STATS_CROSS,
+     * as main_driver.cpp:249-251 requires). */
+    int cross_cell;
 } fhd_params;
 
 /* Injected Gaussian noise for one RK3 step: the "A" and "B" white-noise fields
@@ -394,8 +398,16 @@ int fhd_batch_autotune(fhd_batch* batch, int reps, double* ms, int* best);
  * reference's time loop calls after every step (main_driver.cpp:1235-1241):
  * EvaluateStatsMeans (statsStag.cpp:200-365) and EvaluateVarsCoVarsMom3
  * (:367-691), each followed by the reference's FillBoundary of the cell-centred
- * means/variances.  Without surface coverage (nspec_surfcov = 0) and without
- * the yz-averaged spatial cross-correlations (plot_cross).  Fabs have the
+ * means/variances, and with FHD_STATS_CROSS the yz-averaged spatial
+ * cross-correlations of plot_cross (:46-76): sumToLine of cu, cuMeans and
+ * components 1..nspecies+4 of prim and primMeans, each divided by
+ * n_cells[1]*n_cells[2] (every line entry summed over its y-z plane in the order
+ * k outer, j inner), and EvaluateSpatialCorrelations3D (:868-1105) at x* =
+ * params.cross_cell.  `spatialCross` (device, n_cells[0] * fhd_spatial_cross_ncross
+ * doubles, entry i*ncross + n, the reference's spatialCrossVec) is updated in
+ * place; `dataSliceMeans_xcross` (device, fhd_spatial_cross_nstats doubles)
+ * receives the line averages at x* that the reference appends to its crossMeans
+ * file.  Without surface coverage (nspec_surfcov = 0).  Fabs have the
  * reference's shapes (main_driver.cpp:646-714): cuMeans/cuVars nvars comps,
  * primMeans nprimvars+3 comps, primVars nprimvars+5 comps, coVars 26 comps,
  * mom3/mom4 nvars+1 comps, all cell-centred; velMeans/velVars/cumomMeans/
@@ -406,7 +418,13 @@ int fhd_batch_autotune(fhd_batch* batch, int reps, double* ms, int* best);
 typedef struct {
     fhd_fab cuMeans, cuVars, primMeans, primVars, coVars, mom3, mom4;
     fhd_fab velMeans[3], velVars[3], cumomMeans[3], cumomVars[3];
+    double* spatialCross;            /* FHD_STATS_CROSS only; else may be NULL */
+    double* dataSliceMeans_xcross;   /* FHD_STATS_CROSS only; else may be NULL */
 } fhd_stats;
+/* entries per x cell of spatialCross: 37 + nspecies + 3 (main_driver.cpp:283) */
+int fhd_spatial_cross_ncross(int nspecies);
+/* entries of dataSliceMeans_xcross: 2*nvars + 8 + 2*nspecies (main_driver.cpp:279) */
+int fhd_spatial_cross_nstats(int nspecies);
 
 /* ---- plotfiles --------------------------------------------------------------------
  * WritePlotFileStag (writePlotFileStag.cpp:7-527, declared
@@ -447,13 +465,24 @@ int fhd_plotfile_pack(fhd_ctx* ctx, int flags, fhd_fab out, fhd_fab cu, const fh
  * finished first).  The read fills fabs of the same
  * shapes and returns step = saved step + 1, the time and statsCount, as the
  * reference's restart does; the in-kernel noise needs no saved generator state
- * (it is a function of seed and step). */
+ * (it is a function of seed and step).  With plot_cross, stats->spatialCross
+ * (host or device, n_cells[0] * fhd_spatial_cross_ncross doubles) is written into
+ * the Header after the BoxArray at 16 significant digits, as the reference keeps
+ * spatialCrossVec there (Checkpoint.cpp:112-118), and read back from it
+ * (:343-358).  For the reference's reset_stats, read with stats = NULL and zero
+ * the statistics. */
 int fhd_write_checkpoint(const fhd_params* params, const char* chk_base, int step, double time, int stats_count,
                          fhd_fab cu, const fhd_fab cumom[3], fhd_fab prim, const fhd_fab vel[3],
                          const fhd_stats* stats);
 int fhd_read_checkpoint(const fhd_params* params, const char* chk_base, int restart, int* step, double* time,
                         int* stats_count, fhd_fab cu, const fhd_fab cumom[3], fhd_fab prim, const fhd_fab vel[3],
                         const fhd_stats* stats);
+
+/* WriteSpatialCross3D (writePlotFileStag.cpp:528-549): the text file
+ * <base><step, 9 digits> (the reference's base is "spatialCross"), one line per x
+ * cell with its centre and the ncross entries of spatialCross (host or device
+ * memory), in the reference's number formatting. */
+int fhd_write_spatial_cross(const fhd_params* params, const char* base, int step, const double* spatial_cross);
 
 /* pack, copy to the host and write the plotfile directory (blocks on the stream;
  * allocates and frees a temporary device buffer of the packed size) */
@@ -462,8 +491,8 @@ int fhd_write_plotfile_stag(fhd_ctx* ctx, const char* plot_base_name, int step, 
                             fhd_fab zeta, const fhd_stats* stats);
 
 /* flags of fhd_stats_stag (the reference's plot_means, plot_vars/plot_covars,
- * plot_mom3, plot_mom4 inputs) */
-enum { FHD_STATS_MEANS = 1, FHD_STATS_VARS = 2, FHD_STATS_MOM3 = 4, FHD_STATS_MOM4 = 8 };
+ * plot_mom3, plot_mom4 and plot_cross inputs) */
+enum { FHD_STATS_MEANS = 1, FHD_STATS_VARS = 2, FHD_STATS_MOM3 = 4, FHD_STATS_MOM4 = 8, FHD_STATS_CROSS = 16 };
 
 /* One statistics update with sample count `steps` (the reference's statsCount,
  * 1 for the first sample after a reset): stepsminusone = steps - 1 and

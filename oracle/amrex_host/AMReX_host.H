@@ -21,7 +21,12 @@
 //    their standard normals from a caller-installed source (injected noise),
 //    and return mean + stddev * z as a normal draw would;
 //  * ParmParse reads "key = values" lines from an in-memory table;
-//  * ParallelDescriptor is a single process.
+//  * ParallelDescriptor is a single process;
+//  * sumToLine(mf, icomp, ncomp, domain, dir, local) returns, for every index m
+//    along dir and component n, the sum of mf over the valid box's plane at m in
+//    the host vector's entry m*ncomp + n (the layout the reference indexes),
+//    accumulated from 0.0 in the box's loop order (z slowest, x fastest), so
+//    that for the x line each entry sums its plane with k outer and j inner.
 #pragma once
 
 #include <algorithm>
@@ -133,6 +138,7 @@ namespace Math {
 template <class T> inline T abs(T x) { return std::abs(x); }
 template <int P, class T> inline T powi(T x) { T r = 1; for (int q = 0; q < P; ++q) r *= x; return r; }
 inline double pi() { return 3.14159265358979323846; }
+template <class T> inline T floor(T x) { return std::floor(x); }
 }  // namespace Math
 template <class T> inline const T& min(const T& a, const T& b) { return std::min(a, b); }
 template <class T> inline const T& max(const T& a, const T& b) { return std::max(a, b); }
@@ -783,6 +789,7 @@ inline double second() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 template <class T> inline void ReduceRealSum(T&, int = 0) {}
+inline void ReduceRealSum(Real*, int, int = 0) {}
 template <class T> inline void ReduceRealMax(T&, int = 0) {}
 template <class T> inline void ReduceRealMin(T&, int = 0) {}
 template <class T> inline void ReduceIntSum(T&, int = 0) {}
@@ -876,6 +883,22 @@ public:
         table()[full(k)] = {os.str()};
     }
 };
+
+// ---- sumToLine (one box, one process: the reduction over ranks is the identity) -------
+inline Gpu::HostVector<Real> sumToLine(const MultiFab& mf, int icomp, int ncomp, const Box& domain, int direction,
+                                       bool /*local*/ = false) {
+    Gpu::HostVector<Real> hv((size_t)domain.length(direction) * ncomp, 0.0);
+    const Box b = mf.boxArray()[0];
+    const auto a = mf.const_array(0);
+    for (int n = 0; n < ncomp; ++n)
+        for (int k = b.smallEnd(2); k <= b.bigEnd(2); ++k)
+            for (int j = b.smallEnd(1); j <= b.bigEnd(1); ++j)
+                for (int i = b.smallEnd(0); i <= b.bigEnd(0); ++i) {
+                    const int m = (direction == 0 ? i : direction == 1 ? j : k) - domain.smallEnd(direction);
+                    hv[(size_t)m * ncomp + n] += a(i, j, k, icomp + n);
+                }
+    return hv;
+}
 
 // ---- VisMF and plotfiles: not part of the step ------------------------------------------
 struct VisMF {

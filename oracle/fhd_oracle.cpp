@@ -50,6 +50,7 @@ struct P {
     int stoich_R[FHD_MAX_REACTIONS][MAXS], stoich_PR[FHD_MAX_REACTIONS][MAXS];
     double rate_const[FHD_MAX_REACTIONS], alpha_param[FHD_MAX_REACTIONS], beta_param[FHD_MAX_REACTIONS];
     double T0_chem = 0, avogadro = 0;
+    int cross_cell = 0;   // plot_cross's x* (common::cross_cell)
 } g;
 
 struct Fab {
@@ -1028,6 +1029,7 @@ int orc_set_params(const fhd_params* p) {
     for (int d = 0; d < 3; ++d) {
         g.n[d] = p->n_cells[d];
         g.dx[d] = (p->prob_hi[d] - p->prob_lo[d]) / p->n_cells[d];
+        g.cross_cell = p->cross_cell;
         g.grav[d] = p->grav[d];
     }
     g.k_B = p->k_B;
@@ -1294,10 +1296,131 @@ int orc_fill_random_normal(fhd_fab mf_, int scomp, int ncomp, double mean, doubl
     return FHD_OK;
 }
 
-// evaluateStatsStag3D's per-cell statistics (statsStag.cpp:10-77) without surface
-// coverage or spatial correlations: EvaluateStatsMeans (:200-365) then
+// sumToLine(mf, icomp, ncomp, domain, 0): for every x index i and component n the
+// sum of mf(i, j, k, icomp + n) over the y-z plane, from 0.0 with k outer and j
+// inner (a serial one-box AMReX sumToLine), in entry i*ncomp + n, then divided by
+// n_cells[1]*n_cells[2] as evaluateStatsStag3D does (statsStag.cpp:56-69).
+static std::vector<double> line_average(const Fab& f, int icomp, int ncomp) {
+    const int* N = g.n;
+    std::vector<double> hv((size_t)N[0] * ncomp, 0.0);
+    for (int n = 0; n < ncomp; ++n)
+        for (int k = 0; k < N[2]; ++k)
+            for (int j = 0; j < N[1]; ++j)
+                for (int i = 0; i < N[0]; ++i) hv[(size_t)i * ncomp + n] += f(i, j, k, icomp + n);
+    for (double& v : hv) v /= N[1] * N[2];
+    return hv;
+}
+
+// EvaluateSpatialCorrelations3D (statsStag.cpp:868-1105) on the line averages of
+// cu, cuMeans (components 0..nvars-1) and prim, primMeans (1..nspecies+4): the
+// x* quantities from the lines at cross_cell, then every x cell's running
+// averages and derived correlations in the reference's statement order.  As in
+// the reference, the lines' "Y_k" are prim components 5+k (pressure for k = 0),
+// and entries 37+nspecies+1 and +2 re-apply the update of entries 37 and
+// 37+nspecies-1.
+static void spatial_cross(const Fab& cu, const Fab& cumeans, const Fab& prim, const Fab& primmeans, double* S_,
+                          double* xcross, int64_t steps) {
+    const int ns = g.ns, nvars = 5 + ns, nprims = ns + 4, ncross = 37 + ns + 3, H = ns - 1;
+    const std::vector<double> cu_avg = line_average(cu, 0, nvars), cumeans_avg = line_average(cumeans, 0, nvars);
+    const std::vector<double> prim_avg = line_average(prim, 1, nprims), primmeans_avg = line_average(primmeans, 1, nprims);
+    const double stepsminusone = steps - 1.;
+    const double stepsinv = 1. / steps;
+    const int cc = g.cross_cell;
+    double* dx = xcross;
+    dx[0] = cu_avg[0 + nvars * cc];
+    dx[1] = cumeans_avg[0 + nvars * cc];
+    dx[2] = cu_avg[4 + nvars * cc];
+    dx[3] = cumeans_avg[4 + nvars * cc];
+    for (int d = 0; d < 3; ++d) {
+        dx[4 + 2 * d] = cu_avg[1 + d + nvars * cc];
+        dx[5 + 2 * d] = cumeans_avg[1 + d + nvars * cc];
+    }
+    for (int q = 0; q < 4; ++q) {
+        dx[10 + 2 * q] = prim_avg[q + nprims * cc];
+        dx[11 + 2 * q] = primmeans_avg[q + nprims * cc];
+    }
+    for (int n = 0; n < ns; ++n) {
+        dx[18 + 4 * n + 0] = cu_avg[5 + n + nvars * cc];
+        dx[18 + 4 * n + 1] = cumeans_avg[5 + n + nvars * cc];
+        dx[18 + 4 * n + 2] = prim_avg[4 + n + nprims * cc];
+        dx[18 + 4 * n + 3] = primmeans_avg[4 + n + nprims * cc];
+    }
+    const double meanrhocross = dx[1], meanuxcross = dx[11];
+    double meanYkcross[MAXS], delrhoYkcross[MAXS], delYkcross[MAXS];
+    for (int n = 0; n < ns; ++n) {
+        meanYkcross[n] = dx[18 + 4 * n + 3];
+        delrhoYkcross[n] = dx[18 + 4 * n + 0] - dx[18 + 4 * n + 1];
+        delYkcross[n] = dx[18 + 4 * n + 2] - dx[18 + 4 * n + 3];
+    }
+    const double delrhocross = dx[0] - dx[1], delKcross = dx[2] - dx[3];
+    const double deljxcross = dx[4] - dx[5], deljycross = dx[6] - dx[7], deljzcross = dx[8] - dx[9];
+    const double delTcross = dx[16] - dx[17], delvxcross = dx[10] - dx[11];
+    double cvcross = 0.;
+    for (int l = 0; l < ns; ++l) cvcross = cvcross + g.hcv[l] * dx[18 + 4 * l + 1] / dx[1];
+    const double cvinvcross = 1.0 / cvcross;
+    const double qmeancross = cvcross * dx[17] - 0.5 * (dx[11] * dx[11] + dx[13] * dx[13] + dx[15] * dx[15]);
+    const double delGcross = dx[11] * (dx[4] - dx[5]) + dx[13] * (dx[6] - dx[7]) + dx[15] * (dx[8] - dx[9]);
+    for (int i = 0; i < g.n[0]; ++i) {
+        const double* c = &cu_avg[(size_t)nvars * i];
+        const double* cm = &cumeans_avg[(size_t)nvars * i];
+        const double* pr = &prim_avg[(size_t)nprims * i];
+        const double* pm = &primmeans_avg[(size_t)nprims * i];
+        const double meanrho = cm[0];
+        double meanYk[MAXS], delrhoYk[MAXS], delYk[MAXS];
+        for (int n = 0; n < ns; ++n) {
+            meanYk[n] = pm[4 + n];
+            delrhoYk[n] = c[5 + n] - cm[5 + n];
+            delYk[n] = pr[4 + n] - pm[4 + n];
+        }
+        const double delrho = c[0] - cm[0], delK = c[4] - cm[4];
+        const double deljx = c[1] - cm[1], deljy = c[2] - cm[2], deljz = c[3] - cm[3];
+        const double delT = pr[3] - pm[3], delvx = pr[0] - pm[0];
+        double cv = 0.;
+        for (int l = 0; l < ns; ++l) cv = cv + g.hcv[l] * cm[5 + l] / cm[0];
+        const double cvinv = 1.0 / cv;
+        const double qmean = cv * pm[3] - 0.5 * (pm[0] * pm[0] + pm[1] * pm[1] + pm[2] * pm[2]);
+        const double delG = pm[0] * deljx + pm[1] * deljy + pm[2] * deljz;
+        double* S = S_ + (size_t)ncross * i;
+        auto upd = [&](int q, double x) { S[q] = (S[q] * stepsminusone + x) * stepsinv; };
+        const double pairs[19] = {delrhocross * delrho, delKcross * delK, deljxcross * deljx, deljycross * deljy,
+                                  deljzcross * deljz, deljxcross * delrho, deljxcross * delrhoYk[0],
+                                  deljxcross * delrhoYk[H], delrhocross * delrhoYk[0], delrhocross * delrhoYk[H],
+                                  delrhoYkcross[0] * delrho, delrhoYkcross[H] * delrho, delGcross * delG,
+                                  delGcross * delK, delKcross * delG, delrhocross * delK, delKcross * delrho,
+                                  delrhocross * delG, delGcross * delrho};
+        for (int q = 0; q < 19; ++q) upd(q, pairs[q]);
+        S[19] = (cvinvcross * cvinv / (meanrhocross * meanrho)) *
+                (S[1] + S[12] - S[13] - S[14] + qmean * qmeancross * S[0] - qmeancross * S[15] - qmean * S[16] +
+                 qmeancross * S[17] + qmean * S[18]);
+        S[20] = (cvinvcross / meanrhocross) * (S[16] - S[18] - qmeancross * S[0]);
+        S[21] = (1.0 / meanrhocross) * (S[5] - meanuxcross * S[0]);
+        S[22] = (1.0 / meanrhocross) * (S[6] - meanuxcross * S[8]);
+        S[23] = (1.0 / meanrhocross) * (S[7] - meanuxcross * S[9]);
+        S[24] = (1.0 / (meanrho * meanrhocross)) *
+                (S[6] - meanuxcross * S[8] - meanYk[0] * S[5] + meanuxcross * meanYk[0] * S[0]);
+        S[25] = (1.0 / (meanrho * meanrhocross)) *
+                (S[7] - meanuxcross * S[9] - meanYk[H] * S[5] + meanuxcross * meanYk[H] * S[0]);
+        const double direct[11] = {delTcross * delT, delTcross * delrho, delTcross * delvx, delvxcross * delrho,
+                                   delvxcross * delYk[0], delvxcross * delYk[H], delvxcross * delrhoYk[0],
+                                   delvxcross * delrhoYk[H], delYkcross[0] * delYk[0], delYkcross[H] * delYk[H],
+                                   delYkcross[0] * delYk[H]};
+        for (int q = 0; q < 11; ++q) upd(26 + q, direct[q]);
+        for (int n = 0; n < ns; ++n) upd(37 + n, delrhoYkcross[n] * delrhoYk[n]);
+        upd(37 + ns, delrhoYkcross[H] * delrhoYk[0]);
+        double dd = (S[37] * stepsminusone + delrhoYkcross[0] * delrhoYk[0]) * stepsinv;
+        S[37 + ns + 1] = (1.0 / (meanrho * meanrhocross)) *
+                         (dd - meanYkcross[0] * S[8] - meanYk[0] * S[10] + meanYkcross[0] * meanYk[0] * S[0]);
+        dd = (S[37 + H] * stepsminusone + delrhoYkcross[H] * delrhoYk[H]) * stepsinv;
+        S[37 + ns + 2] = (1.0 / (meanrho * meanrhocross)) *
+                         (dd - meanYkcross[H] * S[9] - meanYk[H] * S[11] + meanYkcross[H] * meanYk[H] * S[0]);
+    }
+}
+
+// evaluateStatsStag3D's statistics (statsStag.cpp:10-77) without surface
+// coverage: EvaluateStatsMeans (:200-365) then
 // FillBoundary of the cell means, EvaluateVarsCoVarsMom3 (:367-691) then
-// FillBoundary of the cell variances, each loop in the reference's order.
+// FillBoundary of the cell variances, each loop in the reference's order, then
+// with FHD_STATS_CROSS the spatial cross-correlations (:46-76).
 // flags as fhd_stats_stag.
 int orc_stats_stag(fhd_fab cu_, fhd_fab prim_, const fhd_fab* mom_, const fhd_stats* st, int64_t steps, int flags) {
     const int* N = g.n;
@@ -1498,6 +1621,11 @@ int orc_stats_stag(fhd_fab cu_, fhd_fab prim_, const fhd_fab* mom_, const fhd_st
         }
         fill_boundary(cuvars);
         fill_boundary(primvars);
+    }
+    if (flags & FHD_STATS_CROSS) {
+        if (g.cross_cell < 0 || g.cross_cell > N[0] - 1 || !st->spatialCross || !st->dataSliceMeans_xcross)
+            return FHD_ERR_BAD_ARG;
+        spatial_cross(cu, cumeans, prim, primmeans, st->spatialCross, st->dataSliceMeans_xcross, steps);
     }
     return FHD_OK;
 }

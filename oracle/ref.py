@@ -65,6 +65,7 @@ def lib():
         L.fhdref_wall_composition.argtypes = [i, P(d), P(d)]
         L.fhdref_wall_state.argtypes = [i, P(d)]
         L.fhdref_set_reservoir_draws.argtypes = [vp, i]
+        L.fhdref_eval_stats3d.argtypes = [vp, vp, pp, pp, pp, P(i), pp, vp, vp, i, i]
         _lib = L
     return _lib
 
@@ -322,3 +323,29 @@ def max_acoustic_cfl(st, dt):
 
 
 SQRT2 = math.sqrt(2.0)
+
+
+def eval_stats(st, stats, steps, flags):
+    """evaluateStatsStag3D (statsStag.cpp:10-76) of the reference on host state
+    ``st`` and host StatsState ``stats`` (mom3 / mom4 allocated; spatialCross with
+    FHD_STATS_CROSS), with the deck's plot_* keys set from ``flags`` (the bits of
+    fhd_stats_stag) and cross_cell from the Params."""
+    p = st.p
+    extra = (f"plot_means = {int(bool(flags & 1))}\nplot_vars = {int(bool(flags & 2))}\n"
+             f"plot_covars = {int(bool(flags & 2))}\nplot_mom3 = {int(bool(flags & 4))}\n"
+             f"plot_mom4 = {int(bool(flags & 8))}\nplot_cross = {int(bool(flags & 16))}\n")
+    global _params
+    _chk(lib().fhdref_init((p.to_inputs() + extra).encode()), "init")
+    _params = None
+    cells = [stats.cuMeans, stats.cuVars, stats.primMeans, stats.primVars, stats.coVars, stats.mom3, stats.mom4]
+    ng = (C.c_int * 7)(*[m.ngrow for m in cells])
+    faces = stats.velMeans + stats.velVars + stats.cumomMeans + stats.cumomVars
+    if stats.spatialCross is not None:
+        sc, xc = stats.spatialCross, stats.dataSliceMeans_xcross
+    else:
+        sc = torch.zeros(p.n_cells[0], 37 + p.nspecies + 3, dtype=torch.float64)
+        xc = torch.zeros(2 * p.nvars + 8 + 2 * p.nspecies, dtype=torch.float64)
+    _chk(lib().fhdref_eval_stats3d(_ptr(st.cu.arr), _ptr(st.prim.arr), _ptrs([m.arr for m in st.vel]),
+                                   _ptrs([m.arr for m in st.cumom]), _ptrs([m.arr for m in cells]), ng,
+                                   _ptrs([m.arr for m in faces]), _ptr(sc), _ptr(xc), sc.shape[1], int(steps)),
+         "evaluateStatsStag3D")

@@ -12,6 +12,7 @@
 // Parameters come from an inputs-deck text read by the reference's own
 // InitializeCommonNamespace / InitializeCompressibleNamespace /
 // InitializeChemistryNamespace and GetHcGas, in main_driver.cpp:43-88's order.
+#include <algorithm>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -387,6 +388,47 @@ int fhdref_chemistry_source(double dt, double dV, double* prim, double* source, 
         wrap(s, source, IntVect(0), nprimvars, g);
         wrap(rc, ranchem, IntVect(0), nreaction, g);
         compute_compressible_chemistry_source_CLE(dt, dV, p, s, rc);
+    });
+}
+
+// evaluateStatsStag3D (statsStag.cpp:10-76) with the deck's plot_means / plot_vars /
+// plot_covars / plot_mom3 / plot_mom4 / plot_cross / cross_cell and no surface
+// coverage.  cells[7] = cuMeans, cuVars, primMeans, primVars, coVars, mom3, mom4
+// (nvars, nvars, nprimvars+3, nprimvars+5, 26, nvars+1, nvars+1 components) with
+// ghost widths ng[7]; faces[12] = velMeans, velVars, cumomMeans, cumomVars (three
+// each, no ghosts); spatial_cross (n_cells[0]*ncross) and xcross
+// (2*nvars+8+2*nspecies) are the reference's spatialCross3D and
+// dataSliceMeans_xcross vectors, updated in place.
+int fhdref_eval_stats3d(double* cu, double* prim, double* const* vel, double* const* mom, double* const* cells,
+                        const int* ng, double* const* faces, double* spatial_cross, double* xcross, int ncross,
+                        int steps) {
+    return guarded([&] {
+        const int g = ngc[0];
+        MultiFab c, p, cm, cv, pm, pv, cov, m3, m4, th, thm, thv, thc;
+        std::array<MultiFab, 3> v, m, vm, vv, mm, mv;
+        wrap(c, cu, IntVect(0), nvars, g);
+        wrap(p, prim, IntVect(0), nprimvars, g);
+        wrap3(v, vel, 1, g, true);
+        wrap3(m, mom, 1, g, true);
+        wrap(cm, cells[0], IntVect(0), nvars, ng[0]);
+        wrap(cv, cells[1], IntVect(0), nvars, ng[1]);
+        wrap(pm, cells[2], IntVect(0), nprimvars + 3, ng[2]);
+        wrap(pv, cells[3], IntVect(0), nprimvars + 5, ng[3]);
+        wrap(cov, cells[4], IntVect(0), 26, ng[4]);
+        wrap(m3, cells[5], IntVect(0), nvars + 1, ng[5]);
+        wrap(m4, cells[6], IntVect(0), nvars + 1, ng[6]);
+        wrap3(vm, faces, 1, 0, true);
+        wrap3(vv, faces + 3, 1, 0, true);
+        wrap3(mm, faces + 6, 1, 0, true);
+        wrap3(mv, faces + 9, 1, 0, true);
+        const int nstats = 2 * nvars + 8 + 2 * nspecies;
+        Vector<Real> sc(spatial_cross, spatial_cross + (size_t)n_cells[0] * ncross);
+        Vector<Real> xc(xcross, xcross + nstats);
+        const Box domain(IntVect(0, 0, 0), IntVect(n_cells[0] - 1, n_cells[1] - 1, n_cells[2] - 1));
+        evaluateStatsStag3D(c, cm, cv, p, pm, pv, v, vm, vv, m, mm, mv, cov, m3, m4, th, thm, thv, thc, xc, sc,
+                            ncross, domain, steps, g_geom);
+        std::copy(sc.begin(), sc.end(), spatial_cross);
+        std::copy(xc.begin(), xc.end(), xcross);
     });
 }
 

@@ -19,8 +19,10 @@
 //       n1..n1+n2-1 on them; writes the final state as `run` does
 //   reference_driver stats <n> <nsteps> <seed> <dt> <out.bin>
 //       nsteps RK3 steps, evaluateStatsStag3D after each (plot_means, plot_vars,
-//       plot_mom3, plot_mom4); writes cuMeans, cuVars, primMeans, primVars,
-//       coVars, mom3, mom4, velMeans, velVars, cumomMeans, cumomVars
+//       plot_mom3, plot_mom4, plot_cross at cross_cell n/2); writes cuMeans,
+//       cuVars, primMeans, primVars, coVars, mom3, mom4, velMeans, velVars,
+//       cumomMeans, cumomVars, spatialCrossVec and dataSliceMeans_xcross, and
+//       WriteSpatialCross3D's spatialCross<nsteps> in the working directory
 //   reference_driver massfrac <n>
 //       start from a state with a zero mass fraction: calculateTransportCoeffs
 //       must report it through the abort handler (exit code 3)
@@ -298,6 +300,8 @@ static int cmd_chk(int n, int n1, int n2, int seed, double dt, const char* out) 
 static int cmd_stats(int n, int nsteps, int seed, double dt, const char* out) {
     set_argon(n, seed);
     common::plot_means = common::plot_vars = common::plot_mom3 = common::plot_mom4 = 1;
+    common::plot_cross = 1;
+    common::cross_cell = n / 2;
     State s(n, Arena::Device, true);
     s.init();
     const Box dom(IntVect(0, 0, 0), IntVect(n - 1, n - 1, n - 1));
@@ -311,14 +315,18 @@ static int cmd_stats(int n, int nsteps, int seed, double dt, const char* out) {
         cmm[d].define(convert(dom, face_nodal(d)), 1, 0);
         cmv[d].define(convert(dom, face_nodal(d)), 1, 0);
     }
-    Vector<Real> slice, cross;
+    // main_driver.cpp:279-285
+    const int ncross = 37 + common::nspecies + 3;
+    Vector<Real> slice(2 * nv + 8 + 2 * common::nspecies, 0.0), cross((size_t)n * ncross, 0.0);
     TurbForcingComp turb;
     for (int step = 0; step < nsteps; ++step) {
         RK3stepStag(s.cu, s.cumom, s.prim, s.vel, s.source, s.eta, s.zeta, s.kappa, s.chi, s.D, s.faceflux,
                     s.edgeflux_x, s.edgeflux_y, s.edgeflux_z, s.cenflux, s.ranchem, s.geom, dt, step, turb);
         evaluateStatsStag3D(s.cu, cuMeans, cuVars, s.prim, primMeans, primVars, s.vel, vm, vv, s.cumom, cmm, cmv,
-                            coVars, mom3, mom4, theta, theta, theta, theta, slice, cross, 0, dom, step + 1, s.geom);
+                            coVars, mom3, mom4, theta, theta, theta, theta, slice, cross, ncross, dom, step + 1,
+                            s.geom);
     }
+    WriteSpatialCross3D(cross, nsteps, s.geom, ncross);
     FILE* f = std::fopen(out, "wb");
     if (!f) return 2;
     for (const MultiFab* m : {&cuMeans, &cuVars, &primMeans, &primVars, &coVars, &mom3, &mom4}) write_all(f, *m);
@@ -326,6 +334,8 @@ static int cmd_stats(int n, int nsteps, int seed, double dt, const char* out) {
     for (int d = 0; d < 3; ++d) write_all(f, vv[d]);
     for (int d = 0; d < 3; ++d) write_all(f, cmm[d]);
     for (int d = 0; d < 3; ++d) write_all(f, cmv[d]);
+    std::fwrite(cross.data(), sizeof(Real), cross.size(), f);
+    std::fwrite(slice.data(), sizeof(Real), slice.size(), f);
     std::fclose(f);
     fhd::ref::finalize();
     return 0;

@@ -51,3 +51,29 @@ def test_checkpoint_refuses_other_shapes(tmp_path):
         read_checkpoint(q, base, 1, StagState(q))
     with pytest.raises(FhdError):
         read_checkpoint(p, base, 2, StagState(p))   # no such checkpoint
+
+
+def test_checkpoint_keeps_spatial_cross_in_the_header(tmp_path):
+    """With plot_cross the Header carries spatialCrossVec after the BoxArray, one
+    value per line at 16 significant digits (Checkpoint.cpp:112-118), and the
+    restart reads those decimal values back (:343-358)."""
+    p = mixture4((5, 4, 6), dx=8e-6)
+    st, _ = randomized(p, 3)
+    stats = StatsState(p, cross=True)
+    g = torch.Generator().manual_seed(4)
+    stats.spatialCross.copy_(torch.randn(stats.spatialCross.shape, generator=g, dtype=torch.float64) * 1e-7)
+    base = str(tmp_path / "chk")
+    path = write_checkpoint(p, base, 3, 1e-10, st, stats, stats_count=3)
+    lines = open(os.path.join(path, "Header")).read().split("\n")
+    end = lines.index(")")
+    vals = [v for v in lines[end + 1:] if v]
+    want = [f"{v:.16g}" for v in stats.spatialCross.flatten().tolist()]
+    assert vals == want
+    back = StatsState(p, cross=True)
+    step, _, count = read_checkpoint(p, base, 3, StagState(p), back)
+    assert (step, count) == (4, 3)
+    assert back.spatialCross.flatten().tolist() == [float(v) for v in want]
+    # without plot_cross nothing follows the BoxArray
+    path = write_checkpoint(p, base, 4, 1e-10, st, StatsState(p), stats_count=3)
+    lines = open(os.path.join(path, "Header")).read().split("\n")
+    assert not [v for v in lines[lines.index(")") + 1:] if v]

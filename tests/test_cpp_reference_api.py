@@ -168,34 +168,42 @@ def test_reference_driver_checkpoint_restart_equals_uninterrupted_run(driver, tm
 @pytest.mark.gpu
 def test_reference_driver_statistics_equal_c_abi_statistics(driver, tmp_path):
     """evaluateStatsStag3D through the reference-named layer (plot_means, plot_vars,
-    plot_mom3, plot_mom4) after every step equals fhd_stats_stag bit for bit."""
+    plot_mom3, plot_mom4, plot_cross) after every step equals fhd_stats_stag bit
+    for bit, and its WriteSpatialCross3D file equals fhd_write_spatial_cross's."""
+    from fhdex_b200 import capi
     from fhdex_b200.context import Context
     from fhdex_b200.stats import StatsState
     n, nsteps, seed = 8, 3, 13
-    p = argon(n, dx=8e-6, seed=seed)
+    p = argon(n, dx=8e-6, seed=seed).replace(cross_cell=n // 2)
     dt = stable_dt(p)
     out = str(tmp_path / "stats.bin")
+    run_dir = tmp_path / "run"
+    run_dir.mkdir()
     r = subprocess.run([driver, "stats", str(n), str(nsteps), str(seed), repr(dt), out],
-                       capture_output=True, text=True, timeout=300)
+                       capture_output=True, text=True, timeout=300, cwd=str(run_dir))
     assert r.returncode == 0, (r.returncode, r.stderr)
     ctx = Context(p)
     st = StagState(p, "cuda")
     ctx.init_state(st)
-    stats = StatsState(p, "cuda")
+    stats = StatsState(p, "cuda", cross=True)
     for step in range(nsteps):
         ctx.rk3_step(st, dt, step, aux=True)
-        ctx.stats_stag(st, stats, step + 1, 15)
+        ctx.stats_stag(st, stats, step + 1, 15 | capi.STATS_CROSS)
     torch.cuda.synchronize()
+    stats.write_spatial_cross(nsteps, str(tmp_path / "spatialCross"))
+    fname = f"spatialCross{nsteps:09d}"
+    assert open(run_dir / fname).read() == open(tmp_path / fname).read()
     mfs = [stats.cuMeans, stats.cuVars, stats.primMeans, stats.primVars, stats.coVars, stats.mom3, stats.mom4]
     mfs += stats.velMeans + stats.velVars + stats.cumomMeans + stats.cumomVars
+    arrs = [m.arr for m in mfs] + [stats.spatialCross, stats.dataSliceMeans_xcross]
     raw = np.fromfile(out, dtype=np.float64)
     off = 0
     bad = []
-    for k, m in enumerate(mfs):
-        size = m.arr.numel()
-        got = torch.from_numpy(raw[off:off + size].copy()).view(m.arr.shape)
+    for k, a in enumerate(arrs):
+        size = a.numel()
+        got = torch.from_numpy(raw[off:off + size].copy()).view(a.shape)
         off += size
-        if not torch.equal(got, m.arr.cpu()):
+        if not torch.equal(got, a.cpu()):
             bad.append(k)
     assert off == raw.size
     assert not bad, bad

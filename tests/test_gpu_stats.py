@@ -74,3 +74,50 @@ def test_running_variances_match_theory_in_equilibrium():
     print({k: f"{v:.4f}" for k, v in ratios.items()})
     for k, r in ratios.items():
         assert r == pytest.approx(1.0, abs=0.03), (k, r)
+
+
+@pytest.mark.parametrize("make,cc", [(lambda: argon((40, 7, 5), dx=8e-6), 17),
+                                     (lambda: mixture4((33, 6, 6), dx=8e-6), 32),
+                                     (lambda: argon((64, 48, 40), dx=8e-6), 0)])
+def test_spatial_cross_bitwise_against_oracle_and_reference(oracle, make, cc):
+    """FHD_STATS_CROSS (k_sum_to_line + k_spatial_cross after the per-cell passes):
+    spatialCross and dataSliceMeans_xcross bit for bit against the oracle over
+    four samples, and against the reference's own evaluateStatsStag3D where
+    oracle/_ref is built.  The sizes give x lines that are not a multiple of the
+    warp and y-z planes that are not a multiple of the kernel's load depth."""
+    from oracle import ref as R
+    p = make().replace(cross_cell=cc)
+    flags = 15 | capi.STATS_CROSS
+    host = StatsState(p, cross=True)
+    theirs = StatsState(p, cross=True) if R.available() else None
+    dev = StatsState(p, "cuda", cross=True)
+    ctx = Context(p)
+    for s in range(1, 5):
+        st = perturbed_state(oracle, p, seed=400 + s, amp=0.05)
+        assert oracle.stats_stag(st, host, s, flags) == 0
+        if theirs is not None:
+            R.eval_stats(st, theirs, s, flags)
+        ctx.stats_stag(st.clone(device="cuda"), dev, s, flags)
+    torch.cuda.synchronize()
+    assert ctx.status() == 0
+    assert torch.equal(dev.spatialCross.cpu(), host.spatialCross)
+    assert torch.equal(dev.dataSliceMeans_xcross.cpu(), host.dataSliceMeans_xcross)
+    bad = [n for n, m in dev.named().items() if not torch.equal(m.arr.cpu(), host.named()[n].arr)]
+    assert not bad, bad
+    if theirs is not None:
+        assert torch.equal(host.spatialCross, theirs.spatialCross)
+        assert torch.equal(host.dataSliceMeans_xcross, theirs.dataSliceMeans_xcross)
+    assert host.spatialCross[:, 0].abs().max() > 0
+
+
+def test_spatial_cross_rejects_bad_arguments():
+    p = argon((6, 5, 4), dx=8e-6).replace(cross_cell=6)
+    ctx = Context(p)
+    st = StagState(p, "cuda", aux=False)
+    ctx.init_state(st)
+    with pytest.raises(capi.FhdError):
+        ctx.stats_stag(st, StatsState(p, "cuda", cross=True), 1, 1 | capi.STATS_CROSS)   # x* outside the box
+    q = p.replace(cross_cell=2)
+    ctx = Context(q)
+    with pytest.raises(capi.FhdError):
+        ctx.stats_stag(st, StatsState(q, "cuda"), 1, 1 | capi.STATS_CROSS)              # no spatialCross buffers

@@ -5,6 +5,7 @@ mean_s = (mean_{s-1} (s-1) + x_s) / s and var_s = (var_{s-1} (s-1) + (x_s - mean
 with the fluctuation of the current sample taken about the current mean."""
 import numpy as np
 import pytest
+import torch
 
 from fhdex_b200 import capi
 from fhdex_b200.params import argon, mixture4
@@ -88,3 +89,67 @@ def test_variances_without_means_are_rejected(oracle):
     p = argon(4, dx=8e-6)
     st = perturbed_state(oracle, p, seed=3)
     assert oracle.stats_stag(st, StatsState(p), 1, capi.STATS_VARS) == capi.FHD_ERR_BAD_ARG
+
+
+@pytest.fixture(scope="module")
+def ref():
+    from oracle import ref as R
+    if not R.available():
+        pytest.skip("oracle/_ref was not built")
+    return R
+
+
+@pytest.mark.parametrize("flags", [15 | capi.STATS_CROSS, capi.STATS_MEANS | capi.STATS_CROSS, 15])
+@pytest.mark.parametrize("make,cc", [(lambda: argon((7, 5, 4), dx=8e-6), 3),
+                                     (lambda: mixture4((6, 4, 5), dx=8e-6), 0),
+                                     (lambda: mixture4((5, 3, 4), dx=8e-6), 4)])
+def test_oracle_statistics_equal_the_reference(oracle, ref, make, cc, flags):
+    """The oracle's evaluateStatsStag3D (per-cell statistics and, with
+    FHD_STATS_CROSS, the yz-averaged spatial cross-correlations at x* = cross_cell)
+    bit for bit against the reference's own statsStag.cpp over five samples."""
+    p = make().replace(cross_cell=cc)
+    mine, theirs = StatsState(p, cross=True), StatsState(p, cross=True)
+    for s in range(1, 6):
+        st = perturbed_state(oracle, p, seed=300 + s, amp=0.05)
+        assert oracle.stats_stag(st, mine, s, flags) == 0
+        ref.eval_stats(st, theirs, s, flags)
+    bad = [n for n, m in mine.named().items() if not torch.equal(m.arr, theirs.named()[n].arr)]
+    assert not bad, bad
+    if flags & capi.STATS_CROSS:
+        assert torch.equal(mine.spatialCross, theirs.spatialCross)
+        assert torch.equal(mine.dataSliceMeans_xcross, theirs.dataSliceMeans_xcross)
+        assert mine.spatialCross[:, 0].abs().max() > 0 and torch.isfinite(mine.spatialCross).all()
+    else:
+        assert not mine.spatialCross.any()
+
+
+def test_spatial_cross_line_averages(oracle):
+    """dataSliceMeans_xcross holds the y-z averages at x* of rho, rhoE, the
+    cell-centred momenta, the velocities, T and, per species, rhoY_k and the prim
+    component 5 + k (the reference's lines read pressure as the first "Y_k")."""
+    p = mixture4((6, 4, 5), dx=8e-6).replace(cross_cell=2)
+    stats = StatsState(p, cross=True)
+    st = perturbed_state(oracle, p, seed=7, amp=0.05)
+    assert oracle.stats_stag(st, stats, 1, capi.STATS_MEANS | capi.STATS_CROSS) == 0
+    x = stats.dataSliceMeans_xcross.numpy()
+    cu, pr = st.cu.valid().numpy()[:, :, :, 2], st.prim.valid().numpy()[:, :, :, 2]
+    np.testing.assert_allclose(x[0], cu[0].mean(), rtol=1e-14)
+    np.testing.assert_allclose(x[2], cu[4].mean(), rtol=1e-14)
+    np.testing.assert_allclose(x[4], cu[1].mean(), rtol=1e-12, atol=1e-30)
+    np.testing.assert_allclose(x[16], pr[4].mean(), rtol=1e-14)
+    for k in range(p.nspecies):
+        np.testing.assert_allclose(x[18 + 4 * k], cu[5 + k].mean(), rtol=1e-14)
+        np.testing.assert_allclose(x[18 + 4 * k + 2], pr[5 + k].mean(), rtol=1e-14)
+    # one sample: the running means of rho, rhoE, the momenta and T equal the
+    # sample (the velocity means are derived from the momentum and density means),
+    # so the conserved-variable correlations are zero
+    for q in (0, 2, 4, 6, 8, 16):
+        assert x[q] == x[q + 1], q
+    assert not stats.spatialCross[:, :19].any()
+
+
+def test_spatial_cross_rejects_a_cross_cell_outside_the_box(oracle):
+    p = argon((4, 3, 3), dx=8e-6).replace(cross_cell=4)
+    stats = StatsState(p, cross=True)
+    st = perturbed_state(oracle, p, seed=1)
+    assert oracle.stats_stag(st, stats, 1, capi.STATS_MEANS | capi.STATS_CROSS) == capi.FHD_ERR_BAD_ARG
