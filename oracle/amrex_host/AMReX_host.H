@@ -37,7 +37,11 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <functional>
+#include <iomanip>
+#include <numeric>
+#include <sstream>
 #include <limits>
 #include <iostream>
 #include <map>
@@ -175,6 +179,8 @@ public:
     IntVect() : vect{0, 0, 0} {}
     IntVect(int i, int j, int k) : vect{i, j, k} {}
     explicit IntVect(int v) : vect{v, v, v} {}
+    explicit IntVect(const int* v) : vect{v[0], v[1], v[2]} {}
+    explicit IntVect(const std::vector<int>& v) : vect{v[0], v[1], v[2]} {}
     int& operator[](int d) { return vect[d]; }
     const int& operator[](int d) const { return vect[d]; }
     bool operator==(const IntVect& o) const { return vect[0] == o[0] && vect[1] == o[1] && vect[2] == o[2]; }
@@ -332,6 +338,7 @@ public:
     std::vector<Box> boxes;
     BoxArray() = default;
     explicit BoxArray(const Box& b) : boxes{b} {}
+    BoxArray(const Box* b, size_t n) : boxes(b, b + n) {}
     void define(const Box& b) { boxes = {b}; }
     int size() const { return (int)boxes.size(); }
     const Box& operator[](int i) const { return boxes[i]; }
@@ -350,6 +357,7 @@ class DistributionMapping {
 public:
     DistributionMapping() = default;
     explicit DistributionMapping(const BoxArray&, int = 1) {}
+    explicit DistributionMapping(std::vector<int>&&) {}
     int operator[](int) const { return 0; }
 };
 
@@ -388,6 +396,10 @@ public:
     Geometry() = default;
     Geometry(const Box& dom, const RealBox& rb, int c, const Array<int, 3>& is_per) { define(dom, rb, c, is_per); }
     Geometry(const Box& dom, const RealBox* rb, int c, const int* is_per) {
+        Array<int, 3> p{is_per[0], is_per[1], is_per[2]};
+        define(dom, *rb, c, p);
+    }
+    void define(const Box& dom, const RealBox* rb, int c, const int* is_per) {
         Array<int, 3> p{is_per[0], is_per[1], is_per[2]};
         define(dom, *rb, c, p);
     }
@@ -460,6 +472,7 @@ public:
     std::vector<Real> own;
     FArrayBox() = default;
     FArrayBox(const Box& b, int ncomp) { resize(b, ncomp); }
+    FArrayBox(const Box& b, int ncomp, Real* p) { wrap(p, b, ncomp); }
     void resize(const Box& b, int ncomp) {
         bx = b;
         nc = ncomp;
@@ -532,6 +545,9 @@ public:
     MultiFab() = default;
     MultiFab(const BoxArray& b, const DistributionMapping& d, int nc, int ng) { define(b, d, nc, ng); }
     MultiFab(const BoxArray& b, const DistributionMapping& d, int nc, const IntVect& ng) { define(b, d, nc, ng); }
+    MultiFab(const BoxArray& b, const DistributionMapping& d, int nc, int ng, const struct MFInfo&) {
+        define(b, d, nc, ng);
+    }
     MultiFab(const MultiFab&) = delete;
     MultiFab& operator=(const MultiFab&) = delete;
     MultiFab(MultiFab&&) = default;
@@ -690,6 +706,12 @@ public:
         FillBoundary(scomp, nc, per);
     }
     // nodal periodic duplicates: the high boundary point takes the low one's value
+    // Multi-box machinery that only ComputeAverages.cpp's slice, pencil and
+    // column functions name (not part of the host build: a call reports itself).
+    std::vector<Array4<Real const>> const_arrays() const { Abort("MultiFab::const_arrays: multi-box API"); }
+    void setFab(int, FArrayBox&&) { Abort("MultiFab::setFab: multi-box API"); }
+    void ParallelAdd(const MultiFab&) { Abort("MultiFab::ParallelAdd: multi-box API"); }
+    void ParallelCopy(const MultiFab&, int = 0, int = 0, int = 0) { Abort("MultiFab::ParallelCopy: multi-box API"); }
     void OverrideSync(const Periodicity& per) {
         const Box v = ba[0];
         auto a = fab.array();
@@ -883,6 +905,56 @@ public:
         table()[full(k)] = {os.str()};
     }
 };
+
+// ---- names of ComputeAverages.cpp's multi-box functions (not part of the host build) ----
+struct MFInfo {
+    MFInfo& SetAlloc(bool) { return *this; }
+};
+struct ReduceOpSum {};
+template <class Op, class T, class F>
+FArrayBox ReduceToPlane(int, const Box&, const MultiFab&, F&&) {
+    Abort("ReduceToPlane: multi-box API");
+}
+
+// ---- file names and plotfiles -------------------------------------------------------------
+inline std::string Concatenate(const std::string& root, int num, int mindigits = 5) {
+    std::ostringstream os;
+    os << root << std::setfill('0') << std::setw(mindigits) << num;
+    return os.str();
+}
+struct CoordSys {
+    enum CoordType { undef = -1, cartesian = 0, RZ = 1, SPHERICAL = 2 };
+};
+// WriteSingleLevelPlotfile does not write files here: it keeps the last plotfile
+// MultiFab's valid region (Array4 order, component slowest), its names, time and
+// step, which the harness reads back (the on-disk format is AMReX's, not the
+// reference's).
+struct PlotfileCapture {
+    std::string name;
+    std::vector<Real> data;
+    std::vector<std::string> names;
+    Real time = 0;
+    int step = 0;
+};
+inline PlotfileCapture& plotfile_capture() {
+    static PlotfileCapture c;
+    return c;
+}
+inline void WriteSingleLevelPlotfile(const std::string& name, const MultiFab& mf, const Vector<std::string>& names,
+                                     const Geometry&, Real time, int step) {
+    PlotfileCapture& c = plotfile_capture();
+    c.name = name;
+    c.names.assign(names.begin(), names.end());
+    c.time = time;
+    c.step = step;
+    c.data.clear();
+    const Box v = mf.boxArray()[0];
+    const auto a = mf.const_array(0);
+    for (int n = 0; n < mf.nComp(); ++n)
+        for (int k = v.lo[2]; k <= v.hi[2]; ++k)
+            for (int j = v.lo[1]; j <= v.hi[1]; ++j)
+                for (int i = v.lo[0]; i <= v.hi[0]; ++i) c.data.push_back(a(i, j, k, n));
+}
 
 // ---- sumToLine (one box, one process: the reduction over ranks is the identity) -------
 inline Gpu::HostVector<Real> sumToLine(const MultiFab& mf, int icomp, int ncomp, const Box& domain, int direction,

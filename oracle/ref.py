@@ -66,6 +66,9 @@ def lib():
         L.fhdref_wall_state.argtypes = [i, P(d)]
         L.fhdref_set_reservoir_draws.argtypes = [vp, i]
         L.fhdref_eval_stats3d.argtypes = [vp, vp, pp, pp, pp, P(i), pp, vp, vp, i, i]
+        L.fhdref_write_spatial_cross.argtypes = [vp, i, i]
+        L.fhdref_plotfile.argtypes = [vp, pp, vp, pp, vp, vp, vp, pp, P(i), pp, i, d, vp, C.c_long, C.c_char_p, i,
+                                      P(i)]
         _lib = L
     return _lib
 
@@ -349,3 +352,44 @@ def eval_stats(st, stats, steps, flags):
                                    _ptrs([m.arr for m in st.cumom]), _ptrs([m.arr for m in cells]), ng,
                                    _ptrs([m.arr for m in faces]), _ptr(sc), _ptr(xc), sc.shape[1], int(steps)),
          "evaluateStatsStag3D")
+
+
+def plotfile(st, stats, flags, step=0, time=0.0):
+    """WritePlotFileStag (writePlotFileStag.cpp:7-527) of the reference on host
+    state ``st`` (with eta, kappa, zeta) and host StatsState ``stats``: returns the
+    composed plotfile MultiFab's valid cells as a (ncomp, nz, ny, nx) tensor and
+    its component names.  ``flags`` are the FHD_PLOT_* bits (plot_means 1,
+    plot_vars 2, plot_covars 4, plot_mom3 8, plot_mom4 16, plot_deltaY_dir x/y/z
+    32/64/128)."""
+    p = st.p
+    dy = {32: 0, 64: 1, 128: 2}.get(flags & 224, -1)
+    extra = (f"plot_means = {int(bool(flags & 1))}\nplot_vars = {int(bool(flags & 2))}\n"
+             f"plot_covars = {int(bool(flags & 4))}\nplot_mom3 = {int(bool(flags & 8))}\n"
+             f"plot_mom4 = {int(bool(flags & 16))}\nplot_deltaY_dir = {dy}\n")
+    global _params
+    _chk(lib().fhdref_init((p.to_inputs() + extra).encode()), "init")
+    _params = None
+    cells = [stats.cuMeans, stats.cuVars, stats.primMeans, stats.primVars, stats.coVars, stats.mom3, stats.mom4]
+    ng = (C.c_int * 7)(*[m.ngrow for m in cells])
+    faces = stats.velMeans + stats.velVars + stats.cumomMeans + stats.cumomVars
+    N = p.n_cells
+    cap = 512 * N[0] * N[1] * N[2]
+    out = torch.zeros(cap, dtype=torch.float64)
+    names = C.create_string_buffer(1 << 16)
+    nc = C.c_int()
+    _chk(lib().fhdref_plotfile(_ptr(st.cu.arr), _ptrs([m.arr for m in st.cumom]), _ptr(st.prim.arr),
+                               _ptrs([m.arr for m in st.vel]), _ptr(st.eta.arr), _ptr(st.kappa.arr),
+                               _ptr(st.zeta.arr), _ptrs([m.arr for m in cells]), ng, _ptrs([m.arr for m in faces]),
+                               int(step), float(time), _ptr(out), cap, names, len(names), C.byref(nc)),
+         "WritePlotFileStag")
+    ncomp = nc.value
+    data = out[:ncomp * N[0] * N[1] * N[2]].view(ncomp, N[2], N[1], N[0])
+    return data, names.value.decode().split("\n")[:ncomp]
+
+
+def write_spatial_cross(p, spatial_cross, step):
+    """The reference's WriteSpatialCross3D (writePlotFileStag.cpp:528-549): writes
+    spatialCross<step, 9 digits> in the current working directory."""
+    init(p)
+    sc = spatial_cross.contiguous()
+    _chk(lib().fhdref_write_spatial_cross(_ptr(sc), int(step), sc.shape[1]), "WriteSpatialCross3D")

@@ -432,6 +432,61 @@ int fhdref_eval_stats3d(double* cu, double* prim, double* const* vel, double* co
     });
 }
 
+// WritePlotFileStag (writePlotFileStag.cpp:7-527) with the deck's plot_means /
+// plot_vars / plot_covars / plot_mom3 / plot_mom4 / plot_deltaY_dir, no surface
+// coverage: the plotfile MultiFab it composes (valid cells, component slowest)
+// into out (capacity cap doubles) and its component names, each ended by '\n',
+// into names (capacity ncap bytes); *ncomp receives the component count.  The
+// state, eta, kappa and zeta have ngc ghosts; cells / ng / faces as
+// fhdref_eval_stats3d.
+int fhdref_plotfile(double* cu, double* const* mom, double* prim, double* const* vel, double* eta, double* kappa,
+                    double* zeta, double* const* cells, const int* ng, double* const* faces, int step, double time,
+                    double* out, long cap, char* names, int ncap, int* ncomp) {
+    return guarded([&] {
+        const int g = ngc[0];
+        MultiFab c, p, e, k, z, cm, cv, pm, pv, cov, m3, m4, sc, scm, scv, scc;
+        std::array<MultiFab, 3> v, m, vm, vv, mm, mv;
+        wrap(c, cu, IntVect(0), nvars, g);
+        wrap(p, prim, IntVect(0), nprimvars, g);
+        wrap(e, eta, IntVect(0), 1, g);
+        wrap(k, kappa, IntVect(0), 1, g);
+        wrap(z, zeta, IntVect(0), 1, g);
+        wrap3(v, vel, 1, g, true);
+        wrap3(m, mom, 1, g, true);
+        wrap(cm, cells[0], IntVect(0), nvars, ng[0]);
+        wrap(cv, cells[1], IntVect(0), nvars, ng[1]);
+        wrap(pm, cells[2], IntVect(0), nprimvars + 3, ng[2]);
+        wrap(pv, cells[3], IntVect(0), nprimvars + 5, ng[3]);
+        wrap(cov, cells[4], IntVect(0), 26, ng[4]);
+        wrap(m3, cells[5], IntVect(0), nvars + 1, ng[5]);
+        wrap(m4, cells[6], IntVect(0), nvars + 1, ng[6]);
+        wrap3(vm, faces, 1, 0, true);
+        wrap3(vv, faces + 3, 1, 0, true);
+        wrap3(mm, faces + 6, 1, 0, true);
+        wrap3(mv, faces + 9, 1, 0, true);
+        WritePlotFileStag(step, time, g_geom, c, cm, cv, m, mm, mv, p, pm, pv, v, vm, vv, cov, m3, m4, sc, scm, scv,
+                          scc, e, k, z);
+        const PlotfileCapture& pc = plotfile_capture();
+        if ((long)pc.data.size() > cap) throw std::runtime_error("fhdref_plotfile: output buffer too small");
+        std::copy(pc.data.begin(), pc.data.end(), out);
+        std::string joined;
+        for (const std::string& n : pc.names) joined += n + "\n";
+        if ((int)joined.size() + 1 > ncap) throw std::runtime_error("fhdref_plotfile: names buffer too small");
+        std::copy(joined.begin(), joined.end(), names);
+        names[joined.size()] = 0;
+        *ncomp = (int)pc.names.size();
+    });
+}
+
+// WriteSpatialCross3D (writePlotFileStag.cpp:528-549): spatialCross<step, 9
+// digits> in the working directory from n_cells[0]*ncross values.
+int fhdref_write_spatial_cross(const double* spatial_cross, int step, int ncross) {
+    return guarded([&] {
+        const Vector<Real> sc(spatial_cross, spatial_cross + (size_t)n_cells[0] * ncross);
+        WriteSpatialCross3D(sc, step, g_geom, ncross);
+    });
+}
+
 int fhdref_max_acoustic_cfl(double* prim, double* const* vel, double dt, double* out) {
     return guarded([&] {
         MultiFab p;

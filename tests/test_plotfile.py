@@ -69,3 +69,36 @@ def test_plotfile_directory_parents_are_created(tmp_path):
     d = str(tmp_path / "runs" / "case1" / "plt000000000")
     write_plotfile_host(p, d, data, 0, 0.0, 0)
     assert read_header(d)["names"] == plotfile_names(p, 0)
+
+
+@pytest.mark.parametrize("make,flags", [(lambda: argon((5, 4, 3), dx=8e-6), 0),
+                                        (lambda: argon((5, 4, 3), dx=8e-6), MEANS | VARS | COVARS | MOM3 | MOM4),
+                                        (lambda: mixture4((4, 3, 5), dx=8e-6, visc_type=3, zeta_ratio=1.0),
+                                         MEANS | VARS | COVARS | MOM3 | MOM4),
+                                        (lambda: mixture4((4, 5, 3), dx=8e-6), MEANS | 32),
+                                        (lambda: mixture4((3, 4, 5), dx=8e-6), VARS | 64),
+                                        (lambda: argon((5, 3, 4), dx=8e-6), MOM4 | 128)])
+def test_restated_composition_and_names_equal_the_references(oracle, make, flags):
+    """The reference's own WritePlotFileStag (oracle/_ref, its plotfile MultiFab
+    captured before the AMReX writer) on random states and statistics: the
+    restated composition (tests/plotfile_reader.py, which the GPU pack is held
+    to) and fhd_plotfile_varname's names equal it bit for bit."""
+    from oracle import ref as R
+    from fhdex_b200.stats import StatsState
+    from tests.helpers import perturbed_state
+    from tests.plotfile_reader import reference_composition
+    if not R.available():
+        pytest.skip("oracle/_ref was not built")
+    p = make()
+    st = perturbed_state(oracle, p, seed=11, amp=0.05)
+    stats = StatsState(p)
+    g = torch.Generator().manual_seed(12)
+    for m in [st.eta, st.kappa, st.zeta] + list(stats.named().values()):
+        m.arr.copy_(torch.rand(m.arr.shape, generator=g, dtype=torch.float64) + 0.5)
+    data, names = R.plotfile(st, stats, flags, step=7, time=1e-9)
+    dy = {32: 0, 64: 1, 128: 2}.get(flags & 224, -1)
+    want = reference_composition(p, st, stats, means=bool(flags & MEANS), varz=bool(flags & VARS),
+                                 covars=bool(flags & COVARS), mom3=bool(flags & MOM3), mom4=bool(flags & MOM4),
+                                 deltay=dy)
+    assert names == plotfile_names(p, flags)
+    assert np.array_equal(data.numpy(), want)

@@ -41,3 +41,26 @@ def test_cross_means_rows(tmp_path):
     assert rows[0].startswith("100 1 1.00123 1.00247 ") and rows[0].endswith(" ")
     assert rows[1].startswith("200 ") and rows[2] == "" and len(rows[0].split()) == 27
     assert os.path.getsize(path) > 0
+
+
+def test_spatial_cross_file_equals_the_references(tmp_path, monkeypatch):
+    """fhd_write_spatial_cross against the reference's own WriteSpatialCross3D
+    (oracle/_ref), byte for byte."""
+    from oracle import ref as R
+    if not R.available():
+        import pytest
+        pytest.skip("oracle/_ref was not built")
+    p = mixture4((7, 3, 4), dx=8e-6).replace(prob_lo=(-2e-5, 0.0, 0.0), prob_hi=(-2e-5 + 5.6e-5, 2.4e-5, 3.2e-5))
+    s = StatsState(p, cross=True)
+    g = torch.Generator().manual_seed(9)
+    s.spatialCross.copy_(torch.randn(s.spatialCross.shape, generator=g, dtype=torch.float64) * 1e-9)
+    s.spatialCross[2, 5] = 0.0
+    s.spatialCross[3, 7] = 1.0
+    mine, theirs = tmp_path / "mine", tmp_path / "ref"
+    mine.mkdir()
+    theirs.mkdir()
+    s.write_spatial_cross(40, str(mine / "spatialCross"))
+    monkeypatch.chdir(theirs)
+    R.write_spatial_cross(p, s.spatialCross, 40)
+    name = "spatialCross000000040"
+    assert (mine / name).read_bytes() == (theirs / name).read_bytes()
