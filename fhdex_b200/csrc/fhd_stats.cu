@@ -378,13 +378,18 @@ static int stats_launch(const StatsArgs& a, bool means, bool vars, const fhd_fab
 // prim and primMeans components 1..nspecies+4), each entry (i, n) divided by
 // n_cells[1]*n_cells[2].  An entry is its y-z plane summed from 0.0 with k outer and
 // j inner, the order of a serial one-box sumToLine, so the sum is one dependent
-// chain: one thread owns one entry and adds in that order.  A warp takes 32
-// consecutive i of one component, so every row it reads is one coalesced 256-byte
-// segment, and each thread issues kLineDepth row loads ahead of its additions: the
-// kernel streams every source component once and is bound by HBM when enough rows
-// are in flight.
+// chain: one thread owns one entry and adds in that order.  A one-warp block takes
+// 32 consecutive i of one component, so every row it reads is one coalesced
+// 256-byte segment.  The chains are few (one per line entry), so the rows reach
+// shared memory through asynchronous 8-byte copies (cp.async) issued
+// kLineStages - 1 batches of kLineRows rows ahead of the additions, and each
+// thread only ever reads the shared-memory column its own copies wrote, so
+// cp.async.wait_group alone orders it (no block barrier).  With few chains each
+// warp runs alone on its SM sub-partition, so the per-row instruction count sets
+// the pace: a batch inside one k-plane takes its 32 row addresses as independent
+// base + u*sy products rather than a running offset.
 constexpr int kMaxLineJobs = 2 * (5 + MAXS) + 2 * (MAXS + 4);
-constexpr int kLineDepth = 32;
+constexpr int kLineRows = 32, kLineStages = 6;   // 48 KiB of shared memory per one-warp block
 struct LineJob {
     const double* src;   // component n of the source at valid cell (0, 0, 0)
     double* dst;         // line entry (0, n)
@@ -393,32 +398,71 @@ struct LineJob {
 };
 struct LineArgs {
     LineJob job[kMaxLineJobs];
-    int njobs, nxp, nx, ny, nz;
+    int njobs, xblocks, nx, ny, nz;   // xblocks: one-warp blocks per job, ceil(nx / 32)
 };
 
-static __global__ void __launch_bounds__(128) k_sum_to_line(const __grid_constant__ LineArgs a) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int c = t / a.nxp, i = t - c * a.nxp;
-    if (c >= a.njobs || i >= a.nx) return;
+FHD_D void cp_async8(double* dst, const double* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+FHD_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+FHD_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+static __global__ void __launch_bounds__(32) k_sum_to_line(const __grid_constant__ LineArgs a) {
+    __shared__ __align__(16) double buf[kLineStages][kLineRows][32];
+    const int lane = threadIdx.x;
+    const int c = blockIdx.x / a.xblocks;
+    const int i = (blockIdx.x - c * a.xblocks) * 32 + lane;
+    if (c >= a.njobs) return;   // uniform over the block
+    const bool on = i < a.nx;
     const LineJob& J = a.job[c];
-    const double* p = J.src + i;
+    const double* p = J.src + (on ? i : 0);
     const int64_t rows = (int64_t)a.ny * a.nz, wrap = J.sz - (int64_t)a.ny * J.sy;
-    double acc = 0.0;
-    int j = 0;
-    int64_t off = 0;   // offset of row (j, k): k*sz + j*sy
-    for (int64_t r0 = 0; r0 < rows; r0 += kLineDepth) {
-        double v[kLineDepth];
+    // the next row to copy: its index rq = k*ny + j, its j and offset k*sz + j*sy
+    int64_t rq = 0, offq = 0;
+    int jq = 0;
+    auto issue = [&](int stage) {   // one group: the next kLineRows rows (possibly none)
+        if (jq + kLineRows <= a.ny && rq + kLineRows <= rows) {
+            // the batch lies in one k-plane: independent row addresses
+            const double* q = p + offq;
+            if (on) {
 #pragma unroll
-        for (int u = 0; u < kLineDepth; ++u) {
-            if (r0 + u < rows) v[u] = __ldg(p + off);
-            off += J.sy;
-            if (++j == a.ny) { j = 0; off += wrap; }
+                for (int u = 0; u < kLineRows; ++u) cp_async8(&buf[stage][u][lane], q + (int64_t)u * J.sy);
+            }
+            rq += kLineRows;
+            offq += (int64_t)kLineRows * J.sy;
+            jq += kLineRows;
+            if (jq == a.ny) { jq = 0; offq += wrap; }
+        } else {
+            for (int u = 0; u < kLineRows; ++u) {
+                if (on && rq < rows) cp_async8(&buf[stage][u][lane], p + offq);
+                ++rq;
+                offq += J.sy;
+                if (++jq == a.ny) { jq = 0; offq += wrap; }
+            }
         }
+        cp_async_commit();
+    };
+#pragma unroll 1
+    for (int st = 0; st < kLineStages - 1; ++st) issue(st);
+    double acc = 0.0;
+    const int64_t nbatch = (rows + kLineRows - 1) / kLineRows;
+#pragma unroll 1
+    for (int64_t b = 0; b < nbatch; ++b) {
+        issue((int)((b + kLineStages - 1) % kLineStages));   // the stage batch b-1 used
+        cp_async_wait<kLineStages - 1>();                    // batch b (group b) has landed
+        const int st = (int)(b % kLineStages);
+        const int64_t r0 = b * kLineRows;
+        if (r0 + kLineRows <= rows) {
 #pragma unroll
-        for (int u = 0; u < kLineDepth; ++u)
-            if (r0 + u < rows) acc += v[u];
+            for (int u = 0; u < kLineRows; ++u) acc += buf[st][u][lane];
+        } else {
+            for (int u = 0; r0 + u < rows; ++u) acc += buf[st][u][lane];
+        }
     }
-    J.dst[(int64_t)i * J.dstride] = acc / (double)rows;
+    cp_async_wait<0>();
+    if (on) J.dst[(int64_t)i * J.dstride] = acc / (double)rows;
 }
 
 // k_spatial_cross: one thread per x cell i updates spatialCross(i, 0..ncross-1) in
@@ -587,12 +631,11 @@ static int cross_launch(const DevParams& P, const fhd_fab& cu, const fhd_fab& pr
     for (int n = 0; n < NP; ++n) la.job[q++] = line_job(prim, 1 + n, L[2] + n, NP);
     for (int n = 0; n < NP; ++n) la.job[q++] = line_job(st.primMeans, 1 + n, L[3] + n, NP);
     la.njobs = q;
-    la.nxp = (nx + 31) & ~31;
+    la.xblocks = (nx + 31) / 32;
     la.nx = nx;
     la.ny = P.n[1];
     la.nz = P.n[2];
-    const int64_t threads = (int64_t)la.nxp * q;
-    k_sum_to_line<<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(la);
+    k_sum_to_line<<<(unsigned)(la.xblocks * q), 32, 0, s>>>(la);
     CrossArgs ca;
     ca.cu = L[0];
     ca.cum = L[1];
