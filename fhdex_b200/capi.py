@@ -95,6 +95,8 @@ class FhdParams(C.Structure):
         ("T_init", C.c_double),
         ("rhobar", C.c_double * MAX_SPECIES),
         ("cross_cell", C.c_int),
+        ("do_1D", C.c_int),
+        ("do_2D", C.c_int),
     ]
 
 

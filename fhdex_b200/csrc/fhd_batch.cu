@@ -491,7 +491,7 @@ int fhd_batch_add(fhd_batch* b, const fhd_params* params, fhd_fab cu, const fhd_
     if (p.nspecies != b->ns || p.precision != (b->mixed ? FHD_PREC_MIXED : FHD_PREC_FP64)) return FHD_ERR_BAD_ARG;
     if (p.algorithm_type != 2 || p.transport_type != 1 || p.advection_type < -1 || p.advection_type > 2 ||
         (p.stoch_stress_form != 0 && p.stoch_stress_form != 1) || ((p.visc_type == 3 || p.visc_type == -3) && p.zeta_ratio < 0) ||
-        p.nreaction != 0 || has_walls(p))
+        p.nreaction != 0 || reference_order(p))
         return FHD_ERR_UNSUPPORTED;
     const int mode = p.stoch_stress_form == 1 ? NM_PHILOX : NM_OFF;
     if (b->mode >= 0 && b->mode != mode && !b->mem.empty()) return FHD_ERR_BAD_ARG;

@@ -36,6 +36,7 @@ struct fhd_ctx {
     // physical boundaries: the periodic directions and the walls' values
     int per[3] = {1, 1, 1};
     bool walls = false;
+    bool refpipe = false;        // walls or a quasi-1-D / 2-D run: the reference-ordered pipeline
     bool reservoir = false;      // a side with bc_mass 3 or 4: the boundary passes run one by one
     bool res4 = false;           // a particle reservoir side (bc_mass 4)
     ResBuffers res{};
@@ -394,6 +395,15 @@ int fhd_create(fhd_ctx** out, const fhd_params* params, int device) {
     if (const int rc = setup_walls(p, per, wall)) return rc;
     const bool walls = !(per[0] && per[1] && per[2]);
     if (walls && p.precision != FHD_PREC_FP64) return FHD_ERR_UNSUPPORTED;
+    // quasi-1-D / 2-D runs: one mode at most, no bulk viscosity (main_driver.cpp:104-118);
+    // FP64 and no particle reservoir here
+    if (p.do_1D < 0 || p.do_1D > 1 || p.do_2D < 0 || p.do_2D > 1 || (p.do_1D && p.do_2D)) return FHD_ERR_BAD_ARG;
+    const bool lowdim = p.do_1D || p.do_2D;
+    if (lowdim && (p.visc_type == 3 || p.visc_type == -3)) return FHD_ERR_BAD_ARG;
+    if (lowdim && p.precision != FHD_PREC_FP64) return FHD_ERR_UNSUPPORTED;
+    if (lowdim && walls)
+        for (int d = 0; d < 3; ++d)
+            if (!per[d] && (p.bc_mass_lo[d] == 4 || p.bc_mass_hi[d] == 4)) return FHD_ERR_UNSUPPORTED;
     fhd_ctx* c = new (std::nothrow) fhd_ctx;
     if (!c) return FHD_ERR_OOM;
     c->prm = p;
@@ -417,6 +427,7 @@ int fhd_create(fhd_ctx** out, const fhd_params* params, int device) {
         }
     for (int d = 0; d < 3; ++d) c->per[d] = per[d];
     c->walls = walls;
+    c->refpipe = walls || lowdim;
     c->wall = wall;
     for (int d = 0; d < 3; ++d) {
         if (!per[d] && (p.bc_mass_lo[d] >= 3 || p.bc_mass_hi[d] >= 3)) c->reservoir = true;
@@ -846,7 +857,8 @@ int fhd_fill_step_noise(fhd_ctx* c, const fhd_noise* nz, int64_t step) {
             if (!rc) rc = noise_fill(P, nz->edge[s][d], 0, 1, 0.0, 1.0, fid_edge(d), s, c->stream);
             // the centre noise is read on the cells grown by 1: in a wall direction
             // its ghost layer holds values of its own
-            if (!rc) rc = noise_fill(P, nz->cen[s][d], 0, 1, 0.0, std::sqrt(2.0), fid_cen(d), s, c->stream, 1);
+            if (!rc) rc = noise_fill(P, nz->cen[s][d], 0, 1, 0.0, d == 0 ? P.csd0 : std::sqrt(2.0), fid_cen(d), s,
+                                     c->stream, 1);
             if (rc) return rc;
             g[ng++] = GhostReq{nz->cen[s][d], 0, 1};
         }
@@ -991,7 +1003,7 @@ static int step_launches(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab p
                   fhd_fab eta, fhd_fab zeta, fhd_fab kappa, fhd_fab chi, fhd_fab D, const fhd_fab* faceflux,
                   const fhd_fab* edgeflux, const fhd_fab* cenflux, const fhd_noise* injected, double dt, int64_t step,
                   bool aux_coef, bool aux_flux, const uint64_t* step_ptr) {
-    if (c->walls)
+    if (c->refpipe)
         return walls_step_launches(c, cu, mom, prim, vel, source, eta, zeta, kappa, chi, D, faceflux, edgeflux,
                                    cenflux, injected, dt, step, aux_coef, aux_flux, step_ptr);
     const int ns = c->prm.nspecies, nprim = 6 + 2 * ns;
@@ -1110,7 +1122,7 @@ int fhd_rk3_step_stag(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab prim
         if (!fab_ok(c, mom[d], FACEN[d], NGC, 1, FHD_F64) || !fab_ok(c, vel[d], FACEN[d], NGC, 1, FHD_F64))
             return FHD_ERR_BAD_ARG;
     if (source.data && !fab_ok(c, source, CELLN, 0, nvars, FHD_F64)) return FHD_ERR_BAD_ARG;
-    if (c->walls && !walls_ghosts_ok(cu, mom, prim, vel)) return FHD_ERR_BAD_ARG;
+    if (c->refpipe && !walls_ghosts_ok(cu, mom, prim, vel)) return FHD_ERR_BAD_ARG;
     const bool aux_coef = eta.data != nullptr;
     if (aux_coef) {
         if (mixed) return FHD_ERR_UNSUPPORTED;
@@ -1152,7 +1164,7 @@ int fhd_rk3_steps_stag(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab pri
     for (int d = 0; d < 3; ++d)
         if (!fab_ok(c, mom[d], FACEN[d], NGC, 1, FHD_F64) || !fab_ok(c, vel[d], FACEN[d], NGC, 1, FHD_F64))
             return FHD_ERR_BAD_ARG;
-    if (c->walls && !walls_ghosts_ok(cu, mom, prim, vel)) return FHD_ERR_BAD_ARG;
+    if (c->refpipe && !walls_ghosts_ok(cu, mom, prim, vel)) return FHD_ERR_BAD_ARG;
     if (nsteps == 0) return FHD_OK;
     cudaSetDevice(c->device);
     int rc = ensure_scratch(c);

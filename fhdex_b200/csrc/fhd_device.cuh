@@ -63,6 +63,11 @@ struct DevParams {
     double voff;                     // 0.6*AKL-1.0
     double cfac;                     // 6.0*CKL-5.0
     double sqrt2, sqrt3;
+    // quasi-1-D / 2-D runs (do_1D / do_2D): dim 1 or 2, else 3; fac2d = (3+sqrt(3))/2,
+    // the 2-D trace factor (fluxStag.cpp:185); csd0 the deviation of the x centre
+    // noise (1 in 1-D, sqrt(2) otherwise: timeStepStag.cpp:208-222)
+    int dim;
+    double fac2d, csd0;
     // noise
     uint32_t key0, key1;             // Philox key
     uint64_t step;                   // Philox counter words 2-3

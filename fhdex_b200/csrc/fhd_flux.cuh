@@ -85,7 +85,7 @@ struct Noise {
     }
     FHD_D void cen_all(const DevParams& P, int i, int j, int k, double (&out)[3]) const {
         if (MODE == NZ_PHILOX) {
-            out[0] = gauss1(P, fid_cen(0), i, j, k, P.sqrt2);
+            out[0] = gauss1(P, fid_cen(0), i, j, k, P.csd0);
             gauss2(P, fid_cen(1), i, j, k, P.sqrt2, out[1], out[2]);
         } else {
 #pragma unroll
@@ -98,7 +98,7 @@ struct Noise {
     FHD_D void cen_and_yz_edge(const DevParams& P, int i, int j, int k, bool edges, double (&wc)[3],
                                double& we2) const {
         if (MODE == NZ_PHILOX) {
-            gauss2sd(P, fid_edge(2), i, j, k, 1.0, P.sqrt2, we2, wc[0]);
+            gauss2sd(P, fid_edge(2), i, j, k, 1.0, P.csd0, we2, wc[0]);
             gauss2(P, fid_cen(1), i, j, k, P.sqrt2, wc[1], wc[2]);
         } else {
             cen_all(P, i, j, k, wc);
@@ -137,7 +137,7 @@ struct Noise {
     FHD_D double cen(const DevParams& P, int d, int i, int j, int k) const {
         if (MODE == NZ_W) return a.ca[d](i, j, k);
         if (MODE == NZ_AB) return comb(a.ca[d](i, j, k), a.cb[d](i, j, k));
-        if (MODE == NZ_PHILOX) return gauss1(P, fid_cen(d), i, j, k, P.sqrt2);
+        if (MODE == NZ_PHILOX) return gauss1(P, fid_cen(d), i, j, k, d == 0 ? P.csd0 : P.sqrt2);
         return 0.0;
     }
 };
@@ -154,12 +154,52 @@ struct CellTaus {
 };
 
 // diagonal stresses at a cell: stochastic fluxStag.cpp:163-206, deterministic :872-924;
-// wc: the three centre noise values W of the cell
-template <int NS, class R, int NZ>
+// wc: the three centre noise values W of the cell.  WL: the reference-ordered
+// pipeline, which also carries the quasi-1-D / 2-D runs (P.dim 1 / 2): only the
+// x (x and y) stresses, the 1-D amplitudes scaled by sqrt(3) and the 2-D trace
+// factor by (3+sqrt(3))/2 (fluxStag.cpp:171-192, 875-904)
+template <int NS, class R, int NZ, bool WL = false>
 FHD_D CellTaus<R> cell_taus_w(const DevParams& P, const Fields<NS, R>& F, const double (&wc)[3], int i, int j, int k) {
     CellTaus<R> t;
     const R eta = F.eta(i, j, k);
     const bool visc3 = (P.visc_type == 3 || P.visc_type == -3);
+    if (WL && P.dim < 3) {
+        if (NZ != NZ_OFF) {
+            const R etaT = eta * R(F.T(i, j, k));
+            R fac1 = dsqrt(R(2.0) * R(P.k_B) * etaT * R(P.volinv) * R(P.dtinv));
+            R fac2 = R(-1.0 / 3.0) * dsqrt(R(2.0) * R(P.k_B) * etaT * R(P.volinv) * R(P.dtinv));
+            const R w0 = R(wc[0]), w1 = R(wc[1]);
+            if (P.dim == 1) {
+                fac1 *= R(P.sqrt3);
+                fac2 *= R(P.sqrt3);
+                const R traceZ = w0;
+                t.s[0] = (fac1 * w0) + (fac2 * traceZ);
+                t.s[1] = R(0.0);
+            } else {
+                fac2 *= R(P.fac2d);
+                const R traceZ = w0 + w1;
+                t.s[0] = (fac1 * w0) + (fac2 * traceZ);
+                t.s[1] = (fac1 * w1) + (fac2 * traceZ);
+            }
+            t.s[2] = R(0.0);
+        } else {
+            t.s[0] = t.s[1] = t.s[2] = R(0.);
+        }
+        const R u_x = divc(P, R(F.vel[0](i + 1, j, k)) - R(F.vel[0](i, j, k)), R(P.dx[0]), R(P.rdx[0]));
+        const R eta23 = divc(P, R(2) * eta, R(3.), R(P.r3));
+        if (P.dim == 1) {
+            const R div = u_x;
+            t.d[0] = R(2) * eta * u_x + (R(0.0) - eta23) * div;
+            t.d[1] = R(0.0);
+        } else {
+            const R v_y = divc(P, R(F.vel[1](i, j + 1, k)) - R(F.vel[1](i, j, k)), R(P.dx[1]), R(P.rdx[1]));
+            const R div = u_x + v_y;
+            t.d[0] = R(2) * eta * u_x + (R(0.0) - eta23) * div;
+            t.d[1] = R(2) * eta * v_y + (R(0.0) - eta23) * div;
+        }
+        t.d[2] = R(0.0);
+        return t;
+    }
     if (NZ != NZ_OFF) {
         const R Tc = R(F.T(i, j, k));
         const R etaT = eta * Tc;
@@ -198,6 +238,14 @@ FHD_D CellTaus<R> cell_taus_w(const DevParams& P, const Fields<NS, R>& F, const 
 // 279-290, 939-1019: the first direction's wall is tested last and wins a corner).
 template <int NS, class R, int NZ, int E, bool WL = false>
 FHD_D Taus<R> edge_taus_w(const DevParams& P, const Fields<NS, R>& F, double wnoise, int i, int j, int k) {
+    // quasi-1-D: no shear stress; quasi-2-D: only xy (fluxStag.cpp:212-214, 241-243,
+    // 270-272, 930-932, 962-964, 995-997)
+    if (WL && (P.dim == 1 || (P.dim == 2 && E != 0))) {
+        Taus<R> z;
+        z.s = R(0.0);
+        z.d = R(0.0);
+        return z;
+    }
     // cells: (a) low-low, (b) low-high, (c) high-low, (d) high-high in the edge's two directions
     int ai, aj, ak, bi, bj, bk, ci, cj, ck;
     if (E == 0) { ai = i - 1; aj = j - 1; ak = k; bi = i - 1; bj = j; bk = k; ci = i; cj = j - 1; ck = k; }
@@ -275,11 +323,11 @@ FHD_D Taus<R> edge_taus_w(const DevParams& P, const Fields<NS, R>& F, double wno
     return t;
 }
 
-template <int NS, class R, int NZ>
+template <int NS, class R, int NZ, bool WL = false>
 FHD_D CellTaus<R> cell_taus(const DevParams& P, const Fields<NS, R>& F, const Noise<NZ>& nz, int i, int j, int k) {
     double wc[3] = {0.0, 0.0, 0.0};
     if (NZ != NZ_OFF) nz.cen_all(P, i, j, k, wc);
-    return cell_taus_w<NS, R, NZ>(P, F, wc, i, j, k);
+    return cell_taus_w<NS, R, NZ, WL>(P, F, wc, i, j, k);
 }
 
 template <int NS, class R, int NZ, int E, bool WL = false>
@@ -314,6 +362,10 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
     const int ws = WL ? wall_face(P, D, D == 0 ? i : (D == 1 ? j : k)) : -1;
     const int gi = ws == 0 ? im : i, gj = ws == 0 ? jm : j, gk = ws == 0 ? km : k;
     const int wside = 2 * D + (ws == 1 ? 1 : 0);
+    // a transverse face of a quasi-1-D (y, z) or 2-D (z) run carries no heat,
+    // species or Dufour flux, stochastic or diffusive (fluxStag.cpp:504-510,
+    // 666-672, 1185-1191, 1324-1330)
+    const bool transverse = WL && ((D == 1 && P.dim == 1) || (D == 2 && P.dim < 3));
     // flux components in the reference's accumulation order
     R heat = R(0.0), vdiag = R(0.0), vshear = R(0.0), duf = R(0.0);
     R spec[NS];
@@ -389,7 +441,7 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
     }
 
     // ---- stochastic part (fluxStag.cpp:298-781) ----
-    if (NZ != NZ_OFF) {
+    if (NZ != NZ_OFF && !transverse) {
         const R Th = R(F.T(i, j, k)), Tl = R(F.T(im, jm, km));
         R kp = (F.kappa(i, j, k) * Th * Th + F.kappa(im, jm, km) * Tl * Tl);
         R meanT = R(0.5) * (Th + Tl);
@@ -479,7 +531,7 @@ FHD_D FaceFlux<NS> face_flux(const DevParams& P, const Fields<NS, R>& F, const N
     }
 
     // ---- diffusive part (fluxStag.cpp:1026-1426) ----
-    {
+    if (!transverse) {
         // wall faces difference over the half cell to the wall value
         const R h = (WL && ws >= 0) ? R(P.hdx[D]) : R(P.dx[D]);
         const R rh = (WL && ws >= 0) ? R(P.rhdx[D]) : R(P.rdx[D]);
@@ -711,10 +763,15 @@ FHD_D double cen_total(const DevParams& P, const Fields<NS, R>& F, const CellTau
         }
     }
     if (P.advection_type >= 0) {
-        const Arr4<const double>& m = F.mom[d];
-        const Arr4<const double>& u = F.vel[d];
-        const int e0 = d == 0, e1 = d == 1, e2 = d == 2;
-        v += 0.25 * (m(i, j, k) + m(i + e0, j + e1, k + e2)) * (u(i, j, k) + u(i + e0, j + e1, k + e2)) + F.p(i, j, k);
+        if (WL && d >= P.dim) {
+            v += 0.0;   // no transverse pressure / advection term in 1-D and 2-D (fluxStag.cpp:1850-1860)
+        } else {
+            const Arr4<const double>& m = F.mom[d];
+            const Arr4<const double>& u = F.vel[d];
+            const int e0 = d == 0, e1 = d == 1, e2 = d == 2;
+            v += 0.25 * (m(i, j, k) + m(i + e0, j + e1, k + e2)) * (u(i, j, k) + u(i + e0, j + e1, k + e2)) +
+                 F.p(i, j, k);
+        }
     }
     return v;
 }

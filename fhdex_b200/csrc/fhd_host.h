@@ -29,6 +29,9 @@ inline bool has_walls(const fhd_params& p) {
     return false;
 }
 
+// runs that take the reference-ordered pipeline: walls, or a quasi-1-D / 2-D run
+inline bool reference_order(const fhd_params& p) { return has_walls(p) || p.do_1D || p.do_2D; }
+
 // Kernel parameters of a run (after GetHcGas): cell widths, the transport model's
 // cell-independent constants in the reference's own operation order
 // (compressible_functions.H:1180-1222), the Philox key and the reciprocals of the
@@ -76,6 +79,9 @@ inline DevParams dev_params(const fhd_params& p, double dt, uint64_t step) {
     P.cfac = 6.0 * CKL - 5.0;
     P.sqrt2 = sqrt(2.0);
     P.sqrt3 = sqrt(3.0);
+    P.dim = p.do_1D ? 1 : (p.do_2D ? 2 : 3);
+    P.fac2d = (3.0 + sqrt(3.0)) / 2.0;
+    P.csd0 = p.do_1D ? 1.0 : sqrt(2.0);
     P.walls = p.walls ? 1 : 0;
     for (int d = 0; d < 3; ++d) {
         P.periodic[d] = !P.walls || (p.bc_vel_lo[d] == -1 && p.bc_vel_hi[d] == -1);

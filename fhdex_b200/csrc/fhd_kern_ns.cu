@@ -80,7 +80,10 @@ int aux_mode(const StageCall& c) {
     }
 }
 
-int FHD_CAT(exact_aux_ns, FHD_NS)(const StageCall& c) { return c.P.walls ? aux_mode<true>(c) : aux_mode<false>(c); }
+// the wall variants also carry the quasi-1-D / 2-D branches
+int FHD_CAT(exact_aux_ns, FHD_NS)(const StageCall& c) {
+    return (c.P.walls || c.P.dim < 3) ? aux_mode<true>(c) : aux_mode<false>(c);
+}
 
 int FHD_CAT(exact_walls_ns, FHD_NS)(const StageCall& c, int part) { return launch_walls_part<FHD_NS>(c, part); }
 
@@ -110,6 +113,8 @@ int FHD_CAT(exact_transport_ns, FHD_NS)(const DevParams& P, fhd_fab prim, fhd_fa
     // the grown box that every coefficient fab and prim cover
     int g = -prim.lo[0];
     for (const fhd_fab* f : {&eta, &zeta, &kappa, &chi, &D}) g = -f->lo[0] < g ? -f->lo[0] : g;
+    // a quasi-1-D run computes them on the box grown by one only (transCoeffs.cpp:18-21)
+    if (P.dim == 1 && g > 1) g = 1;
     a.ng = g;
     a.status = status;
     const int64_t tot = (int64_t)(P.n[0] + 2 * a.ng) * (P.n[1] + 2 * a.ng) * (P.n[2] + 2 * a.ng);

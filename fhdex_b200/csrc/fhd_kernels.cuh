@@ -112,7 +112,7 @@ FHD_D double cen_total_res(const DevParams& P, const Fields<NS, R>& F, const Noi
         if (side >= 0 && P.bc_mass[side] == 4) {
             int c[3] = {i, j, k};
             c[d] += (side & 1) ? -1 : 1;
-            const CellTaus<R> tin = cell_taus<NS, R, NZ>(P, F, nz, c[0], c[1], c[2]);
+            const CellTaus<R> tin = cell_taus<NS, R, NZ, WL>(P, F, nz, c[0], c[1], c[2]);
             return cen_total<NS, R, WL>(P, F, t, d, i, j, k, &tin);
         }
     }
@@ -161,7 +161,7 @@ FHD_D void taus_point(const StageArgs<NS, R, NZ>& a, int q) {
         const bool edges = i >= 0 && j >= 0 && k >= 0;
         double wc[3] = {0.0, 0.0, 0.0}, we[3] = {0.0, 0.0, 0.0};
         if (NZ != NZ_OFF) a.noise.cen_and_yz_edge(P, i, j, k, edges, wc, we[2]);
-        const CellTaus<R> t = cell_taus_w<NS, R, NZ>(P, a.F, wc, i, j, k);
+        const CellTaus<R> t = cell_taus_w<NS, R, NZ, WL>(P, a.F, wc, i, j, k);
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             a.ct(i, j, k, d) = t.s[d];
@@ -556,7 +556,7 @@ struct DirectTaus {
     const DevParams* P;
     const Fields<NS, R>* F;
     const Noise<NZ>* nz;
-    FHD_D CellTaus<R> cell(int i, int j, int k) const { return cell_taus<NS, R, NZ>(*P, *F, *nz, i, j, k); }
+    FHD_D CellTaus<R> cell(int i, int j, int k) const { return cell_taus<NS, R, NZ, WL>(*P, *F, *nz, i, j, k); }
     template <int E>
     FHD_D Taus<R> edge(int i, int j, int k) const { return edge_taus<NS, R, NZ, E, WL>(*P, *F, *nz, i, j, k); }
 };
@@ -636,7 +636,7 @@ static __global__ void __launch_bounds__(128) k_aux_edges_cen(AuxArgs<NS, R, NZ>
             const int64_t r = q - nxy - nxz - nyz;
             const int i = (int)(r % (N[0] + 2)) - 1, j = (int)((r / (N[0] + 2)) % (N[1] + 2)) - 1,
                       k = (int)(r / ((int64_t)(N[0] + 2) * (N[1] + 2))) - 1;
-            const CellTaus<R> t = cell_taus<NS, R, NZ>(P, a.F, a.noise, i, j, k);
+            const CellTaus<R> t = cell_taus<NS, R, NZ, WL>(P, a.F, a.noise, i, j, k);
 #pragma unroll
             for (int d = 0; d < 3; ++d) a.cf[d](i, j, k) = cen_total_res<NS, R, NZ, WL>(P, a.F, a.noise, t, d, i, j, k);
         }

@@ -117,7 +117,7 @@ extern "C" int fhd_rk3_step_stag_noalloc(const fhd_params* params, fhd_fab cu, c
     const int ns = p.nspecies;
     if (ns < 1 || ns > 4 || p.algorithm_type != 2 || p.transport_type != 1 || p.precision != FHD_PREC_FP64 ||
         (p.stoch_stress_form != 0 && p.stoch_stress_form != 1) || p.advection_type < -1 || p.advection_type > 2 ||
-        ((p.visc_type == 3 || p.visc_type == -3) && p.zeta_ratio < 0) || p.nreaction != 0 || has_walls(p))
+        ((p.visc_type == 3 || p.visc_type == -3) && p.zeta_ratio < 0) || p.nreaction != 0 || reference_order(p))
         return FHD_ERR_UNSUPPORTED;
     for (int d = 0; d < 3; ++d)
         if (p.n_cells[d] < 2 || !(p.prob_hi[d] > p.prob_lo[d])) return FHD_ERR_BAD_ARG;

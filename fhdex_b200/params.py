@@ -83,6 +83,10 @@ class Params:
     ngc: int = 2
     # plot_cross's cell x* (common::cross_cell; statsStag.cpp:868-1105)
     cross_cell: int = 0
+    # quasi-1-D / quasi-2-D runs (compressible::do_1D / do_2D): the step's noise only
+    # in x (x and y), timeStepStag.cpp:172-323; transport on one ghost layer in 1-D
+    do_1D: int = 0
+    do_2D: int = 0
 
     @property
     def nvars(self):
@@ -161,6 +165,8 @@ class Params:
         p.rho0 = self.rho0
         p.T_init = self.T_init
         p.cross_cell = self.cross_cell
+        p.do_1D = self.do_1D
+        p.do_2D = self.do_2D
         for i in range(MAX_SPECIES):
             p.rhobar[i] = self.rhobar[i] if i < len(self.rhobar) else 0.0
         return p
@@ -336,7 +342,7 @@ def to_inputs(p: "Params") -> str:
              f"algorithm_type = {p.algorithm_type}", f"visc_type = {p.visc_type}",
              f"advection_type = {p.advection_type}", f"transport_type = {p.transport_type}",
              f"stoch_stress_form = {p.stoch_stress_form}", f"seed = {p.seed}", "prob_type = 1",
-             f"cross_cell = {p.cross_cell}"]
+             f"cross_cell = {p.cross_cell}", f"do_1D = {p.do_1D}", f"do_2D = {p.do_2D}"]
     if p.zeta_ratio >= 0:
         lines.append(f"zeta_ratio = {_fmt(float(p.zeta_ratio))}")
     for key in ("bc_vel_lo", "bc_vel_hi", "bc_mass_lo", "bc_mass_hi", "bc_therm_lo", "bc_therm_hi"):
@@ -396,7 +402,7 @@ def parse_inputs(text: str, base: Params | None = None) -> Params:
         if key in kv:
             upd[key] = float(kv[key][0])
     for key in ("algorithm_type", "visc_type", "advection_type", "transport_type",
-                "stoch_stress_form", "seed", "cross_cell"):
+                "stoch_stress_form", "seed", "cross_cell", "do_1D", "do_2D"):
         if key in kv:
             upd[key] = int(kv[key][0])
     # chemistry keys (chemistry_functions.cpp:45-124); avogadro overrides Runiv

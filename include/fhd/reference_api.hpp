@@ -88,6 +88,9 @@ namespace compressible {
 using fhd::amrex_compat::Real;
 inline int transport_type = 1;
 inline Real zeta_ratio = -1.0;
+// quasi-1-D / quasi-2-D runs (compressible_functions.cpp:58-63)
+inline int do_1D = 0;
+inline int do_2D = 0;
 }  // namespace compressible
 
 namespace common {
@@ -249,6 +252,8 @@ inline fhd_params params_from_globals() {
     p.T_init = common::T_init[0];
     for (int s = 0; s < FHD_MAX_SPECIES; ++s) p.rhobar[s] = common::rhobar[s];
     p.cross_cell = common::cross_cell;
+    p.do_1D = compressible::do_1D;
+    p.do_2D = compressible::do_2D;
     return p;
 }
 

@@ -142,6 +142,15 @@ typedef struct {
      * 0 <= cross_cell < n_cells[0] when fhd_stats_stag is given FHD_STATS_CROSS,
      * as main_driver.cpp:249-251 requires). */
     int cross_cell;
+    /* Quasi-1-D / quasi-2-D runs (deck keys do_1D, do_2D; at most one set): the
+     * step's noise and stresses only in x (in x and y) and no transverse diffusive
+     * fluxes (timeStepStag.cpp:172-323, fluxStag.cpp:171-295, 504-517, 666-680,
+     * 875-1010, 1185-1191, 1324-1330, 1850-1860), transport on one ghost layer in
+     * 1-D (transCoeffs.cpp:18-21).  FP64 only, no bulk viscosity (main_driver.cpp:
+     * 104-118) and no particle reservoir (bc_mass 4); the state's ghost width is
+     * then exactly 2, and the batched and no-allocation steps return
+     * FHD_ERR_UNSUPPORTED. */
+    int do_1D, do_2D;
 } fhd_params;
 
 /* Injected Gaussian noise for one RK3 step: the "A" and "B" white-noise fields

@@ -1023,6 +1023,8 @@ extern "C" {
 
 int orc_set_params(const fhd_params* p) {
     if (!p || p->nspecies < 1 || p->nspecies > MAXS) return FHD_ERR_BAD_ARG;
+    // the quasi-1-D / 2-D runs are held to the reference's own code (oracle/_ref), not restated here
+    if (p->do_1D || p->do_2D) return FHD_ERR_UNSUPPORTED;
     g.ns = p->nspecies;
     g.nvars = 5 + g.ns;
     g.nprimvars = 6 + 2 * g.ns;

@@ -163,18 +163,27 @@ def flux(st, sf, se, sc, dt, w1=1.0, w2=0.0):
 
 
 def step_normals(noise):
-    """The 24 fields of RK3stepStag's MultiFabFillRandomNormal calls, in the
-    reference's order (timeStepStag.cpp:183-222), from a StepNoise (face[s][d]:
-    energy + species comps; edge[s][e]: xy, xz, yz; cen[s][d]: one ghost)."""
+    """The fields of RK3stepStag's MultiFabFillRandomNormal calls, in the
+    reference's order (timeStepStag.cpp:172-222), from a StepNoise (face[s][d]:
+    energy + species comps; edge[s][e]: xy, xz, yz; cen[s][d]: one ghost): 24 in
+    3-D; with do_1D the x faces and the first centre field (4); with do_2D the x
+    and y faces, the xy edges of stochedge_x and stochedge_y and the first two
+    centre fields (12)."""
+    p = noise.p
+    dims = 1 if p.do_1D else 2 if p.do_2D else 3
     out = []
-    for d in range(3):
+    for d in range(dims):
         out += [noise.face[0][d].arr, noise.face[1][d].arr]
     eA = _ref_edges([m.arr for m in noise.edge[0]])
     eB = _ref_edges([m.arr for m in noise.edge[1]])
-    for i in range(2):
-        for e in (i, 2 + i, 4 + i):  # stochedge_x[i], _y[i], _z[i]
+    if dims == 2:
+        for e in (0, 2):  # stochedge_x[0], stochedge_y[0] (both xy)
             out += [eA[e], eB[e]]
-    for d in range(3):
+    elif dims == 3:
+        for i in range(2):
+            for e in (i, 2 + i, 4 + i):  # stochedge_x[i], _y[i], _z[i]
+                out += [eA[e], eB[e]]
+    for d in range(dims):
         out += [noise.cen[0][d].arr, noise.cen[1][d].arr]
     return out
 
@@ -307,9 +316,11 @@ def step_noise(p, seed):
     from fhdex_b200.state import StepNoise
     nz = StepNoise(p)
     g = torch.Generator().manual_seed(seed)
+    # the x centre noise of a quasi-1-D run has variance 1 (timeStepStag.cpp:208-210)
+    cvar = [1.0 if p.do_1D else 2.0, 2.0, 2.0]
     for s_ in range(2):
         for d in range(3):
-            for mf, var in ((nz.face[s_][d], 1.0), (nz.edge[s_][d], 1.0), (nz.cen[s_][d], 2.0)):
+            for mf, var in ((nz.face[s_][d], 1.0), (nz.edge[s_][d], 1.0), (nz.cen[s_][d], cvar[d])):
                 mf.arr.copy_(_m.sqrt(var) * torch.randn(mf.arr.shape, generator=g, dtype=torch.float64))
                 fill_boundary(p, mf, override_sync=True)
         if nz.chem[s_] is not None:

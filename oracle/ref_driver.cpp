@@ -287,6 +287,8 @@ int fhdref_rk3_step(double* cu, double* const* mom, double* prim, double* const*
                     double* const* edgeflux, double* const* cenflux, double* ranchem,
                     const double* const* normals, const double* const* chem, double dt, int step) {
     return guarded([&] {
+        // RK3stepStag's normal fills: 24 in 3-D, 4 with do_1D, 12 with do_2D (timeStepStag.cpp:172-222)
+        const int nfills = do_1D ? 4 : do_2D ? 12 : 24;
         const int g = ngc[0];
         MultiFab c, p, s, e, z, k, ch, d, rc;
         std::array<MultiFab, 3> m, v, ff, cf;
@@ -310,7 +312,7 @@ int fhdref_rk3_step(double* cu, double* const* mom, double* prim, double* const*
         auto& src = amrex::noise_source();
         src.launches = 0;
         src.fill_normal = [&](MultiFab& mf, int scomp, int ncomp, Real mean, Real stddev) {
-            if (call >= 24 || !normals || !normals[call]) throw std::runtime_error("missing injected noise field");
+            if (call >= nfills || !normals || !normals[call]) throw std::runtime_error("missing injected noise field");
             const Box b = mf.fab.box();
             NoiseCall rec{scomp, ncomp, mean, stddev, {}, {}, {}};
             for (int q = 0; q < 3; ++q) { rec.lo[q] = b.lo[q]; rec.hi[q] = b.hi[q]; rec.nodal[q] = b.typ.t[q]; }
@@ -359,7 +361,7 @@ int fhdref_rk3_step(double* cu, double* const* mom, double* prim, double* const*
         src.fill_normal = nullptr;
         src.point_normal = nullptr;
         src.stream = nullptr;
-        if (call != 24) throw std::runtime_error("RK3stepStag made an unexpected number of noise fills");
+        if (call != nfills) throw std::runtime_error("RK3stepStag made an unexpected number of noise fills");
     });
 }
 
