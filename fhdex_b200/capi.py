@@ -97,6 +97,7 @@ class FhdParams(C.Structure):
         ("cross_cell", C.c_int),
         ("do_1D", C.c_int),
         ("do_2D", C.c_int),
+        ("all_correl", C.c_int),
     ]
 
 

@@ -1238,7 +1238,6 @@ int fhd_rk3_steps_stag(fhd_ctx* c, fhd_fab cu, const fhd_fab mom[3], fhd_fab pri
 
 int fhd_stats_stag(fhd_ctx* c, fhd_fab cu, fhd_fab prim, const fhd_fab vel[3], const fhd_fab mom[3],
                    const fhd_stats* st, int64_t steps, int flags) {
-    (void)vel;  // the reference's per-cell statistics take vel but read only the momenta
     if (!c || !mom || !st || steps < 1) return FHD_ERR_BAD_ARG;
     const bool means = flags & FHD_STATS_MEANS, vars = flags & FHD_STATS_VARS;
     if (vars && !means) return FHD_ERR_BAD_ARG;  // statsStag.cpp:38-39
@@ -1261,14 +1260,32 @@ int fhd_stats_stag(fhd_ctx* c, fhd_fab cu, fhd_fab prim, const fhd_fab vel[3], c
         if ((flags & FHD_STATS_MOM3) && !fab_ok(c, st->mom3, CELLN, 0, nvars + 1, FHD_F64)) return FHD_ERR_BAD_ARG;
         if ((flags & FHD_STATS_MOM4) && !fab_ok(c, st->mom4, CELLN, 0, nvars + 1, FHD_F64)) return FHD_ERR_BAD_ARG;
     }
-    const bool cross = flags & FHD_STATS_CROSS;
+    const bool cross = (flags & FHD_STATS_CROSS) && !c->prm.do_2D;
+    const bool cross1d = cross && c->prm.do_1D;
+    // the x* (statsStag.cpp:168-193): cross_cell, or the five equidistant ones with all_correl in 1-D
+    int stars[5] = {c->prm.cross_cell, 0, 0, 0, 0};
+    int nstars = 1;
+    if (cross1d && c->prm.all_correl == 1) {
+        const int n0 = c->prm.n_cells[0];
+        stars[0] = 0;
+        stars[1] = (int)std::floor(1.0 * n0 / 4.0);
+        stars[2] = (int)std::floor(2.0 * n0 / 4.0);
+        stars[3] = (int)std::floor(3.0 * n0 / 4.0);
+        stars[4] = n0 - 1;
+        nstars = 5;
+    }
     if (cross) {
         // main_driver.cpp:249-251
         if (c->prm.cross_cell < 0 || c->prm.cross_cell > c->prm.n_cells[0] - 1) return FHD_ERR_BAD_ARG;
-        if (!st->spatialCross || !st->dataSliceMeans_xcross) return FHD_ERR_BAD_ARG;
+        if (!st->spatialCross || (!cross1d && !st->dataSliceMeans_xcross)) return FHD_ERR_BAD_ARG;
+        if (cross1d) {
+            // the 1-D correlations read vel x and the face momentum / velocity means
+            for (int d = 0; d < 3; ++d)
+                if (!vel || !fab_ok(c, vel[d], FACEN[d], 0, 1, FHD_F64)) return FHD_ERR_BAD_ARG;
+        }
     }
     cudaSetDevice(c->device);
-    if (cross) {
+    if (cross && !cross1d) {
         const size_t need = (size_t)stats_line_doubles(ns, c->prm.n_cells[0]) * sizeof(double);
         if (c->lines_bytes < need) {
             if (c->lines) {
@@ -1282,7 +1299,8 @@ int fhd_stats_stag(fhd_ctx* c, fhd_fab cu, fhd_fab prim, const fhd_fab vel[3], c
         }
     }
     const DevParams P = make_dev(c, 1.0, 0);
-    return exact_stats(P, cu, prim, mom, *st, steps, flags, c->prm.cross_cell, c->lines, c->stream);
+    return exact_stats(P, cu, prim, vel, mom, *st, steps, cross ? flags : (flags & ~FHD_STATS_CROSS), stars, nstars,
+                       c->lines, c->stream);
 }
 
 int fhd_spatial_cross_ncross(int nspecies) {

@@ -108,6 +108,10 @@ bool geometry(const fhd_params& p, const fhd_fab& f, int vlo[3], int vhi[3], int
 }
 
 int ncross_of(const fhd_params& p) { return 37 + p.nspecies + 3; }
+bool lowdim(const fhd_params& p) { return p.do_1D || p.do_2D; }
+// components of a quasi-1-D / 2-D run's spatialCrossMF (main_driver.cpp:717-727)
+int crossmf_ncomp(const fhd_params& p) { return (p.do_1D && p.all_correl == 1 ? 5 : 1) * ncross_of(p); }
+int64_t cells_of(const fhd_params& p) { return (int64_t)p.n_cells[0] * p.n_cells[1] * p.n_cells[2]; }
 
 // spatialCross (host or device) into a host vector
 bool cross_to_host(const fhd_params& p, const double* src, std::vector<double>& out) {
@@ -143,8 +147,16 @@ extern "C" int fhd_write_checkpoint(const fhd_params* params, const char* chk_ba
         cudaGetLastError();
         return FHD_ERR_CUDA;
     }
-    std::vector<double> sc;
-    if (cross && !cross_to_host(*params, stats->spatialCross, sc)) return FHD_ERR_CUDA;
+    // the Header's spatialCrossVec (left at zero by a quasi-1-D / 2-D run, whose
+    // correlations are the MultiFab spatialCrossMF: Checkpoint.cpp:251-256)
+    std::vector<double> sc, scmf;
+    if (cross && !lowdim(*params) && !cross_to_host(*params, stats->spatialCross, sc)) return FHD_ERR_CUDA;
+    if (cross && lowdim(*params)) {
+        sc.assign((size_t)params->n_cells[0] * ncross_of(*params), 0.0);
+        scmf.resize((size_t)cells_of(*params) * crossmf_ncomp(*params));
+        if (!copy_bytes(scmf.data(), stats->spatialCross, scmf.size() * sizeof(double), on_device(stats->spatialCross)))
+            return FHD_ERR_CUDA;
+    }
     const std::string dir = chk_dir(chk_base, step);
     if (!vismf_mkdir(dir) || !vismf_mkdir(dir + "/Level_0")) return FHD_ERR_BAD_ARG;
     FILE* h = std::fopen((dir + "/Header").c_str(), "w");
@@ -164,6 +176,11 @@ extern "C" int fhd_write_checkpoint(const fhd_params* params, const char* chk_ba
             return FHD_ERR_CUDA;
         if (!vismf_write(dir + "/Level_0", e.name, buf.data(), vlo, vhi, type, e.fab.ncomp, ng)) return FHD_ERR_BAD_ARG;
     }
+    if (!scmf.empty()) {
+        const int vlo[3] = {0, 0, 0}, type[3] = {0, 0, 0};
+        if (!vismf_write(dir + "/Level_0", "spatialCrossMF", scmf.data(), vlo, hi, type, crossmf_ncomp(*params), 0))
+            return FHD_ERR_BAD_ARG;
+    }
     return FHD_OK;
 }
 
@@ -182,7 +199,7 @@ extern "C" int fhd_read_checkpoint(const fhd_params* params, const char* chk_bas
     bool hok = std::fgets(title, sizeof(title), h) && std::fscanf(h, "%d %lf %d", &s, &t, &sc) == 3;
     // spatialCrossVec: the values after the BoxArray's closing ")" line
     std::vector<double> cross;
-    if (hok && stats && stats->spatialCross) {
+    if (hok && stats && stats->spatialCross && !lowdim(*params)) {
         char line[512];
         bool end = false;
         while (!end && std::fgets(line, sizeof(line), h)) end = line[0] == ')';
@@ -213,6 +230,13 @@ extern "C" int fhd_read_checkpoint(const fhd_params* params, const char* chk_bas
         }
         if (!copy_bytes(e.fab.data, buf.data(), buf.size() * sizeof(double), dev)) return FHD_ERR_CUDA;
     }
+    // a quasi-1-D / 2-D run's correlations: spatialCrossMF (Checkpoint.cpp:529-535)
+    if (stats && stats->spatialCross && lowdim(*params)) {
+        const int glo[3] = {0, 0, 0}, ghi[3] = {params->n_cells[0] - 1, params->n_cells[1] - 1, params->n_cells[2] - 1};
+        const int type[3] = {0, 0, 0};
+        if (!vismf_read(dir + "/Level_0", "spatialCrossMF", glo, ghi, type, crossmf_ncomp(*params), cross))
+            return FHD_ERR_BAD_ARG;
+    }
     if (!cross.empty()) {
         const bool dev = on_device(stats->spatialCross);
         if (dev && !synced && cudaDeviceSynchronize() != cudaSuccess) {
@@ -228,23 +252,63 @@ extern "C" int fhd_read_checkpoint(const fhd_params* params, const char* chk_bas
     return FHD_OK;
 }
 
-// WriteSpatialCross3D (writePlotFileStag.cpp:528-549): <base><step, 9 digits>, one
+// WriteSpatialCross1D (writePlotFileStag.cpp:551-563): per x*, WriteHorizontalAverage
+// (ComputeAverages.cpp:8-94) of its ncross components of spatialCrossMF along x:
+// each line the cell centre prob_lo[0] + (i+0.5)*dx[0] and the components' y-z
+// averages (each summed from 0.0 with k outer and j inner, divided by
+// n_cells[1]*n_cells[2]), every number at the stream's default 6 significant digits
+// and followed by a space.
+static int write_cross_1d(const fhd_params& p, const char* dir, int step, const double* data) {
+    const int nc = ncross_of(p), nstar = crossmf_ncomp(p) / nc;
+    const int64_t cells = cells_of(p);
+    std::vector<double> mf((size_t)cells * nstar * nc);
+    if (!copy_bytes(mf.data(), data, mf.size() * sizeof(double), on_device(data))) return FHD_ERR_CUDA;
+    const int nx = p.n_cells[0], ny = p.n_cells[1], nz = p.n_cells[2];
+    const double h = (p.prob_hi[0] - p.prob_lo[0]) / nx;
+    for (int s = 0; s < nstar; ++s) {
+        std::vector<double> avg((size_t)nx * (nc + 1), 0.0);
+        for (int n = 0; n < nc; ++n) {
+            const double* c = mf.data() + (size_t)(s * nc + n) * cells;
+            for (int k = 0; k < nz; ++k)
+                for (int j = 0; j < ny; ++j)
+                    for (int i = 0; i < nx; ++i) avg[(size_t)i * (nc + 1) + n + 1] += c[((size_t)k * ny + j) * nx + i];
+        }
+        const int navg = ny * nz;
+        for (int r = 0; r < nx; ++r)
+            for (int n = 1; n < nc + 1; ++n) avg[(size_t)r * (nc + 1) + n] /= navg;
+        for (int r = 0; r < nx; ++r) avg[(size_t)r * (nc + 1)] = p.prob_lo[0] + (r + 0.5) * h;
+        const std::string prefix = std::string(dir) + (nstar == 5 ? std::to_string(s) + "_" : std::string()) +
+                                   "spatialCross1D_";
+        FILE* f = std::fopen(chk_dir(prefix.c_str(), step).c_str(), "w");
+        if (!f) return FHD_ERR_BAD_ARG;
+        for (int r = 0; r < nx; ++r) {
+            for (int n = 0; n < nc + 1; ++n) std::fprintf(f, "%g ", avg[(size_t)r * (nc + 1) + n]);
+            std::fputc('\n', f);
+        }
+        if (std::fclose(f) != 0) return FHD_ERR_BAD_ARG;
+    }
+    return FHD_OK;
+}
+
+// WriteSpatialCross3D (writePlotFileStag.cpp:528-549): <dir>spatialCross<step, 9 digits>, one
 // line per x cell: the cell centre prob_lo[0] + (i+0.5)*dx[0], then the ncross
 // entries, each followed by a space.  The reference sets 16 significant digits
 // only before the first entry, so the first line's centre keeps the stream's
 // default 6 (every later number has 16).
-extern "C" int fhd_write_spatial_cross(const fhd_params* params, const char* base, int step,
+extern "C" int fhd_write_spatial_cross(const fhd_params* params, const char* dir, int step,
                                        const double* spatial_cross) {
-    if (!params || !base || !spatial_cross || step < 0 || params->nspecies < 1 ||
+    if (!params || !dir || !spatial_cross || step < 0 || params->nspecies < 1 ||
         params->nspecies > FHD_MAX_SPECIES || params->n_cells[0] < 1)
         return FHD_ERR_BAD_ARG;
+    if (params->do_2D) return FHD_OK;   // WriteSpatialCross2D is not enabled in the reference
     std::vector<double> sc;
     if (on_device(spatial_cross) && cudaDeviceSynchronize() != cudaSuccess) {
         cudaGetLastError();
         return FHD_ERR_CUDA;
     }
+    if (params->do_1D) return write_cross_1d(*params, dir, step, spatial_cross);
     if (!cross_to_host(*params, spatial_cross, sc)) return FHD_ERR_CUDA;
-    FILE* f = std::fopen(chk_dir(base, step).c_str(), "w");
+    FILE* f = std::fopen(chk_dir((std::string(dir) + "spatialCross").c_str(), step).c_str(), "w");
     if (!f) return FHD_ERR_BAD_ARG;
     const int nc = ncross_of(*params);
     const double h = (params->prob_hi[0] - params->prob_lo[0]) / params->n_cells[0];

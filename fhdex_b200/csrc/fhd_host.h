@@ -208,9 +208,11 @@ int plot_write(const fhd_params& prm, const char* dir, const double* host, const
 int chem_launch(const DevParams& P, const ChemParams& C, const fhd_fab& prim, const fhd_fab& source,
                 const fhd_fab* na, const fhd_fab* nb, int mode, double w, cudaStream_t s);
 // running statistics (fhd_stats.cu, exact TU)
-// lines: device scratch of stats_line_doubles(ns, n_cells[0]) doubles (FHD_STATS_CROSS only)
-int exact_stats(const DevParams& P, const fhd_fab& cu, const fhd_fab& prim, const fhd_fab mom[3],
-                const fhd_stats& st, int64_t steps, int flags, int cross_cell, double* lines, cudaStream_t s);
+// stars: the x* of FHD_STATS_CROSS (one in 3-D; one or five in a quasi-1-D run);
+// lines: device scratch of stats_line_doubles(ns, n_cells[0]) doubles (3-D FHD_STATS_CROSS only)
+int exact_stats(const DevParams& P, const fhd_fab& cu, const fhd_fab& prim, const fhd_fab vel[3], const fhd_fab mom[3],
+                const fhd_stats& st, int64_t steps, int flags, const int* stars, int nstars, double* lines,
+                cudaStream_t s);
 int64_t stats_line_doubles(int ns, int nx);
 int override_sync(const fhd_fab& f, const int ncell[3], cudaStream_t s, const int* periodic = nullptr);
 // wall_ghosts: also fill the first ghost layer of the wall directions (centre noise)

@@ -481,9 +481,116 @@ struct CrossArgs {
     double sm1, sinv;                   // stepsminusone, stepsinv
 };
 
+// The x* quantities and this cell's (or x line's) fluctuations that every
+// correlation update reads (statsStag.cpp:913-1004 in 3-D, :1363-1437 in 1-D).
+template <int NS>
+struct CrossStar {
+    double meanrho, meanux, meanYk[NS], delrhoYk[NS], delYk[NS];
+    double delrho, delK, deljx, deljy, deljz, delT, delvx, cvinv, qmean, delG;
+};
+template <int NS>
+struct CrossHere {
+    double meanrho, meanYk[NS], delrhoYk[NS], delYk[NS];
+    double delrho, delK, deljx, deljy, deljz, delT, delvx, cvinv, qmean, delG;
+};
+
+// the x* quantities from the 18 + 4 nspecies entries of data_xcross
+template <int NS>
+FHD_D CrossStar<NS> cross_star(const double* dx, const double* hcv) {
+    CrossStar<NS> c;
+    c.meanrho = dx[1];
+    c.meanux = dx[11];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+        c.meanYk[n] = dx[18 + 4 * n + 3];
+        c.delrhoYk[n] = dx[18 + 4 * n + 0] - dx[18 + 4 * n + 1];
+        c.delYk[n] = dx[18 + 4 * n + 2] - dx[18 + 4 * n + 3];
+    }
+    c.delrho = dx[0] - dx[1];
+    c.delK = dx[2] - dx[3];
+    c.deljx = dx[4] - dx[5];
+    c.deljy = dx[6] - dx[7];
+    c.deljz = dx[8] - dx[9];
+    c.delT = dx[16] - dx[17];
+    c.delvx = dx[10] - dx[11];
+    double cv = 0.;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) cv = cv + hcv[l] * dx[18 + 4 * l + 1] / dx[1];
+    c.cvinv = 1.0 / cv;
+    c.qmean = cv * dx[17] - 0.5 * (dx[11] * dx[11] + dx[13] * dx[13] + dx[15] * dx[15]);
+    c.delG = dx[11] * (dx[4] - dx[5]) + dx[13] * (dx[6] - dx[7]) + dx[15] * (dx[8] - dx[9]);
+    return c;
+}
+
+// The running averages and derived correlations of one point, entries S(0..ncross-1)
+// at stride qs, in the reference's statement order (a later entry reads the earlier
+// entries' new values; statsStag.cpp:1007-1104 and :1441-1551 are the same
+// statements).  Two reference quirks are kept: the "Y_k" the caller passes, and
+// entries 37+nspecies+1 and +2 re-applying the update of entries 37 and
+// 37+nspecies-1 that were already updated in the same step.
+template <int NS>
+FHD_D void cross_update(double* S, int64_t qs, const CrossStar<NS>& x, const CrossHere<NS>& h, double sm1,
+                        double sinv) {
+    constexpr int H = NS - 1;
+    auto at = [&](int q) -> double& { return S[q * qs]; };
+    auto upd = [&](int q, double v) { at(q) = (at(q) * sm1 + v) * sinv; };
+    upd(0, x.delrho * h.delrho);
+    upd(1, x.delK * h.delK);
+    upd(2, x.deljx * h.deljx);
+    upd(3, x.deljy * h.deljy);
+    upd(4, x.deljz * h.deljz);
+    upd(5, x.deljx * h.delrho);
+    upd(6, x.deljx * h.delrhoYk[0]);
+    upd(7, x.deljx * h.delrhoYk[H]);
+    upd(8, x.delrho * h.delrhoYk[0]);
+    upd(9, x.delrho * h.delrhoYk[H]);
+    upd(10, x.delrhoYk[0] * h.delrho);
+    upd(11, x.delrhoYk[H] * h.delrho);
+    upd(12, x.delG * h.delG);
+    upd(13, x.delG * h.delK);
+    upd(14, x.delK * h.delG);
+    upd(15, x.delrho * h.delK);
+    upd(16, x.delK * h.delrho);
+    upd(17, x.delrho * h.delG);
+    upd(18, x.delG * h.delrho);
+    const double meanrhocross = x.meanrho, meanrho = h.meanrho, meanuxcross = x.meanux;
+    const double qmeancross = x.qmean, qmean = h.qmean;
+    at(19) = (x.cvinv * h.cvinv / (meanrhocross * meanrho)) *
+             (at(1) + at(12) - at(13) - at(14) + qmean * qmeancross * at(0) - qmeancross * at(15) - qmean * at(16) +
+              qmeancross * at(17) + qmean * at(18));
+    at(20) = (x.cvinv / meanrhocross) * (at(16) - at(18) - qmeancross * at(0));
+    at(21) = (1.0 / meanrhocross) * (at(5) - meanuxcross * at(0));
+    at(22) = (1.0 / meanrhocross) * (at(6) - meanuxcross * at(8));
+    at(23) = (1.0 / meanrhocross) * (at(7) - meanuxcross * at(9));
+    at(24) = (1.0 / (meanrho * meanrhocross)) *
+             (at(6) - meanuxcross * at(8) - h.meanYk[0] * at(5) + meanuxcross * h.meanYk[0] * at(0));
+    at(25) = (1.0 / (meanrho * meanrhocross)) *
+             (at(7) - meanuxcross * at(9) - h.meanYk[H] * at(5) + meanuxcross * h.meanYk[H] * at(0));
+    upd(26, x.delT * h.delT);
+    upd(27, x.delT * h.delrho);
+    upd(28, x.delT * h.delvx);
+    upd(29, x.delvx * h.delrho);
+    upd(30, x.delvx * h.delYk[0]);
+    upd(31, x.delvx * h.delYk[H]);
+    upd(32, x.delvx * h.delrhoYk[0]);
+    upd(33, x.delvx * h.delrhoYk[H]);
+    upd(34, x.delYk[0] * h.delYk[0]);
+    upd(35, x.delYk[H] * h.delYk[H]);
+    upd(36, x.delYk[0] * h.delYk[H]);
+#pragma unroll
+    for (int n = 0; n < NS; ++n) upd(37 + n, x.delrhoYk[n] * h.delrhoYk[n]);
+    upd(37 + NS, x.delrhoYk[H] * h.delrhoYk[0]);
+    double dd = (at(37) * sm1 + x.delrhoYk[0] * h.delrhoYk[0]) * sinv;
+    at(37 + NS + 1) = (1.0 / (meanrho * meanrhocross)) *
+                      (dd - x.meanYk[0] * at(8) - h.meanYk[0] * at(10) + x.meanYk[0] * h.meanYk[0] * at(0));
+    dd = (at(37 + H) * sm1 + x.delrhoYk[H] * h.delrhoYk[H]) * sinv;
+    at(37 + NS + 2) = (1.0 / (meanrho * meanrhocross)) *
+                      (dd - x.meanYk[H] * at(9) - h.meanYk[H] * at(11) + x.meanYk[H] * h.meanYk[H] * at(0));
+}
+
 template <int NS>
 static __global__ void __launch_bounds__(128) k_spatial_cross(CrossArgs a) {
-    constexpr int NV = 5 + NS, NP = NS + 4, H = NS - 1;
+    constexpr int NV = 5 + NS, NP = NS + 4;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.nx) return;
     // data_xcross (statsStag.cpp:886-911)
@@ -506,103 +613,103 @@ static __global__ void __launch_bounds__(128) k_spatial_cross(CrossArgs a) {
     }
     if (i == 0)
         for (int q = 0; q < 18 + 4 * NS; ++q) a.xcross[q] = dx[q];
-    // the x* quantities (:913-958)
-    const double meanrhocross = dx[1], meanuxcross = dx[11];
-    double meanYkcross[NS], delrhoYkcross[NS], delYkcross[NS];
-#pragma unroll
-    for (int n = 0; n < NS; ++n) {
-        meanYkcross[n] = dx[18 + 4 * n + 3];
-        delrhoYkcross[n] = dx[18 + 4 * n + 0] - dx[18 + 4 * n + 1];
-        delYkcross[n] = dx[18 + 4 * n + 2] - dx[18 + 4 * n + 3];
-    }
-    const double delrhocross = dx[0] - dx[1], delKcross = dx[2] - dx[3];
-    const double deljxcross = dx[4] - dx[5], deljycross = dx[6] - dx[7], deljzcross = dx[8] - dx[9];
-    const double delTcross = dx[16] - dx[17], delvxcross = dx[10] - dx[11];
-    double cvcross = 0.;
-#pragma unroll
-    for (int l = 0; l < NS; ++l) cvcross = cvcross + a.hcv[l] * dx[18 + 4 * l + 1] / dx[1];
-    const double cvinvcross = 1.0 / cvcross;
-    const double qmeancross = cvcross * dx[17] - 0.5 * (dx[11] * dx[11] + dx[13] * dx[13] + dx[15] * dx[15]);
-    const double delGcross = dx[11] * (dx[4] - dx[5]) + dx[13] * (dx[6] - dx[7]) + dx[15] * (dx[8] - dx[9]);
-
-    // the quantities at x = i (:966-1004)
+    const CrossStar<NS> x = cross_star<NS>(dx, a.hcv);
+    // the x line's quantities (:966-1004); its "Y_k" are the prim line's entries 4+k
     const double *cu = a.cu + (int64_t)NV * i, *cm = a.cum + (int64_t)NV * i;
     const double *pr = a.pr + (int64_t)NP * i, *pm = a.pm + (int64_t)NP * i;
-    const double meanrho = cm[0];
-    double meanYk[NS], delrhoYk[NS], delYk[NS];
+    CrossHere<NS> h;
+    h.meanrho = cm[0];
 #pragma unroll
     for (int n = 0; n < NS; ++n) {
-        meanYk[n] = pm[4 + n];
-        delrhoYk[n] = cu[5 + n] - cm[5 + n];
-        delYk[n] = pr[4 + n] - pm[4 + n];
+        h.meanYk[n] = pm[4 + n];
+        h.delrhoYk[n] = cu[5 + n] - cm[5 + n];
+        h.delYk[n] = pr[4 + n] - pm[4 + n];
     }
-    const double delrho = cu[0] - cm[0], delK = cu[4] - cm[4];
-    const double deljx = cu[1] - cm[1], deljy = cu[2] - cm[2], deljz = cu[3] - cm[3];
-    const double delT = pr[3] - pm[3], delvx = pr[0] - pm[0];
+    h.delrho = cu[0] - cm[0];
+    h.delK = cu[4] - cm[4];
+    h.deljx = cu[1] - cm[1];
+    h.deljy = cu[2] - cm[2];
+    h.deljz = cu[3] - cm[3];
+    h.delT = pr[3] - pm[3];
+    h.delvx = pr[0] - pm[0];
     double cv = 0.;
 #pragma unroll
     for (int l = 0; l < NS; ++l) cv = cv + a.hcv[l] * cm[5 + l] / cm[0];
-    const double cvinv = 1.0 / cv;
-    const double qmean = cv * pm[3] - 0.5 * (pm[0] * pm[0] + pm[1] * pm[1] + pm[2] * pm[2]);
-    const double delG = pm[0] * deljx + pm[1] * deljy + pm[2] * deljz;
+    h.cvinv = 1.0 / cv;
+    h.qmean = cv * pm[3] - 0.5 * (pm[0] * pm[0] + pm[1] * pm[1] + pm[2] * pm[2]);
+    h.delG = pm[0] * h.deljx + pm[1] * h.deljy + pm[2] * h.deljz;
+    cross_update<NS>(a.S + (int64_t)a.ncross * i, 1, x, h, a.sm1, a.sinv);
+}
 
-    double* S = a.S + (int64_t)a.ncross * i;
-    const double sm1 = a.sm1, sinv = a.sinv;
-    auto upd = [&](int q, double x) { S[q] = (S[q] * sm1 + x) * sinv; };
-    // (:1007-1027)
-    upd(0, delrhocross * delrho);
-    upd(1, delKcross * delK);
-    upd(2, deljxcross * deljx);
-    upd(3, deljycross * deljy);
-    upd(4, deljzcross * deljz);
-    upd(5, deljxcross * delrho);
-    upd(6, deljxcross * delrhoYk[0]);
-    upd(7, deljxcross * delrhoYk[H]);
-    upd(8, delrhocross * delrhoYk[0]);
-    upd(9, delrhocross * delrhoYk[H]);
-    upd(10, delrhoYkcross[0] * delrho);
-    upd(11, delrhoYkcross[H] * delrho);
-    upd(12, delGcross * delG);
-    upd(13, delGcross * delK);
-    upd(14, delKcross * delG);
-    upd(15, delrhocross * delK);
-    upd(16, delKcross * delrho);
-    upd(17, delrhocross * delG);
-    upd(18, delGcross * delrho);
-    // derived correlations (:1032-1056)
-    S[19] = (cvinvcross * cvinv / (meanrhocross * meanrho)) *
-            (S[1] + S[12] - S[13] - S[14] + qmean * qmeancross * S[0] - qmeancross * S[15] - qmean * S[16] +
-             qmeancross * S[17] + qmean * S[18]);
-    S[20] = (cvinvcross / meanrhocross) * (S[16] - S[18] - qmeancross * S[0]);
-    S[21] = (1.0 / meanrhocross) * (S[5] - meanuxcross * S[0]);
-    S[22] = (1.0 / meanrhocross) * (S[6] - meanuxcross * S[8]);
-    S[23] = (1.0 / meanrhocross) * (S[7] - meanuxcross * S[9]);
-    S[24] = (1.0 / (meanrho * meanrhocross)) *
-            (S[6] - meanuxcross * S[8] - meanYk[0] * S[5] + meanuxcross * meanYk[0] * S[0]);
-    S[25] = (1.0 / (meanrho * meanrhocross)) *
-            (S[7] - meanuxcross * S[9] - meanYk[H] * S[5] + meanuxcross * meanYk[H] * S[0]);
-    // direct correlations (:1059-1093)
-    upd(26, delTcross * delT);
-    upd(27, delTcross * delrho);
-    upd(28, delTcross * delvx);
-    upd(29, delvxcross * delrho);
-    upd(30, delvxcross * delYk[0]);
-    upd(31, delvxcross * delYk[H]);
-    upd(32, delvxcross * delrhoYk[0]);
-    upd(33, delvxcross * delrhoYk[H]);
-    upd(34, delYkcross[0] * delYk[0]);
-    upd(35, delYkcross[H] * delYk[H]);
-    upd(36, delYkcross[0] * delYk[H]);
+// ---- quasi-1-D: correlations along each y-z pencil (evaluateStatsStag1D) -------------
+// One thread per valid cell; its pencil's cell at x* gives the x* quantities
+// (GetPencilCross, statsStag.cpp:830-858: cu 0..4 and 5+k, cuMeans likewise, prim and
+// primMeans 1..4 and 6+k) and the cell its own (EvaluateSpatialCorrelations1D,
+// :1363-1437: momenta and velocities averaged from the faces, the velocity means
+// from velMeans); the updates are the 3-D ones (:1441-1551) on spatialCrossMF
+// components star*ncross.. (a cell-centred fab without ghosts).
+struct Cross1DArgs {
+    Arr4<const double> cu, cum, pr, pm, mom[3], mm[3], velx, vm[3];
+    double* S;            // spatialCrossMF component 0 at cell (0, 0, 0)
+    int64_t qs;           // component stride (cells of the box)
+    int nx, ny, nz, xs, mf;   // x*, first component star*ncross
+    double hcv[MAXS];
+    double sm1, sinv;
+};
+
+template <int NS>
+static __global__ void __launch_bounds__(128) k_cross_1d(Cross1DArgs a) {
+    const int64_t tot = (int64_t)a.nx * a.ny * a.nz;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < tot; q += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q % a.nx), j = (int)((q / a.nx) % a.ny), k = (int)(q / ((int64_t)a.nx * a.ny));
+        const int xs = a.xs;
+        double dx[18 + 4 * NS];
+        dx[0] = a.cu(xs, j, k, 0);  dx[1] = a.cum(xs, j, k, 0);
+        dx[2] = a.cu(xs, j, k, 4);  dx[3] = a.cum(xs, j, k, 4);
 #pragma unroll
-    for (int n = 0; n < NS; ++n) upd(37 + n, delrhoYkcross[n] * delrhoYk[n]);
-    upd(37 + NS, delrhoYkcross[H] * delrhoYk[0]);
-    // (:1096-1104)
-    double dd = (S[37] * sm1 + delrhoYkcross[0] * delrhoYk[0]) * sinv;
-    S[37 + NS + 1] = (1.0 / (meanrho * meanrhocross)) *
-                     (dd - meanYkcross[0] * S[8] - meanYk[0] * S[10] + meanYkcross[0] * meanYk[0] * S[0]);
-    dd = (S[37 + H] * sm1 + delrhoYkcross[H] * delrhoYk[H]) * sinv;
-    S[37 + NS + 2] = (1.0 / (meanrho * meanrhocross)) *
-                     (dd - meanYkcross[H] * S[9] - meanYk[H] * S[11] + meanYkcross[H] * meanYk[H] * S[0]);
+        for (int d = 0; d < 3; ++d) {
+            dx[4 + 2 * d] = a.cu(xs, j, k, 1 + d);
+            dx[5 + 2 * d] = a.cum(xs, j, k, 1 + d);
+        }
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+            dx[10 + 2 * d] = a.pr(xs, j, k, 1 + d);
+            dx[11 + 2 * d] = a.pm(xs, j, k, 1 + d);
+        }
+#pragma unroll
+        for (int n = 0; n < NS; ++n) {
+            dx[18 + 4 * n + 0] = a.cu(xs, j, k, 5 + n);
+            dx[18 + 4 * n + 1] = a.cum(xs, j, k, 5 + n);
+            dx[18 + 4 * n + 2] = a.pr(xs, j, k, 6 + n);
+            dx[18 + 4 * n + 3] = a.pm(xs, j, k, 6 + n);
+        }
+        const CrossStar<NS> x = cross_star<NS>(dx, a.hcv);
+        CrossHere<NS> h;
+        h.meanrho = a.cum(i, j, k, 0);
+#pragma unroll
+        for (int n = 0; n < NS; ++n) {
+            h.meanYk[n] = a.pm(i, j, k, 6 + n);
+            h.delrhoYk[n] = a.cu(i, j, k, 5 + n) - a.cum(i, j, k, 5 + n);
+            h.delYk[n] = a.pr(i, j, k, 6 + n) - a.pm(i, j, k, 6 + n);
+        }
+        h.delrho = a.cu(i, j, k, 0) - a.cum(i, j, k, 0);
+        h.delK = a.cu(i, j, k, 4) - a.cum(i, j, k, 4);
+        h.deljx = 0.5 * (a.mom[0](i, j, k) + a.mom[0](i + 1, j, k)) - 0.5 * (a.mm[0](i, j, k) + a.mm[0](i + 1, j, k));
+        h.deljy = 0.5 * (a.mom[1](i, j, k) + a.mom[1](i, j + 1, k)) - 0.5 * (a.mm[1](i, j, k) + a.mm[1](i, j + 1, k));
+        h.deljz = 0.5 * (a.mom[2](i, j, k) + a.mom[2](i, j, k + 1)) - 0.5 * (a.mm[2](i, j, k) + a.mm[2](i, j, k + 1));
+        h.delT = a.pr(i, j, k, 4) - a.pm(i, j, k, 4);
+        h.delvx = 0.5 * (a.velx(i, j, k) + a.velx(i + 1, j, k)) - 0.5 * (a.vm[0](i, j, k) + a.vm[0](i + 1, j, k));
+        double cv = 0.;
+#pragma unroll
+        for (int l = 0; l < NS; ++l) cv = cv + a.hcv[l] * a.cum(i, j, k, 5 + l) / a.cum(i, j, k, 0);
+        h.cvinv = 1.0 / cv;
+        const double vxmean = 0.5 * (a.vm[0](i, j, k) + a.vm[0](i + 1, j, k));
+        const double vymean = 0.5 * (a.vm[1](i, j, k) + a.vm[1](i, j + 1, k));
+        const double vzmean = 0.5 * (a.vm[2](i, j, k) + a.vm[2](i, j, k + 1));
+        h.qmean = cv * a.pm(i, j, k, 4) - 0.5 * (vxmean * vxmean + vymean * vymean + vzmean * vzmean);
+        h.delG = vxmean * h.deljx + vymean * h.deljy + vzmean * h.deljz;
+        cross_update<NS>(a.S + (int64_t)a.mf * a.qs + q, a.qs, x, h, a.sm1, a.sinv);
+    }
 }
 
 static LineJob line_job(const fhd_fab& f, int comp, double* dst, int dstride) {
@@ -653,11 +760,44 @@ static int cross_launch(const DevParams& P, const fhd_fab& cu, const fhd_fab& pr
     return cuda_rc(cudaGetLastError());
 }
 
+// quasi-1-D: one launch per x*, in the reference's order (statsStag.cpp:168-193)
+template <int NS>
+static int cross1d_launch(const DevParams& P, const fhd_fab& cu, const fhd_fab& prim, const fhd_fab vel[3],
+                          const fhd_fab mom[3], const fhd_stats& st, const int* stars, int nstars, double sm1,
+                          double sinv, cudaStream_t s) {
+    Cross1DArgs a;
+    a.cu = view<const double>(cu);
+    a.cum = view<const double>(st.cuMeans);
+    a.pr = view<const double>(prim);
+    a.pm = view<const double>(st.primMeans);
+    for (int d = 0; d < 3; ++d) {
+        a.mom[d] = view<const double>(mom[d]);
+        a.mm[d] = view<const double>(st.cumomMeans[d]);
+        a.vm[d] = view<const double>(st.velMeans[d]);
+    }
+    a.velx = view<const double>(vel[0]);
+    a.S = st.spatialCross;
+    a.nx = P.n[0];
+    a.ny = P.n[1];
+    a.nz = P.n[2];
+    a.qs = (int64_t)a.nx * a.ny * a.nz;
+    for (int n = 0; n < MAXS; ++n) a.hcv[n] = n < NS ? P.hcv[n] : 0.0;
+    a.sm1 = sm1;
+    a.sinv = sinv;
+    for (int q = 0; q < nstars; ++q) {
+        a.xs = stars[q];
+        a.mf = q * (37 + NS + 3);
+        k_cross_1d<NS><<<grid_for(a.qs, 128), 128, 0, s>>>(a);
+    }
+    return cuda_rc(cudaGetLastError());
+}
+
 // doubles of the x-line scratch of FHD_STATS_CROSS
 int64_t stats_line_doubles(int ns, int nx) { return (int64_t)(2 * (5 + ns) + 2 * (ns + 4)) * nx; }
 
-int exact_stats(const DevParams& P, const fhd_fab& cu, const fhd_fab& prim, const fhd_fab mom[3],
-                const fhd_stats& st, int64_t steps, int flags, int cross_cell, double* lines, cudaStream_t s) {
+int exact_stats(const DevParams& P, const fhd_fab& cu, const fhd_fab& prim, const fhd_fab vel[3], const fhd_fab mom[3],
+                const fhd_stats& st, int64_t steps, int flags, const int* stars, int nstars, double* lines,
+                cudaStream_t s) {
     StatsArgs a;
     a.P = P;
     a.cu = view<const double>(cu);
@@ -690,12 +830,21 @@ int exact_stats(const DevParams& P, const fhd_fab& cu, const fhd_fab& prim, cons
         case 4: rc = stats_launch<4>(a, means, vars, st.cuMeans, st.primMeans, st.cuVars, st.primVars, s); break;
         default: return FHD_ERR_UNSUPPORTED;
     }
-    if (rc || !(flags & FHD_STATS_CROSS)) return rc;
+    // evaluateStatsStag2D has no correlations
+    if (rc || !(flags & FHD_STATS_CROSS) || P.dim == 2) return rc;
+    if (P.dim == 1) {
+        switch (P.ns) {
+            case 1: return cross1d_launch<1>(P, cu, prim, vel, mom, st, stars, nstars, a.sm1, a.sinv, s);
+            case 2: return cross1d_launch<2>(P, cu, prim, vel, mom, st, stars, nstars, a.sm1, a.sinv, s);
+            case 3: return cross1d_launch<3>(P, cu, prim, vel, mom, st, stars, nstars, a.sm1, a.sinv, s);
+            default: return cross1d_launch<4>(P, cu, prim, vel, mom, st, stars, nstars, a.sm1, a.sinv, s);
+        }
+    }
     switch (P.ns) {
-        case 1: return cross_launch<1>(P, cu, prim, st, cross_cell, a.sm1, a.sinv, lines, s);
-        case 2: return cross_launch<2>(P, cu, prim, st, cross_cell, a.sm1, a.sinv, lines, s);
-        case 3: return cross_launch<3>(P, cu, prim, st, cross_cell, a.sm1, a.sinv, lines, s);
-        default: return cross_launch<4>(P, cu, prim, st, cross_cell, a.sm1, a.sinv, lines, s);
+        case 1: return cross_launch<1>(P, cu, prim, st, stars[0], a.sm1, a.sinv, lines, s);
+        case 2: return cross_launch<2>(P, cu, prim, st, stars[0], a.sm1, a.sinv, lines, s);
+        case 3: return cross_launch<3>(P, cu, prim, st, stars[0], a.sm1, a.sinv, lines, s);
+        default: return cross_launch<4>(P, cu, prim, st, stars[0], a.sm1, a.sinv, lines, s);
     }
 }
 

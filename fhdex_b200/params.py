@@ -87,6 +87,8 @@ class Params:
     # in x (x and y), timeStepStag.cpp:172-323; transport on one ghost layer in 1-D
     do_1D: int = 0
     do_2D: int = 0
+    # quasi-1-D statistics: correlate with five x* instead of cross_cell (compressible::all_correl)
+    all_correl: int = 0
 
     @property
     def nvars(self):
@@ -167,6 +169,7 @@ class Params:
         p.cross_cell = self.cross_cell
         p.do_1D = self.do_1D
         p.do_2D = self.do_2D
+        p.all_correl = self.all_correl
         for i in range(MAX_SPECIES):
             p.rhobar[i] = self.rhobar[i] if i < len(self.rhobar) else 0.0
         return p
@@ -342,7 +345,8 @@ def to_inputs(p: "Params") -> str:
              f"algorithm_type = {p.algorithm_type}", f"visc_type = {p.visc_type}",
              f"advection_type = {p.advection_type}", f"transport_type = {p.transport_type}",
              f"stoch_stress_form = {p.stoch_stress_form}", f"seed = {p.seed}", "prob_type = 1",
-             f"cross_cell = {p.cross_cell}", f"do_1D = {p.do_1D}", f"do_2D = {p.do_2D}"]
+             f"cross_cell = {p.cross_cell}", f"do_1D = {p.do_1D}", f"do_2D = {p.do_2D}",
+             f"all_correl = {p.all_correl}"]
     if p.zeta_ratio >= 0:
         lines.append(f"zeta_ratio = {_fmt(float(p.zeta_ratio))}")
     for key in ("bc_vel_lo", "bc_vel_hi", "bc_mass_lo", "bc_mass_hi", "bc_therm_lo", "bc_therm_hi"):
@@ -402,7 +406,7 @@ def parse_inputs(text: str, base: Params | None = None) -> Params:
         if key in kv:
             upd[key] = float(kv[key][0])
     for key in ("algorithm_type", "visc_type", "advection_type", "transport_type",
-                "stoch_stress_form", "seed", "cross_cell", "do_1D", "do_2D"):
+                "stoch_stress_form", "seed", "cross_cell", "do_1D", "do_2D", "all_correl"):
         if key in kv:
             upd[key] = int(kv[key][0])
     # chemistry keys (chemistry_functions.cpp:45-124); avogadro overrides Runiv

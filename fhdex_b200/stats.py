@@ -14,7 +14,10 @@ Component maps (statsStag.cpp:200-691):
   velMeans/velVars/cumomMeans/cumomVars   face-centred, one per direction
   spatialCross       (cross=True) n_cells[0] x ncross yz-averaged spatial
                      cross-correlations at x* = Params.cross_cell, ncross =
-                     37 + nspecies + 3 (statsStag.cpp:868-1105; main_driver.cpp:283)
+                     37 + nspecies + 3 (statsStag.cpp:868-1105; main_driver.cpp:283);
+                     in a quasi-1-D run the per-pencil correlations, spatialCrossMF
+                     (ncross or 5 ncross comps, nz, ny, nx; statsStag.cpp:1311-1557);
+                     in a quasi-2-D run an ncross-component field left at zero
   dataSliceMeans_xcross  (cross=True) the 2*nvars + 8 + 2*nspecies line
                      averages at x* (the reference's crossMeans file rows)
 """
@@ -55,7 +58,14 @@ class StatsState:
         self.velVars = [MultiFab(N, FACE[d], 1, 0, **kw) for d in range(3)]
         self.cumomMeans = [MultiFab(N, FACE[d], 1, 0, **kw) for d in range(3)]
         self.cumomVars = [MultiFab(N, FACE[d], 1, 0, **kw) for d in range(3)]
-        self.spatialCross = torch.zeros(N[0], ncross(p.nspecies), **kw) if cross else None
+        if cross and p.do_1D:
+            # evaluateStatsStag1D's spatialCrossMF: cell-centred, no ghosts, ncross comps per x*
+            nst = 5 if p.all_correl == 1 else 1
+            self.spatialCross = torch.zeros(nst * ncross(p.nspecies), N[2], N[1], N[0], **kw)
+        elif cross and p.do_2D:
+            self.spatialCross = torch.zeros(ncross(p.nspecies), N[2], N[1], N[0], **kw)
+        else:
+            self.spatialCross = torch.zeros(N[0], ncross(p.nspecies), **kw) if cross else None
         self.dataSliceMeans_xcross = torch.zeros(nstats(p.nspecies), **kw) if cross else None
 
     def named(self):
@@ -87,11 +97,13 @@ class StatsState:
             s.dataSliceMeans_xcross.copy_(self.dataSliceMeans_xcross)
         return s
 
-    def write_spatial_cross(self, step: int, base: str = "spatialCross"):
-        """WriteSpatialCross3D (writePlotFileStag.cpp:528-549): <base><step, 9 digits>."""
+    def write_spatial_cross(self, step: int, dir: str = ""):
+        """WriteSpatialCross3D / WriteSpatialCross1D (writePlotFileStag.cpp:528-563):
+        the reference's file names (spatialCross<step, 9 digits>, or
+        [<s>_]spatialCross1D_<step> in a quasi-1-D run) prefixed by ``dir``."""
         from . import capi
         cp = self.p.to_c()
-        capi.check(capi.load().fhd_write_spatial_cross(cp, base.encode(), step, self.spatialCross.data_ptr()),
+        capi.check(capi.load().fhd_write_spatial_cross(cp, dir.encode(), step, self.spatialCross.data_ptr()),
                    "fhd_write_spatial_cross")
 
     def append_cross_means(self, path: str, step: int):

@@ -696,7 +696,7 @@ inline void WriteSpatialCross3D(const fhd::amrex_compat::Vector<fhd::amrex_compa
     const fhd_params p = params_from_globals();
     if (ncross != fhd_spatial_cross_ncross(p.nspecies) || spatialCross.size() < (size_t)p.n_cells[0] * ncross)
         fail("WriteSpatialCross3D", FHD_ERR_BAD_ARG);
-    check(fhd_write_spatial_cross(&p, "spatialCross", step, spatialCross.data()), "WriteSpatialCross3D");
+    check(fhd_write_spatial_cross(&p, "", step, spatialCross.data()), "WriteSpatialCross3D");
 }
 
 // WriteCheckPoint (Checkpoint.cpp:28-257): chk<step, 9 digits>/ in the working

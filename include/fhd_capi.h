@@ -151,6 +151,10 @@ typedef struct {
      * then exactly 2, and the batched and no-allocation steps return
      * FHD_ERR_UNSUPPORTED. */
     int do_1D, do_2D;
+    /* With do_1D and FHD_STATS_CROSS: 0 correlates with x* = cross_cell, 1 with the
+     * five x* 0, floor(n/4), floor(n/2), floor(3n/4), n-1 (deck key all_correl,
+     * statsStag.cpp:168-193). */
+    int all_correl;
 } fhd_params;
 
 /* Injected Gaussian noise for one RK3 step: the "A" and "B" white-noise fields
@@ -416,7 +420,14 @@ int fhd_batch_autotune(fhd_batch* batch, int reps, double* ms, int* best);
  * doubles, entry i*ncross + n, the reference's spatialCrossVec) is updated in
  * place; `dataSliceMeans_xcross` (device, fhd_spatial_cross_nstats doubles)
  * receives the line averages at x* that the reference appends to its crossMeans
- * file.  Without surface coverage (nspec_surfcov = 0).  Fabs have the
+ * file.  In a quasi-1-D run (params.do_1D) FHD_STATS_CROSS is evaluateStatsStag1D's
+ * (statsStag.cpp:130-197): per y-z pencil the correlations with the pencil's own
+ * cell at x* (GetPencilCross, EvaluateSpatialCorrelations1D :810-866, 1311-1557),
+ * into `spatialCross` as the reference's spatialCrossMF: the valid cells of a
+ * cell-centred MultiFab without ghosts, fhd_spatial_cross_ncross comps per x* (five
+ * x* with params.all_correl), component slowest, x fastest; dataSliceMeans_xcross
+ * is unused.  A quasi-2-D run ignores FHD_STATS_CROSS, as evaluateStatsStag2D does.
+ * Without surface coverage (nspec_surfcov = 0).  Fabs have the
  * reference's shapes (main_driver.cpp:646-714): cuMeans/cuVars nvars comps,
  * primMeans nprimvars+3 comps, primVars nprimvars+5 comps, coVars 26 comps,
  * mom3/mom4 nvars+1 comps, all cell-centred; velMeans/velVars/cumomMeans/
@@ -487,11 +498,15 @@ int fhd_read_checkpoint(const fhd_params* params, const char* chk_base, int rest
                         int* stats_count, fhd_fab cu, const fhd_fab cumom[3], fhd_fab prim, const fhd_fab vel[3],
                         const fhd_stats* stats);
 
-/* WriteSpatialCross3D (writePlotFileStag.cpp:528-549): the text file
- * <base><step, 9 digits> (the reference's base is "spatialCross"), one line per x
- * cell with its centre and the ncross entries of spatialCross (host or device
- * memory), in the reference's number formatting. */
-int fhd_write_spatial_cross(const fhd_params* params, const char* base, int step, const double* spatial_cross);
+/* WriteSpatialCross3D / WriteSpatialCross1D (writePlotFileStag.cpp:528-563) in the
+ * reference's number formatting, from spatialCross in host or device memory, under
+ * the reference's file names prefixed by `dir` ("" for the working directory, else
+ * e.g. "out/"): 3-D runs <dir>spatialCross<step, 9 digits>, one line per x cell with
+ * its centre and the ncross entries; quasi-1-D runs <dir>spatialCross1D_<step> (or,
+ * with all_correl, <dir><s>_spatialCross1D_<step> for the five x*), the y-z averages
+ * of every component per x cell (WriteHorizontalAverage, ComputeAverages.cpp:8-94).
+ * Quasi-2-D runs write nothing (the reference's 2-D writer is not enabled). */
+int fhd_write_spatial_cross(const fhd_params* params, const char* dir, int step, const double* spatial_cross);
 
 /* pack, copy to the host and write the plotfile directory (blocks on the stream;
  * allocates and frees a temporary device buffer of the packed size) */

@@ -67,6 +67,8 @@ def lib():
         L.fhdref_set_reservoir_draws.argtypes = [vp, i]
         L.fhdref_eval_stats3d.argtypes = [vp, vp, pp, pp, pp, P(i), pp, vp, vp, i, i]
         L.fhdref_write_spatial_cross.argtypes = [vp, i, i]
+        L.fhdref_eval_stats_lowdim.argtypes = [vp, vp, pp, pp, pp, P(i), pp, vp, i, i, i]
+        L.fhdref_write_spatial_cross_1d.argtypes = [vp, i, i, i]
         L.fhdref_plotfile.argtypes = [vp, pp, vp, pp, vp, vp, vp, pp, P(i), pp, i, d, vp, C.c_long, C.c_char_p, i,
                                       P(i)]
         _lib = L
@@ -354,10 +356,23 @@ def eval_stats(st, stats, steps, flags):
     cells = [stats.cuMeans, stats.cuVars, stats.primMeans, stats.primVars, stats.coVars, stats.mom3, stats.mom4]
     ng = (C.c_int * 7)(*[m.ngrow for m in cells])
     faces = stats.velMeans + stats.velVars + stats.cumomMeans + stats.cumomVars
+    ncross = 37 + p.nspecies + 3
+    if p.do_1D or p.do_2D:
+        if stats.spatialCross is not None:
+            sc = stats.spatialCross
+        else:
+            N = p.n_cells
+            sc = torch.zeros((5 if p.do_1D and p.all_correl == 1 else 1) * ncross, N[2], N[1], N[0],
+                             dtype=torch.float64)
+        _chk(lib().fhdref_eval_stats_lowdim(_ptr(st.cu.arr), _ptr(st.prim.arr), _ptrs([m.arr for m in st.vel]),
+                                            _ptrs([m.arr for m in st.cumom]), _ptrs([m.arr for m in cells]), ng,
+                                            _ptrs([m.arr for m in faces]), _ptr(sc), sc.shape[0], ncross, int(steps)),
+             "evaluateStatsStag1D/2D")
+        return
     if stats.spatialCross is not None:
         sc, xc = stats.spatialCross, stats.dataSliceMeans_xcross
     else:
-        sc = torch.zeros(p.n_cells[0], 37 + p.nspecies + 3, dtype=torch.float64)
+        sc = torch.zeros(p.n_cells[0], ncross, dtype=torch.float64)
         xc = torch.zeros(2 * p.nvars + 8 + 2 * p.nspecies, dtype=torch.float64)
     _chk(lib().fhdref_eval_stats3d(_ptr(st.cu.arr), _ptr(st.prim.arr), _ptrs([m.arr for m in st.vel]),
                                    _ptrs([m.arr for m in st.cumom]), _ptrs([m.arr for m in cells]), ng,
@@ -404,3 +419,12 @@ def write_spatial_cross(p, spatial_cross, step):
     init(p)
     sc = spatial_cross.contiguous()
     _chk(lib().fhdref_write_spatial_cross(_ptr(sc), int(step), sc.shape[1]), "WriteSpatialCross3D")
+
+
+def write_spatial_cross_1d(p, spatial_cross, step):
+    """The reference's WriteSpatialCross1D (writePlotFileStag.cpp:551-563) into the
+    current working directory."""
+    init(p)
+    sc = spatial_cross.contiguous()
+    _chk(lib().fhdref_write_spatial_cross_1d(_ptr(sc), sc.shape[0], int(step), 37 + p.nspecies + 3),
+         "WriteSpatialCross1D")

@@ -480,6 +480,52 @@ int fhdref_plotfile(double* cu, double* const* mom, double* prim, double* const*
     });
 }
 
+// evaluateStatsStag1D / evaluateStatsStag2D (statsStag.cpp:78-197) of a quasi-1-D /
+// 2-D run (the deck's do_1D / do_2D, all_correl), arguments as fhdref_eval_stats3d;
+// spatial_cross is the storage of spatialCrossMF (cell-centred, no ghosts,
+// ncomp_cross components).
+int fhdref_eval_stats_lowdim(double* cu, double* prim, double* const* vel, double* const* mom, double* const* cells,
+                             const int* ng, double* const* faces, double* spatial_cross, int ncomp_cross, int ncross,
+                             int steps) {
+    return guarded([&] {
+        const int g = ngc[0];
+        MultiFab c, p, cm, cv, pm, pv, cov, m3, m4, th, thm, thv, thc, sc;
+        std::array<MultiFab, 3> v, m, vm, vv, mm, mv;
+        wrap(c, cu, IntVect(0), nvars, g);
+        wrap(p, prim, IntVect(0), nprimvars, g);
+        wrap3(v, vel, 1, g, true);
+        wrap3(m, mom, 1, g, true);
+        wrap(cm, cells[0], IntVect(0), nvars, ng[0]);
+        wrap(cv, cells[1], IntVect(0), nvars, ng[1]);
+        wrap(pm, cells[2], IntVect(0), nprimvars + 3, ng[2]);
+        wrap(pv, cells[3], IntVect(0), nprimvars + 5, ng[3]);
+        wrap(cov, cells[4], IntVect(0), 26, ng[4]);
+        wrap(m3, cells[5], IntVect(0), nvars + 1, ng[5]);
+        wrap(m4, cells[6], IntVect(0), nvars + 1, ng[6]);
+        wrap3(vm, faces, 1, 0, true);
+        wrap3(vv, faces + 3, 1, 0, true);
+        wrap3(mm, faces + 6, 1, 0, true);
+        wrap3(mv, faces + 9, 1, 0, true);
+        wrap(sc, spatial_cross, IntVect(0), ncomp_cross, 0);
+        if (do_1D)
+            evaluateStatsStag1D(c, cm, cv, p, pm, pv, v, vm, vv, m, mm, mv, cov, m3, m4, th, thm, thv, thc, sc, ncross,
+                                steps, g_geom);
+        else
+            evaluateStatsStag2D(c, cm, cv, p, pm, pv, v, vm, vv, m, mm, mv, cov, m3, m4, th, thm, thv, thc, sc, ncross,
+                                steps, g_geom);
+    });
+}
+
+// WriteSpatialCross1D (writePlotFileStag.cpp:551-563) into the working directory
+// from the storage of spatialCrossMF.
+int fhdref_write_spatial_cross_1d(double* spatial_cross, int ncomp_cross, int step, int ncross) {
+    return guarded([&] {
+        MultiFab sc;
+        wrap(sc, spatial_cross, IntVect(0), ncomp_cross, 0);
+        WriteSpatialCross1D(sc, step, g_geom, ncross);
+    });
+}
+
 // WriteSpatialCross3D (writePlotFileStag.cpp:528-549): spatialCross<step, 9
 // digits> in the working directory from n_cells[0]*ncross values.
 int fhdref_write_spatial_cross(const double* spatial_cross, int step, int ncross) {

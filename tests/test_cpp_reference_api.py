@@ -190,7 +190,7 @@ def test_reference_driver_statistics_equal_c_abi_statistics(driver, tmp_path):
         ctx.rk3_step(st, dt, step, aux=True)
         ctx.stats_stag(st, stats, step + 1, 15 | capi.STATS_CROSS)
     torch.cuda.synchronize()
-    stats.write_spatial_cross(nsteps, str(tmp_path / "spatialCross"))
+    stats.write_spatial_cross(nsteps, str(tmp_path) + "/")
     fname = f"spatialCross{nsteps:09d}"
     assert open(run_dir / fname).read() == open(tmp_path / fname).read()
     mfs = [stats.cuMeans, stats.cuVars, stats.primMeans, stats.primVars, stats.coVars, stats.mom3, stats.mom4]

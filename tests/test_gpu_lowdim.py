@@ -126,3 +126,37 @@ def test_lowdim_transport_operator_equals_the_reference(ref):
     for name in ("eta", "zeta", "kappa", "chi", "D"):
         assert torch.equal(getattr(d, name).arr.cpu(), getattr(st, name).arr), name
     assert (st.eta.arr[0, 0] == -7.0).all() and (st.eta.arr[0, 2, 2, 2] != -7.0)
+
+
+@pytest.mark.parametrize("name,all_correl", [("periodic_1d_mix", 0), ("periodic_1d", 1), ("tempgrad_1d", 0),
+                                             ("periodic_2d", 0)])
+def test_lowdim_statistics_equal_the_reference(ref, name, all_correl):
+    """fhd_stats_stag with every flag and FHD_STATS_CROSS in a quasi-1-D run (the
+    per-pencil correlations with x* = cross_cell, or the five x* of all_correl) and
+    in a quasi-2-D run (no correlations), after steps of the run, bit for bit
+    against the reference's evaluateStatsStag1D / 2D."""
+    from fhdex_b200 import capi
+    from fhdex_b200.stats import StatsState
+    p = CASES[name]().replace(cross_cell=3, all_correl=all_correl)
+    st = ref.state_from_reference(p, seed=13)
+    d = st.clone(device="cuda")
+    ctx = Context(p)
+    dt = DT.get(name, stable_dt(p))
+    host = StatsState(p, cross=True)
+    dev = StatsState(p, "cuda", cross=True)
+    flags = 15 | capi.STATS_CROSS
+    for s in range(3):
+        nz = ref.step_noise(p, seed=90 + s)
+        ctx.rk3_step(d, dt, s, noise=nz.to("cuda"), aux=False)
+        ref.rk3_step(st, nz, dt, s)
+        ctx.stats_stag(d, dev, s + 1, flags)
+        ref.eval_stats(st, host, s + 1, flags)
+    torch.cuda.synchronize()
+    bad = [n for n, m in dev.named().items() if not torch.equal(m.arr.cpu(), host.named()[n].arr)]
+    assert not bad, bad
+    assert torch.equal(dev.spatialCross.cpu(), host.spatialCross)
+    if p.do_1D:
+        assert host.spatialCross.abs().max() > 0
+    else:
+        assert not host.spatialCross.any()
+    assert ctx.status() == 0

@@ -85,3 +85,50 @@ def test_reference_step_has_no_transverse_stresses(ref, mode):
     assert st.faceflux[0].arr[nv].abs().max() > 0
     for m in st.state_mfs():
         assert torch.isfinite(m.arr).all()
+
+
+@pytest.mark.parametrize("all_correl", [0, 1])
+def test_1d_correlation_files_equal_the_references(ref, tmp_path, monkeypatch, all_correl):
+    """The reference's evaluateStatsStag1D over three samples fills spatialCrossMF;
+    fhd_write_spatial_cross (host memory) writes the same WriteSpatialCross1D files
+    byte for byte (one file, or five with all_correl)."""
+    from fhdex_b200.stats import StatsState
+    p = mixture4((12, 3, 4), dx=8e-6).replace(do_1D=1, cross_cell=5, all_correl=all_correl)
+    stats = StatsState(p, cross=True)
+    for s in range(1, 4):
+        st = ref.state_from_reference(p, seed=20 + s)
+        ref.eval_stats(st, stats, s, 15 | capi.STATS_CROSS)
+    assert stats.spatialCross.shape[0] == (5 if all_correl else 1) * (37 + 4 + 3)
+    assert stats.spatialCross[0].abs().max() > 0
+    mine, theirs = tmp_path / "mine", tmp_path / "ref"
+    mine.mkdir()
+    theirs.mkdir()
+    stats.write_spatial_cross(9, str(mine) + "/")
+    monkeypatch.chdir(theirs)
+    ref.write_spatial_cross_1d(p, stats.spatialCross, 9)
+    names = sorted(f.name for f in theirs.iterdir())
+    assert names == sorted(f.name for f in mine.iterdir()) and len(names) == (5 if all_correl else 1)
+    for n in names:
+        assert (mine / n).read_bytes() == (theirs / n).read_bytes(), n
+
+
+def test_1d_checkpoint_keeps_spatial_cross_mf(tmp_path):
+    """A quasi-1-D run's checkpoint: spatialCrossMF as a Level_0 MultiFab (bit for bit
+    back), the Header's spatialCrossVec left at zero (Checkpoint.cpp:112-118, 251-256)."""
+    import os
+    from fhdex_b200.checkpoint import read_checkpoint, write_checkpoint
+    from fhdex_b200.state import StagState
+    from fhdex_b200.stats import StatsState
+    p = argon((6, 3, 2), dx=8e-6).replace(do_1D=1, all_correl=1)
+    st = StagState(p)
+    stats = StatsState(p, cross=True)
+    g = torch.Generator().manual_seed(3)
+    stats.spatialCross.copy_(torch.randn(stats.spatialCross.shape, generator=g, dtype=torch.float64))
+    path = write_checkpoint(p, str(tmp_path / "chk"), 2, 0.5, st, stats, stats_count=2)
+    assert os.path.exists(os.path.join(path, "Level_0", "spatialCrossMF_H"))
+    lines = open(os.path.join(path, "Header")).read().split("\n")
+    vals = [v for v in lines[lines.index(")") + 1:] if v]
+    assert vals == ["0"] * (6 * (37 + 2 + 3))
+    back = StatsState(p, cross=True)
+    read_checkpoint(p, str(tmp_path / "chk"), 2, StagState(p), back)
+    assert torch.equal(back.spatialCross, stats.spatialCross)
