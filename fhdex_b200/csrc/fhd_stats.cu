@@ -389,7 +389,8 @@ static int stats_launch(const StatsArgs& a, bool means, bool vars, const fhd_fab
 // the pace: a batch inside one k-plane takes its 32 row addresses as independent
 // base + u*sy products rather than a running offset.
 constexpr int kMaxLineJobs = 2 * (5 + MAXS) + 2 * (MAXS + 4);
-constexpr int kLineRows = 32, kLineStages = 6;   // 48 KiB of shared memory per one-warp block
+constexpr int kLineRows = 32, kLineStages = 12;   // 96 KiB of dynamic shared memory per one-warp block
+constexpr int kLineSmem = kLineStages * kLineRows * 32 * (int)sizeof(double);
 struct LineJob {
     const double* src;   // component n of the source at valid cell (0, 0, 0)
     double* dst;         // line entry (0, n)
@@ -410,7 +411,8 @@ template <int N>
 FHD_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 static __global__ void __launch_bounds__(32) k_sum_to_line(const __grid_constant__ LineArgs a) {
-    __shared__ __align__(16) double buf[kLineStages][kLineRows][32];
+    extern __shared__ __align__(16) double line_smem[];
+    double(*buf)[kLineRows][32] = reinterpret_cast<double(*)[kLineRows][32]>(line_smem);
     const int lane = threadIdx.x;
     const int c = blockIdx.x / a.xblocks;
     const int i = (blockIdx.x - c * a.xblocks) * 32 + lane;
@@ -742,7 +744,10 @@ static int cross_launch(const DevParams& P, const fhd_fab& cu, const fhd_fab& pr
     la.nx = nx;
     la.ny = P.n[1];
     la.nz = P.n[2];
-    k_sum_to_line<<<(unsigned)(la.xblocks * q), 32, 0, s>>>(la);
+    // on every call: the attribute belongs to the current device's copy of the kernel
+    const cudaError_t e = cudaFuncSetAttribute(k_sum_to_line, cudaFuncAttributeMaxDynamicSharedMemorySize, kLineSmem);
+    if (e != cudaSuccess) return cuda_rc(e);
+    k_sum_to_line<<<(unsigned)(la.xblocks * q), 32, kLineSmem, s>>>(la);
     CrossArgs ca;
     ca.cu = L[0];
     ca.cum = L[1];
