@@ -20,6 +20,7 @@ FHD_ERR_TIMEOUT = 5
 FHD_ERR_CUDA = 6
 FHD_ERR_UNSUPPORTED = 7
 FHD_ERR_TOO_LARGE = 8
+FHD_ERR_SINGULAR = 9
 
 FHD_F64 = 0
 FHD_F32 = 1

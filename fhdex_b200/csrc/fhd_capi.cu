@@ -9,6 +9,7 @@
 
 #include "fhd_host.h"
 #include "fhd_chem.cuh"
+#include "fhd_transport_alt.cuh"
 #include "philox.cuh"
 
 using namespace fhd;
@@ -43,6 +44,8 @@ struct fhd_ctx {
     double* res_rec = nullptr;   // test hook: the particle reservoir's draws
     int res_cap = 0;
     WallParams wall{};
+    // the Valk/Waldmann model's pair constants (transport_type 2), device memory
+    VWTable* vwt = nullptr;
     // x-line scratch of the spatial cross-correlations (fhd_stats_stag, FHD_STATS_CROSS)
     double* lines = nullptr;
     size_t lines_bytes = 0;
@@ -105,7 +108,42 @@ bool fab_ok(const fhd_ctx* c, const fhd_fab& f, const int nodal[3], int min_ng, 
     return true;
 }
 
-DevParams make_dev(const fhd_ctx* c, double dt, uint64_t step) { return dev_params(c->prm, dt, step); }
+DevParams make_dev(const fhd_ctx* c, double dt, uint64_t step) {
+    DevParams P = dev_params(c->prm, dt, step);
+    P.vwt = c->vwt;
+    return P;
+}
+
+// IdealMixtureTransportVW's cell-independent parts (compressible_functions.H:1047-1121)
+// and the powers ViscLin and LambdaLin take of the molecular masses, by the reference's
+// own expressions (the host's pow, as the reference's CPU build has it)
+void vw_table(const fhd_params& p, VWTable& t) {
+    std::memset(&t, 0, sizeof(t));
+    const double pi = 3.1415926535897932, k_B = p.k_B;
+    const int ns = p.nspecies;
+    double m[MAXS];
+    for (int n = 0; n < ns; ++n) m[n] = p.molmass[n] * (k_B / p.Runiv);
+    const double Fijstar = -27. / 5.;
+    for (int i = 0; i < ns; ++i) {
+        t.pm2[i] = std::pow(m[i], 2.);
+        for (int j = 0; j < ns; ++j) {
+            const int q = i * MAXS + j;
+            const double diamat = 0.5 * (p.diameter[i] + p.diameter[j]);
+            const double mu = m[i] * m[j] / (m[i] + m[j]);
+            const double Fij = (6.0 * m[i] * m[i] + 13.0 / 5.0 * m[j] * m[j] + 16.0 / 5.0 * m[i] * m[j]) /
+                               (std::pow(m[i] + m[j], 2.));
+            const double sigma11bar = std::sqrt(k_B / (2.0 * pi * mu)) * pi * std::pow(diamat, 2.);
+            t.alphabar[q] = 8.0 / (3.0 * k_B) * mu * mu * (-.5 * sigma11bar);
+            t.DbinC[q] = 3.0 / 16.0 * std::sqrt(2.0 * pi * std::pow(k_B, 3.) * (m[i] + m[j]) / m[i] / m[j]) /
+                         (pi * std::pow(diamat, 2.));
+            t.omegaC[q] = std::sqrt(pi * k_B / (2.0 * mu)) * std::pow(diamat, 2.);
+            t.a1C[q] = 5.0 / (k_B)*m[i] * m[j] / (m[i] + m[j]) * Fij * sigma11bar;
+            t.a2C[q] = 5.0 / (k_B)*m[i] * m[j] * m[i] * m[j] / (std::pow(m[i] + m[j], 3.)) * Fijstar * sigma11bar;
+            t.ps2[q] = std::pow(m[i] + m[j], 2.);
+            t.ps3[q] = std::pow(m[i] + m[j], 3.);
+        }
+    }
+}
 
 // With walls the state has the reference's ghost width exactly (the conditions
 // fill every ghost layer, as the stage buffers have NGC of them)
@@ -282,6 +320,7 @@ const char* fhd_strerror(int code) {
         case FHD_ERR_CUDA: return "CUDA runtime error";
         case FHD_ERR_UNSUPPORTED: return "option outside the implemented scope";
         case FHD_ERR_TOO_LARGE: return "box too large for the 16 MiB static scratch of fhd_rk3_step_stag_noalloc";
+        case FHD_ERR_SINGULAR: return "singular Valk/Waldmann transport system (reference: amrex::Abort in Decomp)";
         default: return "unknown error";
     }
 }
@@ -375,7 +414,11 @@ int fhd_create(fhd_ctx** out, const fhd_params* params, int device) {
     for (int d = 0; d < 3; ++d)
         if (p.n_cells[d] < 2 || !(p.prob_hi[d] > p.prob_lo[d])) return FHD_ERR_BAD_ARG;
     if ((int64_t)p.n_cells[0] * p.n_cells[1] * p.n_cells[2] >= ((int64_t)1 << 32)) return FHD_ERR_UNSUPPORTED;
-    if (p.algorithm_type != 2 || p.transport_type != 1) return FHD_ERR_UNSUPPORTED;
+    // algorithm_type 2 is the multispecies path every staggered deck runs; transport models
+    // 1 Giovangigli, 2 Valk/Waldmann, 3 HCB (binary mixtures only)
+    if (p.algorithm_type != 2 || p.transport_type < 1 || p.transport_type > 3) return FHD_ERR_UNSUPPORTED;
+    if (p.transport_type == 3 && p.nspecies != 2) return FHD_ERR_BAD_ARG;
+    if (p.transport_type != 1 && p.precision != FHD_PREC_FP64) return FHD_ERR_UNSUPPORTED;
     if (p.stoch_stress_form != 0 && p.stoch_stress_form != 1) return FHD_ERR_UNSUPPORTED;
     if (p.advection_type < -1 || p.advection_type > 2) return FHD_ERR_UNSUPPORTED;
     if (p.precision != FHD_PREC_FP64 && p.precision != FHD_PREC_MIXED) return FHD_ERR_BAD_ARG;
@@ -427,7 +470,7 @@ int fhd_create(fhd_ctx** out, const fhd_params* params, int device) {
         }
     for (int d = 0; d < 3; ++d) c->per[d] = per[d];
     c->walls = walls;
-    c->refpipe = walls || lowdim;
+    c->refpipe = walls || lowdim || p.transport_type != 1;
     c->wall = wall;
     for (int d = 0; d < 3; ++d) {
         if (!per[d] && (p.bc_mass_lo[d] >= 3 || p.bc_mass_hi[d] >= 3)) c->reservoir = true;
@@ -448,6 +491,16 @@ int fhd_create(fhd_ctx** out, const fhd_params* params, int device) {
         return FHD_ERR_OOM;
     }
     cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream);
+    if (p.transport_type == 2) {
+        VWTable t;
+        vw_table(c->prm, t);
+        if (cudaMalloc(&c->vwt, sizeof(VWTable)) != cudaSuccess ||
+            cudaMemcpy(c->vwt, &t, sizeof(VWTable), cudaMemcpyHostToDevice) != cudaSuccess) {
+            cudaGetLastError();
+            fhd_destroy(c);
+            return FHD_ERR_OOM;
+        }
+    }
     *out = c;
     return FHD_OK;
 }
@@ -459,6 +512,7 @@ int fhd_destroy(fhd_ctx* c) {
     if (c->scratch) cudaFree(c->scratch);
     if (c->coef) cudaFree(c->coef);
     if (c->lines) cudaFree(c->lines);
+    if (c->vwt) cudaFree(c->vwt);
     if (c->res.base) cudaFree(c->res.base);
     if (c->hbuf) cudaFree(c->hbuf);
     for (auto& e : c->evs) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }

@@ -68,6 +68,10 @@ struct DevParams {
     // noise (1 in 1-D, sqrt(2) otherwise: timeStepStag.cpp:208-222)
     int dim;
     double fac2d, csd0;
+    // transport model (transCoeffs.cpp:58-73): 1 Giovangigli, 2 Valk/Waldmann (pair
+    // constants in the device table vwt), 3 HCB binary
+    int transport_type;
+    const struct VWTable* vwt;
     // noise
     uint32_t key0, key1;             // Philox key
     uint64_t step;                   // Philox counter words 2-3

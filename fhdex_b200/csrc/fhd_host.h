@@ -82,6 +82,8 @@ inline DevParams dev_params(const fhd_params& p, double dt, uint64_t step) {
     P.dim = p.do_1D ? 1 : (p.do_2D ? 2 : 3);
     P.fac2d = (3.0 + sqrt(3.0)) / 2.0;
     P.csd0 = p.do_1D ? 1.0 : sqrt(2.0);
+    P.transport_type = p.transport_type;
+    P.vwt = nullptr;
     P.walls = p.walls ? 1 : 0;
     for (int d = 0; d < 3; ++d) {
         P.periodic[d] = !P.walls || (p.bc_vel_lo[d] == -1 && p.bc_vel_hi[d] == -1);

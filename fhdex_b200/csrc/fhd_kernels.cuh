@@ -13,6 +13,7 @@
 //   k_noise_*   Philox noise fills;  k_init_uniform  InitConsVarStag prob_type 1
 #pragma once
 #include "fhd_flux.cuh"
+#include "fhd_transport_alt.cuh"
 
 namespace fhd {
 
@@ -538,8 +539,13 @@ static __global__ void __launch_bounds__(128) k_transport(TransArgs<NS> a) {
 #pragma unroll
         for (int n = 0; n < NS; ++n) Y[n] = a.prim(i, j, k, 6 + n);
         Coeffs<NS, double> c;
-        if (!transport_gio<NS, double>(P, a.prim(i, j, k, 0), a.prim(i, j, k, 4), a.prim(i, j, k, 5), Y, c))
+        if (P.transport_type != 1) {
+            // Valk/Waldmann or HCB binary (runs with these models take this kernel)
+            const int st = transport_alt<NS>(P, a.prim(i, j, k, 0), a.prim(i, j, k, 4), a.prim(i, j, k, 5), Y, c);
+            if (st) flag(a.status, st);
+        } else if (!transport_gio<NS, double>(P, a.prim(i, j, k, 0), a.prim(i, j, k, 4), a.prim(i, j, k, 5), Y, c)) {
             flag(a.status, ST_MASSFRAC);
+        }
         a.eta(i, j, k) = c.eta;
         a.kappa(i, j, k) = c.kappa;
         a.zeta(i, j, k) = c.zeta;

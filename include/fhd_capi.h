@@ -48,7 +48,8 @@ enum {
     FHD_ERR_TIMEOUT = 5,     /* a bounded device wait gave up                     */
     FHD_ERR_CUDA = 6,        /* a CUDA runtime call failed                        */
     FHD_ERR_UNSUPPORTED = 7, /* option outside the implemented scope              */
-    FHD_ERR_TOO_LARGE = 8    /* box does not fit fhd_rk3_step_stag_noalloc's scratch */
+    FHD_ERR_TOO_LARGE = 8,   /* box does not fit fhd_rk3_step_stag_noalloc's scratch */
+    FHD_ERR_SINGULAR = 9     /* a singular Valk/Waldmann system (the reference's Decomp aborts) */
 };
 
 /* fab element types */

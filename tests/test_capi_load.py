@@ -62,6 +62,9 @@ def test_strerror_is_callable_without_gpu():
     (dict(advection_type=3), "FHD_ERR_UNSUPPORTED"),
     (dict(precision=7), "FHD_ERR_BAD_ARG"),
     (dict(visc_type=3, zeta_ratio=-1.0), "FHD_ERR_BAD_ARG"),
+    (dict(transport_type=4), "FHD_ERR_UNSUPPORTED"),
+    (dict(transport_type=0), "FHD_ERR_UNSUPPORTED"),
+    (dict(transport_type=2, precision=1), "FHD_ERR_UNSUPPORTED"),
 ])
 def test_create_rejects_out_of_scope_parameters_without_gpu(change, code):
     """fhd_create validates the run before touching a device: out-of-scope options
