@@ -411,8 +411,14 @@ int fhd_create(fhd_ctx** out, const fhd_params* params, int device) {
     *out = nullptr;
     const fhd_params& p = *params;
     if (p.nspecies < 1 || p.nspecies > 4) return FHD_ERR_UNSUPPORTED;
-    for (int d = 0; d < 3; ++d)
-        if (p.n_cells[d] < 2 || !(p.prob_hi[d] > p.prob_lo[d])) return FHD_ERR_BAD_ARG;
+    // one cell is a direction of a quasi-2-D (z) or quasi-1-D (y, z) run, as the reference's
+    // driver requires those runs for such boxes (main_driver.cpp:125-140); it stays periodic
+    for (int d = 0; d < 3; ++d) {
+        const bool thin_ok = (d == 2 && p.do_2D == 1) || (d >= 1 && p.do_1D == 1);
+        if (p.n_cells[d] < 1 || (p.n_cells[d] < 2 && !thin_ok) || !(p.prob_hi[d] > p.prob_lo[d]))
+            return FHD_ERR_BAD_ARG;
+        if (p.n_cells[d] == 1 && p.walls && (p.bc_vel_lo[d] != -1 || p.bc_vel_hi[d] != -1)) return FHD_ERR_BAD_ARG;
+    }
     if ((int64_t)p.n_cells[0] * p.n_cells[1] * p.n_cells[2] >= ((int64_t)1 << 32)) return FHD_ERR_UNSUPPORTED;
     // algorithm_type 2 is the multispecies path every staggered deck runs; transport models
     // 1 Giovangigli, 2 Valk/Waldmann, 3 HCB (binary mixtures only)

@@ -39,6 +39,22 @@ def test_create_refuses_without_gpu(change, code):
     assert _create_rc(mixture4((6, 5, 4), dx=8e-6).replace(**change)) == getattr(capi, code)
 
 
+@pytest.mark.parametrize("n,mode,ok", [((8, 6, 1), "do_2D", True), ((8, 1, 1), "do_1D", True),
+                                       ((8, 6, 1), "do_1D", True), ((8, 6, 1), None, False),
+                                       ((8, 1, 6), "do_2D", False), ((1, 6, 6), "do_1D", False)])
+def test_one_cell_directions_only_in_their_modes(n, mode, ok):
+    """A one-cell direction is z of a quasi-2-D run or y / z of a quasi-1-D run, as the
+    reference's driver has it (main_driver.cpp:125-140); elsewhere it is refused."""
+    p = argon(n, dx=8e-6)
+    if mode:
+        p = p.replace(**{mode: 1})
+    rc = _create_rc(p)
+    if ok:
+        assert rc not in (capi.FHD_ERR_BAD_ARG, capi.FHD_ERR_UNSUPPORTED)
+    else:
+        assert rc == capi.FHD_ERR_BAD_ARG
+
+
 def test_create_refuses_the_particle_reservoir_in_1d():
     p = with_walls(argon((8, 4, 4), dx=8e-6), x=dict(vel=2, therm=2, mass=4, t=(300.0, 300.0),
                                                    Yk=((0.5, 0.5), (0.5, 0.5)))).replace(do_1D=1)
