@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "fhd_launch.cuh"
+#include "fhd_linesum.cuh"
 #include "fhd_vismf.h"
 
 namespace fhd {
@@ -42,32 +43,10 @@ struct PlotArgs {
     int ncomp;
 };
 
-// plane averages of Y_k for plot_deltaY_dir: thread (r, n) sums the cells with
-// coordinate r along `dir` in the order k, j, i, then divides by the plane's cell count
-struct HAvgArgs {
-    Arr4<const double> y;  // prim, pre-offset to Y_0
-    double* avg;           // [r * ns + n]
-    int n[3], dir, ns;
-};
-static __global__ void __launch_bounds__(128) k_plot_havg(HAvgArgs a) {
-    const int npts = a.n[a.dir];
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= npts * a.ns) return;
-    const int r = t / a.ns, c = t % a.ns;
-    double s = 0.0;
-    if (a.dir == 2) {
-        for (int j = 0; j < a.n[1]; ++j)
-            for (int i = 0; i < a.n[0]; ++i) s += a.y(i, j, r, c);
-    } else if (a.dir == 1) {
-        for (int k = 0; k < a.n[2]; ++k)
-            for (int i = 0; i < a.n[0]; ++i) s += a.y(i, r, k, c);
-    } else {
-        for (int k = 0; k < a.n[2]; ++k)
-            for (int j = 0; j < a.n[1]; ++j) s += a.y(r, j, k, c);
-    }
-    const int navg = a.dir == 0 ? a.n[1] * a.n[2] : (a.dir == 1 ? a.n[0] * a.n[2] : a.n[0] * a.n[1]);
-    a.avg[r * a.ns + c] = s / navg;
-}
+// plane averages of Y_k for plot_deltaY_dir (WriteHorizontalAverageToMF,
+// ComputeAverages.cpp:96-190): k_sum_to_line (fhd_linesum.cuh), entry r of species n
+// the cells with coordinate r along dir summed in the order k, j, i and divided by
+// the plane's cell count, into avg[r * ns + n]
 
 // out component c0 + n = (-average) + Y_n, block (z-plane, species) as the pack
 struct DeltaYArgs {
@@ -224,15 +203,16 @@ int plot_pack(const fhd_params& prm, int flags, fhd_fab out, const fhd_fab& cu, 
         cudaGetLastError();
         return FHD_ERR_OOM;
     }
-    HAvgArgs h;
-    h.y = view<const double>(prim, 6);
-    h.avg = avg;
-    for (int d = 0; d < 3; ++d) h.n[d] = prm.n_cells[d];
-    h.dir = dir;
-    h.ns = ns;
-    k_plot_havg<<<(npts * ns + 127) / 128, 128, 0, s>>>(h);
+    LineArgs la;
+    for (int c = 0; c < ns; ++c) la.job[c] = line_job_dir(prim, 6 + c, dir, avg + c, ns);
+    la.njobs = ns;
+    rc = launch_line_sums(la, prm.n_cells, dir, s);
+    if (rc) {
+        cudaFreeAsync(avg, s);
+        return rc;
+    }
     DeltaYArgs dy;
-    dy.y = h.y;
+    dy.y = view<const double>(prim, 6);
     dy.out = a.out;
     dy.avg = avg;
     for (int d = 0; d < 3; ++d) dy.n[d] = prm.n_cells[d];

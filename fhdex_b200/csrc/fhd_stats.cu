@@ -19,6 +19,7 @@
 //                    cross-correlations (statsStag.cpp:46-76)
 // Every pass reads and writes each operand once per point: it is bound by HBM.
 #include "fhd_launch.cuh"
+#include "fhd_linesum.cuh"
 
 namespace fhd {
 
@@ -374,98 +375,10 @@ static int stats_launch(const StatsArgs& a, bool means, bool vars, const fhd_fab
 // evaluateStatsStag3D's x-line averages (statsStag.cpp:46-74) and
 // EvaluateSpatialCorrelations3D (:868-1105), after the means and variances.
 //
-// k_sum_to_line: the four sumToLine results (cu and cuMeans components 0..nvars-1,
-// prim and primMeans components 1..nspecies+4), each entry (i, n) divided by
-// n_cells[1]*n_cells[2].  An entry is its y-z plane summed from 0.0 with k outer and
-// j inner, the order of a serial one-box sumToLine, so the sum is one dependent
-// chain: one thread owns one entry and adds in that order.  A one-warp block takes
-// 32 consecutive i of one component, so every row it reads is one coalesced
-// 256-byte segment.  The chains are few (one per line entry), so the rows reach
-// shared memory through asynchronous 8-byte copies (cp.async) issued
-// kLineStages - 1 batches of kLineRows rows ahead of the additions, and each
-// thread only ever reads the shared-memory column its own copies wrote, so
-// cp.async.wait_group alone orders it (no block barrier).  With few chains each
-// warp runs alone on its SM sub-partition, so the per-row instruction count sets
-// the pace: a batch inside one k-plane takes its 32 row addresses as independent
-// base + u*sy products rather than a running offset.
-constexpr int kMaxLineJobs = 2 * (5 + MAXS) + 2 * (MAXS + 4);
-constexpr int kLineRows = 32, kLineStages = 12;   // 96 KiB of dynamic shared memory per one-warp block
-constexpr int kLineSmem = kLineStages * kLineRows * 32 * (int)sizeof(double);
-struct LineJob {
-    const double* src;   // component n of the source at valid cell (0, 0, 0)
-    double* dst;         // line entry (0, n)
-    int64_t sy, sz;      // source strides of j and k (doubles)
-    int dstride;         // line entries per i (the source's component count)
-};
-struct LineArgs {
-    LineJob job[kMaxLineJobs];
-    int njobs, xblocks, nx, ny, nz;   // xblocks: one-warp blocks per job, ceil(nx / 32)
-};
-
-FHD_D void cp_async8(double* dst, const double* src) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
-}
-FHD_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-FHD_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
-static __global__ void __launch_bounds__(32) k_sum_to_line(const __grid_constant__ LineArgs a) {
-    extern __shared__ __align__(16) double line_smem[];
-    double(*buf)[kLineRows][32] = reinterpret_cast<double(*)[kLineRows][32]>(line_smem);
-    const int lane = threadIdx.x;
-    const int c = blockIdx.x / a.xblocks;
-    const int i = (blockIdx.x - c * a.xblocks) * 32 + lane;
-    if (c >= a.njobs) return;   // uniform over the block
-    const bool on = i < a.nx;
-    const LineJob& J = a.job[c];
-    const double* p = J.src + (on ? i : 0);
-    const int64_t rows = (int64_t)a.ny * a.nz, wrap = J.sz - (int64_t)a.ny * J.sy;
-    // the next row to copy: its index rq = k*ny + j, its j and offset k*sz + j*sy
-    int64_t rq = 0, offq = 0;
-    int jq = 0;
-    auto issue = [&](int stage) {   // one group: the next kLineRows rows (possibly none)
-        if (jq + kLineRows <= a.ny && rq + kLineRows <= rows) {
-            // the batch lies in one k-plane: independent row addresses
-            const double* q = p + offq;
-            if (on) {
-#pragma unroll
-                for (int u = 0; u < kLineRows; ++u) cp_async8(&buf[stage][u][lane], q + (int64_t)u * J.sy);
-            }
-            rq += kLineRows;
-            offq += (int64_t)kLineRows * J.sy;
-            jq += kLineRows;
-            if (jq == a.ny) { jq = 0; offq += wrap; }
-        } else {
-            for (int u = 0; u < kLineRows; ++u) {
-                if (on && rq < rows) cp_async8(&buf[stage][u][lane], p + offq);
-                ++rq;
-                offq += J.sy;
-                if (++jq == a.ny) { jq = 0; offq += wrap; }
-            }
-        }
-        cp_async_commit();
-    };
-#pragma unroll 1
-    for (int st = 0; st < kLineStages - 1; ++st) issue(st);
-    double acc = 0.0;
-    const int64_t nbatch = (rows + kLineRows - 1) / kLineRows;
-#pragma unroll 1
-    for (int64_t b = 0; b < nbatch; ++b) {
-        issue((int)((b + kLineStages - 1) % kLineStages));   // the stage batch b-1 used
-        cp_async_wait<kLineStages - 1>();                    // batch b (group b) has landed
-        const int st = (int)(b % kLineStages);
-        const int64_t r0 = b * kLineRows;
-        if (r0 + kLineRows <= rows) {
-#pragma unroll
-            for (int u = 0; u < kLineRows; ++u) acc += buf[st][u][lane];
-        } else {
-            for (int u = 0; r0 + u < rows; ++u) acc += buf[st][u][lane];
-        }
-    }
-    cp_async_wait<0>();
-    if (on) J.dst[(int64_t)i * J.dstride] = acc / (double)rows;
-}
+// The four sumToLine results (cu and cuMeans components 0..nvars-1, prim and
+// primMeans components 1..nspecies+4) along x, each entry (i, n) its y-z plane summed
+// with k outer and j inner and divided by n_cells[1]*n_cells[2]: k_sum_to_line
+// (fhd_linesum.cuh).
 
 // k_spatial_cross: one thread per x cell i updates spatialCross(i, 0..ncross-1) in
 // the reference's statement order (a later entry reads the earlier entries' new
@@ -714,18 +627,6 @@ static __global__ void __launch_bounds__(128) k_cross_1d(Cross1DArgs a) {
     }
 }
 
-static LineJob line_job(const fhd_fab& f, int comp, double* dst, int dstride) {
-    const int64_t sx = f.hi[0] - f.lo[0] + 1, sy = sx * (f.hi[1] - f.lo[1] + 1);
-    const int64_t sc = sy * (f.hi[2] - f.lo[2] + 1);
-    LineJob J;
-    J.src = static_cast<const double*>(f.data) + comp * sc - f.lo[2] * sy - f.lo[1] * sx - f.lo[0];
-    J.dst = dst;
-    J.sy = sx;
-    J.sz = sy;
-    J.dstride = dstride;
-    return J;
-}
-
 template <int NS>
 static int cross_launch(const DevParams& P, const fhd_fab& cu, const fhd_fab& prim, const fhd_stats& st,
                         int cross_cell, double sm1, double sinv, double* lines, cudaStream_t s) {
@@ -735,19 +636,13 @@ static int cross_launch(const DevParams& P, const fhd_fab& cu, const fhd_fab& pr
     double* L[4] = {lines, lines + (int64_t)NV * nx, lines + (int64_t)2 * NV * nx,
                     lines + (int64_t)(2 * NV + NP) * nx};
     int q = 0;
-    for (int n = 0; n < NV; ++n) la.job[q++] = line_job(cu, n, L[0] + n, NV);
-    for (int n = 0; n < NV; ++n) la.job[q++] = line_job(st.cuMeans, n, L[1] + n, NV);
-    for (int n = 0; n < NP; ++n) la.job[q++] = line_job(prim, 1 + n, L[2] + n, NP);
-    for (int n = 0; n < NP; ++n) la.job[q++] = line_job(st.primMeans, 1 + n, L[3] + n, NP);
+    for (int n = 0; n < NV; ++n) la.job[q++] = line_job_dir(cu, n, 0, L[0] + n, NV);
+    for (int n = 0; n < NV; ++n) la.job[q++] = line_job_dir(st.cuMeans, n, 0, L[1] + n, NV);
+    for (int n = 0; n < NP; ++n) la.job[q++] = line_job_dir(prim, 1 + n, 0, L[2] + n, NP);
+    for (int n = 0; n < NP; ++n) la.job[q++] = line_job_dir(st.primMeans, 1 + n, 0, L[3] + n, NP);
     la.njobs = q;
-    la.xblocks = (nx + 31) / 32;
-    la.nx = nx;
-    la.ny = P.n[1];
-    la.nz = P.n[2];
-    // on every call: the attribute belongs to the current device's copy of the kernel
-    const cudaError_t e = cudaFuncSetAttribute(k_sum_to_line, cudaFuncAttributeMaxDynamicSharedMemorySize, kLineSmem);
-    if (e != cudaSuccess) return cuda_rc(e);
-    k_sum_to_line<<<(unsigned)(la.xblocks * q), 32, kLineSmem, s>>>(la);
+    const int rc = launch_line_sums(la, P.n, 0, s);
+    if (rc) return rc;
     CrossArgs ca;
     ca.cu = L[0];
     ca.cum = L[1];
