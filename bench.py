@@ -87,7 +87,15 @@ def make_params(args):
         p = mixture4(args.n, dx=args.dx, precision=prec, seed=args.seed)
     else:
         raise SystemExit("--ns must be 1 (single gas), 2 (argon parity form) or 4 (mixture)")
-    return with_bench_walls(p, getattr(args, "walls", "none"))
+    p = with_bench_walls(p, getattr(args, "walls", "none"))
+    # quasi-1-D / 2-D runs and the other transport models take the reference-ordered pipeline
+    mode = getattr(args, "lowdim", "none")
+    if mode != "none":
+        p = p.replace(do_1D=int(mode == "1d"), do_2D=int(mode == "2d"))
+    model = getattr(args, "transport", "gio")
+    if model != "gio":
+        p = p.replace(transport_type={"vw": 2, "hcb": 3}[model])
+    return p
 
 
 def with_bench_walls(p, kind):
@@ -312,7 +320,10 @@ def config_dict(args, p, dt, tile):
     return {
         "workload": (("2 NO2 <-> N2O4 (chemistry source, CLE)" if p.nreaction > 0 else
                       {1: "argon (single gas)", 2: "argon (2 identical species)"}.get(p.nspecies, "4-species mixture"))
-                     + f" {p.n_cells[0]}^3, dx={p.dx[0]:g} cm, {'periodic' if getattr(args, 'walls', 'none') == 'none' else args.walls + ' walls'}, {args.precision}, in-kernel Philox noise"),
+                     + f" {p.n_cells[0]}^3, dx={p.dx[0]:g} cm, {'periodic' if getattr(args, 'walls', 'none') == 'none' else args.walls + ' walls'}, {args.precision}, in-kernel Philox noise"
+                     + ("" if getattr(args, "lowdim", "none") == "none" else f", quasi-{args.lowdim[0]}-D run")
+                     + ("" if getattr(args, "transport", "gio") == "gio" else
+                        {"vw": ", Valk/Waldmann transport", "hcb": ", HCB binary transport"}[args.transport])),
         "n_cells": list(p.n_cells), "nspecies": p.nspecies, "precision": args.precision, "dt_s": dt,
         "noise": "philox-4x32-10 in kernel", "tile": tile,
         "l2": "inputs larger than L2 (state ~%.1f GB)" % (state_gb(p)),
@@ -1037,6 +1048,10 @@ def main():
     ap.add_argument("--ns", type=int, default=2)
     ap.add_argument("--walls", default="none", choices=["none", "tempgrad", "reservoir"],
                     help="step mode: physical boundaries of the reference's regression runs (FP64)")
+    ap.add_argument("--lowdim", default="none", choices=["none", "1d", "2d"],
+                    help="quasi-1-D / 2-D run (do_1D / do_2D) on the same box")
+    ap.add_argument("--transport", default="gio", choices=["gio", "vw", "hcb"],
+                    help="transport model: Giovangigli (default), Valk/Waldmann, HCB binary")
     ap.add_argument("--gas", default="argon", choices=["argon", "no2"],
                     help="argon: --ns selects the species form; no2: 2 NO2 <-> N2O4 with the chemistry source")
     ap.add_argument("--dx", type=float, default=8e-6)
