@@ -23,6 +23,10 @@
 //   WriteCheckPoint,
 //   ReadCheckPoint             src_compressible_stag/compressible_functions_stag.H:188-243
 //   evaluateStatsStag3D        src_compressible_stag/compressible_functions_stag.H:257-273
+//   evaluateStatsStag2D,
+//   evaluateStatsStag1D        src_compressible_stag/compressible_functions_stag.H:275-305
+//   WriteSpatialCross3D,
+//   WriteSpatialCross1D        src_compressible_stag/compressible_functions_stag.H:41-43
 //
 // As in the reference, physics parameters are process globals in namespaces
 // `common`, `compressible` and `chemistry` (src_common/common_namespace.H,
@@ -88,9 +92,11 @@ namespace compressible {
 using fhd::amrex_compat::Real;
 inline int transport_type = 1;
 inline Real zeta_ratio = -1.0;
-// quasi-1-D / quasi-2-D runs (compressible_functions.cpp:58-63)
+// quasi-1-D / quasi-2-D runs (compressible_functions.cpp:58-66); all_correl: 1-D
+// correlations at five x* instead of one
 inline int do_1D = 0;
 inline int do_2D = 0;
+inline int all_correl = 0;
 }  // namespace compressible
 
 namespace common {
@@ -254,6 +260,7 @@ inline fhd_params params_from_globals() {
     p.cross_cell = common::cross_cell;
     p.do_1D = compressible::do_1D;
     p.do_2D = compressible::do_2D;
+    p.all_correl = compressible::all_correl;
     return p;
 }
 
@@ -699,11 +706,102 @@ inline void WriteSpatialCross3D(const fhd::amrex_compat::Vector<fhd::amrex_compa
     check(fhd_write_spatial_cross(&p, "", step, spatialCross.data()), "WriteSpatialCross3D");
 }
 
+// evaluateStatsStag1D / evaluateStatsStag2D (statsStag.cpp:78-197), for quasi-1-D /
+// 2-D runs (compressible::do_1D / do_2D): the per-cell statistics as evaluateStatsStag3D,
+// and in 1-D with plot_cross the per-pencil spatial correlations into spatialCross1D (a
+// cell-centred MultiFab without ghosts in the device arena, ncross components, or
+// 5*ncross with compressible::all_correl, as main_driver.cpp:717-727 defines it).
+inline void evaluateStatsStagLowDim(fhd::amrex_compat::MultiFab& cons, fhd::amrex_compat::MultiFab& consMean,
+                                    fhd::amrex_compat::MultiFab& consVar, fhd::amrex_compat::MultiFab& prim_in,
+                                    fhd::amrex_compat::MultiFab& primMean, fhd::amrex_compat::MultiFab& primVar,
+                                    const std::array<fhd::amrex_compat::MultiFab, 3>& vel,
+                                    std::array<fhd::amrex_compat::MultiFab, 3>& velMean,
+                                    std::array<fhd::amrex_compat::MultiFab, 3>& velVar,
+                                    const std::array<fhd::amrex_compat::MultiFab, 3>& cumom,
+                                    std::array<fhd::amrex_compat::MultiFab, 3>& cumomMean,
+                                    std::array<fhd::amrex_compat::MultiFab, 3>& cumomVar,
+                                    fhd::amrex_compat::MultiFab& coVar, fhd::amrex_compat::MultiFab& mom3,
+                                    fhd::amrex_compat::MultiFab& mom4, fhd::amrex_compat::MultiFab& spatialCross,
+                                    const int ncross, const int steps, const char* where) {
+    using namespace fhd::ref;
+    const bool cross = common::plot_cross && compressible::do_1D;
+    const int flags = (common::plot_means ? FHD_STATS_MEANS : 0) |
+                      ((common::plot_vars || common::plot_covars) ? FHD_STATS_VARS : 0) |
+                      (common::plot_mom3 ? FHD_STATS_MOM3 : 0) | (common::plot_mom4 ? FHD_STATS_MOM4 : 0) |
+                      (cross ? FHD_STATS_CROSS : 0);
+    if (!flags) return;
+    fhd_stats st;
+    std::memset(&st, 0, sizeof(st));
+    st.cuMeans = consMean.fab();
+    st.cuVars = consVar.fab();
+    st.primMeans = primMean.fab();
+    st.primVars = primVar.fab();
+    st.coVars = coVar.fab();
+    st.mom3 = mom3.fab();
+    st.mom4 = mom4.fab();
+    for (int d = 0; d < 3; ++d) {
+        st.velMeans[d] = velMean[d].fab();
+        st.velVars[d] = velVar[d].fab();
+        st.cumomMeans[d] = cumomMean[d].fab();
+        st.cumomVars[d] = cumomVar[d].fab();
+    }
+    if (cross) {
+        const int want = (compressible::all_correl == 1 ? 5 : 1) * ncross;
+        if (ncross != fhd_spatial_cross_ncross(common::nspecies) || spatialCross.nComp() != want ||
+            spatialCross.nGrow() != 0)
+            fail(where, FHD_ERR_BAD_ARG);
+        require_device(spatialCross, where);
+        st.spatialCross = spatialCross.dataPtr();
+    }
+    fhd_fab vl[3], mom[3];
+    fabs_of(vel, vl);
+    fabs_of(cumom, mom);
+    check(fhd_stats_stag(context(), cons.fab(), prim_in.fab(), vl, mom, &st, steps, flags), where);
+}
+
+#define FHD_REF_STATS_LOWDIM_ARGS                                                                                \
+    fhd::amrex_compat::MultiFab &cons, fhd::amrex_compat::MultiFab &consMean, fhd::amrex_compat::MultiFab &consVar, \
+        fhd::amrex_compat::MultiFab &prim_in, fhd::amrex_compat::MultiFab &primMean,                              \
+        fhd::amrex_compat::MultiFab &primVar, const std::array<fhd::amrex_compat::MultiFab, 3> &vel,              \
+        std::array<fhd::amrex_compat::MultiFab, 3> &velMean, std::array<fhd::amrex_compat::MultiFab, 3> &velVar,  \
+        const std::array<fhd::amrex_compat::MultiFab, 3> &cumom,                                                  \
+        std::array<fhd::amrex_compat::MultiFab, 3> &cumomMean, std::array<fhd::amrex_compat::MultiFab, 3> &cumomVar, \
+        fhd::amrex_compat::MultiFab &coVar, fhd::amrex_compat::MultiFab &mom3, fhd::amrex_compat::MultiFab &mom4,  \
+        fhd::amrex_compat::MultiFab & /*theta*/, fhd::amrex_compat::MultiFab & /*thetaMean*/,                     \
+        fhd::amrex_compat::MultiFab & /*thetaVar*/, fhd::amrex_compat::MultiFab & /*thetacoVar*/,                  \
+        fhd::amrex_compat::MultiFab &spatialCross, const int ncross, const int steps,                             \
+        const fhd::amrex_compat::Geometry & /*geom*/
+
+inline void evaluateStatsStag1D(FHD_REF_STATS_LOWDIM_ARGS) {
+    evaluateStatsStagLowDim(cons, consMean, consVar, prim_in, primMean, primVar, vel, velMean, velVar, cumom,
+                            cumomMean, cumomVar, coVar, mom3, mom4, spatialCross, ncross, steps, "evaluateStatsStag1D");
+}
+inline void evaluateStatsStag2D(FHD_REF_STATS_LOWDIM_ARGS) {
+    evaluateStatsStagLowDim(cons, consMean, consVar, prim_in, primMean, primVar, vel, velMean, velVar, cumom,
+                            cumomMean, cumomVar, coVar, mom3, mom4, spatialCross, ncross, steps, "evaluateStatsStag2D");
+}
+#undef FHD_REF_STATS_LOWDIM_ARGS
+
+// WriteSpatialCross1D (writePlotFileStag.cpp:551-563): spatialCross1D_<step, 9 digits>
+// (five <s>_spatialCross1D_<step> files with compressible::all_correl) in the working
+// directory, from the device MultiFab evaluateStatsStag1D updates.
+inline void WriteSpatialCross1D(const fhd::amrex_compat::MultiFab& spatialCross, int step,
+                                const fhd::amrex_compat::Geometry& /*geom*/, const int ncross) {
+    using namespace fhd::ref;
+    const fhd_params p = params_from_globals();
+    const int want = (p.all_correl == 1 ? 5 : 1) * ncross;
+    if (!p.do_1D || ncross != fhd_spatial_cross_ncross(p.nspecies) || spatialCross.nComp() != want ||
+        spatialCross.nGrow() != 0)
+        fail("WriteSpatialCross1D", FHD_ERR_BAD_ARG);
+    check(fhd_write_spatial_cross(&p, "", step, spatialCross.dataPtr()), "WriteSpatialCross1D");
+}
+
 // WriteCheckPoint (Checkpoint.cpp:28-257): chk<step, 9 digits>/ in the working
 // directory with the state, every defined statistics MultiFab and, with
-// plot_cross, spatialCrossVec in the Header.  The surface-coverage, 1-D / 2-D
-// cross-correlation and turbulence-forcing records are not written (none of
-// them exists on this path); the noise needs no generator state.
+// plot_cross, spatialCrossVec in the Header; a quasi-1-D / 2-D run also writes
+// spatialCrossMF (Level_0/spatialCrossMF, whether or not plot_cross is set, as
+// Checkpoint.cpp:251-256 does).  The surface-coverage and turbulence-forcing records
+// are not written (neither exists on this path); the noise needs no generator state.
 inline void WriteCheckPoint(int step, const fhd::amrex_compat::Real time, int statsCount,
                             const fhd::amrex_compat::Geometry& /*geom*/, const fhd::amrex_compat::MultiFab& cu,
                             const fhd::amrex_compat::MultiFab& cuMeans, const fhd::amrex_compat::MultiFab& cuVars,
@@ -720,7 +818,7 @@ inline void WriteCheckPoint(int step, const fhd::amrex_compat::Real time, int st
                             const fhd::amrex_compat::MultiFab& /*surfcovMeans*/,
                             const fhd::amrex_compat::MultiFab& /*surfcovVars*/,
                             const fhd::amrex_compat::MultiFab& /*surfcovcoVars*/,
-                            const fhd::amrex_compat::MultiFab& /*spatialCrossMF*/,
+                            const fhd::amrex_compat::MultiFab& spatialCrossMF,
                             const fhd::amrex_compat::Vector<fhd::amrex_compat::Real>& spatialCrossVec,
                             int ncross, TurbForcingComp& /*turbforce*/) {
     using namespace fhd::ref;
@@ -743,7 +841,12 @@ inline void WriteCheckPoint(int step, const fhd::amrex_compat::Real time, int st
     fabs_of(cumom, mom);
     fabs_of(vel, vl);
     const fhd_params p = params_from_globals();
-    if (common::plot_cross) {
+    if (p.do_1D || p.do_2D) {
+        if (ncross != fhd_spatial_cross_ncross(p.nspecies) ||
+            spatialCrossMF.nComp() != (p.do_1D && p.all_correl == 1 ? 5 : 1) * ncross || spatialCrossMF.nGrow() != 0)
+            fail("WriteCheckPoint", FHD_ERR_BAD_ARG);
+        st.spatialCross = spatialCrossMF.dataPtr();
+    } else if (common::plot_cross) {
         if (ncross != fhd_spatial_cross_ncross(p.nspecies) || spatialCrossVec.size() < (size_t)p.n_cells[0] * ncross)
             fail("WriteCheckPoint", FHD_ERR_BAD_ARG);
         st.spatialCross = const_cast<double*>(spatialCrossVec.data());
@@ -757,9 +860,11 @@ inline void WriteCheckPoint(int step, const fhd::amrex_compat::Real time, int st
 // the cell-centred means/variances, none for the others; mom3 / mom4 only with
 // plot_mom3 / plot_mom4), reads chk<common::restart, 9 digits>/ into them and sets
 // step to the saved step + 1, time and statsCount.  With plot_cross the Header's
-// spatialCrossVec is read into spatialCrossVec (n_cells[0] * ncross entries); with
-// reset_stats the statistics and spatialCrossVec are zeroed instead of read
-// (Checkpoint.cpp:343-358, 498-519).
+// spatialCrossVec is read into spatialCrossVec (n_cells[0] * ncross entries); a
+// quasi-1-D / 2-D run defines spatialCrossMF (ncross components, 5 * ncross with
+// do_1D and all_correl; no ghosts) and reads it (Checkpoint.cpp:529-533).  With
+// reset_stats the statistics, spatialCrossVec and spatialCrossMF are zeroed instead
+// of read (Checkpoint.cpp:343-358, 498-519).
 inline void ReadCheckPoint(int& step, fhd::amrex_compat::Real& time, int& statsCount,
                            fhd::amrex_compat::Geometry& /*geom*/, const fhd::amrex_compat::Box& domain,
                            fhd::amrex_compat::MultiFab& cu, fhd::amrex_compat::MultiFab& cuMeans,
@@ -775,7 +880,7 @@ inline void ReadCheckPoint(int& step, fhd::amrex_compat::Real& time, int& statsC
                            fhd::amrex_compat::MultiFab& mom4, fhd::amrex_compat::MultiFab& /*surfcov*/,
                            fhd::amrex_compat::MultiFab& /*surfcovMeans*/, fhd::amrex_compat::MultiFab& /*surfcovVars*/,
                            fhd::amrex_compat::MultiFab& /*surfcovcoVars*/,
-                           fhd::amrex_compat::MultiFab& /*spatialCrossMF*/,
+                           fhd::amrex_compat::MultiFab& spatialCrossMF,
                            fhd::amrex_compat::Vector<fhd::amrex_compat::Real>& spatialCrossVec, int ncross,
                            TurbForcingComp& /*turbforce*/, fhd::amrex_compat::BoxArray& ba,
                            fhd::amrex_compat::DistributionMapping& /*dmap*/) {
@@ -822,7 +927,12 @@ inline void ReadCheckPoint(int& step, fhd::amrex_compat::Real& time, int& statsC
     fabs_of(vel, vl);
     const fhd_params p = params_from_globals();
     const bool reset = common::reset_stats == 1;
-    if (common::plot_cross) {
+    if (p.do_1D || p.do_2D) {
+        if (ncross != fhd_spatial_cross_ncross(ns)) fail("ReadCheckPoint", FHD_ERR_BAD_ARG);
+        spatialCrossMF.define(domain, (p.do_1D && p.all_correl == 1 ? 5 : 1) * ncross, 0);
+        spatialCrossMF.setVal(0.0);
+        if (!reset) st.spatialCross = spatialCrossMF.dataPtr();
+    } else if (common::plot_cross) {
         if (ncross != fhd_spatial_cross_ncross(ns)) fail("ReadCheckPoint", FHD_ERR_BAD_ARG);
         spatialCrossVec.resize((size_t)common::n_cells[0] * ncross);
         if (!reset) st.spatialCross = spatialCrossVec.data();
@@ -843,7 +953,7 @@ inline void ReadCheckPoint(int& step, fhd::amrex_compat::Real& time, int& statsC
         }
         if (common::plot_mom3) mom3.setVal(0.0);
         if (common::plot_mom4) mom4.setVal(0.0);
-        if (common::plot_cross) spatialCrossVec.assign(spatialCrossVec.size(), 0.0);
+        if (common::plot_cross && !p.do_1D && !p.do_2D) spatialCrossVec.assign(spatialCrossVec.size(), 0.0);
     }
 }
 

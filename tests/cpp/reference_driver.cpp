@@ -23,6 +23,13 @@
 //       cuVars, primMeans, primVars, coVars, mom3, mom4, velMeans, velVars,
 //       cumomMeans, cumomVars, spatialCrossVec and dataSliceMeans_xcross, and
 //       WriteSpatialCross3D's spatialCross<nsteps> in the working directory
+//   reference_driver stats1d <nx> <ny> <nsteps> <seed> <dt> <all_correl> <out.bin>
+//       a quasi-1-D run (do_1D) on an nx x ny x ny box: nsteps RK3 steps,
+//       evaluateStatsStag1D after each (every statistic, plot_cross at cross_cell 3),
+//       WriteSpatialCross1D at step nsteps in the working directory, then
+//       WriteCheckPoint / ReadCheckPoint of chk<nsteps> (spatialCrossMF must come
+//       back bit for bit, else exit 6); writes cuMeans, cuVars, primMeans,
+//       primVars, coVars, mom3, mom4 and spatialCrossMF
 //   reference_driver massfrac <n>
 //       start from a state with a zero mass fraction: calculateTransportCoeffs
 //       must report it through the abort handler (exit code 3)
@@ -42,13 +49,13 @@ struct Caught : std::runtime_error {
 };
 [[noreturn]] static void throwing_handler(const char* msg) { throw Caught(msg); }
 
-static void set_argon(int n, int seed) {
+static void set_argon(int n, int seed, int ny = -1) {
     const double dx = 8e-6;
     common::nspecies = 2;
     for (int d = 0; d < 3; ++d) {
-        common::n_cells[d] = n;
+        common::n_cells[d] = d == 0 || ny < 0 ? n : ny;
         common::prob_lo[d] = 0.0;
-        common::prob_hi[d] = n * dx;
+        common::prob_hi[d] = common::n_cells[d] * dx;
     }
     for (int s = 0; s < 2; ++s) {
         common::molmass[s] = 39.95;
@@ -103,11 +110,12 @@ struct State {
     std::array<MultiFab, 3> cumom, vel, faceflux, cenflux;
     std::array<MultiFab, 2> edgeflux_x, edgeflux_y, edgeflux_z;
 
-    State(int n, Arena a, bool byproducts) {
+    // on the box common::n_cells
+    State(Arena a, bool byproducts) {
         ns = common::nspecies;
         nvars = 5 + ns;
         nprimvars = 6 + 2 * ns;
-        const Box dom(IntVect(0, 0, 0), IntVect(n - 1, n - 1, n - 1));
+        const Box dom(IntVect(0, 0, 0), IntVect(common::n_cells[0] - 1, common::n_cells[1] - 1, common::n_cells[2] - 1));
         RealBox rb;
         for (int d = 0; d < 3; ++d) {
             rb.lo[d] = common::prob_lo[d];
@@ -161,7 +169,7 @@ static void print_shape(const char* name, const MultiFab& m) {
 
 static int cmd_shapes(int n) {
     set_argon(n, 1);
-    State s(n, Arena::Host, true);
+    State s(Arena::Host, true);
     print_shape("cu", s.cu);
     print_shape("prim", s.prim);
     for (int d = 0; d < 3; ++d) print_shape(("cumom" + std::to_string(d)).c_str(), s.cumom[d]);
@@ -204,13 +212,13 @@ static int cmd_run(const std::string& arena, int n, int nsteps, int seed, double
     else
         set_argon(n, seed);
     // initialise on the device, as the reference's GPU build does
-    State dev(n, Arena::Device, true);
+    State dev(Arena::Device, true);
     dev.init();
     if (arena == "device") {
         step_all(dev, dt, nsteps);
     } else {
         // a CPU build's MultiFabs: state in pinned host memory, no by-products
-        State host(n, Arena::Pinned, false);
+        State host(Arena::Pinned, false);
         MultiFab::Copy(host.cu, dev.cu);
         MultiFab::Copy(host.prim, dev.prim);
         for (int d = 0; d < 3; ++d) {
@@ -238,7 +246,7 @@ static int cmd_run(const std::string& arena, int n, int nsteps, int seed, double
 
 static int cmd_plot(int n, int nsteps, int seed, double dt, const char* base) {
     set_argon(n, seed);
-    State s(n, Arena::Device, true);
+    State s(Arena::Device, true);
     s.init();
     step_all(s, dt, nsteps);
     MultiFab none;
@@ -252,7 +260,7 @@ static int cmd_plot(int n, int nsteps, int seed, double dt, const char* base) {
 
 static int cmd_chk(int n, int n1, int n2, int seed, double dt, const char* out) {
     set_argon(n, seed);
-    State s(n, Arena::Device, true);
+    State s(Arena::Device, true);
     s.init();
     step_all(s, dt, n1);
     const Box dom(IntVect(0, 0, 0), IntVect(n - 1, n - 1, n - 1));
@@ -271,7 +279,7 @@ static int cmd_chk(int n, int n1, int n2, int seed, double dt, const char* out) 
     WriteCheckPoint(n1 - 1, n1 * dt, 0, s.geom, s.cu, cuMeans, cuVars, s.prim, primMeans, primVars, s.cumom, cmm, cmv,
                     s.vel, vm, vv, coVars, none, none, none, none, none, none, none, cross, 0, turb);
     // restart into fresh MultiFabs
-    State r(n, Arena::Device, false);
+    State r(Arena::Device, false);
     MultiFab rcm, rcv, rpm, rpv, rco, rm3, rm4, sc0, sc1, sc2, sc3, scross;
     std::array<MultiFab, 3> rcmm, rcmv, rvm, rvv;
     BoxArray ba;
@@ -302,7 +310,7 @@ static int cmd_stats(int n, int nsteps, int seed, double dt, const char* out) {
     common::plot_means = common::plot_vars = common::plot_mom3 = common::plot_mom4 = 1;
     common::plot_cross = 1;
     common::cross_cell = n / 2;
-    State s(n, Arena::Device, true);
+    State s(Arena::Device, true);
     s.init();
     const Box dom(IntVect(0, 0, 0), IntVect(n - 1, n - 1, n - 1));
     const int nv = s.nvars, np = s.nprimvars;
@@ -341,12 +349,77 @@ static int cmd_stats(int n, int nsteps, int seed, double dt, const char* out) {
     return 0;
 }
 
+static bool same(const MultiFab& a, const MultiFab& b) {
+    std::vector<Real> ha, hb;
+    a.copyToHost(ha);
+    b.copyToHost(hb);
+    return ha.size() == hb.size() && std::memcmp(ha.data(), hb.data(), ha.size() * sizeof(Real)) == 0;
+}
+
+static int cmd_stats1d(int nx, int ny, int nsteps, int seed, double dt, int all_correl, const char* out) {
+    set_argon(nx, seed, ny);
+    compressible::do_1D = 1;
+    compressible::all_correl = all_correl;
+    common::plot_means = common::plot_vars = common::plot_mom3 = common::plot_mom4 = 1;
+    common::plot_cross = 1;
+    common::cross_cell = 3;
+    State s(Arena::Device, true);
+    s.init();
+    const Box dom(IntVect(0, 0, 0), IntVect(nx - 1, ny - 1, ny - 1));
+    const int nv = s.nvars, np = s.nprimvars;
+    MultiFab cuMeans(dom, nv, 2), cuVars(dom, nv, 2), primMeans(dom, np + 3, 2), primVars(dom, np + 5, 2),
+        coVars(dom, 26, 0), mom3(dom, nv + 1, 0), mom4(dom, nv + 1, 0), theta;
+    std::array<MultiFab, 3> vm, vv, cmm, cmv;
+    for (int d = 0; d < 3; ++d) {
+        vm[d].define(convert(dom, face_nodal(d)), 1, 0);
+        vv[d].define(convert(dom, face_nodal(d)), 1, 0);
+        cmm[d].define(convert(dom, face_nodal(d)), 1, 0);
+        cmv[d].define(convert(dom, face_nodal(d)), 1, 0);
+    }
+    // main_driver.cpp:283, 717-723
+    const int ncross = 37 + common::nspecies + 3;
+    MultiFab crossMF(dom, (all_correl ? 5 : 1) * ncross, 0);
+    crossMF.setVal(0.0);
+    TurbForcingComp turb;
+    for (int step = 0; step < nsteps; ++step) {
+        RK3stepStag(s.cu, s.cumom, s.prim, s.vel, s.source, s.eta, s.zeta, s.kappa, s.chi, s.D, s.faceflux,
+                    s.edgeflux_x, s.edgeflux_y, s.edgeflux_z, s.cenflux, s.ranchem, s.geom, dt, step, turb);
+        evaluateStatsStag1D(s.cu, cuMeans, cuVars, s.prim, primMeans, primVars, s.vel, vm, vv, s.cumom, cmm, cmv,
+                            coVars, mom3, mom4, theta, theta, theta, theta, crossMF, ncross, step + 1, s.geom);
+    }
+    WriteSpatialCross1D(crossMF, nsteps, s.geom, ncross);
+    Vector<Real> crossVec;
+    MultiFab none;
+    WriteCheckPoint(nsteps, nsteps * dt, nsteps, s.geom, s.cu, cuMeans, cuVars, s.prim, primMeans, primVars, s.cumom,
+                    cmm, cmv, s.vel, vm, vv, coVars, mom3, mom4, none, none, none, none, crossMF, crossVec, ncross,
+                    turb);
+    State r(Arena::Device, false);
+    MultiFab rcm, rcv, rpm, rpv, rco, rm3, rm4, sc0, rcross;
+    std::array<MultiFab, 3> rcmm, rcmv, rvm, rvv;
+    BoxArray ba;
+    DistributionMapping dm;
+    int rstep = -1, count = -1;
+    Real time = -1.0;
+    common::restart = nsteps;
+    ReadCheckPoint(rstep, time, count, r.geom, dom, r.cu, rcm, rcv, r.prim, rpm, rpv, r.cumom, rcmm, rcmv, r.vel, rvm,
+                   rvv, rco, rm3, rm4, sc0, sc0, sc0, sc0, rcross, crossVec, ncross, turb, ba, dm);
+    if (rstep != nsteps + 1 || count != nsteps || !same(rcross, crossMF) || !same(rcm, cuMeans) || !same(rm4, mom4))
+        return 6;
+    FILE* f = std::fopen(out, "wb");
+    if (!f) return 2;
+    for (const MultiFab* m : {&cuMeans, &cuVars, &primMeans, &primVars, &coVars, &mom3, &mom4, &crossMF})
+        write_all(f, *m);
+    std::fclose(f);
+    fhd::ref::finalize();
+    return 0;
+}
+
 static int cmd_massfrac(int n) {
     set_argon(n, 1);
     common::rhobar[0] = 1.0;  // species 2 absent: Y_2 = 0
     common::rhobar[1] = 0.0;
     fhd::ref::abort_handler = throwing_handler;
-    State s(n, Arena::Device, true);
+    State s(Arena::Device, true);
     try {
         s.init();
     } catch (const Caught& e) {
@@ -374,6 +447,9 @@ int main(int argc, char** argv) {
         if (cmd == "stats" && argc == 7)
             return cmd_stats(std::atoi(argv[2]), std::atoi(argv[3]), std::atoi(argv[4]), std::strtod(argv[5], nullptr),
                              argv[6]);
+        if (cmd == "stats1d" && argc == 9)
+            return cmd_stats1d(std::atoi(argv[2]), std::atoi(argv[3]), std::atoi(argv[4]), std::atoi(argv[5]),
+                               std::strtod(argv[6], nullptr), std::atoi(argv[7]), argv[8]);
         if (cmd == "chk" && argc == 8)
             return cmd_chk(std::atoi(argv[2]), std::atoi(argv[3]), std::atoi(argv[4]), std::atoi(argv[5]),
                            std::strtod(argv[6], nullptr), argv[7]);

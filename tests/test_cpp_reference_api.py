@@ -208,3 +208,51 @@ def test_reference_driver_statistics_equal_c_abi_statistics(driver, tmp_path):
     assert off == raw.size
     assert not bad, bad
     assert stats.cuVars.arr.abs().max().item() > 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("all_correl", [0, 1])
+def test_reference_driver_lowdim_statistics_equal_c_abi_statistics(driver, tmp_path, all_correl):
+    """A quasi-1-D run through the reference-named layer: evaluateStatsStag1D after
+    every step equals fhd_stats_stag bit for bit (per-pencil correlations in
+    spatialCrossMF, one x* or the five of all_correl), WriteSpatialCross1D's files
+    equal fhd_write_spatial_cross's, and WriteCheckPoint / ReadCheckPoint carry
+    spatialCrossMF through a restart (checked inside the driver)."""
+    from fhdex_b200 import capi
+    from fhdex_b200.context import Context
+    from fhdex_b200.stats import StatsState
+    nx, ny, nsteps, seed = 16, 4, 3, 17
+    p = argon((nx, ny, ny), dx=8e-6, seed=seed).replace(do_1D=1, cross_cell=3, all_correl=all_correl)
+    dt = stable_dt(p)
+    out = str(tmp_path / "stats1d.bin")
+    run_dir = tmp_path / "run"
+    run_dir.mkdir()
+    r = subprocess.run([driver, "stats1d", str(nx), str(ny), str(nsteps), str(seed), repr(dt), str(all_correl), out],
+                       capture_output=True, text=True, timeout=300, cwd=str(run_dir))
+    assert r.returncode == 0, (r.returncode, r.stderr)
+    ctx = Context(p)
+    st = StagState(p, "cuda")
+    ctx.init_state(st)
+    stats = StatsState(p, "cuda", cross=True)
+    for step in range(nsteps):
+        ctx.rk3_step(st, dt, step, aux=True)
+        ctx.stats_stag(st, stats, step + 1, 15 | capi.STATS_CROSS)
+    torch.cuda.synchronize()
+    stats.write_spatial_cross(nsteps, str(tmp_path) + "/")
+    names = [f"{s}_spatialCross1D_{nsteps:09d}" for s in range(5)] if all_correl else [f"spatialCross1D_{nsteps:09d}"]
+    for fname in names:
+        assert open(run_dir / fname).read() == open(tmp_path / fname).read(), fname
+    arrs = [m.arr for m in (stats.cuMeans, stats.cuVars, stats.primMeans, stats.primVars, stats.coVars,
+                            stats.mom3, stats.mom4)] + [stats.spatialCross]
+    raw = np.fromfile(out, dtype=np.float64)
+    off = 0
+    bad = []
+    for k, a in enumerate(arrs):
+        size = a.numel()
+        got = torch.from_numpy(raw[off:off + size].copy()).view(a.shape)
+        off += size
+        if not torch.equal(got, a.cpu()):
+            bad.append(k)
+    assert off == raw.size
+    assert not bad, bad
+    assert stats.spatialCross.abs().max().item() > 0
