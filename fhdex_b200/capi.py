@@ -21,6 +21,7 @@ FHD_ERR_CUDA = 6
 FHD_ERR_UNSUPPORTED = 7
 FHD_ERR_TOO_LARGE = 8
 FHD_ERR_SINGULAR = 9
+FHD_ERR_IO = 10
 
 FHD_F64 = 0
 FHD_F32 = 1

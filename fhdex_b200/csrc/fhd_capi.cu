@@ -321,6 +321,7 @@ const char* fhd_strerror(int code) {
         case FHD_ERR_UNSUPPORTED: return "option outside the implemented scope";
         case FHD_ERR_TOO_LARGE: return "box too large for the 16 MiB static scratch of fhd_rk3_step_stag_noalloc";
         case FHD_ERR_SINGULAR: return "singular Valk/Waldmann transport system (reference: amrex::Abort in Decomp)";
+        case FHD_ERR_IO: return "file I/O failed (directory, open, write, read or close)";
         default: return "unknown error";
     }
 }

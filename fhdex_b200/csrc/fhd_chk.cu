@@ -158,15 +158,15 @@ extern "C" int fhd_write_checkpoint(const fhd_params* params, const char* chk_ba
             return FHD_ERR_CUDA;
     }
     const std::string dir = chk_dir(chk_base, step);
-    if (!vismf_mkdir(dir) || !vismf_mkdir(dir + "/Level_0")) return FHD_ERR_BAD_ARG;
+    if (!vismf_mkdir(dir) || !vismf_mkdir(dir + "/Level_0")) return FHD_ERR_IO;
     FILE* h = std::fopen((dir + "/Header").c_str(), "w");
-    if (!h) return FHD_ERR_BAD_ARG;
+    if (!h) return FHD_ERR_IO;
     const int lo[3] = {0, 0, 0}, hi[3] = {params->n_cells[0] - 1, params->n_cells[1] - 1, params->n_cells[2] - 1},
               cc[3] = {0, 0, 0};
     std::fprintf(h, "Checkpoint file for FHDeX/compressStag\n%d\n%.17g\n%d\n(1 0\n%s\n)\n\n", step, time, stats_count,
                  vismf_box(lo, hi, cc).c_str());
     for (double v : sc) std::fprintf(h, "%.16g\n", v);
-    if (std::fclose(h) != 0) return FHD_ERR_BAD_ARG;
+    if (std::fclose(h) != 0) return FHD_ERR_IO;
     std::vector<double> buf;
     for (const Entry& e : E) {
         int vlo[3], vhi[3], type[3], ng;
@@ -174,12 +174,12 @@ extern "C" int fhd_write_checkpoint(const fhd_params* params, const char* chk_ba
         buf.resize((size_t)fab_elems(e.fab));
         if (!copy_bytes(buf.data(), e.fab.data, buf.size() * sizeof(double), on_device(e.fab.data)))
             return FHD_ERR_CUDA;
-        if (!vismf_write(dir + "/Level_0", e.name, buf.data(), vlo, vhi, type, e.fab.ncomp, ng)) return FHD_ERR_BAD_ARG;
+        if (!vismf_write(dir + "/Level_0", e.name, buf.data(), vlo, vhi, type, e.fab.ncomp, ng)) return FHD_ERR_IO;
     }
     if (!scmf.empty()) {
         const int vlo[3] = {0, 0, 0}, type[3] = {0, 0, 0};
         if (!vismf_write(dir + "/Level_0", "spatialCrossMF", scmf.data(), vlo, hi, type, crossmf_ncomp(*params), 0))
-            return FHD_ERR_BAD_ARG;
+            return FHD_ERR_IO;
     }
     return FHD_OK;
 }
@@ -192,7 +192,7 @@ extern "C" int fhd_read_checkpoint(const fhd_params* params, const char* chk_bas
         return FHD_ERR_BAD_ARG;
     const std::string dir = chk_dir(chk_base, restart);
     FILE* h = std::fopen((dir + "/Header").c_str(), "r");
-    if (!h) return FHD_ERR_BAD_ARG;
+    if (!h) return FHD_ERR_IO;
     char title[256];
     int s = 0, sc = 0;
     double t = 0;
@@ -219,7 +219,8 @@ extern "C" int fhd_read_checkpoint(const fhd_params* params, const char* chk_bas
             glo[d] = vlo[d] - ng;
             ghi[d] = vhi[d] + ng;
         }
-        if (!vismf_read(dir + "/Level_0", e.name, glo, ghi, type, e.fab.ncomp, buf)) return FHD_ERR_BAD_ARG;
+        const int vr = vismf_read(dir + "/Level_0", e.name, glo, ghi, type, e.fab.ncomp, buf);
+        if (vr != kVisOk) return vr == kVisShape ? FHD_ERR_BAD_ARG : FHD_ERR_IO;
         const bool dev = on_device(e.fab.data);
         if (dev && !synced) {
             if (cudaDeviceSynchronize() != cudaSuccess) {
@@ -234,8 +235,8 @@ extern "C" int fhd_read_checkpoint(const fhd_params* params, const char* chk_bas
     if (stats && stats->spatialCross && lowdim(*params)) {
         const int glo[3] = {0, 0, 0}, ghi[3] = {params->n_cells[0] - 1, params->n_cells[1] - 1, params->n_cells[2] - 1};
         const int type[3] = {0, 0, 0};
-        if (!vismf_read(dir + "/Level_0", "spatialCrossMF", glo, ghi, type, crossmf_ncomp(*params), cross))
-            return FHD_ERR_BAD_ARG;
+        const int vr = vismf_read(dir + "/Level_0", "spatialCrossMF", glo, ghi, type, crossmf_ncomp(*params), cross);
+        if (vr != kVisOk) return vr == kVisShape ? FHD_ERR_BAD_ARG : FHD_ERR_IO;
     }
     if (!cross.empty()) {
         const bool dev = on_device(stats->spatialCross);
@@ -280,12 +281,12 @@ static int write_cross_1d(const fhd_params& p, const char* dir, int step, const 
         const std::string prefix = std::string(dir) + (nstar == 5 ? std::to_string(s) + "_" : std::string()) +
                                    "spatialCross1D_";
         FILE* f = std::fopen(chk_dir(prefix.c_str(), step).c_str(), "w");
-        if (!f) return FHD_ERR_BAD_ARG;
+        if (!f) return FHD_ERR_IO;
         for (int r = 0; r < nx; ++r) {
             for (int n = 0; n < nc + 1; ++n) std::fprintf(f, "%g ", avg[(size_t)r * (nc + 1) + n]);
             std::fputc('\n', f);
         }
-        if (std::fclose(f) != 0) return FHD_ERR_BAD_ARG;
+        if (std::fclose(f) != 0) return FHD_ERR_IO;
     }
     return FHD_OK;
 }
@@ -309,7 +310,7 @@ extern "C" int fhd_write_spatial_cross(const fhd_params* params, const char* dir
     if (params->do_1D) return write_cross_1d(*params, dir, step, spatial_cross);
     if (!cross_to_host(*params, spatial_cross, sc)) return FHD_ERR_CUDA;
     FILE* f = std::fopen(chk_dir((std::string(dir) + "spatialCross").c_str(), step).c_str(), "w");
-    if (!f) return FHD_ERR_BAD_ARG;
+    if (!f) return FHD_ERR_IO;
     const int nc = ncross_of(*params);
     const double h = (params->prob_hi[0] - params->prob_lo[0]) / params->n_cells[0];
     for (int i = 0; i < params->n_cells[0]; ++i) {
@@ -317,5 +318,5 @@ extern "C" int fhd_write_spatial_cross(const fhd_params* params, const char* dir
         for (int n = 0; n < nc; ++n) std::fprintf(f, "%.16g ", sc[(size_t)i * nc + n]);
         std::fputc('\n', f);
     }
-    return std::fclose(f) == 0 ? FHD_OK : FHD_ERR_BAD_ARG;
+    return std::fclose(f) == 0 ? FHD_OK : FHD_ERR_IO;
 }

@@ -249,11 +249,11 @@ int plot_write(const fhd_params& prm, const char* dir, const double* host, const
     const int nc = (int)names.size();
     const int* n = prm.n_cells;
     const std::string root(dir);
-    if (!vismf_mkdir(root) || !vismf_mkdir(root + "/Level_0")) return FHD_ERR_BAD_ARG;
+    if (!vismf_mkdir(root) || !vismf_mkdir(root + "/Level_0")) return FHD_ERR_IO;
     double dx[3];
     for (int d = 0; d < 3; ++d) dx[d] = (prm.prob_hi[d] - prm.prob_lo[d]) / n[d];
     FILE* h = std::fopen((root + "/Header").c_str(), "w");
-    if (!h) return FHD_ERR_BAD_ARG;
+    if (!h) return FHD_ERR_IO;
     std::fprintf(h, "HyperCLaw-V1.1\n%d\n", nc);
     for (const std::string& s : names) std::fprintf(h, "%s\n", s.c_str());
     std::fprintf(h, "3\n%.17g\n0\n", time);
@@ -269,7 +269,7 @@ int plot_write(const fhd_params& prm, const char* dir, const double* host, const
     // Level_0/Cell_H and Cell_D_00000: the one-box MultiFab, no ghosts
     const int lo[3] = {0, 0, 0}, hi[3] = {n[0] - 1, n[1] - 1, n[2] - 1}, type[3] = {0, 0, 0};
     const bool cok = vismf_write(root + "/Level_0", "Cell", host, lo, hi, type, nc, 0);
-    return (hok && cok) ? FHD_OK : FHD_ERR_BAD_ARG;
+    return (hok && cok) ? FHD_OK : FHD_ERR_IO;
 }
 
 }  // namespace fhd

@@ -71,29 +71,31 @@ inline bool vismf_write(const std::string& dir, const std::string& name, const d
 }
 
 // Reads <dir>/<name>_D_00000 into `out` after checking that it holds exactly the
-// box glo..ghi of index type `type` with `ncomp` components.
-inline bool vismf_read(const std::string& dir, const std::string& name, const int glo[3], const int ghi[3],
-                       const int type[3], int ncomp, std::vector<double>& out) {
+// box glo..ghi of index type `type` with `ncomp` components: kVisOk, kVisIo (the
+// file is missing, unreadable or short) or kVisShape (it holds another box).
+enum { kVisOk = 0, kVisIo = 1, kVisShape = 2 };
+inline int vismf_read(const std::string& dir, const std::string& name, const int glo[3], const int ghi[3],
+                      const int type[3], int ncomp, std::vector<double>& out) {
     FILE* f = std::fopen((dir + "/" + name + "_D_00000").c_str(), "rb");
-    if (!f) return false;
+    if (!f) return kVisIo;
     char line[512];
     if (!std::fgets(line, sizeof(line), f)) {
         std::fclose(f);
-        return false;
+        return kVisIo;
     }
     char want[512];
     std::snprintf(want, sizeof(want), "FAB %s%s %d\n", vismf_real_descriptor(), vismf_box(glo, ghi, type).c_str(),
                   ncomp);
     if (std::strcmp(line, want) != 0) {
         std::fclose(f);
-        return false;
+        return kVisShape;
     }
     int64_t pts = 1;
     for (int d = 0; d < 3; ++d) pts *= (int64_t)(ghi[d] - glo[d] + 1);
     out.resize((size_t)pts * ncomp);
     const bool ok = std::fread(out.data(), sizeof(double), out.size(), f) == out.size();
     std::fclose(f);
-    return ok;
+    return ok ? kVisOk : kVisIo;
 }
 
 }  // namespace fhd

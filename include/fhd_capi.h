@@ -49,7 +49,8 @@ enum {
     FHD_ERR_CUDA = 6,        /* a CUDA runtime call failed                        */
     FHD_ERR_UNSUPPORTED = 7, /* option outside the implemented scope              */
     FHD_ERR_TOO_LARGE = 8,   /* box does not fit fhd_rk3_step_stag_noalloc's scratch */
-    FHD_ERR_SINGULAR = 9     /* a singular Valk/Waldmann system (the reference's Decomp aborts) */
+    FHD_ERR_SINGULAR = 9,    /* a singular Valk/Waldmann system (the reference's Decomp aborts) */
+    FHD_ERR_IO = 10          /* a file could not be created, written, read or closed   */
 };
 
 /* fab element types */
@@ -491,7 +492,10 @@ int fhd_plotfile_pack(fhd_ctx* ctx, int flags, fhd_fab out, fhd_fab cu, const fh
  * the Header after the BoxArray at 16 significant digits, as the reference keeps
  * spatialCrossVec there (Checkpoint.cpp:112-118), and read back from it
  * (:343-358).  For the reference's reset_stats, read with stats = NULL and zero
- * the statistics. */
+ * the statistics.  A directory or file that cannot be created, opened, written,
+ * read or closed gives FHD_ERR_IO; a checkpoint that holds other shapes or is not
+ * a compressible-staggered checkpoint gives FHD_ERR_BAD_ARG.  The file writers
+ * below (spatial cross, plotfiles) report file failures as FHD_ERR_IO as well. */
 int fhd_write_checkpoint(const fhd_params* params, const char* chk_base, int step, double time, int stats_count,
                          fhd_fab cu, const fhd_fab cumom[3], fhd_fab prim, const fhd_fab vel[3],
                          const fhd_stats* stats);

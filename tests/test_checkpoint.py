@@ -77,3 +77,29 @@ def test_checkpoint_keeps_spatial_cross_in_the_header(tmp_path):
     path = write_checkpoint(p, base, 4, 1e-10, st, StatsState(p), stats_count=3)
     lines = open(os.path.join(path, "Header")).read().split("\n")
     assert not [v for v in lines[lines.index(")") + 1:] if v]
+
+
+def test_file_failures_are_io_errors(tmp_path):
+    """A missing checkpoint or an output directory that cannot be created gives
+    FHD_ERR_IO, a checkpoint of other shapes FHD_ERR_BAD_ARG."""
+    from fhdex_b200 import capi
+    p = mixture4((5, 4, 6), dx=8e-6)
+    st, stats = randomized(p, 3)
+    base = str(tmp_path / "chk")
+    write_checkpoint(p, base, 2, 0.0, st)
+    with pytest.raises(FhdError) as e:
+        read_checkpoint(p, base, 3, StagState(p))
+    assert e.value.code == capi.FHD_ERR_IO
+    q = mixture4((5, 4, 7), dx=8e-6)
+    with pytest.raises(FhdError) as e:
+        read_checkpoint(q, base, 2, StagState(q))
+    assert e.value.code == capi.FHD_ERR_BAD_ARG
+    blocker = tmp_path / "file"
+    blocker.write_text("x")
+    with pytest.raises(FhdError) as e:
+        write_checkpoint(p, str(blocker / "chk"), 1, 0.0, st)
+    assert e.value.code == capi.FHD_ERR_IO
+    s = StatsState(p, cross=True)
+    with pytest.raises(FhdError) as e:
+        s.write_spatial_cross(1, str(blocker) + "/")
+    assert e.value.code == capi.FHD_ERR_IO
