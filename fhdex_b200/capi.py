@@ -195,6 +195,8 @@ def _declare(lib):
         "fhd_sf_nsamples": (C.c_int64, [vp]),
         "fhd_sf_fort_structure": (i, [vp, fab, i]),
         "fhd_sf_finalize": (i, [vp, fab, fab, fab, i]),
+        "fhd_sf_create_stack": (i, [P(vp), P(i), i, i, i, P(i), P(i), P(d), i]),
+        "fhd_sf_stack_average": (i, [vp, fab, fab, i]),
         "fhd_batch_create": (i, [P(vp), i, i, i]),
         "fhd_batch_destroy": (i, [vp]),
         "fhd_batch_set_stream": (i, [vp, vp]),

@@ -6,6 +6,11 @@ variables, accumulated on the device (cuFFT + one fused accumulation kernel).
     for step in ...:
         sf.fort_structure(variables)          # MultiFab with the variables as components
     real, imag, mag = sf.finalize(zero_avg=1)  # k = 0 at n_cells // 2
+
+A quasi-2-D run's per-z-slice or a quasi-1-D run's per-x-pencil structure factors
+(main_driver.cpp:923-993) are one stacked object: ``StructFact(p.n_cells, names,
+scaling, stack="z_slices" | "x_pencils")`` takes the whole box's variables, and
+``stack_average()`` gives the reference's averaged (mag, realimag) output.
 """
 from __future__ import annotations
 
@@ -28,10 +33,16 @@ def default_pairs(nvar: int):
     return a, b
 
 
+STACKS = {None: 0, "z_slices": 1, "x_pencils": 2}
+
+
 class StructFact:
-    def __init__(self, n_cells, var_names, var_scaling, pairs=None, device: int = 0):
+    def __init__(self, n_cells, var_names, var_scaling, pairs=None, device: int = 0, stack=None):
         self.lib = capi.load()
         self.n_cells = tuple(int(x) for x in n_cells)
+        self.stack = stack
+        nx, ny, nz = self.n_cells
+        self.member = {None: (nx, ny, nz), "z_slices": (nx, ny, 1), "x_pencils": (nx, 1, 1)}[stack]
         self.var_names = list(var_names)
         self.device = device
         nvar = len(self.var_names)
@@ -46,7 +57,8 @@ class StructFact:
         cb = (C.c_int * len(pb))(*pb)
         sc = (C.c_double * len(pa))(*var_scaling)
         self._h = C.c_void_p()
-        check(self.lib.fhd_sf_create(C.byref(self._h), n, nvar, len(pa), ca, cb, sc, device), "fhd_sf_create")
+        check(self.lib.fhd_sf_create_stack(C.byref(self._h), n, STACKS[stack], nvar, len(pa), ca, cb, sc, device),
+              "fhd_sf_create_stack")
 
     @property
     def ncov(self) -> int:
@@ -72,6 +84,16 @@ class StructFact:
         check(self.lib.fhd_sf_finalize(self._h, out[0].fab(), out[1].fab(), out[2].fab(), zero_avg),
               "fhd_sf_finalize")
         return tuple(out)
+
+    def stack_average(self, zero_avg: int = 1):
+        """(mag, realimag) MultiFabs of the member shape: AddToExternal of every
+        member in order, then times 1/members (main_driver.cpp:1592-1618, 1683-1711)."""
+        self._stream()
+        dev = f"cuda:{self.device}"
+        mag = MultiFab(self.member, CELL, self.ncov, 0, device=dev)
+        ri = MultiFab(self.member, CELL, 2 * self.ncov, 0, device=dev)
+        check(self.lib.fhd_sf_stack_average(self._h, mag.fab(), ri.fab(), zero_avg), "fhd_sf_stack_average")
+        return mag, ri
 
     def close(self):
         if self._h:

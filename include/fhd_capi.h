@@ -558,6 +558,24 @@ int fhd_sf_fort_structure(fhd_sf* sf, fhd_fab variables, int reset);
  * magnitude).  The accumulators are left unchanged. */
 int fhd_sf_finalize(fhd_sf* sf, fhd_fab cov_real, fhd_fab cov_imag, fhd_fab cov_mag, int zero_avg);
 
+/* Stacks of structure factors of the quasi-2-D and quasi-1-D runs
+ * (main_driver.cpp:923-993, 1503-1557, 1592-1711): one StructFact per z slice
+ * (FHD_SF_Z_SLICES, do_2D: members z = 0..n_cells[2]-1 of n_cells[0] x
+ * n_cells[1] x 1, ExtractSlice) or per x pencil (FHD_SF_X_PENCILS, do_1D: member
+ * i at y = i / n_cells[1], z = i % n_cells[1] of n_cells[0] x 1 x 1,
+ * ExtractXPencil; needs n_cells[1] == n_cells[2], since for other shapes that
+ * enumeration reads pencils outside the box).  All members transform in one
+ * batched cuFFT per variable.  fhd_sf_fort_structure takes the whole box's
+ * variables fab and samples every member; fhd_sf_stack_average is the
+ * reference's output loop: zeroed mag (ncov comps) and realimag (2 ncov comps:
+ * real then imaginary) fabs of the member shape, AddToExternal of every member
+ * in order (its Finalize, StructFact.cpp:979-1009), then mult by 1/members.
+ * fhd_sf_finalize is refused for a stack. */
+enum { FHD_SF_BOX = 0, FHD_SF_Z_SLICES = 1, FHD_SF_X_PENCILS = 2 };
+int fhd_sf_create_stack(fhd_sf** sf, const int n_cells[3], int kind, int nvar, int ncov, const int* pairA,
+                        const int* pairB, const double* var_scaling, int device);
+int fhd_sf_stack_average(fhd_sf* sf, fhd_fab mag, fhd_fab realimag, int zero_avg);
+
 /* RK3stepStag without any device allocation, for callers that cannot allocate:
  * code whose device memory is owned by an arena that a stray cudaMalloc would
  * fail or fragment, framework callbacks that forbid allocation on their hot

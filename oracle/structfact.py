@@ -86,3 +86,42 @@ class StructFactOracle:
         mag = 0.0 + out[0] * out[0]
         mag = mag + out[1] * out[1]
         return out[0], out[1], np.sqrt(mag)
+
+
+class StructFactStackOracle:
+    """The quasi-2-D runs' per-z-slice and the quasi-1-D runs' per-x-pencil
+    StructFact vectors (main_driver.cpp:923-993, 1503-1557) and their averaged
+    output (AddToExternal of every member, StructFact.cpp:979-1009, then the mult
+    by 1/members, main_driver.cpp:1592-1618, 1683-1711)."""
+
+    def __init__(self, shape_zyx, kind, nvar, var_scaling, pairs=None):
+        nz, ny, nx = shape_zyx
+        self.kind = kind
+        if kind == "z_slices":
+            # member z = i: ExtractSlice(mf, Flattened, 2, i, ...)
+            self.take = [(lambda v, z=z: v[:, z:z + 1, :, :]) for z in range(nz)]
+            mshape = (1, ny, nx)
+        else:
+            # member i: ExtractXPencil(mf, pencil, i / ny, i % ny, ...) (y, z)
+            assert ny == nz
+            self.take = [(lambda v, i=i: v[:, i % ny:i % ny + 1, i // ny:i // ny + 1, :]) for i in range(ny * nz)]
+            mshape = (1, 1, nx)
+        self.members = [StructFactOracle(mshape, nvar, var_scaling, pairs) for _ in self.take]
+
+    @property
+    def nsamples(self):
+        return self.members[0].nsamples
+
+    def fort_structure(self, variables, reset=0):
+        for m, take in zip(self.members, self.take):
+            m.fort_structure(take(variables), reset=reset)
+
+    def stack_average(self, zero_avg=1):
+        sm = sr = si = 0.0
+        for m in self.members:
+            re, im, mag = m.finalize(zero_avg)
+            sm = sm + mag
+            sr = sr + re
+            si = si + im
+        inv = 1.0 / len(self.members)
+        return sm * inv, np.concatenate([sr, si]) * inv

@@ -73,3 +73,43 @@ def test_density_structure_factor_of_the_step_is_flat():
     th = equilibrium_variances(p)["rho"]
     assert s.sum() / (s.size - 1) / th == pytest.approx(1.0, abs=0.03)
     sf.close()
+
+
+@pytest.mark.parametrize("stack,shape_xyz,ng,pairs", [("z_slices", (8, 6, 5), 0, None),
+                                                      ("z_slices", (7, 4, 3), 2, ([2, 0], [1, 1])),
+                                                      ("x_pencils", (16, 3, 3), 1, None),
+                                                      ("x_pencils", (9, 4, 4), 0, ([1, 2, 0], [0, 2, 1]))])
+def test_structure_factor_stacks_match_oracle(stack, shape_xyz, ng, pairs):
+    """The quasi-2-D per-slice and quasi-1-D per-pencil structure factors (one
+    batched cuFFT over the members) and the reference's averaged output of them
+    against the NumPy restatement (one StructFact per member, AddToExternal in
+    member order, 1/members): norm-relative error below 1e-12, with a reset."""
+    from oracle.structfact import StructFactStackOracle
+    nvar = 3
+    rng = np.random.default_rng(11)
+    ncov = len(pairs[0]) if pairs else nvar * (nvar + 1) // 2
+    scaling = list(rng.uniform(0.5, 2.0, ncov))
+    sf = StructFact(shape_xyz, ["a", "b", "c"], scaling, pairs=pairs, stack=stack)
+    zyx = shape_xyz[::-1]
+    ora = StructFactStackOracle(zyx, stack, nvar, scaling, pairs=pairs)
+    mf = MultiFab(shape_xyz, CELL, nvar, ng, device="cuda")
+    for s in range(4):
+        v = rng.standard_normal((nvar,) + zyx)
+        v[1] = 0.5 * v[0] + 0.2 * v[1]
+        v[2] += np.linspace(0.0, 1.0, zyx[0])[:, None, None]   # members differ
+        mf.valid().copy_(torch.from_numpy(v))
+        reset = 1 if s == 1 else 0
+        sf.fort_structure(mf, reset=reset)
+        ora.fort_structure(v, reset=reset)
+    assert sf.nsamples == ora.nsamples == 3
+    for zero_avg in (0, 1):
+        mag, ri = sf.stack_average(zero_avg)
+        rmag, rri = ora.stack_average(zero_avg)
+        assert mag.valid().shape[1:] == rmag.shape[1:]
+        assert rel(mag.valid().cpu().numpy(), rmag) < 1e-12
+        assert rel(ri.valid().cpu().numpy(), rri) < 1e-12
+    from fhdex_b200.capi import FhdError
+    with pytest.raises(FhdError):
+        sf.finalize()
+    torch.cuda.synchronize()
+    sf.close()

@@ -49,3 +49,34 @@ def test_white_noise_structure_factor_is_flat():
 
 def test_default_pairs_match_reference_order():
     assert default_pairs(3) == ([0, 1, 2, 1, 2, 2], [0, 0, 0, 1, 1, 2])
+
+
+def test_structure_factor_stack_refusals():
+    """Stacks refuse an unknown kind and x pencils of a box with n_cells[1] !=
+    n_cells[2] (the reference's pencil enumeration would leave the box) before
+    touching a device."""
+    import ctypes as C
+    from fhdex_b200 import capi
+    lib = capi.load()
+    h = C.c_void_p()
+    sc = (C.c_double * 1)(1.0)
+    n = (C.c_int * 3)(8, 4, 3)
+    assert lib.fhd_sf_create_stack(C.byref(h), n, 2, 1, 1, None, None, sc, 0) == capi.FHD_ERR_UNSUPPORTED
+    assert lib.fhd_sf_create_stack(C.byref(h), n, 3, 1, 1, None, None, sc, 0) == capi.FHD_ERR_BAD_ARG
+    n1 = (C.c_int * 3)(1, 4, 4)
+    assert lib.fhd_sf_create_stack(C.byref(h), n1, 2, 1, 1, None, None, sc, 0) == capi.FHD_ERR_BAD_ARG
+
+
+def test_stack_oracle_members_are_box_oracles():
+    """A z-slice stack of one slice is the box structure factor of that slice."""
+    import numpy as np
+    from oracle.structfact import StructFactOracle, StructFactStackOracle
+    rng = np.random.default_rng(2)
+    v = rng.standard_normal((2, 1, 6, 8))
+    a = StructFactStackOracle((1, 6, 8), "z_slices", 2, [1.0, 2.0, 0.5])
+    b = StructFactOracle((1, 6, 8), 2, [1.0, 2.0, 0.5])
+    a.fort_structure(v)
+    b.fort_structure(v)
+    mag, ri = a.stack_average(1)
+    re, im, m = b.finalize(1)
+    assert np.array_equal(mag, m * 1.0) and np.array_equal(ri[:3], re) and np.array_equal(ri[3:], im)
