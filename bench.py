@@ -899,7 +899,9 @@ def run_sf(args):
     var.valid(1).copy_(st.cu.valid(4))
     var.valid(2).copy_(st.prim.valid(4))
     var.valid(3).copy_(st.cu.valid(1))
-    sf = StructFact(p.n_cells, ["rho", "rhoE", "T", "jx"], [1.0] * (nvar * (nvar + 1) // 2))
+    stack = None if args.sf_stack == "none" else args.sf_stack
+    nmem = {None: 1, "z_slices": p.n_cells[2], "x_pencils": p.n_cells[1] * p.n_cells[2]}[stack]
+    sf = StructFact(p.n_cells, ["rho", "rhoE", "T", "jx"], [1.0] * (nvar * (nvar + 1) // 2), stack=stack)
     for s in range(args.warmup):
         sf.fort_structure(var)
     torch.cuda.synchronize()
@@ -919,7 +921,9 @@ def run_sf(args):
     print(json.dumps({"mode": "sf", "metric": "structure-factor samples x cells / s", "unit": "cell-samples/s",
                       "value": cells / (ms / 1e3), "ms_per_sample": ms, "steps": args.steps, "nvar": nvar,
                       "ncov": sf.ncov, "config": {"workload": f"StructFact of 4 variables, 10 pairs, "
-                                                              f"{p.n_cells[0]}^3"},
+                                                              f"{p.n_cells[0]}^3"
+                                                              + ("" if stack is None else
+                                                                 f", one per {stack[2:-1]} ({nmem} members)")},
                       "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                                    "frac": achieved / peak, "peak_kind": peak_kind,
                                    "algorithmic_bytes_per_launch": alg,
@@ -1057,6 +1061,8 @@ def main():
     ap.add_argument("--dx", type=float, default=8e-6)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--tile", default="auto")
+    ap.add_argument("--sf-stack", default="none", choices=["none", "z_slices", "x_pencils"],
+                    help="--mode sf: the quasi-2-D per-slice or quasi-1-D per-pencil stack")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
