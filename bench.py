@@ -912,6 +912,13 @@ def run_sf(args):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
+    avg_ms = None
+    if stack is not None:   # the output loop, once (it runs at plot time, not per sample)
+        e0.record()
+        sf.stack_average()
+        e1.record()
+        torch.cuda.synchronize()
+        avg_ms = e0.elapsed_time(e1)
     cells = p.n_cells[0] * p.n_cells[1] * p.n_cells[2]
     # per point: pack (read + write 8 B), FFT (read 8 B, write the 8 B half spectrum) and
     # the accumulation's spectrum read (8 B) per variable; covariance read + write per pair
@@ -919,7 +926,8 @@ def run_sf(args):
     peak, peak_kind = measured_peak()
     achieved = alg / (ms / 1e3) / 1e9
     print(json.dumps({"mode": "sf", "metric": "structure-factor samples x cells / s", "unit": "cell-samples/s",
-                      "value": cells / (ms / 1e3), "ms_per_sample": ms, "steps": args.steps, "nvar": nvar,
+                      "value": cells / (ms / 1e3), "ms_per_sample": ms, "stack_average_ms": avg_ms,
+                      "steps": args.steps, "nvar": nvar,
                       "ncov": sf.ncov, "config": {"workload": f"StructFact of 4 variables, 10 pairs, "
                                                               f"{p.n_cells[0]}^3"
                                                               + ("" if stack is None else

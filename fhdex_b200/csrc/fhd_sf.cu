@@ -163,14 +163,18 @@ struct SfAvgArgs {
 // The reference's stack output loop (main_driver.cpp:1592-1618, 1683-1711): for
 // every member in order, AddToExternal (StructFact.cpp:979-1009: Finalize of a
 // copy, then x_mag += mag, x_realimag += (re, im), from zero), then both outputs
-// times 1/members.  One thread per member point (i, j, k) owns its shifted
-// destination and walks the members.
+// times 1/members.  One thread per (pair, member point): it owns that pair's
+// shifted destination and walks the members in order (a pencil stack has only
+// n_cells[0] points, so the pairs multiply the independent chains).
 __global__ void __launch_bounds__(256) k_sf_stack_avg(SfAvgArgs a) {
-    for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < a.Nm; l += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t tot = a.Nm * a.ncov;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot; t += (int64_t)gridDim.x * blockDim.x) {
+        const int c = int(t / a.Nm);
+        const int64_t l = t - (int64_t)c * a.Nm;
         const int i = int(l % a.nx), j = int((l / a.nx) % a.ny), k = int(l / ((int64_t)a.nx * a.ny));
         const int ip = (i + a.nx / 2) % a.nx, jp = (j + a.ny / 2) % a.ny, kp = (k + a.nz / 2) % a.nz;
         const bool zero = a.zero_avg == 1 && i == 0 && j == 0 && k == 0;
-        for (int c = 0; c < a.ncov; ++c) {
+        {
             double sm = 0.0, sr = 0.0, si = 0.0;
             for (int64_t b = 0; b < a.nmem; ++b) {
                 const int64_t q = b * a.Nm + l;
@@ -456,7 +460,7 @@ int fhd_sf_stack_average(fhd_sf* s, fhd_fab mag, fhd_fab realimag, int zero_avg)
     a.scale = s->dscale;
     a.omag = view<double>(mag);
     a.ori = view<double>(realimag);
-    k_sf_stack_avg<<<grid_for(a.Nm, 256), 256, 0, s->stream>>>(a);
+    k_sf_stack_avg<<<grid_for(a.Nm * a.ncov, 256), 256, 0, s->stream>>>(a);
     return cuda_rc(cudaGetLastError());
 }
 
